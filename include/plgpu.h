@@ -1,0 +1,226 @@
+/*
+ * plgpu.h -- C ABI of libplgpu, the B200 (sm_100a) implementation of ProtLocus's
+ * alignment hot path.
+ *
+ * The library is a drop-in for the reference's GPU translation units
+ * (nasw-cuda.o, nasw-ext-gpu.o, hmm-gpu.o): it exports the same symbols with the
+ * same signatures and semantics, so the reference's map.c / align.c / hmm.c link
+ * against it unchanged (swap the objects in the reference Makefile's OBJS).
+ *
+ * Plain C, no CUDA or torch types.  Every declaration cites the reference
+ * interface it replaces as file:line within the reference project.
+ *
+ * Types ns_opt_t / ns_rst_t are layout-identical to nasw.h:62-82; when nasw.h
+ * has already been included its definitions are used instead.
+ */
+#ifndef PLGPU_H
+#define PLGPU_H
+
+#include <stdint.h>
+#include <string.h>
+
+#ifndef NASW_H
+/* CIGAR operators (nasw.h:33-44) */
+#define NS_CIGAR_M	0
+#define NS_CIGAR_I	1
+#define NS_CIGAR_D	2
+#define NS_CIGAR_N	3
+#define NS_CIGAR_F	10
+#define NS_CIGAR_G	11
+#define NS_CIGAR_U	12
+#define NS_CIGAR_V	13
+#define NS_CIGAR_E	14
+#define NS_CIGAR_STR   "MIDNSHP=XBFGUVE"
+
+/* option flags (nasw.h:46-49) */
+#define NS_F_CIGAR      0x1
+#define NS_F_EXT_LEFT   0x2
+#define NS_F_EXT_RIGHT  0x4
+#define NS_F_GPU        0x8
+
+#define NS_SPSC_OFFSET 64  /* nasw.h:55 */
+
+/* alignment options; must stay layout-identical to nasw.h:62-75 */
+typedef struct {
+	int32_t flag;
+	int32_t go, ge, io, fs;
+	int32_t xdrop, end_bonus;
+	int32_t asize;
+	int32_t gpu_device;
+	int64_t gpu_min_cells;
+	int32_t sp[6];
+	int32_t sp_null_bonus;
+	float ie_coef;
+	const int8_t *sc;
+	const int8_t *pssm;
+	uint8_t *nt4, *aa20, *codon;
+} ns_opt_t;
+
+/* alignment result; layout-identical to nasw.h:77-82 */
+typedef struct {
+	int32_t n_cigar, m_cigar;
+	int32_t nt_len, aa_len;
+	int32_t score;
+	uint32_t *cigar;
+} ns_rst_t;
+
+typedef struct ns_gpu_request_s ns_gpu_request_t;
+
+/* gapless prefilter records (nasw.h:157-171) */
+typedef struct {
+	int64_t target_offset, target_length;
+	int64_t query_offset;
+	int32_t query_length;
+	int32_t anchor_offset, anchor_count;
+	int32_t reverse;
+} ns_gpu_gapless_candidate_t;
+typedef struct {
+	int64_t target_block;
+	int32_t query_end;
+	int32_t reserved;
+} ns_gpu_gapless_anchor_t;
+typedef struct {
+	uint64_t batches, candidates, anchors, seed_positions;
+} ns_gpu_gapless_profile_t;
+
+typedef struct ns_ext_batch_s ns_ext_batch_t;
+#endif /* NASW_H */
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------------
+ * Spliced global DP with CIGAR (replaces nasw-cuda.cu:516-1145)
+ * ------------------------------------------------------------------------- */
+
+/* nasw.h:141 -- 1 when the device is ready; idempotent and thread-safe. */
+int ns_gpu_init(int32_t device);
+/* nasw.h:142 -- text of the last error ("none" when healthy). */
+const char *ns_gpu_error(void);
+/* nasw.h:143 -- device name, "none" before ns_gpu_init(). */
+const char *ns_gpu_name(void);
+/* nasw.h:144 -- requests completed on the device (monotonic). */
+uint64_t ns_gpu_dispatch_count(void);
+/* nasw.h:145 -- kernel launches of the request path (monotonic). */
+uint64_t ns_gpu_launch_count(void);
+/* nasw.h:146-148 -- accumulated host-observed phase times. */
+double ns_gpu_h2d_seconds(void);
+double ns_gpu_kernel_seconds(void);
+double ns_gpu_d2h_seconds(void);
+/* nasw.h:150 -- queue one global spliced DP.  NULL when not taken: nl < 3,
+ * al < 1, al*max(sc)+end_bonus > 30000 (the 16-bit contract), or device not
+ * ready.  A non-NULL request must be consumed exactly once by ns_gpu_wait();
+ * km must stay valid until then.  Thread-safe. */
+ns_gpu_request_t *ns_gpu_submit(void *km, const char *ns, int32_t nl, const char *as, int32_t al,
+		const ns_opt_t *opt, const uint8_t *ss);
+/* nasw.h:151 -- block until done; 1 = r filled (nt_len, aa_len, score and the
+ * CIGAR appended into r->cigar from the request's km), 0 = failed.  Frees the
+ * request either way. */
+int ns_gpu_wait(ns_gpu_request_t *request, ns_rst_t *r);
+/* nasw.h:152 -- submit + wait. */
+int ns_gpu_global(void *km, const char *ns, int32_t nl, const char *as, int32_t al,
+		const ns_opt_t *opt, const uint8_t *ss, ns_rst_t *r);
+
+/* ---------------------------------------------------------------------------
+ * Gapless 3-frame X-drop prefilter (replaces nasw-cuda.cu:1151-1412)
+ * ------------------------------------------------------------------------- */
+
+/* nasw.h:172 */
+void ns_gpu_gapless_profile(ns_gpu_gapless_profile_t *profile);
+/* nasw.h:173 */
+int ns_gpu_gapless_supported(void);
+/* nasw.h:174 */
+void ns_gpu_gapless_reset_target(void);
+/* nasw.h:178-184 -- 1 = scores[] filled (INT32_MIN: no usable seed). */
+int ns_gpu_gapless_score_batch(const uint8_t *packed_nt, int64_t packed_nt_bases,
+		const uint8_t *queries, int64_t query_aa,
+		const ns_gpu_gapless_candidate_t *candidates, int32_t n_candidates,
+		const ns_gpu_gapless_anchor_t *anchors, int64_t n_anchors,
+		int32_t block_width, int32_t kmer, int32_t xdrop,
+		const int8_t *score_matrix, int32_t asize, const uint8_t *codon,
+		int32_t *scores);
+
+/* ---------------------------------------------------------------------------
+ * Batched end-extension DP (replaces nasw-ext-gpu.c:931-1114)
+ * ------------------------------------------------------------------------- */
+
+/* nasw.h:204 */
+ns_ext_batch_t *ns_ext_batch_init(void *km);
+/* nasw.h:205 */
+int32_t ns_ext_batch_add(ns_ext_batch_t *b, const char *ns, int32_t nl, const char *as, int32_t al,
+		const ns_opt_t *opt, const uint8_t *ss);
+/* nasw.h:206 */
+int32_t ns_ext_batch_flush(ns_ext_batch_t *b);
+/* nasw.h:207 */
+int ns_ext_batch_ready(ns_ext_batch_t *b, int32_t id);
+/* nasw.h:208 */
+void ns_ext_batch_wait(ns_ext_batch_t *b);
+/* nasw.h:209 */
+const ns_rst_t *ns_ext_batch_get(ns_ext_batch_t *b, int32_t id);
+/* nasw.h:210 */
+void ns_ext_batch_destroy(ns_ext_batch_t *b);
+/* nasw.h:211-212 */
+uint64_t ns_ext_gpu_launch_count(void);
+uint64_t ns_ext_gpu_request_count(void);
+
+/* ---------------------------------------------------------------------------
+ * Bulk entry points (no counterpart in the reference: the reference only has
+ * the per-request queue above).  They take many DP jobs at once, with the
+ * length binning, the persistent wavefront kernel and the device traceback
+ * exposed directly.  Used by the benchmark and by callers that already hold
+ * a whole batch.
+ * ------------------------------------------------------------------------- */
+
+/* One global spliced DP job inside packed buffers. */
+typedef struct {
+	int64_t nt_off;   /* first nucleotide in the packed nt buffer (ASCII or 0-4 codes) */
+	int64_t aa_off;   /* first residue in the packed protein buffer (ASCII) */
+	int64_t ss_off;   /* splice-score track offset in the ss buffer, -1 = none */
+	int32_t nl, al;
+} pl_splice_job_t;
+
+/* Result of one job.  cigar_off indexes the caller's CIGAR buffer; the CIGAR
+ * has exactly the words ns_global_gs_auto() (nasw-sse.c:980) would produce. */
+typedef struct {
+	int32_t score;
+	int32_t n_cigar;
+	int64_t cigar_off;
+	int32_t mode;      /* 16 or 32: the DP width the job ran at (ns_global_gs_auto's rule) */
+	int32_t status;    /* 0 = ok; <0 = error (see pl_last_error()) */
+} pl_splice_result_t;
+
+typedef struct pl_engine_s pl_engine_t;
+
+/* Create an engine on the current CUDA device.  trace_budget_bytes bounds the
+ * device traceback arena (jobs run in waves that fit); 0 = default. */
+pl_engine_t *pl_engine_create(int32_t device, int64_t trace_budget_bytes);
+void pl_engine_destroy(pl_engine_t *e);
+const char *pl_last_error(void);
+
+/* Host buffers in, host results out (H2D, kernels and D2H inside).
+ * cigar_cap is the capacity of `cigar` in words; each job may need up to
+ * nl + al + 4 words.  Returns 1 on success. */
+int pl_splice_batch_host(pl_engine_t *e, const ns_opt_t *opt,
+		const pl_splice_job_t *jobs, int32_t n_jobs,
+		const uint8_t *nt, int64_t nt_len, const uint8_t *aa, int64_t aa_len,
+		const uint8_t *ss, int64_t ss_len,
+		pl_splice_result_t *results, uint32_t *cigar, int64_t cigar_cap);
+
+/* Device buffers in and out (all pointers are device pointers; `jobs` too),
+ * launched on `stream` (a cudaStream_t passed as void*, NULL = default).
+ * Synchronous with respect to the stream.  Returns 1 on success. */
+int pl_splice_batch_device(pl_engine_t *e, const ns_opt_t *opt,
+		const pl_splice_job_t *jobs_host, const pl_splice_job_t *jobs_dev, int32_t n_jobs,
+		const uint8_t *nt, const uint8_t *aa, const uint8_t *ss,
+		pl_splice_result_t *results_dev, uint32_t *cigar_dev, int64_t cigar_cap,
+		void *stream);
+
+/* Kernel launches issued by this library since load (all entry points). */
+uint64_t pl_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PLGPU_H */

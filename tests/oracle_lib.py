@@ -1,0 +1,114 @@
+"""Test-side access to the oracle (test infrastructure only).
+
+Two CPU implementations of the reference algorithm are loaded through ctypes:
+  * ``ref``  -- the reference's own CPU code (nasw-sse.c, nasw-tab.c, kalloc.c,
+    hmm.c) compiled from its sources by oracle/Makefile into oracle/_ref/;
+  * ``port`` -- this repository's C restatement (oracle/ns_port.c etc.) built
+    into oracle/_build/.
+Both are checkers only; the product path never loads them.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import platform
+import subprocess
+
+from protlocus_b200.abi import NsOpt, NsRst
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE = os.path.join(ROOT, "oracle")
+REF_SO = os.path.join(ORACLE, "_ref", "libnsref.so")
+PORT_SO = os.path.join(ORACLE, "_build", "libnsport.so")
+
+_ref = None
+_port = None
+_libc = C.CDLL(None)
+_libc.free.argtypes = [C.c_void_p]
+
+
+def build_port():
+    if not os.path.exists(PORT_SO):
+        subprocess.run(["make", "-C", ORACLE, "port"], check=True, capture_output=True)
+
+
+def ref_lib():
+    """The compiled reference, or None when oracle/_ref was not built on this machine."""
+    global _ref
+    if _ref is None and os.path.exists(REF_SO):
+        lib = C.CDLL(REF_SO)
+        if lib.ns_make_tables(1) != 0:
+            raise RuntimeError("reference ns_make_tables(1) failed")
+        for fn in ("ns_global_gs16b", "ns_global_gs32b", "ns_global_gs_auto"):
+            f = getattr(lib, fn)
+            f.argtypes = [C.c_void_p, C.c_char_p, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(NsOpt),
+                          C.c_void_p, C.POINTER(NsRst)]
+            f.restype = None
+        lib.ns_ext_stripe_width.argtypes = [C.POINTER(NsOpt), C.c_int32]
+        lib.ns_ext_stripe_width.restype = C.c_int32
+        _ref = lib
+    return _ref
+
+
+def port_lib():
+    global _port
+    if _port is None:
+        build_port()
+        lib = C.CDLL(PORT_SO)
+        lib.port_global_gs16b.argtypes = [C.c_char_p, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(NsOpt),
+                                          C.c_void_p, C.POINTER(NsRst), C.c_int32]
+        lib.port_global_gs32b.argtypes = [C.c_char_p, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(NsOpt),
+                                          C.c_void_p, C.POINTER(NsRst)]
+        lib.port_global_gs_auto.argtypes = lib.port_global_gs16b.argtypes
+        lib.port_needs_wide.argtypes = [C.POINTER(NsOpt), C.c_int32]
+        lib.port_needs_wide.restype = C.c_int32
+        _port = lib
+    return _port
+
+
+def host_avx2() -> bool:
+    """Whether the reference CPU kernel dispatches ext DPs to AVX2 on this host."""
+    if platform.machine() not in ("x86_64", "AMD64"):
+        return False
+    try:
+        with open("/proc/cpuinfo") as f:
+            return " avx2" in f.read()
+    except OSError:
+        return False
+
+
+def _take(r: NsRst):
+    cig = [r.cigar[k] for k in range(r.n_cigar)] if r.n_cigar else []
+    if r.cigar:
+        _libc.free(C.cast(r.cigar, C.c_void_p))
+    return (r.score, r.nt_len, r.aa_len, cig)
+
+
+def _buf(x):
+    if x is None:
+        return None
+    if isinstance(x, (bytes, bytearray)):
+        return C.c_char_p(bytes(x))
+    return C.c_char_p(bytes(x))
+
+
+def ref_run(fn: str, ns: bytes, aa: bytes, opt, ss: bytes | None = None):
+    """Run reference `fn` (ns_global_gs16b / gs32b / gs_auto); returns (score, nt_len, aa_len, cigar)."""
+    lib = ref_lib()
+    r = NsRst()
+    ssb = C.create_string_buffer(bytes(ss), len(ss)) if ss is not None else None
+    getattr(lib, fn)(None, ns, len(ns), aa, len(aa), opt.ptr, ssb, C.byref(r))
+    return _take(r)
+
+
+def port_run(fn: str, ns: bytes, aa: bytes, opt, ss: bytes | None = None, avx2: bool | None = None):
+    lib = port_lib()
+    r = NsRst()
+    ssb = C.create_string_buffer(bytes(ss), len(ss)) if ss is not None else None
+    if avx2 is None:
+        avx2 = host_avx2()
+    if fn == "gs32b":
+        lib.port_global_gs32b(ns, len(ns), aa, len(aa), opt.ptr, ssb, C.byref(r))
+    else:
+        getattr(lib, "port_global_" + fn)(ns, len(ns), aa, len(aa), opt.ptr, ssb, C.byref(r), int(avx2))
+    return _take(r)
