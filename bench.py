@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Benchmark of the batched global spliced DP (the alignment hot path).
+
+One step = one pass of the hot path over the batched workload: 4096 synthetic
+protein/window pairs searched on both strands (8192 global spliced DPs with
+CIGAR): input preparation, the wavefront DP, device traceback and CIGAR
+compaction.  Metric: GCUPS, cells = (nl-2)*al per DP (nasw-cuda.cu:793),
+bit-exact with the reference CPU path.
+
+  value   device-resident inputs (uploaded once), pl_splice_batch_device per step,
+          CUDA events on the launching stream, max over ranks
+  e2e     pl_splice_batch_host per step from pinned host buffers: H2D of the
+          step's inputs, all kernels, D2H of the results and CIGARs
+  roofline  the DP kernel (k_splice_dp): algorithmic int16 lane-ops per cell
+          (65 with traceback, counted from the reference SSE kernel) x cells,
+          divided by the DP kernel's own CUDA-event time, against the integer
+          pipe's lane-op peak measured live on this device (pl_measure_int_peak)
+  cpu_baseline  the reference's ns_global_gs_auto compiled from its own sources
+          (oracle/_ref), driven by the reference's kt_for over all host cores, on
+          a bounded random sample of the same jobs
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun each rank runs its own batch (seed 1+rank): weak scaling, no
+collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import signal
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from protlocus_b200 import lib as L  # noqa: E402
+from protlocus_b200 import workload as W  # noqa: E402
+from protlocus_b200.abi import NS_F_CIGAR, Options, SpliceJob, SpliceResult  # noqa: E402
+
+METRIC = "spliced-DP GCUPS (bit-exact) at 1 B200"
+OPS_PER_CELL = 65  # int16 lane-ops per cell with traceback bits, counted from nasw-sse.c:465-553
+WORKLOAD = ("batched global spliced DP: 4096 protein/window pairs x 2 strands = 8192 DPs with CIGAR; "
+            "protein log-normal median 350 aa (50-2500), window uniform 1-50 kb, Poisson(4) introns, "
+            "25% divergence, ProtLocus default scoring")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--pairs", type=int, default=4096)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def pack(jobs):
+    n = len(jobs)
+    nl = np.array([len(a) for a, _ in jobs], dtype=np.int32)
+    al = np.array([len(b) for _, b in jobs], dtype=np.int32)
+    nt_off = np.zeros(n, dtype=np.int64)
+    aa_off = np.zeros(n, dtype=np.int64)
+    nt_off[1:] = np.cumsum(nl[:-1])
+    aa_off[1:] = np.cumsum(al[:-1])
+    nt = np.frombuffer(b"".join(a for a, _ in jobs), dtype=np.uint8)
+    aa = np.frombuffer(b"".join(b for _, b in jobs), dtype=np.uint8)
+    tab = (SpliceJob * n)()
+    for q in range(n):
+        tab[q].nt_off, tab[q].aa_off, tab[q].ss_off, tab[q].nl, tab[q].al = nt_off[q], aa_off[q], -1, nl[q], al[q]
+    return nt, aa, nt_off, aa_off, nl, al, tab
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.send_signal(signal.SIGTERM)
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(", ") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows if len(r) >= 9 for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(jobs, nt, aa, nt_off, aa_off, nl, al, opt, target_s, steps=1):
+    """The reference CPU path over a bounded random sample, all host threads.
+    Returns (GCUPS, threads, kind, sample description, seconds per step)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    threads = os.cpu_count() or 1
+    ref = O.ref_lib()
+    if ref is not None:
+        fn, kind = ref.ref_bench_global, "reference"
+    else:
+        fn, kind = O.port_lib().port_bench_global, "port"
+    fn.restype = C.c_double
+    fn.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                   C.c_void_p, C.c_void_p, C.c_void_p]
+    n = len(nl)
+    rng = np.random.default_rng(12345)
+    perm = rng.permutation(n)
+    cells = (nl.astype(np.int64) - 2) * al
+    # calibrate on a small sample: ~0.5 GCUPS per thread for the SSE kernel
+    budget = target_s * 0.5e9 * threads
+    take, acc = [], 0
+    for q in perm:
+        if acc + cells[q] > budget and take:
+            continue
+        take.append(q)
+        acc += int(cells[q])
+        if acc >= budget:
+            break
+    take = np.array(sorted(take), dtype=np.int64)
+    s_nl, s_al = nl[take].copy(), al[take].copy()
+    s_nt_off, s_aa_off = nt_off[take].copy(), aa_off[take].copy()
+    score = np.zeros(len(take), dtype=np.int32)
+    ncig = np.zeros(len(take), dtype=np.int32)
+    secs = []
+    for _ in range(steps):
+        t = fn(threads, len(take), nt.ctypes.data, s_nt_off.ctypes.data, s_nl.ctypes.data, aa.ctypes.data,
+               s_aa_off.ctypes.data, s_al.ctypes.data, C.addressof(opt.c), score.ctypes.data, ncig.ctypes.data)
+        secs.append(t)
+    sample = (f"{len(take)} of {n} DP jobs (seeded random subset, {acc / 1e9:.2f} G cells), ns_global_gs_auto "
+              f"with CIGAR, {threads} threads via kt_for")
+    return acc / min(secs) / 1e9, threads, kind, sample, secs, acc
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    jobs = W.batch_pairs(args.pairs, seed=1)
+    nt, aa, nt_off, aa_off, nl, al, _ = pack(jobs)
+    opt = Options(flag=NS_F_CIGAR)
+    per_step = args.cpu_seconds / 2
+    gcups_w, threads, kind, sample, secs_w, cells = cpu_baseline(jobs, nt, aa, nt_off, aa_off, nl, al, opt,
+                                                                 per_step, steps=max(args.warmup, 0) or 1)
+    gcups, threads, kind, sample, secs, cells = cpu_baseline(jobs, nt, aa, nt_off, aa_off, nl, al, opt, per_step,
+                                                             steps=args.steps)
+    total = sum(secs)
+    value = cells * len(secs) / total / 1e9
+    line = {"metric": METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total / len(secs) * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "n_jobs": int(len(nl)), "step": "bounded sample of the workload"},
+            "cpu_baseline": {"value": round(value, 3), "unit": "GCUPS", "cores": threads, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": round(value, 3), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    jobs = W.batch_pairs(args.pairs, seed=1 + rank)
+    nt, aa, nt_off, aa_off, nl, al, tab = pack(jobs)
+    n = len(jobs)
+    cells = int(((nl.astype(np.int64) - 2) * al).sum())
+    opt = Options(flag=NS_F_CIGAR)
+    eng = L.Engine(local)
+    cap = n * 4096
+    d_nt = torch.from_numpy(nt.copy()).to("cuda")
+    d_aa = torch.from_numpy(aa.copy()).to("cuda")
+    d_res = torch.zeros(n * C.sizeof(SpliceResult), dtype=torch.uint8, device="cuda")
+    d_cig = torch.zeros(cap, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    total = C.c_int64()
+
+    def step_device():
+        ok = eng.lib.pl_splice_batch_device(eng.h, opt.ptr, tab, n, d_nt.data_ptr(), d_aa.data_ptr(), None,
+                                            d_res.data_ptr(), d_cig.data_ptr(), cap, C.byref(total),
+                                            stream.cuda_stream)
+        if not ok:
+            raise RuntimeError("pl_splice_batch_device: " + L.error())
+
+    for _ in range(args.warmup):
+        step_device()
+    res = (SpliceResult * n).from_buffer_copy(d_res.cpu().numpy().tobytes())
+    bad = sum(1 for r in res if r.status != 0)
+    if bad:
+        raise RuntimeError(f"{bad} jobs failed")
+    int32_peak, i16x2_peak = L.measure_int_peak(local)
+    peak = max(int32_peak, i16x2_peak)
+
+    clocks = Clocks(local)
+    eng.set_timing(True)
+    launches0 = L.load().pl_kernel_launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step_device()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = L.load().pl_kernel_launch_count() - launches0
+    t = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    value = world * cells * args.steps / t / 1e9
+    tm = eng.times()
+    plan = eng.last_plan()
+    dp_s = tm["dp_ms"] / 1e3
+    achieved = tm["cells"] * OPS_PER_CELL / dp_s if dp_s > 0 else 0.0
+    dp_gcups = tm["cells"] / dp_s / 1e9 if dp_s > 0 else 0.0
+
+    e2e = None
+    if not args.no_e2e:
+        h_nt = torch.from_numpy(nt.copy()).pin_memory()
+        h_aa = torch.from_numpy(aa.copy()).pin_memory()
+        h_cig = torch.zeros(cap, dtype=torch.int32).pin_memory()
+        h_res = (SpliceResult * n)()
+        est = torch.cuda.ExternalStream(eng.stream)
+
+        def step_host():
+            ok = eng.lib.pl_splice_batch_host(eng.h, opt.ptr, tab, n, h_nt.data_ptr(), h_nt.numel(), h_aa.data_ptr(),
+                                              h_aa.numel(), None, 0, h_res, h_cig.data_ptr(), cap)
+            if not ok:
+                raise RuntimeError("pl_splice_batch_host: " + L.error())
+
+        for _ in range(max(1, args.warmup)):
+            step_host()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(est)
+        for _ in range(args.steps):
+            step_host()
+        e1.record(est)
+        torch.cuda.synchronize()
+        barrier()
+        te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+        d2h = n * C.sizeof(SpliceResult) + 4 * sum(h_res[q].n_cigar for q in range(n))
+        e2e = {"value": round(world * cells * args.steps / te / 1e9, 3), "unit": "GCUPS",
+               "h2d_bytes_per_step": int(nt.nbytes + aa.nbytes + n * C.sizeof(SpliceJob)),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": round(te / args.steps * 1e3, 2),
+               "api": "pl_splice_batch_host (C ABI, pinned host buffers)"}
+
+    cpu = None
+    if rank == 0:
+        gcups, threads, kind, sample, _secs, _acc = cpu_baseline(jobs, nt, aa, nt_off, aa_off, nl, al, opt,
+                                                                 args.cpu_seconds)
+        cpu = {"value": round(gcups, 3), "unit": "GCUPS", "cores": threads, "kind": kind, "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(t / args.steps * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_jobs": n, "cells_per_step": cells, "seed": "1+rank",
+                       "l2": "inputs and the per-step traceback arena (tens of GB) are far larger than L2",
+                       "waves": plan["waves"], "coop_jobs": plan["coop"], "parallelism": f"{world} independent ranks"},
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "int", "kernel": "k_splice_dp", "achieved": achieved, "peak": peak,
+                         "unit": "lane-ops/s", "frac": achieved / peak if peak else None, "traffic": None,
+                         "ops_per_cell": OPS_PER_CELL, "dp_kernel_gcups": round(dp_gcups, 3),
+                         "peak_source": "measured live: pl_measure_int_peak (int32 %.3g, int16x2 %.3g lane-ops/s)"
+                                        % (int32_peak, i16x2_peak),
+                         "phase_ms_per_step": {k: round(v / args.steps, 2) for k, v in tm.items() if k.endswith("_ms")}},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -123,48 +123,6 @@ int ns_gpu_global(void *km, const char *ns, int32_t nl, const char *as, int32_t 
 		const ns_opt_t *opt, const uint8_t *ss, ns_rst_t *r);
 
 /* ---------------------------------------------------------------------------
- * Gapless 3-frame X-drop prefilter (replaces nasw-cuda.cu:1151-1412)
- * ------------------------------------------------------------------------- */
-
-/* nasw.h:172 */
-void ns_gpu_gapless_profile(ns_gpu_gapless_profile_t *profile);
-/* nasw.h:173 */
-int ns_gpu_gapless_supported(void);
-/* nasw.h:174 */
-void ns_gpu_gapless_reset_target(void);
-/* nasw.h:178-184 -- 1 = scores[] filled (INT32_MIN: no usable seed). */
-int ns_gpu_gapless_score_batch(const uint8_t *packed_nt, int64_t packed_nt_bases,
-		const uint8_t *queries, int64_t query_aa,
-		const ns_gpu_gapless_candidate_t *candidates, int32_t n_candidates,
-		const ns_gpu_gapless_anchor_t *anchors, int64_t n_anchors,
-		int32_t block_width, int32_t kmer, int32_t xdrop,
-		const int8_t *score_matrix, int32_t asize, const uint8_t *codon,
-		int32_t *scores);
-
-/* ---------------------------------------------------------------------------
- * Batched end-extension DP (replaces nasw-ext-gpu.c:931-1114)
- * ------------------------------------------------------------------------- */
-
-/* nasw.h:204 */
-ns_ext_batch_t *ns_ext_batch_init(void *km);
-/* nasw.h:205 */
-int32_t ns_ext_batch_add(ns_ext_batch_t *b, const char *ns, int32_t nl, const char *as, int32_t al,
-		const ns_opt_t *opt, const uint8_t *ss);
-/* nasw.h:206 */
-int32_t ns_ext_batch_flush(ns_ext_batch_t *b);
-/* nasw.h:207 */
-int ns_ext_batch_ready(ns_ext_batch_t *b, int32_t id);
-/* nasw.h:208 */
-void ns_ext_batch_wait(ns_ext_batch_t *b);
-/* nasw.h:209 */
-const ns_rst_t *ns_ext_batch_get(ns_ext_batch_t *b, int32_t id);
-/* nasw.h:210 */
-void ns_ext_batch_destroy(ns_ext_batch_t *b);
-/* nasw.h:211-212 */
-uint64_t ns_ext_gpu_launch_count(void);
-uint64_t ns_ext_gpu_request_count(void);
-
-/* ---------------------------------------------------------------------------
  * Bulk entry points (no counterpart in the reference: the reference only has
  * the per-request queue above).  They take many DP jobs at once, with the
  * length binning, the persistent wavefront kernel and the device traceback
@@ -207,14 +165,34 @@ int pl_splice_batch_host(pl_engine_t *e, const ns_opt_t *opt,
 		const uint8_t *ss, int64_t ss_len,
 		pl_splice_result_t *results, uint32_t *cigar, int64_t cigar_cap);
 
-/* Device buffers in and out (all pointers are device pointers; `jobs` too),
- * launched on `stream` (a cudaStream_t passed as void*, NULL = default).
- * Synchronous with respect to the stream.  Returns 1 on success. */
+/* Device-resident inputs and outputs: nt/aa/ss/results/cigar are device
+ * pointers; the job table is read on the host (it drives the planning).
+ * Work is issued on `stream` (a cudaStream_t passed as void*, NULL = the
+ * engine's own stream) and the call returns once it has completed.
+ * *total_cigar (optional) receives the number of CIGAR words produced; jobs
+ * beyond cigar_cap get status -2.  Returns 1 on success. */
 int pl_splice_batch_device(pl_engine_t *e, const ns_opt_t *opt,
-		const pl_splice_job_t *jobs_host, const pl_splice_job_t *jobs_dev, int32_t n_jobs,
+		const pl_splice_job_t *jobs, int32_t n_jobs,
 		const uint8_t *nt, const uint8_t *aa, const uint8_t *ss,
 		pl_splice_result_t *results_dev, uint32_t *cigar_dev, int64_t cigar_cap,
-		void *stream);
+		int64_t *total_cigar, void *stream);
+
+/* Optional CUDA-event timing of every batch phase (prep, DP kernel, traceback,
+ * compaction), accumulated until the next pl_engine_set_timing() call. */
+int pl_engine_set_timing(pl_engine_t *e, int32_t enable);
+void pl_engine_times(const pl_engine_t *e, double *prep_ms, double *dp_ms, double *traceback_ms,
+		double *compact_ms, int64_t *dp_launches, int64_t *cells);
+
+/* The engine's own CUDA stream (a cudaStream_t as void*). */
+void *pl_engine_stream(const pl_engine_t *e);
+
+/* Measured integer-pipe throughput of a device, in lane-operations per second:
+ * int32 add+max chains and int16x2 (__vadd2 + __vmaxs2) chains at full
+ * occupancy.  The DP kernels are bound by this pipe.  Returns 1 on success. */
+int pl_measure_int_peak(int32_t device, double *int32_lane_ops, double *int16x2_lane_ops);
+
+/* Number of trace waves, cooperative jobs and DP launches of the last batch. */
+void pl_engine_last_plan(const pl_engine_t *e, int32_t *n_waves, int32_t *n_coop, int32_t *n_dp_launches);
 
 /* Kernel launches issued by this library since load (all entry points). */
 uint64_t pl_kernel_launch_count(void);

@@ -1,0 +1,49 @@
+/*
+ * ref_bench.c -- ORACLE timing driver (test/bench infrastructure only).
+ *
+ * Linked into oracle/_ref/libnsref.so next to the reference's nasw-sse.c,
+ * nasw-tab.c, kalloc.c and kthread.c.  Runs the reference CPU path
+ * ns_global_gs_auto (nasw-sse.c:980-999) with NS_F_CIGAR over a list of jobs,
+ * spread over host threads with the reference's own kt_for (kthread.c:54), the
+ * way the mapping pipeline drives it.  Used as bench.py's CPU baseline and by
+ * `bench.py --impl reference`.
+ */
+#define _POSIX_C_SOURCE 200809L
+#include <stdint.h>
+#include <stdlib.h>
+#include <time.h>
+#include "nasw.h"
+#include "kthread.h"
+
+typedef struct {
+	const char *nt, *aa;
+	const int64_t *nt_off, *aa_off;
+	const int32_t *nl, *al;
+	const ns_opt_t *opt;
+	int32_t *score, *n_cigar;
+} ref_bench_t;
+
+static void ref_bench_worker(void *data, long i, int tid)
+{
+	ref_bench_t *b = (ref_bench_t*)data;
+	ns_rst_t r;
+	(void)tid;
+	ns_rst_init(&r);
+	ns_global_gs_auto(0, b->nt + b->nt_off[i], b->nl[i], b->aa + b->aa_off[i], b->al[i], b->opt, 0, &r);
+	b->score[i] = r.score, b->n_cigar[i] = r.n_cigar;
+	free(r.cigar);
+}
+
+/* returns wall seconds */
+double ref_bench_global(int32_t n_threads, int32_t n_jobs, const char *nt, const int64_t *nt_off, const int32_t *nl,
+		const char *aa, const int64_t *aa_off, const int32_t *al, const ns_opt_t *opt, int32_t *score, int32_t *n_cigar)
+{
+	ref_bench_t b;
+	struct timespec t0, t1;
+	b.nt = nt, b.aa = aa, b.nt_off = nt_off, b.aa_off = aa_off, b.nl = nl, b.al = al, b.opt = opt;
+	b.score = score, b.n_cigar = n_cigar;
+	clock_gettime(CLOCK_MONOTONIC, &t0);
+	kt_for(n_threads, ref_bench_worker, &b, n_jobs);
+	clock_gettime(CLOCK_MONOTONIC, &t1);
+	return (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
+}

@@ -1,0 +1,80 @@
+/*
+ * plk.h -- plain-C interface between the host layer (plgpu.c) and the sm_100a
+ * kernels (splice.cu).  Only POD structs and C function prototypes; no CUDA
+ * types other than the opaque stream handle passed as void*.
+ */
+#ifndef PLK_H
+#define PLK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PLK_WARPS_PER_CTA 8     /* a CTA is one 256-lane wavefront (large jobs) or 8 independent warps */
+#define PLK_ROWS 8              /* DP rows owned by one lane of a strip */
+#define PLK_RING_INTS 12        /* column state handed from one strip to the next (9 used, 48-byte entries) */
+
+/* scoring parameters and lookup tables, passed to kernels by value */
+typedef struct {
+	int32_t go, ge, io, fs, end_bonus, xdrop;
+	int32_t sp[6];
+	int32_t sp_null_bonus;
+	float ie_coef;
+	int8_t sc[22 * 22];
+	uint8_t nt4[256], aa20[256], codon[64];
+	uint8_t aa_x;               /* aa20['X'] */
+	uint8_t pad[3];
+} plk_params_t;
+
+/* per-job metadata, device resident */
+typedef struct {
+	int64_t nt_off, aa_off, ss_off;  /* inputs (ss_off < 0: no splice-score track) */
+	int64_t prep_off;                /* nas[nl] | aas[al] | donor[nl+1] | acceptor[nl+1], 8-aligned */
+	int64_t trace_off;               /* first trace word (uint16) of this job in the wave arena */
+	int64_t tmp_off;                 /* reversed CIGAR scratch (uint32 words), capacity nl+al+8 */
+	int64_t out_off;                 /* final CIGAR offset in the output buffer (filled by the scan) */
+	int32_t nl, al;
+	int32_t mode;                    /* 0: int16 (lower clamp suffices), 1: int32 (gs32b), 2: int16 both clamps */
+	int32_t slen;                    /* segment length of the striping being reproduced */
+	int32_t nw;                      /* warps cooperating on the job: 1 or PLK_WARPS_PER_CTA */
+	int32_t pad0;
+	int32_t score, n_tmp;            /* outputs of the DP / traceback */
+	int32_t status, pad;
+} plk_job_t;
+
+/* bytes of preparation scratch for a job (8-aligned) */
+static inline int64_t plk_prep_bytes(int32_t nl, int32_t al)
+{
+	return ((int64_t)nl + al + 2 * ((int64_t)nl + 1) + 7) / 8 * 8;
+}
+
+/* trace words of a job in the strip layout (strips of 32*nw*PLK_ROWS rows) */
+static inline int64_t plk_trace_words(int32_t nl, int32_t al, int32_t nw)
+{
+	int64_t h = 32LL * nw * PLK_ROWS, nr = (int64_t)nl - 2, strips = (nr + h - 1) / h;
+	return strips * h * (int64_t)al;
+}
+
+/* launchers; all return a cudaError_t value as int */
+int plk_prep(const plk_job_t *jobs, int32_t n_jobs, const uint8_t *nt, const uint8_t *aa, const uint8_t *ss,
+		uint8_t *prep, const plk_params_t *p, void *stream);
+/* order_coop: jobs run by a whole CTA (nw = PLK_WARPS_PER_CTA); order_solo: one warp each.
+ * counters: 2 ints of device scratch.  ring: PLK_WARPS_PER_CTA * n_ctas * ring_stride_ints ints. */
+int plk_splice_dp(plk_job_t *jobs, const int32_t *order_coop, int32_t n_coop, const int32_t *order_solo,
+		int32_t n_solo, int32_t *counters, const uint8_t *prep, uint16_t *trace, int32_t *ring,
+		int64_t ring_stride_ints, int32_t n_ctas, int32_t mode, const plk_params_t *p, void *stream);
+int plk_traceback(plk_job_t *jobs, const int32_t *order, int32_t n_order, const uint16_t *trace,
+		uint32_t *tmp, void *stream);
+int plk_scan_compact(plk_job_t *jobs, int32_t n_jobs, const uint32_t *tmp, uint32_t *out, int64_t out_cap,
+		int64_t *total_words, void *result_recs, void *stream);
+/* CTAs of the DP kernel that fit on one SM at once (occupancy) */
+int plk_dp_ctas_per_sm(int32_t mode);
+uint64_t plk_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,665 @@
+/*
+ * splice.cu -- sm_100a kernels of the global spliced protein-to-DNA DP
+ * (the GPU replacement of nasw-cuda.cu:151-401 and of the host backtrack
+ * nasw-cuda.cu:676-707; semantics of nasw-sse.c:351-567 and :779-973).
+ *
+ * Kernels
+ *   k_prep       per-position input preparation (nasw-sse.c:95-159): codon
+ *                translation, donor/acceptor penalties with the int8 wrap of the
+ *                reference, optional splice-score track.
+ *   k_splice_dp  the DP.  One warp per job (persistent, jobs pulled from a
+ *                length-sorted queue).  A job's rows are cut into strips of
+ *                32*R rows; lane t owns rows [tR, tR+R) of the strip and walks
+ *                the protein columns one per step, one step behind lane t-1
+ *                (anti-diagonal wavefront).  The column state of the three rows
+ *                above a lane (H and D of rows i-1..i-3, A/B/C of row i-1) comes
+ *                from lane t-1 by __shfl_up_sync; lane 0 gets it from lane 31 of
+ *                the previous strip through a per-warp ring in L2.  The
+ *                reference's striped schedule (vsize lanes of slen columns, a
+ *                first pass with the insertion chain restarted at every segment
+ *                start, then the lazy-F correction) is reproduced exactly with
+ *                three running values per row: ip (first-pass insertion), ic
+ *                (carried insertion) and lh (first-pass H of the previous
+ *                column).  Saturating int16 arithmetic is emulated in int32.
+ *                Trace words (state in bits 0-3, extension bits 4-8) are written
+ *                with one 16-byte store per lane per step into a diagonal-major
+ *                layout, so every warp store is a contiguous 512-byte run.
+ *   k_traceback  one thread per job walks the trace (nasw-sse.c:44-93) and
+ *                writes the run-length merged CIGAR in reverse.
+ *   k_scan / k_compact  exclusive scan of CIGAR lengths and the reversed copy
+ *                into the dense output with ns_fix_tiny_UV (nasw-sse.c:34-42).
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "plk.h"
+#include "../../include/plgpu.h"
+
+static unsigned long long g_launches = 0;
+
+#define FULL 0xffffffffu
+
+/* ------------------------------------------------------------------ arithmetic modes
+ * MODE 0: int16 semantics where no value can reach +32767 (al*max(sc)+256 < 32767):
+ *         _mm_subs/_mm_adds_epi16 reduce to a clamp at -32768.
+ * MODE 1: int32 semantics of ns_global_gs32b (no saturation, neg_inf -2^30).
+ * MODE 2: int16 semantics with both clamps (long proteins). */
+template <int MODE> struct Ar;
+template <> struct Ar<0> {
+	static constexpr int NEG = -32768;
+	static __device__ __forceinline__ int sub(int x, int k) { return max(x - k, NEG); }
+	static __device__ __forceinline__ int add(int x, int k) { return max(x + k, NEG); }
+};
+template <> struct Ar<1> {
+	static constexpr int NEG = -0x40000000;
+	static __device__ __forceinline__ int sub(int x, int k) { return x - k; }
+	static __device__ __forceinline__ int add(int x, int k) { return x + k; }
+};
+template <> struct Ar<2> {
+	static constexpr int NEG = -32768;
+	static __device__ __forceinline__ int sub(int x, int k) { return min(max(x - k, NEG), 32767); }
+	static __device__ __forceinline__ int add(int x, int k) { return min(max(x + k, NEG), 32767); }
+};
+
+/* ------------------------------------------------------------------ preparation */
+
+__global__ void k_prep(const plk_job_t *__restrict__ jobs, int n_jobs, const uint8_t *__restrict__ nt,
+		const uint8_t *__restrict__ aa, const uint8_t *__restrict__ ss, uint8_t *__restrict__ prep, plk_params_t P)
+{
+	__shared__ uint8_t s_nt4[256], s_aa20[256], s_codon[64];
+	for (int x = threadIdx.x; x < 256; x += blockDim.x) s_nt4[x] = P.nt4[x], s_aa20[x] = P.aa20[x];
+	for (int x = threadIdx.x; x < 64; x += blockDim.x) s_codon[x] = P.codon[x];
+	__syncthreads();
+	for (int jb = blockIdx.x; jb < n_jobs; jb += gridDim.x) {
+		const plk_job_t J = jobs[jb];
+		const int nl = J.nl, al = J.al;
+		const uint8_t *ns = nt + J.nt_off, *as = aa + J.aa_off, *sst = J.ss_off >= 0 ? ss + J.ss_off : 0;
+		uint8_t *nas = prep + J.prep_off, *aas = nas + nl;
+		int8_t *donor = (int8_t*)(aas + al), *acceptor = donor + nl + 1;
+		const int max_spsc = (P.io + 1) / 2 - 1;
+#define B4(q) ((q) >= 0 && (q) < nl ? s_nt4[ns[(q)]] : 4)
+		for (int j = threadIdx.x; j < al; j += blockDim.x) aas[j] = s_aa20[as[j]];
+		for (int p = threadIdx.x; p <= nl; p += blockDim.x) {
+			int dv = P.sp[3], av = P.sp[3];
+			if (p < nl - 3) { /* nasw-sse.c:124-131 */
+				const int b0 = B4(p), b1 = B4(p + 1), b2 = B4(p + 2), b3 = B4(p + 3);
+				int t = 3;
+				if (b1 == 2 && b2 == 3) t = (b3 == 0 || b3 == 2) ? (b0 == 2 ? -1 : 4) : 0;
+				else if (b1 == 2 && b2 == 1 && b0 == 2) t = 1;
+				else if (b1 == 0 && b2 == 3) t = 2;
+				dv = t < 0 ? 0 : P.sp[t];
+			}
+			int8_t d8 = (int8_t)dv, a8 = (int8_t)av;
+			if (p >= 1 && p < nl) { /* nasw-sse.c:132-141 */
+				const int bm1 = B4(p - 1), b0 = B4(p);
+				int t = 3, pen = 0;
+				if (bm1 == 0 && b0 == 2) {
+					const int bm2 = B4(p - 2);
+					t = (p >= 2 && (bm2 == 1 || bm2 == 3)) ? -1 : 0;
+					for (int q = p - 4; q >= 0 && q > p - 7; --q) {
+						const int bq = B4(q);
+						if (bq != 1 && bq != 3) pen += P.sp[5];
+					}
+				} else if (bm1 == 0 && b0 == 1) t = 2;
+				a8 = (int8_t)(t < 0 ? 0 : P.sp[t]);
+				if (t == -1 || t == 0) a8 = (int8_t)(a8 + pen);
+			}
+			if (sst && p + 1 >= 1 && p + 1 < nl) { /* nasw-sse.c:142-156 */
+				const uint8_t x = sst[p + 1];
+				int spsc = (int8_t)(x >> 1) - (int8_t)NS_SPSC_OFFSET;
+				if (spsc > max_spsc) spsc = max_spsc;
+				if (x == 0xff) d8 = (int8_t)(d8 - P.sp_null_bonus), a8 = (int8_t)(a8 - P.sp_null_bonus);
+				else if (x & 1) a8 = (int8_t)(a8 - spsc);
+				else d8 = (int8_t)(d8 - spsc);
+			}
+			donor[p] = d8, acceptor[p] = a8;
+			if (p < nl) { /* nasw-sse.c:95-108 */
+				const int b2 = B4(p), b1 = B4(p - 1), b0 = B4(p - 2);
+				nas[p] = (p >= 2 && b0 < 4 && b1 < 4 && b2 < 4) ? s_codon[(b0 << 4 | b1 << 2 | b2) & 0x3f] : P.aa_x;
+			}
+		}
+#undef B4
+	}
+}
+
+/* ------------------------------------------------------------------ the DP */
+
+struct DpShared {
+	int32_t sct[22 * 22];                               /* score table, transposed: sct[b*22 + a] */
+	int32_t slot[2][PLK_WARPS_PER_CTA][PLK_RING_INTS];  /* warp-to-warp hand-off of a cooperative wavefront */
+	int32_t job;
+	int32_t pre[PLK_WARPS_PER_CTA][PLK_RING_INTS] __attribute__((aligned(16)));
+};
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+	const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+/*
+ * Trace word of a cell (all modes): bits 0-3 = 15 - state (state 0..9 in the
+ * candidate order of nasw-sse.c:464-536), bits 4-8 = extension bits of I, D,
+ * A, B, C, bit 9 = raised by the carried insertion (the reference's lazy-F
+ * bit; state 1 when read without a pending extension).
+ *
+ * MODE 0 works in a scaled domain: every DP value is kept times 16, so the low
+ * four bits of a running maximum can carry the index of the candidate that
+ * set it.  A candidate k enters as value*16 + (15-k); the maximum of the
+ * encoded candidates is the maximum value, ties going to the smallest k --
+ * exactly the strictly-greater, first-wins order of the reference -- and no
+ * compare/select per candidate is needed.  Values entering only the maximum
+ * need no clamp at -32768: the running maximum starts clamped, so a value
+ * below the floor can neither win nor tie.  Stored states (I, D, A, B, C) are
+ * clamped exactly; sat(sat(x-a)-b) is max(max(x-a, NEG)-b, NEG).
+ */
+template <int NW>
+__device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[PLK_ROWS], const int ah1, const int ah2,
+		const int ah3, const bool row2, const int *__restrict__ sct_b, const int (&code)[PLK_ROWS],
+		const int (&gi)[PLK_ROWS], const int (&dn)[PLK_ROWS + 2], const int (&ac)[PLK_ROWS + 2],
+		int (&ip)[PLK_ROWS], int (&lh)[PLK_ROWS], const int (&ic)[PLK_ROWS], const int c16[8],
+		int (&o)[9], unsigned (&z)[PLK_ROWS], int (&hn)[PLK_ROWS])
+{
+	constexpr int R = PLK_ROWS, N16 = -32768 * 16;
+	const int GO = c16[0], GE = c16[1], IO = c16[2], F6 = c16[3], F7 = c16[4], F8 = c16[5], F9 = c16[6], FS = c16[7];
+	int h1 = in[0], h2 = in[1], h3 = in[2], d1 = in[3], d2 = in[4], d3 = in[5], va = in[6], vb = in[7], vc = in[8];
+#pragma unroll
+	for (int r = 0; r < R; ++r) {
+		int h1m1 = r >= 1 ? hm[r - 1] : ah1;
+		int h2m1 = r >= 2 ? hm[r - 2] : (r == 1 ? ah1 : ah2);
+		int h3m1 = r >= 3 ? hm[r - 3] : (r == 2 ? ah1 : (r == 1 ? ah2 : ah3));
+		if (r == 0 && row2) h1m1 = FS, h2m1 = FS, h3m1 = 0; /* column -1 while row 2 is computed: {0, -fs, -fs} */
+		int he = max(h3m1 + sct_b[code[r]], N16 + 15);       /* 0: H(i-3,j-1) + s(i,j) */
+		int t = max(lh[r] - GO, N16);
+		const unsigned p4 = ip[r] > t;
+		ip[r] = max(max(t, ip[r]) - GE, N16);
+		he = max(he, ip[r] + 14);                            /* 1: I */
+		int u = max(h3 - GO, N16);
+		const unsigned p5 = d3 > u;
+		const int dnew = max(max(u, d3) + gi[r], N16);
+		he = max(he, dnew + 13);                             /* 2: D */
+		u = max(h1 - IO, N16);
+		t = max(u + dn[r], N16);
+		const unsigned p6 = va > t;
+		const int anew = max(t, va);
+		he = max(he, anew + ac[r + 2] + 12);                 /* 3: A - a(i) */
+		u = max(h1m1 - IO, N16);
+		t = max(u + dn[r + 1], N16);
+		const unsigned p7 = vb > t;
+		const int bnew = max(t, vb);
+		he = max(he, bnew + ac[r] + 11);                     /* 4: B - a(i-2) */
+		t = max(u + dn[r + 2], N16);
+		const unsigned p8 = vc > t;
+		const int cnew = max(t, vc);
+		he = max(he, cnew + ac[r + 1] + 10);                 /* 5: C - a(i-1) */
+		he = max(he, h1 + F6);                               /* 6: H(i-1,j) - f */
+		he = max(he, h2 + F7);                               /* 7: H(i-2,j) - f */
+		he = max(he, h1m1 + F8);                             /* 8: H(i-1,j-1) - f */
+		he = max(he, h2m1 + F9);                             /* 9: H(i-2,j-1) - f */
+		const int hfp = he & ~15;
+		lh[r] = hfp;
+		const unsigned p9 = ic[r] > he;                      /* raised by the carried insertion */
+		const int h = max(ic[r], hfp);
+		z[r] = (unsigned)(he & 15) | p4 << 4 | p5 << 5 | p6 << 6 | p7 << 7 | p8 << 8 | p9 << 9;
+		hn[r] = h;
+		h3 = h2, h2 = h1, h1 = h;
+		d3 = d2, d2 = d1, d1 = dnew;
+		va = anew, vb = bnew, vc = cnew;
+	}
+	o[0] = h1, o[1] = h2, o[2] = h3, o[3] = d1, o[4] = d2, o[5] = d3, o[6] = va, o[7] = vb, o[8] = vc;
+}
+
+/* Straightforward formulation for the 32-bit width (MODE 1) and the doubly
+ * clamped int16 case (MODE 2). */
+template <int MODE>
+__device__ __forceinline__ void cells_plain(const int (&in)[9], int (&hm)[PLK_ROWS], const int ah1, const int ah2,
+		const int ah3, const bool row2, const bool seg, const bool first, const int *__restrict__ sct_b,
+		const int (&code)[PLK_ROWS], const int (&gi)[PLK_ROWS], const int (&dn)[PLK_ROWS + 2],
+		const int (&ac)[PLK_ROWS + 2], int (&ip)[PLK_ROWS], int (&lh)[PLK_ROWS], int (&ic)[PLK_ROWS],
+		const plk_params_t &P, int (&o)[9], unsigned (&z)[PLK_ROWS], int (&hn)[PLK_ROWS])
+{
+	typedef Ar<MODE> A;
+	constexpr int R = PLK_ROWS;
+	const int NEG = A::NEG, go = P.go, ge = P.ge, goe = P.go + P.ge, io = P.io, fs = P.fs;
+	int h1 = in[0], h2 = in[1], h3 = in[2], d1 = in[3], d2 = in[4], d3 = in[5], va = in[6], vb = in[7], vc = in[8];
+#pragma unroll
+	for (int r = 0; r < R; ++r) {
+		int h1m1 = r >= 1 ? hm[r - 1] : ah1;
+		int h2m1 = r >= 2 ? hm[r - 2] : (r == 1 ? ah1 : ah2);
+		int h3m1 = r >= 3 ? hm[r - 3] : (r == 2 ? ah1 : (r == 1 ? ah2 : ah3));
+		if (r == 0 && row2) h1m1 = -fs, h2m1 = -fs, h3m1 = 0;
+		const int S = sct_b[code[r]];
+		const int dim1 = dn[r], di = dn[r + 1], dip1 = dn[r + 2], aim2 = ac[r], aim1 = ac[r + 1], ai = ac[r + 2];
+		int it = 16, icr;
+		if (seg) {
+			const int hop = A::sub(lh[r], goe), iext = A::sub(ip[r], ge), c0 = max(hop, iext);
+			const int older = A::sub(ic[r], ge);
+			it = first ? 0 : (c0 >= older ? (iext > hop ? 16 : 0) : 16);
+			icr = first ? NEG : max(c0, older);
+			ip[r] = NEG, lh[r] = NEG;
+		} else icr = A::sub(ic[r], ge);
+		ic[r] = icr;
+		int h, t, u, y = 0;
+		unsigned zz = 0;
+		h = A::add(h3m1, S);
+		t = A::sub(lh[r], go);
+		zz |= ip[r] > t ? 1u << 4 : 0u;
+		t = max(t, ip[r]);
+		ip[r] = A::sub(t, ge);
+		y = ip[r] > h ? 1 : y;
+		h = max(h, ip[r]);
+		u = A::sub(h3, go);
+		zz |= d3 > u ? 1u << 5 : 0u;
+		t = A::sub(max(u, d3), gi[r]);
+		const int dnew = t;
+		y = t > h ? 2 : y;
+		h = max(h, t);
+		u = A::sub(h1, io);
+		t = A::sub(u, dim1);
+		zz |= va > t ? 1u << 6 : 0u;
+		t = max(t, va);
+		const int anew = t;
+		t = A::sub(t, ai);
+		y = t > h ? 3 : y;
+		h = max(h, t);
+		u = A::sub(h1m1, io);
+		t = A::sub(u, di);
+		zz |= vb > t ? 1u << 7 : 0u;
+		t = max(t, vb);
+		const int bnew = t;
+		t = A::sub(t, aim2);
+		y = t > h ? 4 : y;
+		h = max(h, t);
+		t = A::sub(u, dip1);
+		zz |= vc > t ? 1u << 8 : 0u;
+		t = max(t, vc);
+		const int cnew = t;
+		t = A::sub(t, aim1);
+		y = t > h ? 5 : y;
+		h = max(h, t);
+		t = A::sub(h1, fs);
+		y = t > h ? 6 : y;
+		h = max(h, t);
+		t = A::sub(h2, fs);
+		y = t > h ? 7 : y;
+		h = max(h, t);
+		t = A::sub(h1m1, fs);
+		y = t > h ? 8 : y;
+		h = max(h, t);
+		t = A::sub(h2m1, fs);
+		y = t > h ? 9 : y;
+		h = max(h, t);
+		lh[r] = h;
+		if (icr > h) { /* raised by the carried insertion */
+			h = icr;
+			zz = MODE == 1 ? ((unsigned)it | 14u | 1u << 9) /* 32-bit: the word is replaced by 1|i_trace, nasw-sse.c:949 */
+				: (zz | (unsigned)(15 - y) | 1u << 9);
+		} else zz |= (unsigned)(15 - y);
+		z[r] = zz;
+		hn[r] = h;
+		h3 = h2, h2 = h1, h1 = h;
+		d3 = d2, d2 = d1, d1 = dnew;
+		va = anew, vb = bnew, vc = cnew;
+	}
+	o[0] = h1, o[1] = h2, o[2] = h3, o[3] = d1, o[4] = d2, o[5] = d3, o[6] = va, o[7] = vb, o[8] = vc;
+}
+
+/* One DP job on a wavefront of NW warps (32*NW lanes).  All threads of the
+ * group call this with the same job; `L` is the lane index in the wavefront. */
+template <int MODE, int NW>
+__device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t *__restrict__ prep,
+		uint16_t *__restrict__ trace, int32_t *__restrict__ myring, DpShared &sh, const plk_params_t &P,
+		const int L, const int wib)
+{
+	constexpr int R = PLK_ROWS, NL = 32 * NW, HS = NL * R;
+	constexpr int SC = MODE == 0 ? 16 : 1;                  /* value scale of the mode */
+	const int NEG = Ar<MODE>::NEG * SC;
+	const int lane = L & 31, w = L >> 5;
+	const int nl = J->nl, al = J->al, slen = J->slen;
+	const uint8_t *nas = prep + J->prep_off, *aas = nas + nl;
+	const int8_t *donor = (const int8_t*)(aas + al), *acceptor = donor + nl + 1;
+	uint16_t *tr = trace + J->trace_off;
+	const int nr = nl - 2, nstrip = (nr + HS - 1) / HS;
+	const int Pc = al > NL ? al : NL + 1;  /* period >= NL+1 keeps lane 0's one-step ring prefetch behind the writer */
+	const int total = nstrip * Pc + NL - 1;
+	int32_t *pre = sh.pre[wib];          /* lane 0's prefetched ring entry (cp.async target) */
+	const int c16[8] = { 16 * P.go, 16 * P.ge, 16 * P.io, -16 * P.fs + 9, -16 * P.fs + 8, -16 * P.fs + 7,
+		-16 * P.fs + 6, -16 * P.fs };
+	const int GOE = 16 * (P.go + P.ge), GE16 = 16 * P.ge;
+
+	int c = -L, k = 0, cs = 0, dcol = 0, i0 = 0;
+	int ip[R], lh[R], ic[R], hm[R], code[R], gi[R], dn[R + 2], ac[R + 2];
+	int ah1 = NEG, ah2 = NEG, ah3 = NEG; /* H(i0-1..i0-3, c-1) */
+	int o[9];
+#pragma unroll
+	for (int q = 0; q < 9; ++q) o[q] = NEG;
+#pragma unroll
+	for (int r = 0; r < R; ++r) ip[r] = lh[r] = ic[r] = hm[r] = NEG, code[r] = 0, gi[r] = 0;
+#pragma unroll
+	for (int r = 0; r < R + 2; ++r) dn[r] = ac[r] = 0;
+
+	for (int s = 0; s < total; ++s) {
+		/* column state of the rows above: lane-1's output of the previous step */
+		int in[9];
+#pragma unroll
+		for (int q = 0; q < 9; ++q) in[q] = __shfl_up_sync(FULL, o[q], 1);
+		const bool started = c >= 0 && k < nstrip;
+		if (lane == 0 && started) {
+			if (w == 0) {
+				if (k > 0) cp_async_wait_all();
+#pragma unroll
+				for (int q = 0; q < 9; ++q) in[q] = k == 0 ? NEG : pre[q];
+			} else {
+				const int32_t *sl = sh.slot[(s - 1) & 1][wib - 1];
+#pragma unroll
+				for (int q = 0; q < 9; ++q) in[q] = sl[q];
+			}
+		}
+		if (started && c == 0) { /* strip start: per-row constants, column -1 */
+			i0 = 2 + k * HS + L * R;
+#pragma unroll
+			for (int r = 0; r < R; ++r) {
+				const int i = i0 + r;
+				code[r] = i < nl ? nas[i] : 0;
+				gi[r] = MODE == 0 ? -16 * (code[r] == 20 ? P.fs : P.ge) : (code[r] == 20 ? P.fs : P.ge);
+				ip[r] = lh[r] = ic[r] = hm[r] = NEG;
+			}
+#pragma unroll
+			for (int r = 0; r < R + 2; ++r) {
+				const int pd = i0 - 1 + r, pa = i0 - 2 + r;
+				const int dv = pd <= nl ? donor[pd] : 0, av = pa <= nl ? acceptor[pa] : 0;
+				dn[r] = MODE == 0 ? -16 * dv : dv;
+				ac[r] = MODE == 0 ? -16 * av : av;
+			}
+			ah1 = ah2 = ah3 = NEG;
+			cs = 0, dcol = L % al;
+		}
+		if (started && c < al && i0 < nl) {
+			const bool seg = cs == 0, first = c == 0, row2 = first && i0 == 2;
+			const int *sct_b = sh.sct + 22 * aas[c];
+			int hn[R];
+			unsigned z[R];
+			if (MODE == 0) {
+				/* the striped schedule's segment hand-over (nasw-sse.c:537-553): rare, so branched */
+				if (seg) {
+#pragma unroll
+					for (int r = 0; r < R; ++r) {
+						const int hop = max(lh[r] - GOE, NEG), iext = max(ip[r] - GE16, NEG);
+						ic[r] = max(max(hop, iext), max(ic[r] - GE16, NEG));
+						ip[r] = NEG, lh[r] = NEG;
+					}
+				} else {
+#pragma unroll
+					for (int r = 0; r < R; ++r) ic[r] = max(ic[r] - GE16, NEG);
+				}
+				cells_scaled<NW>(in, hm, ah1, ah2, ah3, row2, sct_b, code, gi, dn, ac, ip, lh, ic, c16, o, z, hn);
+			} else {
+				cells_plain<MODE>(in, hm, ah1, ah2, ah3, row2, seg, first, sct_b, code, gi, dn, ac, ip, lh, ic, P,
+						o, z, hn);
+			}
+			if (c == al - 1) { /* the final score H(nl-1, al-1) */
+				const int rl = nl - 1 - i0;
+#pragma unroll
+				for (int r = 0; r < R; ++r)
+					if (r == rl) J->score = MODE == 0 ? hn[r] >> 4 : hn[r];
+			}
+			/* trace: one 16-byte store per lane, contiguous across the lanes of a strip */
+			uint4 tw;
+			tw.x = (z[0] & 0xffff) | (z[1] << 16);
+			tw.y = (z[2] & 0xffff) | (z[3] << 16);
+			tw.z = (z[4] & 0xffff) | (z[5] << 16);
+			tw.w = (z[6] & 0xffff) | (z[7] << 16);
+			*(uint4*)(tr + (((int64_t)k * al + dcol) * NL + L) * R) = tw;
+			if (L == NL - 1) {
+				int32_t *e = myring + (int64_t)c * PLK_RING_INTS;
+#pragma unroll
+				for (int q = 0; q < 9; ++q) __stcg(e + q, o[q]);
+			}
+#pragma unroll
+			for (int r = 0; r < R; ++r) hm[r] = hn[r];
+			ah1 = in[0], ah2 = in[1], ah3 = in[2];
+		}
+		if (NW > 1) {
+			if (lane == 31) {
+				int32_t *sl = sh.slot[s & 1][wib];
+#pragma unroll
+				for (int q = 0; q < 9; ++q) sl[q] = o[q];
+			}
+			__syncthreads();
+		} else __syncwarp();
+		/* advance; lane 0 of the wavefront prefetches the ring entry of its next position */
+		++c;
+		if (c > 0) {
+			if (++cs == slen) cs = 0;
+			if (++dcol >= al) dcol = 0;
+		}
+		if (c == Pc) c = 0, ++k;
+		if (L == 0 && k >= 1 && k < nstrip && c < al) {
+			const int32_t *e = myring + (int64_t)c * PLK_RING_INTS;
+			cp_async16(pre, e), cp_async16(pre + 4, e + 4), cp_async16(pre + 8, e + 8);
+		}
+	}
+	if (L == 0) cp_async_wait_all();
+}
+
+/* Persistent DP kernel: first every CTA takes cooperative jobs (a whole CTA per
+ * job) until that queue is empty, then every warp takes solo jobs.  Both queues
+ * are sorted by decreasing size on the host (longest-processing-time first). */
+template <int MODE>
+__global__ void __launch_bounds__(32 * PLK_WARPS_PER_CTA, 2)
+k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop, int n_coop,
+		const int32_t *__restrict__ order_solo, int n_solo, int32_t *counters,
+		const uint8_t *__restrict__ prep, uint16_t *__restrict__ trace, int32_t *__restrict__ ring,
+		int64_t ring_stride, plk_params_t P)
+{
+	__shared__ DpShared sh;
+	for (int x = threadIdx.x; x < 22 * 22; x += blockDim.x) { /* sct[b*22 + a] = s(a, b), scaled and tagged in mode 0 */
+		const int b = x / 22, a = x % 22, v = P.sc[a * 22 + b];
+		sh.sct[x] = MODE == 0 ? v * 16 + 15 : v;
+	}
+	__syncthreads();
+	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+	for (;;) {
+		if (threadIdx.x == 0) sh.job = atomicAdd(&counters[0], 1);
+		__syncthreads();
+		const int idx = sh.job;
+		__syncthreads();
+		if (idx >= n_coop) break;
+		dp_job<MODE, PLK_WARPS_PER_CTA>(jobs + order_coop[idx], prep, trace,
+				ring + (int64_t)blockIdx.x * PLK_WARPS_PER_CTA * ring_stride, sh, P, threadIdx.x, wib);
+		__syncthreads();
+	}
+	int32_t *myring = ring + ((int64_t)blockIdx.x * PLK_WARPS_PER_CTA + wib) * ring_stride;
+	for (;;) {
+		int idx = 0;
+		if (lane == 0) idx = atomicAdd(&counters[1], 1);
+		idx = __shfl_sync(FULL, idx, 0);
+		if (idx >= n_solo) break;
+		dp_job<MODE, 1>(jobs + order_solo[idx], prep, trace, myring, sh, P, lane, wib);
+		__syncwarp();
+	}
+}
+
+/* ------------------------------------------------------------------ traceback */
+
+__device__ __forceinline__ void tb_push(uint32_t *out, int &n, uint32_t op, int len)
+{ /* ns_push_cigar merge rule (nasw.h:219-229) */
+	if (n == 0 || op != (out[n - 1] & 0xf) || op == NS_CIGAR_F || op == NS_CIGAR_G) out[n++] = (uint32_t)len << 4 | op;
+	else out[n - 1] += (uint32_t)len << 4;
+}
+
+/* Traceback: one warp per job.  The walk is inherently sequential, so the warp
+ * stages the trace words around the current cell in shared memory -- a tile of
+ * 8 row-chunks (64 rows) x 32 columns, one coalesced round of 16-byte loads --
+ * and lane 0 walks inside the tile until the path leaves it. */
+#define TB_CHUNKS 8
+#define TB_COLS 32
+#define TB_WARPS 8
+__global__ void __launch_bounds__(32 * TB_WARPS) k_traceback(plk_job_t *__restrict__ jobs,
+		const int32_t *__restrict__ order, int n_order, const uint16_t *__restrict__ trace, uint32_t *__restrict__ tmp)
+{
+	__shared__ uint4 s_tile[TB_WARPS][TB_CHUNKS][TB_COLS]; /* 8 trace words (rows) per entry */
+	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+	const int q = blockIdx.x * TB_WARPS + wib;
+	if (q >= n_order) return;
+	plk_job_t *J = jobs + order[q];
+	const int nl = J->nl, al = J->al;
+	const uint16_t *tr = trace + J->trace_off;
+	uint32_t *out = tmp + J->tmp_off;
+	const int nlanes = 32 * J->nw, hs = nlanes * PLK_ROWS;
+	int i = nl - 1, j = al - 1, last = 0, n = 0;
+	while (i >= 2 && j >= 0) {
+		/* stage the tile whose top-right corner holds (i, j) */
+		const int qc = (i - 2) / PLK_ROWS, jc = j;
+#pragma unroll
+		for (int m = 0; m < TB_CHUNKS * TB_COLS / 32; ++m) {
+			const int idx = lane + 32 * m, dq = idx / TB_COLS, dc = idx % TB_COLS;
+			const int ch = qc - dq, col = jc - dc;
+			if (ch >= 0 && col >= 0) {
+				const int ra = ch * PLK_ROWS, k = ra / hs, t = (ra / PLK_ROWS) % nlanes;
+				int d = col + t;
+				if (d >= al) d %= al;
+				s_tile[wib][dq][dc] = *(const uint4*)(tr + (((int64_t)k * al + d) * nlanes + t) * PLK_ROWS);
+			}
+		}
+		__syncwarp();
+		if (lane == 0) {
+			while (i >= 2 && j >= 0) {
+				const int dq = qc - (i - 2) / PLK_ROWS, dc = jc - j;
+				if (dq >= TB_CHUNKS || dc >= TB_COLS) break;
+				const uint16_t *cell = (const uint16_t*)&s_tile[wib][dq][dc];
+				const int x = cell[(i - 2) % PLK_ROWS];
+				const int state = last != 0 ? last : (x >> 9 & 1) ? 1 : 15 - (x & 0xf);
+				const int ext = state >= 1 && state <= 5 ? (x >> (state + 3)) & 1 : 0;
+				switch (state) {
+				case 0: tb_push(out, n, NS_CIGAR_M, 1), i -= 3, --j; break;
+				case 1: tb_push(out, n, NS_CIGAR_I, 1), --j; break;
+				case 2: tb_push(out, n, NS_CIGAR_D, 1), i -= 3; break;
+				case 3: tb_push(out, n, NS_CIGAR_N, 1), --i; break;
+				case 4: tb_push(out, n, NS_CIGAR_U, 1), --i; if (!ext) --j; break;
+				case 5: tb_push(out, n, NS_CIGAR_V, 1), --i; if (!ext) --j; break;
+				case 6: tb_push(out, n, NS_CIGAR_F, 1), --i; break;
+				case 7: tb_push(out, n, NS_CIGAR_F, 2), i -= 2; break;
+				case 8: tb_push(out, n, NS_CIGAR_G, 1), --i, --j; break;
+				default: tb_push(out, n, NS_CIGAR_G, 2), i -= 2, --j; break;
+				}
+				last = state >= 1 && state <= 5 && ext ? state : 0;
+			}
+		}
+		i = __shfl_sync(FULL, i, 0), j = __shfl_sync(FULL, j, 0);
+		last = __shfl_sync(FULL, last, 0), n = __shfl_sync(FULL, n, 0);
+		__syncwarp();
+	}
+	if (lane == 0) {
+		if (j > 0) tb_push(out, n, NS_CIGAR_I, j);
+		if (i >= 0) {
+			const int l = (i + 1) / 3, t = (i + 1) % 3;
+			if (l > 0) tb_push(out, n, NS_CIGAR_D, l);
+			if (t != 0) tb_push(out, n, NS_CIGAR_F, t);
+		}
+		J->n_tmp = n;
+	}
+}
+
+/* exclusive scan of the CIGAR lengths in job order (single CTA) */
+__global__ void k_scan(plk_job_t *jobs, int n_jobs, int64_t *total)
+{
+	__shared__ int64_t s_part[1024];
+	const int tid = threadIdx.x, nt = blockDim.x;
+	const int per = (n_jobs + nt - 1) / nt, b = tid * per, e = min(n_jobs, b + per);
+	int64_t acc = 0;
+	for (int q = b; q < e; ++q) acc += jobs[q].n_tmp;
+	s_part[tid] = acc;
+	__syncthreads();
+	for (int off = 1; off < nt; off <<= 1) {
+		int64_t v = tid >= off ? s_part[tid - off] : 0;
+		__syncthreads();
+		s_part[tid] += v;
+		__syncthreads();
+	}
+	int64_t run = s_part[tid] - acc;
+	for (int q = b; q < e; ++q) jobs[q].out_off = run, run += jobs[q].n_tmp;
+	if (tid == nt - 1) *total = s_part[tid];
+}
+
+__global__ void k_compact(const plk_job_t *__restrict__ jobs, int n_jobs, const uint32_t *__restrict__ tmp,
+		uint32_t *__restrict__ out, int64_t out_cap, pl_splice_result_t *__restrict__ res)
+{
+	const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+	if (w >= n_jobs) return;
+	const plk_job_t J = jobs[w];
+	const int n = J.n_tmp;
+	const bool fits = J.out_off + n <= out_cap;
+	for (int q = lane; q < n && fits; q += 32) {
+		uint32_t x = tmp[J.tmp_off + n - 1 - q];
+		const uint32_t op = x & 0xf;
+		if ((op == NS_CIGAR_U || op == NS_CIGAR_V) && (x >> 4) < 3) x = x >> 4 << 4 | NS_CIGAR_G;
+		out[J.out_off + q] = x;
+	}
+	if (lane == 0) {
+		pl_splice_result_t r;
+		r.score = J.score, r.n_cigar = n, r.cigar_off = J.out_off, r.mode = J.mode == 1 ? 32 : 16;
+		r.status = fits ? J.status : -2;
+		res[w] = r;
+	}
+}
+
+/* ------------------------------------------------------------------ launchers */
+
+extern "C" int plk_prep(const plk_job_t *jobs, int32_t n_jobs, const uint8_t *nt, const uint8_t *aa,
+		const uint8_t *ss, uint8_t *prep, const plk_params_t *p, void *stream)
+{
+	if (n_jobs <= 0) return 0;
+	const int grid = n_jobs < 65535 ? n_jobs : 65535;
+	k_prep<<<grid, 256, 0, (cudaStream_t)stream>>>(jobs, n_jobs, nt, aa, ss, prep, *p);
+	__sync_fetch_and_add(&g_launches, 1ull);
+	return (int)cudaGetLastError();
+}
+
+extern "C" int plk_dp_ctas_per_sm(int32_t mode)
+{
+	int n = 0;
+	cudaError_t e;
+	if (mode == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_splice_dp<1>, 32 * PLK_WARPS_PER_CTA, 0);
+	else if (mode == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_splice_dp<2>, 32 * PLK_WARPS_PER_CTA, 0);
+	else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_splice_dp<0>, 32 * PLK_WARPS_PER_CTA, 0);
+	return e == cudaSuccess ? n : -1;
+}
+
+extern "C" int plk_splice_dp(plk_job_t *jobs, const int32_t *order_coop, int32_t n_coop, const int32_t *order_solo,
+		int32_t n_solo, int32_t *counters, const uint8_t *prep, uint16_t *trace, int32_t *ring,
+		int64_t ring_stride_ints, int32_t n_ctas, int32_t mode, const plk_params_t *p, void *stream)
+{
+	if (n_coop + n_solo <= 0) return 0;
+	cudaStream_t st = (cudaStream_t)stream;
+	cudaError_t e = cudaMemsetAsync(counters, 0, 2 * sizeof(int32_t), st);
+	if (e != cudaSuccess) return (int)e;
+	const dim3 grid(n_ctas), block(32 * PLK_WARPS_PER_CTA);
+	if (mode == 1) k_splice_dp<1><<<grid, block, 0, st>>>(jobs, order_coop, n_coop, order_solo, n_solo, counters, prep, trace, ring, ring_stride_ints, *p);
+	else if (mode == 2) k_splice_dp<2><<<grid, block, 0, st>>>(jobs, order_coop, n_coop, order_solo, n_solo, counters, prep, trace, ring, ring_stride_ints, *p);
+	else k_splice_dp<0><<<grid, block, 0, st>>>(jobs, order_coop, n_coop, order_solo, n_solo, counters, prep, trace, ring, ring_stride_ints, *p);
+	__sync_fetch_and_add(&g_launches, 1ull);
+	return (int)cudaGetLastError();
+}
+
+extern "C" int plk_traceback(plk_job_t *jobs, const int32_t *order, int32_t n_order, const uint16_t *trace,
+		uint32_t *tmp, void *stream)
+{
+	if (n_order <= 0) return 0;
+	k_traceback<<<(n_order + TB_WARPS - 1) / TB_WARPS, 32 * TB_WARPS, 0, (cudaStream_t)stream>>>(jobs, order, n_order, trace, tmp);
+	__sync_fetch_and_add(&g_launches, 1ull);
+	return (int)cudaGetLastError();
+}
+
+extern "C" int plk_scan_compact(plk_job_t *jobs, int32_t n_jobs, const uint32_t *tmp, uint32_t *out, int64_t out_cap,
+		int64_t *total_words, void *result_recs, void *stream)
+{
+	if (n_jobs <= 0) return 0;
+	cudaStream_t st = (cudaStream_t)stream;
+	k_scan<<<1, 1024, 0, st>>>(jobs, n_jobs, total_words);
+	k_compact<<<(n_jobs * 32 + 255) / 256, 256, 0, st>>>(jobs, n_jobs, tmp, out, out_cap, (pl_splice_result_t*)result_recs);
+	__sync_fetch_and_add(&g_launches, 2ull);
+	return (int)cudaGetLastError();
+}
+
+extern "C" uint64_t plk_launches(void) { return __sync_fetch_and_add(&g_launches, 0ull); }

@@ -1,0 +1,182 @@
+"""ctypes binding of libplgpu.so (the C ABI declared in include/plgpu.h).
+
+Loading fails loudly when the library has not been built: there is no
+Python or CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+from .abi import NsOpt, NsRst, SpliceJob, SpliceResult
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libplgpu.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "plgpu.h")
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C protlocus_b200/csrc` "
+                           "(or __graft_entry__.build()); there is no fallback")
+    lib = C.CDLL(LIB_PATH)
+    lib.ns_gpu_init.argtypes = [C.c_int32]
+    lib.ns_gpu_init.restype = C.c_int
+    for fn in ("ns_gpu_error", "ns_gpu_name", "pl_last_error"):
+        getattr(lib, fn).restype = C.c_char_p
+    for fn in ("ns_gpu_dispatch_count", "ns_gpu_launch_count", "pl_kernel_launch_count"):
+        getattr(lib, fn).restype = C.c_uint64
+    for fn in ("ns_gpu_h2d_seconds", "ns_gpu_kernel_seconds", "ns_gpu_d2h_seconds"):
+        getattr(lib, fn).restype = C.c_double
+    lib.ns_gpu_submit.argtypes = [C.c_void_p, C.c_char_p, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(NsOpt), C.c_void_p]
+    lib.ns_gpu_submit.restype = C.c_void_p
+    lib.ns_gpu_wait.argtypes = [C.c_void_p, C.POINTER(NsRst)]
+    lib.ns_gpu_wait.restype = C.c_int
+    lib.ns_gpu_global.argtypes = [C.c_void_p, C.c_char_p, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(NsOpt),
+                                  C.c_void_p, C.POINTER(NsRst)]
+    lib.ns_gpu_global.restype = C.c_int
+    lib.pl_engine_create.argtypes = [C.c_int32, C.c_int64]
+    lib.pl_engine_create.restype = C.c_void_p
+    lib.pl_engine_destroy.argtypes = [C.c_void_p]
+    lib.pl_engine_last_plan.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    lib.pl_splice_batch_host.argtypes = [C.c_void_p, C.POINTER(NsOpt), C.POINTER(SpliceJob), C.c_int32,
+                                         C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                         C.POINTER(SpliceResult), C.c_void_p, C.c_int64]
+    lib.pl_splice_batch_host.restype = C.c_int
+    lib.pl_splice_batch_device.argtypes = [C.c_void_p, C.POINTER(NsOpt), C.POINTER(SpliceJob), C.c_int32,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                           C.POINTER(C.c_int64), C.c_void_p]
+    lib.pl_splice_batch_device.restype = C.c_int
+    lib.pl_engine_set_timing.argtypes = [C.c_void_p, C.c_int32]
+    lib.pl_engine_times.argtypes = [C.c_void_p] + [C.POINTER(C.c_double)] * 4 + [C.POINTER(C.c_int64)] * 2
+    lib.pl_engine_stream.argtypes = [C.c_void_p]
+    lib.pl_engine_stream.restype = C.c_void_p
+    lib.pl_measure_int_peak.argtypes = [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.pl_measure_int_peak.restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def declared_symbols(header: str = HEADER) -> list[str]:
+    """Function names declared in include/plgpu.h."""
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"^[A-Za-z_][\w \*]*?\b(\w+)\s*\(", text, flags=re.M)
+    return sorted({n for n in names if n not in ("if", "while", "for", "return", "sizeof")})
+
+
+def error() -> str:
+    return load().pl_last_error().decode()
+
+
+_libc = C.CDLL(None)
+_libc.free.argtypes = [C.c_void_p]
+
+
+class Engine:
+    """A pl_engine_t on one device (bulk global spliced DP)."""
+
+    def __init__(self, device: int = 0, trace_budget_bytes: int = 0):
+        self.lib = load()
+        self.h = self.lib.pl_engine_create(device, trace_budget_bytes)
+        if not self.h:
+            raise RuntimeError("pl_engine_create failed: " + error())
+
+    def close(self):
+        if self.h:
+            self.lib.pl_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_timing(self, on: bool = True):
+        """(Re)start CUDA-event timing of the batch phases."""
+        if not self.lib.pl_engine_set_timing(self.h, int(on)):
+            raise RuntimeError("pl_engine_set_timing failed: " + error())
+
+    def times(self):
+        v = [C.c_double() for _ in range(4)]
+        n = [C.c_int64() for _ in range(2)]
+        self.lib.pl_engine_times(self.h, *[C.byref(x) for x in v], *[C.byref(x) for x in n])
+        return {"prep_ms": v[0].value, "dp_ms": v[1].value, "traceback_ms": v[2].value,
+                "compact_ms": v[3].value, "dp_launches": n[0].value, "cells": n[1].value}
+
+    @property
+    def stream(self) -> int:
+        return self.lib.pl_engine_stream(self.h) or 0
+
+    def last_plan(self):
+        w, c, d = C.c_int32(), C.c_int32(), C.c_int32()
+        self.lib.pl_engine_last_plan(self.h, C.byref(w), C.byref(c), C.byref(d))
+        return {"waves": w.value, "coop": c.value, "dp_launches": d.value}
+
+    def align_host(self, opt, pairs, ss=None):
+        """pairs: list of (nt bytes, protein bytes); ss: None or list of (bytes|None).
+        Returns a list of (score, cigar words, width)."""
+        n = len(pairs)
+        jobs = (SpliceJob * n)()
+        nt_parts, aa_parts, ss_parts = [], [], []
+        pos_nt = pos_aa = 0
+        for q, (nt, aa) in enumerate(pairs):
+            jobs[q].nt_off, jobs[q].aa_off, jobs[q].nl, jobs[q].al = pos_nt, pos_aa, len(nt), len(aa)
+            s = ss[q] if ss is not None else None
+            jobs[q].ss_off = pos_nt if s is not None else -1
+            nt_parts.append(nt)
+            aa_parts.append(aa)
+            ss_parts.append(s if s is not None else bytes(len(nt)))
+            pos_nt += len(nt)
+            pos_aa += len(aa)
+        ntb = np.frombuffer(b"".join(nt_parts), dtype=np.uint8)
+        aab = np.frombuffer(b"".join(aa_parts), dtype=np.uint8)
+        ssb = np.frombuffer(b"".join(ss_parts), dtype=np.uint8) if ss is not None else None
+        cap = sum(len(a) + len(b) + 8 for a, b in pairs)
+        cig = np.zeros(max(cap, 1), dtype=np.uint32)
+        res = (SpliceResult * n)()
+        ok = self.lib.pl_splice_batch_host(self.h, opt.ptr, jobs, n, ntb.ctypes.data, ntb.size, aab.ctypes.data,
+                                           aab.size, ssb.ctypes.data if ssb is not None else None,
+                                           ssb.size if ssb is not None else 0, res, cig.ctypes.data, cig.size)
+        if not ok:
+            raise RuntimeError("pl_splice_batch_host failed: " + error())
+        out = []
+        for q in range(n):
+            r = res[q]
+            if r.status != 0:
+                raise RuntimeError(f"job {q}: status {r.status}")
+            out.append((r.score, cig[r.cigar_off:r.cigar_off + r.n_cigar].tolist(), r.mode))
+        return out
+
+
+def measure_int_peak(device: int = 0):
+    """Measured integer-pipe lane-op rates (int32, int16x2) of the device."""
+    a, b = C.c_double(), C.c_double()
+    if not load().pl_measure_int_peak(device, C.byref(a), C.byref(b)):
+        raise RuntimeError("pl_measure_int_peak failed")
+    return a.value, b.value
+
+
+def gpu_init(device: int = 0) -> bool:
+    return bool(load().ns_gpu_init(device))
+
+
+def gpu_global(ns: bytes, aa: bytes, opt, ss: bytes | None = None):
+    """ns_gpu_global(): returns (ok, score, nt_len, aa_len, cigar words)."""
+    lib = load()
+    r = NsRst()
+    ssb = C.create_string_buffer(bytes(ss), len(ss)) if ss is not None else None
+    ok = lib.ns_gpu_global(None, ns, len(ns), aa, len(aa), opt.ptr, ssb, C.byref(r))
+    cig = [r.cigar[k] for k in range(r.n_cigar)] if ok and r.n_cigar else []
+    if r.cigar:
+        _libc.free(C.cast(r.cigar, C.c_void_p))
+    return bool(ok), r.score, r.nt_len, r.aa_len, cig

@@ -58,28 +58,39 @@ def revcomp(s: bytes) -> bytes:
     return s.translate(_COMP)[::-1]
 
 
+_AA20_B = np.frombuffer(AA20.encode(), dtype=np.uint8)
+_NT_B = np.frombuffer(b"ACGT", dtype=np.uint8)
+_SUB_CDF = np.cumsum(_SUB, axis=1)
+_AA_IDX = np.full(256, 0, dtype=np.int64)
+for _k, _ch in enumerate(AA20):
+    _AA_IDX[ord(_ch)] = _k
+# codon choices per residue index: table [20, 6] of codon strings padded by repetition
+_CODON_TAB = np.array([[(_CODONS[a] * 6)[j] for j in range(6)] for a in AA20])
+_CODON_N = np.array([len(_CODONS[a]) for a in AA20])
+
+
 def random_protein(rng: np.random.Generator, n: int) -> str:
-    return "".join(AA20[k] for k in rng.choice(20, size=n, p=P7_BG))
+    return _AA20_B[rng.choice(20, size=n, p=P7_BG)].tobytes().decode()
 
 
 def mutate(rng: np.random.Generator, prot: str, divergence: float) -> str:
-    out = []
-    for ch in prot:
-        if rng.random() < divergence:
-            a = AA20.index(ch)
-            out.append(AA20[rng.choice(20, p=_SUB[a])])
-        else:
-            out.append(ch)
-    return "".join(out)
+    idx = _AA_IDX[np.frombuffer(prot.encode(), dtype=np.uint8)]
+    hit = rng.random(len(idx)) < divergence
+    u = rng.random(len(idx))
+    new = (u[:, None] > _SUB_CDF[idx]).sum(axis=1).clip(0, 19)
+    out = np.where(hit, new, idx)
+    return _AA20_B[out].tobytes().decode()
 
 
 def reverse_translate(rng: np.random.Generator, prot: str) -> str:
-    return "".join(_CODONS[ch][rng.integers(len(_CODONS[ch]))] for ch in prot)
+    idx = _AA_IDX[np.frombuffer(prot.encode(), dtype=np.uint8)]
+    pick = (rng.random(len(idx)) * _CODON_N[idx]).astype(np.int64)
+    return "".join(_CODON_TAB[idx, pick].tolist())
 
 
 def random_dna(rng: np.random.Generator, n: int, gc: float = 0.5) -> str:
     p = [(1 - gc) / 2, gc / 2, gc / 2, (1 - gc) / 2]
-    return "".join(_NT[k] for k in rng.choice(4, size=n, p=p))
+    return _NT_B[rng.choice(4, size=n, p=p)].tobytes().decode()
 
 
 def _intron(rng: np.random.Generator, length: int) -> str:
@@ -157,16 +168,11 @@ def random_pair(rng: np.random.Generator, max_al: int = 60, n_rate: float = 0.01
     al = int(rng.integers(1, max_al + 1))
     nl = int(rng.integers(3, 3 * al + 121))
     aa = random_protein(rng, al).encode()
-    nt = bytes(b"N"[0] if rng.random() < n_rate else b"ACGT"[rng.integers(4)] for _ in range(nl))
+    nt = np.where(rng.random(nl) < n_rate, ord("N"), _NT_B[rng.integers(0, 4, size=nl)]).astype(np.uint8).tobytes()
     return nt, aa
 
 
 def random_ss(rng: np.random.Generator, nl: int, rate: float = 0.2) -> bytes:
     """Splice-score track like the reference's tests: mostly unset (0xff), some donor/acceptor scores."""
-    out = bytearray(nl)
-    for i in range(nl):
-        if rng.random() < rate:
-            out[i] = ((int(rng.integers(0, 128)) << 1) | int(rng.integers(0, 2))) & 0xff
-        else:
-            out[i] = 0xff
-    return bytes(out)
+    val = ((rng.integers(0, 128, size=nl) << 1) | rng.integers(0, 2, size=nl)) & 0xff
+    return np.where(rng.random(nl) < rate, val, 0xff).astype(np.uint8).tobytes()

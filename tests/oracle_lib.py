@@ -14,7 +14,7 @@ import os
 import platform
 import subprocess
 
-from protlocus_b200.abi import NsOpt, NsRst
+from protlocus_b200.abi import AA_I2C, BLOSUM62, NS_F_CIGAR, NS_S_NONE, NsOpt, NsRst, Options
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE = os.path.join(ROOT, "oracle")
@@ -112,3 +112,30 @@ def port_run(fn: str, ns: bytes, aa: bytes, opt, ss: bytes | None = None, avx2: 
     else:
         getattr(lib, "port_global_" + fn)(ns, len(ns), aa, len(aa), opt.ptr, ssb, C.byref(r), int(avx2))
     return _take(r)
+
+
+def run(fn: str, ns: bytes, aa: bytes, opt, ss: bytes | None = None):
+    """The checker's answer for `fn` in {"gs16b", "gs32b", "gs_auto"}: the reference build when it
+    is present on this machine, else the restatement (pinned to the same golden vectors)."""
+    if ref_lib() is not None:
+        return ref_run("ns_global_" + fn, ns, aa, opt, ss)
+    return port_run(fn, ns, aa, opt, ss)
+
+
+def make_options(spec: dict) -> Options:
+    """Option sets used by the golden fixtures (tests/golden/make_golden.py)."""
+    kind = spec["name"]
+    flag = spec.get("flag", NS_F_CIGAR)
+    if kind == "protlocus":  # ProtLocus defaults, options.c:125-138 via align.c:59-71
+        return Options(flag=flag, io=spec.get("io", 29), end_bonus=spec.get("end_bonus", 5),
+                       xdrop=spec.get("xdrop", 100))
+    if kind == "nasw_init":  # ns_opt_init(), nasw-tab.c:131-147
+        return Options.nasw_defaults(flag=flag)
+    if kind == "mkqtw":      # test/test_dp32.c:15-18
+        return Options.nasw_defaults(flag=flag, go=3, ge=1, io=100, fs=100, sp_model=NS_S_NONE)
+    if kind == "ww127":      # test/test_gpu.c:107-112
+        m = BLOSUM62.copy()
+        w = AA_I2C.index("W")
+        m[w, w] = 127
+        return Options.nasw_defaults(flag=flag, matrix=m)
+    raise ValueError(kind)
