@@ -194,6 +194,26 @@ int pl_measure_int_peak(int32_t device, double *int32_lane_ops, double *int16x2_
 /* Number of trace waves, cooperative jobs and DP launches of the last batch. */
 void pl_engine_last_plan(const pl_engine_t *e, int32_t *n_waves, int32_t *n_coop, int32_t *n_dp_launches);
 
+/* Allocation-free variant of pl_splice_batch_device() -- no counterpart in the
+ * reference.  For callers that cannot allocate device memory on this path: a
+ * program that gives all free device memory to its own pool and runs under that
+ * fixed budget, or a latency-sensitive loop that cannot take the device-wide
+ * synchronisation of cudaMalloc/cudaFree.  Inputs and outputs are the caller's
+ * device pointers; all scratch comes from one fixed 96 MiB device array that the
+ * library reserves at load time on every GPU it is used on.  Limits per call:
+ * at most 4096 jobs, proteins of at most 2048 residues, and scratch (about 2
+ * bytes per DP cell) within the array -- larger batches are rejected with a
+ * message (pl_noalloc_error) before any GPU work.  Calls share the array: the
+ * function returns only after its stream has finished and holds a library lock
+ * for its whole duration, so calls never overlap on the GPU.  The first call on
+ * a device looks up the array's address and caches it; make it before any
+ * stream capture begins.  Returns 1 on success. */
+int pl_splice_batch_noalloc(const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n_jobs,
+		const uint8_t *nt, const uint8_t *aa, const uint8_t *ss,
+		pl_splice_result_t *results_dev, uint32_t *cigar_dev, int64_t cigar_cap,
+		int64_t *total_cigar, void *stream);
+const char *pl_noalloc_error(void);
+
 /* Kernel launches issued by this library since load (all entry points). */
 uint64_t pl_kernel_launch_count(void);
 

@@ -61,6 +61,11 @@ def load() -> C.CDLL:
     lib.pl_engine_stream.restype = C.c_void_p
     lib.pl_measure_int_peak.argtypes = [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.pl_measure_int_peak.restype = C.c_int
+    lib.pl_splice_batch_noalloc.argtypes = [C.POINTER(NsOpt), C.POINTER(SpliceJob), C.c_int32, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                            C.POINTER(C.c_int64), C.c_void_p]
+    lib.pl_splice_batch_noalloc.restype = C.c_int
+    lib.pl_noalloc_error.restype = C.c_char_p
     _lib = lib
     return lib
 
