@@ -61,7 +61,16 @@ def parse():
     ap.add_argument("--pairs", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--uniform", default=None, metavar="N:NL:AL",
+                    help="profiling case instead of the batched workload: N planted loci of window NL and protein AL")
     return ap.parse_args()
+
+
+def make_jobs(args, seed):
+    if args.uniform:
+        n, nl, al = (int(x) for x in args.uniform.split(":"))
+        return [W.single_locus(seed=seed * 100003 + q, al=al, window=nl) for q in range(n)]
+    return W.batch_pairs(args.pairs, seed=seed)
 
 
 def pack(jobs):
@@ -166,7 +175,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    jobs = W.batch_pairs(args.pairs, seed=1)
+    jobs = make_jobs(args, 1)
     nt, aa, nt_off, aa_off, nl, al, _ = pack(jobs)
     opt = Options(flag=NS_F_CIGAR)
     per_step = args.cpu_seconds / 2
@@ -211,7 +220,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    jobs = W.batch_pairs(args.pairs, seed=1 + rank)
+    jobs = make_jobs(args, 1 + rank)
     nt, aa, nt_off, aa_off, nl, al, tab = pack(jobs)
     n = len(jobs)
     cells = int(((nl.astype(np.int64) - 2) * al).sum())
@@ -307,7 +316,7 @@ def main():
             "metric": METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(t / args.steps * 1e3, 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_jobs": n, "cells_per_step": cells, "seed": "1+rank",
+            "config": {"workload": WORKLOAD if not args.uniform else "profiling case " + args.uniform, "n_jobs": n, "cells_per_step": cells, "seed": "1+rank",
                        "l2": "inputs and the per-step traceback arena (tens of GB) are far larger than L2",
                        "waves": plan["waves"], "coop_jobs": plan["coop"], "parallelism": f"{world} independent ranks"},
             "e2e": e2e,
