@@ -217,6 +217,74 @@ const char *pl_noalloc_error(void);
 /* Kernel launches issued by this library since load (all entry points). */
 uint64_t pl_kernel_launch_count(void);
 
+/* ---------------------------------------------------------------------------
+ * Batched extension DP (replaces nasw-ext-gpu.c and nasw-ext-kernel.h).
+ * Results equal ns_global_gs16b() (nasw-sse.c:763-772) with the request's
+ * NS_F_EXT_LEFT / NS_F_EXT_RIGHT flag exactly: nt_len, aa_len and score of the
+ * x-drop extension, no CIGAR.  A request without an extension flag gets the
+ * plain global score H(nl-1, al-1) with nt_len = nl, aa_len = al, as
+ * ns_global_gs16b returns it without NS_F_CIGAR.  Every request runs on the
+ * device: position-specific scores (ns_opt_t.pssm), any protein length and
+ * mixed left/right requests included; requests with nl < 3 get the
+ * reference's no-row answer (nt_len 0) without a DP.
+ * ------------------------------------------------------------------------- */
+/* nasw.h:203 -- NULL when no device is usable (the caller then runs the CPU). */
+ns_ext_batch_t *ns_ext_batch_init(void *km);
+/* nasw.h:204 -- queue one request; returns its id.  Pointers must stay valid
+ * until the result has been fetched. */
+int32_t ns_ext_batch_add(ns_ext_batch_t *b, const char *ns, int32_t nl, const char *as, int32_t al,
+		const ns_opt_t *opt, const uint8_t *ss);
+/* nasw.h:205 -- hand the queued requests to the device; does not wait.
+ * Returns the number submitted. */
+int32_t ns_ext_batch_flush(ns_ext_batch_t *b);
+/* nasw.h:206 -- 1 when request `id` has completed (non-blocking). */
+int ns_ext_batch_ready(ns_ext_batch_t *b, int32_t id);
+/* nasw.h:207 -- sleep until some outstanding flush of b completes. */
+void ns_ext_batch_wait(ns_ext_batch_t *b);
+/* nasw.h:208 -- block until request `id` is done; the result stays valid until
+ * a later flush after every result of its flush was fetched. */
+const ns_rst_t *ns_ext_batch_get(ns_ext_batch_t *b, int32_t id);
+/* nasw.h:209 -- waits for b's outstanding flushes, then frees b. */
+void ns_ext_batch_destroy(ns_ext_batch_t *b);
+/* nasw.h:210-211 -- kernel launches of the extension path / requests run on the device. */
+uint64_t ns_ext_gpu_launch_count(void);
+uint64_t ns_ext_gpu_request_count(void);
+
+/* Bulk extension entry points (no counterpart in the reference, which only has
+ * the batch object above).  One job per request inside packed buffers. */
+typedef struct {
+	int64_t nt_off;    /* nucleotides in the packed nt buffer (ASCII or 0-4 codes) */
+	int64_t aa_off;    /* residues in the packed protein buffer (ASCII) */
+	int64_t ss_off;    /* splice-score track in the ss buffer, -1 = none */
+	int64_t pssm_off;  /* al x 22 int8 position-specific scores in the pssm buffer (query order), -1 = none */
+	int32_t nl, al;
+	int32_t flag;      /* NS_F_EXT_LEFT, NS_F_EXT_RIGHT, or 0 for the plain global score */
+	int32_t width;     /* stripe width of the CPU kernel being matched: 8, 16, or 0 = pl_ext_stripe_width() */
+} pl_ext_job_t;
+typedef struct {
+	int32_t nt_len, aa_len, score;
+	int32_t status;    /* 0 = ok; <0 = error (see pl_last_error()) */
+} pl_ext_result_t;
+/* Stripe width the reference CPU kernel uses on this host (nasw-sse.c:744-750):
+ * 16 for extension requests with al >= 16 when the CPU has AVX2, else 8.  The
+ * environment variable PLGPU_EXT_STRIPE=8 or 16 overrides the CPU probe (to
+ * match a reference built with no_avx2=1, or results from another machine). */
+int32_t pl_ext_stripe_width(const ns_opt_t *opt, int32_t al);
+/* Host buffers in, host results out.  opt->flag's extension bits and opt->pssm
+ * are ignored: every job carries its own.  Returns 1 on success. */
+int pl_ext_batch_host(pl_engine_t *e, const ns_opt_t *opt, const pl_ext_job_t *jobs, int32_t n_jobs,
+		const uint8_t *nt, int64_t nt_len, const uint8_t *aa, int64_t aa_len, const uint8_t *ss, int64_t ss_len,
+		const int8_t *pssm, int64_t pssm_len, pl_ext_result_t *results);
+/* Device-resident inputs and results (job table on the host); work is issued
+ * on `stream` (NULL = the engine's stream) and the call returns when it has
+ * completed.  Returns 1 on success. */
+int pl_ext_batch_device(pl_engine_t *e, const ns_opt_t *opt, const pl_ext_job_t *jobs, int32_t n_jobs,
+		const uint8_t *nt, const uint8_t *aa, const uint8_t *ss, const int8_t *pssm,
+		pl_ext_result_t *results_dev, void *stream);
+/* DP cells of the last extension batch: rows the DP actually ran (the x-drop
+ * stops a request early) times padded columns, and the nominal (nl-2)*al. */
+void pl_ext_last_cells(const pl_engine_t *e, int64_t *cells_run, int64_t *cells_nominal);
+
 #ifdef __cplusplus
 }
 #endif

@@ -233,8 +233,11 @@ static void port_dp(const ns_opt_t *opt, port_mode_t m, int32_t nl, int32_t al,
 	prof = Hmax + ncol;
 	for (i = 0; i < ncol * 12; ++i) buf[i] = NEG;
 	for (a = 0; a < opt->asize; ++a) /* query profile, nasw-sse.c:223-235 (padding = neg_inf) */
-		for (c = 0; c < ncol; ++c)
-			prof[a * ncol + c] = c >= al ? NEG : opt->sc[a * opt->asize + aas[c]];
+		for (c = 0; c < ncol; ++c) {
+			/* position-specific scores (nasw-sse.c:217-221): rows in query order, reversed for a left extension */
+			const int32_t q = (opt->flag & NS_F_EXT_LEFT) ? al - 1 - c : c;
+			prof[a * ncol + c] = c >= al ? NEG : opt->pssm ? opt->pssm[q * opt->asize + a] : opt->sc[a * opt->asize + aas[c]];
+		}
 
 	for (i = 2; i < nl; ++i) {
 		int32_t *H = Hr[i & 3], *H1 = Hr[(i - 1) & 3], *H2 = Hr[(i - 2) & 3], *H3 = Hr[(i - 3) & 3];

@@ -124,7 +124,20 @@ class SpliceResult(C.Structure):
                 ("mode", C.c_int32), ("status", C.c_int32)]
 
 
+class ExtJob(C.Structure):
+    """pl_ext_job_t"""
+    _fields_ = [("nt_off", C.c_int64), ("aa_off", C.c_int64), ("ss_off", C.c_int64), ("pssm_off", C.c_int64),
+                ("nl", C.c_int32), ("al", C.c_int32), ("flag", C.c_int32), ("width", C.c_int32)]
+
+
+class ExtResult(C.Structure):
+    """pl_ext_result_t"""
+    _fields_ = [("nt_len", C.c_int32), ("aa_len", C.c_int32), ("score", C.c_int32), ("status", C.c_int32)]
+
+
 assert C.sizeof(NsOpt) == 120, C.sizeof(NsOpt)
+assert C.sizeof(ExtJob) == 48
+assert C.sizeof(ExtResult) == 16
 assert C.sizeof(SpliceJob) == 32
 assert C.sizeof(SpliceResult) == 24
 
@@ -161,8 +174,20 @@ class Options:
     def with_flag(self, flag: int) -> "Options":
         n = Options.__new__(Options)
         n.nt4, n.aa20, n.codon, n.mat = self.nt4, self.aa20, self.codon, self.mat
+        n.pssm_arr = getattr(self, "pssm_arr", None)
         n.c = NsOpt.from_buffer_copy(self.c)
         n.c.flag = flag
+        return n
+
+    def with_pssm(self, pssm: np.ndarray | None) -> "Options":
+        """A copy whose ns_opt_t.pssm points at `pssm` (al x 22 int8, rows in query order; nasw.h:73)."""
+        n = self.with_flag(self.c.flag)
+        if pssm is None:
+            n.pssm_arr = None
+            n.c.pssm = None
+        else:
+            n.pssm_arr = np.ascontiguousarray(pssm, dtype=np.int8).reshape(-1)
+            n.c.pssm = n.pssm_arr.ctypes.data_as(C.POINTER(C.c_int8))
         return n
 
     @classmethod

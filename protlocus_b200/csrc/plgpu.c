@@ -33,8 +33,8 @@
 #include <cuda_runtime_api.h>
 #include "plk.h"
 #include "../../include/plgpu.h"
+#include "plhost.h"
 
-#define PL_EXPORT __attribute__((visibility("default")))
 
 /* ------------------------------------------------------------------ km allocator hooks
  * The CIGAR of a request is appended into the caller's kalloc arena, as
@@ -57,7 +57,7 @@ __attribute__((weak)) void kfree(void *km, void *ptr)
 static pthread_mutex_t pl_err_mu = PTHREAD_MUTEX_INITIALIZER;
 static char pl_err[1024] = "none";
 
-static void pl_set_error(const char *fmt, ...)
+void pl_set_error(const char *fmt, ...)
 {
 	va_list ap;
 	pthread_mutex_lock(&pl_err_mu);
@@ -69,16 +69,9 @@ static void pl_set_error(const char *fmt, ...)
 
 PL_EXPORT const char *pl_last_error(void) { return pl_err; }
 
-#define CK(call) do { cudaError_t _e = (call); if (_e != cudaSuccess) { \
-	pl_set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, __LINE__); goto fail; } } while (0)
-#define CKK(call) do { int _e = (call); if (_e != 0) { \
-	pl_set_error("%s failed: %s", #call, cudaGetErrorString((cudaError_t)_e)); goto fail; } } while (0)
-
 /* ------------------------------------------------------------------ buffers */
 
-typedef struct { void *p; size_t cap; } dbuf_t;
-
-static int dbuf_ensure(dbuf_t *b, size_t need)
+int dbuf_ensure(dbuf_t *b, size_t need)
 {
 	if (need == 0) need = 16;
 	if (b->cap >= need) return 1;
@@ -93,25 +86,7 @@ static int dbuf_ensure(dbuf_t *b, size_t need)
 	return 1;
 }
 
-static void dbuf_free(dbuf_t *b) { if (b->p) cudaFree(b->p); b->p = 0, b->cap = 0; }
-
-struct pl_engine_s {
-	int device, n_sm, ctas_per_sm[3];
-	cudaStream_t stream;
-	int64_t trace_budget;
-	dbuf_t jobs, order, counters, prep, trace, ring, tmp, total, nt, aa, ss, res, cig;
-	/* host planning scratch */
-	plk_job_t *hj;
-	int32_t *horder, *hwave, m_jobs;
-	int32_t last_waves, last_coop, last_dp_launches;
-	/* optional CUDA-event timing of the phases: prep, DP, traceback, compaction */
-	int timing;
-	cudaEvent_t ev[2 + 4 * 64];
-	int n_ev;
-	unsigned char ev_kind[2 + 4 * 64];
-	double acc_ms[4];
-	int64_t acc_dp_launches, acc_cells;
-};
+void dbuf_free(dbuf_t *b) { if (b->p) cudaFree(b->p); b->p = 0, b->cap = 0; }
 
 #define PL_TIME(e, st, k) do { if ((e)->timing && (e)->n_ev < (int)(sizeof((e)->ev) / sizeof((e)->ev[0]))) { \
 	(e)->ev_kind[(e)->n_ev] = (k); cudaEventRecord((e)->ev[(e)->n_ev++], (st)); } } while (0)
@@ -151,6 +126,7 @@ PL_EXPORT void pl_engine_destroy(pl_engine_t *e)
 	dbuf_free(&e->jobs), dbuf_free(&e->order), dbuf_free(&e->counters), dbuf_free(&e->prep);
 	dbuf_free(&e->trace), dbuf_free(&e->ring), dbuf_free(&e->tmp), dbuf_free(&e->total);
 	dbuf_free(&e->nt), dbuf_free(&e->aa), dbuf_free(&e->ss), dbuf_free(&e->res), dbuf_free(&e->cig);
+	pl_ext_engine_free(e);
 	if (e->stream) cudaStreamDestroy(e->stream);
 	free(e->hj), free(e->horder), free(e->hwave);
 	free(e);
@@ -193,13 +169,13 @@ PL_EXPORT void pl_engine_last_plan(const pl_engine_t *e, int32_t *n_waves, int32
 
 /* ------------------------------------------------------------------ planning */
 
-static int pl_params(const ns_opt_t *opt, plk_params_t *p)
+int pl_params(const ns_opt_t *opt, plk_params_t *p, int for_ext)
 {
 	int i;
 	if (!opt || !opt->sc || !opt->nt4 || !opt->aa20 || !opt->codon) { pl_set_error("incomplete ns_opt_t"); return 0; }
 	if (opt->asize != 22) { pl_set_error("asize %d unsupported (22 only)", opt->asize); return 0; }
-	if (opt->pssm) { pl_set_error("position-specific scores are CPU-only in the reference (nasw.h:73)"); return 0; }
-	if (opt->flag & (NS_F_EXT_LEFT | NS_F_EXT_RIGHT)) { pl_set_error("extension DPs go through ns_ext_batch_*, not the global path"); return 0; }
+	if (!for_ext && opt->pssm) { pl_set_error("position-specific scores are CPU-only in the reference's global path (nasw.h:73)"); return 0; }
+	if (!for_ext && (opt->flag & (NS_F_EXT_LEFT | NS_F_EXT_RIGHT))) { pl_set_error("extension DPs go through the ext entry points, not the global path"); return 0; }
 	memset(p, 0, sizeof(*p));
 	p->go = opt->go, p->ge = opt->ge, p->io = opt->io, p->fs = opt->fs;
 	p->end_bonus = opt->end_bonus, p->xdrop = opt->xdrop;
@@ -211,7 +187,7 @@ static int pl_params(const ns_opt_t *opt, plk_params_t *p)
 	return 1;
 }
 
-static int pl_max_sub(const ns_opt_t *opt)
+int pl_max_sub(const ns_opt_t *opt)
 {
 	int i, m = 0;
 	for (i = 0; i < opt->asize * opt->asize; ++i) if (m < opt->sc[i]) m = opt->sc[i];
@@ -258,7 +234,7 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 
 	e->last_waves = e->last_coop = e->last_dp_launches = 0;
 	if (n <= 0) { if (total_out) *total_out = 0; return 1; }
-	if (!pl_params(opt, &P)) return 0;
+	if (!pl_params(opt, &P, 0)) return 0;
 	if (!pl_grow_host(e, n)) return 0;
 	max_sub = pl_max_sub(opt);
 	slots = (int64_t)e->n_sm * e->ctas_per_sm[0] * PLK_WARPS_PER_CTA;

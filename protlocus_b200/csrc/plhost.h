@@ -1,0 +1,52 @@
+/*
+ * plhost.h -- internals shared by the host translation units of libplgpu
+ * (plgpu.c: engine, global DP, request queue; plext.c: extension DP).
+ */
+#ifndef PLHOST_H
+#define PLHOST_H
+#include <cuda_runtime_api.h>
+#include "plk.h"
+#include "../../include/plgpu.h"
+
+#define PL_EXPORT __attribute__((visibility("default")))
+
+#define CK(call) do { cudaError_t _e = (call); if (_e != cudaSuccess) { \
+	pl_set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, __LINE__); goto fail; } } while (0)
+#define CKK(call) do { int _e = (call); if (_e != 0) { \
+	pl_set_error("%s failed: %s", #call, cudaGetErrorString((cudaError_t)_e)); goto fail; } } while (0)
+
+/* grow-only device buffer */
+typedef struct { void *p; size_t cap; } dbuf_t;
+int dbuf_ensure(dbuf_t *b, size_t need);
+void dbuf_free(dbuf_t *b);
+
+struct pl_engine_s {
+	int device, n_sm, ctas_per_sm[3];
+	cudaStream_t stream;
+	int64_t trace_budget;
+	dbuf_t jobs, order, counters, prep, trace, ring, tmp, total, nt, aa, ss, res, cig;
+	/* extension DP */
+	dbuf_t x_jobs, x_order, x_counter, x_prep, x_ring, x_nt, x_aa, x_ss, x_pssm, x_res;
+	plk_ext_job_t *x_hj;
+	int32_t *x_horder, x_m;
+	int32_t x_last_launches;
+	int64_t x_cells_run, x_cells_nominal;
+	/* host planning scratch */
+	plk_job_t *hj;
+	int32_t *horder, *hwave, m_jobs;
+	int32_t last_waves, last_coop, last_dp_launches;
+	/* optional CUDA-event timing of the phases: prep, DP, traceback, compaction */
+	int timing;
+	cudaEvent_t ev[2 + 4 * 64];
+	int n_ev;
+	unsigned char ev_kind[2 + 4 * 64];
+	double acc_ms[4];
+	int64_t acc_dp_launches, acc_cells;
+};
+
+void pl_set_error(const char *fmt, ...);
+int pl_params(const ns_opt_t *opt, plk_params_t *p, int for_ext);
+int pl_max_sub(const ns_opt_t *opt);
+void pl_ext_engine_free(pl_engine_t *e);
+
+#endif

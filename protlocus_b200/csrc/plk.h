@@ -44,6 +44,21 @@ typedef struct {
 	int32_t status, pad;
 } plk_job_t;
 
+/* per-request metadata of the extension DP, device resident */
+typedef struct {
+	int64_t nt_off, aa_off, ss_off;  /* inputs (ss_off < 0: no splice-score track) */
+	int64_t pssm_off;                /* al x 22 position-specific scores in query order (< 0: none) */
+	int64_t prep_off;                /* nas[nl] | aas[al] | donor[nl+1] | acceptor[nl+1] */
+	int32_t nl, al;
+	int32_t left;                    /* 0: right extension, 1: left (reversed inputs), 2: plain global score */
+	int32_t slen, ncol;              /* stripe segment length and padded column count slen*width */
+	int32_t mode;                    /* 0: int16 lower clamp only, 2: both clamps */
+	int32_t variant;                 /* bit 0: position-specific scores, bit 1: wide row keys */
+	int32_t nt_len, aa_len, score;   /* outputs */
+	int32_t status;                  /* 0 = ok */
+	int32_t pad;
+} plk_ext_job_t;
+
 /* bytes of preparation scratch for a job (8-aligned) */
 static inline int64_t plk_prep_bytes(int32_t nl, int32_t al)
 {
@@ -69,6 +84,22 @@ int plk_traceback(plk_job_t *jobs, const int32_t *order, int32_t n_order, const 
 		uint32_t *tmp, void *stream);
 int plk_scan_compact(plk_job_t *jobs, int32_t n_jobs, const uint32_t *tmp, uint32_t *out, int64_t out_cap,
 		int64_t *total_words, void *result_recs, void *stream);
+/* extension DP: preparation in either orientation, then the score-only DP over
+ * `order` (one warp per request).  counter: 16 bytes of device scratch -- int32 [0]
+ * is the queue position (reset per launch), uint64 at byte 8 accumulates the DP
+ * cells run (rows processed x al; reset by the caller); ring:
+ * plk_ext_warps_per_cta() * n_ctas * ring_stride_ints ints; pssm: base of the
+ * position-specific score buffer (variant bit 0). */
+int plk_ext_prep(const plk_ext_job_t *jobs, int32_t n_jobs, const uint8_t *nt, const uint8_t *aa, const uint8_t *ss,
+		uint8_t *prep, const plk_params_t *p, void *stream);
+int plk_ext_dp(plk_ext_job_t *jobs, const int32_t *order, int32_t n_jobs, int32_t *counter, const uint8_t *prep,
+		const int8_t *pssm, int32_t *ring, int64_t ring_stride_ints, int32_t n_ctas, int32_t mode, int32_t variant,
+		const plk_params_t *p, void *stream);
+int plk_ext_ctas_per_sm(int32_t mode, int32_t variant);
+int plk_ext_warps_per_cta(void);
+/* results[q] (pl_ext_result_t) from the job table */
+int plk_ext_results(const plk_ext_job_t *jobs, int32_t n_jobs, void *results, void *stream);
+void plk_add_launches(uint64_t n);
 /* CTAs of the DP kernel that fit on one SM at once (occupancy) */
 int plk_dp_ctas_per_sm(int32_t mode);
 uint64_t plk_launches(void);

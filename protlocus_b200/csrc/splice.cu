@@ -36,29 +36,7 @@
 
 static unsigned long long g_launches = 0;
 
-#define FULL 0xffffffffu
-
-/* ------------------------------------------------------------------ arithmetic modes
- * MODE 0: int16 semantics where no value can reach +32767 (al*max(sc)+256 < 32767):
- *         _mm_subs/_mm_adds_epi16 reduce to a clamp at -32768.
- * MODE 1: int32 semantics of ns_global_gs32b (no saturation, neg_inf -2^30).
- * MODE 2: int16 semantics with both clamps (long proteins). */
-template <int MODE> struct Ar;
-template <> struct Ar<0> {
-	static constexpr int NEG = -32768;
-	static __device__ __forceinline__ int sub(int x, int k) { return max(x - k, NEG); }
-	static __device__ __forceinline__ int add(int x, int k) { return max(x + k, NEG); }
-};
-template <> struct Ar<1> {
-	static constexpr int NEG = -0x40000000;
-	static __device__ __forceinline__ int sub(int x, int k) { return x - k; }
-	static __device__ __forceinline__ int add(int x, int k) { return x + k; }
-};
-template <> struct Ar<2> {
-	static constexpr int NEG = -32768;
-	static __device__ __forceinline__ int sub(int x, int k) { return min(max(x - k, NEG), 32767); }
-	static __device__ __forceinline__ int add(int x, int k) { return min(max(x + k, NEG), 32767); }
-};
+#include "dp_common.cuh"
 
 /* ------------------------------------------------------------------ preparation */
 
@@ -75,49 +53,9 @@ __global__ void k_prep(const plk_job_t *__restrict__ jobs, int n_jobs, const uin
 		const uint8_t *ns = nt + J.nt_off, *as = aa + J.aa_off, *sst = J.ss_off >= 0 ? ss + J.ss_off : 0;
 		uint8_t *nas = prep + J.prep_off, *aas = nas + nl;
 		int8_t *donor = (int8_t*)(aas + al), *acceptor = donor + nl + 1;
-		const int max_spsc = (P.io + 1) / 2 - 1;
-#define B4(q) ((q) >= 0 && (q) < nl ? s_nt4[ns[(q)]] : 4)
 		for (int j = threadIdx.x; j < al; j += blockDim.x) aas[j] = s_aa20[as[j]];
-		for (int p = threadIdx.x; p <= nl; p += blockDim.x) {
-			int dv = P.sp[3], av = P.sp[3];
-			if (p < nl - 3) { /* nasw-sse.c:124-131 */
-				const int b0 = B4(p), b1 = B4(p + 1), b2 = B4(p + 2), b3 = B4(p + 3);
-				int t = 3;
-				if (b1 == 2 && b2 == 3) t = (b3 == 0 || b3 == 2) ? (b0 == 2 ? -1 : 4) : 0;
-				else if (b1 == 2 && b2 == 1 && b0 == 2) t = 1;
-				else if (b1 == 0 && b2 == 3) t = 2;
-				dv = t < 0 ? 0 : P.sp[t];
-			}
-			int8_t d8 = (int8_t)dv, a8 = (int8_t)av;
-			if (p >= 1 && p < nl) { /* nasw-sse.c:132-141 */
-				const int bm1 = B4(p - 1), b0 = B4(p);
-				int t = 3, pen = 0;
-				if (bm1 == 0 && b0 == 2) {
-					const int bm2 = B4(p - 2);
-					t = (p >= 2 && (bm2 == 1 || bm2 == 3)) ? -1 : 0;
-					for (int q = p - 4; q >= 0 && q > p - 7; --q) {
-						const int bq = B4(q);
-						if (bq != 1 && bq != 3) pen += P.sp[5];
-					}
-				} else if (bm1 == 0 && b0 == 1) t = 2;
-				a8 = (int8_t)(t < 0 ? 0 : P.sp[t]);
-				if (t == -1 || t == 0) a8 = (int8_t)(a8 + pen);
-			}
-			if (sst && p + 1 >= 1 && p + 1 < nl) { /* nasw-sse.c:142-156 */
-				const uint8_t x = sst[p + 1];
-				int spsc = (int8_t)(x >> 1) - (int8_t)NS_SPSC_OFFSET;
-				if (spsc > max_spsc) spsc = max_spsc;
-				if (x == 0xff) d8 = (int8_t)(d8 - P.sp_null_bonus), a8 = (int8_t)(a8 - P.sp_null_bonus);
-				else if (x & 1) a8 = (int8_t)(a8 - spsc);
-				else d8 = (int8_t)(d8 - spsc);
-			}
-			donor[p] = d8, acceptor[p] = a8;
-			if (p < nl) { /* nasw-sse.c:95-108 */
-				const int b2 = B4(p), b1 = B4(p - 1), b0 = B4(p - 2);
-				nas[p] = (p >= 2 && b0 < 4 && b1 < 4 && b2 < 4) ? s_codon[(b0 << 4 | b1 << 2 | b2) & 0x3f] : P.aa_x;
-			}
-		}
-#undef B4
+		for (int p = threadIdx.x; p <= nl; p += blockDim.x)
+			prep_fwd_pos(p, ns, nl, sst, s_nt4, s_codon, P, nas, donor, acceptor);
 	}
 }
 
@@ -130,12 +68,6 @@ struct DpShared {
 	int32_t pre[PLK_WARPS_PER_CTA][PLK_RING_INTS] __attribute__((aligned(16)));
 };
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
-{
-	const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 /*
  * Trace word of a cell (all modes): bits 0-3 = 15 - state (state 0..9 in the
@@ -663,3 +595,4 @@ extern "C" int plk_scan_compact(plk_job_t *jobs, int32_t n_jobs, const uint32_t 
 }
 
 extern "C" uint64_t plk_launches(void) { return __sync_fetch_and_add(&g_launches, 0ull); }
+extern "C" void plk_add_launches(uint64_t n) { __sync_fetch_and_add(&g_launches, (unsigned long long)n); }

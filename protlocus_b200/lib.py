@@ -11,7 +11,7 @@ import re
 
 import numpy as np
 
-from .abi import NsOpt, NsRst, SpliceJob, SpliceResult
+from .abi import ExtJob, ExtResult, NsOpt, NsRst, SpliceJob, SpliceResult
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libplgpu.so")
@@ -66,6 +66,31 @@ def load() -> C.CDLL:
                                             C.POINTER(C.c_int64), C.c_void_p]
     lib.pl_splice_batch_noalloc.restype = C.c_int
     lib.pl_noalloc_error.restype = C.c_char_p
+    lib.pl_ext_stripe_width.argtypes = [C.POINTER(NsOpt), C.c_int32]
+    lib.pl_ext_stripe_width.restype = C.c_int32
+    lib.pl_ext_batch_host.argtypes = [C.c_void_p, C.POINTER(NsOpt), C.POINTER(ExtJob), C.c_int32,
+                                      C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                      C.c_void_p, C.c_int64, C.POINTER(ExtResult)]
+    lib.pl_ext_batch_host.restype = C.c_int
+    lib.pl_ext_batch_device.argtypes = [C.c_void_p, C.POINTER(NsOpt), C.POINTER(ExtJob), C.c_int32,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.pl_ext_batch_device.restype = C.c_int
+    lib.pl_ext_last_cells.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.ns_ext_batch_init.argtypes = [C.c_void_p]
+    lib.ns_ext_batch_init.restype = C.c_void_p
+    lib.ns_ext_batch_add.argtypes = [C.c_void_p, C.c_char_p, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(NsOpt),
+                                     C.c_void_p]
+    lib.ns_ext_batch_add.restype = C.c_int32
+    lib.ns_ext_batch_flush.argtypes = [C.c_void_p]
+    lib.ns_ext_batch_flush.restype = C.c_int32
+    lib.ns_ext_batch_ready.argtypes = [C.c_void_p, C.c_int32]
+    lib.ns_ext_batch_ready.restype = C.c_int
+    lib.ns_ext_batch_wait.argtypes = [C.c_void_p]
+    lib.ns_ext_batch_get.argtypes = [C.c_void_p, C.c_int32]
+    lib.ns_ext_batch_get.restype = C.POINTER(NsRst)
+    lib.ns_ext_batch_destroy.argtypes = [C.c_void_p]
+    for fn in ("ns_ext_gpu_launch_count", "ns_ext_gpu_request_count"):
+        getattr(lib, fn).restype = C.c_uint64
     _lib = lib
     return lib
 
@@ -161,6 +186,107 @@ class Engine:
                 raise RuntimeError(f"job {q}: status {r.status}")
             out.append((r.score, cig[r.cigar_off:r.cigar_off + r.n_cigar].tolist(), r.mode))
         return out
+
+
+    def ext_host(self, opt, reqs):
+        """Batched extension DP through pl_ext_batch_host.  reqs: list of dicts with
+        keys nt, aa (bytes), flag (NS_F_EXT_LEFT/RIGHT or 0), optional ss (bytes),
+        pssm (al x 22 int8 array) and width (8/16, default: this host's rule).
+        Returns a list of (score, nt_len, aa_len)."""
+        n = len(reqs)
+        jobs = (ExtJob * n)()
+        nt_parts, aa_parts, ss_parts, ps_parts = [], [], [], []
+        pn = pa = pss = pps = 0
+        for q, r in enumerate(reqs):
+            nt, aa = r["nt"], r["aa"]
+            j = jobs[q]
+            j.nt_off, j.aa_off, j.nl, j.al = pn, pa, len(nt), len(aa)
+            j.flag, j.width = r.get("flag", 0), r.get("width", 0)
+            j.ss_off = j.pssm_off = -1
+            nt_parts.append(nt)
+            aa_parts.append(aa)
+            pn += len(nt)
+            pa += len(aa)
+            if r.get("ss") is not None:
+                j.ss_off = pss
+                ss_parts.append(bytes(r["ss"]))
+                pss += len(r["ss"])
+            if r.get("pssm") is not None:
+                m = np.ascontiguousarray(r["pssm"], dtype=np.int8).reshape(-1)
+                j.pssm_off = pps
+                ps_parts.append(m.tobytes())
+                pps += m.size
+        ntb = np.frombuffer(b"".join(nt_parts) or b"\0", dtype=np.uint8)
+        aab = np.frombuffer(b"".join(aa_parts) or b"\0", dtype=np.uint8)
+        ssb = np.frombuffer(b"".join(ss_parts), dtype=np.uint8) if ss_parts else None
+        psb = np.frombuffer(b"".join(ps_parts), dtype=np.int8) if ps_parts else None
+        res = (ExtResult * max(n, 1))()
+        ok = self.lib.pl_ext_batch_host(self.h, opt.ptr, jobs, n, ntb.ctypes.data, ntb.size, aab.ctypes.data,
+                                        aab.size, ssb.ctypes.data if ssb is not None else None,
+                                        ssb.size if ssb is not None else 0,
+                                        psb.ctypes.data if psb is not None else None,
+                                        psb.size if psb is not None else 0, res)
+        if not ok:
+            raise RuntimeError("pl_ext_batch_host failed: " + error())
+        out = []
+        for q in range(n):
+            if res[q].status != 0:
+                raise RuntimeError(f"ext job {q}: status {res[q].status}")
+            out.append((res[q].score, res[q].nt_len, res[q].aa_len))
+        return out
+
+    def ext_last_cells(self):
+        a, b = C.c_int64(), C.c_int64()
+        self.lib.pl_ext_last_cells(self.h, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+
+def ext_stripe_width(opt, al: int) -> int:
+    return int(load().pl_ext_stripe_width(opt.ptr, al))
+
+
+class ExtBatch:
+    """The reference's batch object (ns_ext_batch_*): add / flush / ready / wait / get."""
+
+    def __init__(self):
+        self.lib = load()
+        self.h = self.lib.ns_ext_batch_init(None)
+        if not self.h:
+            raise RuntimeError("ns_ext_batch_init returned NULL: " + error())
+        self._keep = []
+
+    def add(self, nt: bytes, aa: bytes, opt, ss: bytes | None = None) -> int:
+        ntb, aab = C.create_string_buffer(nt, len(nt)), C.create_string_buffer(aa, len(aa))
+        ssb = C.create_string_buffer(bytes(ss), len(ss)) if ss is not None else None
+        self._keep += [ntb, aab, ssb, opt]  # inputs must stay valid until fetched (nasw.h:201-202)
+        return self.lib.ns_ext_batch_add(self.h, ntb, len(nt), aab, len(aa), opt.ptr, ssb)
+
+    def flush(self) -> int:
+        return self.lib.ns_ext_batch_flush(self.h)
+
+    def ready(self, rid: int) -> bool:
+        return bool(self.lib.ns_ext_batch_ready(self.h, rid))
+
+    def wait(self):
+        self.lib.ns_ext_batch_wait(self.h)
+
+    def get(self, rid: int):
+        p = self.lib.ns_ext_batch_get(self.h, rid)
+        if not p:
+            raise KeyError(rid)
+        r = p.contents
+        return (r.score, r.nt_len, r.aa_len)
+
+    def close(self):
+        if self.h:
+            self.lib.ns_ext_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def measure_int_peak(device: int = 0):

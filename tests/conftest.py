@@ -26,3 +26,10 @@ def golden():
     import json
     with open(os.path.join(HERE, "golden", "splice_golden.json")) as f:
         return json.load(f)
+
+
+@pytest.fixture(scope="session")
+def ext_golden():
+    import json
+    with open(os.path.join(HERE, "golden", "ext_golden.json")) as f:
+        return json.load(f)

@@ -19,6 +19,7 @@ from protlocus_b200.abi import AA_I2C, BLOSUM62, NS_F_CIGAR, NS_S_NONE, NsOpt, N
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE = os.path.join(ROOT, "oracle")
 REF_SO = os.path.join(ORACLE, "_ref", "libnsref.so")
+REF8_SO = os.path.join(ORACLE, "_ref", "libnsref8.so")  # built with the reference's no-AVX2 switch
 PORT_SO = os.path.join(ORACLE, "_build", "libnsport.so")
 
 _ref = None
@@ -32,22 +33,37 @@ def build_port():
         subprocess.run(["make", "-C", ORACLE, "port"], check=True, capture_output=True)
 
 
+def _load_ref(path):
+    lib = C.CDLL(path)
+    if lib.ns_make_tables(1) != 0:
+        raise RuntimeError("reference ns_make_tables(1) failed")
+    for fn in ("ns_global_gs16b", "ns_global_gs32b", "ns_global_gs_auto"):
+        f = getattr(lib, fn)
+        f.argtypes = [C.c_void_p, C.c_char_p, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(NsOpt),
+                      C.c_void_p, C.POINTER(NsRst)]
+        f.restype = None
+    lib.ns_ext_stripe_width.argtypes = [C.POINTER(NsOpt), C.c_int32]
+    lib.ns_ext_stripe_width.restype = C.c_int32
+    return lib
+
+
 def ref_lib():
     """The compiled reference, or None when oracle/_ref was not built on this machine."""
     global _ref
     if _ref is None and os.path.exists(REF_SO):
-        lib = C.CDLL(REF_SO)
-        if lib.ns_make_tables(1) != 0:
-            raise RuntimeError("reference ns_make_tables(1) failed")
-        for fn in ("ns_global_gs16b", "ns_global_gs32b", "ns_global_gs_auto"):
-            f = getattr(lib, fn)
-            f.argtypes = [C.c_void_p, C.c_char_p, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(NsOpt),
-                          C.c_void_p, C.POINTER(NsRst)]
-            f.restype = None
-        lib.ns_ext_stripe_width.argtypes = [C.POINTER(NsOpt), C.c_int32]
-        lib.ns_ext_stripe_width.restype = C.c_int32
-        _ref = lib
+        _ref = _load_ref(REF_SO)
     return _ref
+
+
+_ref8 = None
+
+
+def ref8_lib():
+    """The reference compiled without AVX2 dispatch (8-lane ext stripes), or None."""
+    global _ref8
+    if _ref8 is None and os.path.exists(REF8_SO):
+        _ref8 = _load_ref(REF8_SO)
+    return _ref8
 
 
 def port_lib():
@@ -92,9 +108,10 @@ def _buf(x):
     return C.c_char_p(bytes(x))
 
 
-def ref_run(fn: str, ns: bytes, aa: bytes, opt, ss: bytes | None = None):
-    """Run reference `fn` (ns_global_gs16b / gs32b / gs_auto); returns (score, nt_len, aa_len, cigar)."""
-    lib = ref_lib()
+def ref_run(fn: str, ns: bytes, aa: bytes, opt, ss: bytes | None = None, width8: bool = False):
+    """Run reference `fn` (ns_global_gs16b / gs32b / gs_auto); returns (score, nt_len, aa_len, cigar).
+    width8 selects the build without AVX2 dispatch (8-lane ext stripes)."""
+    lib = ref8_lib() if width8 else ref_lib()
     r = NsRst()
     ssb = C.create_string_buffer(bytes(ss), len(ss)) if ss is not None else None
     getattr(lib, fn)(None, ns, len(ns), aa, len(aa), opt.ptr, ssb, C.byref(r))
@@ -139,3 +156,14 @@ def make_options(spec: dict) -> Options:
         m[w, w] = 127
         return Options.nasw_defaults(flag=flag, matrix=m)
     raise ValueError(kind)
+
+
+def make_ext_options(spec: dict) -> Options:
+    """Option sets of the extension fixtures (tests/golden/make_ext_golden.py): make_options plus
+    seeded position-specific scores (al x 22, uniform in [-6, 9]) when spec has pssm_seed."""
+    import numpy as np
+    o = make_options(spec)
+    if spec.get("pssm_seed") is not None:
+        rng = np.random.default_rng(spec["pssm_seed"])
+        o = o.with_pssm(rng.integers(-6, 10, size=(spec["al"], 22)).astype(np.int8))
+    return o

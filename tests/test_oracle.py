@@ -39,6 +39,15 @@ def test_port_matches_golden(oracle, golden):
     assert n == len(golden["cases"]) and n > 400
 
 
+def test_port_matches_ext_golden(oracle, ext_golden):
+    """The restatement reproduces every extension golden vector of the reference (both stripe widths)."""
+    for c in ext_golden["cases"]:
+        opt = oracle.make_ext_options(c["opt"])
+        ss = bytes.fromhex(c["ss"]) if c["ss"] else None
+        got = oracle.port_run("gs16b", c["nt"].encode(), c["aa"].encode(), opt, ss, avx2=c["width"] == 16)
+        assert got[:3] == (c["score"], c["nt_len"], c["aa_len"]), c
+
+
 def test_dp32_known_answers(oracle):
     """test/test_dp32.c assertions, on the restatement."""
     opt = Options.nasw_defaults(flag=NS_F_CIGAR, go=3, ge=1, io=100, fs=100, sp_model=0)
