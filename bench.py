@@ -43,7 +43,7 @@ sys.path.insert(0, ROOT)
 
 from protlocus_b200 import lib as L  # noqa: E402
 from protlocus_b200 import workload as W  # noqa: E402
-from protlocus_b200.abi import NS_F_CIGAR, Options, SpliceJob, SpliceResult  # noqa: E402
+from protlocus_b200.abi import NS_F_CIGAR, ExtJob, ExtResult, Options, SpliceJob, SpliceResult  # noqa: E402
 
 METRIC = "spliced-DP GCUPS (bit-exact) at 1 B200"
 OPS_PER_CELL = 65  # int16 lane-ops per cell with traceback bits, counted from nasw-sse.c:465-553
@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--pairs", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="global", choices=["global", "ext"],
+                    help="global: the batched global spliced DP (headline); ext: the batched extension DP")
+    ap.add_argument("--requests", type=int, default=65536, help="extension requests per step (--workload ext)")
     ap.add_argument("--uniform", default=None, metavar="N:NL:AL",
                     help="profiling case instead of the batched workload: N planted loci of window NL and protein AL")
     return ap.parse_args()
@@ -198,6 +201,8 @@ def run_reference(args):
 
 def main():
     args = parse()
+    if args.workload == "ext":
+        return run_reference_ext(args) if args.impl == "reference" else main_ext(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -327,6 +332,224 @@ def main():
                          "peak_source": "measured live: pl_measure_int_peak (int32 %.3g, int16x2 %.3g lane-ops/s)"
                                         % (int32_peak, i16x2_peak),
                          "phase_ms_per_step": {k: round(v / args.steps, 2) for k, v in tm.items() if k.endswith("_ms")}},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+# ---------------------------------------------------------------------------- extension DP
+
+EXT_METRIC = "extension-DP GCUPS (bit-exact, nominal cells (nl-2)*al per request) at 1 B200"
+EXT_OPS_PER_CELL = 31  # int16 lane-ops per cell of the score-only kernel, counted from nasw-sse.c:366-419
+EXT_WORKLOAD = ("batched extension DP: 65536 requests, protein window 64-256 aa, nt window 3x + 60-600 nt slack "
+                "(+ introns), alternating left/right, mutated gene copy over 30-100% of the window then random "
+                "sequence (x-drop ends the DP), ProtLocus default scoring")
+
+
+def ext_pack(reqs, width=0):
+    n = len(reqs)
+    nl = np.array([len(a) for a, _, _ in reqs], dtype=np.int32)
+    al = np.array([len(b) for _, b, _ in reqs], dtype=np.int32)
+    flag = np.array([f for _, _, f in reqs], dtype=np.int32)
+    nt_off = np.zeros(n, dtype=np.int64)
+    aa_off = np.zeros(n, dtype=np.int64)
+    nt_off[1:] = np.cumsum(nl[:-1])
+    aa_off[1:] = np.cumsum(al[:-1])
+    nt = np.frombuffer(b"".join(a for a, _, _ in reqs), dtype=np.uint8)
+    aa = np.frombuffer(b"".join(b for _, b, _ in reqs), dtype=np.uint8)
+    tab = (ExtJob * n)()
+    for q in range(n):
+        j = tab[q]
+        j.nt_off, j.aa_off, j.ss_off, j.pssm_off = int(nt_off[q]), int(aa_off[q]), -1, -1
+        j.nl, j.al, j.flag, j.width = int(nl[q]), int(al[q]), int(flag[q]), width
+    return nt, aa, nt_off, aa_off, nl, al, flag, tab
+
+
+def cpu_baseline_ext(nt, aa, nt_off, aa_off, nl, al, flag, opt, target_s, steps=1):
+    """The reference's ns_global_gs16b with each request's extension flag over a bounded random
+    sample, all host threads (kt_for).  Returns (nominal GCUPS, threads, kind, sample, secs, cells)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    threads = os.cpu_count() or 1
+    ref = O.ref_lib()
+    if ref is None:
+        raise RuntimeError("the extension CPU baseline needs oracle/_ref/libnsref.so (make -C oracle ref)")
+    fn = ref.ref_bench_ext
+    fn.restype = C.c_double
+    fn.argtypes = [C.c_int32, C.c_int32] + [C.c_void_p] * 11
+    n = len(nl)
+    perm = np.random.default_rng(12345).permutation(n)
+    cells = (nl.astype(np.int64) - 2) * al
+    budget = target_s * 1.0e9 * threads  # ~1 GCUPS per thread (nominal cells) for the AVX2 kernel
+    k = int(np.searchsorted(np.cumsum(cells[perm]), budget)) + 1
+    take = np.sort(perm[:min(k, n)])
+    acc = int(cells[take].sum())
+    s_nl, s_al, s_fl = nl[take].copy(), al[take].copy(), flag[take].copy()
+    s_nt_off, s_aa_off = nt_off[take].copy(), aa_off[take].copy()
+    out = [np.zeros(len(take), dtype=np.int32) for _ in range(3)]
+    secs = []
+    for _ in range(steps):
+        secs.append(fn(threads, len(take), nt.ctypes.data, s_nt_off.ctypes.data, s_nl.ctypes.data, aa.ctypes.data,
+                       s_aa_off.ctypes.data, s_al.ctypes.data, s_fl.ctypes.data, C.addressof(opt.c),
+                       out[0].ctypes.data, out[1].ctypes.data, out[2].ctypes.data))
+    sample = (f"{len(take)} of {n} extension requests (seeded random subset, {acc / 1e9:.2f} G nominal cells), "
+              f"ns_global_gs16b with NS_F_EXT_LEFT/RIGHT, {threads} threads via kt_for")
+    return acc / min(secs) / 1e9, threads, "reference", sample, secs, acc
+
+
+def run_reference_ext(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    reqs = W.ext_requests(args.requests, seed=2)
+    nt, aa, nt_off, aa_off, nl, al, flag, _ = ext_pack(reqs)
+    opt = Options()
+    per_step = args.cpu_seconds / 2
+    cpu_baseline_ext(nt, aa, nt_off, aa_off, nl, al, flag, opt, per_step, steps=max(args.warmup, 1))
+    gcups, threads, kind, sample, secs, cells = cpu_baseline_ext(nt, aa, nt_off, aa_off, nl, al, flag, opt, per_step,
+                                                                 steps=args.steps)
+    value = cells * len(secs) / sum(secs) / 1e9
+    line = {"metric": EXT_METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sum(secs) / len(secs) * 1e3, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
+            "impl": "reference", "config": {"workload": EXT_WORKLOAD, "n_requests": int(len(nl)),
+                                            "step": "bounded sample of the workload"},
+            "cpu_baseline": {"value": round(value, 3), "unit": "GCUPS", "cores": threads, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": round(value, 3), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main_ext(args):
+    import torch
+    import torch.distributed as dist
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    reqs = W.ext_requests(args.requests, seed=2 + rank)
+    nt, aa, nt_off, aa_off, nl, al, flag, tab = ext_pack(reqs)
+    n = len(reqs)
+    nominal = int(((nl.astype(np.int64) - 2) * al).sum())
+    opt = Options()
+    eng = L.Engine(local)
+    d_nt = torch.from_numpy(nt.copy()).to("cuda")
+    d_aa = torch.from_numpy(aa.copy()).to("cuda")
+    d_res = torch.zeros(n * C.sizeof(ExtResult), dtype=torch.uint8, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > L2 (126 MB): written between steps
+    stream = torch.cuda.current_stream()
+
+    def step_device():
+        if not eng.lib.pl_ext_batch_device(eng.h, opt.ptr, tab, n, d_nt.data_ptr(), d_aa.data_ptr(), None, None,
+                                           d_res.data_ptr(), stream.cuda_stream):
+            raise RuntimeError("pl_ext_batch_device: " + L.error())
+
+    for _ in range(args.warmup):
+        step_device()
+    res = (ExtResult * n).from_buffer_copy(d_res.cpu().numpy().tobytes())
+    if any(r.status != 0 for r in res):
+        raise RuntimeError("extension requests failed")
+    cells_run, _ = eng.ext_last_cells()
+    int32_peak, i16x2_peak = L.measure_int_peak(local)
+    peak = max(int32_peak, i16x2_peak)
+
+    clocks = Clocks(local)
+    eng.set_timing(True)
+    launches0 = L.load().pl_kernel_launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step_device()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t += e0.elapsed_time(e1) / 1e3
+    barrier()
+    clk = clocks.stop()
+    launches = L.load().pl_kernel_launch_count() - launches0
+    t = max_over_ranks(t)
+    value = world * nominal * args.steps / t / 1e9
+    tm = eng.times()
+    dp_s = tm["dp_ms"] / 1e3
+    achieved = tm["cells"] * EXT_OPS_PER_CELL / dp_s if dp_s > 0 else 0.0
+
+    e2e = None
+    if not args.no_e2e:
+        h_nt = torch.from_numpy(nt.copy()).pin_memory()
+        h_aa = torch.from_numpy(aa.copy()).pin_memory()
+        h_res = (ExtResult * n)()
+        est = torch.cuda.ExternalStream(eng.stream)
+
+        def step_host():
+            if not eng.lib.pl_ext_batch_host(eng.h, opt.ptr, tab, n, h_nt.data_ptr(), h_nt.numel(), h_aa.data_ptr(),
+                                             h_aa.numel(), None, 0, None, 0, h_res):
+                raise RuntimeError("pl_ext_batch_host: " + L.error())
+
+        for _ in range(max(1, args.warmup)):
+            step_host()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(est)
+        for _ in range(args.steps):
+            step_host()
+        e1.record(est)
+        torch.cuda.synchronize()
+        barrier()
+        te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+        e2e = {"value": round(world * nominal * args.steps / te / 1e9, 3), "unit": "GCUPS",
+               "h2d_bytes_per_step": int(nt.nbytes + aa.nbytes + n * C.sizeof(ExtJob)),
+               "d2h_bytes_per_step": int(n * C.sizeof(ExtResult)), "ms_per_step": round(te / args.steps * 1e3, 2),
+               "requests_per_s": round(world * n * args.steps / te, 1),
+               "api": "pl_ext_batch_host (C ABI, pinned host buffers)"}
+
+    cpu = None
+    if rank == 0:
+        gcups, threads, kind, sample, _s, _c = cpu_baseline_ext(nt, aa, nt_off, aa_off, nl, al, flag, opt,
+                                                                args.cpu_seconds)
+        cpu = {"value": round(gcups, 3), "unit": "GCUPS", "cores": threads, "kind": kind, "sample": sample}
+    if rank == 0:
+        line = {
+            "metric": EXT_METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(t / args.steps * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
+            "config": {"workload": EXT_WORKLOAD, "n_requests": n, "nominal_cells_per_step": nominal,
+                       "algorithmic_cells_per_step": int(cells_run), "seed": "2+rank",
+                       "stripe_width": "host rule (16 lanes on an AVX2 host, as the reference CPU kernel)",
+                       "l2": "a 256 MB buffer is written between timed steps", "parallelism": f"{world} independent ranks"},
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "int", "kernel": "k_ext_dp", "achieved": achieved, "peak": peak,
+                         "unit": "lane-ops/s", "frac": achieved / peak if peak else None, "traffic": None,
+                         "ops_per_cell": EXT_OPS_PER_CELL,
+                         "dp_kernel_gcups_algorithmic": round(tm["cells"] / dp_s / 1e9, 3) if dp_s > 0 else None,
+                         "peak_source": "measured live: pl_measure_int_peak (int32 %.3g, int16x2 %.3g lane-ops/s)"
+                                        % (int32_peak, i16x2_peak),
+                         "phase_ms_per_step": {"prep_ms": round(tm["prep_ms"] / args.steps, 3),
+                                               "dp_ms": round(tm["dp_ms"] / args.steps, 3)}},
             "cpu_baseline": cpu,
             "clocks": clk,
         }

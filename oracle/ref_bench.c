@@ -47,3 +47,41 @@ double ref_bench_global(int32_t n_threads, int32_t n_jobs, const char *nt, const
 	clock_gettime(CLOCK_MONOTONIC, &t1);
 	return (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
 }
+
+/* Extension DPs: the reference's ns_global_gs16b (nasw-sse.c:763-772) with each
+ * job's NS_F_EXT_LEFT / NS_F_EXT_RIGHT flag, no CIGAR, over kt_for -- the CPU
+ * path ns_ext_batch_* replaces (nasw-ext-gpu.c:118-122). */
+typedef struct {
+	const char *nt, *aa;
+	const int64_t *nt_off, *aa_off;
+	const int32_t *nl, *al, *flag;
+	const ns_opt_t *opt;
+	int32_t *score, *nt_len, *aa_len;
+} ref_bench_ext_t;
+
+static void ref_bench_ext_worker(void *data, long i, int tid)
+{
+	ref_bench_ext_t *b = (ref_bench_ext_t*)data;
+	ns_opt_t o = *b->opt;
+	ns_rst_t r;
+	(void)tid;
+	o.flag = (o.flag & ~(NS_F_CIGAR | NS_F_EXT_LEFT | NS_F_EXT_RIGHT)) | b->flag[i];
+	ns_rst_init(&r);
+	ns_global_gs16b(0, b->nt + b->nt_off[i], b->nl[i], b->aa + b->aa_off[i], b->al[i], &o, 0, &r);
+	b->score[i] = r.score, b->nt_len[i] = r.nt_len, b->aa_len[i] = r.aa_len;
+	free(r.cigar);
+}
+
+double ref_bench_ext(int32_t n_threads, int32_t n_jobs, const char *nt, const int64_t *nt_off, const int32_t *nl,
+		const char *aa, const int64_t *aa_off, const int32_t *al, const int32_t *flag, const ns_opt_t *opt,
+		int32_t *score, int32_t *nt_len, int32_t *aa_len)
+{
+	ref_bench_ext_t b;
+	struct timespec t0, t1;
+	b.nt = nt, b.aa = aa, b.nt_off = nt_off, b.aa_off = aa_off, b.nl = nl, b.al = al, b.flag = flag, b.opt = opt;
+	b.score = score, b.nt_len = nt_len, b.aa_len = aa_len;
+	clock_gettime(CLOCK_MONOTONIC, &t0);
+	kt_for(n_threads, ref_bench_ext_worker, &b, n_jobs);
+	clock_gettime(CLOCK_MONOTONIC, &t1);
+	return (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
+}

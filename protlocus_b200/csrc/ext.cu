@@ -213,6 +213,7 @@ __device__ __forceinline__ void ext_job(plk_ext_job_t *__restrict__ J, const uin
 
 	/* row-scan state (warp-uniform) */
 	int best_sc = NEG, best_row = -1, best_col = 0, M = INT_MIN, ks = 0, next_scan = glob ? INT_MAX : 31 + ncol - 1;
+	int last_row = nl - 1;  /* last row the reference processes: the x-drop row, else nl-1 */
 
 	for (int s = 0; s < total; ++s) {
 		int in[9];
@@ -356,6 +357,7 @@ __device__ __forceinline__ void ext_job(plk_ext_job_t *__restrict__ J, const uin
 				best_col = K::col((KeyT)fk);
 				M = mx;
 			}
+			if (bm != 0) last_row = 2 + ks * EXT_STRIP + brk_lane * R + brk_r;
 			const bool done = bm != 0 || ks == nstrip - 1;
 			++ks, next_scan += Pc;
 			__syncwarp();
@@ -375,8 +377,8 @@ __device__ __forceinline__ void ext_job(plk_ext_job_t *__restrict__ J, const uin
 	if (lane == 0) {
 		if (glob) J->nt_len = nl, J->aa_len = al, J->status = 0;
 		else J->nt_len = best_row + 1, J->aa_len = best_col + 1, J->score = best_sc, J->status = best_row >= 2 ? 0 : -1;
-		const int64_t rows = glob ? nr : min((int64_t)nr, (int64_t)ks * EXT_STRIP); /* rows the DP ran */
-		atomicAdd(cells_acc, (unsigned long long)(rows * al));
+		/* algorithmic cells: rows 2..last_row (the rows the reference's loop visits) x al */
+		atomicAdd(cells_acc, (unsigned long long)((int64_t)(last_row - 1) * al));
 	}
 	__syncwarp();
 }

@@ -35,12 +35,20 @@ static int pl_host_avx2(void)
 #endif
 }
 
+static pthread_once_t pl_lanes_once = PTHREAD_ONCE_INIT;
+static int pl_wide_lanes;  /* 1: the CPU kernel this library matches dispatches ext DPs to AVX2 */
+
+static void pl_lanes_init(void)
+{
+	const char *env = getenv("PLGPU_EXT_STRIPE");
+	pl_wide_lanes = pl_host_avx2();
+	if (env && (atoi(env) == 8 || atoi(env) == 16)) pl_wide_lanes = atoi(env) == 16;
+}
+
 PL_EXPORT int32_t pl_ext_stripe_width(const ns_opt_t *opt, int32_t al)
 { /* nasw-sse.c:744-750 */
-	const char *env = getenv("PLGPU_EXT_STRIPE");
-	int avx2 = pl_host_avx2();
-	if (env && (atoi(env) == 8 || atoi(env) == 16)) avx2 = atoi(env) == 16;
-	return (opt->flag & (NS_F_EXT_LEFT | NS_F_EXT_RIGHT)) && al >= 16 && avx2 ? 16 : 8;
+	pthread_once(&pl_lanes_once, pl_lanes_init);
+	return (opt->flag & (NS_F_EXT_LEFT | NS_F_EXT_RIGHT)) && al >= 16 && pl_wide_lanes ? 16 : 8;
 }
 
 /* ------------------------------------------------------------------ bulk engine */
@@ -54,12 +62,17 @@ void pl_ext_engine_free(pl_engine_t *e)
 	e->x_hj = 0, e->x_horder = 0, e->x_m = 0;
 }
 
-typedef struct { int64_t key; int32_t idx; } pl_xkey_t;
-static int pl_xkey_cmp(const void *a, const void *b)
-{ /* group (mode, variant) ascending, then cells descending */
-	const pl_xkey_t *x = (const pl_xkey_t*)a, *y = (const pl_xkey_t*)b;
-	if (x->key != y->key) return x->key < y->key ? -1 : 1;
-	return x->idx - y->idx;
+/* Queue order: by (mode, variant) group, and inside a group by decreasing DP size
+ * (longest first for load balance).  Sizes are bucketed on a quarter-octave log
+ * scale, which is all the balancing needs, so one counting sort does it. */
+#define PL_XBUCKETS (8 * 4 * 64)
+static int pl_xbucket(const plk_ext_job_t *J)
+{
+	const int64_t cells = (int64_t)(J->nl - 2) * J->ncol;
+	int lg = 0, frac;
+	while (lg < 62 && (cells >> (lg + 1)) > 0) ++lg;
+	frac = lg >= 2 ? (int)((cells >> (lg - 2)) & 3) : 0;
+	return (J->mode / 2 * 4 + J->variant) * 256 + (255 - (lg * 4 + frac > 255 ? 255 : lg * 4 + frac));
 }
 
 /* the reference's answer when the DP has no row (nl < 3): the row loop of
@@ -78,7 +91,7 @@ static int pl_ext_run(pl_engine_t *e, const ns_opt_t *opt, const pl_ext_job_t *j
 		cudaStream_t st)
 {
 	plk_params_t P;
-	pl_xkey_t *key = 0;
+	int32_t *key = 0;   /* bucket counts, then bucket starts */
 	int32_t q, n_dp = 0, max_sub;
 	int64_t prep_total = 0, cells_nominal = 0;
 	unsigned long long cells_run = 0;
@@ -95,7 +108,7 @@ static int pl_ext_run(pl_engine_t *e, const ns_opt_t *opt, const pl_ext_job_t *j
 		e->x_m = e->x_hj && e->x_horder ? n : 0;
 		if (!e->x_m) { pl_set_error("out of host memory"); return 0; }
 	}
-	key = (pl_xkey_t*)malloc(sizeof(pl_xkey_t) * (size_t)n);
+	key = (int32_t*)calloc(PL_XBUCKETS + 1, sizeof(int32_t));
 	if (!key) { pl_set_error("out of host memory"); return 0; }
 	max_sub = pl_max_sub(opt);
 	for (q = 0; q < n; ++q) {
@@ -130,12 +143,12 @@ static int pl_ext_run(pl_engine_t *e, const ns_opt_t *opt, const pl_ext_job_t *j
 		}
 		J->prep_off = prep_total, prep_total += plk_prep_bytes(x->nl, x->al);
 		cells_nominal += (int64_t)(x->nl - 2) * x->al;
-		key[n_dp].key = ((int64_t)(J->mode * 4 + J->variant) << 56) | ((1ll << 56) - 1 - (int64_t)(x->nl - 2) * J->ncol);
-		key[n_dp].idx = q;
+		++key[pl_xbucket(J) + 1];
 		++n_dp;
 	}
-	qsort(key, (size_t)n_dp, sizeof(pl_xkey_t), pl_xkey_cmp);
-	for (q = 0; q < n_dp; ++q) e->x_horder[q] = key[q].idx;
+	for (q = 0; q < PL_XBUCKETS; ++q) key[q + 1] += key[q];
+	for (q = 0; q < n; ++q)
+		if (jobs[q].nl >= 3) e->x_horder[key[pl_xbucket(&e->x_hj[q])]++] = q;
 	if (!dbuf_ensure(&e->x_jobs, sizeof(plk_ext_job_t) * (size_t)n) ||
 			!dbuf_ensure(&e->x_order, sizeof(int32_t) * (size_t)(n_dp > 0 ? n_dp : 1)) ||
 			!dbuf_ensure(&e->x_counter, 64) || !dbuf_ensure(&e->x_prep, (size_t)(prep_total > 0 ? prep_total : 16)))
@@ -145,7 +158,10 @@ static int pl_ext_run(pl_engine_t *e, const ns_opt_t *opt, const pl_ext_job_t *j
 	if (n_dp > 0) {
 		int32_t g0 = 0;
 		CK(cudaMemcpyAsync(e->x_order.p, e->x_horder, sizeof(int32_t) * (size_t)n_dp, cudaMemcpyHostToDevice, st));
+		e->n_ev = 0;
+		PL_TIME(e, st, 0);
 		CKK(plk_ext_prep((const plk_ext_job_t*)e->x_jobs.p, n, nt, aa, ss, (uint8_t*)e->x_prep.p, &P, st));
+		PL_TIME(e, st, 0);
 		++e->x_last_launches;
 		while (g0 < n_dp) { /* one launch per (mode, variant) group */
 			const plk_ext_job_t *J0 = &e->x_hj[e->x_horder[g0]];
@@ -163,9 +179,11 @@ static int pl_ext_run(pl_engine_t *e, const ns_opt_t *opt, const pl_ext_job_t *j
 				ctas = (g1 - g0 + plk_ext_warps_per_cta() - 1) / plk_ext_warps_per_cta();
 			stride = ((int64_t)max_ncol + 1) * PLK_RING_INTS;
 			if (!dbuf_ensure(&e->x_ring, sizeof(int32_t) * (size_t)(stride * ctas * plk_ext_warps_per_cta()))) goto fail;
+			PL_TIME(e, st, 1);
 			CKK(plk_ext_dp((plk_ext_job_t*)e->x_jobs.p, (const int32_t*)e->x_order.p + g0, g1 - g0,
 					(int32_t*)e->x_counter.p, (const uint8_t*)e->x_prep.p, pssm, (int32_t*)e->x_ring.p, stride,
 					ctas, mode, variant, &P, st));
+			PL_TIME(e, st, 1);
 			++e->x_last_launches;
 			g0 = g1;
 		}
@@ -175,6 +193,16 @@ static int pl_ext_run(pl_engine_t *e, const ns_opt_t *opt, const pl_ext_job_t *j
 	CK(cudaMemcpyAsync(&cells_run, (char*)e->x_counter.p + 8, sizeof(cells_run), cudaMemcpyDeviceToHost, st));
 	CK(cudaStreamSynchronize(st));
 	e->x_cells_run = (int64_t)cells_run, e->x_cells_nominal = cells_nominal;
+	if (e->timing && n_dp > 0) { /* event pairs: prep, then one per DP launch */
+		int k;
+		float ms;
+		for (k = 0; k + 1 < e->n_ev; k += 2) {
+			cudaEventElapsedTime(&ms, e->ev[k], e->ev[k + 1]);
+			e->acc_ms[e->ev_kind[k]] += ms;
+		}
+		e->acc_dp_launches += e->x_last_launches - 2;
+		e->acc_cells += (int64_t)cells_run;
+	}
 	ok = 1;
 fail:
 	free(key);

@@ -88,9 +88,6 @@ int dbuf_ensure(dbuf_t *b, size_t need)
 
 void dbuf_free(dbuf_t *b) { if (b->p) cudaFree(b->p); b->p = 0, b->cap = 0; }
 
-#define PL_TIME(e, st, k) do { if ((e)->timing && (e)->n_ev < (int)(sizeof((e)->ev) / sizeof((e)->ev[0]))) { \
-	(e)->ev_kind[(e)->n_ev] = (k); cudaEventRecord((e)->ev[(e)->n_ev++], (st)); } } while (0)
-
 PL_EXPORT uint64_t pl_kernel_launch_count(void) { return plk_launches(); }
 
 PL_EXPORT pl_engine_t *pl_engine_create(int32_t device, int64_t trace_budget_bytes)

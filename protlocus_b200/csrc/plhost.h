@@ -44,6 +44,10 @@ struct pl_engine_s {
 	int64_t acc_dp_launches, acc_cells;
 };
 
+/* records a timing event of phase k (0 prep, 1 DP, 2 traceback, 3 compaction) when timing is on */
+#define PL_TIME(e, st, k) do { if ((e)->timing && (e)->n_ev < (int)(sizeof((e)->ev) / sizeof((e)->ev[0]))) { \
+	(e)->ev_kind[(e)->n_ev] = (k); cudaEventRecord((e)->ev[(e)->n_ev++], (st)); } } while (0)
+
 void pl_set_error(const char *fmt, ...);
 int pl_params(const ns_opt_t *opt, plk_params_t *p, int for_ext);
 int pl_max_sub(const ns_opt_t *opt);

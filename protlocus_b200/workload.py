@@ -176,3 +176,31 @@ def random_ss(rng: np.random.Generator, nl: int, rate: float = 0.2) -> bytes:
     """Splice-score track like the reference's tests: mostly unset (0xff), some donor/acceptor scores."""
     val = ((rng.integers(0, 128, size=nl) << 1) | rng.integers(0, 2, size=nl)) & 0xff
     return np.where(rng.random(nl) < rate, val, 0xff).astype(np.uint8).tobytes()
+
+
+def ext_requests(n: int, seed: int = 2, *, win_min: int = 64, win_max: int = 256, divergence: float = 0.25,
+                 intron_lambda: float = 0.5, intron_median: float = 150.0, intron_sigma: float = 0.8,
+                 slack_min: int = 60, slack_max: int = 600):
+    """Extension requests shaped like the seed-extension configuration: protein windows of
+    64-256 aa (the request window the reference extends over), nucleotide windows of
+    3x the protein window plus slack.  A mutated, possibly spliced and frameshifted copy
+    of the protein's anchored part (30-100 % of the window, from the anchor outwards)
+    starts at the anchor end of the window; random sequence follows, where the x-drop
+    ends the DP.  Alternate requests extend right (anchor at the start) and left (anchor
+    at the end).  Returns a list of (nt, protein, flag)."""
+    from .abi import NS_F_EXT_LEFT, NS_F_EXT_RIGHT
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n):
+        L = int(rng.integers(win_min, win_max + 1))
+        prot = random_protein(rng, L)
+        m = int(rng.integers(max(8, int(0.3 * L)), L + 1))
+        k = int(rng.poisson(intron_lambda))
+        introns = [int(max(20, round(math.exp(rng.normal(math.log(intron_median), intron_sigma))))) for _ in range(k)]
+        left = bool(q & 1)
+        part = prot[L - m:] if left else prot[:m]
+        gene = build_gene(rng, part, divergence=divergence, n_frameshift=int(rng.integers(0, 2)), intron_lengths=introns)
+        tail = random_dna(rng, max(0, 3 * L + int(rng.integers(slack_min, slack_max + 1)) + sum(introns) - len(gene)))
+        nt = tail + gene if left else gene + tail
+        out.append((nt.encode(), prot.encode(), NS_F_EXT_LEFT if left else NS_F_EXT_RIGHT))
+    return out
