@@ -86,6 +86,10 @@ typedef struct {
 typedef struct ns_ext_batch_s ns_ext_batch_t;
 #endif /* NASW_H */
 
+#ifndef PROTLOCUS_H
+typedef struct mp_hmm_s mp_hmm_t;  /* protlocus.h:67, opaque (hmm.c:14-22) */
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -281,8 +285,47 @@ int pl_ext_batch_host(pl_engine_t *e, const ns_opt_t *opt, const pl_ext_job_t *j
 int pl_ext_batch_device(pl_engine_t *e, const ns_opt_t *opt, const pl_ext_job_t *jobs, int32_t n_jobs,
 		const uint8_t *nt, const uint8_t *aa, const uint8_t *ss, const int8_t *pssm,
 		pl_ext_result_t *results_dev, void *stream);
-/* DP cells of the last extension batch: rows the DP actually ran (the x-drop
- * stops a request early) times padded columns, and the nominal (nl-2)*al. */
+/* ---------------------------------------------------------------------------
+ * Integer profile-HMM DP (replaces hmm-gpu.c; semantics of mp_hmm_dp_score,
+ * hmm.c:252-291): one profile, many regions of nt4 codes, one frame-0 codon
+ * per DP row, score = the maximum M or I value (int32, exact).
+ * ------------------------------------------------------------------------- */
+/* mppriv.h:132 -- score n regions (nt + off[k], len[k] nucleotides) against h;
+ * 1 = every score[k] filled with exactly mp_hmm_dp_score(h, nt + off[k],
+ * len[k]), 0 = not taken (no device, or the host program lacks hmm.c's
+ * accessors).  h's device tables are built on first use and cached in its GPU
+ * slot (mp_hmm_gpu_slot(h, 0), hmm.c:215) until mp_hmm_gpu_release().
+ * Thread-safe (calls are serialised on one device queue). */
+int mp_hmm_dp_score_gpu_batch(const mp_hmm_t *h, int32_t n, const uint8_t *nt, int64_t l_nt,
+		const int32_t *off, const int32_t *len, int32_t *score);
+/* mppriv.h:129 -- one region; INT32_MIN when not taken or nlen < 3. */
+int32_t mp_hmm_dp_score_gpu(const mp_hmm_t *h, const uint8_t *nt, int32_t nlen);
+/* mppriv.h:134 -- free h's cached device tables (mp_hmm_destroy calls it, hmm.c:207-212). */
+void mp_hmm_gpu_release(mp_hmm_t *h);
+
+/* Bulk profile-HMM entry points (no counterpart in the reference).  A profile
+ * is given as the reference parser's tables (hmm.c:112-195): emit m x 20 int16
+ * in HMMER column order ACDEFGHIKLMNPQRSTVWY, trans m x 7 int16 (m->m, m->i,
+ * m->d, i->m, i->i, d->m, d->d), and codon_alpha[64]: for codon b0<<4|b1<<2|b2
+ * the HMMER column of its amino acid, 20 for a stop codon (ns_tab_codon through
+ * mp_hmm_aa20_to_alpha, hmm.c:229-250). */
+typedef struct pl_hmm_profile_s pl_hmm_profile_t;
+pl_hmm_profile_t *pl_hmm_profile_create(int32_t device, int32_t m, const int16_t *emit, const int16_t *trans,
+		const uint8_t *codon_alpha);
+void pl_hmm_profile_destroy(pl_hmm_profile_t *p);
+/* Host buffers: nt (l_nt nucleotide codes 0-4), off/len/score arrays of n regions.  Returns 1 on success. */
+int pl_hmm_score_host(pl_engine_t *e, const pl_hmm_profile_t *p, int32_t n, const uint8_t *nt, int64_t l_nt,
+		const int32_t *off, const int32_t *len, int32_t *score);
+/* Device nt and scores; off/len on the host (they drive the planning).  Work on
+ * `stream` (NULL = the engine's); returns when done.  Returns 1 on success. */
+int pl_hmm_score_device(pl_engine_t *e, const pl_hmm_profile_t *p, int32_t n, const uint8_t *nt,
+		const int32_t *off, const int32_t *len, int32_t *score_dev, void *stream);
+/* DP cells (codon rows x m) of the last HMM batch of this engine. */
+int64_t pl_hmm_last_cells(const pl_engine_t *e);
+
+/* DP cells of the last extension batch: the rows the reference's row loop
+ * visits (up to the x-drop row, nasw-sse.c:361-447) times al, and the nominal
+ * (nl-2)*al. */
 void pl_ext_last_cells(const pl_engine_t *e, int64_t *cells_run, int64_t *cells_nominal);
 
 #ifdef __cplusplus

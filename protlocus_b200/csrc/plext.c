@@ -415,6 +415,11 @@ PL_EXPORT int32_t ns_ext_batch_flush(ns_ext_batch_t *b)
 	}
 	b->n = b->m = 0;
 	free(b->opts), b->opts = 0;
+	{ /* counted when handed to the device, as nasw-ext-gpu.c:994 does; nl < 3 has no DP row */
+		uint64_t nd = 0;
+		for (k = 0; k < n; ++k) nd += g->req[k].nl >= 3;
+		__sync_fetch_and_add(&xr_requests, nd);
+	}
 	if (b->gens) { xr_gen_t *t = b->gens; while (t->gnext) t = t->gnext; t->gnext = g; }
 	else b->gens = g;
 	pthread_mutex_lock(&xr_mu);
@@ -525,7 +530,6 @@ static int xr_run(const ns_opt_t *o, const xr_ref_t *refs, int32_t n)
 			r->rst.n_cigar = 0, r->rst.nt_len = res[q].nt_len, r->rst.aa_len = res[q].aa_len, r->rst.score = res[q].score;
 		}
 		__sync_fetch_and_add(&xr_launches, (uint64_t)xr_engine->x_last_launches);
-		__sync_fetch_and_add(&xr_requests, (uint64_t)n);
 	}
 out:
 	if (!ok) { /* no CPU path to fall back on: fail loudly */

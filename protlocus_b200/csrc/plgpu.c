@@ -38,18 +38,17 @@
 
 /* ------------------------------------------------------------------ km allocator hooks
  * The CIGAR of a request is appended into the caller's kalloc arena, as
- * nasw.h:219-229 does.  kalloc itself belongs to the host program (kalloc.c of
- * the reference); these weak definitions only serve callers that link no
- * kalloc (Python, tests) and always pass km == NULL. */
-__attribute__((weak)) void *krealloc(void *km, void *ptr, size_t size)
+ * nasw.h:219-229 does.  kalloc belongs to the host program (kalloc.c of the
+ * reference); the library only holds a weak reference to krealloc, so the
+ * linker exports the program's definition to it.  Callers that link no kalloc
+ * (Python, tests) must pass km == NULL and get plain realloc. */
+extern void *krealloc(void *km, void *ptr, size_t size) __attribute__((weak));
+
+static void *pl_krealloc(void *km, void *ptr, size_t size)
 {
-	if (km) { fprintf(stderr, "[plgpu] krealloc with a km arena but no kalloc linked\n"); abort(); }
+	if (krealloc) return krealloc(km, ptr, size);
+	if (km) { fprintf(stderr, "[plgpu] a km arena was passed but the program links no kalloc\n"); abort(); }
 	return realloc(ptr, size);
-}
-__attribute__((weak)) void kfree(void *km, void *ptr)
-{
-	if (km) { fprintf(stderr, "[plgpu] kfree with a km arena but no kalloc linked\n"); abort(); }
-	free(ptr);
 }
 
 /* ------------------------------------------------------------------ errors */
@@ -124,6 +123,7 @@ PL_EXPORT void pl_engine_destroy(pl_engine_t *e)
 	dbuf_free(&e->trace), dbuf_free(&e->ring), dbuf_free(&e->tmp), dbuf_free(&e->total);
 	dbuf_free(&e->nt), dbuf_free(&e->aa), dbuf_free(&e->ss), dbuf_free(&e->res), dbuf_free(&e->cig);
 	pl_ext_engine_free(e);
+	pl_hmm_engine_free(e);
 	if (e->stream) cudaStreamDestroy(e->stream);
 	free(e->hj), free(e->horder), free(e->hwave);
 	free(e);
@@ -647,7 +647,7 @@ PL_EXPORT int ns_gpu_wait(ns_gpu_request_t *r, ns_rst_t *rst)
 			if (rst->n_cigar == 0 || op != (rst->cigar[rst->n_cigar - 1] & 0xf) || op == NS_CIGAR_F || op == NS_CIGAR_G) {
 				if (rst->n_cigar == rst->m_cigar) {
 					rst->m_cigar += (rst->m_cigar >> 1) + 8;
-					rst->cigar = (uint32_t*)krealloc(r->km, rst->cigar, sizeof(uint32_t) * (size_t)rst->m_cigar);
+					rst->cigar = (uint32_t*)pl_krealloc(r->km, rst->cigar, sizeof(uint32_t) * (size_t)rst->m_cigar);
 				}
 				rst->cigar[rst->n_cigar++] = len << 4 | op;
 			} else rst->cigar[rst->n_cigar - 1] += len << 4;

@@ -31,6 +31,11 @@ struct pl_engine_s {
 	int32_t *x_horder, x_m;
 	int32_t x_last_launches;
 	int64_t x_cells_run, x_cells_nominal;
+	/* integer HMM DP */
+	dbuf_t h_off, h_len, h_rowoff, h_rows, h_order, h_counter, h_edge, h_nt, h_score;
+	void *h_hbuf;
+	size_t h_hcap;
+	int64_t h_last_cells;
 	/* host planning scratch */
 	plk_job_t *hj;
 	int32_t *horder, *hwave, m_jobs;
@@ -52,5 +57,6 @@ void pl_set_error(const char *fmt, ...);
 int pl_params(const ns_opt_t *opt, plk_params_t *p, int for_ext);
 int pl_max_sub(const ns_opt_t *opt);
 void pl_ext_engine_free(pl_engine_t *e);
+void pl_hmm_engine_free(pl_engine_t *e);
 
 #endif

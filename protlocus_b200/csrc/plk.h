@@ -59,6 +59,15 @@ typedef struct {
 	int32_t pad;
 } plk_ext_job_t;
 
+/* a profile of the integer HMM DP on the device (hmm.c:14-22 tables, re-laid out) */
+typedef struct {
+	const int16_t *emit_t;   /* [21][mpad]: emissions by HMMER column (row 20: zeros, no emission), column j-1 */
+	const int32_t *trans_t;  /* [7][mpad]: m->m, m->i, m->d, i->m, i->i, d->m, d->d of column j-1; -2^28 beyond m */
+	int32_t m, mpad;         /* profile length, padded to the 256-column tile */
+} plk_hmm_prof_t;
+#define PLK_HMM_TILE 256
+#define PLK_HMM_SMEM_MAX (96 * 1024)  /* emissions staged in shared memory up to mpad = 2048 */
+
 /* bytes of preparation scratch for a job (8-aligned) */
 static inline int64_t plk_prep_bytes(int32_t nl, int32_t al)
 {
@@ -100,6 +109,15 @@ int plk_ext_warps_per_cta(void);
 /* results[q] (pl_ext_result_t) from the job table */
 int plk_ext_results(const plk_ext_job_t *jobs, int32_t n_jobs, void *results, void *stream);
 void plk_add_launches(uint64_t n);
+/* integer HMM DP: codon rows of every region, then one warp per region (order) */
+int plk_hmm_codons(const uint8_t *nt, const int32_t *off, const int32_t *len, const int64_t *row_off, int32_t n,
+		const uint8_t *codon_alpha, uint8_t *rows, void *stream);
+int plk_hmm_dp(const plk_hmm_prof_t *p, const uint8_t *rows, const int64_t *row_off, const int32_t *len,
+		const int32_t *order, int32_t n, int32_t *counter, void *edge, int64_t edge_stride_rows, int32_t n_ctas,
+		int32_t *score, void *stream);
+int plk_hmm_ctas_per_sm(int32_t mpad);
+int plk_hmm_warps_per_cta(void);
+int plk_hmm_smem_bytes(int32_t mpad);
 /* CTAs of the DP kernel that fit on one SM at once (occupancy) */
 int plk_dp_ctas_per_sm(int32_t mode);
 uint64_t plk_launches(void);

@@ -91,6 +91,19 @@ def load() -> C.CDLL:
     lib.ns_ext_batch_destroy.argtypes = [C.c_void_p]
     for fn in ("ns_ext_gpu_launch_count", "ns_ext_gpu_request_count"):
         getattr(lib, fn).restype = C.c_uint64
+    lib.pl_hmm_profile_create.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.pl_hmm_profile_create.restype = C.c_void_p
+    lib.pl_hmm_profile_destroy.argtypes = [C.c_void_p]
+    lib.pl_hmm_score_host.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
+                                      C.c_void_p, C.c_void_p]
+    lib.pl_hmm_score_host.restype = C.c_int
+    lib.pl_hmm_score_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p]
+    lib.pl_hmm_score_device.restype = C.c_int
+    lib.pl_hmm_last_cells.argtypes = [C.c_void_p]
+    lib.pl_hmm_last_cells.restype = C.c_int64
+    lib.mp_hmm_dp_score_gpu.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
+    lib.mp_hmm_dp_score_gpu.restype = C.c_int32
     _lib = lib
     return lib
 
@@ -239,6 +252,47 @@ class Engine:
         a, b = C.c_int64(), C.c_int64()
         self.lib.pl_ext_last_cells(self.h, C.byref(a), C.byref(b))
         return a.value, b.value
+
+
+    def hmm_score(self, profile: "HmmProfile", regions):
+        """Integer profile DP of each region (nt4 code arrays) against one profile: list of int scores."""
+        n = len(regions)
+        lens = np.array([len(r) for r in regions], dtype=np.int32)
+        offs = np.zeros(n, dtype=np.int32)
+        if n > 1:
+            offs[1:] = np.cumsum(lens[:-1])
+        nt = np.concatenate([np.asarray(r, dtype=np.uint8) for r in regions]) if n else np.zeros(0, np.uint8)
+        nt = np.ascontiguousarray(nt if nt.size else np.zeros(1, np.uint8))
+        score = np.zeros(max(n, 1), dtype=np.int32)
+        if not self.lib.pl_hmm_score_host(self.h, profile.h, n, nt.ctypes.data, int(lens.sum()), offs.ctypes.data,
+                                          lens.ctypes.data, score.ctypes.data):
+            raise RuntimeError("pl_hmm_score_host failed: " + error())
+        return score[:n].tolist()
+
+
+class HmmProfile:
+    """A pl_hmm_profile_t: the reference parser's tables (emit m x 20, trans m x 7, HMMER order) on a device."""
+
+    def __init__(self, emit, trans, codon_alpha, device: int = 0):
+        self.lib = load()
+        e = np.ascontiguousarray(emit, dtype=np.int16).reshape(-1, 20)
+        t = np.ascontiguousarray(trans, dtype=np.int16).reshape(-1, 7)
+        c = np.ascontiguousarray(codon_alpha, dtype=np.uint8)
+        self.m = e.shape[0]
+        self.h = self.lib.pl_hmm_profile_create(device, self.m, e.ctypes.data, t.ctypes.data, c.ctypes.data)
+        if not self.h:
+            raise RuntimeError("pl_hmm_profile_create failed: " + error())
+
+    def close(self):
+        if self.h:
+            self.lib.pl_hmm_profile_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def ext_stripe_width(opt, al: int) -> int:

@@ -33,3 +33,10 @@ def ext_golden():
     import json
     with open(os.path.join(HERE, "golden", "ext_golden.json")) as f:
         return json.load(f)
+
+
+@pytest.fixture(scope="session")
+def hmm_golden():
+    import json
+    with open(os.path.join(HERE, "golden", "hmm_golden.json")) as f:
+        return json.load(f)

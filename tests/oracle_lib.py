@@ -167,3 +167,17 @@ def make_ext_options(spec: dict) -> Options:
         rng = np.random.default_rng(spec["pssm_seed"])
         o = o.with_pssm(rng.integers(-6, 10, size=(spec["al"], 22)).astype(np.int8))
     return o
+
+
+def port_hmm(m: int, emit, trans, codon_alpha, nt) -> int:
+    """The restatement of mp_hmm_dp_score (oracle/hmm_port.c) on one region of nt4 codes."""
+    import numpy as np
+    lib = port_lib()
+    lib.port_hmm_dp_score.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
+    lib.port_hmm_dp_score.restype = C.c_int32
+    e = np.ascontiguousarray(emit, dtype=np.int16)
+    t = np.ascontiguousarray(trans, dtype=np.int16)
+    c = np.ascontiguousarray(codon_alpha, dtype=np.uint8)
+    b = np.ascontiguousarray(nt, dtype=np.uint8)
+    return int(lib.port_hmm_dp_score(m, e.ctypes.data, t.ctypes.data, c.ctypes.data,
+                                     b.ctypes.data if b.size else None, b.size))

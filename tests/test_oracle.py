@@ -48,6 +48,32 @@ def test_port_matches_ext_golden(oracle, ext_golden):
         assert got[:3] == (c["score"], c["nt_len"], c["aa_len"]), c
 
 
+def test_port_matches_hmm_golden(oracle, hmm_golden):
+    """The restatement of mp_hmm_dp_score reproduces every reference score of the HMM fixture."""
+    import numpy as np
+    from protlocus_b200 import hmm as H
+    ca = H.codon_alpha()
+    for p in hmm_golden["profiles"]:
+        for r, s in zip(p["regions"], p["scores"]):
+            nt = np.frombuffer(bytes.fromhex(r), dtype=np.uint8)
+            assert oracle.port_hmm(p["m"], p["emit"], p["trans"], ca, nt) == s
+
+
+def test_hmm_parser_matches_reference_tables(hmm_golden):
+    """parse_hmmer3 gives the reference parser's int16 tables for the fixture's synthetic profiles."""
+    import numpy as np
+    from protlocus_b200 import hmm as H
+    g = hmm_golden["synthetic"]
+    texts, _ = H.synthetic_profiles(g["n"], seed=g["seed"], m_min=g["m_min"], m_max=g["m_max"])
+    mine = H.parse_hmmer3("".join(texts))
+    ref = [p for p in hmm_golden["profiles"] if p["source"].startswith("synthetic")]
+    assert len(mine) == len(ref)
+    for a, b in zip(mine, ref):
+        assert a["m"] == b["m"]
+        assert (a["emit"].reshape(-1) == np.array(b["emit"], dtype=np.int16)).all()
+        assert (a["trans"].reshape(-1) == np.array(b["trans"], dtype=np.int16)).all()
+
+
 def test_dp32_known_answers(oracle):
     """test/test_dp32.c assertions, on the restatement."""
     opt = Options.nasw_defaults(flag=NS_F_CIGAR, go=3, ge=1, io=100, fs=100, sp_model=0)
