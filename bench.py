@@ -61,8 +61,11 @@ def parse():
     ap.add_argument("--pairs", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="global", choices=["global", "ext"],
-                    help="global: the batched global spliced DP (headline); ext: the batched extension DP")
+    ap.add_argument("--workload", default="global", choices=["global", "ext", "hmm"],
+                    help="global: the batched global spliced DP (headline); ext: the batched extension DP; "
+                         "hmm: the integer profile-HMM DP")
+    ap.add_argument("--profiles", type=int, default=16, help="profiles per step (--workload hmm)")
+    ap.add_argument("--regions", type=int, default=4096, help="regions per profile (--workload hmm)")
     ap.add_argument("--requests", type=int, default=65536, help="extension requests per step (--workload ext)")
     ap.add_argument("--uniform", default=None, metavar="N:NL:AL",
                     help="profiling case instead of the batched workload: N planted loci of window NL and protein AL")
@@ -203,6 +206,8 @@ def main():
     args = parse()
     if args.workload == "ext":
         return run_reference_ext(args) if args.impl == "reference" else main_ext(args)
+    if args.workload == "hmm":
+        return run_reference_hmm(args) if args.impl == "reference" else main_hmm(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -554,6 +559,223 @@ def main_ext(args):
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+# ---------------------------------------------------------------------------- profile-HMM DP
+
+HMM_METRIC = "profile-HMM DP GCUPS (exact int32, cells = frame-0 codon rows x profile length) at 1 B200"
+HMM_OPS_PER_CELL = 17  # int32 ops per cell of mp_hmm_dp_score's inner loop (hmm.c:274-285)
+
+
+def hmm_workload(args, seed):
+    from protlocus_b200 import hmm as H
+    texts, probs = H.synthetic_profiles(args.profiles, seed=seed, m_min=50, m_max=800)
+    profs = H.parse_hmmer3("".join(texts))
+    rng = np.random.default_rng(seed + 1000)
+    batches = []
+    for pr, p in zip(profs, probs):
+        regs = H.regions(rng, p, args.regions, 300, 3000)
+        lens = np.array([len(r) for r in regs], dtype=np.int32)
+        offs = np.zeros(len(regs), dtype=np.int32)
+        offs[1:] = np.cumsum(lens[:-1])
+        batches.append((np.concatenate(regs), offs, lens))
+    desc = (f"profile-HMM DP: {args.profiles} synthetic Plan7 profiles (m uniform 50-800, Dirichlet-perturbed "
+            f"background, M->M ~0.95, HMMER3 text through the parser), {args.regions} regions each of 300-3000 nt "
+            "(45% GC, half with a planted profile-sampled domain), one batch per profile")
+    return texts, profs, batches, desc
+
+
+def cpu_baseline_hmm(texts, batches, target_s):
+    """The reference's mp_hmm_dp_score (its own parser's tables) over kt_for on a bounded sample of regions."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    ref = O.ref_lib()
+    if ref is None:
+        raise RuntimeError("the HMM CPU baseline needs oracle/_ref/libnsref.so (make -C oracle ref)")
+    ref.mp_hmm_open.restype, ref.mp_hmm_open.argtypes = C.c_void_p, [C.c_char_p]
+    ref.mp_hmm_read1.restype, ref.mp_hmm_read1.argtypes = C.c_void_p, [C.c_void_p]
+    ref.mp_hmm_length.argtypes = [C.c_void_p]
+    ref.mp_hmm_close.argtypes = [C.c_void_p]
+    ref.mp_hmm_destroy.argtypes = [C.c_void_p]
+    ref.ref_bench_hmm.restype = C.c_double
+    ref.ref_bench_hmm.argtypes = [C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    threads = os.cpu_count() or 1
+    with tempfile.NamedTemporaryFile("w", suffix=".hmm", delete=False) as f:
+        f.write("".join(texts))
+        path = f.name
+    fh = ref.mp_hmm_open(path.encode())
+    hs = [ref.mp_hmm_read1(fh) for _ in texts]
+    budget = target_s * 0.8e9 * threads / len(texts)  # ~0.8 GCUPS per thread, spread over the profiles
+    cells = secs = 0.0
+    n_reg = 0
+    for h, (nt, offs, lens) in zip(hs, batches):
+        m = ref.mp_hmm_length(h)
+        k = int(np.searchsorted(np.cumsum((lens // 3).astype(np.int64) * m), budget)) + 1
+        k = min(k, len(lens))
+        score = np.zeros(k, dtype=np.int32)
+        secs += ref.ref_bench_hmm(threads, h, k, nt.ctypes.data, offs.ctypes.data, lens.ctypes.data, score.ctypes.data)
+        cells += float((lens[:k] // 3).astype(np.int64).sum() * m)
+        n_reg += k
+    for h in hs:
+        ref.mp_hmm_destroy(h)
+    ref.mp_hmm_close(fh)
+    os.unlink(path)
+    sample = (f"{n_reg} regions over {len(texts)} profiles ({cells / 1e9:.2f} G cells), mp_hmm_dp_score, "
+              f"{threads} threads via kt_for")
+    return cells / secs / 1e9, threads, sample, secs, cells
+
+
+def run_reference_hmm(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    texts, _profs, batches, desc = hmm_workload(args, 3)
+    cpu_baseline_hmm(texts, batches, args.cpu_seconds / 4)
+    vals, tot = [], 0.0
+    for _ in range(args.steps):
+        v, threads, sample, secs, _c = cpu_baseline_hmm(texts, batches, args.cpu_seconds / 2)
+        vals.append(v)
+        tot += secs
+    value = statistics.mean(vals)
+    line = {"metric": HMM_METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(tot / args.steps * 1e3, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "impl": "reference", "config": {"workload": desc, "step": "bounded sample of the workload"},
+            "cpu_baseline": {"value": round(value, 3), "unit": "GCUPS", "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": round(value, 3), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main_hmm(args):
+    import torch
+    import torch.distributed as dist
+    from protlocus_b200 import hmm as H
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    texts, profs, batches, desc = hmm_workload(args, 3 + rank)
+    ca = H.codon_alpha()
+    eng = L.Engine(local)
+    hp = [L.HmmProfile(p["emit"], p["trans"], ca, local) for p in profs]
+    cells = sum(int((ln // 3).astype(np.int64).sum()) * p["m"] for p, (_, _, ln) in zip(profs, batches))
+    d_nt = [torch.from_numpy(nt).to("cuda") for nt, _, _ in batches]
+    d_sc = [torch.zeros(len(ln), dtype=torch.int32, device="cuda") for _, _, ln in batches]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step_device():
+        for p, (nt, offs, lens), dn, ds in zip(hp, batches, d_nt, d_sc):
+            if not eng.lib.pl_hmm_score_device(eng.h, p.h, len(lens), dn.data_ptr(), offs.ctypes.data,
+                                               lens.ctypes.data, ds.data_ptr(), stream.cuda_stream):
+                raise RuntimeError("pl_hmm_score_device: " + L.error())
+
+    for _ in range(args.warmup):
+        step_device()
+    int32_peak, i16x2_peak = L.measure_int_peak(local)
+    clocks = Clocks(local)
+    eng.set_timing(True)
+    launches0 = L.load().pl_kernel_launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step_device()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t += e0.elapsed_time(e1) / 1e3
+    barrier()
+    clk = clocks.stop()
+    launches = L.load().pl_kernel_launch_count() - launches0
+    t = max_over_ranks(t)
+    value = world * cells * args.steps / t / 1e9
+    tm = eng.times()
+    dp_s = tm["dp_ms"] / 1e3
+    achieved = tm["cells"] * HMM_OPS_PER_CELL / dp_s if dp_s > 0 else 0.0
+
+    e2e = None
+    if not args.no_e2e:
+        h_nt = [torch.from_numpy(nt).pin_memory() for nt, _, _ in batches]
+        h_sc = [np.zeros(len(ln), dtype=np.int32) for _, _, ln in batches]
+        est = torch.cuda.ExternalStream(eng.stream)
+
+        def step_host():
+            for p, (nt, offs, lens), hn, hs in zip(hp, batches, h_nt, h_sc):
+                if not eng.lib.pl_hmm_score_host(eng.h, p.h, len(lens), hn.data_ptr(), hn.numel(), offs.ctypes.data,
+                                                 lens.ctypes.data, hs.ctypes.data):
+                    raise RuntimeError("pl_hmm_score_host: " + L.error())
+
+        for _ in range(max(1, args.warmup)):
+            step_host()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(est)
+        for _ in range(args.steps):
+            step_host()
+        e1.record(est)
+        torch.cuda.synchronize()
+        barrier()
+        te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+        e2e = {"value": round(world * cells * args.steps / te / 1e9, 3), "unit": "GCUPS",
+               "h2d_bytes_per_step": int(sum(nt.nbytes + 8 * len(ln) for nt, _, ln in batches)),
+               "d2h_bytes_per_step": int(sum(4 * len(ln) for _, _, ln in batches)),
+               "ms_per_step": round(te / args.steps * 1e3, 2), "api": "pl_hmm_score_host (C ABI, pinned host buffers)"}
+        # parity of this run's scores with the device path
+        ref_sc = [ds.cpu().numpy() for ds in d_sc]
+        if any((a != b).any() for a, b in zip(ref_sc, h_sc)):
+            raise RuntimeError("host and device HMM scores differ")
+
+    cpu = None
+    if rank == 0:
+        v, threads, sample, _s, _c = cpu_baseline_hmm(texts, batches, args.cpu_seconds)
+        cpu = {"value": round(v, 3), "unit": "GCUPS", "cores": threads, "kind": "reference", "sample": sample}
+    if rank == 0:
+        line = {
+            "metric": HMM_METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(t / args.steps * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": desc, "cells_per_step": cells, "seed": "3+rank",
+                       "l2": "a 256 MB buffer is written between timed steps", "parallelism": f"{world} independent ranks"},
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "int", "kernel": "k_hmm_dp", "achieved": achieved, "peak": int32_peak,
+                         "unit": "lane-ops/s", "frac": achieved / int32_peak if int32_peak else None, "traffic": None,
+                         "ops_per_cell": HMM_OPS_PER_CELL,
+                         "dp_kernel_gcups": round(tm["cells"] / dp_s / 1e9, 3) if dp_s > 0 else None,
+                         "peak_source": "measured live: pl_measure_int_peak, int32 add+max chains (%.3g lane-ops/s)"
+                                        % int32_peak,
+                         "phase_ms_per_step": {"codons_ms": round(tm["prep_ms"] / args.steps, 3),
+                                               "dp_ms": round(tm["dp_ms"] / args.steps, 3)}},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    for p in hp:
+        p.close()
     eng.close()
     if world > 1:
         dist.destroy_process_group()

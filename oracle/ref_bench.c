@@ -85,3 +85,33 @@ double ref_bench_ext(int32_t n_threads, int32_t n_jobs, const char *nt, const in
 	clock_gettime(CLOCK_MONOTONIC, &t1);
 	return (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
 }
+
+/* Profile-HMM regions: the reference's mp_hmm_dp_score (hmm.c:252-291) over kt_for,
+ * the CPU path of mp_hmm_batch_flush (hmm.c:319-335). */
+typedef struct mp_hmm_s mp_hmm_t;
+int32_t mp_hmm_dp_score(const mp_hmm_t *h, const uint8_t *nt, int32_t nlen);
+typedef struct {
+	const mp_hmm_t *h;
+	const uint8_t *nt;
+	const int32_t *off, *len;
+	int32_t *score;
+} ref_bench_hmm_t;
+
+static void ref_bench_hmm_worker(void *data, long i, int tid)
+{
+	ref_bench_hmm_t *b = (ref_bench_hmm_t*)data;
+	(void)tid;
+	b->score[i] = mp_hmm_dp_score(b->h, b->nt + b->off[i], b->len[i]);
+}
+
+double ref_bench_hmm(int32_t n_threads, const mp_hmm_t *h, int32_t n, const uint8_t *nt, const int32_t *off,
+		const int32_t *len, int32_t *score)
+{
+	ref_bench_hmm_t b;
+	struct timespec t0, t1;
+	b.h = h, b.nt = nt, b.off = off, b.len = len, b.score = score;
+	clock_gettime(CLOCK_MONOTONIC, &t0);
+	kt_for(n_threads, ref_bench_hmm_worker, &b, n);
+	clock_gettime(CLOCK_MONOTONIC, &t1);
+	return (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
+}

@@ -158,7 +158,9 @@ def regions(rng: np.random.Generator, probs: np.ndarray, n: int, len_min: int = 
             m = probs.shape[0]
             a, b = sorted(int(x) for x in rng.integers(0, m + 1, size=2))
             if b - a >= 10:
-                dom = "".join(ALPHABET[int(rng.choice(20, p=probs[i] / probs[i].sum()))] for i in range(a, b))
+                cdf = np.cumsum(probs[a:b] / probs[a:b].sum(axis=1, keepdims=True), axis=1)
+                pick = (rng.random(b - a)[:, None] > cdf).sum(axis=1).clip(0, 19)
+                dom = "".join(ALPHABET[int(x)] for x in pick)
                 cds = reverse_translate(rng, dom)
                 start = 3 * int(rng.integers(0, max(1, (L - len(cds)) // 3)))
                 s = (s[:start] + cds + s[start + len(cds):])[:max(L, start + len(cds))]
