@@ -204,3 +204,94 @@ def ext_requests(n: int, seed: int = 2, *, win_min: int = 64, win_max: int = 256
         nt = tail + gene if left else gene + tail
         out.append((nt.encode(), prot.encode(), NS_F_EXT_LEFT if left else NS_F_EXT_RIGHT))
     return out
+
+
+def pack_nt4(seq: np.ndarray) -> np.ndarray:
+    """4-bit packed nucleotide codes, two per byte, low nibble first (ntseq.c:66-69)."""
+    s = np.asarray(seq, dtype=np.uint8)
+    if s.size & 1:
+        s = np.concatenate([s, np.zeros(1, np.uint8)])
+    return (s[0::2] | (s[1::2] << 4)).astype(np.uint8)
+
+
+GAPLESS_CAND_DTYPE = np.dtype([("target_offset", "<i8"), ("target_length", "<i8"), ("query_offset", "<i8"),
+                               ("query_length", "<i4"), ("anchor_offset", "<i4"), ("anchor_count", "<i4"),
+                               ("reverse", "<i4")])
+GAPLESS_ANCHOR_DTYPE = np.dtype([("target_block", "<i8"), ("query_end", "<i4"), ("reserved", "<i4")])
+
+
+def gapless_workload(n_genes: int, genome_len: int, n_candidates: int, seed: int = 4, *, n_contigs: int = 64,
+                     al: int = 500, divergence: float = 0.25, n_intron: int = 3, frac_true: float = 0.3,
+                     anchors_per_cand: int = 8, kmer: int = 6, bbit: int = 8, gc: float = 0.45):
+    """Inputs of the gapless prefilter shaped like the seed-extension configuration: a genome
+    of n_contigs contigs at 45% GC with n_genes planted genes (a 25%-divergent copy of an
+    al-residue protein split by n_intron GT..AG introns of 80-2000 bp, on either strand),
+    the n_genes source proteins as queries, and n_candidates candidates of 1 to
+    anchors_per_cand anchors each.  A fraction frac_true of the candidates sits on its
+    protein's planted gene with anchors on the true codon positions (target_block = the
+    oriented 2^bbit block holding the anchor's last codon base, give or take six bases);
+    the others are decoys on a random contig and strand.  Frameshifts are left out so that
+    anchor positions are exact.  Returns numpy arrays laid out as
+    ns_gpu_gapless_candidate_t / ns_gpu_gapless_anchor_t (nasw.h:157-167)."""
+    from .abi import make_tables
+    rng = np.random.default_rng(seed)
+    nt4, aa20, _ = make_tables()
+    ctg_len = np.full(n_contigs, genome_len // n_contigs, dtype=np.int64)
+    ctg_len[: genome_len % n_contigs] += 1
+    ctg_off = np.zeros(n_contigs, dtype=np.int64)
+    ctg_off[1:] = np.cumsum(ctg_len[:-1])
+    p = [(1 - gc) / 2, gc / 2, gc / 2, (1 - gc) / 2]
+    genome = rng.choice(4, size=genome_len, p=p).astype(np.uint8)
+    prots, genes = [], []  # genes: (contig, reverse, codon-end per residue in oriented coordinates)
+    slot = max(1, genome_len // max(1, n_genes))
+    for g in range(n_genes):
+        prot = random_protein(rng, al)
+        cds = reverse_translate(rng, mutate(rng, prot, divergence))
+        cuts = np.sort(rng.choice(np.arange(1, al), size=min(n_intron, al - 1), replace=False))
+        ilen = [int(round(math.exp(rng.uniform(math.log(80), math.log(2000))))) for _ in cuts]
+        parts, ends, prev, shift = [], np.zeros(al, dtype=np.int64), 0, 0
+        for c, L in zip(list(cuts) + [al], ilen + [0]):
+            parts.append(cds[3 * prev:3 * c])
+            ends[prev:c] = np.arange(prev, c) * 3 + 2 + shift
+            if L:
+                parts.append(_intron(rng, L))
+                shift += max(L, 8)
+            prev = c
+        gene = nt4[np.frombuffer("".join(parts).encode(), dtype=np.uint8)]
+        G = gene.size
+        start = g * slot + int(rng.integers(0, max(1, slot - G)))
+        k = int(np.searchsorted(ctg_off, start, side="right") - 1)
+        if start + G > ctg_off[k] + ctg_len[k]:
+            start = int(ctg_off[k] + max(0, ctg_len[k] - G - 1))
+        local = start - int(ctg_off[k])
+        rev = bool(rng.random() < 0.5)
+        if rev:  # the reverse complement is stored; read in reverse orientation it is the gene
+            genome[start:start + G] = 3 - gene[::-1]
+            ostart = int(ctg_len[k]) - (local + G)
+        else:
+            genome[start:start + G] = gene
+            ostart = local
+        prots.append(prot.encode())
+        genes.append((k, rev, ends + ostart))
+    q_off = np.zeros(n_genes, dtype=np.int64)
+    q_off[1:] = np.cumsum([len(x) for x in prots[:-1]])
+    queries = aa20[np.frombuffer(b"".join(prots), dtype=np.uint8)]
+    cand = np.zeros(n_candidates, dtype=GAPLESS_CAND_DTYPE)
+    anc = np.zeros(n_candidates * anchors_per_cand, dtype=GAPLESS_ANCHOR_DTYPE)
+    na = 0
+    for ci in range(n_candidates):
+        gi = int(rng.integers(0, n_genes))
+        k, rev, ends = genes[gi]
+        true = rng.random() < frac_true
+        if not true:
+            k, rev = int(rng.integers(0, n_contigs)), bool(rng.random() < 0.5)
+        cnt = int(rng.integers(1, anchors_per_cand + 1))
+        qe = np.sort(rng.choice(np.arange(kmer - 1, al), size=cnt, replace=False))
+        pos = ends[qe] - int(rng.integers(0, 7)) if true else rng.integers(0, int(ctg_len[k]), size=cnt)
+        cand[ci] = (ctg_off[k], ctg_len[k], q_off[gi], al, na, cnt, int(rev))
+        anc["target_block"][na:na + cnt] = (np.maximum(pos, 0) >> bbit) << bbit
+        anc["query_end"][na:na + cnt] = qe
+        na += cnt
+    return {"packed": pack_nt4(genome), "bases": genome_len, "queries": queries.astype(np.uint8),
+            "candidates": cand, "anchors": anc[:na].copy(), "block_width": 1 << bbit, "kmer": kmer,
+            "contig_offsets": ctg_off, "contig_lengths": ctg_len}

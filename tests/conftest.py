@@ -40,3 +40,13 @@ def hmm_golden():
     import json
     with open(os.path.join(HERE, "golden", "hmm_golden.json")) as f:
         return json.load(f)
+
+
+@pytest.fixture(scope="session")
+def gapless_golden():
+    """Scores of the reference's gapless kernel with the generator that regenerates its inputs."""
+    import json
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import make_gapless_golden as G
+    with open(os.path.join(HERE, "golden", "gapless_golden.json")) as f:
+        return json.load(f), G

@@ -181,3 +181,20 @@ def port_hmm(m: int, emit, trans, codon_alpha, nt) -> int:
     b = np.ascontiguousarray(nt, dtype=np.uint8)
     return int(lib.port_hmm_dp_score(m, e.ctypes.data, t.ctypes.data, c.ctypes.data,
                                      b.ctypes.data if b.size else None, b.size))
+
+
+def port_gapless(w: dict, block_width: int, kmer: int, xdrop: int, mat, codon):
+    """The restatement of the gapless prefilter (oracle/gapless_port.c) on workload dict w
+    (packed, queries, candidates, anchors as from protlocus_b200.workload.gapless_workload)."""
+    import numpy as np
+    lib = port_lib()
+    f = lib.port_gapless_score_batch
+    f.argtypes = [C.c_void_p] * 3 + [C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32,
+                                     C.c_void_p, C.c_void_p]
+    m = np.ascontiguousarray(mat, dtype=np.int8)
+    cd = np.ascontiguousarray(codon, dtype=np.uint8)
+    sc = np.zeros(len(w["candidates"]), dtype=np.int32)
+    f(w["packed"].ctypes.data, w["queries"].ctypes.data, w["candidates"].ctypes.data, len(w["candidates"]),
+      w["anchors"].ctypes.data, block_width, kmer, xdrop, m.ctypes.data, int(round(len(m.reshape(-1)) ** 0.5)),
+      cd.ctypes.data, sc.ctypes.data)
+    return sc
