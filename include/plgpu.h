@@ -323,6 +323,45 @@ int pl_hmm_score_device(pl_engine_t *e, const pl_hmm_profile_t *p, int32_t n, co
 /* DP cells (codon rows x m) of the last HMM batch of this engine. */
 int64_t pl_hmm_last_cells(const pl_engine_t *e);
 
+/* ---------------------------------------------------------------------------
+ * Gapless X-drop candidate prefilter (replaces ns_gapless_xdrop_batch and its
+ * entry points, nasw-cuda.cu:1151-1395; scores bit-exact).
+ * ------------------------------------------------------------------------- */
+/* nasw.h:171 -- 1: this library always has the kernel. */
+int ns_gpu_gapless_supported(void);
+/* nasw.h:172 -- forget the resident genome; the next batch re-uploads it. */
+void ns_gpu_gapless_reset_target(void);
+/* nasw.h:170 -- batches, candidates, anchors and seed positions (anchors x block_width) so far. */
+void ns_gpu_gapless_profile(ns_gpu_gapless_profile_t *profile);
+/* nasw.h:176-181 -- scores[i] = candidate i's gapless score, INT32_MIN when no anchor
+ * gave a usable seed.  packed_nt: 4-bit codes, 2 bases per byte, low nibble first;
+ * queries: aa20 codes; score_matrix: asize x asize; codon: 64 aa20 codes.  Needs
+ * ns_gpu_init() first; returns 0 on failure (ns_gpu_error() says why).  The genome
+ * stays resident while the caller passes the same pointer and length.  Thread-safe
+ * (calls are serialised). */
+int ns_gpu_gapless_score_batch(const uint8_t *packed_nt, int64_t packed_nt_bases,
+		const uint8_t *queries, int64_t query_aa,
+		const ns_gpu_gapless_candidate_t *candidates, int32_t n_candidates,
+		const ns_gpu_gapless_anchor_t *anchors, int64_t n_anchors,
+		int32_t block_width, int32_t kmer, int32_t xdrop,
+		const int8_t *score_matrix, int32_t asize, const uint8_t *codon,
+		int32_t *scores);
+/* Bulk gapless entry points (no counterpart in the reference): the same scoring on
+ * an engine, without the genome cache.  _host takes host buffers; _device takes
+ * device pointers for the genome, queries, candidates, anchors and scores (matrix
+ * and codon table on the host) and runs on `stream` (NULL = the engine's).  Limits:
+ * block_width <= 8192, kmer <= 64, 21 <= asize <= 32.  Return 1 on success. */
+int pl_gapless_score_host(pl_engine_t *e, const uint8_t *packed_nt, int64_t packed_nt_bases,
+		const uint8_t *queries, int64_t query_aa, const ns_gpu_gapless_candidate_t *candidates, int32_t n_candidates,
+		const ns_gpu_gapless_anchor_t *anchors, int64_t n_anchors, int32_t block_width, int32_t kmer, int32_t xdrop,
+		const int8_t *score_matrix, int32_t asize, const uint8_t *codon, int32_t *scores);
+int pl_gapless_score_device(pl_engine_t *e, const uint8_t *packed_nt, int64_t packed_nt_bases,
+		const uint8_t *queries, int64_t query_aa, const ns_gpu_gapless_candidate_t *candidates, int32_t n_candidates,
+		const ns_gpu_gapless_anchor_t *anchors, int64_t n_anchors, int32_t block_width, int32_t kmer, int32_t xdrop,
+		const int8_t *score_matrix, int32_t asize, const uint8_t *codon, int32_t *scores_dev, void *stream);
+/* Extension steps (both sides, all anchors) walked by the last gapless batch of this engine. */
+int64_t pl_gapless_last_steps(const pl_engine_t *e);
+
 /* DP cells of the last extension batch: the rows the reference's row loop
  * visits (up to the x-drop row, nasw-sse.c:361-447) times al, and the nominal
  * (nl-2)*al. */

@@ -124,6 +124,7 @@ PL_EXPORT void pl_engine_destroy(pl_engine_t *e)
 	dbuf_free(&e->nt), dbuf_free(&e->aa), dbuf_free(&e->ss), dbuf_free(&e->res), dbuf_free(&e->cig);
 	pl_ext_engine_free(e);
 	pl_hmm_engine_free(e);
+	pl_gapless_engine_free(e);
 	if (e->stream) cudaStreamDestroy(e->stream);
 	free(e->hj), free(e->horder), free(e->hwave);
 	free(e);
@@ -595,6 +596,24 @@ PL_EXPORT int ns_gpu_init(int32_t device)
 fail:
 	pthread_mutex_unlock(&ns_mu);
 	return 0;
+}
+
+/* device of the request queue once ns_gpu_init() succeeded, else -1 (other translation units
+ * that require ns_gpu_init first, as the reference's gapless entry does, ask here) */
+int pl_ns_device(void)
+{
+	int d;
+	pthread_mutex_lock(&ns_mu);
+	d = ns_ready && ns_engine ? ns_engine->device : -1;
+	pthread_mutex_unlock(&ns_mu);
+	return d;
+}
+
+void pl_ns_set_error(const char *msg)
+{
+	pthread_mutex_lock(&ns_mu);
+	snprintf(ns_msg, sizeof(ns_msg), "%s", msg);
+	pthread_mutex_unlock(&ns_mu);
 }
 
 PL_EXPORT const char *ns_gpu_error(void) { return ns_msg; }

@@ -36,6 +36,11 @@ struct pl_engine_s {
 	void *h_hbuf;
 	size_t h_hcap;
 	int64_t h_last_cells;
+	/* gapless prefilter */
+	dbuf_t g_packed, g_queries, g_cand, g_anchors, g_mat, g_codon, g_scores, g_steps;
+	const uint8_t *g_cached_src;   /* host genome currently resident (ns_gpu_gapless_* cache) */
+	int64_t g_cached_bases;
+	int64_t g_last_steps;
 	/* host planning scratch */
 	plk_job_t *hj;
 	int32_t *horder, *hwave, m_jobs;
@@ -58,5 +63,8 @@ int pl_params(const ns_opt_t *opt, plk_params_t *p, int for_ext);
 int pl_max_sub(const ns_opt_t *opt);
 void pl_ext_engine_free(pl_engine_t *e);
 void pl_hmm_engine_free(pl_engine_t *e);
+void pl_gapless_engine_free(pl_engine_t *e);
+int pl_ns_device(void);
+void pl_ns_set_error(const char *msg);
 
 #endif

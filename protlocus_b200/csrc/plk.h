@@ -118,6 +118,12 @@ int plk_hmm_dp(const plk_hmm_prof_t *p, const uint8_t *rows, const int64_t *row_
 int plk_hmm_ctas_per_sm(int32_t mpad);
 int plk_hmm_warps_per_cta(void);
 int plk_hmm_smem_bytes(int32_t mpad);
+/* gapless prefilter: one warp per candidate; steps accumulates the extension steps walked */
+int plk_gapless(const uint8_t *packed, int64_t bases, const uint8_t *queries, int64_t query_aa, const void *cand,
+		int32_t n_cand, const void *anchors, int64_t n_anchors, int32_t block_width, int32_t kmer, int32_t xdrop,
+		const int8_t *mat_dev, int32_t asize, const uint8_t *codon_dev, int32_t *scores, unsigned long long *steps,
+		int32_t n_sm, void *stream);
+int plk_gapless_smem_bytes(int32_t block_width, int32_t kmer);
 /* CTAs of the DP kernel that fit on one SM at once (occupancy) */
 int plk_dp_ctas_per_sm(int32_t mode);
 uint64_t plk_launches(void);

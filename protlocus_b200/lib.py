@@ -104,6 +104,18 @@ def load() -> C.CDLL:
     lib.pl_hmm_last_cells.restype = C.c_int64
     lib.mp_hmm_dp_score_gpu.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
     lib.mp_hmm_dp_score_gpu.restype = C.c_int32
+    gl = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int32, C.c_void_p, C.c_int64,
+          C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
+    lib.ns_gpu_gapless_score_batch.argtypes = gl
+    lib.ns_gpu_gapless_score_batch.restype = C.c_int
+    lib.pl_gapless_score_host.argtypes = [C.c_void_p] + gl
+    lib.pl_gapless_score_host.restype = C.c_int
+    lib.pl_gapless_score_device.argtypes = [C.c_void_p] + gl + [C.c_void_p]
+    lib.pl_gapless_score_device.restype = C.c_int
+    lib.pl_gapless_last_steps.argtypes = [C.c_void_p]
+    lib.pl_gapless_last_steps.restype = C.c_int64
+    lib.ns_gpu_gapless_profile.argtypes = [C.c_void_p]
+    lib.ns_gpu_gapless_reset_target.argtypes = []
     _lib = lib
     return lib
 
@@ -268,6 +280,34 @@ class Engine:
                                           lens.ctypes.data, score.ctypes.data):
             raise RuntimeError("pl_hmm_score_host failed: " + error())
         return score[:n].tolist()
+
+    def gapless_score(self, w: dict, block_width: int, kmer: int, xdrop: int, mat, codon) -> np.ndarray:
+        """pl_gapless_score_host on workload dict w: one int32 score per candidate."""
+        args, keep = gapless_args(w, block_width, kmer, xdrop, mat, codon)
+        sc = np.zeros(len(w["candidates"]), dtype=np.int32)
+        if not self.lib.pl_gapless_score_host(self.h, *args, sc.ctypes.data):
+            raise RuntimeError("pl_gapless_score_host failed: " + error())
+        return sc
+
+
+def gapless_args(w: dict, block_width: int, kmer: int, xdrop: int, mat, codon):
+    """The ns_gpu_gapless_score_batch argument list (after the engine) for workload dict w."""
+    m = np.ascontiguousarray(mat, dtype=np.int8)
+    cd = np.ascontiguousarray(codon, dtype=np.uint8)
+    keep = (m, cd)
+    args = [w["packed"].ctypes.data, int(w["bases"]), w["queries"].ctypes.data, int(w["queries"].size),
+            w["candidates"].ctypes.data, len(w["candidates"]), w["anchors"].ctypes.data, len(w["anchors"]),
+            block_width, kmer, xdrop, m.ctypes.data, int(round(m.size ** 0.5)), cd.ctypes.data]
+    return args, keep
+
+
+def gapless_reference_entry(w: dict, block_width: int, kmer: int, xdrop: int, mat, codon) -> np.ndarray:
+    """ns_gpu_gapless_score_batch (the reference's entry point; needs gpu_init first)."""
+    args, keep = gapless_args(w, block_width, kmer, xdrop, mat, codon)
+    sc = np.zeros(len(w["candidates"]), dtype=np.int32)
+    if not load().ns_gpu_gapless_score_batch(*args, sc.ctypes.data):
+        raise RuntimeError("ns_gpu_gapless_score_batch failed: " + load().ns_gpu_error().decode())
+    return sc
 
 
 class HmmProfile:
