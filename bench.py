@@ -61,9 +61,10 @@ def parse():
     ap.add_argument("--pairs", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="global", choices=["global", "ext", "hmm"],
+    ap.add_argument("--workload", default="global", choices=["global", "ext", "hmm", "gapless"],
                     help="global: the batched global spliced DP (headline); ext: the batched extension DP; "
-                         "hmm: the integer profile-HMM DP")
+                         "hmm: the integer profile-HMM DP; gapless: the gapless X-drop prefilter")
+    ap.add_argument("--candidates", type=int, default=131072, help="candidates of 8 anchors (--workload gapless)")
     ap.add_argument("--profiles", type=int, default=16, help="profiles per step (--workload hmm)")
     ap.add_argument("--regions", type=int, default=4096, help="regions per profile (--workload hmm)")
     ap.add_argument("--requests", type=int, default=65536, help="extension requests per step (--workload ext)")
@@ -208,6 +209,8 @@ def main():
         return run_reference_ext(args) if args.impl == "reference" else main_ext(args)
     if args.workload == "hmm":
         return run_reference_hmm(args) if args.impl == "reference" else main_hmm(args)
+    if args.workload == "gapless":
+        return run_reference_gapless(args) if args.impl == "reference" else main_gapless(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -779,6 +782,188 @@ def main_hmm(args):
     eng.close()
     if world > 1:
         dist.destroy_process_group()
+    return 0
+
+
+# ---------------------------------------------------------------------------- gapless prefilter
+
+GL_METRIC = "gapless prefilter G seed positions/s (anchors x block_width, bit-exact scores) at 1 B200"
+GL_OPS_PER_POS = 12  # int ops per seed position: kmer=6 score lookups + adds (nasw-cuda.cu:1204-1214)
+
+
+def gapless_inputs(args, seed):
+    from protlocus_b200.abi import BLOSUM62, make_tables, set_stop_sc
+    w = W.gapless_workload(10000, 100_000_000, args.candidates, seed=seed, fixed_anchors=True)
+    mat = np.ascontiguousarray(set_stop_sc(BLOSUM62, 23), dtype=np.int8)
+    desc = (f"gapless prefilter: 100 Mb genome (64 contigs, 45% GC) with 10000 planted 500-aa genes (25% divergence, "
+            f"3 introns, either strand), {args.candidates} candidates x 8 anchors = {len(w['anchors'])} anchors "
+            "(30% on their gene, 70% decoys), block_width 256, kmer 6, xdrop 40, BLOSUM62 with stop -23")
+    return w, mat, make_tables()[2], desc
+
+
+def cpu_port_gapless(w, mat, codon, target_s):
+    """The C restatement (the reference has no CPU twin of this kernel) on a bounded sample of
+    candidates, split across all host threads (ctypes releases the GIL)."""
+    import threading
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    threads = os.cpu_count() or 1
+    n = len(w["candidates"])
+    k = min(n, max(threads, int(target_s * 4000 * threads)))  # ~4000 candidates/s/thread
+    cand = w["candidates"][:k].copy()
+    out = np.zeros(k, dtype=np.int32)
+    lib = O.port_lib()
+    f = lib.port_gapless_score_batch
+    f.argtypes = [C.c_void_p] * 3 + [C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                     C.c_int32, C.c_void_p, C.c_void_p]
+    bounds = np.linspace(0, k, threads + 1).astype(int)
+
+    def run(a, b):
+        if b > a:
+            f(w["packed"].ctypes.data, w["queries"].ctypes.data, cand[a:].ctypes.data, b - a, w["anchors"].ctypes.data,
+              256, 6, 40, mat.ctypes.data, 22, codon.ctypes.data, out[a:].ctypes.data)
+
+    t0 = time.perf_counter()
+    th = [threading.Thread(target=run, args=(bounds[i], bounds[i + 1])) for i in range(threads)]
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    secs = time.perf_counter() - t0
+    pos = int(cand["anchor_count"].clip(0, 32).sum()) * 256
+    return pos / secs / 1e9, threads, f"{k} of {n} candidates ({pos} seed positions), oracle restatement, {threads} threads", out
+
+
+def run_reference_gapless(args):
+    """The reference's own implementation of this path is its CUDA kernel (no CPU twin exists): built from
+    nasw-cuda.cu into oracle/_ref/libnscuda_ref.so and timed through its ns_gpu_gapless_score_batch."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    path = os.path.join(ROOT, "oracle", "_ref", "libnscuda_ref.so")
+    if not os.path.exists(path):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libnscuda_ref.so not built"}))
+        return 0
+    w, mat, codon, desc = gapless_inputs(args, 5)
+    ref = C.CDLL(path)
+    if not ref.ns_gpu_init(0):
+        print(json.dumps({"impl": "reference", "unavailable": "reference ns_gpu_init failed"}))
+        return 0
+    args_l, keep = L.gapless_args(w, 256, 6, 40, mat, codon)
+    ref.ns_gpu_gapless_score_batch.argtypes = L.load().ns_gpu_gapless_score_batch.argtypes
+    sc = np.zeros(len(w["candidates"]), dtype=np.int32)
+    for _ in range(max(1, args.warmup)):
+        ref.ns_gpu_gapless_score_batch(*args_l, sc.ctypes.data)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        if not ref.ns_gpu_gapless_score_batch(*args_l, sc.ctypes.data):
+            raise RuntimeError("reference gapless batch failed")
+    secs = (time.perf_counter() - t0) / args.steps
+    pos = len(w["anchors"]) * 256
+    v = pos / secs / 1e9
+    line = {"metric": GL_METRIC, "value": round(v, 3), "unit": "G seed positions/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(secs * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": desc, "implementation": "the reference's CUDA kernel (nasw-cuda.cu) on this GPU, "
+                                                           "ns_gpu_gapless_score_batch with its genome cache"},
+            "cpu_baseline": None,
+            "e2e": {"value": round(v, 3), "unit": "G seed positions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main_gapless(args):
+    import torch
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    w, mat, codon, desc = gapless_inputs(args, 5 + rank)
+    n, na = len(w["candidates"]), len(w["anchors"])
+    pos = na * 256
+    eng = L.Engine(local)
+    d = {k: torch.from_numpy(w[k].view(np.uint8).reshape(-1).copy()).to("cuda")
+         for k in ("packed", "queries", "candidates", "anchors")}
+    d_sc = torch.zeros(n, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step_device():
+        if not eng.lib.pl_gapless_score_device(eng.h, d["packed"].data_ptr(), int(w["bases"]), d["queries"].data_ptr(),
+                                               int(w["queries"].size), d["candidates"].data_ptr(), n,
+                                               d["anchors"].data_ptr(), na, 256, 6, 40, mat.ctypes.data, 22,
+                                               codon.ctypes.data, d_sc.data_ptr(), stream.cuda_stream):
+            raise RuntimeError("pl_gapless_score_device: " + L.error())
+
+    for _ in range(args.warmup):
+        step_device()
+    int32_peak, _ = L.measure_int_peak(local)
+    clocks = Clocks(local)
+    eng.set_timing(True)
+    launches0 = L.load().pl_kernel_launch_count()
+    torch.cuda.synchronize()
+    clocks.start()
+    t = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step_device()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t += e0.elapsed_time(e1) / 1e3
+    clk = clocks.stop()
+    launches = L.load().pl_kernel_launch_count() - launches0
+    tm = eng.times()
+    k_s = tm["dp_ms"] / 1e3
+    steps_walked = int(eng.lib.pl_gapless_last_steps(eng.h))
+    value = world * pos * args.steps / t / 1e9
+    achieved = pos * args.steps * GL_OPS_PER_POS / k_s if k_s > 0 else 0.0
+    # end to end through the reference-facing entry point: host buffers, genome resident after the first call
+    assert L.gpu_init(local)
+    ref_sc = d_sc.cpu().numpy()
+    e_args, keep = L.gapless_args(w, 256, 6, 40, mat, codon)
+    h_sc = np.zeros(n, dtype=np.int32)
+    for _ in range(max(1, args.warmup)):
+        L.load().ns_gpu_gapless_score_batch(*e_args, h_sc.ctypes.data)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        if not L.load().ns_gpu_gapless_score_batch(*e_args, h_sc.ctypes.data):
+            raise RuntimeError("ns_gpu_gapless_score_batch failed")
+    te = (time.perf_counter() - t0) / args.steps
+    if (h_sc != ref_sc).any():
+        raise RuntimeError("entry points disagree")
+    e2e = {"value": round(world * pos / te / 1e9, 3), "unit": "G seed positions/s",
+           "h2d_bytes_per_step": int(w["queries"].nbytes + w["candidates"].nbytes + w["anchors"].nbytes + 22 * 22 + 64),
+           "d2h_bytes_per_step": int(4 * n), "ms_per_step": round(te * 1e3, 2),
+           "api": "ns_gpu_gapless_score_batch (the reference's C entry point; genome resident across calls as in "
+                  "nasw-cuda.cu:1362-1367), wall clock per call"}
+    cpu = None
+    if rank == 0:
+        v, threads, sample, out = cpu_port_gapless(w, mat, codon, args.cpu_seconds)
+        if (out != ref_sc[:len(out)]).any():
+            raise RuntimeError("device scores differ from the restatement")
+        cpu = {"value": round(v, 3), "unit": "G seed positions/s", "cores": threads, "kind": "port", "sample": sample}
+        line = {"metric": GL_METRIC, "value": round(value, 3), "unit": "G seed positions/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t / args.steps * 1e3, 2),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+                "data": "synthetic",
+                "config": {"workload": desc, "candidates": n, "anchors": na, "seed_positions_per_step": pos,
+                           "extension_steps_per_step": steps_walked, "candidates_per_s": round(world * n * args.steps / t, 1),
+                           "l2": "a 256 MB buffer is written between timed steps (the 50 MB genome itself fits in L2)",
+                           "parallelism": f"{world} independent ranks"},
+                "e2e": e2e, "gpu_launches": int(launches),
+                "roofline": {"bound": "int", "kernel": "k_gapless", "achieved": achieved, "peak": int32_peak,
+                             "unit": "lane-ops/s", "frac": achieved / int32_peak if int32_peak else None,
+                             "traffic": None, "ops_per_seed_position": GL_OPS_PER_POS,
+                             "kernel_ms_per_step": round(tm["dp_ms"] / args.steps, 3),
+                             "peak_source": "measured live: pl_measure_int_peak, int32 (%.3g lane-ops/s)" % int32_peak},
+                "cpu_baseline": cpu, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    eng.close()
     return 0
 
 

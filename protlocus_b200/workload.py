@@ -222,12 +222,14 @@ GAPLESS_ANCHOR_DTYPE = np.dtype([("target_block", "<i8"), ("query_end", "<i4"), 
 
 def gapless_workload(n_genes: int, genome_len: int, n_candidates: int, seed: int = 4, *, n_contigs: int = 64,
                      al: int = 500, divergence: float = 0.25, n_intron: int = 3, frac_true: float = 0.3,
-                     anchors_per_cand: int = 8, kmer: int = 6, bbit: int = 8, gc: float = 0.45):
+                     anchors_per_cand: int = 8, kmer: int = 6, bbit: int = 8, gc: float = 0.45,
+                     fixed_anchors: bool = False):
     """Inputs of the gapless prefilter shaped like the seed-extension configuration: a genome
     of n_contigs contigs at 45% GC with n_genes planted genes (a 25%-divergent copy of an
     al-residue protein split by n_intron GT..AG introns of 80-2000 bp, on either strand),
     the n_genes source proteins as queries, and n_candidates candidates of 1 to
-    anchors_per_cand anchors each.  A fraction frac_true of the candidates sits on its
+    anchors_per_cand anchors each (exactly anchors_per_cand with fixed_anchors, as the
+    mapper's evenly spaced pick gives for chains of 8 or more anchors, map.c:474-507).  A fraction frac_true of the candidates sits on its
     protein's planted gene with anchors on the true codon positions (target_block = the
     oriented 2^bbit block holding the anchor's last codon base, give or take six bases);
     the others are decoys on a random contig and strand.  Frameshifts are left out so that
@@ -285,7 +287,7 @@ def gapless_workload(n_genes: int, genome_len: int, n_candidates: int, seed: int
         true = rng.random() < frac_true
         if not true:
             k, rev = int(rng.integers(0, n_contigs)), bool(rng.random() < 0.5)
-        cnt = int(rng.integers(1, anchors_per_cand + 1))
+        cnt = anchors_per_cand if fixed_anchors else int(rng.integers(1, anchors_per_cand + 1))
         qe = np.sort(rng.choice(np.arange(kmer - 1, al), size=cnt, replace=False))
         pos = ends[qe] - int(rng.integers(0, 7)) if true else rng.integers(0, int(ctg_len[k]), size=cnt)
         cand[ci] = (ctg_off[k], ctg_len[k], q_off[gi], al, na, cnt, int(rev))
