@@ -362,6 +362,32 @@ int pl_gapless_score_device(pl_engine_t *e, const uint8_t *packed_nt, int64_t pa
 /* Extension steps (both sides, all anchors) walked by the last gapless batch of this engine. */
 int64_t pl_gapless_last_steps(const pl_engine_t *e);
 
+/* ---------------------------------------------------------------------------
+ * Recheck Forward score (no C ABI in the reference: rc_score is static in
+ * recheck.c:283-440 and runs from its kt_for worker, recheck.c:546-568).
+ * Multihit-local Forward in log space, float, with the optional null2
+ * (ByExpectation) bias correction: bits = (fwd - null1 - bias) / ln 2 and the
+ * bias in bits, exactly the two numbers rc_score returns, to float rounding
+ * (reduction order differs; agreement within 1e-5 relative).
+ * ------------------------------------------------------------------------- */
+typedef struct pl_rc_profile_s pl_rc_profile_t;
+/* A search profile as recheck.c builds it (rc_prof_t, recheck.c:66-72): msc
+ * M x 21 match log-odds in nats (column 20 = degenerate residue), tsc M x 8
+ * transitions in the order MM, IM, DM, BM, MI, II, MD, DD (recheck.c:74).
+ * M <= 2048. */
+pl_rc_profile_t *pl_rc_profile_create(int32_t device, int32_t M, const float *msc, const float *tsc);
+void pl_rc_profile_destroy(pl_rc_profile_t *p);
+/* Score n peptides: peptide q is dsq[off[q] .. off[q]+len[q]) (residue codes
+ * 0-19 in HMMER order ACDEFGHIKLMNPQRSTVWY, 20 = other, as recheck.c:52-62
+ * encodes them; len >= 1) against profiles[prof_id[q]].  do_null2 as recheck's
+ * default (its -n option turns it off); pairs above 2^25 cells skip it, as
+ * recheck.c:273 does.  Host buffers; returns 1 on success. */
+int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *profiles, int32_t n_prof, int32_t n,
+		const int32_t *prof_id, const uint8_t *dsq, int64_t dsq_len, const int64_t *off, const int32_t *len,
+		int32_t do_null2, float *bits, float *bias);
+/* DP cells (sum of L*M) of the last recheck batch of this engine. */
+int64_t pl_rc_last_cells(const pl_engine_t *e);
+
 /* DP cells of the last extension batch: the rows the reference's row loop
  * visits (up to the x-drop row, nasw-sse.c:361-447) times al, and the nominal
  * (nl-2)*al. */

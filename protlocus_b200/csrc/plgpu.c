@@ -125,6 +125,7 @@ PL_EXPORT void pl_engine_destroy(pl_engine_t *e)
 	pl_ext_engine_free(e);
 	pl_hmm_engine_free(e);
 	pl_gapless_engine_free(e);
+	pl_rc_engine_free(e);
 	if (e->stream) cudaStreamDestroy(e->stream);
 	free(e->hj), free(e->horder), free(e->hwave);
 	free(e);

@@ -41,6 +41,9 @@ struct pl_engine_s {
 	const uint8_t *g_cached_src;   /* host genome currently resident (ns_gpu_gapless_* cache) */
 	int64_t g_cached_bases;
 	int64_t g_last_steps;
+	/* recheck Forward */
+	dbuf_t r_prof, r_pep, r_dsq, r_order, r_counter, r_scratch, r_bits, r_bias;
+	int64_t r_last_cells;
 	/* host planning scratch */
 	plk_job_t *hj;
 	int32_t *horder, *hwave, m_jobs;
@@ -64,6 +67,7 @@ int pl_max_sub(const ns_opt_t *opt);
 void pl_ext_engine_free(pl_engine_t *e);
 void pl_hmm_engine_free(pl_engine_t *e);
 void pl_gapless_engine_free(pl_engine_t *e);
+void pl_rc_engine_free(pl_engine_t *e);
 int pl_ns_device(void);
 void pl_ns_set_error(const char *msg);
 

@@ -124,6 +124,25 @@ int plk_gapless(const uint8_t *packed, int64_t bases, const uint8_t *queries, in
 		const int8_t *mat_dev, int32_t asize, const uint8_t *codon_dev, int32_t *scores, unsigned long long *steps,
 		int32_t n_sm, void *stream);
 int plk_gapless_smem_bytes(int32_t block_width, int32_t kmer);
+
+/* profile of the recheck Forward (recheck.c:66-72 search profile): device pointers */
+typedef struct {
+	const float *msc;   /* [M][21] match log-odds in nats, column 20 = degenerate residue */
+	const float *tsc;   /* [M][8] transitions (recheck.c:74 order) */
+	int32_t M, pad;
+} plk_rc_prof_t;
+/* one peptide */
+typedef struct {
+	int64_t dsq_off;      /* residue codes 0-20 */
+	int64_t scratch_off;  /* float offset of the null2 scratch: 4*(L+1)*(M+1) + 6*(L+1) floats */
+	int32_t len, prof, null2, pad;
+} plk_rc_pep_t;
+#define PLK_RC_MAX_C 64                 /* columns per lane: profiles up to 32*64 = 2048 positions */
+#define PLK_RC_MAX_M (32 * PLK_RC_MAX_C)
+int plk_rc_forward(const plk_rc_prof_t *prof, const plk_rc_pep_t *pep, const uint8_t *dsq, const int32_t *order,
+		int32_t n, int32_t *counter, float *scratch, float *bits, float *bias, int32_t max_m, int32_t n_sm,
+		void *stream);
+int plk_rc_smem_per_warp(int32_t max_m);
 /* CTAs of the DP kernel that fit on one SM at once (occupancy) */
 int plk_dp_ctas_per_sm(int32_t mode);
 uint64_t plk_launches(void);

@@ -1,0 +1,170 @@
+/*
+ * plrc.c -- host layer of the recheck Forward score (the device replacement of
+ * recheck.c's rc_score and its kt_for worker, recheck.c:283-440 and :546-568).
+ *
+ * Profiles are the search profiles recheck.c builds (rc_prof_t's msc / tsc,
+ * recheck.c:66-72 and :197-249), uploaded once with pl_rc_profile_create.  A
+ * batch scores peptides against their own profiles; with null2 every peptide
+ * needs scratch of 4*(L+1)*(M+1) + 6*(L+1) floats (the Forward and Backward M/I
+ * rows and the special states of every row), and a batch whose
+ * scratch exceeds the engine's budget runs in waves.  As in recheck.c, the
+ * null2 correction is skipped for a pair above 2^25 DP cells
+ * (RC_NULL2_MAXCELLS, recheck.c:273).
+ */
+#define _POSIX_C_SOURCE 200809L
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "plhost.h"
+
+#define RC_NULL2_MAXCELLS 33554432LL
+
+struct pl_rc_profile_s {
+	int device;
+	plk_rc_prof_t k;
+};
+
+PL_EXPORT pl_rc_profile_t *pl_rc_profile_create(int32_t device, int32_t M, const float *msc, const float *tsc)
+{
+	pl_rc_profile_t *p;
+	if (M < 1 || M > PLK_RC_MAX_M || !msc || !tsc) {
+		pl_set_error("recheck profile of length %d (1..%d supported)", M, PLK_RC_MAX_M);
+		return 0;
+	}
+	p = (pl_rc_profile_t*)calloc(1, sizeof(*p));
+	if (!p) { pl_set_error("out of host memory"); return 0; }
+	p->device = device, p->k.M = M;
+	CK(cudaSetDevice(device));
+	CK(cudaMalloc((void**)&p->k.msc, sizeof(float) * 21 * (size_t)M));
+	CK(cudaMalloc((void**)&p->k.tsc, sizeof(float) * 8 * (size_t)M));
+	CK(cudaMemcpy((void*)p->k.msc, msc, sizeof(float) * 21 * (size_t)M, cudaMemcpyHostToDevice));
+	CK(cudaMemcpy((void*)p->k.tsc, tsc, sizeof(float) * 8 * (size_t)M, cudaMemcpyHostToDevice));
+	return p;
+fail:
+	if (p->k.msc) cudaFree((void*)p->k.msc);
+	if (p->k.tsc) cudaFree((void*)p->k.tsc);
+	free(p);
+	return 0;
+}
+
+PL_EXPORT void pl_rc_profile_destroy(pl_rc_profile_t *p)
+{
+	if (!p) return;
+	cudaSetDevice(p->device);
+	cudaFree((void*)p->k.msc), cudaFree((void*)p->k.tsc);
+	free(p);
+}
+
+void pl_rc_engine_free(pl_engine_t *e)
+{
+	dbuf_free(&e->r_prof), dbuf_free(&e->r_pep), dbuf_free(&e->r_dsq), dbuf_free(&e->r_order);
+	dbuf_free(&e->r_counter), dbuf_free(&e->r_scratch), dbuf_free(&e->r_bits), dbuf_free(&e->r_bias);
+}
+
+typedef struct { int64_t key; int32_t idx; } pl_rkey_t;
+static int pl_rkey_cmp(const void *a, const void *b)
+{
+	const pl_rkey_t *x = (const pl_rkey_t*)a, *y = (const pl_rkey_t*)b;
+	if (x->key != y->key) return x->key > y->key ? -1 : 1;
+	return x->idx - y->idx;
+}
+
+PL_EXPORT int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *profiles, int32_t n_prof, int32_t n,
+		const int32_t *prof_id, const uint8_t *dsq, int64_t dsq_len, const int64_t *off, const int32_t *len,
+		int32_t do_null2, float *bits, float *bias)
+{
+	plk_rc_prof_t *hp = 0;
+	plk_rc_pep_t *pep = 0;
+	pl_rkey_t *key = 0;
+	int32_t *order = 0, q, max_m = 1;
+	int64_t budget, cells_total = 0;
+	cudaStream_t st;
+	int ok = 0;
+	if (!e) { pl_set_error("no engine"); return 0; }
+	if (n <= 0) return 1;
+	st = e->stream;
+	CK(cudaSetDevice(e->device));
+	hp = (plk_rc_prof_t*)malloc(sizeof(*hp) * (size_t)(n_prof > 0 ? n_prof : 1));
+	pep = (plk_rc_pep_t*)calloc((size_t)n, sizeof(*pep));
+	key = (pl_rkey_t*)malloc(sizeof(*key) * (size_t)n);
+	order = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+	if (!hp || !pep || !key || !order) { pl_set_error("out of host memory"); goto fail; }
+	for (q = 0; q < n_prof; ++q) {
+		if (!profiles[q] || profiles[q]->device != e->device) { pl_set_error("profile %d missing or on another device", q); goto fail; }
+		hp[q] = profiles[q]->k;
+		if (hp[q].M > max_m) max_m = hp[q].M;
+	}
+	for (q = 0; q < n; ++q) {
+		const int32_t pid = prof_id[q], L = len[q];
+		int64_t cells;
+		if (pid < 0 || pid >= n_prof) { pl_set_error("peptide %d: profile %d of %d", q, pid, n_prof); goto fail; }
+		if (L < 1 || off[q] < 0 || off[q] + L > dsq_len) { pl_set_error("peptide %d: length %d at %lld", q, L, (long long)off[q]); goto fail; }
+		cells = (int64_t)(L + 1) * (hp[pid].M + 1);
+		pep[q].dsq_off = off[q], pep[q].len = L, pep[q].prof = pid;
+		pep[q].null2 = do_null2 && cells <= RC_NULL2_MAXCELLS;
+		pep[q].scratch_off = 0;  /* set per wave below */
+		key[q].key = (int64_t)L * hp[pid].M, key[q].idx = q;
+		cells_total += (int64_t)L * hp[pid].M;
+	}
+	{ /* residue codes index the 21-column score rows */
+		int64_t j;
+		for (j = 0; j < dsq_len; ++j)
+			if (dsq[j] > 20) { pl_set_error("residue code %d at %lld (0-20 expected)", dsq[j], (long long)j); goto fail; }
+	}
+	qsort(key, (size_t)n, sizeof(*key), pl_rkey_cmp);
+	if (!dbuf_ensure(&e->r_prof, sizeof(*hp) * (size_t)(n_prof > 0 ? n_prof : 1)) ||
+			!dbuf_ensure(&e->r_pep, sizeof(*pep) * (size_t)n) || !dbuf_ensure(&e->r_dsq, (size_t)dsq_len) ||
+			!dbuf_ensure(&e->r_order, sizeof(int32_t) * (size_t)n) || !dbuf_ensure(&e->r_counter, 64) ||
+			!dbuf_ensure(&e->r_bits, sizeof(float) * (size_t)n) || !dbuf_ensure(&e->r_bias, sizeof(float) * (size_t)n))
+		goto fail;
+	CK(cudaMemcpyAsync(e->r_prof.p, hp, sizeof(*hp) * (size_t)n_prof, cudaMemcpyHostToDevice, st));
+	CK(cudaMemcpyAsync(e->r_dsq.p, dsq, (size_t)dsq_len, cudaMemcpyHostToDevice, st));
+	/* waves: longest first, scratch within the budget (the largest single peptide always fits) */
+	budget = e->trace_budget;
+	e->n_ev = 0;
+	{
+		int32_t w0 = 0;
+		while (w0 < n) {
+			int32_t w1 = w0;
+			int64_t used = 0;
+			while (w1 < n) {
+				plk_rc_pep_t *p = &pep[key[w1].idx];
+				const int64_t need = p->null2 ? 4 * (int64_t)(p->len + 1) * (hp[p->prof].M + 1) + 6 * (int64_t)(p->len + 1) : 0;
+				if (w1 > w0 && (used + need) * (int64_t)sizeof(float) > budget) break;
+				p->scratch_off = used, used += (need + 3) / 4 * 4;
+				order[w1] = key[w1].idx;
+				++w1;
+			}
+			if (!dbuf_ensure(&e->r_scratch, (size_t)(used > 0 ? used : 4) * sizeof(float))) goto fail;
+			CK(cudaMemcpyAsync(e->r_pep.p, pep, sizeof(*pep) * (size_t)n, cudaMemcpyHostToDevice, st));
+			CK(cudaMemcpyAsync((int32_t*)e->r_order.p + w0, order + w0, sizeof(int32_t) * (size_t)(w1 - w0),
+					cudaMemcpyHostToDevice, st));
+			PL_TIME(e, st, 1);
+			CKK(plk_rc_forward((const plk_rc_prof_t*)e->r_prof.p, (const plk_rc_pep_t*)e->r_pep.p,
+					(const uint8_t*)e->r_dsq.p, (const int32_t*)e->r_order.p + w0, w1 - w0, (int32_t*)e->r_counter.p,
+					(float*)e->r_scratch.p, (float*)e->r_bits.p, (float*)e->r_bias.p, max_m, e->n_sm, st));
+			PL_TIME(e, st, 1);
+			CK(cudaStreamSynchronize(st));  /* the next wave reuses the scratch and the job table */
+			w0 = w1;
+		}
+	}
+	CK(cudaMemcpyAsync(bits, e->r_bits.p, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, st));
+	CK(cudaMemcpyAsync(bias, e->r_bias.p, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	if (e->timing) {
+		int k;
+		float ms;
+		for (k = 0; k + 1 < e->n_ev; k += 2) {
+			cudaEventElapsedTime(&ms, e->ev[k], e->ev[k + 1]);
+			e->acc_ms[e->ev_kind[k]] += ms;
+		}
+		e->acc_dp_launches += e->n_ev / 2, e->acc_cells += cells_total;
+	}
+	e->r_last_cells = cells_total;
+	ok = 1;
+fail:
+	free(hp), free(pep), free(key), free(order);
+	return ok;
+}
+
+PL_EXPORT int64_t pl_rc_last_cells(const pl_engine_t *e) { return e ? e->r_last_cells : 0; }

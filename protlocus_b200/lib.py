@@ -116,6 +116,14 @@ def load() -> C.CDLL:
     lib.pl_gapless_last_steps.restype = C.c_int64
     lib.ns_gpu_gapless_profile.argtypes = [C.c_void_p]
     lib.ns_gpu_gapless_reset_target.argtypes = []
+    lib.pl_rc_profile_create.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]
+    lib.pl_rc_profile_create.restype = C.c_void_p
+    lib.pl_rc_profile_destroy.argtypes = [C.c_void_p]
+    lib.pl_rc_score_host.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64,
+                                     C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
+    lib.pl_rc_score_host.restype = C.c_int
+    lib.pl_rc_last_cells.argtypes = [C.c_void_p]
+    lib.pl_rc_last_cells.restype = C.c_int64
     _lib = lib
     return lib
 
@@ -288,6 +296,50 @@ class Engine:
         if not self.lib.pl_gapless_score_host(self.h, *args, sc.ctypes.data):
             raise RuntimeError("pl_gapless_score_host failed: " + error())
         return sc
+
+
+    def rc_score(self, profiles, peptides, do_null2: bool = True):
+        """Recheck Forward scores.  profiles: list of RcProfile; peptides: list of (profile index,
+        residue-code array).  Returns (bits, bias) float32 arrays."""
+        n = len(peptides)
+        pid = np.array([p for p, _ in peptides], dtype=np.int32)
+        lens = np.array([len(d) for _, d in peptides], dtype=np.int32)
+        offs = np.zeros(n, dtype=np.int64)
+        if n > 1:
+            offs[1:] = np.cumsum(lens[:-1])
+        dsq = np.ascontiguousarray(np.concatenate([np.asarray(d, dtype=np.uint8) for _, d in peptides]))
+        handles = (C.c_void_p * len(profiles))(*[p.h for p in profiles])
+        bits = np.zeros(n, dtype=np.float32)
+        bias = np.zeros(n, dtype=np.float32)
+        if not self.lib.pl_rc_score_host(self.h, handles, len(profiles), n, pid.ctypes.data, dsq.ctypes.data, dsq.size,
+                                         offs.ctypes.data, lens.ctypes.data, int(do_null2), bits.ctypes.data,
+                                         bias.ctypes.data):
+            raise RuntimeError("pl_rc_score_host failed: " + error())
+        return bits, bias
+
+
+class RcProfile:
+    """A pl_rc_profile_t: recheck's search profile (msc M x 21, tsc M x 8, float32) on a device."""
+
+    def __init__(self, msc, tsc, device: int = 0):
+        self.lib = load()
+        m = np.ascontiguousarray(msc, dtype=np.float32).reshape(-1, 21)
+        t = np.ascontiguousarray(tsc, dtype=np.float32).reshape(-1, 8)
+        self.M = m.shape[0]
+        self.h = self.lib.pl_rc_profile_create(device, self.M, m.ctypes.data, t.ctypes.data)
+        if not self.h:
+            raise RuntimeError("pl_rc_profile_create failed: " + error())
+
+    def close(self):
+        if self.h:
+            self.lib.pl_rc_profile_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def gapless_args(w: dict, block_width: int, kmer: int, xdrop: int, mat, codon):

@@ -198,3 +198,63 @@ def port_gapless(w: dict, block_width: int, kmer: int, xdrop: int, mat, codon):
       w["anchors"].ctypes.data, block_width, kmer, xdrop, m.ctypes.data, int(round(len(m.reshape(-1)) ** 0.5)),
       cd.ctypes.data, sc.ctypes.data)
     return sc
+
+
+RECHECK_SO = os.path.join(ORACLE, "_ref", "librecheck_ref.so")
+_rc = None
+
+
+def rc_lib():
+    """The reference's recheck.c (rc_score and its profile reader) built by oracle/Makefile, or None."""
+    global _rc
+    if _rc is None and os.path.exists(RECHECK_SO):
+        lib = C.CDLL(RECHECK_SO)
+        lib.ref_rc_load.argtypes = [C.c_char_p, C.POINTER(C.c_void_p)]
+        lib.ref_rc_M.argtypes = [C.c_void_p, C.c_int]
+        lib.ref_rc_msc.argtypes = lib.ref_rc_tsc.argtypes = [C.c_void_p, C.c_int]
+        lib.ref_rc_msc.restype = lib.ref_rc_tsc.restype = C.POINTER(C.c_float)
+        lib.ref_rc_encode.argtypes = [C.c_char_p, C.c_int32, C.c_void_p]
+        lib.ref_rc_score.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int32, C.c_int, C.POINTER(C.c_float),
+                                     C.POINTER(C.c_float)]
+        lib.ref_rc_bench.restype = C.c_double
+        lib.ref_rc_bench.argtypes = [C.c_int, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_int, C.c_void_p, C.c_void_p]
+        _rc = lib
+    return _rc
+
+
+def rc_load(text: str):
+    """Parse HMMER3 text with the reference's rc_read_prof: (handle, [(M, msc, tsc), ...])."""
+    import tempfile
+    import numpy as np
+    lib = rc_lib()
+    with tempfile.NamedTemporaryFile("w", suffix=".hmm", delete=False) as f:
+        f.write(text)
+        path = f.name
+    h = C.c_void_p()
+    n = lib.ref_rc_load(path.encode(), C.byref(h))
+    os.unlink(path)
+    if n < 0:
+        raise RuntimeError("rc_read_prof failed")
+    out = []
+    for k in range(n):
+        M = lib.ref_rc_M(h, k)
+        msc = np.ctypeslib.as_array(lib.ref_rc_msc(h, k), shape=(M * 21,)).copy()
+        tsc = np.ctypeslib.as_array(lib.ref_rc_tsc(h, k), shape=(M * 8,)).copy()
+        out.append((M, msc, tsc))
+    return h, out
+
+
+def rc_encode(seq: bytes):
+    import numpy as np
+    d = np.zeros(len(seq), dtype=np.uint8)
+    rc_lib().ref_rc_encode(seq, len(seq), d.ctypes.data)
+    return d
+
+
+def rc_ref_score(handle, k: int, dsq, null2: bool = True):
+    import numpy as np
+    b, s = C.c_float(), C.c_float()
+    d = np.ascontiguousarray(dsq, dtype=np.uint8)
+    rc_lib().ref_rc_score(handle, k, d.ctypes.data, d.size, int(null2), C.byref(b), C.byref(s))
+    return b.value, s.value
