@@ -61,9 +61,11 @@ def parse():
     ap.add_argument("--pairs", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="global", choices=["global", "ext", "hmm", "gapless"],
+    ap.add_argument("--workload", default="global", choices=["global", "ext", "hmm", "gapless", "forward"],
                     help="global: the batched global spliced DP (headline); ext: the batched extension DP; "
-                         "hmm: the integer profile-HMM DP; gapless: the gapless X-drop prefilter")
+                         "hmm: the integer profile-HMM DP; gapless: the gapless X-drop prefilter; "
+                         "forward: the recheck Forward score")
+    ap.add_argument("--peptides", type=int, default=20000, help="peptides per step (--workload forward)")
     ap.add_argument("--candidates", type=int, default=131072, help="candidates of 8 anchors (--workload gapless)")
     ap.add_argument("--profiles", type=int, default=16, help="profiles per step (--workload hmm)")
     ap.add_argument("--regions", type=int, default=4096, help="regions per profile (--workload hmm)")
@@ -211,6 +213,8 @@ def main():
         return run_reference_hmm(args) if args.impl == "reference" else main_hmm(args)
     if args.workload == "gapless":
         return run_reference_gapless(args) if args.impl == "reference" else main_gapless(args)
+    if args.workload == "forward":
+        return main_forward(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -963,6 +967,106 @@ def main_gapless(args):
                              "peak_source": "measured live: pl_measure_int_peak, int32 (%.3g lane-ops/s)" % int32_peak},
                 "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line), flush=True)
+    eng.close()
+    return 0
+
+
+# ---------------------------------------------------------------------------- recheck Forward
+
+FW_METRIC = "recheck Forward GCUPS (float, null2 on; cells = peptide length x profile length) at 1 B200"
+
+
+def forward_workload(args, seed):
+    from protlocus_b200 import hmm as H
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    if O.rc_lib() is None:
+        raise RuntimeError("--workload forward builds its profiles with recheck.c's reader (oracle/_ref/librecheck_ref.so)")
+    texts, probs = H.synthetic_profiles(200, seed=seed, m_min=50, m_max=800)
+    handle, profs = O.rc_load("".join(texts))
+    rng = np.random.default_rng(seed + 7)
+    pid = rng.integers(0, len(profs), size=args.peptides).astype(np.int32)
+    lens = rng.integers(50, 601, size=args.peptides).astype(np.int32)
+    dsq = rng.integers(0, 20, size=int(lens.sum())).astype(np.uint8)
+    off = np.zeros(args.peptides, dtype=np.int64)
+    off[1:] = np.cumsum(lens[:-1])
+    desc = (f"recheck Forward: {args.peptides} peptides of 50-600 residues, each against one of 200 synthetic "
+            "Plan7 profiles (m 50-800) read by recheck.c's rc_read_prof, null2 bias correction on")
+    return handle, profs, pid, lens, dsq, off, desc
+
+
+def main_forward(args):
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    handle, profs, pid, lens, dsq, off, desc = forward_workload(args, 11)
+    threads = os.cpu_count() or 1
+    cells = int((lens.astype(np.int64) * np.array([profs[k][0] for k in pid])).sum())
+    if args.impl == "reference":
+        k = max(threads, min(len(pid), int(args.cpu_seconds * 15 * threads)))
+        bits = np.zeros(k, dtype=np.float32)
+        bias = np.zeros(k, dtype=np.float32)
+        secs = O.rc_lib().ref_rc_bench(threads, handle, k, pid.ctypes.data, dsq.ctypes.data, off.ctypes.data,
+                                       lens.ctypes.data, 1, bits.ctypes.data, bias.ctypes.data)
+        c = int((lens[:k].astype(np.int64) * np.array([profs[q][0] for q in pid[:k]])).sum())
+        v = c / secs / 1e9
+        print(json.dumps({"metric": FW_METRIC, "value": round(v, 4), "unit": "GCUPS", "n_gpus": 1, "steps": 1,
+                          "warmup": 0, "ms_per_step": round(secs * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+                          "config": {"workload": desc}, "e2e": {"value": round(v, 4), "unit": "GCUPS",
+                                                                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                          "cpu_baseline": {"value": round(v, 4), "unit": "GCUPS", "cores": threads, "kind": "reference",
+                                           "sample": f"{k} peptides, recheck.c rc_score via kt_for"}}), flush=True)
+        return 0
+    torch.cuda.set_device(local)
+    eng = L.Engine(local)
+    gp = [L.RcProfile(msc, tsc, local) for _, msc, tsc in profs]
+    handles = (C.c_void_p * len(gp))(*[p.h for p in gp])
+    bits = np.zeros(len(pid), dtype=np.float32)
+    bias = np.zeros(len(pid), dtype=np.float32)
+
+    def step():
+        if not eng.lib.pl_rc_score_host(eng.h, handles, len(gp), len(pid), pid.ctypes.data, dsq.ctypes.data, dsq.size,
+                                        off.ctypes.data, lens.ctypes.data, 1, bits.ctypes.data, bias.ctypes.data):
+            raise RuntimeError("pl_rc_score_host: " + L.error())
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    eng.set_timing(True)
+    launches0 = L.load().pl_kernel_launch_count()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    te = (time.perf_counter() - t0) / args.steps
+    launches = L.load().pl_kernel_launch_count() - launches0
+    tm = eng.times()
+    kern_s = tm["dp_ms"] / 1e3 / args.steps
+    # reference sample on the host cores
+    k = max(threads, min(len(pid), int(args.cpu_seconds * 15 * threads)))
+    rb = np.zeros(k, dtype=np.float32)
+    rs = np.zeros(k, dtype=np.float32)
+    secs = O.rc_lib().ref_rc_bench(threads, handle, k, pid.ctypes.data, dsq.ctypes.data, off.ctypes.data,
+                                   lens.ctypes.data, 1, rb.ctypes.data, rs.ctypes.data)
+    err = float(np.max(np.abs(bits[:k] - rb) / np.maximum(1.0, np.abs(rb))))
+    c = int((lens[:k].astype(np.int64) * np.array([profs[q][0] for q in pid[:k]])).sum())
+    line = {"metric": FW_METRIC, "value": round(cells / kern_s / 1e9, 3), "unit": "GCUPS", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(kern_s * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": desc, "cells_per_step": cells, "max_rel_err_vs_reference": err},
+            "e2e": {"value": round(cells / te / 1e9, 3), "unit": "GCUPS", "ms_per_step": round(te * 1e3, 2),
+                    "h2d_bytes_per_step": int(dsq.nbytes + 20 * len(pid)), "d2h_bytes_per_step": int(8 * len(pid)),
+                    "api": "pl_rc_score_host (C ABI, host buffers), wall clock"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "mufu/fp32", "kernel": "k_rc_forward", "achieved": None, "peak": None, "frac": None,
+                         "note": "transcendental-bound (expf + log1pf per logsum); row chains serial by design"},
+            "cpu_baseline": {"value": round(c / secs / 1e9, 4), "unit": "GCUPS", "cores": threads, "kind": "reference",
+                             "sample": f"{k} peptides, recheck.c rc_score via kt_for"}}
+    print(json.dumps(line), flush=True)
+    for p in gp:
+        p.close()
     eng.close()
     return 0
 

@@ -57,7 +57,8 @@ void ref_rc_score(const rc_prof_t *p, int k, const uint8_t *dsq, int32_t L, int 
 
 typedef struct {
 	const rc_prof_t *prof;
-	const int32_t *prof_id, *off, *len;
+	const int32_t *prof_id, *len;
+	const int64_t *off;
 	const uint8_t *dsq;
 	int do_null2;
 	rc_scratch_t *scr;
@@ -72,7 +73,7 @@ static void ref_rc_worker(void *data, long i, int tid)
 
 /* rc_score of every peptide over kt_for; returns wall seconds */
 double ref_rc_bench(int n_threads, const rc_prof_t *prof, int32_t n, const int32_t *prof_id, const uint8_t *dsq,
-		const int32_t *off, const int32_t *len, int do_null2, float *bits, float *bias)
+		const int64_t *off, const int32_t *len, int do_null2, float *bits, float *bias)
 {
 	ref_rc_bench_t b;
 	struct timespec t0, t1;
