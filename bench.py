@@ -44,8 +44,10 @@ sys.path.insert(0, ROOT)
 from protlocus_b200 import lib as L  # noqa: E402
 from protlocus_b200 import workload as W  # noqa: E402
 from protlocus_b200.abi import NS_F_CIGAR, ExtJob, ExtResult, Options, SpliceJob, SpliceResult  # noqa: E402
+from protlocus_b200.ranks import Ranks, job_rate  # noqa: E402
 
 METRIC = "spliced-DP GCUPS (bit-exact) at 1 B200"
+DP_DRAM_BYTES_PER_CELL = 2.08  # ncu: k_splice_dp dram__bytes_read+write per cell (trace words are 2.0 B/cell)
 OPS_PER_CELL = 65  # int16 lane-ops per cell with traceback bits, counted from nasw-sse.c:465-553
 WORKLOAD = ("batched global spliced DP: 4096 protein/window pairs x 2 strands = 8192 DPs with CIGAR; "
             "protein log-normal median 350 aa (50-2500), window uniform 1-50 kb, Poisson(4) introns, "
@@ -218,29 +220,14 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     import torch
-    import torch.distributed as dist
-    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    R = Ranks("nccl")
+    rank, world, local, barrier, max_over_ranks = R.rank, R.world, R.local, R.barrier, R.max
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    jobs = make_jobs(args, 1 + rank)
+    jobs = make_jobs(args, R.seed(1))
     nt, aa, nt_off, aa_off, nl, al, tab = pack(jobs)
     n = len(jobs)
     cells = int(((nl.astype(np.int64) - 2) * al).sum())
+    cells_all = R.sum(cells)  # units of the whole job (every rank takes this collective)
     opt = Options(flag=NS_F_CIGAR)
     eng = L.Engine(local)
     cap = n * 4096
@@ -283,7 +270,7 @@ def main():
     clk = clocks.stop()
     launches = L.load().pl_kernel_launch_count() - launches0
     t = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
-    value = world * cells * args.steps / t / 1e9
+    value = cells_all * args.steps / t / 1e9
     tm = eng.times()
     plan = eng.last_plan()
     dp_s = tm["dp_ms"] / 1e3
@@ -317,7 +304,7 @@ def main():
         barrier()
         te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
         d2h = n * C.sizeof(SpliceResult) + 4 * sum(h_res[q].n_cigar for q in range(n))
-        e2e = {"value": round(world * cells * args.steps / te / 1e9, 3), "unit": "GCUPS",
+        e2e = {"value": round(cells_all * args.steps / te / 1e9, 3), "unit": "GCUPS",
                "h2d_bytes_per_step": int(nt.nbytes + aa.nbytes + n * C.sizeof(SpliceJob)),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": round(te / args.steps * 1e3, 2),
                "api": "pl_splice_batch_host (C ABI, pinned host buffers)"}
@@ -339,7 +326,11 @@ def main():
             "e2e": e2e,
             "gpu_launches": int(launches),
             "roofline": {"bound": "int", "kernel": "k_splice_dp", "achieved": achieved, "peak": peak,
-                         "unit": "lane-ops/s", "frac": achieved / peak if peak else None, "traffic": None,
+                         "unit": "lane-ops/s", "frac": achieved / peak if peak else None,
+                         "traffic": (int(DP_DRAM_BYTES_PER_CELL * tm["cells"] / tm["dp_launches"])
+                                     if tm["dp_launches"] else None),
+                         "traffic_source": "ncu dram bytes read+write of one k_splice_dp launch on the uniform "
+                                           "2400x2000x350 case (2.08 B/cell), scaled by this run's cells per launch",
                          "ops_per_cell": OPS_PER_CELL, "dp_kernel_gcups": round(dp_gcups, 3),
                          "peak_source": "measured live: pl_measure_int_peak (int32 %.3g, int16x2 %.3g lane-ops/s)"
                                         % (int32_peak, i16x2_peak),
@@ -349,8 +340,7 @@ def main():
         }
         print(json.dumps(line), flush=True)
     eng.close()
-    if world > 1:
-        dist.destroy_process_group()
+    R.close()
     return 0
 
 
@@ -439,29 +429,14 @@ def run_reference_ext(args):
 
 def main_ext(args):
     import torch
-    import torch.distributed as dist
-    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    R = Ranks("nccl")
+    rank, world, local, barrier, max_over_ranks = R.rank, R.world, R.local, R.barrier, R.max
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    reqs = W.ext_requests(args.requests, seed=2 + rank)
+    reqs = W.ext_requests(args.requests, seed=R.seed(2))
     nt, aa, nt_off, aa_off, nl, al, flag, tab = ext_pack(reqs)
     n = len(reqs)
     nominal = int(((nl.astype(np.int64) - 2) * al).sum())
+    nominal_all, n_all = R.sum(nominal), R.sum(n)  # whole job (every rank takes these collectives)
     opt = Options()
     eng = L.Engine(local)
     d_nt = torch.from_numpy(nt.copy()).to("cuda")
@@ -503,7 +478,7 @@ def main_ext(args):
     clk = clocks.stop()
     launches = L.load().pl_kernel_launch_count() - launches0
     t = max_over_ranks(t)
-    value = world * nominal * args.steps / t / 1e9
+    value = nominal_all * args.steps / t / 1e9
     tm = eng.times()
     dp_s = tm["dp_ms"] / 1e3
     achieved = tm["cells"] * EXT_OPS_PER_CELL / dp_s if dp_s > 0 else 0.0
@@ -532,10 +507,10 @@ def main_ext(args):
         torch.cuda.synchronize()
         barrier()
         te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
-        e2e = {"value": round(world * nominal * args.steps / te / 1e9, 3), "unit": "GCUPS",
+        e2e = {"value": round(nominal_all * args.steps / te / 1e9, 3), "unit": "GCUPS",
                "h2d_bytes_per_step": int(nt.nbytes + aa.nbytes + n * C.sizeof(ExtJob)),
                "d2h_bytes_per_step": int(n * C.sizeof(ExtResult)), "ms_per_step": round(te / args.steps * 1e3, 2),
-               "requests_per_s": round(world * n * args.steps / te, 1),
+               "requests_per_s": round(n_all * args.steps / te, 1),
                "api": "pl_ext_batch_host (C ABI, pinned host buffers)"}
 
     cpu = None
@@ -567,8 +542,7 @@ def main_ext(args):
         }
         print(json.dumps(line), flush=True)
     eng.close()
-    if world > 1:
-        dist.destroy_process_group()
+    R.close()
     return 0
 
 
@@ -660,31 +634,15 @@ def run_reference_hmm(args):
 
 def main_hmm(args):
     import torch
-    import torch.distributed as dist
-    from protlocus_b200 import hmm as H
-    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    R = Ranks("nccl")
+    rank, world, local, barrier, max_over_ranks = R.rank, R.world, R.local, R.barrier, R.max
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    texts, profs, batches, desc = hmm_workload(args, 3 + rank)
+    texts, profs, batches, desc = hmm_workload(args, R.seed(3))
     ca = H.codon_alpha()
     eng = L.Engine(local)
     hp = [L.HmmProfile(p["emit"], p["trans"], ca, local) for p in profs]
     cells = sum(int((ln // 3).astype(np.int64).sum()) * p["m"] for p, (_, _, ln) in zip(profs, batches))
+    cells_all = R.sum(cells)  # whole job (every rank takes this collective)
     d_nt = [torch.from_numpy(nt).to("cuda") for nt, _, _ in batches]
     d_sc = [torch.zeros(len(ln), dtype=torch.int32, device="cuda") for _, _, ln in batches]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -718,7 +676,7 @@ def main_hmm(args):
     clk = clocks.stop()
     launches = L.load().pl_kernel_launch_count() - launches0
     t = max_over_ranks(t)
-    value = world * cells * args.steps / t / 1e9
+    value = cells_all * args.steps / t / 1e9
     tm = eng.times()
     dp_s = tm["dp_ms"] / 1e3
     achieved = tm["cells"] * HMM_OPS_PER_CELL / dp_s if dp_s > 0 else 0.0
@@ -747,7 +705,7 @@ def main_hmm(args):
         torch.cuda.synchronize()
         barrier()
         te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
-        e2e = {"value": round(world * cells * args.steps / te / 1e9, 3), "unit": "GCUPS",
+        e2e = {"value": round(cells_all * args.steps / te / 1e9, 3), "unit": "GCUPS",
                "h2d_bytes_per_step": int(sum(nt.nbytes + 8 * len(ln) for nt, _, ln in batches)),
                "d2h_bytes_per_step": int(sum(4 * len(ln) for _, _, ln in batches)),
                "ms_per_step": round(te / args.steps * 1e3, 2), "api": "pl_hmm_score_host (C ABI, pinned host buffers)"}
@@ -784,8 +742,7 @@ def main_hmm(args):
     for p in hp:
         p.close()
     eng.close()
-    if world > 1:
-        dist.destroy_process_group()
+    R.close()
     return 0
 
 
@@ -877,16 +834,12 @@ def run_reference_gapless(args):
 
 def main_gapless(args):
     import torch
-    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    w, mat, codon, desc = gapless_inputs(args, 5 + rank)
+    R = Ranks("nccl")
+    rank, world, local, barrier, max_over_ranks = R.rank, R.world, R.local, R.barrier, R.max
+    w, mat, codon, desc = gapless_inputs(args, R.seed(5))
     n, na = len(w["candidates"]), len(w["anchors"])
     pos = na * 256
+    pos_all, n_all = R.sum(pos), R.sum(n)  # whole job (every rank takes these collectives)
     eng = L.Engine(local)
     d = {k: torch.from_numpy(w[k].view(np.uint8).reshape(-1).copy()).to("cuda")
          for k in ("packed", "queries", "candidates", "anchors")}
@@ -907,6 +860,7 @@ def main_gapless(args):
     clocks = Clocks(local)
     eng.set_timing(True)
     launches0 = L.load().pl_kernel_launch_count()
+    barrier()
     torch.cuda.synchronize()
     clocks.start()
     t = 0.0
@@ -918,12 +872,14 @@ def main_gapless(args):
         e1.record(stream)
         torch.cuda.synchronize()
         t += e0.elapsed_time(e1) / 1e3
+    barrier()
     clk = clocks.stop()
+    t = max_over_ranks(t)
     launches = L.load().pl_kernel_launch_count() - launches0
     tm = eng.times()
     k_s = tm["dp_ms"] / 1e3
     steps_walked = int(eng.lib.pl_gapless_last_steps(eng.h))
-    value = world * pos * args.steps / t / 1e9
+    value = pos_all * args.steps / t / 1e9
     achieved = pos * args.steps * GL_OPS_PER_POS / k_s if k_s > 0 else 0.0
     # end to end through the reference-facing entry point: host buffers, genome resident after the first call
     assert L.gpu_init(local)
@@ -937,10 +893,10 @@ def main_gapless(args):
     for _ in range(args.steps):
         if not L.load().ns_gpu_gapless_score_batch(*e_args, h_sc.ctypes.data):
             raise RuntimeError("ns_gpu_gapless_score_batch failed")
-    te = (time.perf_counter() - t0) / args.steps
+    te = max_over_ranks((time.perf_counter() - t0) / args.steps)
     if (h_sc != ref_sc).any():
         raise RuntimeError("entry points disagree")
-    e2e = {"value": round(world * pos / te / 1e9, 3), "unit": "G seed positions/s",
+    e2e = {"value": round(pos_all / te / 1e9, 3), "unit": "G seed positions/s",
            "h2d_bytes_per_step": int(w["queries"].nbytes + w["candidates"].nbytes + w["anchors"].nbytes + 22 * 22 + 64),
            "d2h_bytes_per_step": int(4 * n), "ms_per_step": round(te * 1e3, 2),
            "api": "ns_gpu_gapless_score_batch (the reference's C entry point; genome resident across calls as in "
@@ -956,7 +912,7 @@ def main_gapless(args):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
                 "data": "synthetic",
                 "config": {"workload": desc, "candidates": n, "anchors": na, "seed_positions_per_step": pos,
-                           "extension_steps_per_step": steps_walked, "candidates_per_s": round(world * n * args.steps / t, 1),
+                           "extension_steps_per_step": steps_walked, "candidates_per_s": round(n_all * args.steps / t, 1),
                            "l2": "a 256 MB buffer is written between timed steps (the 50 MB genome itself fits in L2)",
                            "parallelism": f"{world} independent ranks"},
                 "e2e": e2e, "gpu_launches": int(launches),
@@ -968,6 +924,7 @@ def main_gapless(args):
                 "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line), flush=True)
     eng.close()
+    R.close()
     return 0
 
 

@@ -297,3 +297,50 @@ def gapless_workload(n_genes: int, genome_len: int, n_candidates: int, seed: int
     return {"packed": pack_nt4(genome), "bases": genome_len, "queries": queries.astype(np.uint8),
             "candidates": cand, "anchors": anc[:na].copy(), "block_width": 1 << bbit, "kmer": kmer,
             "contig_offsets": ctg_off, "contig_lengths": ctg_len}
+
+
+def genome_fasta(n_genes: int, seed: int = 5, *, n_contigs: int = 4, contig_len: int = 200_000,
+                 al_min: int = 80, al_max: int = 600, divergence: float = 0.2, n_decoys: int = 4,
+                 max_frameshift: int = 1, gc: float = 0.45,
+                 proteins: list[str] | None = None) -> tuple[str, str]:
+    """A genome and a protein set for running the whole mapping program: n_contigs contigs of
+    contig_len bases at the given GC, with n_genes planted genes (a `divergence`-mutated copy of
+    a random al_min..al_max residue protein, 0..max_frameshift frameshifts and 0-4 GT..AG
+    introns of 60-1500 bp, either strand, one gene per slot so they never overlap), and a
+    protein FASTA with the n_genes source proteins followed by n_decoys unrelated proteins.
+    With `proteins` given, those are planted instead of random ones (n_genes = their number).
+    Returns (genome FASTA text, protein FASTA text)."""
+    rng = np.random.default_rng(seed)
+    if proteins is not None:
+        n_genes = len(proteins)
+    contigs = [list(random_dna(rng, contig_len, gc)) for _ in range(n_contigs)]
+    per = max(1, -(-n_genes // n_contigs))
+    slot = contig_len // per
+    prots = []
+    for g in range(n_genes):
+        prot = proteins[g] if proteins is not None else random_protein(rng, int(rng.integers(al_min, al_max + 1)))
+        introns = [int(round(math.exp(rng.uniform(math.log(60), math.log(1500)))))
+                   for _ in range(int(rng.integers(0, 5)))]
+        gene = build_gene(rng, prot, divergence=divergence, n_frameshift=int(rng.integers(0, max_frameshift + 1)),
+                          intron_lengths=introns)
+        if rng.random() < 0.5:
+            gene = revcomp(gene.encode()).decode()
+        c, s = g % n_contigs, g // n_contigs
+        room = slot - len(gene)
+        if room < 2:
+            continue
+        start = s * slot + int(rng.integers(1, room))
+        contigs[c][start:start + len(gene)] = list(gene)
+        prots.append((f"gene{g}", prot))
+    for d in range(n_decoys):
+        prots.append((f"decoy{d}", random_protein(rng, int(rng.integers(al_min, al_max + 1)))))
+
+    def fasta(records):
+        out = []
+        for name, seq in records:
+            out.append(f">{name}\n")
+            out.extend(seq[i:i + 80] + "\n" for i in range(0, len(seq), 80))
+        return "".join(out)
+
+    genome = fasta([(f"ctg{c}", "".join(contigs[c])) for c in range(n_contigs)])
+    return genome, fasta(prots)

@@ -1,0 +1,108 @@
+"""The reference's whole mapping program, linked against this library, gives the
+same output as its CPU build.
+
+oracle/Makefile's `progs` target builds, from the reference's own sources where
+they lie, the mapping program (main.c and every object of its default build)
+three ways: protlocus_cpu (default build, the GPU entry points are
+nasw-opencl.c's stubs), protlocus_plgpu (nasw-opencl.o, nasw-ext-gpu.o and
+hmm-gpu.o replaced by libplgpu) and protlocus_cuda (the reference's
+`make cuda=1` build, nasw-cuda.cu for sm_100a).
+
+* `--gpu --gpu-min-cells=0` sends every spliced global DP (align.c:74-83,
+  nasw-sse.c:984-986) and every terminal extension (align.c:753) through
+  libplgpu: the PAF (with cs/cg tags) and GFF3 outputs must equal the CPU
+  build's byte for byte, on protein and on HMM-profile queries (the profile
+  path also reaches mp_hmm_dp_score_gpu_batch, hmm.c:324);
+* `--gpu-prefilter` ranks candidates with the gapless X-drop score
+  (map.c:1014-1090); there is no CPU build of it, so the reference's CUDA build
+  is the reference: both programs keep the DP on the CPU and must print the
+  same hits, and libplgpu with `--gpu` on top must print them too.
+
+Inputs: seeded synthetic genomes with planted spliced genes
+(protlocus_b200.workload.genome_fasta).
+"""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from protlocus_b200 import hmm as H
+from protlocus_b200 import workload as W
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.path.join(ROOT, "oracle", "_ref")
+CPU, PLGPU, CUDA = (os.path.join(REF, n) for n in ("protlocus_cpu", "protlocus_plgpu", "protlocus_cuda"))
+need = pytest.mark.skipif(not (os.path.exists(CPU) and os.path.exists(PLGPU)),
+                          reason="oracle/_ref programs not built (needs the reference tree)")
+AA = "ACDEFGHIKLMNPQRSTVWY"
+
+
+def run(binary, args, env=None):
+    p = subprocess.run([binary, "-t8", "--profile", *args], capture_output=True, text=True, timeout=600,
+                       env=dict(os.environ, **(env or {})))
+    assert p.returncode == 0, p.stderr[-3000:]
+    assert "GPU unavailable" not in p.stderr and "ignoring --gpu-prefilter" not in p.stderr, p.stderr[-3000:]
+    prof = dict(re.findall(r"(\w+)=([0-9.]+)", p.stderr.split("[M::profile]")[-1].splitlines()[0]))
+    return p.stdout, prof
+
+
+@pytest.fixture(scope="module")
+def protein_inputs(tmp_path_factory):
+    d = tmp_path_factory.mktemp("prog")
+    g, p = W.genome_fasta(96, seed=21, n_contigs=6, contig_len=400_000, al_min=60, al_max=900,
+                          divergence=0.25, n_decoys=8, max_frameshift=2)
+    (d / "genome.fa").write_text(g)
+    (d / "prot.fa").write_text(p)
+    return str(d / "genome.fa"), str(d / "prot.fa")
+
+
+@pytest.fixture(scope="module")
+def hmm_inputs(tmp_path_factory):
+    d = tmp_path_factory.mktemp("prog_hmm")
+    texts, probs = H.synthetic_profiles(16, seed=22, m_min=80, m_max=400, concentration=1.0)
+    rng = np.random.default_rng(23)
+    prots = ["".join(AA[rng.choice(20, p=row / row.sum())] for row in pm) for pm in probs]
+    g, _ = W.genome_fasta(0, seed=24, n_contigs=4, contig_len=200_000, proteins=prots, divergence=0.08)
+    (d / "genome.fa").write_text(g)
+    (d / "q.hmm").write_text("".join(texts))
+    return str(d / "genome.fa"), str(d / "q.hmm")
+
+
+@need
+@pytest.mark.parametrize("fmt", ["paf", "gff"])
+def test_program_protein_queries_gpu_dp(protein_inputs, fmt):
+    genome, prot = protein_inputs
+    extra = ["--gff"] if fmt == "gff" else []
+    want, _ = run(CPU, [*extra, genome, prot])
+    got, prof = run(PLGPU, ["--gpu", "--gpu-min-cells=0", *extra, genome, prot])
+    assert len(want.splitlines()) >= 80
+    assert int(prof["gpu_dp"]) > 0 and int(prof["gpu_launch"]) > 0, prof
+    assert got == want
+
+
+@need
+def test_program_hmm_queries_gpu_dp(hmm_inputs):
+    genome, q = hmm_inputs
+    want, _ = run(CPU, [genome, q])
+    got, prof = run(PLGPU, ["--gpu", "--gpu-min-cells=0", genome, q], env={"MP_HMM_GPU": "1"})
+    assert len(want.splitlines()) >= 12
+    assert got == want
+
+
+@need
+@pytest.mark.skipif(not os.path.exists(CUDA), reason="oracle/_ref/protlocus_cuda not built")
+@pytest.mark.parametrize("topk", [1, 3])
+def test_program_gpu_prefilter(protein_inputs, topk):
+    genome, prot = protein_inputs
+    args = ["--gpu-prefilter", f"--gpu-prefilter-topk={topk}", "--gpu-prefilter-diversity=0"]
+    want, prof_ref = run(CUDA, [*args, genome, prot])
+    got, prof = run(PLGPU, [*args, genome, prot])
+    assert int(prof["prefilter_candidate"]) > 0
+    assert prof["prefilter_survivor"] == prof_ref["prefilter_survivor"]
+    assert got == want
+    got_dp, _ = run(PLGPU, ["--gpu", "--gpu-min-cells=0", *args, genome, prot])
+    assert got_dp == want
