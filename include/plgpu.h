@@ -393,6 +393,45 @@ int64_t pl_rc_last_cells(const pl_engine_t *e);
  * (nl-2)*al. */
 void pl_ext_last_cells(const pl_engine_t *e, int64_t *cells_run, int64_t *cells_nominal);
 
+/* ---------------------------------------------------------------------------
+ * Learned candidate prefilter (augments the candidate selection of
+ * map.c:1014-1089 / hit.c:217-263; no reference counterpart).  A 4-layer BF16
+ * MLP (in_dim -> hidden x 3 -> 16, ReLU) on the tensor cores predicts from a
+ * candidate's features whether the exact spliced DP over its window will pass
+ * (output column 0, a logit) and where the alignment lies in the window
+ * (columns 1-2, start and end as fractions of the window).  Kept candidates
+ * still get every reported alignment from the exact DP.
+ * ------------------------------------------------------------------------- */
+#define PL_PF_FDIM 576
+typedef struct pl_pf_model_s pl_pf_model_t;
+/* in_dim: a multiple of 64 (PL_PF_FDIM for pl_pf_features_device rows); hidden 128 or 256. */
+pl_pf_model_t *pl_pf_model_create(int32_t device, int32_t in_dim, int32_t hidden, uint64_t seed);
+void pl_pf_model_destroy(pl_pf_model_t *m);
+/* parameters as fp32, layer by layer: W [out x in] row-major then bias [out] */
+int64_t pl_pf_model_size(const pl_pf_model_t *m);
+int pl_pf_model_get(const pl_pf_model_t *m, float *params, int64_t n);
+int pl_pf_model_set(pl_pf_model_t *m, const float *params, int64_t n);
+/* Features of n candidates (nt_off, aa_off, nl, al of each job; ss_off ignored) over
+ * device buffers nt (the window on the strand the DP reads) and aa (ASCII).
+ * feats: bf16 [ceil(n/128)*128 x PL_PF_FDIM] device (pad rows are zeroed);
+ * chain: int32 [n x 4] device, the best anchor chain's first/last window position
+ * and first/last residue (-1 without a chain). */
+int pl_pf_features_device(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n,
+		const uint8_t *nt, const uint8_t *aa, void *feats, int32_t *chain, void *stream);
+/* Scores of n candidates: out f32 [ceil(n/128)*128 x 16] device, from feats as above. */
+int pl_pf_predict(pl_pf_model_t *m, const void *feats, int64_t n, float *out, void *stream);
+/* `steps` Adam steps on minibatches perm[s*batch .. (s+1)*batch) (s counts steps
+ * modulo n_perm / batch) of feats (bf16 rows) and targets (f32 [label, start,
+ * end, box weight] rows), device buffers; batch a multiple of 128.  Loss per step
+ * into loss_log (host, `steps` floats) when not null. */
+int pl_pf_train(pl_pf_model_t *m, const void *feats, const float *targets, const int32_t *perm, int64_t n_perm,
+		int32_t batch, int32_t steps, float lr, float pos_weight, float box_weight, float *loss_log, void *stream);
+/* One tensor-core GEMM C = A . B^T (+ bias, ReLU, mask), bf16 operands with K
+ * contiguous; M % 128 == 0, K % 64 == 0, N and n_tile multiples of 16, n_tile <= 256. */
+int pl_pf_gemm(int32_t device, const void *A, int64_t lda, const void *B, int64_t ldb, int32_t M, int32_t N, int32_t K,
+		int32_t n_tile, const float *bias, int32_t relu, const void *mask, int64_t ldm, void *C, int64_t ldc, void *CT,
+		int64_t ldct, float *Cf, int64_t ldcf, int32_t *err, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

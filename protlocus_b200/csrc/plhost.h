@@ -44,6 +44,8 @@ struct pl_engine_s {
 	/* recheck Forward */
 	dbuf_t r_prof, r_pep, r_dsq, r_order, r_counter, r_scratch, r_bits, r_bias;
 	int64_t r_last_cells;
+	/* learned-prefilter features */
+	dbuf_t pf_cand;
 	/* host planning scratch */
 	plk_job_t *hj;
 	int32_t *horder, *hwave, m_jobs;
@@ -68,6 +70,7 @@ void pl_ext_engine_free(pl_engine_t *e);
 void pl_hmm_engine_free(pl_engine_t *e);
 void pl_gapless_engine_free(pl_engine_t *e);
 void pl_rc_engine_free(pl_engine_t *e);
+void pl_pf_engine_free(pl_engine_t *e);
 int pl_ns_device(void);
 void pl_ns_set_error(const char *msg);
 

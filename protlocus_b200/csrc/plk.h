@@ -147,6 +147,46 @@ int plk_rc_smem_per_warp(int32_t max_m);
 int plk_dp_ctas_per_sm(int32_t mode);
 uint64_t plk_launches(void);
 
+/* BF16 GEMM on the tensor cores (mlp.cu): C = A . B^T + bias, optional ReLU / mask,
+ * outputs bf16 row-major, bf16 transposed and/or f32.  Pointers are device memory. */
+typedef struct {
+	const void *A; int64_t lda;      /* bf16 [M x K] */
+	const void *B; int64_t ldb;      /* bf16 [N x K] */
+	int32_t M, N, K, n_tile;
+	const float *bias;
+	int32_t relu, pad0;
+	const void *mask; int64_t ldm;   /* bf16 [M x N]: output zeroed where mask <= 0 */
+	void *C; int64_t ldc;            /* bf16 [M x N] */
+	void *CT; int64_t ldct;          /* bf16 [N x M] */
+	float *Cf; int64_t ldcf;         /* f32 [M x N] */
+	int32_t *err;
+} plk_gemm_t;
+int plk_gemm_smem(int32_t n_tile);
+int plk_gemm_bf16(const plk_gemm_t *a, void *stream);
+int plk_mlp_gather(const void *F, int32_t fdim, const int32_t *perm, int64_t n_perm, const int32_t *step,
+		int32_t B, const float *tgt, int32_t tdim, void *X, void *XT, float *T, void *stream);
+int plk_mlp_loss(const float *out, int32_t ldo, const float *T, int32_t B, float pos_w, float box_w,
+		void *dout, int32_t ldd, void *doutT, float *loss_sum, void *stream);
+int plk_mlp_colsum(const void *dZT, int32_t B, int32_t N, float *db, void *stream);
+int plk_mlp_adam(float *p, float *m, float *v, const float *grad, int64_t ldg, int32_t rows, int32_t cols,
+		const int32_t *step, float lr, float b1, float b2, float eps, float wd, void *W, int64_t ldw, void *WT,
+		int64_t ldwt, void *stream);
+int plk_mlp_step_inc(int32_t *step, float *loss_sum, float *loss_log, int32_t log_cap, void *stream);
+
+/* learned-prefilter features (pffeat.cu) */
+#define PLK_PF_FDIM 576
+typedef struct { uint8_t nt4[256], aa20[256], codon[64]; } plk_pf_tabs_t;
+typedef struct { int64_t nt_off, aa_off; int32_t nl, al; } plk_pf_cand_t;
+typedef struct {
+	const plk_pf_cand_t *cand;
+	int64_t n;
+	const uint8_t *nt, *aa;
+	plk_pf_tabs_t tabs;
+	void *feats;       /* bf16 [n x PLK_PF_FDIM] */
+	int32_t *chain;    /* [n x 4]: first/last chained window position, first/last chained residue (-1: none) */
+} plk_pf_feat_args_t;
+int plk_pf_features(const plk_pf_feat_args_t *a, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

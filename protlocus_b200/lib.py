@@ -124,6 +124,27 @@ def load() -> C.CDLL:
     lib.pl_rc_score_host.restype = C.c_int
     lib.pl_rc_last_cells.argtypes = [C.c_void_p]
     lib.pl_rc_last_cells.restype = C.c_int64
+    lib.pl_pf_model_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_uint64]
+    lib.pl_pf_model_create.restype = C.c_void_p
+    lib.pl_pf_model_destroy.argtypes = [C.c_void_p]
+    lib.pl_pf_model_size.argtypes = [C.c_void_p]
+    lib.pl_pf_model_size.restype = C.c_int64
+    lib.pl_pf_model_get.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+    lib.pl_pf_model_get.restype = C.c_int
+    lib.pl_pf_model_set.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+    lib.pl_pf_model_set.restype = C.c_int
+    lib.pl_pf_features_device.argtypes = [C.c_void_p, C.POINTER(NsOpt), C.POINTER(SpliceJob), C.c_int32, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.pl_pf_features_device.restype = C.c_int
+    lib.pl_pf_predict.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+    lib.pl_pf_predict.restype = C.c_int
+    lib.pl_pf_train.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32,
+                                C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_void_p]
+    lib.pl_pf_train.restype = C.c_int
+    lib.pl_pf_gemm.argtypes = [C.c_int32, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32, C.c_int32,
+                               C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
+                               C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+    lib.pl_pf_gemm.restype = C.c_int
     _lib = lib
     return lib
 

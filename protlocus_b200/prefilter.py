@@ -1,0 +1,483 @@
+"""Learned candidate prefilter: host side.
+
+A chained candidate is a protein and the genomic window its chain spans, on one
+strand.  The plain path runs the exact spliced DP (pl_splice_batch_device) over
+every candidate window; a candidate "passes" when the DP score is positive (the
+`sc > 0` test of mp_reg_will_output, map.c:459-461).  The learned path computes
+features on the device (pl_pf_features_device), scores them with a 4-layer BF16
+MLP on the tensor cores (pl_pf_predict), drops candidates predicted to fail,
+tightens the windows of the others to the predicted alignment span plus a
+margin, and runs the same exact DP there; a kept candidate whose tightened DP
+does not pass falls back to its full window.  Every reported alignment comes
+from the exact DP; the plain path is the judge of recall.
+
+Training pairs are the plain path's own outcomes: label = pass, and for passing
+candidates the first and last aligned codon of the plain alignment (CIGAR M ops)
+as fractions of the window.
+
+Synthetic candidates (make_candidates) follow the batched configuration: per
+protein (log-normal length, median 350 aa, 50-2500) one window of 1-50 kb holding
+a 25%-divergent copy split by Poisson(4) introns (log-normal, median 150 bp, cap
+20 kb) with 0-2 frameshifts; its candidates are that window on both strands, a
+partial window cutting the gene, and five windows of other proteins' genes on a
+random strand.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+
+import numpy as np
+
+from . import lib as L
+from . import workload as W
+from .abi import NS_F_CIGAR, Options, SpliceJob, SpliceResult
+
+FDIM = 576
+JOB_DTYPE = np.dtype([("nt_off", "<i8"), ("aa_off", "<i8"), ("ss_off", "<i8"), ("nl", "<i4"), ("al", "<i4")])
+KIND_OWN_PLUS, KIND_OWN_MINUS, KIND_PARTIAL, KIND_OTHER = 0, 1, 2, 3
+
+
+def make_candidates(seed: int, n_prot: int = 4096, n_other: int = 5, *, win_min: int = 1000, win_max: int = 50000,
+                    divergence: float = 0.25) -> dict:
+    """Candidates of one synthetic genome seed (3 + n_other per protein)."""
+    rng = np.random.default_rng(seed * 1000003 + 17)
+    nt_parts, aa_parts = [], []
+    off_p = np.zeros(n_prot, np.int64)
+    off_m = np.zeros(n_prot, np.int64)
+    wlen = np.zeros(n_prot, np.int32)
+    gpos = np.zeros((n_prot, 2), np.int64)
+    aoff = np.zeros(n_prot, np.int64)
+    alen = np.zeros(n_prot, np.int32)
+    pn = pa = 0
+    for i in range(n_prot):
+        al = int(np.clip(round(math.exp(rng.normal(math.log(350.0), 0.6))), 50, 2500))
+        prot = W.random_protein(rng, al)
+        k = int(rng.poisson(4.0))
+        introns = [int(min(20000, max(20, round(math.exp(rng.normal(math.log(150.0), 0.8)))))) for _ in range(k)]
+        gene = W.build_gene(rng, prot, divergence=divergence, n_frameshift=int(rng.integers(0, 3)),
+                            intron_lengths=introns)
+        w = max(int(rng.integers(win_min, win_max + 1)), len(gene) + 200)
+        left = int(rng.integers(100, w - len(gene) - 99))
+        win = (W.random_dna(rng, left) + gene + W.random_dna(rng, w - len(gene) - left)).encode()
+        nt_parts += [win, W.revcomp(win)]
+        off_p[i], off_m[i] = pn, pn + w
+        pn += 2 * w
+        wlen[i] = w
+        gpos[i] = (left, left + len(gene))
+        aa_parts.append(prot.encode())
+        aoff[i], alen[i] = pa, al
+        pa += al
+    per = 3 + n_other
+    n = n_prot * per
+    jobs = np.zeros(n, JOB_DTYPE)
+    prot_id = np.repeat(np.arange(n_prot, dtype=np.int32), per)
+    kind = np.tile(np.array([KIND_OWN_PLUS, KIND_OWN_MINUS, KIND_PARTIAL] + [KIND_OTHER] * n_other, np.int8), n_prot)
+    jobs["ss_off"] = -1
+    jobs["aa_off"] = aoff[prot_id]
+    jobs["al"] = alen[prot_id]
+    base = np.arange(n_prot) * per
+    jobs["nt_off"][base], jobs["nl"][base] = off_p, wlen
+    jobs["nt_off"][base + 1], jobs["nl"][base + 1] = off_m, wlen
+    # partial: the window cut inside the gene, keeping the part before or after the cut
+    frac = rng.uniform(0.3, 0.7, n_prot)
+    cut = (gpos[:, 0] + frac * (gpos[:, 1] - gpos[:, 0])).astype(np.int64)
+    keep_left = rng.random(n_prot) < 0.5
+    jobs["nt_off"][base + 2] = np.where(keep_left, off_p, off_p + cut)
+    jobs["nl"][base + 2] = np.where(keep_left, cut, wlen - cut)
+    for t in range(n_other):
+        j = (np.arange(n_prot) + rng.integers(1, n_prot, n_prot)) % n_prot
+        minus = rng.random(n_prot) < 0.5
+        jobs["nt_off"][base + 3 + t] = np.where(minus, off_m[j], off_p[j])
+        jobs["nl"][base + 3 + t] = wlen[j]
+    return {"nt": np.frombuffer(b"".join(nt_parts), np.uint8), "aa": np.frombuffer(b"".join(aa_parts), np.uint8),
+            "jobs": jobs, "prot": prot_id, "kind": kind, "seed": seed}
+
+
+def job_ptr(jobs: np.ndarray):
+    return C.cast(jobs.ctypes.data, C.POINTER(SpliceJob))
+
+
+def cigar_bounds(cig: np.ndarray, res, min_run: int = 10) -> tuple[np.ndarray, np.ndarray]:
+    """First nucleotide of the first and end of the last run of >= min_run codon
+    matches (M) in each job's CIGAR (words as ns_push_cigar writes them; -1 without
+    one).  A global alignment over a wide window typically opens with a few residues
+    at the window start and a long intron, and closes the same way; the runs skip
+    those."""
+    n = len(res)
+    offs = np.array([r.cigar_off for r in res], np.int64)
+    cnt = np.array([r.n_cigar for r in res], np.int64)
+    start = np.full(n, -1, np.int64)
+    end = np.full(n, -1, np.int64)
+    if n == 0 or cnt.sum() == 0:
+        return start, end
+    idx = np.concatenate([np.arange(o, o + c) for o, c in zip(offs, cnt)])
+    w = cig[idx].astype(np.int64)
+    op, ln = w & 15, w >> 4
+    ntc = np.where((op == 0) | (op == 2), 3 * ln, np.where(op == 1, 0, ln))
+    cum = np.cumsum(ntc)
+    seg = np.repeat(np.arange(n), cnt)
+    first = np.concatenate([[0], np.cumsum(cnt)[:-1]])
+    base = cum[first] - ntc[first]
+    pos = np.arange(len(w))
+    isM = (op == 0) & (ln >= min_run)
+    big = len(w) + 1
+    fm = np.full(n, big)
+    lm = np.full(n, -1)
+    np.minimum.at(fm, seg[isM], pos[isM])
+    np.maximum.at(lm, seg[isM], pos[isM])
+    has = lm >= 0
+    start[has] = cum[fm[has]] - ntc[fm[has]] - base[has]
+    end[has] = cum[lm[has]] - base[has]
+    return start, end
+
+
+class PrefilterModel:
+    """The MLP on the device (pl_pf_model_*)."""
+
+    def __init__(self, device: int = 0, hidden: int = 256, seed: int = 1, params: np.ndarray | None = None):
+        self.lib = L.load()
+        self.device, self.hidden = device, hidden
+        self.h = self.lib.pl_pf_model_create(device, FDIM, hidden, seed)
+        if not self.h:
+            raise RuntimeError("pl_pf_model_create: " + L.error())
+        if params is not None:
+            self.set_params(params)
+
+    def size(self) -> int:
+        return int(self.lib.pl_pf_model_size(self.h))
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.size(), np.float32)
+        if not self.lib.pl_pf_model_get(self.h, p.ctypes.data, p.size):
+            raise RuntimeError(L.error())
+        return p
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        if not self.lib.pl_pf_model_set(self.h, p.ctypes.data, p.size):
+            raise RuntimeError(L.error())
+
+    def train(self, feats, targets, perm, batch: int, steps: int, lr: float, pos_w: float, box_w: float) -> np.ndarray:
+        log = np.zeros(max(steps, 1), np.float32)
+        if not self.lib.pl_pf_train(self.h, feats.data_ptr(), targets.data_ptr(), perm.data_ptr(), perm.numel(), batch,
+                                    steps, lr, pos_w, box_w, log.ctypes.data, None):
+            raise RuntimeError("pl_pf_train: " + L.error())
+        return log[:steps]
+
+    def predict(self, feats, n: int, out=None):
+        import torch
+        npad = (n + 127) // 128 * 128
+        if out is None:
+            out = torch.zeros(npad, 16, dtype=torch.float32, device=f"cuda:{self.device}")
+        stream = torch.cuda.current_stream().cuda_stream
+        if not self.lib.pl_pf_predict(self.h, feats.data_ptr(), n, out.data_ptr(), stream):
+            raise RuntimeError("pl_pf_predict: " + L.error())
+        return out
+
+    def close(self):
+        if self.h:
+            self.lib.pl_pf_model_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Pipeline:
+    """Device-resident candidate set with the plain and learned paths over it."""
+
+    def __init__(self, eng: L.Engine, cand: dict):
+        import torch
+        self.eng, self.cand = eng, cand
+        self.opt = Options(flag=NS_F_CIGAR)
+        dev = f"cuda:{eng.device}" if hasattr(eng, "device") else "cuda"
+        self.dev = dev
+        self.d_nt = torch.from_numpy(cand["nt"].copy()).to(dev)
+        self.d_aa = torch.from_numpy(cand["aa"].copy()).to(dev)
+        self.n = len(cand["jobs"])
+
+    def features(self):
+        import torch
+        npad = (self.n + 127) // 128 * 128
+        feats = torch.empty(npad, FDIM, dtype=torch.bfloat16, device=self.dev)
+        chain = torch.empty(max(self.n, 1), 4, dtype=torch.int32, device=self.dev)
+        stream = torch.cuda.current_stream().cuda_stream
+        if not self.eng.lib.pl_pf_features_device(self.eng.h, self.opt.ptr, job_ptr(self.cand["jobs"]), self.n,
+                                                  self.d_nt.data_ptr(), self.d_aa.data_ptr(), feats.data_ptr(),
+                                                  chain.data_ptr(), stream):
+            raise RuntimeError("pl_pf_features_device: " + L.error())
+        return feats, chain
+
+    def dp(self, jobs: np.ndarray, bounds: bool = False):
+        """Exact spliced DP with CIGAR over `jobs` (device-resident sequences): scores, and
+        the aligned span (first/last codon match) when bounds."""
+        import torch
+        n = len(jobs)
+        if n == 0:
+            z = np.zeros(0, np.int64)
+            return np.zeros(0, np.int32), z, z
+        cap = int(jobs["al"].astype(np.int64).sum() * 4 + 256 * n)
+        d_res = torch.zeros(n * C.sizeof(SpliceResult), dtype=torch.uint8, device=self.dev)
+        d_cig = torch.zeros(cap, dtype=torch.int32, device=self.dev)
+        total = C.c_int64()
+        stream = torch.cuda.current_stream().cuda_stream
+        if not self.eng.lib.pl_splice_batch_device(self.eng.h, self.opt.ptr, job_ptr(jobs), n, self.d_nt.data_ptr(),
+                                                   self.d_aa.data_ptr(), None, d_res.data_ptr(), d_cig.data_ptr(),
+                                                   cap, C.byref(total), stream):
+            raise RuntimeError("pl_splice_batch_device: " + L.error())
+        res = (SpliceResult * n).from_buffer_copy(d_res.cpu().numpy().tobytes())
+        score = np.array([r.score for r in res], np.int32)
+        if not bounds:
+            return score, None, None
+        cig = d_cig[: int(total.value)].cpu().numpy()
+        s, e = cigar_bounds(cig, res)
+        return score, s, e
+
+    def targets(self, score, s, e):
+        """[label, start fraction, end fraction, box weight] rows for training."""
+        nl = self.cand["jobs"]["nl"].astype(np.float64)
+        y = (score > 0).astype(np.float32)
+        T = np.zeros((self.n, 4), np.float32)
+        T[:, 0] = y
+        T[:, 1] = np.where(y > 0, s / nl, 0.0)
+        T[:, 2] = np.where(y > 0, e / nl, 0.0)
+        T[:, 3] = y
+        return T
+
+    def tightened(self, keep: np.ndarray, out: np.ndarray, margin: int, rel: float) -> np.ndarray:
+        """Jobs of the kept candidates with windows cut to the predicted span plus
+        margin + rel * span on both sides (at least 3 nt, within the window)."""
+        jobs = self.cand["jobs"][keep].copy()
+        nl = jobs["nl"].astype(np.int64)
+        ps = np.clip(out[keep, 1], 0.0, 1.0) * nl
+        pe = np.clip(out[keep, 2], 0.0, 1.0) * nl
+        lo, hi = np.minimum(ps, pe), np.maximum(ps, pe)
+        pad = margin + rel * (hi - lo)
+        s = np.clip(np.floor(lo - pad), 0, nl).astype(np.int64)
+        e = np.clip(np.ceil(hi + pad), 0, nl).astype(np.int64)
+        short = e - s < 3
+        s[short], e[short] = 0, nl[short]
+        jobs["nt_off"] += s
+        jobs["nl"] = (e - s).astype(np.int32)
+        return jobs
+
+    def learned(self, model: PrefilterModel, tau: float, margin: int, rel: float, feats=None):
+        """The learned path: (pass mask over all candidates, stats)."""
+        import torch
+        t0 = time.perf_counter()
+        if feats is None:
+            feats, _ = self.features()
+        out = model.predict(feats, self.n)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        o = out[: self.n, :3].cpu().numpy()
+        logit_tau = math.log(tau / (1.0 - tau))
+        keep = np.nonzero(o[:, 0] >= logit_tau)[0]
+        jobs = self.tightened(keep, o, margin, rel)
+        sc, _, _ = self.dp(jobs)
+        t2 = time.perf_counter()
+        fail = keep[sc <= 0]
+        sc2, _, _ = self.dp(self.cand["jobs"][fail])
+        torch.cuda.synchronize()
+        t3 = time.perf_counter()
+        passed = np.zeros(self.n, bool)
+        passed[keep[sc > 0]] = True
+        passed[fail[sc2 > 0]] = True
+        cells_tight = int(((jobs["nl"].astype(np.int64) - 2) * jobs["al"]).sum())
+        stats = {"kept": int(len(keep)), "fallback": int(len(fail)), "cells_tight": cells_tight,
+                 "s_score": t1 - t0, "s_dp": t2 - t1, "s_fallback": t3 - t2, "s_total": t3 - t0}
+        return passed, stats
+
+
+def _gen(args):
+    seed, n_prot = args
+    return make_candidates(seed, n_prot)
+
+
+def candidate_stream(seeds, n_prot: int, workers: int = 8):
+    """make_candidates over seeds, generated ahead in spawned worker processes."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    if workers <= 1:
+        for sd in seeds:
+            yield make_candidates(sd, n_prot)
+        return
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        yield from ex.map(_gen, [(sd, n_prot) for sd in seeds])
+
+
+def build_set(eng: L.Engine, seeds, n_prot: int, workers: int = 8, log=None):
+    """Training/validation rows of the given seeds: bf16 features [N x FDIM] and f32
+    targets [N x 4] on the device (N = candidates of all seeds), plus host-side
+    labels, kinds and plain-path DP time."""
+    import torch
+    feats, targets, labels, kinds, dp_s = [], [], [], [], 0.0
+    for cand in candidate_stream(seeds, n_prot, workers):
+        pipe = Pipeline(eng, cand)
+        f, _ = pipe.features()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sc, s, e = pipe.dp(cand["jobs"], bounds=True)
+        dp_s += time.perf_counter() - t0
+        T = pipe.targets(sc, s, e)
+        feats.append(f[: pipe.n])
+        targets.append(torch.from_numpy(T).to(pipe.dev))
+        labels.append(T[:, 0] > 0.5)
+        kinds.append(cand["kind"])
+        if log:
+            log(f"seed {cand['seed']}: {pipe.n} candidates, {int(T[:, 0].sum())} pass, DP {time.perf_counter() - t0:.2f} s")
+        del pipe
+    n = sum(int(x.shape[0]) for x in feats)
+    npad = (n + 127) // 128 * 128
+    F = torch.zeros(npad, FDIM, dtype=torch.bfloat16, device=feats[0].device)
+    r = 0
+    for x in feats:
+        F[r: r + x.shape[0]] = x
+        r += x.shape[0]
+    return {"feats": F, "targets": torch.cat(targets), "n": n, "labels": np.concatenate(labels),
+            "kinds": np.concatenate(kinds), "dp_s": dp_s}
+
+
+def train(model: PrefilterModel, data: dict, epochs: int = 8, batch: int = 4096, lr: float = 1e-3,
+          pos_w: float = 4.0, box_w: float = 2.0, seed: int = 7) -> np.ndarray:
+    """Adam over `epochs` shuffled passes of the rows (one captured CUDA graph per step)."""
+    import torch
+    n = data["n"]
+    rng = np.random.default_rng(seed)
+    steps_per = n // batch
+    perm = np.concatenate([rng.permutation(n)[: steps_per * batch] for _ in range(epochs)]).astype(np.int32)
+    d_perm = torch.from_numpy(perm).to(data["feats"].device)
+    return model.train(data["feats"], data["targets"], d_perm, batch, steps_per * epochs, lr, pos_w, box_w)
+
+
+def calibrate(model: PrefilterModel, pipe: Pipeline, labels: np.ndarray, recall: float = 0.999,
+              margins=(0, 100, 200, 400, 800, 1600), rel: float = 0.1):
+    """Threshold tau keeping `recall` of the passing candidates of a validation set, and
+    the smallest margin whose tightened windows still pass for all kept passers but
+    a 1e-3 fraction (those fall back to their full windows)."""
+    import torch
+    feats, _ = pipe.features()
+    out = model.predict(feats, pipe.n)
+    torch.cuda.synchronize()
+    o = out[: pipe.n, :3].cpu().numpy()
+    z = o[labels, 0]
+    k = int(math.floor((1.0 - recall) * len(z)))
+    zt = float(np.sort(z)[k]) if len(z) else 0.0
+    tau = 1.0 / (1.0 + math.exp(-zt))
+    keep = np.nonzero(o[:, 0] >= zt)[0]
+    pos_keep = keep[labels[keep]]
+    chosen = margins[-1]
+    for m in margins:
+        jobs = pipe.tightened(pos_keep, o, m, rel)
+        sc, _, _ = pipe.dp(jobs)
+        if (sc <= 0).mean() <= 1e-3:
+            chosen = m
+            break
+    return tau, chosen, {"kept": int(len(keep)), "kept_pass": int(len(pos_keep)), "n": pipe.n}
+
+
+def save(path: str, model: PrefilterModel, **meta):
+    np.savez(path, params=model.params(), hidden=model.hidden, **meta)
+
+
+def load_model(path: str, device: int = 0):
+    z = np.load(path, allow_pickle=False)
+    model = PrefilterModel(device, hidden=int(z["hidden"]), params=z["params"])
+    meta = {k: z[k] for k in z.files if k not in ("params", "hidden")}
+    return model, meta
+
+
+def evaluate(eng: L.Engine, model: PrefilterModel, cand: dict, tau: float, margin: int, rel: float,
+             repeats: int = 3) -> dict:
+    """Plain path vs learned path on one candidate set, inputs resident on the device:
+    candidates per second of each (best of `repeats` after a warm-up) and the learned
+    path's recall of the plain path's passing candidates."""
+    import torch
+    pipe = Pipeline(eng, cand)
+    plain, _, _ = pipe.dp(cand["jobs"])  # warm-up
+    t_plain = []
+    for _ in range(repeats):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        plain, _, _ = pipe.dp(cand["jobs"])
+        torch.cuda.synchronize()
+        t_plain.append(time.perf_counter() - t0)
+    pipe.learned(model, tau, margin, rel)  # warm-up
+    runs = []
+    for _ in range(repeats):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        passed, st = pipe.learned(model, tau, margin, rel)
+        torch.cuda.synchronize()
+        st["wall"] = time.perf_counter() - t0
+        runs.append((passed, st))
+    passed, st = min(runs, key=lambda r: r[1]["wall"])
+    pos = plain > 0
+    jobs = cand["jobs"]
+    cells_plain = int(((jobs["nl"].astype(np.int64) - 2) * jobs["al"]).sum())
+    return {"n": pipe.n, "plain_pass": int(pos.sum()), "recall": float(passed[pos].mean()) if pos.any() else 1.0,
+            "extra_pass": int((passed & ~pos).sum()), "plain_s": min(t_plain), "learned_s": st["wall"],
+            "plain_loci_per_s": pipe.n / min(t_plain), "learned_loci_per_s": pipe.n / st["wall"],
+            "speedup": min(t_plain) / st["wall"], "cells_plain": cells_plain, **st}
+
+
+def main(argv=None):
+    import argparse
+    import json
+    import sys
+    ap = argparse.ArgumentParser(description="train / evaluate the learned candidate prefilter")
+    ap.add_argument("cmd", choices=["train", "eval"])
+    ap.add_argument("--train-seeds", default="1-63")
+    ap.add_argument("--val-seed", type=int, default=64)
+    ap.add_argument("--eval-seed", type=int, default=65)
+    ap.add_argument("--n-prot", type=int, default=4096)
+    ap.add_argument("--epochs", type=int, default=8)
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--recall", type=float, default=0.999, help="validation recall the threshold keeps")
+    ap.add_argument("--rel", type=float, default=0.1)
+    ap.add_argument("--workers", type=int, default=8)
+    ap.add_argument("--model", default=None, help="weights (.npz): written by train, read by eval")
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    log = (lambda s: print(s, file=sys.stderr, flush=True))
+    eng = L.Engine(a.device)
+    if a.cmd == "train":
+        lo, hi = (int(x) for x in a.train_seeds.split("-"))
+        t0 = time.perf_counter()
+        data = build_set(eng, range(lo, hi + 1), a.n_prot, a.workers, log)
+        t1 = time.perf_counter()
+        model = PrefilterModel(a.device, seed=1)
+        losses = train(model, data, a.epochs, a.batch, a.lr)
+        t2 = time.perf_counter()
+        log(f"{data['n']} rows ({int(data['labels'].sum())} pass) built in {t1 - t0:.1f} s; "
+            f"{len(losses)} steps in {t2 - t1:.2f} s; loss {losses[:50].mean():.4f} -> {losses[-50:].mean():.4f}")
+        del data
+        cand = make_candidates(a.val_seed, a.n_prot)
+        pipe = Pipeline(eng, cand)
+        plain, _, _ = pipe.dp(cand["jobs"])
+        tau, margin, info = calibrate(model, pipe, plain > 0, a.recall, rel=a.rel)
+        log(f"calibrated on seed {a.val_seed}: tau {tau:.3g}, margin {margin}, {info}")
+        out = a.model or "prefilter.npz"
+        save(out, model, tau=tau, margin=margin, rel=a.rel, train_seeds=a.train_seeds, n_prot=a.n_prot,
+             epochs=a.epochs, loss_first=float(losses[:50].mean()), loss_last=float(losses[-50:].mean()),
+             train_rows=len(losses) * a.batch // a.epochs, train_s=t2 - t1)
+        print(json.dumps({"model": out, "tau": tau, "margin": margin, "train_steps": len(losses),
+                          "train_s": round(t2 - t1, 3), "loss_first": float(losses[:50].mean()),
+                          "loss_last": float(losses[-50:].mean())}))
+    else:
+        model, meta = load_model(a.model, a.device)
+        cand = make_candidates(a.eval_seed, a.n_prot)
+        r = evaluate(eng, model, cand, float(meta["tau"]), int(meta["margin"]), float(meta["rel"]))
+        print(json.dumps(r))
+    eng.close()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
