@@ -249,14 +249,23 @@ class Pipeline:
         T[:, 3] = y
         return T
 
-    def tightened(self, keep: np.ndarray, out: np.ndarray, margin: int, rel: float) -> np.ndarray:
-        """Jobs of the kept candidates with windows cut to the predicted span plus
+    def tightened(self, keep: np.ndarray, out: np.ndarray, chain: np.ndarray | None, margin: int,
+                  rel: float = 0.0) -> np.ndarray:
+        """Jobs of the kept candidates with windows cut to the union of the predicted
+        alignment span and the span the best anchor chain implies (its first anchor
+        minus 3x the residues before it, its last plus 3x the residues after it), plus
         margin + rel * span on both sides (at least 3 nt, within the window)."""
         jobs = self.cand["jobs"][keep].copy()
         nl = jobs["nl"].astype(np.int64)
+        al = jobs["al"].astype(np.int64)
         ps = np.clip(out[keep, 1], 0.0, 1.0) * nl
         pe = np.clip(out[keep, 2], 0.0, 1.0) * nl
         lo, hi = np.minimum(ps, pe), np.maximum(ps, pe)
+        if chain is not None:
+            c = chain[keep].astype(np.int64)
+            has = c[:, 0] >= 0
+            lo = np.where(has, np.minimum(lo, c[:, 0] - 3 * c[:, 2] - 2), lo)
+            hi = np.where(has, np.maximum(hi, c[:, 1] + 3 * (al - 1 - c[:, 3]) + 1), hi)
         pad = margin + rel * (hi - lo)
         s = np.clip(np.floor(lo - pad), 0, nl).astype(np.int64)
         e = np.clip(np.ceil(hi + pad), 0, nl).astype(np.int64)
@@ -266,22 +275,24 @@ class Pipeline:
         jobs["nl"] = (e - s).astype(np.int32)
         return jobs
 
-    def learned(self, model: PrefilterModel, tau: float, margin: int, rel: float, feats=None):
-        """The learned path: (pass mask over all candidates, stats)."""
+    def learned(self, model: PrefilterModel, tau: float, margin: int, rel: float = 0.0, tau_fb: float = 0.0):
+        """The learned path: (pass mask over all candidates, stats).  Candidates with
+        p >= tau run the exact DP on their tightened windows; those that do not pass
+        there and have p >= tau_fb run it again on the full window."""
         import torch
         t0 = time.perf_counter()
-        if feats is None:
-            feats, _ = self.features()
+        feats, chain = self.features()
         out = model.predict(feats, self.n)
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
         o = out[: self.n, :3].cpu().numpy()
-        logit_tau = math.log(tau / (1.0 - tau))
-        keep = np.nonzero(o[:, 0] >= logit_tau)[0]
-        jobs = self.tightened(keep, o, margin, rel)
+        ch = chain[: self.n].cpu().numpy()
+        t1 = time.perf_counter()
+        z = o[:, 0]
+        keep = np.nonzero(z >= _logit(tau))[0]
+        jobs = self.tightened(keep, o, ch, margin, rel)
         sc, _, _ = self.dp(jobs)
         t2 = time.perf_counter()
         fail = keep[sc <= 0]
+        fail = fail[z[fail] >= _logit(tau_fb)]
         sc2, _, _ = self.dp(self.cand["jobs"][fail])
         torch.cuda.synchronize()
         t3 = time.perf_counter()
@@ -292,6 +303,14 @@ class Pipeline:
         stats = {"kept": int(len(keep)), "fallback": int(len(fail)), "cells_tight": cells_tight,
                  "s_score": t1 - t0, "s_dp": t2 - t1, "s_fallback": t3 - t2, "s_total": t3 - t0}
         return passed, stats
+
+
+def _logit(p: float) -> float:
+    if p <= 0.0:
+        return -math.inf
+    if p >= 1.0:
+        return math.inf
+    return math.log(p / (1.0 - p))
 
 
 def _gen(args):
@@ -355,30 +374,45 @@ def train(model: PrefilterModel, data: dict, epochs: int = 8, batch: int = 4096,
     return model.train(data["feats"], data["targets"], d_perm, batch, steps_per * epochs, lr, pos_w, box_w)
 
 
-def calibrate(model: PrefilterModel, pipe: Pipeline, labels: np.ndarray, recall: float = 0.999,
-              margins=(0, 100, 200, 400, 800, 1600), rel: float = 0.1):
-    """Threshold tau keeping `recall` of the passing candidates of a validation set, and
-    the smallest margin whose tightened windows still pass for all kept passers but
-    a 1e-3 fraction (those fall back to their full windows)."""
+def calibrate(model: PrefilterModel, pipe: Pipeline, labels: np.ndarray, recall: float = 0.998,
+              cls_recall: float = 0.999, margins=(0, 100, 200, 400, 800), max_tight_fail: float = 0.003):
+    """Decision parameters from a validation set: tau keeps cls_recall of the passing
+    candidates; margin is the smallest whose tightened windows fail for at most
+    max_tight_fail of the kept passers; tau_fb is the highest fallback threshold that
+    still leaves the path's recall of the passers at `recall`."""
     import torch
-    feats, _ = pipe.features()
+    feats, chain = pipe.features()
     out = model.predict(feats, pipe.n)
     torch.cuda.synchronize()
     o = out[: pipe.n, :3].cpu().numpy()
-    z = o[labels, 0]
-    k = int(math.floor((1.0 - recall) * len(z)))
-    zt = float(np.sort(z)[k]) if len(z) else 0.0
-    tau = 1.0 / (1.0 + math.exp(-zt))
-    keep = np.nonzero(o[:, 0] >= zt)[0]
-    pos_keep = keep[labels[keep]]
-    chosen = margins[-1]
+    ch = chain[: pipe.n].cpu().numpy()
+    z = o[:, 0]
+    zp = np.sort(z[labels])
+    k = int(math.floor((1.0 - cls_recall) * len(zp)))
+    zt = float(zp[k]) if len(zp) else 0.0
+    keep = np.nonzero(z >= zt)[0]
+    chosen, sc = margins[-1], None
     for m in margins:
-        jobs = pipe.tightened(pos_keep, o, m, rel)
-        sc, _, _ = pipe.dp(jobs)
-        if (sc <= 0).mean() <= 1e-3:
+        sc, _, _ = pipe.dp(pipe.tightened(keep, o, ch, m))
+        kp = labels[keep]
+        if kp.sum() == 0 or ((sc <= 0) & kp).sum() <= max_tight_fail * kp.sum():
             chosen = m
             break
-    return tau, chosen, {"kept": int(len(keep)), "kept_pass": int(len(pos_keep)), "n": pipe.n}
+    fail = keep[sc <= 0]
+    missed_cls = int(labels.sum()) - int(labels[keep].sum())
+    allowed = int(math.floor((1.0 - recall) * labels.sum())) - missed_cls
+    zf = np.sort(z[fail[labels[fail]]])  # passers the tightened windows lose
+    if allowed < 0 or len(zf) == 0:
+        z_fb = zt if len(zf) else math.inf
+    elif allowed >= len(zf):
+        z_fb = math.inf
+    else:
+        z_fb = float(zf[allowed])
+    tau = 1.0 / (1.0 + math.exp(-zt))
+    tau_fb = 1.0 if z_fb == math.inf else 1.0 / (1.0 + math.exp(-z_fb))
+    info = {"kept": int(len(keep)), "kept_pass": int(labels[keep].sum()), "n": pipe.n, "tight_fail": int(len(fail)),
+            "tight_fail_pass": int(len(zf)), "fallback": int((z[fail] >= z_fb).sum())}
+    return tau, chosen, tau_fb, info
 
 
 def save(path: str, model: PrefilterModel, **meta):
@@ -392,7 +426,7 @@ def load_model(path: str, device: int = 0):
     return model, meta
 
 
-def evaluate(eng: L.Engine, model: PrefilterModel, cand: dict, tau: float, margin: int, rel: float,
+def evaluate(eng: L.Engine, model: PrefilterModel, cand: dict, tau: float, margin: int, tau_fb: float,
              repeats: int = 3) -> dict:
     """Plain path vs learned path on one candidate set, inputs resident on the device:
     candidates per second of each (best of `repeats` after a warm-up) and the learned
@@ -407,12 +441,12 @@ def evaluate(eng: L.Engine, model: PrefilterModel, cand: dict, tau: float, margi
         plain, _, _ = pipe.dp(cand["jobs"])
         torch.cuda.synchronize()
         t_plain.append(time.perf_counter() - t0)
-    pipe.learned(model, tau, margin, rel)  # warm-up
+    pipe.learned(model, tau, margin, 0.0, tau_fb)  # warm-up
     runs = []
     for _ in range(repeats):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        passed, st = pipe.learned(model, tau, margin, rel)
+        passed, st = pipe.learned(model, tau, margin, 0.0, tau_fb)
         torch.cuda.synchronize()
         st["wall"] = time.perf_counter() - t0
         runs.append((passed, st))
@@ -431,7 +465,7 @@ def main(argv=None):
     import json
     import sys
     ap = argparse.ArgumentParser(description="train / evaluate the learned candidate prefilter")
-    ap.add_argument("cmd", choices=["train", "eval"])
+    ap.add_argument("cmd", choices=["train", "calibrate", "eval"])
     ap.add_argument("--train-seeds", default="1-63")
     ap.add_argument("--val-seed", type=int, default=64)
     ap.add_argument("--eval-seed", type=int, default=65)
@@ -439,14 +473,14 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=8)
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--recall", type=float, default=0.999, help="validation recall the threshold keeps")
-    ap.add_argument("--rel", type=float, default=0.1)
+    ap.add_argument("--recall", type=float, default=0.998, help="validation recall of the whole learned path")
     ap.add_argument("--workers", type=int, default=8)
-    ap.add_argument("--model", default=None, help="weights (.npz): written by train, read by eval")
+    ap.add_argument("--model", default=None, help="weights (.npz): written by train/calibrate, read by eval")
     ap.add_argument("--device", type=int, default=0)
     a = ap.parse_args(argv)
     log = (lambda s: print(s, file=sys.stderr, flush=True))
     eng = L.Engine(a.device)
+    out = a.model or "prefilter.npz"
     if a.cmd == "train":
         lo, hi = (int(x) for x in a.train_seeds.split("-"))
         t0 = time.perf_counter()
@@ -457,23 +491,25 @@ def main(argv=None):
         t2 = time.perf_counter()
         log(f"{data['n']} rows ({int(data['labels'].sum())} pass) built in {t1 - t0:.1f} s; "
             f"{len(losses)} steps in {t2 - t1:.2f} s; loss {losses[:50].mean():.4f} -> {losses[-50:].mean():.4f}")
+        meta = {"train_seeds": a.train_seeds, "n_prot": a.n_prot, "epochs": a.epochs, "train_rows": data["n"],
+                "train_pass": int(data["labels"].sum()), "train_steps": len(losses), "train_s": t2 - t1,
+                "loss_first": float(losses[:50].mean()), "loss_last": float(losses[-50:].mean())}
         del data
+    else:
+        model, meta = load_model(out if a.cmd == "calibrate" else a.model, a.device)
+        meta = {k: v.item() if hasattr(v, "item") else v for k, v in meta.items()}
+    if a.cmd in ("train", "calibrate"):
         cand = make_candidates(a.val_seed, a.n_prot)
         pipe = Pipeline(eng, cand)
         plain, _, _ = pipe.dp(cand["jobs"])
-        tau, margin, info = calibrate(model, pipe, plain > 0, a.recall, rel=a.rel)
-        log(f"calibrated on seed {a.val_seed}: tau {tau:.3g}, margin {margin}, {info}")
-        out = a.model or "prefilter.npz"
-        save(out, model, tau=tau, margin=margin, rel=a.rel, train_seeds=a.train_seeds, n_prot=a.n_prot,
-             epochs=a.epochs, loss_first=float(losses[:50].mean()), loss_last=float(losses[-50:].mean()),
-             train_rows=len(losses) * a.batch // a.epochs, train_s=t2 - t1)
-        print(json.dumps({"model": out, "tau": tau, "margin": margin, "train_steps": len(losses),
-                          "train_s": round(t2 - t1, 3), "loss_first": float(losses[:50].mean()),
-                          "loss_last": float(losses[-50:].mean())}))
+        tau, margin, tau_fb, info = calibrate(model, pipe, plain > 0, a.recall)
+        log(f"calibrated on seed {a.val_seed}: tau {tau:.4g}, margin {margin}, tau_fb {tau_fb:.4g}, {info}")
+        meta.update(tau=tau, margin=margin, tau_fb=tau_fb, val_seed=a.val_seed, val_recall=a.recall)
+        save(out, model, **meta)
+        print(json.dumps({"model": out, **{k: (v if not isinstance(v, np.generic) else v.item()) for k, v in meta.items()}}))
     else:
-        model, meta = load_model(a.model, a.device)
         cand = make_candidates(a.eval_seed, a.n_prot)
-        r = evaluate(eng, model, cand, float(meta["tau"]), int(meta["margin"]), float(meta["rel"]))
+        r = evaluate(eng, model, cand, float(meta["tau"]), int(meta["margin"]), float(meta["tau_fb"]))
         print(json.dumps(r))
     eng.close()
     return 0
