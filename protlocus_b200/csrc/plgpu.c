@@ -194,6 +194,26 @@ int pl_max_sub(const ns_opt_t *opt)
 	return m;
 }
 
+/* A job runs on a whole CTA (a 2048-row cooperative wavefront) when it holds more
+ * than this multiple of a warp's share of its wave's cells: fewer, longer jobs then
+ * finish with the rest instead of trailing them.  PLGPU_COOP_RATIO overrides it
+ * (the tuning sweep of the batched workload). */
+static double g_coop_ratio = 0.7;
+static pthread_once_t g_coop_once = PTHREAD_ONCE_INIT;
+static void pl_coop_ratio_init(void)
+{
+	const char *v = getenv("PLGPU_COOP_RATIO");
+	if (v && *v) {
+		const double x = atof(v);
+		if (x > 0.0) g_coop_ratio = x;
+	}
+}
+double pl_coop_ratio(void)
+{
+	pthread_once(&g_coop_once, pl_coop_ratio_init);
+	return g_coop_ratio;
+}
+
 typedef struct { int64_t cells; int32_t idx; } pl_key_t;
 static int pl_cmp_cells_desc(const void *a, const void *b)
 {
@@ -296,7 +316,8 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 		const int32_t j = sorted[q];
 		plk_job_t *J = &e->hj[j];
 		const int64_t cells = (int64_t)(J->nl - 2) * J->al, share = wave_cells[e->hwave[j]] / slots;
-		if (J->al >= 200 && J->nl - 2 >= 32 * PLK_WARPS_PER_CTA * PLK_ROWS && cells * 10 > share * 7) J->nw = PLK_WARPS_PER_CTA;
+		if (J->al >= 200 && J->nl - 2 >= 32 * PLK_WARPS_PER_CTA * PLK_ROWS && (double)cells > share * pl_coop_ratio())
+			J->nw = PLK_WARPS_PER_CTA;
 		J->trace_off = wave_bytes[e->hwave[j]] / 2;
 		wave_bytes[e->hwave[j]] += (plk_trace_words(J->nl, J->al, J->nw) * 2 + 15) / 16 * 16;
 	}

@@ -92,6 +92,13 @@ __device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[PLK_R
 		int (&ip)[PLK_ROWS], int (&lh)[PLK_ROWS], const int (&ic)[PLK_ROWS], const int c16[8],
 		int (&o)[9], unsigned (&z)[PLK_ROWS], int (&hn)[PLK_ROWS])
 {
+	/* The integer pipe is the bound, so the update is written in the DPX forms that
+	 * issue one instruction each: __viaddmax_s32 (max(a + b, c)) for every clamped
+	 * state, __vibmax_s32 (max with the a >= b predicate) where a trace bit is the
+	 * comparison of the two operands of a max, and __vimax3_s32 to fold two
+	 * candidates into the running maximum at once (their tag adds can issue on the
+	 * FMA pipe).  The maximum of the encoded candidates does not depend on the
+	 * order in which they are folded. */
 	constexpr int R = PLK_ROWS, N16 = -32768 * 16;
 	const int GO = c16[0], GE = c16[1], IO = c16[2], F6 = c16[3], F7 = c16[4], F8 = c16[5], F9 = c16[6], FS = c16[7];
 	int h1 = in[0], h2 = in[1], h3 = in[2], d1 = in[3], d2 = in[4], d3 = in[5], va = in[6], vb = in[7], vc = in[8];
@@ -101,38 +108,37 @@ __device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[PLK_R
 		int h2m1 = r >= 2 ? hm[r - 2] : (r == 1 ? ah1 : ah2);
 		int h3m1 = r >= 3 ? hm[r - 3] : (r == 2 ? ah1 : (r == 1 ? ah2 : ah3));
 		if (r == 0 && row2) h1m1 = FS, h2m1 = FS, h3m1 = 0; /* column -1 while row 2 is computed: {0, -fs, -fs} */
-		int he = max(h3m1 + sct_b[code[r]], N16 + 15);       /* 0: H(i-3,j-1) + s(i,j) */
-		int t = max(lh[r] - GO, N16);
-		const unsigned p4 = ip[r] > t;
-		ip[r] = max(max(t, ip[r]) - GE, N16);
-		he = max(he, ip[r] + 14);                            /* 1: I */
-		int u = max(h3 - GO, N16);
-		const unsigned p5 = d3 > u;
-		const int dnew = max(max(u, d3) + gi[r], N16);
-		he = max(he, dnew + 13);                             /* 2: D */
-		u = max(h1 - IO, N16);
-		t = max(u + dn[r], N16);
-		const unsigned p6 = va > t;
-		const int anew = max(t, va);
-		he = max(he, anew + ac[r + 2] + 12);                 /* 3: A - a(i) */
-		u = max(h1m1 - IO, N16);
-		t = max(u + dn[r + 1], N16);
-		const unsigned p7 = vb > t;
-		const int bnew = max(t, vb);
-		he = max(he, bnew + ac[r] + 11);                     /* 4: B - a(i-2) */
-		t = max(u + dn[r + 2], N16);
-		const unsigned p8 = vc > t;
-		const int cnew = max(t, vc);
-		he = max(he, cnew + ac[r + 1] + 10);                 /* 5: C - a(i-1) */
-		he = max(he, h1 + F6);                               /* 6: H(i-1,j) - f */
-		he = max(he, h2 + F7);                               /* 7: H(i-2,j) - f */
-		he = max(he, h1m1 + F8);                             /* 8: H(i-1,j-1) - f */
-		he = max(he, h2m1 + F9);                             /* 9: H(i-2,j-1) - f */
+		bool q4, q5, q6, q7, q8, q9;
+		/* 1: I -- p4 = I(c-1) > H'(c-1) - go */
+		const int t4 = __viaddmax_s32(lh[r], -GO, N16);
+		const int im = __vibmax_s32(t4, ip[r], &q4);
+		ip[r] = __viaddmax_s32(im, -GE, N16);
+		/* 2: D -- p5 = D(i-3) > H(i-3) - go */
+		const int u5 = __viaddmax_s32(h3, -GO, N16);
+		const int dm = __vibmax_s32(u5, d3, &q5);
+		const int dnew = __viaddmax_s32(dm, gi[r], N16);
+		/* 3-5: phase-0/1/2 introns */
+		const int ua = __viaddmax_s32(h1, -IO, N16);
+		const int t6 = __viaddmax_s32(ua, dn[r], N16);
+		const int anew = __vibmax_s32(t6, va, &q6);
+		const int ub = __viaddmax_s32(h1m1, -IO, N16);
+		const int t7 = __viaddmax_s32(ub, dn[r + 1], N16);
+		const int bnew = __vibmax_s32(t7, vb, &q7);
+		const int t8 = __viaddmax_s32(ub, dn[r + 2], N16);
+		const int cnew = __vibmax_s32(t8, vc, &q8);
+		/* candidates 0..9, each value*16 + (15 - k) */
+		int he = __viaddmax_s32(h3m1, sct_b[code[r]], N16 + 15);   /* 0: H(i-3,j-1) + s(i,j) */
+		he = __vimax3_s32(he, ip[r] + 14, dnew + 13);               /* 1: I, 2: D */
+		he = __vimax3_s32(he, anew + ac[r + 2] + 12, bnew + ac[r] + 11); /* 3: A - a(i), 4: B - a(i-2) */
+		he = __vimax3_s32(he, cnew + ac[r + 1] + 10, h1 + F6);      /* 5: C - a(i-1), 6: H(i-1,j) - f */
+		he = __vimax3_s32(he, h2 + F7, h1m1 + F8);                  /* 7: H(i-2,j) - f, 8: H(i-1,j-1) - f */
+		he = __viaddmax_s32(h2m1, F9, he);                          /* 9: H(i-2,j-1) - f */
 		const int hfp = he & ~15;
 		lh[r] = hfp;
-		const unsigned p9 = ic[r] > he;                      /* raised by the carried insertion */
-		const int h = max(ic[r], hfp);
-		z[r] = (unsigned)(he & 15) | p4 << 4 | p5 << 5 | p6 << 6 | p7 << 7 | p8 << 8 | p9 << 9;
+		/* the carried insertion is a multiple of 16: ic > he exactly when ic > hfp */
+		const int h = __vibmax_s32(hfp, ic[r], &q9);
+		z[r] = (unsigned)(he & 15) | (q4 ? 0u : 1u << 4) | (q5 ? 0u : 1u << 5) | (q6 ? 0u : 1u << 6) |
+		       (q7 ? 0u : 1u << 7) | (q8 ? 0u : 1u << 8) | (q9 ? 0u : 1u << 9);
 		hn[r] = h;
 		h3 = h2, h2 = h1, h1 = h;
 		d3 = d2, d2 = d1, d1 = dnew;
