@@ -487,6 +487,43 @@ __global__ void __launch_bounds__(32 * TB_WARPS) k_traceback(plk_job_t *__restri
 		i = __shfl_sync(FULL, i, 0), j = __shfl_sync(FULL, j, 0);
 		last = __shfl_sync(FULL, last, 0), n = __shfl_sync(FULL, n, 0);
 		__syncwarp();
+		/* Inside an intron run (A/B/C extended: the path climbs column j one row per
+		 * step while the state's extension bit stays set) the warp scans 256 rows of
+		 * the column at once: each lane reads one 8-row trace word, and the run ends at
+		 * the highest row <= i whose bit is clear.  The rows of the run become one
+		 * merged N/U/V op, exactly what the row-by-row walk pushes. */
+		while (last >= 3 && last <= 5 && i >= 2 && j >= 0) {
+			const int ch_top = (i - 2) / PLK_ROWS, ch = ch_top - lane;
+			const int bit = last + 3;
+			int end_row = -1;
+			if (ch >= 0) {
+				const int ra = ch * PLK_ROWS, k = ra / hs, t = (ra / PLK_ROWS) % nlanes;
+				int d = j + t;
+				if (d >= al) d %= al;
+				const uint4 w4 = *(const uint4*)(tr + (((int64_t)k * al + d) * nlanes + t) * PLK_ROWS);
+				const uint32_t wd[4] = { w4.x, w4.y, w4.z, w4.w };
+#pragma unroll
+				for (int r = PLK_ROWS - 1; r >= 0; --r) {
+					const int row = ra + 2 + r;
+					const uint32_t x = (wd[r >> 1] >> ((r & 1) * 16)) & 0xffffu;
+					if (end_row < 0 && row <= i && !((x >> bit) & 1u)) end_row = row;
+				}
+			}
+#pragma unroll
+			for (int o = 16; o >= 1; o >>= 1) end_row = max(end_row, __shfl_xor_sync(FULL, end_row, o));
+			const int low = max(2, (ch_top - 31) * PLK_ROWS + 2);
+			const int op = last == 3 ? NS_CIGAR_N : (last == 4 ? NS_CIGAR_U : NS_CIGAR_V);
+			if (end_row >= low) { /* the run ends at end_row: its step clears the state (and moves j for U/V) */
+				if (lane == 0) tb_push(out, n, op, i - end_row + 1);
+				i = end_row - 1;
+				if (last != 3) --j;
+				last = 0;
+			} else {              /* every row down to `low` extends the run */
+				if (lane == 0) tb_push(out, n, op, i - low + 1);
+				i = low - 1;
+			}
+			n = __shfl_sync(FULL, n, 0);
+		}
 	}
 	if (lane == 0) {
 		if (j > 0) tb_push(out, n, NS_CIGAR_I, j);
