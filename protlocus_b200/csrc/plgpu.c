@@ -316,7 +316,7 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 		const int32_t j = sorted[q];
 		plk_job_t *J = &e->hj[j];
 		const int64_t cells = (int64_t)(J->nl - 2) * J->al, share = wave_cells[e->hwave[j]] / slots;
-		if (J->al >= 200 && J->nl - 2 >= 32 * PLK_WARPS_PER_CTA * PLK_ROWS && (double)cells > share * pl_coop_ratio())
+		if (J->al >= 200 && J->nl - 2 >= 32 * PLK_WARPS_PER_CTA * PLK_DP_ROWS && (double)cells > share * pl_coop_ratio())
 			J->nw = PLK_WARPS_PER_CTA;
 		J->trace_off = wave_bytes[e->hwave[j]] / 2;
 		wave_bytes[e->hwave[j]] += (plk_trace_words(J->nl, J->al, J->nw) * 2 + 15) / 16 * 16;

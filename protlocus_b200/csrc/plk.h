@@ -13,7 +13,10 @@ extern "C" {
 #endif
 
 #define PLK_WARPS_PER_CTA 8     /* a CTA is one 256-lane wavefront (large jobs) or 8 independent warps */
-#define PLK_ROWS 8              /* DP rows owned by one lane of a strip */
+#define PLK_ROWS 8              /* DP rows owned by one lane of a strip (extension DP) */
+#ifndef PLK_DP_ROWS
+#define PLK_DP_ROWS 8           /* DP rows owned by one lane of a strip (global DP and its trace layout) */
+#endif
 #define PLK_RING_INTS 12        /* column state handed from one strip to the next (9 used, 48-byte entries) */
 
 /* scoring parameters and lookup tables, passed to kernels by value */
@@ -74,10 +77,10 @@ static inline int64_t plk_prep_bytes(int32_t nl, int32_t al)
 	return ((int64_t)nl + al + 2 * ((int64_t)nl + 1) + 7) / 8 * 8;
 }
 
-/* trace words of a job in the strip layout (strips of 32*nw*PLK_ROWS rows) */
+/* trace words of a job in the strip layout (strips of 32*nw*PLK_DP_ROWS rows) */
 static inline int64_t plk_trace_words(int32_t nl, int32_t al, int32_t nw)
 {
-	int64_t h = 32LL * nw * PLK_ROWS, nr = (int64_t)nl - 2, strips = (nr + h - 1) / h;
+	int64_t h = 32LL * nw * PLK_DP_ROWS, nr = (int64_t)nl - 2, strips = (nr + h - 1) / h;
 	return strips * h * (int64_t)al;
 }
 

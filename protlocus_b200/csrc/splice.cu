@@ -61,6 +61,25 @@ __global__ void k_prep(const plk_job_t *__restrict__ jobs, int n_jobs, const uin
 
 /* ------------------------------------------------------------------ the DP */
 
+/* the R trace words of a lane and step, stored and loaded as one vector */
+#if PLK_DP_ROWS == 8
+typedef uint4 trace_vec_t;
+#define PLK_DP_MIN_CTAS 2
+#elif PLK_DP_ROWS == 4
+typedef uint2 trace_vec_t;
+#define PLK_DP_MIN_CTAS 3
+#else
+#error "PLK_DP_ROWS must be 4 or 8"
+#endif
+
+__device__ __forceinline__ void store_trace(uint16_t *p, const unsigned (&z)[PLK_DP_ROWS])
+{
+	uint32_t w[PLK_DP_ROWS / 2];
+#pragma unroll
+	for (int q = 0; q < PLK_DP_ROWS / 2; ++q) w[q] = (z[2 * q] & 0xffffu) | (z[2 * q + 1] << 16);
+	*(trace_vec_t*)p = *(const trace_vec_t*)w;
+}
+
 struct DpShared {
 	int32_t sct[22 * 22];                               /* score table, transposed: sct[b*22 + a] */
 	int32_t slot[2][PLK_WARPS_PER_CTA][PLK_RING_INTS];  /* warp-to-warp hand-off of a cooperative wavefront */
@@ -86,11 +105,11 @@ struct DpShared {
  * clamped exactly; sat(sat(x-a)-b) is max(max(x-a, NEG)-b, NEG).
  */
 template <int NW>
-__device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[PLK_ROWS], const int ah1, const int ah2,
-		const int ah3, const bool row2, const int *__restrict__ sct_b, const int (&code)[PLK_ROWS],
-		const int (&gi)[PLK_ROWS], const int (&dn)[PLK_ROWS + 2], const int (&ac)[PLK_ROWS + 2],
-		int (&ip)[PLK_ROWS], int (&lh)[PLK_ROWS], const int (&ic)[PLK_ROWS], const int c16[8],
-		int (&o)[9], unsigned (&z)[PLK_ROWS], int (&hn)[PLK_ROWS])
+__device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[PLK_DP_ROWS], const int ah1, const int ah2,
+		const int ah3, const bool row2, const int *__restrict__ sct_b, const int (&code)[PLK_DP_ROWS],
+		const int (&gi)[PLK_DP_ROWS], const int (&dn)[PLK_DP_ROWS + 2], const int (&ac)[PLK_DP_ROWS + 2],
+		int (&ip)[PLK_DP_ROWS], int (&lh)[PLK_DP_ROWS], const int (&ic)[PLK_DP_ROWS], const int c16[8],
+		int (&o)[9], unsigned (&z)[PLK_DP_ROWS], int (&hn)[PLK_DP_ROWS])
 {
 	/* The integer pipe is the bound, so the update is written in the DPX forms that
 	 * issue one instruction each: __viaddmax_s32 (max(a + b, c)) for every clamped
@@ -99,7 +118,7 @@ __device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[PLK_R
 	 * candidates into the running maximum at once (their tag adds can issue on the
 	 * FMA pipe).  The maximum of the encoded candidates does not depend on the
 	 * order in which they are folded. */
-	constexpr int R = PLK_ROWS, N16 = -32768 * 16;
+	constexpr int R = PLK_DP_ROWS, N16 = -32768 * 16;
 	const int GO = c16[0], GE = c16[1], IO = c16[2], F6 = c16[3], F7 = c16[4], F8 = c16[5], F9 = c16[6], FS = c16[7];
 	int h1 = in[0], h2 = in[1], h3 = in[2], d1 = in[3], d2 = in[4], d3 = in[5], va = in[6], vb = in[7], vc = in[8];
 #pragma unroll
@@ -150,14 +169,14 @@ __device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[PLK_R
 /* Straightforward formulation for the 32-bit width (MODE 1) and the doubly
  * clamped int16 case (MODE 2). */
 template <int MODE>
-__device__ __forceinline__ void cells_plain(const int (&in)[9], int (&hm)[PLK_ROWS], const int ah1, const int ah2,
+__device__ __forceinline__ void cells_plain(const int (&in)[9], int (&hm)[PLK_DP_ROWS], const int ah1, const int ah2,
 		const int ah3, const bool row2, const bool seg, const bool first, const int *__restrict__ sct_b,
-		const int (&code)[PLK_ROWS], const int (&gi)[PLK_ROWS], const int (&dn)[PLK_ROWS + 2],
-		const int (&ac)[PLK_ROWS + 2], int (&ip)[PLK_ROWS], int (&lh)[PLK_ROWS], int (&ic)[PLK_ROWS],
-		const plk_params_t &P, int (&o)[9], unsigned (&z)[PLK_ROWS], int (&hn)[PLK_ROWS])
+		const int (&code)[PLK_DP_ROWS], const int (&gi)[PLK_DP_ROWS], const int (&dn)[PLK_DP_ROWS + 2],
+		const int (&ac)[PLK_DP_ROWS + 2], int (&ip)[PLK_DP_ROWS], int (&lh)[PLK_DP_ROWS], int (&ic)[PLK_DP_ROWS],
+		const plk_params_t &P, int (&o)[9], unsigned (&z)[PLK_DP_ROWS], int (&hn)[PLK_DP_ROWS])
 {
 	typedef Ar<MODE> A;
-	constexpr int R = PLK_ROWS;
+	constexpr int R = PLK_DP_ROWS;
 	const int NEG = A::NEG, go = P.go, ge = P.ge, goe = P.go + P.ge, io = P.io, fs = P.fs;
 	int h1 = in[0], h2 = in[1], h3 = in[2], d1 = in[3], d2 = in[4], d3 = in[5], va = in[6], vb = in[7], vc = in[8];
 #pragma unroll
@@ -249,7 +268,7 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 		uint16_t *__restrict__ trace, int32_t *__restrict__ myring, DpShared &sh, const plk_params_t &P,
 		const int L, const int wib)
 {
-	constexpr int R = PLK_ROWS, NL = 32 * NW, HS = NL * R;
+	constexpr int R = PLK_DP_ROWS, NL = 32 * NW, HS = NL * R;
 	constexpr int SC = MODE == 0 ? 16 : 1;                  /* value scale of the mode */
 	const int NEG = Ar<MODE>::NEG * SC;
 	const int lane = L & 31, w = L >> 5;
@@ -341,13 +360,8 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 				for (int r = 0; r < R; ++r)
 					if (r == rl) J->score = MODE == 0 ? hn[r] >> 4 : hn[r];
 			}
-			/* trace: one 16-byte store per lane, contiguous across the lanes of a strip */
-			uint4 tw;
-			tw.x = (z[0] & 0xffff) | (z[1] << 16);
-			tw.y = (z[2] & 0xffff) | (z[3] << 16);
-			tw.z = (z[4] & 0xffff) | (z[5] << 16);
-			tw.w = (z[6] & 0xffff) | (z[7] << 16);
-			*(uint4*)(tr + (((int64_t)k * al + dcol) * NL + L) * R) = tw;
+			/* trace: one store of R 16-bit words per lane, contiguous across the lanes of a strip */
+			store_trace(tr + (((int64_t)k * al + dcol) * NL + L) * R, z);
 			if (L == NL - 1) {
 				int32_t *e = myring + (int64_t)c * PLK_RING_INTS;
 #pragma unroll
@@ -384,7 +398,7 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
  * job) until that queue is empty, then every warp takes solo jobs.  Both queues
  * are sorted by decreasing size on the host (longest-processing-time first). */
 template <int MODE>
-__global__ void __launch_bounds__(32 * PLK_WARPS_PER_CTA, 2)
+__global__ void __launch_bounds__(32 * PLK_WARPS_PER_CTA, PLK_DP_MIN_CTAS)
 k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop, int n_coop,
 		const int32_t *__restrict__ order_solo, int n_solo, int32_t *counters,
 		const uint8_t *__restrict__ prep, uint16_t *__restrict__ trace, int32_t *__restrict__ ring,
@@ -430,13 +444,13 @@ __device__ __forceinline__ void tb_push(uint32_t *out, int &n, uint32_t op, int 
  * stages the trace words around the current cell in shared memory -- a tile of
  * 8 row-chunks (64 rows) x 32 columns, one coalesced round of 16-byte loads --
  * and lane 0 walks inside the tile until the path leaves it. */
-#define TB_CHUNKS 8
+#define TB_CHUNKS (64 / PLK_DP_ROWS)
 #define TB_COLS 32
 #define TB_WARPS 8
 __global__ void __launch_bounds__(32 * TB_WARPS) k_traceback(plk_job_t *__restrict__ jobs,
 		const int32_t *__restrict__ order, int n_order, const uint16_t *__restrict__ trace, uint32_t *__restrict__ tmp)
 {
-	__shared__ uint4 s_tile[TB_WARPS][TB_CHUNKS][TB_COLS]; /* 8 trace words (rows) per entry */
+	__shared__ trace_vec_t s_tile[TB_WARPS][TB_CHUNKS][TB_COLS]; /* the trace words of R rows per entry */
 	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
 	const int q = blockIdx.x * TB_WARPS + wib;
 	if (q >= n_order) return;
@@ -444,29 +458,29 @@ __global__ void __launch_bounds__(32 * TB_WARPS) k_traceback(plk_job_t *__restri
 	const int nl = J->nl, al = J->al;
 	const uint16_t *tr = trace + J->trace_off;
 	uint32_t *out = tmp + J->tmp_off;
-	const int nlanes = 32 * J->nw, hs = nlanes * PLK_ROWS;
+	const int nlanes = 32 * J->nw, hs = nlanes * PLK_DP_ROWS;
 	int i = nl - 1, j = al - 1, last = 0, n = 0;
 	while (i >= 2 && j >= 0) {
 		/* stage the tile whose top-right corner holds (i, j) */
-		const int qc = (i - 2) / PLK_ROWS, jc = j;
+		const int qc = (i - 2) / PLK_DP_ROWS, jc = j;
 #pragma unroll
 		for (int m = 0; m < TB_CHUNKS * TB_COLS / 32; ++m) {
 			const int idx = lane + 32 * m, dq = idx / TB_COLS, dc = idx % TB_COLS;
 			const int ch = qc - dq, col = jc - dc;
 			if (ch >= 0 && col >= 0) {
-				const int ra = ch * PLK_ROWS, k = ra / hs, t = (ra / PLK_ROWS) % nlanes;
+				const int ra = ch * PLK_DP_ROWS, k = ra / hs, t = (ra / PLK_DP_ROWS) % nlanes;
 				int d = col + t;
 				if (d >= al) d %= al;
-				s_tile[wib][dq][dc] = *(const uint4*)(tr + (((int64_t)k * al + d) * nlanes + t) * PLK_ROWS);
+				s_tile[wib][dq][dc] = *(const trace_vec_t*)(tr + (((int64_t)k * al + d) * nlanes + t) * PLK_DP_ROWS);
 			}
 		}
 		__syncwarp();
 		if (lane == 0) {
 			while (i >= 2 && j >= 0) {
-				const int dq = qc - (i - 2) / PLK_ROWS, dc = jc - j;
+				const int dq = qc - (i - 2) / PLK_DP_ROWS, dc = jc - j;
 				if (dq >= TB_CHUNKS || dc >= TB_COLS) break;
 				const uint16_t *cell = (const uint16_t*)&s_tile[wib][dq][dc];
-				const int x = cell[(i - 2) % PLK_ROWS];
+				const int x = cell[(i - 2) % PLK_DP_ROWS];
 				const int state = last != 0 ? last : (x >> 9 & 1) ? 1 : 15 - (x & 0xf);
 				const int ext = state >= 1 && state <= 5 ? (x >> (state + 3)) & 1 : 0;
 				switch (state) {
@@ -488,30 +502,30 @@ __global__ void __launch_bounds__(32 * TB_WARPS) k_traceback(plk_job_t *__restri
 		last = __shfl_sync(FULL, last, 0), n = __shfl_sync(FULL, n, 0);
 		__syncwarp();
 		/* Inside an intron run (A/B/C extended: the path climbs column j one row per
-		 * step while the state's extension bit stays set) the warp scans 256 rows of
-		 * the column at once: each lane reads one 8-row trace word, and the run ends at
+		 * step while the state's extension bit stays set) the warp scans 32*R rows of
+		 * the column at once: each lane reads one R-row trace word, and the run ends at
 		 * the highest row <= i whose bit is clear.  The rows of the run become one
 		 * merged N/U/V op, exactly what the row-by-row walk pushes. */
 		while (last >= 3 && last <= 5 && i >= 2 && j >= 0) {
-			const int ch_top = (i - 2) / PLK_ROWS, ch = ch_top - lane;
+			const int ch_top = (i - 2) / PLK_DP_ROWS, ch = ch_top - lane;
 			const int bit = last + 3;
 			int end_row = -1;
 			if (ch >= 0) {
-				const int ra = ch * PLK_ROWS, k = ra / hs, t = (ra / PLK_ROWS) % nlanes;
+				const int ra = ch * PLK_DP_ROWS, k = ra / hs, t = (ra / PLK_DP_ROWS) % nlanes;
 				int d = j + t;
 				if (d >= al) d %= al;
-				const uint4 w4 = *(const uint4*)(tr + (((int64_t)k * al + d) * nlanes + t) * PLK_ROWS);
-				const uint32_t wd[4] = { w4.x, w4.y, w4.z, w4.w };
+				const trace_vec_t wv = *(const trace_vec_t*)(tr + (((int64_t)k * al + d) * nlanes + t) * PLK_DP_ROWS);
+				const uint16_t *wd = (const uint16_t*)&wv;
 #pragma unroll
-				for (int r = PLK_ROWS - 1; r >= 0; --r) {
+				for (int r = PLK_DP_ROWS - 1; r >= 0; --r) {
 					const int row = ra + 2 + r;
-					const uint32_t x = (wd[r >> 1] >> ((r & 1) * 16)) & 0xffffu;
+					const uint32_t x = wd[r];
 					if (end_row < 0 && row <= i && !((x >> bit) & 1u)) end_row = row;
 				}
 			}
 #pragma unroll
 			for (int o = 16; o >= 1; o >>= 1) end_row = max(end_row, __shfl_xor_sync(FULL, end_row, o));
-			const int low = max(2, (ch_top - 31) * PLK_ROWS + 2);
+			const int low = max(2, (ch_top - 31) * PLK_DP_ROWS + 2);
 			const int op = last == 3 ? NS_CIGAR_N : (last == 4 ? NS_CIGAR_U : NS_CIGAR_V);
 			if (end_row >= low) { /* the run ends at end_row: its step clears the state (and moves j for U/V) */
 				if (lane == 0) tb_push(out, n, op, i - end_row + 1);
