@@ -21,7 +21,7 @@
  *                three running values per row: ip (first-pass insertion), ic
  *                (carried insertion) and lh (first-pass H of the previous
  *                column).  Saturating int16 arithmetic is emulated in int32.
- *                Trace words (state in bits 0-3, extension bits 4-8) are written
+ *                Trace words (state in bits 0-3, extension and lazy-F flags) are written
  *                with one 16-byte store per lane per step into a diagonal-major
  *                layout, so every warp store is a contiguous 512-byte run.
  *   k_traceback  one thread per job walks the trace (nasw-sse.c:44-93) and
@@ -90,9 +90,12 @@ struct DpShared {
 
 /*
  * Trace word of a cell (all modes): bits 0-3 = 15 - state (state 0..9 in the
- * candidate order of nasw-sse.c:464-536), bits 4-8 = extension bits of I, D,
- * A, B, C, bit 9 = raised by the carried insertion (the reference's lazy-F
- * bit; state 1 when read without a pending extension).
+ * candidate order of nasw-sse.c:464-536); extension bits of I (bit 4), D (bit 5),
+ * C (bit 6), A (bit 12), B (bit 13); bit 14 = raised by the carried insertion (the
+ * reference's lazy-F bit; state 1 when read without a pending extension).  Bits
+ * 7-11 and 15 are undefined.  The positions let MODE 0 gather the six flags from
+ * the signs of six differences with three byte permutes (a sign-replicated byte
+ * per flag, two flags per permute) and three bit-selects.
  *
  * MODE 0 works in a scaled domain: every DP value is kept times 16, so the low
  * four bits of a running maximum can carry the index of the candidate that
@@ -104,6 +107,15 @@ struct DpShared {
  * below the floor can neither win nor tie.  Stored states (I, D, A, B, C) are
  * clamped exactly; sat(sat(x-a)-b) is max(max(x-a, NEG)-b, NEG).
  */
+/* byte 0 = 0xFF if a < 0 else 0, byte 1 = the same for b (prmt selector nibbles with
+ * the sign-replicate bit set: 0xB = byte 3 of a, 0xF = byte 3 of b) */
+__device__ __forceinline__ unsigned sign_bytes(int a, int b)
+{
+	unsigned d;
+	asm("prmt.b32 %0, %1, %2, 0x00FB;" : "=r"(d) : "r"(a), "r"(b));
+	return d;
+}
+
 template <int NW>
 __device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[PLK_DP_ROWS], const int ah1, const int ah2,
 		const int ah3, const bool row2, const int *__restrict__ sct_b, const int (&code)[PLK_DP_ROWS],
@@ -127,24 +139,28 @@ __device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[PLK_D
 		int h2m1 = r >= 2 ? hm[r - 2] : (r == 1 ? ah1 : ah2);
 		int h3m1 = r >= 3 ? hm[r - 3] : (r == 2 ? ah1 : (r == 1 ? ah2 : ah3));
 		if (r == 0 && row2) h1m1 = FS, h2m1 = FS, h3m1 = 0; /* column -1 while row 2 is computed: {0, -fs, -fs} */
-		bool q4, q5, q6, q7, q8, q9;
+		/* each extension flag is the sign of a difference: x > y exactly when y - x < 0
+		 * (|values| < 2^21, no overflow) */
 		/* 1: I -- p4 = I(c-1) > H'(c-1) - go */
 		const int t4 = __viaddmax_s32(lh[r], -GO, N16);
-		const int im = __vibmax_s32(t4, ip[r], &q4);
-		ip[r] = __viaddmax_s32(im, -GE, N16);
+		const int d4 = t4 - ip[r];
+		ip[r] = __viaddmax_s32(max(t4, ip[r]), -GE, N16);
 		/* 2: D -- p5 = D(i-3) > H(i-3) - go */
 		const int u5 = __viaddmax_s32(h3, -GO, N16);
-		const int dm = __vibmax_s32(u5, d3, &q5);
-		const int dnew = __viaddmax_s32(dm, gi[r], N16);
+		const int d5 = u5 - d3;
+		const int dnew = __viaddmax_s32(max(u5, d3), gi[r], N16);
 		/* 3-5: phase-0/1/2 introns */
 		const int ua = __viaddmax_s32(h1, -IO, N16);
 		const int t6 = __viaddmax_s32(ua, dn[r], N16);
-		const int anew = __vibmax_s32(t6, va, &q6);
+		const int d6 = t6 - va;
+		const int anew = max(t6, va);
 		const int ub = __viaddmax_s32(h1m1, -IO, N16);
 		const int t7 = __viaddmax_s32(ub, dn[r + 1], N16);
-		const int bnew = __vibmax_s32(t7, vb, &q7);
+		const int d7 = t7 - vb;
+		const int bnew = max(t7, vb);
 		const int t8 = __viaddmax_s32(ub, dn[r + 2], N16);
-		const int cnew = __vibmax_s32(t8, vc, &q8);
+		const int d8 = t8 - vc;
+		const int cnew = max(t8, vc);
 		/* candidates 0..9, each value*16 + (15 - k) */
 		int he = __viaddmax_s32(h3m1, sct_b[code[r]], N16 + 15);   /* 0: H(i-3,j-1) + s(i,j) */
 		he = __vimax3_s32(he, ip[r] + 14, dnew + 13);               /* 1: I, 2: D */
@@ -155,9 +171,14 @@ __device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[PLK_D
 		const int hfp = he & ~15;
 		lh[r] = hfp;
 		/* the carried insertion is a multiple of 16: ic > he exactly when ic > hfp */
-		const int h = __vibmax_s32(hfp, ic[r], &q9);
-		z[r] = (unsigned)(he & 15) | (q4 ? 0u : 1u << 4) | (q5 ? 0u : 1u << 5) | (q6 ? 0u : 1u << 6) |
-		       (q7 ? 0u : 1u << 7) | (q8 ? 0u : 1u << 8) | (q9 ? 0u : 1u << 9);
+		const int d9 = hfp - ic[r];
+		const int h = max(hfp, ic[r]);
+		const unsigned pa = sign_bytes(d4, d6);  /* p4 -> bit 4, p6 -> bit 12 */
+		const unsigned pb = sign_bytes(d5, d7);  /* p5 -> bit 5, p7 -> bit 13 */
+		const unsigned pc = sign_bytes(d8, d9);  /* p8 -> bit 6, p9 -> bit 14 */
+		unsigned zz = (pa & 0x1010u) | (pb & ~0x1010u);
+		zz = (zz & 0x3030u) | (pc & ~0x3030u);
+		z[r] = ((unsigned)he & 0xFu) | (zz & ~0xFu);
 		hn[r] = h;
 		h3 = h2, h2 = h1, h1 = h;
 		d3 = d2, d2 = d1, d1 = dnew;
@@ -213,7 +234,7 @@ __device__ __forceinline__ void cells_plain(const int (&in)[9], int (&hm)[PLK_DP
 		h = max(h, t);
 		u = A::sub(h1, io);
 		t = A::sub(u, dim1);
-		zz |= va > t ? 1u << 6 : 0u;
+		zz |= va > t ? 1u << 12 : 0u;
 		t = max(t, va);
 		const int anew = t;
 		t = A::sub(t, ai);
@@ -221,14 +242,14 @@ __device__ __forceinline__ void cells_plain(const int (&in)[9], int (&hm)[PLK_DP
 		h = max(h, t);
 		u = A::sub(h1m1, io);
 		t = A::sub(u, di);
-		zz |= vb > t ? 1u << 7 : 0u;
+		zz |= vb > t ? 1u << 13 : 0u;
 		t = max(t, vb);
 		const int bnew = t;
 		t = A::sub(t, aim2);
 		y = t > h ? 4 : y;
 		h = max(h, t);
 		t = A::sub(u, dip1);
-		zz |= vc > t ? 1u << 8 : 0u;
+		zz |= vc > t ? 1u << 6 : 0u;
 		t = max(t, vc);
 		const int cnew = t;
 		t = A::sub(t, aim1);
@@ -249,8 +270,8 @@ __device__ __forceinline__ void cells_plain(const int (&in)[9], int (&hm)[PLK_DP
 		lh[r] = h;
 		if (icr > h) { /* raised by the carried insertion */
 			h = icr;
-			zz = MODE == 1 ? ((unsigned)it | 14u | 1u << 9) /* 32-bit: the word is replaced by 1|i_trace, nasw-sse.c:949 */
-				: (zz | (unsigned)(15 - y) | 1u << 9);
+			zz = MODE == 1 ? ((unsigned)it | 14u | 1u << 14) /* 32-bit: the word is replaced by 1|i_trace, nasw-sse.c:949 */
+				: (zz | (unsigned)(15 - y) | 1u << 14);
 		} else zz |= (unsigned)(15 - y);
 		z[r] = zz;
 		hn[r] = h;
@@ -434,6 +455,9 @@ k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop
 
 /* ------------------------------------------------------------------ traceback */
 
+/* trace-word bit of the extension flag of state 1..5 (I, D, A, B, C) */
+__device__ __forceinline__ int tb_ext_bit(int state) { return (0x6DC540 >> (4 * state)) & 15; }
+
 __device__ __forceinline__ void tb_push(uint32_t *out, int &n, uint32_t op, int len)
 { /* ns_push_cigar merge rule (nasw.h:219-229) */
 	if (n == 0 || op != (out[n - 1] & 0xf) || op == NS_CIGAR_F || op == NS_CIGAR_G) out[n++] = (uint32_t)len << 4 | op;
@@ -481,8 +505,8 @@ __global__ void __launch_bounds__(32 * TB_WARPS) k_traceback(plk_job_t *__restri
 				if (dq >= TB_CHUNKS || dc >= TB_COLS) break;
 				const uint16_t *cell = (const uint16_t*)&s_tile[wib][dq][dc];
 				const int x = cell[(i - 2) % PLK_DP_ROWS];
-				const int state = last != 0 ? last : (x >> 9 & 1) ? 1 : 15 - (x & 0xf);
-				const int ext = state >= 1 && state <= 5 ? (x >> (state + 3)) & 1 : 0;
+				const int state = last != 0 ? last : (x >> 14 & 1) ? 1 : 15 - (x & 0xf);
+				const int ext = state >= 1 && state <= 5 ? (x >> tb_ext_bit(state)) & 1 : 0;
 				switch (state) {
 				case 0: tb_push(out, n, NS_CIGAR_M, 1), i -= 3, --j; break;
 				case 1: tb_push(out, n, NS_CIGAR_I, 1), --j; break;
@@ -508,7 +532,7 @@ __global__ void __launch_bounds__(32 * TB_WARPS) k_traceback(plk_job_t *__restri
 		 * merged N/U/V op, exactly what the row-by-row walk pushes. */
 		while (last >= 3 && last <= 5 && i >= 2 && j >= 0) {
 			const int ch_top = (i - 2) / PLK_DP_ROWS, ch = ch_top - lane;
-			const int bit = last + 3;
+			const int bit = tb_ext_bit(last);
 			int end_row = -1;
 			if (ch >= 0) {
 				const int ra = ch * PLK_DP_ROWS, k = ra / hs, t = (ra / PLK_DP_ROWS) % nlanes;
