@@ -144,11 +144,11 @@ __device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[PLK_D
 		/* 1: I -- p4 = I(c-1) > H'(c-1) - go */
 		const int t4 = __viaddmax_s32(lh[r], -GO, N16);
 		const int d4 = t4 - ip[r];
-		ip[r] = __viaddmax_s32(max(t4, ip[r]), -GE, N16);
+		ip[r] = __vimax3_s32(t4 - GE, ip[r] - GE, N16);  /* max(max(t4, ip) - ge, floor) */
 		/* 2: D -- p5 = D(i-3) > H(i-3) - go */
 		const int u5 = __viaddmax_s32(h3, -GO, N16);
 		const int d5 = u5 - d3;
-		const int dnew = __viaddmax_s32(max(u5, d3), gi[r], N16);
+		const int dnew = __vimax3_s32(u5 + gi[r], d3 + gi[r], N16);  /* max(max(u, D) + gi, floor) */
 		/* 3-5: phase-0/1/2 introns */
 		const int ua = __viaddmax_s32(h1, -IO, N16);
 		const int t6 = __viaddmax_s32(ua, dn[r], N16);
