@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--pairs", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the engine's default tuning instead of autotuning it on the workload (global DP)")
     ap.add_argument("--workload", default="global", choices=["global", "ext", "hmm", "gapless", "forward", "prefilter"],
                     help="global: the batched global spliced DP (headline); ext: the batched extension DP; "
                          "hmm: the integer profile-HMM DP; gapless: the gapless X-drop prefilter; "
@@ -248,6 +250,15 @@ def main():
         if not ok:
             raise RuntimeError("pl_splice_batch_device: " + L.error())
 
+    tuning = {"r4_rows": None, "coop_ratio": None, "autotuned": False}
+    if not args.no_autotune:
+        r4, ratio = C.c_int32(), C.c_double()
+        if not eng.lib.pl_engine_autotune(eng.h, opt.ptr, tab, n, d_nt.data_ptr(), d_aa.data_ptr(), None,
+                                          C.byref(r4), C.byref(ratio)):
+            raise RuntimeError("pl_engine_autotune: " + L.error())
+        tuning = {"r4_rows": r4.value, "coop_ratio": ratio.value, "autotuned": True}
+    else:
+        tuning.update(eng.tuning())
     for _ in range(args.warmup):
         step_device()
     res = (SpliceResult * n).from_buffer_copy(d_res.cpu().numpy().tobytes())
@@ -325,7 +336,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
             "config": {"workload": WORKLOAD if not args.uniform else "profiling case " + args.uniform, "n_jobs": n, "cells_per_step": cells, "seed": "1+rank",
                        "l2": "inputs and the per-step traceback arena (tens of GB) are far larger than L2",
-                       "waves": plan["waves"], "coop_jobs": plan["coop"], "parallelism": f"{world} independent ranks"},
+                       "waves": plan["waves"], "coop_jobs": plan["coop"], "parallelism": f"{world} independent ranks",
+                       "tuning": tuning},
             "e2e": e2e,
             "gpu_launches": int(launches),
             "roofline": {"bound": "int", "kernel": "k_splice_dp", "achieved": achieved, "peak": peak,

@@ -194,6 +194,15 @@ void *pl_engine_stream(const pl_engine_t *e);
  * int32 add+max chains and int16x2 (__vadd2 + __vmaxs2) chains at full
  * occupancy.  The DP kernels are bound by this pipe.  Returns 1 on success. */
 int pl_measure_int_peak(int32_t device, double *int32_lane_ops, double *int16x2_lane_ops);
+/* Tuning of the batched global DP: jobs with at most r4_rows DP rows (nl - 2) run 4
+ * rows per lane, the rest 8; a job takes a whole CTA when it holds more than
+ * coop_ratio times a warp's share of its wave's cells.  set: negative / non-positive
+ * arguments keep the current value.  autotune: times the given batch (results
+ * discarded) under a grid of both, keeps the fastest on the engine and reports it. */
+void pl_engine_set_tuning(pl_engine_t *e, int32_t r4_rows, double coop_ratio);
+void pl_engine_get_tuning(const pl_engine_t *e, int32_t *r4_rows, double *coop_ratio);
+int pl_engine_autotune(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n,
+		const uint8_t *nt, const uint8_t *aa, const uint8_t *ss, int32_t *r4_rows, double *coop_ratio);
 
 /* Number of trace waves, cooperative jobs and DP launches of the last batch. */
 void pl_engine_last_plan(const pl_engine_t *e, int32_t *n_waves, int32_t *n_coop, int32_t *n_dp_launches);

@@ -122,11 +122,11 @@ static int na_run(const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n_jo
 		J->nl = x->nl, J->al = x->al;
 		J->mode = bound + opt->end_bonus > 30000 ? 1 : (bound + 256 >= 32767 ? 2 : 0);
 		J->slen = J->mode == 1 ? (x->al + 3) / 4 : (x->al + 7) / 8;
-		J->nw = 1;
+		J->nw = 1, J->rows = PLK_DP_ROWS;
 		J->score = INT32_MIN;
 		J->prep_off = prep_total, prep_total += plk_prep_bytes(x->nl, x->al);
 		J->tmp_off = tmp_total, tmp_total += (int64_t)x->nl + x->al + 8;
-		J->trace_off = trace_total / 2, trace_total += (plk_trace_words(x->nl, x->al, 1) * 2 + 15) / 16 * 16;
+		J->trace_off = trace_total / 2, trace_total += (plk_trace_words(x->nl, x->al, 1, PLK_DP_ROWS) * 2 + 15) / 16 * 16;
 		if (x->al > max_al) max_al = x->al;
 	}
 	/* carve the array: jobs | order | counters | total | prep | tmp | ring | trace */
@@ -169,7 +169,7 @@ static int na_run(const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n_jo
 			int32_t n_m = 0;
 			while (pos + n_m < n_jobs && g_na_jobs[g_na_order[pos + n_m]].mode == m) ++n_m;
 			if (n_m > 0 && (e = (cudaError_t)plk_splice_dp(d_jobs, d_order + pos, 0, d_order + pos, n_m, d_cnt, d_prep,
-					d_trace, d_ring, ring_stride, PL_NOALLOC_CTAS, m, &P, st)) != cudaSuccess)
+					d_trace, d_ring, ring_stride, PL_NOALLOC_CTAS, m, PLK_DP_ROWS, &P, st)) != cudaSuccess)
 				goto cuda_fail;
 			pos += n_m;
 		}

@@ -99,9 +99,14 @@ PL_EXPORT pl_engine_t *pl_engine_create(int32_t device, int64_t trace_budget_byt
 	CK(cudaSetDevice(device));
 	CK(cudaDeviceGetAttribute(&e->n_sm, cudaDevAttrMultiProcessorCount, device));
 	for (m = 0; m < 3; ++m) {
-		e->ctas_per_sm[m] = plk_dp_ctas_per_sm(m);
-		if (e->ctas_per_sm[m] < 1) { pl_set_error("DP kernel does not fit on an SM (mode %d)", m); goto fail; }
+		int r;
+		for (r = 0; r < 2; ++r) {
+			e->ctas_per_sm[m][r] = plk_dp_ctas_per_sm(m, r == 0 ? 8 : 4);
+			if (e->ctas_per_sm[m][r] < 1) { pl_set_error("DP kernel does not fit on an SM (mode %d)", m); goto fail; }
+		}
 	}
+	e->coop_ratio = pl_coop_ratio();
+	e->r4_rows = pl_r4_rows();
 	CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
 	CK(cudaMemGetInfo(&free_b, &total_b));
 	if (trace_budget_bytes <= 0) { /* default: 40% of free memory, at most 72 GB */
@@ -214,6 +219,23 @@ double pl_coop_ratio(void)
 	return g_coop_ratio;
 }
 
+/* Jobs with at most this many DP rows (nl - 2) run with 4 rows per lane (80 registers,
+ * three CTAs per SM), the rest with 8 (128 registers, two CTAs per SM): 4 pays on
+ * short windows, 8 on long ones.  PLGPU_R4_ROWS overrides the default; the engine's
+ * autotuner (pl_engine_autotune) picks it for a workload. */
+static int32_t g_r4_rows = 0;
+static pthread_once_t g_r4_once = PTHREAD_ONCE_INIT;
+static void pl_r4_rows_init(void)
+{
+	const char *v = getenv("PLGPU_R4_ROWS");
+	if (v && *v) g_r4_rows = atoi(v);
+}
+int32_t pl_r4_rows(void)
+{
+	pthread_once(&g_r4_once, pl_r4_rows_init);
+	return g_r4_rows;
+}
+
 typedef struct { int64_t cells; int32_t idx; } pl_key_t;
 static int pl_cmp_cells_desc(const void *a, const void *b)
 {
@@ -224,8 +246,9 @@ static int pl_cmp_cells_desc(const void *a, const void *b)
 
 static int pl_max_ctas(const pl_engine_t *e)
 {
-	int m, c = 0;
-	for (m = 0; m < 3; ++m) if (e->ctas_per_sm[m] > c) c = e->ctas_per_sm[m];
+	int m, r, c = 0;
+	for (m = 0; m < 3; ++m)
+		for (r = 0; r < 2; ++r) if (e->ctas_per_sm[m][r] > c) c = e->ctas_per_sm[m][r];
 	return c;
 }
 
@@ -257,7 +280,7 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 	if (!pl_params(opt, &P, 0)) return 0;
 	if (!pl_grow_host(e, n)) return 0;
 	max_sub = pl_max_sub(opt);
-	slots = (int64_t)e->n_sm * e->ctas_per_sm[0] * PLK_WARPS_PER_CTA;
+	slots = (int64_t)e->n_sm * e->ctas_per_sm[0][0] * PLK_WARPS_PER_CTA;
 
 	/* 1. per-job metadata with nw = 1 sizes */
 	for (q = 0; q < n; ++q) {
@@ -274,13 +297,14 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 		J->mode = bound + opt->end_bonus > 30000 ? 1 : (bound + 256 >= 32767 ? 2 : 0);
 		J->slen = J->mode == 1 ? (x->al + 3) / 4 : (x->al + 7) / 8;
 		J->nw = 1;
+		J->rows = x->nl - 2 <= e->r4_rows ? 4 : PLK_DP_ROWS;
 		J->prep_off = prep_total, prep_total += plk_prep_bytes(x->nl, x->al);
 		J->tmp_off = tmp_total, tmp_total += (int64_t)x->nl + x->al + 8;
 		J->score = INT32_MIN;
 		if (x->al > max_al) max_al = x->al;
-		trace_total += plk_trace_words(x->nl, x->al, PLK_WARPS_PER_CTA) * 2;
-		if (plk_trace_words(x->nl, x->al, PLK_WARPS_PER_CTA) * 2 > max_trace)
-			max_trace = plk_trace_words(x->nl, x->al, PLK_WARPS_PER_CTA) * 2;
+		trace_total += plk_trace_words(x->nl, x->al, PLK_WARPS_PER_CTA, J->rows) * 2;
+		if (plk_trace_words(x->nl, x->al, PLK_WARPS_PER_CTA, J->rows) * 2 > max_trace)
+			max_trace = plk_trace_words(x->nl, x->al, PLK_WARPS_PER_CTA, J->rows) * 2;
 	}
 	if (max_trace > e->trace_budget) {
 		pl_set_error("one job needs %lld trace bytes, over the budget of %lld", (long long)max_trace, (long long)e->trace_budget);
@@ -307,7 +331,7 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 		int32_t best = 0;
 		for (w = 1; w < n_waves; ++w) if (wave_bytes[w] < wave_bytes[best]) best = w;
 		e->hwave[j] = best;
-		wave_bytes[best] += plk_trace_words(e->hj[j].nl, e->hj[j].al, PLK_WARPS_PER_CTA) * 2;
+		wave_bytes[best] += plk_trace_words(e->hj[j].nl, e->hj[j].al, PLK_WARPS_PER_CTA, e->hj[j].rows) * 2;
 		wave_cells[best] += (int64_t)(e->hj[j].nl - 2) * e->hj[j].al;
 	}
 	/* 3. cooperative or solo, trace offsets inside each wave's arena */
@@ -316,10 +340,10 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 		const int32_t j = sorted[q];
 		plk_job_t *J = &e->hj[j];
 		const int64_t cells = (int64_t)(J->nl - 2) * J->al, share = wave_cells[e->hwave[j]] / slots;
-		if (J->al >= 200 && J->nl - 2 >= 32 * PLK_WARPS_PER_CTA * PLK_DP_ROWS && (double)cells > share * pl_coop_ratio())
+		if (J->al >= 200 && J->nl - 2 >= 32 * PLK_WARPS_PER_CTA * J->rows && (double)cells > share * e->coop_ratio)
 			J->nw = PLK_WARPS_PER_CTA;
 		J->trace_off = wave_bytes[e->hwave[j]] / 2;
-		wave_bytes[e->hwave[j]] += (plk_trace_words(J->nl, J->al, J->nw) * 2 + 15) / 16 * 16;
+		wave_bytes[e->hwave[j]] += (plk_trace_words(J->nl, J->al, J->nw, J->rows) * 2 + 15) / 16 * 16;
 	}
 	{
 		int64_t need_trace = 0;
@@ -339,16 +363,19 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 	{
 		int32_t pos = 0;
 		for (w = 0; w < n_waves; ++w) {
-			int m;
-			for (m = 0; m < 3; ++m) {
-				int pass;
-				for (pass = 0; pass < 2; ++pass)
-					for (q = 0; q < n; ++q) {
-						const int32_t j = sorted[q];
-						const plk_job_t *J = &e->hj[j];
-						if (e->hwave[j] == w && J->mode == m && (J->nw > 1) == (pass == 0)) e->horder[pos++] = j;
-					}
-			}
+			int m, r;
+			for (m = 0; m < 3; ++m)
+				for (r = 0; r < 2; ++r) {
+					const int rows = r == 0 ? 8 : 4;
+					int pass;
+					for (pass = 0; pass < 2; ++pass)
+						for (q = 0; q < n; ++q) {
+							const int32_t j = sorted[q];
+							const plk_job_t *J = &e->hj[j];
+							if (e->hwave[j] == w && J->mode == m && J->rows == rows && (J->nw > 1) == (pass == 0))
+								e->horder[pos++] = j;
+						}
+				}
 		}
 	}
 	CK(cudaMemcpyAsync(e->jobs.p, e->hj, sizeof(plk_job_t) * (size_t)n, cudaMemcpyHostToDevice, st));
@@ -361,26 +388,29 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 		int32_t pos = 0;
 		for (w = 0; w < n_waves; ++w) {
 			const int32_t wave_start = pos;
-			int m;
-			for (m = 0; m < 3; ++m) {
-				int32_t n_coop = 0, n_solo = 0;
-				while (pos + n_coop < n && e->hwave[e->horder[pos + n_coop]] == w && e->hj[e->horder[pos + n_coop]].mode == m &&
-						e->hj[e->horder[pos + n_coop]].nw > 1) ++n_coop;
-				while (pos + n_coop + n_solo < n && e->hwave[e->horder[pos + n_coop + n_solo]] == w &&
-						e->hj[e->horder[pos + n_coop + n_solo]].mode == m) ++n_solo;
-				if (n_coop + n_solo > 0) {
-					const int32_t *ord = (const int32_t*)e->order.p + pos;
-					const int64_t stride = ((int64_t)max_al + 1) * PLK_RING_INTS;
-					const int32_t ctas = e->n_sm * e->ctas_per_sm[m];
-					PL_TIME(e, st, 1);
-					CKK(plk_splice_dp((plk_job_t*)e->jobs.p, ord, n_coop, ord + n_coop, n_solo, (int32_t*)e->counters.p,
-							(const uint8_t*)e->prep.p, (uint16_t*)e->trace.p, (int32_t*)e->ring.p, stride, ctas, m, &P, st));
-					PL_TIME(e, st, 1);
-					++e->last_dp_launches;
-					wave_n_coop += n_coop;
+			int m, r;
+			for (m = 0; m < 3; ++m)
+				for (r = 0; r < 2; ++r) {
+					const int rows = r == 0 ? 8 : 4;
+					int32_t n_coop = 0, n_solo = 0;
+#define PL_IN_GROUP(x) (e->hwave[e->horder[(x)]] == w && e->hj[e->horder[(x)]].mode == m && e->hj[e->horder[(x)]].rows == rows)
+					while (pos + n_coop < n && PL_IN_GROUP(pos + n_coop) && e->hj[e->horder[pos + n_coop]].nw > 1) ++n_coop;
+					while (pos + n_coop + n_solo < n && PL_IN_GROUP(pos + n_coop + n_solo)) ++n_solo;
+#undef PL_IN_GROUP
+					if (n_coop + n_solo > 0) {
+						const int32_t *ord = (const int32_t*)e->order.p + pos;
+						const int64_t stride = ((int64_t)max_al + 1) * PLK_RING_INTS;
+						const int32_t ctas = e->n_sm * e->ctas_per_sm[m][r];
+						PL_TIME(e, st, 1);
+						CKK(plk_splice_dp((plk_job_t*)e->jobs.p, ord, n_coop, ord + n_coop, n_solo, (int32_t*)e->counters.p,
+								(const uint8_t*)e->prep.p, (uint16_t*)e->trace.p, (int32_t*)e->ring.p, stride, ctas, m, rows,
+								&P, st));
+						PL_TIME(e, st, 1);
+						++e->last_dp_launches;
+						wave_n_coop += n_coop;
+					}
+					pos += n_coop + n_solo;
 				}
-				pos += n_coop + n_solo;
-			}
 			PL_TIME(e, st, 2);
 			CKK(plk_traceback((plk_job_t*)e->jobs.p, (const int32_t*)e->order.p + wave_start, pos - wave_start,
 					(const uint16_t*)e->trace.p, (uint32_t*)e->tmp.p, st));
@@ -408,6 +438,70 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 	ok = 1;
 fail:
 	free(wave_bytes), free(wave_cells);
+	return ok;
+}
+
+PL_EXPORT void pl_engine_set_tuning(pl_engine_t *e, int32_t r4_rows, double coop_ratio)
+{
+	if (!e) return;
+	if (r4_rows >= 0) e->r4_rows = r4_rows;
+	if (coop_ratio > 0.0) e->coop_ratio = coop_ratio;
+}
+
+PL_EXPORT void pl_engine_get_tuning(const pl_engine_t *e, int32_t *r4_rows, double *coop_ratio)
+{
+	if (!e) return;
+	if (r4_rows) *r4_rows = e->r4_rows;
+	if (coop_ratio) *coop_ratio = e->coop_ratio;
+}
+
+static double pl_now(void)
+{
+	struct timespec ts;
+	clock_gettime(CLOCK_MONOTONIC, &ts);
+	return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+/* Autotuner of the batched global DP: runs the batch under every pair of (rows-per-lane
+ * bin boundary, cooperative-job ratio) of a small grid, keeps the fastest for this
+ * engine and reports it.  The batch should look like the workload (the same length
+ * distributions); its results are discarded. */
+PL_EXPORT int pl_engine_autotune(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n,
+		const uint8_t *nt, const uint8_t *aa, const uint8_t *ss, int32_t *r4_rows_out, double *coop_ratio_out)
+{
+	static const int32_t r4s[] = { 0, 1536, 3072, 6144, 12288 };
+	static const double ratios[] = { 0.5, 0.7, 1.0 };
+	pl_splice_result_t *res = 0;
+	uint32_t *cig = 0;
+	int64_t cap = 0, total = 0;
+	int32_t q, best_r4 = e ? e->r4_rows : 0;
+	double best_ratio = e ? e->coop_ratio : 0.7, best_t = 1e30;
+	int a, b, ok = 0, timing;
+	if (!e || n <= 0) { pl_set_error("autotune: no engine or empty batch"); return 0; }
+	CK(cudaSetDevice(e->device));
+	for (q = 0; q < n; ++q) cap += (int64_t)jobs[q].al + 64;
+	CK(cudaMalloc((void**)&res, sizeof(pl_splice_result_t) * (size_t)n));
+	CK(cudaMalloc((void**)&cig, sizeof(uint32_t) * (size_t)cap));
+	timing = e->timing, e->timing = 0;
+	if (!pl_run(e, opt, jobs, n, nt, aa, ss, res, cig, cap, &total, e->stream)) goto done;  /* warm-up */
+	for (a = 0; a < (int)(sizeof(r4s) / sizeof(r4s[0])); ++a)
+		for (b = 0; b < (int)(sizeof(ratios) / sizeof(ratios[0])); ++b) {
+			double t0, t;
+			e->r4_rows = r4s[a], e->coop_ratio = ratios[b];
+			t0 = pl_now();
+			if (!pl_run(e, opt, jobs, n, nt, aa, ss, res, cig, cap, &total, e->stream)) goto done;
+			t = pl_now() - t0;
+			if (t < best_t) best_t = t, best_r4 = r4s[a], best_ratio = ratios[b];
+		}
+	ok = 1;
+done:
+	e->timing = timing;
+	e->r4_rows = best_r4, e->coop_ratio = best_ratio;
+	if (r4_rows_out) *r4_rows_out = best_r4;
+	if (coop_ratio_out) *coop_ratio_out = best_ratio;
+fail:
+	if (res) cudaFree(res);
+	if (cig) cudaFree(cig);
 	return ok;
 }
 

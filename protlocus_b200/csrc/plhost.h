@@ -21,7 +21,9 @@ int dbuf_ensure(dbuf_t *b, size_t need);
 void dbuf_free(dbuf_t *b);
 
 struct pl_engine_s {
-	int device, n_sm, ctas_per_sm[3];
+	int device, n_sm, ctas_per_sm[3][2];   /* per DP width mode, per rows per lane (8, 4) */
+	int32_t r4_rows;                        /* jobs with at most this many DP rows take 4 rows per lane */
+	double coop_ratio;                      /* cooperative-job threshold (pl_coop_ratio by default) */
 	cudaStream_t stream;
 	int64_t trace_budget;
 	dbuf_t jobs, order, counters, prep, trace, ring, tmp, total, nt, aa, ss, res, cig;
@@ -64,6 +66,8 @@ struct pl_engine_s {
 	(e)->ev_kind[(e)->n_ev] = (k); cudaEventRecord((e)->ev[(e)->n_ev++], (st)); } } while (0)
 
 void pl_set_error(const char *fmt, ...);
+double pl_coop_ratio(void);
+int32_t pl_r4_rows(void);
 int pl_params(const ns_opt_t *opt, plk_params_t *p, int for_ext);
 int pl_max_sub(const ns_opt_t *opt);
 void pl_ext_engine_free(pl_engine_t *e);

@@ -14,9 +14,9 @@ extern "C" {
 
 #define PLK_WARPS_PER_CTA 8     /* a CTA is one 256-lane wavefront (large jobs) or 8 independent warps */
 #define PLK_ROWS 8              /* DP rows owned by one lane of a strip (extension DP) */
-#ifndef PLK_DP_ROWS
-#define PLK_DP_ROWS 8           /* DP rows owned by one lane of a strip (global DP and its trace layout) */
-#endif
+/* the global DP gives every lane of a strip PLK_DP_ROWS (8) or 4 rows, chosen per job
+ * (plk_job_t.rows): the trace layout, the kernel instance and the traceback follow */
+#define PLK_DP_ROWS 8
 #define PLK_RING_INTS 12        /* column state handed from one strip to the next (9 used, 48-byte entries) */
 
 /* scoring parameters and lookup tables, passed to kernels by value */
@@ -42,7 +42,7 @@ typedef struct {
 	int32_t mode;                    /* 0: int16 (lower clamp suffices), 1: int32 (gs32b), 2: int16 both clamps */
 	int32_t slen;                    /* segment length of the striping being reproduced */
 	int32_t nw;                      /* warps cooperating on the job: 1 or PLK_WARPS_PER_CTA */
-	int32_t pad0;
+	int32_t rows;                    /* DP rows per lane of a strip: 8 or 4 */
 	int32_t score, n_tmp;            /* outputs of the DP / traceback */
 	int32_t status, pad;
 } plk_job_t;
@@ -77,10 +77,10 @@ static inline int64_t plk_prep_bytes(int32_t nl, int32_t al)
 	return ((int64_t)nl + al + 2 * ((int64_t)nl + 1) + 7) / 8 * 8;
 }
 
-/* trace words of a job in the strip layout (strips of 32*nw*PLK_DP_ROWS rows) */
-static inline int64_t plk_trace_words(int32_t nl, int32_t al, int32_t nw)
+/* trace words of a job in the strip layout (strips of 32*nw*rows rows) */
+static inline int64_t plk_trace_words(int32_t nl, int32_t al, int32_t nw, int32_t rows)
 {
-	int64_t h = 32LL * nw * PLK_DP_ROWS, nr = (int64_t)nl - 2, strips = (nr + h - 1) / h;
+	int64_t h = 32LL * nw * rows, nr = (int64_t)nl - 2, strips = (nr + h - 1) / h;
 	return strips * h * (int64_t)al;
 }
 
@@ -91,7 +91,7 @@ int plk_prep(const plk_job_t *jobs, int32_t n_jobs, const uint8_t *nt, const uin
  * counters: 2 ints of device scratch.  ring: PLK_WARPS_PER_CTA * n_ctas * ring_stride_ints ints. */
 int plk_splice_dp(plk_job_t *jobs, const int32_t *order_coop, int32_t n_coop, const int32_t *order_solo,
 		int32_t n_solo, int32_t *counters, const uint8_t *prep, uint16_t *trace, int32_t *ring,
-		int64_t ring_stride_ints, int32_t n_ctas, int32_t mode, const plk_params_t *p, void *stream);
+		int64_t ring_stride_ints, int32_t n_ctas, int32_t mode, int32_t rows, const plk_params_t *p, void *stream);
 int plk_traceback(plk_job_t *jobs, const int32_t *order, int32_t n_order, const uint16_t *trace,
 		uint32_t *tmp, void *stream);
 int plk_scan_compact(plk_job_t *jobs, int32_t n_jobs, const uint32_t *tmp, uint32_t *out, int64_t out_cap,
@@ -147,7 +147,7 @@ int plk_rc_forward(const plk_rc_prof_t *prof, const plk_rc_pep_t *pep, const uin
 		void *stream);
 int plk_rc_smem_per_warp(int32_t max_m);
 /* CTAs of the DP kernel that fit on one SM at once (occupancy) */
-int plk_dp_ctas_per_sm(int32_t mode);
+int plk_dp_ctas_per_sm(int32_t mode, int32_t rows);
 uint64_t plk_launches(void);
 
 /* BF16 GEMM on the tensor cores (mlp.cu): C = A . B^T + bias, optional ReLU / mask,

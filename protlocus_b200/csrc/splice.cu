@@ -62,22 +62,17 @@ __global__ void k_prep(const plk_job_t *__restrict__ jobs, int n_jobs, const uin
 /* ------------------------------------------------------------------ the DP */
 
 /* the R trace words of a lane and step, stored and loaded as one vector */
-#if PLK_DP_ROWS == 8
-typedef uint4 trace_vec_t;
-#define PLK_DP_MIN_CTAS 2
-#elif PLK_DP_ROWS == 4
-typedef uint2 trace_vec_t;
-#define PLK_DP_MIN_CTAS 3
-#else
-#error "PLK_DP_ROWS must be 4 or 8"
-#endif
+template <int R> struct TraceVec;
+template <> struct TraceVec<8> { typedef uint4 T; };
+template <> struct TraceVec<4> { typedef uint2 T; };
 
-__device__ __forceinline__ void store_trace(uint16_t *p, const unsigned (&z)[PLK_DP_ROWS])
+template <int R>
+__device__ __forceinline__ void store_trace(uint16_t *p, const unsigned (&z)[R])
 {
-	uint32_t w[PLK_DP_ROWS / 2];
+	uint32_t w[R / 2];
 #pragma unroll
-	for (int q = 0; q < PLK_DP_ROWS / 2; ++q) w[q] = (z[2 * q] & 0xffffu) | (z[2 * q + 1] << 16);
-	*(trace_vec_t*)p = *(const trace_vec_t*)w;
+	for (int q = 0; q < R / 2; ++q) w[q] = (z[2 * q] & 0xffffu) | (z[2 * q + 1] << 16);
+	*(typename TraceVec<R>::T*)p = *(const typename TraceVec<R>::T*)w;
 }
 
 struct DpShared {
@@ -116,12 +111,12 @@ __device__ __forceinline__ unsigned sign_bytes(int a, int b)
 	return d;
 }
 
-template <int NW>
-__device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[PLK_DP_ROWS], const int ah1, const int ah2,
-		const int ah3, const bool row2, const int *__restrict__ sct_b, const int (&code)[PLK_DP_ROWS],
-		const int (&gi)[PLK_DP_ROWS], const int (&dn)[PLK_DP_ROWS + 2], const int (&ac)[PLK_DP_ROWS + 2],
-		int (&ip)[PLK_DP_ROWS], int (&lh)[PLK_DP_ROWS], const int (&ic)[PLK_DP_ROWS], const int c16[8],
-		int (&o)[9], unsigned (&z)[PLK_DP_ROWS], int (&hn)[PLK_DP_ROWS])
+template <int NW, int R>
+__device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[R], const int ah1, const int ah2,
+		const int ah3, const bool row2, const int *__restrict__ sct_b, const int (&code)[R],
+		const int (&gi)[R], const int (&dn)[R + 2], const int (&ac)[R + 2],
+		int (&ip)[R], int (&lh)[R], const int (&ic)[R], const int c16[8],
+		int (&o)[9], unsigned (&z)[R], int (&hn)[R])
 {
 	/* The integer pipe is the bound, so the update is written in the DPX forms that
 	 * issue one instruction each: __viaddmax_s32 (max(a + b, c)) for every clamped
@@ -130,7 +125,7 @@ __device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[PLK_D
 	 * candidates into the running maximum at once (their tag adds can issue on the
 	 * FMA pipe).  The maximum of the encoded candidates does not depend on the
 	 * order in which they are folded. */
-	constexpr int R = PLK_DP_ROWS, N16 = -32768 * 16;
+	constexpr int N16 = -32768 * 16;
 	const int GO = c16[0], GE = c16[1], IO = c16[2], F6 = c16[3], F7 = c16[4], F8 = c16[5], F9 = c16[6], FS = c16[7];
 	int h1 = in[0], h2 = in[1], h3 = in[2], d1 = in[3], d2 = in[4], d3 = in[5], va = in[6], vb = in[7], vc = in[8];
 #pragma unroll
@@ -189,15 +184,14 @@ __device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[PLK_D
 
 /* Straightforward formulation for the 32-bit width (MODE 1) and the doubly
  * clamped int16 case (MODE 2). */
-template <int MODE>
-__device__ __forceinline__ void cells_plain(const int (&in)[9], int (&hm)[PLK_DP_ROWS], const int ah1, const int ah2,
+template <int MODE, int R>
+__device__ __forceinline__ void cells_plain(const int (&in)[9], int (&hm)[R], const int ah1, const int ah2,
 		const int ah3, const bool row2, const bool seg, const bool first, const int *__restrict__ sct_b,
-		const int (&code)[PLK_DP_ROWS], const int (&gi)[PLK_DP_ROWS], const int (&dn)[PLK_DP_ROWS + 2],
-		const int (&ac)[PLK_DP_ROWS + 2], int (&ip)[PLK_DP_ROWS], int (&lh)[PLK_DP_ROWS], int (&ic)[PLK_DP_ROWS],
-		const plk_params_t &P, int (&o)[9], unsigned (&z)[PLK_DP_ROWS], int (&hn)[PLK_DP_ROWS])
+		const int (&code)[R], const int (&gi)[R], const int (&dn)[R + 2],
+		const int (&ac)[R + 2], int (&ip)[R], int (&lh)[R], int (&ic)[R],
+		const plk_params_t &P, int (&o)[9], unsigned (&z)[R], int (&hn)[R])
 {
 	typedef Ar<MODE> A;
-	constexpr int R = PLK_DP_ROWS;
 	const int NEG = A::NEG, go = P.go, ge = P.ge, goe = P.go + P.ge, io = P.io, fs = P.fs;
 	int h1 = in[0], h2 = in[1], h3 = in[2], d1 = in[3], d2 = in[4], d3 = in[5], va = in[6], vb = in[7], vc = in[8];
 #pragma unroll
@@ -284,12 +278,12 @@ __device__ __forceinline__ void cells_plain(const int (&in)[9], int (&hm)[PLK_DP
 
 /* One DP job on a wavefront of NW warps (32*NW lanes).  All threads of the
  * group call this with the same job; `L` is the lane index in the wavefront. */
-template <int MODE, int NW>
+template <int MODE, int NW, int R>
 __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t *__restrict__ prep,
 		uint16_t *__restrict__ trace, int32_t *__restrict__ myring, DpShared &sh, const plk_params_t &P,
 		const int L, const int wib)
 {
-	constexpr int R = PLK_DP_ROWS, NL = 32 * NW, HS = NL * R;
+	constexpr int NL = 32 * NW, HS = NL * R;
 	constexpr int SC = MODE == 0 ? 16 : 1;                  /* value scale of the mode */
 	const int NEG = Ar<MODE>::NEG * SC;
 	const int lane = L & 31, w = L >> 5;
@@ -370,9 +364,9 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 #pragma unroll
 					for (int r = 0; r < R; ++r) ic[r] = max(ic[r] - GE16, NEG);
 				}
-				cells_scaled<NW>(in, hm, ah1, ah2, ah3, row2, sct_b, code, gi, dn, ac, ip, lh, ic, c16, o, z, hn);
+				cells_scaled<NW, R>(in, hm, ah1, ah2, ah3, row2, sct_b, code, gi, dn, ac, ip, lh, ic, c16, o, z, hn);
 			} else {
-				cells_plain<MODE>(in, hm, ah1, ah2, ah3, row2, seg, first, sct_b, code, gi, dn, ac, ip, lh, ic, P,
+				cells_plain<MODE, R>(in, hm, ah1, ah2, ah3, row2, seg, first, sct_b, code, gi, dn, ac, ip, lh, ic, P,
 						o, z, hn);
 			}
 			if (c == al - 1) { /* the final score H(nl-1, al-1) */
@@ -382,7 +376,7 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 					if (r == rl) J->score = MODE == 0 ? hn[r] >> 4 : hn[r];
 			}
 			/* trace: one store of R 16-bit words per lane, contiguous across the lanes of a strip */
-			store_trace(tr + (((int64_t)k * al + dcol) * NL + L) * R, z);
+			store_trace<R>(tr + (((int64_t)k * al + dcol) * NL + L) * R, z);
 			if (L == NL - 1) {
 				int32_t *e = myring + (int64_t)c * PLK_RING_INTS;
 #pragma unroll
@@ -418,8 +412,8 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 /* Persistent DP kernel: first every CTA takes cooperative jobs (a whole CTA per
  * job) until that queue is empty, then every warp takes solo jobs.  Both queues
  * are sorted by decreasing size on the host (longest-processing-time first). */
-template <int MODE>
-__global__ void __launch_bounds__(32 * PLK_WARPS_PER_CTA, PLK_DP_MIN_CTAS)
+template <int MODE, int R>
+__global__ void __launch_bounds__(32 * PLK_WARPS_PER_CTA, R == 8 ? 2 : 3)
 k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop, int n_coop,
 		const int32_t *__restrict__ order_solo, int n_solo, int32_t *counters,
 		const uint8_t *__restrict__ prep, uint16_t *__restrict__ trace, int32_t *__restrict__ ring,
@@ -438,7 +432,7 @@ k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop
 		const int idx = sh.job;
 		__syncthreads();
 		if (idx >= n_coop) break;
-		dp_job<MODE, PLK_WARPS_PER_CTA>(jobs + order_coop[idx], prep, trace,
+		dp_job<MODE, PLK_WARPS_PER_CTA, R>(jobs + order_coop[idx], prep, trace,
 				ring + (int64_t)blockIdx.x * PLK_WARPS_PER_CTA * ring_stride, sh, P, threadIdx.x, wib);
 		__syncthreads();
 	}
@@ -448,7 +442,7 @@ k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop
 		if (lane == 0) idx = atomicAdd(&counters[1], 1);
 		idx = __shfl_sync(FULL, idx, 0);
 		if (idx >= n_solo) break;
-		dp_job<MODE, 1>(jobs + order_solo[idx], prep, trace, myring, sh, P, lane, wib);
+		dp_job<MODE, 1, R>(jobs + order_solo[idx], prep, trace, myring, sh, P, lane, wib);
 		__syncwarp();
 	}
 }
@@ -468,43 +462,67 @@ __device__ __forceinline__ void tb_push(uint32_t *out, int &n, uint32_t op, int 
  * stages the trace words around the current cell in shared memory -- a tile of
  * 8 row-chunks (64 rows) x 32 columns, one coalesced round of 16-byte loads --
  * and lane 0 walks inside the tile until the path leaves it. */
-#define TB_CHUNKS (64 / PLK_DP_ROWS)
+#define TB_GROUPS 8   /* 8-row groups per tile: 64 rows */
 #define TB_COLS 32
 #define TB_WARPS 8
+
+/* the R trace words of chunk ch (R rows of one lane of a strip) in column col, into w[0..R) */
+__device__ __forceinline__ void tb_load_chunk(const uint16_t *__restrict__ tr, int R, int nlanes, int al, int ch, int col,
+		uint16_t (&w)[8])
+{
+	const int ra = ch * R, hs = nlanes * R, k = ra / hs, t = ch % nlanes;
+	int d = col + t;
+	if (d >= al) d %= al;
+	const uint16_t *src = tr + (((int64_t)k * al + d) * nlanes + t) * R;
+	if (R == 8) {
+		const uint4 v = *(const uint4*)src;
+		*(uint4*)w = v;
+	} else {
+		const uint2 v = *(const uint2*)src;
+		*(uint2*)w = v;
+	}
+}
+
 __global__ void __launch_bounds__(32 * TB_WARPS) k_traceback(plk_job_t *__restrict__ jobs,
 		const int32_t *__restrict__ order, int n_order, const uint16_t *__restrict__ trace, uint32_t *__restrict__ tmp)
 {
-	__shared__ trace_vec_t s_tile[TB_WARPS][TB_CHUNKS][TB_COLS]; /* the trace words of R rows per entry */
+	__shared__ uint4 s_tile[TB_WARPS][TB_GROUPS][TB_COLS]; /* the trace words of 8 rows per entry */
 	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
 	const int q = blockIdx.x * TB_WARPS + wib;
 	if (q >= n_order) return;
 	plk_job_t *J = jobs + order[q];
-	const int nl = J->nl, al = J->al;
+	const int nl = J->nl, al = J->al, R = J->rows;
 	const uint16_t *tr = trace + J->trace_off;
 	uint32_t *out = tmp + J->tmp_off;
-	const int nlanes = 32 * J->nw, hs = nlanes * PLK_DP_ROWS;
+	const int nlanes = 32 * J->nw;
 	int i = nl - 1, j = al - 1, last = 0, n = 0;
 	while (i >= 2 && j >= 0) {
-		/* stage the tile whose top-right corner holds (i, j) */
-		const int qc = (i - 2) / PLK_DP_ROWS, jc = j;
+		/* stage the tile whose top-right corner holds (i, j): 8-row groups, one or two chunks each */
+		const int qc = (i - 2) / 8, jc = j;
 #pragma unroll
-		for (int m = 0; m < TB_CHUNKS * TB_COLS / 32; ++m) {
+		for (int m = 0; m < TB_GROUPS * TB_COLS / 32; ++m) {
 			const int idx = lane + 32 * m, dq = idx / TB_COLS, dc = idx % TB_COLS;
-			const int ch = qc - dq, col = jc - dc;
-			if (ch >= 0 && col >= 0) {
-				const int ra = ch * PLK_DP_ROWS, k = ra / hs, t = (ra / PLK_DP_ROWS) % nlanes;
-				int d = col + t;
-				if (d >= al) d %= al;
-				s_tile[wib][dq][dc] = *(const trace_vec_t*)(tr + (((int64_t)k * al + d) * nlanes + t) * PLK_DP_ROWS);
+			const int g = qc - dq, col = jc - dc;
+			if (g >= 0 && col >= 0) {
+				__align__(16) uint16_t w[8];
+				if (R == 8) tb_load_chunk(tr, 8, nlanes, al, g, col, w);
+				else {
+					/* chunks 2g and 2g+1 sit in the same strip (nlanes is even) */
+					__align__(8) uint16_t w2[8];
+					tb_load_chunk(tr, 4, nlanes, al, 2 * g, col, w);
+					tb_load_chunk(tr, 4, nlanes, al, 2 * g + 1, col, w2);
+					*(uint2*)(w + 4) = *(const uint2*)w2;
+				}
+				s_tile[wib][dq][dc] = *(const uint4*)w;
 			}
 		}
 		__syncwarp();
 		if (lane == 0) {
 			while (i >= 2 && j >= 0) {
-				const int dq = qc - (i - 2) / PLK_DP_ROWS, dc = jc - j;
-				if (dq >= TB_CHUNKS || dc >= TB_COLS) break;
+				const int dq = qc - (i - 2) / 8, dc = jc - j;
+				if (dq >= TB_GROUPS || dc >= TB_COLS) break;
 				const uint16_t *cell = (const uint16_t*)&s_tile[wib][dq][dc];
-				const int x = cell[(i - 2) % PLK_DP_ROWS];
+				const int x = cell[(i - 2) % 8];
 				const int state = last != 0 ? last : (x >> 14 & 1) ? 1 : 15 - (x & 0xf);
 				const int ext = state >= 1 && state <= 5 ? (x >> tb_ext_bit(state)) & 1 : 0;
 				switch (state) {
@@ -527,29 +545,26 @@ __global__ void __launch_bounds__(32 * TB_WARPS) k_traceback(plk_job_t *__restri
 		__syncwarp();
 		/* Inside an intron run (A/B/C extended: the path climbs column j one row per
 		 * step while the state's extension bit stays set) the warp scans 32*R rows of
-		 * the column at once: each lane reads one R-row trace word, and the run ends at
-		 * the highest row <= i whose bit is clear.  The rows of the run become one
-		 * merged N/U/V op, exactly what the row-by-row walk pushes. */
+		 * the column at once: each lane reads one R-row chunk, and the run ends at the
+		 * highest row <= i whose bit is clear.  The rows of the run become one merged
+		 * N/U/V op, exactly what the row-by-row walk pushes. */
 		while (last >= 3 && last <= 5 && i >= 2 && j >= 0) {
-			const int ch_top = (i - 2) / PLK_DP_ROWS, ch = ch_top - lane;
+			const int ch_top = (i - 2) / R, ch = ch_top - lane;
 			const int bit = tb_ext_bit(last);
 			int end_row = -1;
 			if (ch >= 0) {
-				const int ra = ch * PLK_DP_ROWS, k = ra / hs, t = (ra / PLK_DP_ROWS) % nlanes;
-				int d = j + t;
-				if (d >= al) d %= al;
-				const trace_vec_t wv = *(const trace_vec_t*)(tr + (((int64_t)k * al + d) * nlanes + t) * PLK_DP_ROWS);
-				const uint16_t *wd = (const uint16_t*)&wv;
+				__align__(16) uint16_t w[8];
+				tb_load_chunk(tr, R, nlanes, al, ch, j, w);
+				const int ra = ch * R;
 #pragma unroll
-				for (int r = PLK_DP_ROWS - 1; r >= 0; --r) {
+				for (int r = 7; r >= 0; --r) {
 					const int row = ra + 2 + r;
-					const uint32_t x = wd[r];
-					if (end_row < 0 && row <= i && !((x >> bit) & 1u)) end_row = row;
+					if (r < R && end_row < 0 && row <= i && !((w[r] >> bit) & 1u)) end_row = row;
 				}
 			}
 #pragma unroll
 			for (int o = 16; o >= 1; o >>= 1) end_row = max(end_row, __shfl_xor_sync(FULL, end_row, o));
-			const int low = max(2, (ch_top - 31) * PLK_DP_ROWS + 2);
+			const int low = max(2, (ch_top - 31) * R + 2);
 			const int op = last == 3 ? NS_CIGAR_N : (last == 4 ? NS_CIGAR_U : NS_CIGAR_V);
 			if (end_row >= low) { /* the run ends at end_row: its step clears the state (and moves j for U/V) */
 				if (lane == 0) tb_push(out, n, op, i - end_row + 1);
@@ -629,28 +644,38 @@ extern "C" int plk_prep(const plk_job_t *jobs, int32_t n_jobs, const uint8_t *nt
 	return (int)cudaGetLastError();
 }
 
-extern "C" int plk_dp_ctas_per_sm(int32_t mode)
+template <int MODE, int R>
+static int dp_occupancy()
 {
 	int n = 0;
-	cudaError_t e;
-	if (mode == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_splice_dp<1>, 32 * PLK_WARPS_PER_CTA, 0);
-	else if (mode == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_splice_dp<2>, 32 * PLK_WARPS_PER_CTA, 0);
-	else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_splice_dp<0>, 32 * PLK_WARPS_PER_CTA, 0);
+	const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_splice_dp<MODE, R>, 32 * PLK_WARPS_PER_CTA, 0);
 	return e == cudaSuccess ? n : -1;
+}
+
+extern "C" int plk_dp_ctas_per_sm(int32_t mode, int32_t rows)
+{
+	if (rows == 4) return mode == 1 ? dp_occupancy<1, 4>() : mode == 2 ? dp_occupancy<2, 4>() : dp_occupancy<0, 4>();
+	return mode == 1 ? dp_occupancy<1, 8>() : mode == 2 ? dp_occupancy<2, 8>() : dp_occupancy<0, 8>();
 }
 
 extern "C" int plk_splice_dp(plk_job_t *jobs, const int32_t *order_coop, int32_t n_coop, const int32_t *order_solo,
 		int32_t n_solo, int32_t *counters, const uint8_t *prep, uint16_t *trace, int32_t *ring,
-		int64_t ring_stride_ints, int32_t n_ctas, int32_t mode, const plk_params_t *p, void *stream)
+		int64_t ring_stride_ints, int32_t n_ctas, int32_t mode, int32_t rows, const plk_params_t *p, void *stream)
 {
 	if (n_coop + n_solo <= 0) return 0;
+	if (rows != 4 && rows != 8) return (int)cudaErrorInvalidValue;
 	cudaStream_t st = (cudaStream_t)stream;
 	cudaError_t e = cudaMemsetAsync(counters, 0, 2 * sizeof(int32_t), st);
 	if (e != cudaSuccess) return (int)e;
 	const dim3 grid(n_ctas), block(32 * PLK_WARPS_PER_CTA);
-	if (mode == 1) k_splice_dp<1><<<grid, block, 0, st>>>(jobs, order_coop, n_coop, order_solo, n_solo, counters, prep, trace, ring, ring_stride_ints, *p);
-	else if (mode == 2) k_splice_dp<2><<<grid, block, 0, st>>>(jobs, order_coop, n_coop, order_solo, n_solo, counters, prep, trace, ring, ring_stride_ints, *p);
-	else k_splice_dp<0><<<grid, block, 0, st>>>(jobs, order_coop, n_coop, order_solo, n_solo, counters, prep, trace, ring, ring_stride_ints, *p);
+#define DP_LAUNCH(M, RR) k_splice_dp<M, RR><<<grid, block, 0, st>>>(jobs, order_coop, n_coop, order_solo, n_solo, \
+		counters, prep, trace, ring, ring_stride_ints, *p)
+	if (rows == 4) {
+		if (mode == 1) DP_LAUNCH(1, 4); else if (mode == 2) DP_LAUNCH(2, 4); else DP_LAUNCH(0, 4);
+	} else {
+		if (mode == 1) DP_LAUNCH(1, 8); else if (mode == 2) DP_LAUNCH(2, 8); else DP_LAUNCH(0, 8);
+	}
+#undef DP_LAUNCH
 	__sync_fetch_and_add(&g_launches, 1ull);
 	return (int)cudaGetLastError();
 }

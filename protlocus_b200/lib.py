@@ -124,6 +124,11 @@ def load() -> C.CDLL:
     lib.pl_rc_score_host.restype = C.c_int
     lib.pl_rc_last_cells.argtypes = [C.c_void_p]
     lib.pl_rc_last_cells.restype = C.c_int64
+    lib.pl_engine_set_tuning.argtypes = [C.c_void_p, C.c_int32, C.c_double]
+    lib.pl_engine_get_tuning.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+    lib.pl_engine_autotune.argtypes = [C.c_void_p, C.POINTER(NsOpt), C.POINTER(SpliceJob), C.c_int32, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+    lib.pl_engine_autotune.restype = C.c_int
     lib.pl_pf_model_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_uint64]
     lib.pl_pf_model_create.restype = C.c_void_p
     lib.pl_pf_model_destroy.argtypes = [C.c_void_p]
@@ -200,6 +205,15 @@ class Engine:
     @property
     def stream(self) -> int:
         return self.lib.pl_engine_stream(self.h) or 0
+
+    def set_tuning(self, r4_rows: int = -1, coop_ratio: float = 0.0):
+        """Rows-per-lane bin boundary and cooperative-job ratio of the global DP (see plgpu.h)."""
+        self.lib.pl_engine_set_tuning(self.h, int(r4_rows), float(coop_ratio))
+
+    def tuning(self):
+        r, c = C.c_int32(), C.c_double()
+        self.lib.pl_engine_get_tuning(self.h, C.byref(r), C.byref(c))
+        return {"r4_rows": r.value, "coop_ratio": c.value}
 
     def last_plan(self):
         w, c, d = C.c_int32(), C.c_int32(), C.c_int32()

@@ -43,6 +43,10 @@ def _check(engine, oracle, opt, pairs, ss=None, fn="gs_auto"):
 
 def test_golden_vectors(engine, oracle, golden):
     """Every global-DP golden vector produced by the reference, run through the bulk path."""
+    _golden(engine, oracle, golden)
+
+
+def _golden(engine, oracle, golden):
     by_opt = {}
     for c in golden["cases"]:
         if c["opt"].get("flag", NS_F_CIGAR) & (NS_F_EXT_LEFT | NS_F_EXT_RIGHT):
@@ -149,6 +153,65 @@ def test_cooperative_jobs_and_waves(oracle):
         _check(e, oracle, Options(flag=NS_F_CIGAR), pairs)
         plan = e.last_plan()
         assert plan["coop"] > 0 and plan["waves"] > 1, plan
+    finally:
+        e.close()
+
+
+@pytest.mark.parametrize("r4_rows,ratio", [(1 << 30, 0.7), (1 << 30, 0.05), (3000, 0.3)])
+def test_four_rows_per_lane(oracle, golden, r4_rows, ratio):
+    """Jobs on the 4-rows-per-lane kernels (all of them, or those up to 3000 rows beside
+    8-row ones), solo and cooperative, over golden vectors, planted loci and a forced
+    multi-wave plan."""
+    e = L.Engine(0, trace_budget_bytes=64 << 20)
+    try:
+        e.set_tuning(r4_rows, ratio)
+        assert e.tuning()["r4_rows"] == r4_rows
+        rng = np.random.default_rng(31)
+        pairs = []
+        for q in range(8):
+            al = int(rng.integers(200, 480))
+            nt, aa = W.single_locus(seed=1300 + q, al=al, window=int(rng.integers(2500, 12000)), n_intron=3)
+            pairs += [(nt, aa), (W.revcomp(nt), aa)]
+        pairs += [W.random_pair(rng, max_al=60) for _ in range(150)]
+        _check(e, oracle, Options(flag=NS_F_CIGAR), pairs)
+        plan = e.last_plan()
+        assert plan["coop"] > 0, plan
+        _golden(e, oracle, golden)
+    finally:
+        e.close()
+
+
+def test_autotune_picks_a_grid_point(oracle):
+    """The autotuner runs the batch under its grid, keeps a point of it on the engine,
+    and the batch still comes out bit-exact under the kept tuning."""
+    torch = pytest.importorskip("torch")
+    import ctypes as C
+    from protlocus_b200.abi import SpliceJob
+    rng = np.random.default_rng(41)
+    pairs = []
+    for q in range(10):
+        al = int(rng.integers(200, 420))
+        nt, aa = W.single_locus(seed=1500 + q, al=al, window=int(rng.integers(1500, 9000)), n_intron=2)
+        pairs.append((nt, aa))
+    pairs += [W.random_pair(rng, max_al=60) for _ in range(100)]
+    n = len(pairs)
+    tab = (SpliceJob * n)()
+    nt_off = aa_off = 0
+    for q, (nt, aa) in enumerate(pairs):
+        tab[q].nt_off, tab[q].aa_off, tab[q].ss_off, tab[q].nl, tab[q].al = nt_off, aa_off, -1, len(nt), len(aa)
+        nt_off += len(nt)
+        aa_off += len(aa)
+    d_nt = torch.from_numpy(np.frombuffer(b"".join(p[0] for p in pairs), np.uint8).copy()).cuda()
+    d_aa = torch.from_numpy(np.frombuffer(b"".join(p[1] for p in pairs), np.uint8).copy()).cuda()
+    e = L.Engine(0)
+    try:
+        opt = Options(flag=NS_F_CIGAR)
+        r4, ratio = C.c_int32(), C.c_double()
+        assert e.lib.pl_engine_autotune(e.h, opt.ptr, tab, n, d_nt.data_ptr(), d_aa.data_ptr(), None, C.byref(r4),
+                                        C.byref(ratio)), L.error()
+        assert r4.value in (0, 1536, 3072, 6144, 12288) and ratio.value in (0.5, 0.7, 1.0)
+        assert e.tuning() == {"r4_rows": r4.value, "coop_ratio": ratio.value}
+        _check(e, oracle, opt, pairs)
     finally:
         e.close()
 
