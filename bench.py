@@ -1088,7 +1088,9 @@ def main_prefilter(args):
     model, meta = P.load_model(PF_MODEL, local)
     tau, margin, tau_fb = float(meta["tau"]), int(meta["margin"]), float(meta["tau_fb"])
     pipe = P.Pipeline(eng, cand)
-    plain, _, _ = pipe.dp(jobs)
+    if not args.no_autotune:
+        pipe.autotune_paths(model, tau, margin, tau_fb)
+    plain, _, _ = pipe.plain()
     for _ in range(max(3, args.warmup)):
         pipe.learned(model, tau, margin, 0.0, tau_fb)
     clocks = Clocks(local)
@@ -1114,7 +1116,7 @@ def main_prefilter(args):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        pipe.dp(jobs)
+        pipe.plain()
     torch.cuda.synchronize()
     t_plain = R.max((time.perf_counter() - t0) / args.steps)
     # end to end: candidate sequences from pinned host memory, pass flags back
@@ -1150,6 +1152,7 @@ def main_prefilter(args):
                            "model": f"4-layer BF16 MLP {model.hidden} wide, trained on "
                                     f"{int(meta['train_rows'])} plain-DP outcomes of seeds {meta['train_seeds']}",
                            "tau": tau, "margin_nt": margin, "tau_fallback": tau_fb,
+                           "tuning_plain": pipe.tune_plain, "tuning_learned": pipe.tune_learned,
                            "l2": "the candidate sequences (205 MB) and the DP trace arena exceed L2"},
                 "plain": {"value": round(n_all / t_plain, 1), "unit": "candidates/s", "ms_per_step": round(t_plain * 1e3, 2),
                           "cells_per_step": cells_plain},

@@ -200,6 +200,30 @@ class Pipeline:
         self.d_nt = torch.from_numpy(cand["nt"].copy()).to(dev)
         self.d_aa = torch.from_numpy(cand["aa"].copy()).to(dev)
         self.n = len(cand["jobs"])
+        self.tune_plain = self.tune_learned = None  # engine tuning per path (None: the engine's own)
+
+    def autotune(self, jobs: np.ndarray) -> dict:
+        """pl_engine_autotune over `jobs` (sequences resident on the device); returns the tuning."""
+        r4, ratio = C.c_int32(), C.c_double()
+        if not self.eng.lib.pl_engine_autotune(self.eng.h, self.opt.ptr, job_ptr(jobs), len(jobs), self.d_nt.data_ptr(),
+                                               self.d_aa.data_ptr(), None, C.byref(r4), C.byref(ratio)):
+            raise RuntimeError("pl_engine_autotune: " + L.error())
+        return {"r4_rows": r4.value, "coop_ratio": ratio.value}
+
+    def autotune_paths(self, model: "PrefilterModel", tau: float, margin: int, tau_fb: float):
+        """Separate engine tunings for the plain path (full windows) and the learned path
+        (tightened windows), each chosen by the autotuner on its own jobs."""
+        self.tune_plain = self.autotune(self.cand["jobs"])
+        feats, chain = self.features()
+        out = model.predict(feats, self.n)
+        o = out[: self.n, :3].cpu().numpy()
+        keep = np.nonzero(o[:, 0] >= _logit(tau))[0]
+        self.tune_learned = self.autotune(self.tightened(keep, o, chain[: self.n].cpu().numpy(), margin))
+        return self.tune_plain, self.tune_learned
+
+    def _use(self, tuning):
+        if tuning is not None:
+            self.eng.set_tuning(tuning["r4_rows"], tuning["coop_ratio"])
 
     def features(self):
         import torch
@@ -212,6 +236,11 @@ class Pipeline:
                                                   chain.data_ptr(), stream):
             raise RuntimeError("pl_pf_features_device: " + L.error())
         return feats, chain
+
+    def plain(self, bounds: bool = False):
+        """The plain path: the exact DP over every candidate's full window."""
+        self._use(self.tune_plain)
+        return self.dp(self.cand["jobs"], bounds)
 
     def dp(self, jobs: np.ndarray, bounds: bool = False):
         """Exact spliced DP with CIGAR over `jobs` (device-resident sequences): scores, and
@@ -289,10 +318,12 @@ class Pipeline:
         z = o[:, 0]
         keep = np.nonzero(z >= _logit(tau))[0]
         jobs = self.tightened(keep, o, ch, margin, rel)
+        self._use(self.tune_learned)
         sc, _, _ = self.dp(jobs)
         t2 = time.perf_counter()
         fail = keep[sc <= 0]
         fail = fail[z[fail] >= _logit(tau_fb)]
+        self._use(self.tune_plain)
         sc2, _, _ = self.dp(self.cand["jobs"][fail])
         torch.cuda.synchronize()
         t3 = time.perf_counter()
@@ -433,12 +464,13 @@ def evaluate(eng: L.Engine, model: PrefilterModel, cand: dict, tau: float, margi
     path's recall of the plain path's passing candidates."""
     import torch
     pipe = Pipeline(eng, cand)
-    plain, _, _ = pipe.dp(cand["jobs"])  # warm-up
+    pipe.autotune_paths(model, tau, margin, tau_fb)
+    plain, _, _ = pipe.plain()  # warm-up
     t_plain = []
     for _ in range(repeats):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        plain, _, _ = pipe.dp(cand["jobs"])
+        plain, _, _ = pipe.plain()
         torch.cuda.synchronize()
         t_plain.append(time.perf_counter() - t0)
     pipe.learned(model, tau, margin, 0.0, tau_fb)  # warm-up
@@ -457,7 +489,8 @@ def evaluate(eng: L.Engine, model: PrefilterModel, cand: dict, tau: float, margi
     return {"n": pipe.n, "plain_pass": int(pos.sum()), "recall": float(passed[pos].mean()) if pos.any() else 1.0,
             "extra_pass": int((passed & ~pos).sum()), "plain_s": min(t_plain), "learned_s": st["wall"],
             "plain_loci_per_s": pipe.n / min(t_plain), "learned_loci_per_s": pipe.n / st["wall"],
-            "speedup": min(t_plain) / st["wall"], "cells_plain": cells_plain, **st}
+            "speedup": min(t_plain) / st["wall"], "cells_plain": cells_plain, "tune_plain": pipe.tune_plain,
+            "tune_learned": pipe.tune_learned, **st}
 
 
 def main(argv=None):
