@@ -441,6 +441,46 @@ int pl_pf_gemm(int32_t device, const void *A, int64_t lda, const void *B, int64_
 		int32_t n_tile, const float *bias, int32_t relu, const void *mask, int64_t ldm, void *C, int64_t ldc, void *CT,
 		int64_t ldct, float *Cf, int64_t ldcf, int32_t *err, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Alignment statistics and exon features from the CIGAR (the work of
+ * align.c:148-269, mp_extra_cal), batched on the device.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+	int64_t cigar_off;   /* CIGAR words (nasw.h ops) of the alignment in the cigar buffer */
+	int64_t nt_off;      /* target bases (0-3 A/C/G/T, 4 N) from the region start r->vs */
+	int64_t aa_off;      /* protein (ASCII) from r->qs */
+	int64_t pssm_off;    /* position-specific rows (asize wide) from r->qs, or -1: the matrix */
+	int64_t l_nt;        /* target bases available from r->vs */
+	int64_t vs, ve;      /* r->vs, r->ve */
+	int64_t feat_off;    /* first feature slot of this alignment in the feature buffer */
+	int32_t qs, qe;      /* r->qs, r->qe */
+	int32_t n_cigar;
+	int32_t has_stop;    /* r->qe == qlen && r->p->dist_stop == 0 (mp_extra_stop before the call) */
+	int32_t feat_cap;    /* feature slots reserved (introns + 2 always suffice) */
+	int32_t pad;
+} pl_extra_job_t;
+/* mp_feat_t (protlocus.h:230-237), layout-identical */
+typedef struct {
+	int64_t vs, ve;
+	int32_t qs, qe;
+	int16_t type, phase;      /* type 0: CDS, 1: stop codon */
+	int32_t n_fs, n_stop;
+	int32_t score, n_iden, blen;
+	char donor[2], acceptor[2];
+} pl_feat_t;
+typedef struct {
+	int32_t blen, n_iden, n_plus, n_fs, n_stop, dp_max;  /* the mp_extra_t fields mp_extra_cal sets */
+	int32_t n_exon, n_feat;   /* r->n_exon, r->n_feat */
+	int32_t ok;               /* 0: the CIGAR's span does not match the region (the reference drops r->p, r->feat) */
+	int32_t pad;
+} pl_extra_result_t;
+/* Host buffers.  go/ge/fs/asize/mat: the mapping options (mp_mapopt_t); codon / aa20:
+ * the genetic code and residue tables (ns_tab_codon, ns_tab_aa20). */
+int pl_extra_cal_host(pl_engine_t *e, int32_t go, int32_t ge, int32_t fs, int32_t asize, const int8_t *mat,
+		const uint8_t *codon, const uint8_t *aa20, const pl_extra_job_t *jobs, int32_t n,
+		const uint32_t *cigar, int64_t n_cigar_words, const uint8_t *nt, int64_t l_nt, const uint8_t *aa, int64_t l_aa,
+		const int8_t *pssm, int64_t l_pssm, pl_extra_result_t *results, pl_feat_t *feats, int64_t n_feat_slots);
+
 #ifdef __cplusplus
 }
 #endif

@@ -201,3 +201,25 @@ class Options:
 
 def cigar_str(words) -> str:
     return "".join(f"{w >> 4}{NS_CIGAR_STR[w & 0xf]}" for w in words)
+
+
+class ExtraJob(C.Structure):
+    """pl_extra_job_t"""
+    _fields_ = [("cigar_off", C.c_int64), ("nt_off", C.c_int64), ("aa_off", C.c_int64), ("pssm_off", C.c_int64),
+                ("l_nt", C.c_int64), ("vs", C.c_int64), ("ve", C.c_int64), ("feat_off", C.c_int64),
+                ("qs", C.c_int32), ("qe", C.c_int32), ("n_cigar", C.c_int32), ("has_stop", C.c_int32),
+                ("feat_cap", C.c_int32), ("pad", C.c_int32)]
+
+
+class Feat(C.Structure):
+    """pl_feat_t (mp_feat_t, protlocus.h:230-237)"""
+    _fields_ = [("vs", C.c_int64), ("ve", C.c_int64), ("qs", C.c_int32), ("qe", C.c_int32), ("type", C.c_int16),
+                ("phase", C.c_int16), ("n_fs", C.c_int32), ("n_stop", C.c_int32), ("score", C.c_int32),
+                ("n_iden", C.c_int32), ("blen", C.c_int32), ("donor", C.c_char * 2), ("acceptor", C.c_char * 2)]
+
+
+class ExtraResult(C.Structure):
+    """pl_extra_result_t"""
+    _fields_ = [("blen", C.c_int32), ("n_iden", C.c_int32), ("n_plus", C.c_int32), ("n_fs", C.c_int32),
+                ("n_stop", C.c_int32), ("dp_max", C.c_int32), ("n_exon", C.c_int32), ("n_feat", C.c_int32),
+                ("ok", C.c_int32), ("pad", C.c_int32)]

@@ -1,0 +1,68 @@
+/*
+ * plfeat.c -- host side of the batched alignment statistics / exon features
+ * (extra.cu): uploads a batch of alignments, runs one warp per alignment and
+ * returns the mp_extra_cal results (align.c:148-269) with their features.
+ */
+#define _POSIX_C_SOURCE 200809L
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "plhost.h"
+
+void pl_feat_engine_free(pl_engine_t *e)
+{
+	dbuf_free(&e->f_jobs), dbuf_free(&e->f_cig), dbuf_free(&e->f_nt), dbuf_free(&e->f_aa), dbuf_free(&e->f_pssm);
+	dbuf_free(&e->f_mat), dbuf_free(&e->f_res), dbuf_free(&e->f_feat);
+}
+
+PL_EXPORT int pl_extra_cal_host(pl_engine_t *e, int32_t go, int32_t ge, int32_t fs, int32_t asize, const int8_t *mat,
+		const uint8_t *codon, const uint8_t *aa20, const pl_extra_job_t *jobs, int32_t n,
+		const uint32_t *cigar, int64_t n_cigar_words, const uint8_t *nt, int64_t l_nt, const uint8_t *aa, int64_t l_aa,
+		const int8_t *pssm, int64_t l_pssm, pl_extra_result_t *results, pl_feat_t *feats, int64_t n_feat_slots)
+{
+	plk_extra_args_t a;
+	cudaStream_t st;
+	int32_t q;
+	if (!e || !mat || !codon || !aa20 || asize <= 0 || asize > 32) { pl_set_error("extra: missing tables"); return 0; }
+	if (n <= 0) return 1;
+	for (q = 0; q < n; ++q) { /* every read of the device kernel stays inside the given buffers */
+		const pl_extra_job_t *J = &jobs[q];
+		if (J->n_cigar < 0 || J->cigar_off < 0 || J->cigar_off + J->n_cigar > n_cigar_words || J->nt_off < 0 ||
+				J->l_nt < 0 || J->nt_off + J->l_nt > l_nt || J->aa_off < 0 || J->qe < J->qs ||
+				J->aa_off + (J->qe - J->qs) > l_aa || J->feat_off < 0 || J->feat_cap < 0 ||
+				J->feat_off + J->feat_cap > n_feat_slots ||
+				(J->pssm_off >= 0 && (!pssm || J->pssm_off + (int64_t)(J->qe - J->qs) * asize > l_pssm))) {
+			pl_set_error("alignment %d: offsets outside the buffers", q);
+			return 0;
+		}
+	}
+	CK(cudaSetDevice(e->device));
+	st = e->stream;
+	if (!dbuf_ensure(&e->f_jobs, sizeof(plk_extra_job_t) * (size_t)n) ||
+			!dbuf_ensure(&e->f_cig, sizeof(uint32_t) * (size_t)(n_cigar_words > 0 ? n_cigar_words : 1)) ||
+			!dbuf_ensure(&e->f_nt, (size_t)(l_nt > 0 ? l_nt : 1)) || !dbuf_ensure(&e->f_aa, (size_t)(l_aa > 0 ? l_aa : 1)) ||
+			!dbuf_ensure(&e->f_pssm, (size_t)(l_pssm > 0 ? l_pssm : 1)) || !dbuf_ensure(&e->f_mat, (size_t)asize * asize) ||
+			!dbuf_ensure(&e->f_res, sizeof(plk_extra_res_t) * (size_t)n) ||
+			!dbuf_ensure(&e->f_feat, sizeof(plk_feat_t) * (size_t)(n_feat_slots > 0 ? n_feat_slots : 1)))
+		goto fail;
+	/* the public and kernel records are layout-identical */
+	CK(cudaMemcpyAsync(e->f_jobs.p, jobs, sizeof(plk_extra_job_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+	if (n_cigar_words > 0) CK(cudaMemcpyAsync(e->f_cig.p, cigar, sizeof(uint32_t) * (size_t)n_cigar_words, cudaMemcpyHostToDevice, st));
+	if (l_nt > 0) CK(cudaMemcpyAsync(e->f_nt.p, nt, (size_t)l_nt, cudaMemcpyHostToDevice, st));
+	if (l_aa > 0) CK(cudaMemcpyAsync(e->f_aa.p, aa, (size_t)l_aa, cudaMemcpyHostToDevice, st));
+	if (pssm && l_pssm > 0) CK(cudaMemcpyAsync(e->f_pssm.p, pssm, (size_t)l_pssm, cudaMemcpyHostToDevice, st));
+	CK(cudaMemcpyAsync(e->f_mat.p, mat, (size_t)asize * asize, cudaMemcpyHostToDevice, st));
+	memset(&a, 0, sizeof(a));
+	a.jobs = (const plk_extra_job_t*)e->f_jobs.p, a.n = n, a.cigar = (const uint32_t*)e->f_cig.p;
+	a.nt = (const uint8_t*)e->f_nt.p, a.aa = (const uint8_t*)e->f_aa.p, a.pssm = (const int8_t*)e->f_pssm.p;
+	a.mat = (const int8_t*)e->f_mat.p, a.go = go, a.ge = ge, a.fs = fs, a.asize = asize;
+	memcpy(a.codon, codon, 64), memcpy(a.aa20, aa20, 256);
+	a.res = (plk_extra_res_t*)e->f_res.p, a.feat = (plk_feat_t*)e->f_feat.p;
+	CKK(plk_extra(&a, st));
+	CK(cudaMemcpyAsync(results, e->f_res.p, sizeof(plk_extra_res_t) * (size_t)n, cudaMemcpyDeviceToHost, st));
+	if (n_feat_slots > 0) CK(cudaMemcpyAsync(feats, e->f_feat.p, sizeof(plk_feat_t) * (size_t)n_feat_slots, cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	return 1;
+fail:
+	return 0;
+}

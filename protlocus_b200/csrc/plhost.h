@@ -48,6 +48,8 @@ struct pl_engine_s {
 	int64_t r_last_cells;
 	/* learned-prefilter features */
 	dbuf_t pf_cand;
+	/* alignment statistics / exon features */
+	dbuf_t f_jobs, f_cig, f_nt, f_aa, f_pssm, f_mat, f_res, f_feat;
 	/* host planning scratch */
 	plk_job_t *hj;
 	int32_t *horder, *hwave, m_jobs;
@@ -75,6 +77,7 @@ void pl_hmm_engine_free(pl_engine_t *e);
 void pl_gapless_engine_free(pl_engine_t *e);
 void pl_rc_engine_free(pl_engine_t *e);
 void pl_pf_engine_free(pl_engine_t *e);
+void pl_feat_engine_free(pl_engine_t *e);
 int pl_ns_device(void);
 void pl_ns_set_error(const char *msg);
 

@@ -190,6 +190,39 @@ typedef struct {
 } plk_pf_feat_args_t;
 int plk_pf_features(const plk_pf_feat_args_t *a, void *stream);
 
+/* per-alignment statistics and exon features from the CIGAR (extra.cu) */
+typedef struct {
+	int64_t cigar_off, nt_off, aa_off, pssm_off;  /* pssm_off < 0: score with the matrix */
+	int64_t l_nt;                                 /* window bases available from the region start */
+	int64_t vs, ve;                               /* the region on the target (oriented, half-open) */
+	int64_t feat_off;
+	int32_t qs, qe, n_cigar, has_stop, feat_cap, pad;
+} plk_extra_job_t;
+typedef struct {
+	int64_t vs, ve;
+	int32_t qs, qe;
+	int16_t type, phase;
+	int32_t n_fs, n_stop;
+	int32_t score, n_iden, blen;
+	char donor[2], acceptor[2];
+} plk_feat_t;
+typedef struct {
+	int32_t blen, n_iden, n_plus, n_fs, n_stop, dp_max, n_exon, n_feat, ok, pad;
+} plk_extra_res_t;
+typedef struct {
+	const plk_extra_job_t *jobs;
+	int64_t n;
+	const uint32_t *cigar;
+	const uint8_t *nt, *aa;
+	const int8_t *pssm;
+	const int8_t *mat;           /* asize x asize, device */
+	int32_t go, ge, fs, asize;
+	uint8_t codon[64], aa20[256];
+	plk_extra_res_t *res;
+	plk_feat_t *feat;
+} plk_extra_args_t;
+int plk_extra(const plk_extra_args_t *a, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,7 +11,7 @@ import re
 
 import numpy as np
 
-from .abi import ExtJob, ExtResult, NsOpt, NsRst, SpliceJob, SpliceResult
+from .abi import ExtraJob, ExtraResult, Feat, ExtJob, ExtResult, NsOpt, NsRst, SpliceJob, SpliceResult
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libplgpu.so")
@@ -124,6 +124,11 @@ def load() -> C.CDLL:
     lib.pl_rc_score_host.restype = C.c_int
     lib.pl_rc_last_cells.argtypes = [C.c_void_p]
     lib.pl_rc_last_cells.restype = C.c_int64
+    lib.pl_extra_cal_host.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.POINTER(ExtraJob), C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
+                                      C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.POINTER(ExtraResult),
+                                      C.POINTER(Feat), C.c_int64]
+    lib.pl_extra_cal_host.restype = C.c_int
     lib.pl_engine_set_tuning.argtypes = [C.c_void_p, C.c_int32, C.c_double]
     lib.pl_engine_get_tuning.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
     lib.pl_engine_autotune.argtypes = [C.c_void_p, C.POINTER(NsOpt), C.POINTER(SpliceJob), C.c_int32, C.c_void_p,
@@ -205,6 +210,47 @@ class Engine:
     @property
     def stream(self) -> int:
         return self.lib.pl_engine_stream(self.h) or 0
+
+    def extra_cal(self, alns, go: int, ge: int, fs: int, mat, codon, aa20):
+        """Alignment statistics and exon features on the device.  alns: list of dicts with
+        cigar (words), nt4 (0-4 codes from r->vs), aa (bytes from r->qs), vs, ve, qs, qe,
+        has_stop and optional pssm (asize-wide rows).  Returns [(ExtraResult, [Feat])]."""
+        n = len(alns)
+        jobs = (ExtraJob * n)()
+        cig, nts, aas, pss = [], [], [], []
+        co = no = ao = po = fo = 0
+        for q, a in enumerate(alns):
+            J = jobs[q]
+            c = np.asarray(a["cigar"], np.uint32)
+            J.cigar_off, J.n_cigar = co, len(c)
+            J.nt_off, J.l_nt = no, len(a["nt4"])
+            J.aa_off = ao
+            J.pssm_off = po if a.get("pssm") is not None else -1
+            J.vs, J.ve, J.qs, J.qe, J.has_stop = a["vs"], a["ve"], a["qs"], a["qe"], int(a["has_stop"])
+            J.feat_off, J.feat_cap = fo, len(c) + 2
+            cig.append(c)
+            nts.append(np.asarray(a["nt4"], np.uint8))
+            aas.append(a["aa"])
+            co, no, ao, fo = co + len(c), no + len(a["nt4"]), ao + len(a["aa"]), fo + len(c) + 2
+            if a.get("pssm") is not None:
+                p = np.asarray(a["pssm"], np.int8).reshape(-1)
+                pss.append(p)
+                po += p.size
+        cg = np.ascontiguousarray(np.concatenate(cig) if cig else np.zeros(1, np.uint32))
+        nt = np.ascontiguousarray(np.concatenate(nts) if nts else np.zeros(1, np.uint8))
+        aa = np.frombuffer(b"".join(aas) or b"X", np.uint8).copy()
+        ps = np.ascontiguousarray(np.concatenate(pss)) if pss else None
+        m = np.ascontiguousarray(np.asarray(mat, np.int8))
+        cd = np.ascontiguousarray(np.asarray(codon, np.uint8))
+        a20 = np.ascontiguousarray(np.asarray(aa20, np.uint8))
+        res = (ExtraResult * n)()
+        feats = (Feat * max(fo, 1))()
+        if not self.lib.pl_extra_cal_host(self.h, go, ge, fs, 22, m.ctypes.data, cd.ctypes.data, a20.ctypes.data, jobs,
+                                          n, cg.ctypes.data, co, nt.ctypes.data, no, aa.ctypes.data, ao,
+                                          None if ps is None else ps.ctypes.data, po, res, feats, fo):
+            raise RuntimeError("pl_extra_cal_host: " + error())
+        return [(res[q], [feats[jobs[q].feat_off + k] for k in range(min(res[q].n_feat, jobs[q].feat_cap))])
+                for q in range(n)]
 
     def set_tuning(self, r4_rows: int = -1, coop_ratio: float = 0.0):
         """Rows-per-lane bin boundary and cooperative-job ratio of the global DP (see plgpu.h)."""

@@ -14,6 +14,8 @@ import os
 import platform
 import subprocess
 
+import numpy as np
+
 from protlocus_b200.abi import AA_I2C, BLOSUM62, NS_F_CIGAR, NS_S_NONE, NsOpt, NsRst, Options
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -258,3 +260,46 @@ def rc_ref_score(handle, k: int, dsq, null2: bool = True):
     d = np.ascontiguousarray(dsq, dtype=np.uint8)
     rc_lib().ref_rc_score(handle, k, d.ctypes.data, d.size, int(null2), C.byref(b), C.byref(s))
     return b.value, s.value
+
+
+class RefFeat(C.Structure):
+    """mp_feat_t (protlocus.h:230-237)"""
+    _fields_ = [("vs", C.c_int64), ("ve", C.c_int64), ("qs", C.c_int32), ("qe", C.c_int32), ("type", C.c_int16),
+                ("phase", C.c_int16), ("n_fs", C.c_int32), ("n_stop", C.c_int32), ("score", C.c_int32),
+                ("n_iden", C.c_int32), ("blen", C.c_int32), ("donor", C.c_char * 2), ("acceptor", C.c_char * 2)]
+
+
+_extra = None
+
+
+def extra_lib():
+    """oracle/_ref/libextra_ref.so: the reference's own mp_extra_cal, or None where it was not built."""
+    global _extra
+    if _extra is None:
+        path = os.path.join(ROOT, "oracle", "_ref", "libextra_ref.so")
+        if not os.path.exists(path):
+            return None
+        lib = C.CDLL(path)
+        lib.ref_extra_cal.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_char_p, C.c_int64, C.c_int64,
+                                      C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
+        lib.ref_extra_cal.restype = C.c_int
+        _extra = lib
+    return _extra
+
+
+def ref_extra(cigar, nt4, aa: bytes, vs: int, ve: int, qs: int, qe: int, has_stop: bool, go: int, ge: int, fs: int,
+              mat, pssm=None):
+    """(stats [blen, n_iden, n_plus, n_fs, n_stop, dp_max, n_exon, n_feat, ok], [RefFeat]) of the reference."""
+    lib = extra_lib()
+    cig = np.ascontiguousarray(np.asarray(cigar, dtype=np.uint32))
+    nt = np.ascontiguousarray(np.asarray(nt4, dtype=np.uint8))
+    m = np.ascontiguousarray(np.asarray(mat, dtype=np.int8))
+    ps = None if pssm is None else np.ascontiguousarray(np.asarray(pssm, dtype=np.int8))
+    stats = np.zeros(9, dtype=np.int32)
+    cap = len(cig) + 4
+    feats = (RefFeat * cap)()
+    lib.ref_extra_cal(cig.ctypes.data, len(cig), nt.ctypes.data, len(nt), aa, vs, ve, qs, qe, int(has_stop),
+                      None if ps is None else ps.ctypes.data, go, ge, fs, m.ctypes.data, stats.ctypes.data, feats, cap)
+    n = int(stats[7]) if stats[8] else 0
+    return stats.tolist(), [feats[k] for k in range(n)]
