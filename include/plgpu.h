@@ -481,6 +481,21 @@ int pl_extra_cal_host(pl_engine_t *e, int32_t go, int32_t ge, int32_t fs, int32_
 		const uint32_t *cigar, int64_t n_cigar_words, const uint8_t *nt, int64_t l_nt, const uint8_t *aa, int64_t l_aa,
 		const int8_t *pssm, int64_t l_pssm, pl_extra_result_t *results, pl_feat_t *feats, int64_t n_feat_slots);
 
+/* ---------------------------------------------------------------------------
+ * Prescreen banded gapped alignment (prescreen.c:346-382, ps_gapped) of many
+ * (profile, ORF, diagonal) candidates: local affine-gap alignment of the profile's
+ * PSSM (L rows x 22 int8) against the ORF's residue codes (0-21) within
+ * |t - i - diag| <= band (band <= 0: full), score only.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+	int64_t pssm_off;    /* first byte of the L x 22 rows in the pssm buffer */
+	int64_t orf_off;     /* first residue code of the ORF in the orf buffer */
+	int32_t L, n;        /* profile length, ORF length */
+	int32_t diag, band;  /* ps_cand_t.diag, mp_psopt_t.band */
+} pl_ps_job_t;
+int pl_ps_gapped_host(pl_engine_t *e, const pl_ps_job_t *jobs, int32_t n, const int8_t *pssm, int64_t l_pssm,
+		const uint8_t *orf, int64_t l_orf, int32_t go, int32_t ge, int32_t *scores);
+
 #ifdef __cplusplus
 }
 #endif

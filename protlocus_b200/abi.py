@@ -223,3 +223,9 @@ class ExtraResult(C.Structure):
     _fields_ = [("blen", C.c_int32), ("n_iden", C.c_int32), ("n_plus", C.c_int32), ("n_fs", C.c_int32),
                 ("n_stop", C.c_int32), ("dp_max", C.c_int32), ("n_exon", C.c_int32), ("n_feat", C.c_int32),
                 ("ok", C.c_int32), ("pad", C.c_int32)]
+
+
+class PsJob(C.Structure):
+    """pl_ps_job_t"""
+    _fields_ = [("pssm_off", C.c_int64), ("orf_off", C.c_int64), ("L", C.c_int32), ("n", C.c_int32),
+                ("diag", C.c_int32), ("band", C.c_int32)]

@@ -66,3 +66,57 @@ PL_EXPORT int pl_extra_cal_host(pl_engine_t *e, int32_t go, int32_t ge, int32_t 
 fail:
 	return 0;
 }
+
+void pl_ps_engine_free(pl_engine_t *e)
+{
+	dbuf_free(&e->s_jobs), dbuf_free(&e->s_pssm), dbuf_free(&e->s_orf), dbuf_free(&e->s_scr), dbuf_free(&e->s_score);
+}
+
+PL_EXPORT int pl_ps_gapped_host(pl_engine_t *e, const pl_ps_job_t *jobs, int32_t n, const int8_t *pssm, int64_t l_pssm,
+		const uint8_t *orf, int64_t l_orf, int32_t go, int32_t ge, int32_t *scores)
+{
+	plk_ps_job_t *hj = 0;
+	plk_ps_args_t a;
+	cudaStream_t st;
+	int64_t scr = 0;
+	int32_t q;
+	int ok = 0;
+	if (!e) { pl_set_error("no engine"); return 0; }
+	if (n <= 0) return 1;
+	hj = (plk_ps_job_t*)malloc(sizeof(*hj) * (size_t)n);
+	if (!hj) { pl_set_error("out of host memory"); return 0; }
+	for (q = 0; q < n; ++q) {
+		const pl_ps_job_t *J = &jobs[q];
+		int64_t k;
+		if (J->L < 0 || J->n < 0 || J->pssm_off < 0 || J->orf_off < 0 || J->pssm_off + (int64_t)J->L * 22 > l_pssm ||
+				J->orf_off + J->n > l_orf) {
+			pl_set_error("candidate %d: profile or ORF outside the buffers", q);
+			goto fail;
+		}
+		for (k = 0; k < J->n; ++k) /* every residue code indexes a 22-wide score row */
+			if (orf[J->orf_off + k] > 21) { pl_set_error("candidate %d: residue code %d", q, orf[J->orf_off + k]); goto fail; }
+		hj[q].pssm_off = J->pssm_off, hj[q].orf_off = J->orf_off, hj[q].scratch_off = scr;
+		hj[q].L = J->L, hj[q].n = J->n, hj[q].diag = J->diag, hj[q].band = J->band;
+		scr += (int64_t)J->n + 1;
+	}
+	CK(cudaSetDevice(e->device));
+	st = e->stream;
+	if (!dbuf_ensure(&e->s_jobs, sizeof(*hj) * (size_t)n) || !dbuf_ensure(&e->s_pssm, (size_t)(l_pssm > 0 ? l_pssm : 1)) ||
+			!dbuf_ensure(&e->s_orf, (size_t)(l_orf > 0 ? l_orf : 1)) ||
+			!dbuf_ensure(&e->s_scr, sizeof(int) * 2 * (size_t)(scr > 0 ? scr : 1)) ||
+			!dbuf_ensure(&e->s_score, sizeof(int32_t) * (size_t)n))
+		goto fail;
+	CK(cudaMemcpyAsync(e->s_jobs.p, hj, sizeof(*hj) * (size_t)n, cudaMemcpyHostToDevice, st));
+	if (l_pssm > 0) CK(cudaMemcpyAsync(e->s_pssm.p, pssm, (size_t)l_pssm, cudaMemcpyHostToDevice, st));
+	if (l_orf > 0) CK(cudaMemcpyAsync(e->s_orf.p, orf, (size_t)l_orf, cudaMemcpyHostToDevice, st));
+	memset(&a, 0, sizeof(a));
+	a.jobs = (const plk_ps_job_t*)e->s_jobs.p, a.n = n, a.pssm = (const int8_t*)e->s_pssm.p;
+	a.orf = (const uint8_t*)e->s_orf.p, a.go = go, a.ge = ge, a.scratch = (int*)e->s_scr.p, a.score = (int32_t*)e->s_score.p;
+	CKK(plk_ps_gapped(&a, st));
+	CK(cudaMemcpyAsync(scores, e->s_score.p, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	ok = 1;
+fail:
+	free(hj);
+	return ok;
+}

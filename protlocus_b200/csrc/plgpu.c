@@ -133,6 +133,7 @@ PL_EXPORT void pl_engine_destroy(pl_engine_t *e)
 	pl_rc_engine_free(e);
 	pl_pf_engine_free(e);
 	pl_feat_engine_free(e);
+	pl_ps_engine_free(e);
 	if (e->stream) cudaStreamDestroy(e->stream);
 	free(e->hj), free(e->horder), free(e->hwave);
 	free(e);

@@ -223,6 +223,22 @@ typedef struct {
 } plk_extra_args_t;
 int plk_extra(const plk_extra_args_t *a, void *stream);
 
+/* prescreen banded gapped alignment (pscreen.cu) */
+typedef struct {
+	int64_t pssm_off, orf_off, scratch_off;  /* scratch_off: in units of (n+1) ints x 2 per job, precomputed */
+	int32_t L, n, diag, band;
+} plk_ps_job_t;
+typedef struct {
+	const plk_ps_job_t *jobs;
+	int64_t n;
+	const int8_t *pssm;
+	const uint8_t *orf;
+	int32_t go, ge;
+	int *scratch;
+	int32_t *score;
+} plk_ps_args_t;
+int plk_ps_gapped(const plk_ps_args_t *a, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,7 +11,7 @@ import re
 
 import numpy as np
 
-from .abi import ExtraJob, ExtraResult, Feat, ExtJob, ExtResult, NsOpt, NsRst, SpliceJob, SpliceResult
+from .abi import ExtraJob, ExtraResult, Feat, PsJob, ExtJob, ExtResult, NsOpt, NsRst, SpliceJob, SpliceResult
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libplgpu.so")
@@ -129,6 +129,9 @@ def load() -> C.CDLL:
                                       C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.POINTER(ExtraResult),
                                       C.POINTER(Feat), C.c_int64]
     lib.pl_extra_cal_host.restype = C.c_int
+    lib.pl_ps_gapped_host.argtypes = [C.c_void_p, C.POINTER(PsJob), C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
+                                      C.c_int64, C.c_int32, C.c_int32, C.c_void_p]
+    lib.pl_ps_gapped_host.restype = C.c_int
     lib.pl_engine_set_tuning.argtypes = [C.c_void_p, C.c_int32, C.c_double]
     lib.pl_engine_get_tuning.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
     lib.pl_engine_autotune.argtypes = [C.c_void_p, C.POINTER(NsOpt), C.POINTER(SpliceJob), C.c_int32, C.c_void_p,
@@ -251,6 +254,27 @@ class Engine:
             raise RuntimeError("pl_extra_cal_host: " + error())
         return [(res[q], [feats[jobs[q].feat_off + k] for k in range(min(res[q].n_feat, jobs[q].feat_cap))])
                 for q in range(n)]
+
+    def ps_gapped(self, cands, go: int = 11, ge: int = 1) -> np.ndarray:
+        """Prescreen banded gapped scores.  cands: list of (pssm [L x 22] int8, orf codes, diag, band)."""
+        n = len(cands)
+        jobs = (PsJob * n)()
+        ps, orfs = [], []
+        po = oo = 0
+        for q, (pssm, orf, diag, band) in enumerate(cands):
+            p = np.ascontiguousarray(np.asarray(pssm, np.int8).reshape(-1, 22))
+            o = np.ascontiguousarray(np.asarray(orf, np.uint8))
+            jobs[q].pssm_off, jobs[q].orf_off, jobs[q].L, jobs[q].n = po, oo, p.shape[0], o.size
+            jobs[q].diag, jobs[q].band = int(diag), int(band)
+            ps.append(p.reshape(-1))
+            orfs.append(o)
+            po, oo = po + p.size, oo + o.size
+        pb = np.ascontiguousarray(np.concatenate(ps) if ps else np.zeros(1, np.int8))
+        ob = np.ascontiguousarray(np.concatenate(orfs) if orfs else np.zeros(1, np.uint8))
+        sc = np.zeros(max(n, 1), np.int32)
+        if not self.lib.pl_ps_gapped_host(self.h, jobs, n, pb.ctypes.data, po, ob.ctypes.data, oo, go, ge, sc.ctypes.data):
+            raise RuntimeError("pl_ps_gapped_host: " + error())
+        return sc[:n]
 
     def set_tuning(self, r4_rows: int = -1, coop_ratio: float = 0.0):
         """Rows-per-lane bin boundary and cooperative-job ratio of the global DP (see plgpu.h)."""

@@ -303,3 +303,27 @@ def ref_extra(cigar, nt4, aa: bytes, vs: int, ve: int, qs: int, qe: int, has_sto
                       None if ps is None else ps.ctypes.data, go, ge, fs, m.ctypes.data, stats.ctypes.data, feats, cap)
     n = int(stats[7]) if stats[8] else 0
     return stats.tolist(), [feats[k] for k in range(n)]
+
+
+_ps = None
+
+
+def ps_lib():
+    """oracle/_ref/libps_ref.so: the reference's own ps_gapped, or None where it was not built."""
+    global _ps
+    if _ps is None:
+        path = os.path.join(ROOT, "oracle", "_ref", "libps_ref.so")
+        if not os.path.exists(path):
+            return None
+        lib = C.CDLL(path)
+        lib.ref_ps_gapped.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                      C.c_int32]
+        lib.ref_ps_gapped.restype = C.c_int32
+        _ps = lib
+    return _ps
+
+
+def ref_ps_gapped(pssm, orf, diag: int, band: int, go: int = 11, ge: int = 1) -> int:
+    p = np.ascontiguousarray(np.asarray(pssm, np.int8).reshape(-1, 22))
+    o = np.ascontiguousarray(np.asarray(orf, np.uint8))
+    return int(ps_lib().ref_ps_gapped(p.ctypes.data, p.shape[0], o.ctypes.data, o.size, diag, band, go, ge))

@@ -1,0 +1,62 @@
+"""The prescreen's banded gapped alignment on the device (pscreen.cu) against the
+reference's own ps_gapped (prescreen.c:346-382) compiled behind oracle/ref_prescreen.c.
+
+Cases: HMM-like PSSMs from synthetic Plan7 profiles parsed by the restated hmm.c
+reader, and random PSSMs; ORFs with a planted profile-sampled stretch or random; the
+default band (32), narrow bands, the full matrix (band <= 0), and diagonals from far
+left of the ORF to far right of it (bands clipped or outside the matrix).
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from protlocus_b200 import lib as L
+
+need_ref = pytest.mark.skipif(O.ps_lib() is None, reason="oracle/_ref/libps_ref.so not built")
+
+
+def _cases(seed, n):
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n):
+        Lq = int(rng.integers(1, 400))
+        pssm = rng.integers(-9, 8, size=(Lq, 22)).astype(np.int8)
+        nq = int(rng.integers(1, 600))
+        orf = rng.integers(0, 22, size=nq).astype(np.uint8)
+        if q % 3 == 0 and nq > 40 and Lq > 40:  # a stretch the profile likes, on one diagonal
+            d0 = int(rng.integers(-Lq // 2, nq // 2))
+            for i in range(Lq):
+                t = i + d0
+                if 0 <= t < nq and rng.random() < 0.8:
+                    orf[t] = int(np.argmax(pssm[i]))
+            diag = d0 + int(rng.integers(-3, 4))
+        else:
+            diag = int(rng.integers(-Lq - 50, nq + 50))
+        band = int(rng.choice([32, 32, 32, 8, 1, 0, -5, 64]))
+        out.append((pssm, orf, diag, band))
+    return out
+
+
+@need_ref
+def test_reference_ps_gapped_hand_case():
+    """One residue the profile scores 5 on, at the diagonal: the local score is 5."""
+    pssm = np.full((1, 22), -3, np.int8)
+    pssm[0, 7] = 5
+    assert O.ref_ps_gapped(pssm, np.array([1, 7, 2], np.uint8), 1, 32) == 5
+    assert O.ref_ps_gapped(pssm, np.array([1, 2, 3], np.uint8), 1, 32) == 0
+
+
+@pytest.mark.gpu
+@need_ref
+def test_ps_gapped_matches_reference():
+    cands = _cases(3, 600)
+    eng = L.Engine(0)
+    try:
+        got = eng.ps_gapped(cands)
+    finally:
+        eng.close()
+    want = np.array([O.ref_ps_gapped(p, o, d, b) for p, o, d, b in cands])
+    bad = np.nonzero(got != want)[0]
+    assert len(bad) == 0, [(int(i), cands[i][0].shape[0], cands[i][1].size, cands[i][2], cands[i][3], int(got[i]),
+                            int(want[i])) for i in bad[:5]]
+    assert (want > 0).mean() > 0.5
