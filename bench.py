@@ -65,11 +65,13 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the engine's default tuning instead of autotuning it on the workload (global DP)")
-    ap.add_argument("--workload", default="global", choices=["global", "ext", "hmm", "gapless", "forward", "prefilter"],
+    ap.add_argument("--workload", default="global",
+                    choices=["global", "ext", "hmm", "gapless", "forward", "prefilter", "extra", "prescreen"],
                     help="global: the batched global spliced DP (headline); ext: the batched extension DP; "
                          "hmm: the integer profile-HMM DP; gapless: the gapless X-drop prefilter; "
                          "forward: the recheck Forward score; prefilter: learned candidate prefilter vs the plain "
-                         "batched DP over the held-out seed's candidates")
+                         "batched DP over the held-out seed's candidates; extra: alignment statistics and exon "
+                         "features from the CIGAR; prescreen: banded gapped profile-ORF alignment")
     ap.add_argument("--peptides", type=int, default=20000, help="peptides per step (--workload forward)")
     ap.add_argument("--candidates", type=int, default=131072, help="candidates of 8 anchors (--workload gapless)")
     ap.add_argument("--profiles", type=int, default=16, help="profiles per step (--workload hmm)")
@@ -222,6 +224,10 @@ def main():
         return main_forward(args)
     if args.workload == "prefilter":
         return main_prefilter(args)
+    if args.workload == "extra":
+        return main_extra(args)
+    if args.workload == "prescreen":
+        return main_prescreen(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -1173,6 +1179,160 @@ def main_prefilter(args):
                 "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line), flush=True)
     model.close()
+    eng.close()
+    R.close()
+    return 0
+
+
+# ---------------------------------------------------------------------------- alignment statistics / features
+
+def _simple_line(metric, value, unit, args, world, ms, dtype, desc, e2e, launches, roofline, cpu, clk, extra=None):
+    line = {"metric": metric, "value": round(value, 3), "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": {"workload": desc, **(extra or {})},
+            "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
+def main_extra(args):
+    """One step = pl_extra_cal_host over the alignments of the batched global DP (4096 pairs x 2
+    strands): mp_extra_cal's counts and exon features for each, host buffers in and out."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    from protlocus_b200.abi import BLOSUM62, make_tables
+    R = Ranks("nccl")
+    jobs = make_jobs(args, R.seed(1))
+    nt, aa, nt_off, aa_off, nl, al, tab = pack(jobs)
+    n = len(jobs)
+    opt = Options(flag=NS_F_CIGAR)
+    eng = L.Engine(R.local)
+    got = eng.align_host(opt, jobs)
+    nt4, aa20, codon = make_tables()
+    mat = np.asarray(BLOSUM62, np.int8).reshape(-1)
+    alns = []
+    for q, (score, cig, _w) in enumerate(got):
+        alns.append({"cigar": cig, "nt4": nt4[nt[nt_off[q]: nt_off[q] + nl[q]]], "aa": bytes(aa[aa_off[q]: aa_off[q] + al[q]]),
+                     "vs": 0, "ve": int(nl[q]), "qs": 0, "qe": int(al[q]), "has_stop": q % 4 == 0})
+    pk = eng.extra_pack(alns)
+    for _ in range(max(3, args.warmup)):
+        eng.extra_run(pk, 11, 1, 23, mat, codon, aa20)
+    clocks = Clocks(R.local)
+    eng.set_timing(True)
+    launches0 = L.load().pl_kernel_launch_count()
+    R.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.extra_run(pk, 11, 1, 23, mat, codon, aa20)
+    te = R.max((time.perf_counter() - t0) / args.steps)
+    res = [(pk["res"][q], None) for q in range(n)]
+    clk = clocks.stop()
+    launches = L.load().pl_kernel_launch_count() - launches0
+    k_s = eng.times()["dp_ms"] / 1e3 / args.steps
+    bad = sum(1 for r, _ in res if not r.ok)
+    n_all = R.sum(n)
+    ncig = sum(len(a["cigar"]) for a in alns)
+    nfeat = sum(r.n_feat for r, _ in res)
+    # algorithmic bytes: the aligned codons' bases and residues, the CIGAR, the records in and out
+    alg = int(sum(3 * a["qe"] + a["qe"] for a in alns) + 4 * ncig + 80 * n + 56 * nfeat)
+    peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    cpu = None
+    if R.is_root:
+        k = min(n, 2000)
+        t1 = time.perf_counter()
+        for a in alns[:k]:
+            O.ref_extra(a["cigar"], a["nt4"], a["aa"], a["vs"], a["ve"], a["qs"], a["qe"], a["has_stop"], 11, 1, 23, mat)
+        v = k / (time.perf_counter() - t1)
+        cpu = {"value": round(v, 1), "unit": "alignments/s", "cores": 1, "kind": "reference",
+               "sample": f"{k} alignments, align.c mp_extra_cal (compiled from the reference) called one by one"}
+        _simple_line("alignment statistics + exon features (mp_extra_cal) alignments/s at 1 B200", n_all / k_s,
+                     "alignments/s", args, R.world, k_s * 1e3, "int32",
+                     f"{n} global spliced alignments of the batched DP (4096 pairs x 2 strands), {ncig} CIGAR ops",
+                     {"value": round(n_all / te, 1), "unit": "alignments/s", "ms_per_step": round(te * 1e3, 2),
+                      "h2d_bytes_per_step": int(sum(len(a["nt4"]) + a["qe"] for a in alns) + 4 * ncig + 64 * n),
+                      "d2h_bytes_per_step": int(40 * n + 56 * (ncig + 2 * n)), "api": "pl_extra_cal_host, wall clock"},
+                     launches, {"bound": "hbm", "kernel": "k_extra", "achieved": alg / k_s / 1e9, "peak": peak,
+                                "unit": "GB/s", "frac": alg / k_s / 1e9 / peak, "traffic": None,
+                                "note": "algorithmic bytes: 4 B per aligned residue, 4 B per CIGAR op, the records"},
+                     cpu, clk, {"span_mismatches": bad, "features": nfeat})
+    eng.close()
+    R.close()
+    return 0
+
+
+PS_OPS_PER_CELL = 11  # int32 ops per banded cell (prescreen.c:368-378): add, 2 sub + max, 3 max, 2 sub + max, max
+
+
+def main_prescreen(args):
+    """One step = pl_ps_gapped_host over 20,000 (profile, ORF, diagonal) candidates: PSSMs of
+    50-800 rows, ORFs of 100-1500 residues with a planted profile-favoured stretch on half of
+    them, band 32 (the default), host buffers in and out."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    R = Ranks("nccl")
+    rng = np.random.default_rng(R.seed(9))
+    n = 20000
+    cands = []
+    for q in range(n):
+        Lq = int(rng.integers(50, 801))
+        pssm = rng.integers(-9, 8, size=(Lq, 22)).astype(np.int8)
+        nq = int(rng.integers(100, 1501))
+        orf = rng.integers(0, 22, size=nq).astype(np.uint8)
+        d0 = int(rng.integers(-Lq // 2, max(1, nq - Lq // 2)))
+        if q % 2 == 0:
+            rows = np.arange(Lq)
+            t = rows + d0
+            ok = (t >= 0) & (t < nq) & (rng.random(Lq) < 0.7)
+            orf[t[ok]] = np.argmax(pssm[rows[ok]], axis=1).astype(np.uint8)
+        cands.append((pssm, orf, d0 + int(rng.integers(-2, 3)), 32))
+    eng = L.Engine(R.local)
+    pk = eng.ps_pack(cands)
+    for _ in range(max(3, args.warmup)):
+        eng.ps_run(pk)
+    clocks = Clocks(R.local)
+    eng.set_timing(True)
+    launches0 = L.load().pl_kernel_launch_count()
+    R.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sc = eng.ps_run(pk)
+    te = R.max((time.perf_counter() - t0) / args.steps)
+    clk = clocks.stop()
+    launches = L.load().pl_kernel_launch_count() - launches0
+    tm = eng.times()
+    k_s = tm["dp_ms"] / 1e3 / args.steps
+    cells = tm["cells"] // args.steps
+    cells_all = R.sum(cells)
+    int32_peak, _ = L.measure_int_peak(R.local)
+    achieved = cells * PS_OPS_PER_CELL / k_s
+    cpu = None
+    if R.is_root:
+        k = 400
+        t1 = time.perf_counter()
+        for p, o, d, b in cands[:k]:
+            O.ref_ps_gapped(p, o, d, b)
+        secs = time.perf_counter() - t1
+        c_k = sum(min(b_hi, o.size - 1) - max(b_lo, 0) + 1 for p, o, d, b in cands[:k]
+                  for b_lo, b_hi in [(i + d - 32, i + d + 32) for i in range(p.shape[0])] if min(b_hi, o.size - 1) >= max(b_lo, 0))
+        cpu = {"value": round(c_k / secs / 1e9, 4), "unit": "GCUPS", "cores": 1, "kind": "reference",
+               "sample": f"{k} candidates, prescreen.c ps_gapped (compiled from the reference) called one by one"}
+        _simple_line("prescreen banded gapped alignment GCUPS at 1 B200", cells_all / k_s / 1e9, "GCUPS", args, R.world,
+                     k_s * 1e3, "int32",
+                     f"{n} profile x ORF candidates: PSSM 50-800 rows, ORF 100-1500 aa, band 32, half planted",
+                     {"value": round(cells_all / te / 1e9, 3), "unit": "GCUPS", "ms_per_step": round(te * 1e3, 2),
+                      "h2d_bytes_per_step": int(sum(p.size + o.size for p, o, _, _ in cands) + 24 * n),
+                      "d2h_bytes_per_step": 4 * n, "api": "pl_ps_gapped_host, wall clock"},
+                     launches, {"bound": "int", "kernel": "k_ps_gapped", "achieved": achieved, "peak": int32_peak,
+                                "unit": "lane-ops/s", "frac": achieved / int32_peak if int32_peak else None,
+                                "traffic": None, "ops_per_cell": PS_OPS_PER_CELL,
+                                "peak_source": "measured live: pl_measure_int_peak, int32"},
+                     cpu, clk, {"cells_per_step": int(cells), "positive_scores": int((sc > 0).sum())})
     eng.close()
     R.close()
     return 0

@@ -9,6 +9,19 @@
 #include <string.h>
 #include "plhost.h"
 
+/* accumulates the recorded kernel events of this call into the engine's timers (phase 1) */
+static void pl_feat_times(pl_engine_t *e, int64_t cells)
+{
+	int k;
+	float ms;
+	if (!e->timing) return;
+	for (k = 0; k + 1 < e->n_ev; k += 2) {
+		cudaEventElapsedTime(&ms, e->ev[k], e->ev[k + 1]);
+		e->acc_ms[e->ev_kind[k]] += ms;
+	}
+	e->acc_dp_launches += e->n_ev / 2, e->acc_cells += cells;
+}
+
 void pl_feat_engine_free(pl_engine_t *e)
 {
 	dbuf_free(&e->f_jobs), dbuf_free(&e->f_cig), dbuf_free(&e->f_nt), dbuf_free(&e->f_aa), dbuf_free(&e->f_pssm);
@@ -58,10 +71,18 @@ PL_EXPORT int pl_extra_cal_host(pl_engine_t *e, int32_t go, int32_t ge, int32_t 
 	a.mat = (const int8_t*)e->f_mat.p, a.go = go, a.ge = ge, a.fs = fs, a.asize = asize;
 	memcpy(a.codon, codon, 64), memcpy(a.aa20, aa20, 256);
 	a.res = (plk_extra_res_t*)e->f_res.p, a.feat = (plk_feat_t*)e->f_feat.p;
+	e->n_ev = 0;
+	PL_TIME(e, st, 1);
 	CKK(plk_extra(&a, st));
+	PL_TIME(e, st, 1);
 	CK(cudaMemcpyAsync(results, e->f_res.p, sizeof(plk_extra_res_t) * (size_t)n, cudaMemcpyDeviceToHost, st));
 	if (n_feat_slots > 0) CK(cudaMemcpyAsync(feats, e->f_feat.p, sizeof(plk_feat_t) * (size_t)n_feat_slots, cudaMemcpyDeviceToHost, st));
 	CK(cudaStreamSynchronize(st));
+	{
+		int64_t codons = 0;
+		for (q = 0; q < n; ++q) codons += jobs[q].qe - jobs[q].qs;
+		pl_feat_times(e, codons);
+	}
 	return 1;
 fail:
 	return 0;
@@ -112,9 +133,26 @@ PL_EXPORT int pl_ps_gapped_host(pl_engine_t *e, const pl_ps_job_t *jobs, int32_t
 	memset(&a, 0, sizeof(a));
 	a.jobs = (const plk_ps_job_t*)e->s_jobs.p, a.n = n, a.pssm = (const int8_t*)e->s_pssm.p;
 	a.orf = (const uint8_t*)e->s_orf.p, a.go = go, a.ge = ge, a.scratch = (int*)e->s_scr.p, a.score = (int32_t*)e->s_score.p;
+	e->n_ev = 0;
+	PL_TIME(e, st, 1);
 	CKK(plk_ps_gapped(&a, st));
+	PL_TIME(e, st, 1);
 	CK(cudaMemcpyAsync(scores, e->s_score.p, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, st));
 	CK(cudaStreamSynchronize(st));
+	{ /* cells: the banded (or full) rows inside the ORF */
+		int64_t cells = 0;
+		for (q = 0; q < n; ++q) {
+			int32_t i;
+			const pl_ps_job_t *J = &jobs[q];
+			for (i = 0; i < J->L; ++i) {
+				int32_t lo = J->band > 0 ? i + J->diag - J->band : 0, hi = J->band > 0 ? i + J->diag + J->band : J->n - 1;
+				if (lo < 0) lo = 0;
+				if (hi > J->n - 1) hi = J->n - 1;
+				if (hi >= lo) cells += hi - lo + 1;
+			}
+		}
+		pl_feat_times(e, cells);
+	}
 	ok = 1;
 fail:
 	free(hj);

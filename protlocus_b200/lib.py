@@ -214,10 +214,10 @@ class Engine:
     def stream(self) -> int:
         return self.lib.pl_engine_stream(self.h) or 0
 
-    def extra_cal(self, alns, go: int, ge: int, fs: int, mat, codon, aa20):
-        """Alignment statistics and exon features on the device.  alns: list of dicts with
-        cigar (words), nt4 (0-4 codes from r->vs), aa (bytes from r->qs), vs, ve, qs, qe,
-        has_stop and optional pssm (asize-wide rows).  Returns [(ExtraResult, [Feat])]."""
+    @staticmethod
+    def extra_pack(alns):
+        """Packs alignments for extra_run: list of dicts with cigar (words), nt4 (0-4 codes from
+        r->vs), aa (bytes from r->qs), vs, ve, qs, qe, has_stop and optional pssm rows."""
         n = len(alns)
         jobs = (ExtraJob * n)()
         cig, nts, aas, pss = [], [], [], []
@@ -239,24 +239,37 @@ class Engine:
                 p = np.asarray(a["pssm"], np.int8).reshape(-1)
                 pss.append(p)
                 po += p.size
-        cg = np.ascontiguousarray(np.concatenate(cig) if cig else np.zeros(1, np.uint32))
-        nt = np.ascontiguousarray(np.concatenate(nts) if nts else np.zeros(1, np.uint8))
-        aa = np.frombuffer(b"".join(aas) or b"X", np.uint8).copy()
-        ps = np.ascontiguousarray(np.concatenate(pss)) if pss else None
+        return {"n": n, "jobs": jobs, "n_cig": co, "n_nt": no, "n_aa": ao, "n_pssm": po, "n_feat": fo,
+                "cig": np.ascontiguousarray(np.concatenate(cig) if cig else np.zeros(1, np.uint32)),
+                "nt": np.ascontiguousarray(np.concatenate(nts) if nts else np.zeros(1, np.uint8)),
+                "aa": np.frombuffer(b"".join(aas) or b"X", np.uint8).copy(),
+                "pssm": np.ascontiguousarray(np.concatenate(pss)) if pss else None,
+                "res": (ExtraResult * max(n, 1))(), "feats": (Feat * max(fo, 1))()}
+
+    def extra_run(self, pk, go: int, ge: int, fs: int, mat, codon, aa20):
+        """pl_extra_cal_host over a packed batch; results stay in pk["res"] / pk["feats"]."""
         m = np.ascontiguousarray(np.asarray(mat, np.int8))
         cd = np.ascontiguousarray(np.asarray(codon, np.uint8))
         a20 = np.ascontiguousarray(np.asarray(aa20, np.uint8))
-        res = (ExtraResult * n)()
-        feats = (Feat * max(fo, 1))()
-        if not self.lib.pl_extra_cal_host(self.h, go, ge, fs, 22, m.ctypes.data, cd.ctypes.data, a20.ctypes.data, jobs,
-                                          n, cg.ctypes.data, co, nt.ctypes.data, no, aa.ctypes.data, ao,
-                                          None if ps is None else ps.ctypes.data, po, res, feats, fo):
+        if not self.lib.pl_extra_cal_host(self.h, go, ge, fs, 22, m.ctypes.data, cd.ctypes.data, a20.ctypes.data,
+                                          pk["jobs"], pk["n"], pk["cig"].ctypes.data, pk["n_cig"], pk["nt"].ctypes.data,
+                                          pk["n_nt"], pk["aa"].ctypes.data, pk["n_aa"],
+                                          None if pk["pssm"] is None else pk["pssm"].ctypes.data, pk["n_pssm"],
+                                          pk["res"], pk["feats"], pk["n_feat"]):
             raise RuntimeError("pl_extra_cal_host: " + error())
-        return [(res[q], [feats[jobs[q].feat_off + k] for k in range(min(res[q].n_feat, jobs[q].feat_cap))])
-                for q in range(n)]
+        return pk
 
-    def ps_gapped(self, cands, go: int = 11, ge: int = 1) -> np.ndarray:
-        """Prescreen banded gapped scores.  cands: list of (pssm [L x 22] int8, orf codes, diag, band)."""
+    def extra_cal(self, alns, go: int, ge: int, fs: int, mat, codon, aa20):
+        """Alignment statistics and exon features on the device (see extra_pack).
+        Returns [(ExtraResult, [Feat])]."""
+        pk = self.extra_run(self.extra_pack(alns), go, ge, fs, mat, codon, aa20)
+        jobs, res, feats = pk["jobs"], pk["res"], pk["feats"]
+        return [(res[q], [feats[jobs[q].feat_off + k] for k in range(min(res[q].n_feat, jobs[q].feat_cap))])
+                for q in range(pk["n"])]
+
+    @staticmethod
+    def ps_pack(cands):
+        """Packs (pssm [L x 22] int8, orf codes, diag, band) candidates for ps_run."""
         n = len(cands)
         jobs = (PsJob * n)()
         ps, orfs = [], []
@@ -269,12 +282,20 @@ class Engine:
             ps.append(p.reshape(-1))
             orfs.append(o)
             po, oo = po + p.size, oo + o.size
-        pb = np.ascontiguousarray(np.concatenate(ps) if ps else np.zeros(1, np.int8))
-        ob = np.ascontiguousarray(np.concatenate(orfs) if orfs else np.zeros(1, np.uint8))
-        sc = np.zeros(max(n, 1), np.int32)
-        if not self.lib.pl_ps_gapped_host(self.h, jobs, n, pb.ctypes.data, po, ob.ctypes.data, oo, go, ge, sc.ctypes.data):
+        return {"n": n, "jobs": jobs, "n_pssm": po, "n_orf": oo,
+                "pssm": np.ascontiguousarray(np.concatenate(ps) if ps else np.zeros(1, np.int8)),
+                "orf": np.ascontiguousarray(np.concatenate(orfs) if orfs else np.zeros(1, np.uint8)),
+                "score": np.zeros(max(n, 1), np.int32)}
+
+    def ps_run(self, pk, go: int = 11, ge: int = 1) -> np.ndarray:
+        if not self.lib.pl_ps_gapped_host(self.h, pk["jobs"], pk["n"], pk["pssm"].ctypes.data, pk["n_pssm"],
+                                          pk["orf"].ctypes.data, pk["n_orf"], go, ge, pk["score"].ctypes.data):
             raise RuntimeError("pl_ps_gapped_host: " + error())
-        return sc[:n]
+        return pk["score"][: pk["n"]]
+
+    def ps_gapped(self, cands, go: int = 11, ge: int = 1) -> np.ndarray:
+        """Prescreen banded gapped scores of (pssm [L x 22] int8, orf codes, diag, band) candidates."""
+        return self.ps_run(self.ps_pack(cands), go, ge)
 
     def set_tuning(self, r4_rows: int = -1, coop_ratio: float = 0.0):
         """Rows-per-lane bin boundary and cooperative-job ratio of the global DP (see plgpu.h)."""
