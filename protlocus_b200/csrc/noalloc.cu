@@ -108,6 +108,7 @@ static int na_run(const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n_jo
 	P.sp_null_bonus = opt->sp_null_bonus, P.ie_coef = opt->ie_coef;
 	memcpy(P.sc, opt->sc, 22 * 22), memcpy(P.nt4, opt->nt4, 256), memcpy(P.aa20, opt->aa20, 256), memcpy(P.codon, opt->codon, 64);
 	P.aa_x = opt->aa20['X'];
+	plk_fill_scaled(&P);
 	for (i = 0; i < 22 * 22; ++i) if (max_sub < opt->sc[i]) max_sub = opt->sc[i];
 
 	/* plan: one wave, one warp per job, width by ns_global_gs_auto's rule (nasw-sse.c:987-996) */
@@ -134,7 +135,7 @@ static int na_run(const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n_jo
 		const int64_t ring_stride = ((int64_t)max_al + 1) * PLK_RING_INTS;
 		const int64_t o_jobs = 0, o_order = na_align(o_jobs + (int64_t)sizeof(plk_job_t) * n_jobs);
 		const int64_t o_cnt = na_align(o_order + 4LL * n_jobs), o_tot = o_cnt + 256;
-		const int64_t o_prep = o_tot + 256, o_tmp = na_align(o_prep + prep_total);
+		const int64_t o_prep = o_tot + 256, o_tmp = na_align(o_prep + prep_total + PLK_PREP_SLACK);
 		const int64_t o_ring = na_align(o_tmp + 4 * tmp_total);
 		const int64_t o_trace = na_align(o_ring + 4 * ring_stride * PL_NOALLOC_CTAS * PLK_WARPS_PER_CTA);
 		off = o_trace + trace_total;

@@ -191,6 +191,7 @@ int pl_params(const ns_opt_t *opt, plk_params_t *p, int for_ext)
 	memcpy(p->sc, opt->sc, 22 * 22);
 	memcpy(p->nt4, opt->nt4, 256), memcpy(p->aa20, opt->aa20, 256), memcpy(p->codon, opt->codon, 64);
 	p->aa_x = opt->aa20['X'];
+	plk_fill_scaled(p);
 	return 1;
 }
 
@@ -353,7 +354,7 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 		if (!dbuf_ensure(&e->trace, (size_t)need_trace)) goto fail;
 	}
 	if (!dbuf_ensure(&e->jobs, sizeof(plk_job_t) * (size_t)n) || !dbuf_ensure(&e->order, sizeof(int32_t) * (size_t)n) ||
-			!dbuf_ensure(&e->counters, 64) || !dbuf_ensure(&e->prep, (size_t)prep_total) ||
+			!dbuf_ensure(&e->counters, 64) || !dbuf_ensure(&e->prep, (size_t)prep_total + PLK_PREP_SLACK) ||
 			!dbuf_ensure(&e->tmp, sizeof(uint32_t) * (size_t)tmp_total) || !dbuf_ensure(&e->total, 64))
 		goto fail;
 	{

@@ -29,7 +29,20 @@ typedef struct {
 	uint8_t nt4[256], aa20[256], codon[64];
 	uint8_t aa_x;               /* aa20['X'] */
 	uint8_t pad[3];
+	/* the global DP's penalties in its x16 tagged domain (filled by the host so the
+	 * kernel reads them as constants): go, ge, io, -fs + 9/8/7/6 (frameshift
+	 * candidates 6-9 with their tags), -fs, go + ge */
+	int32_t s16[9];
 } plk_params_t;
+
+/* fills plk_params_t.s16 from go/ge/io/fs (every host path that builds parameters calls it) */
+static inline void plk_fill_scaled(plk_params_t *p)
+{
+	int i;
+	p->s16[0] = 16 * p->go, p->s16[1] = 16 * p->ge, p->s16[2] = 16 * p->io;
+	for (i = 0; i < 4; ++i) p->s16[3 + i] = -16 * p->fs + 9 - i;
+	p->s16[7] = -16 * p->fs, p->s16[8] = 16 * (p->go + p->ge);
+}
 
 /* per-job metadata, device resident */
 typedef struct {
@@ -70,6 +83,10 @@ typedef struct {
 } plk_hmm_prof_t;
 #define PLK_HMM_TILE 256
 #define PLK_HMM_SMEM_MAX (96 * 1024)  /* emissions staged in shared memory up to mpad = 2048 */
+
+/* bytes after the last job's preparation scratch that the DP may read (its row
+ * inputs are copied in whole 16-byte chunks) */
+#define PLK_PREP_SLACK 64
 
 /* bytes of preparation scratch for a job (8-aligned) */
 static inline int64_t plk_prep_bytes(int32_t nl, int32_t al)

@@ -75,12 +75,44 @@ __device__ __forceinline__ void store_trace(uint16_t *p, const unsigned (&z)[R])
 	*(typename TraceVec<R>::T*)p = *(const typename TraceVec<R>::T*)w;
 }
 
+/* Bytes of one staged row-input block: 32*R + 2 bytes starting anywhere inside a
+ * 16-byte chunk, copied as whole chunks (R = 8 at most). */
+#define ROWBLK 288
+
 struct DpShared {
 	int32_t sct[22 * 22];                               /* score table, transposed: sct[b*22 + a] */
 	int32_t slot[2][PLK_WARPS_PER_CTA][PLK_RING_INTS];  /* warp-to-warp hand-off of a cooperative wavefront */
 	int32_t job;
 	int32_t pre[PLK_WARPS_PER_CTA][PLK_RING_INTS] __attribute__((aligned(16)));
+	/* per warp, double-buffered by strip parity: the codons, donor and acceptor
+	 * penalties of the warp's 32*R rows of a strip, staged ahead of the strip */
+	uint8_t rows[PLK_WARPS_PER_CTA][2][3][ROWBLK] __attribute__((aligned(16)));
 };
+
+/* Stage the row inputs of the warp's block of a strip, rows [b, b + 32R): codons
+ * nas[b..], donor[b-1..] and acceptor[b-2..], 32R+2 bytes each.  Each block is
+ * copied as 16-byte cp.async chunks from the 16-byte boundary at or below its
+ * start; chunks that start past the end of their array are skipped (their bytes
+ * are never read: the readers apply the row bounds).  Lanes 1-31 issue the
+ * copies; lane 0 keeps its own cp.async queue for the strip hand-off ring.  The
+ * preparation arrays sit inside a 16-byte aligned allocation with at least 16
+ * bytes after the last one. */
+template <int R>
+__device__ __forceinline__ void stage_rows(uint8_t (*buf)[ROWBLK], const uint8_t *nas, const int8_t *donor,
+		const int8_t *acceptor, const int nl, const int b, const int lane)
+{
+	constexpr int CH = (32 * R + 2 + 15 + 15) / 16;  /* chunks per block */
+	static_assert(CH * 16 <= ROWBLK, "row block");
+	if (lane == 0) return;
+#pragma unroll
+	for (int g = lane - 1; g < 3 * CH; g += 31) {
+		const int a = g / CH, j = g - a * CH;
+		const uint8_t *s = a == 0 ? nas + b : (const uint8_t*)(a == 1 ? donor + b - 1 : acceptor + b - 2);
+		const uint8_t *end = a == 0 ? nas + nl : (const uint8_t*)(a == 1 ? donor : acceptor) + nl + 1;
+		const uint8_t *src = (const uint8_t*)((uintptr_t)s & ~(uintptr_t)15) + 16 * j;
+		if (src < end) cp_async16(buf[a] + 16 * j, src);
+	}
+}
 
 
 /*
@@ -115,7 +147,7 @@ template <int NW, int R>
 __device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[R], const int ah1, const int ah2,
 		const int ah3, const bool row2, const int *__restrict__ sct_b, const int (&code)[R],
 		const int (&gi)[R], const int (&dn)[R + 2], const int (&ac)[R + 2],
-		int (&ip)[R], int (&lh)[R], const int (&ic)[R], const int c16[8],
+		int (&ip)[R], int (&lh)[R], const int (&ic)[R], const int *__restrict__ c16,
 		int (&o)[9], unsigned (&z)[R], int (&hn)[R])
 {
 	/* The integer pipe is the bound, so the update is written in the DPX forms that
@@ -295,9 +327,9 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 	const int Pc = al > NL ? al : NL + 1;  /* period >= NL+1 keeps lane 0's one-step ring prefetch behind the writer */
 	const int total = nstrip * Pc + NL - 1;
 	int32_t *pre = sh.pre[wib];          /* lane 0's prefetched ring entry (cp.async target) */
-	const int c16[8] = { 16 * P.go, 16 * P.ge, 16 * P.io, -16 * P.fs + 9, -16 * P.fs + 8, -16 * P.fs + 7,
-		-16 * P.fs + 6, -16 * P.fs };
-	const int GOE = 16 * (P.go + P.ge), GE16 = 16 * P.ge;
+	uint8_t (*rowbuf)[3][ROWBLK] = sh.rows[wib];
+	const int *c16 = P.s16;             /* x16 penalties, read as kernel constants */
+	const int GOE = P.s16[8], GE16 = P.s16[1];
 
 	int c = -L, k = 0, cs = 0, dcol = 0, i0 = 0;
 	int ip[R], lh[R], ic[R], hm[R], code[R], gi[R], dn[R + 2], ac[R + 2];
@@ -309,37 +341,55 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 	for (int r = 0; r < R; ++r) ip[r] = lh[r] = ic[r] = hm[r] = NEG, code[r] = 0, gi[r] = 0;
 #pragma unroll
 	for (int r = 0; r < R + 2; ++r) dn[r] = ac[r] = 0;
+	/* the first strip's row inputs, and the ring entry of the first strip (the -inf row) */
+	stage_rows<R>(rowbuf[0], nas, donor, acceptor, nl, 2 + w * 32 * R, lane);
+	if (L == 0) {
+#pragma unroll
+		for (int q = 0; q < 9; ++q) pre[q] = NEG;
+	}
+	cp_async_wait_all();
+	__syncwarp();
+	/* warp-uniform: the step at which the warp's lane 0 next starts a strip, and that strip */
 
 	for (int s = 0; s < total; ++s) {
+		if (__shfl_sync(FULL, c, 0) == 0) {
+			/* lane 0 of the warp starts a strip: the strip's row inputs (staged one
+			 * period ago) are visible after the wait; stage those of the next strip */
+			cp_async_wait_all();
+			__syncwarp();
+			const int kn = (s - 32 * w) / Pc + 1;
+			if (kn < nstrip) stage_rows<R>(rowbuf[kn & 1], nas, donor, acceptor, nl, 2 + kn * HS + w * 32 * R, lane);
+		}
 		/* column state of the rows above: lane-1's output of the previous step */
 		int in[9];
 #pragma unroll
 		for (int q = 0; q < 9; ++q) in[q] = __shfl_up_sync(FULL, o[q], 1);
 		const bool started = c >= 0 && k < nstrip;
 		if (lane == 0 && started) {
-			if (w == 0) {
-				if (k > 0) cp_async_wait_all();
-#pragma unroll
-				for (int q = 0; q < 9; ++q) in[q] = k == 0 ? NEG : pre[q];
-			} else {
-				const int32_t *sl = sh.slot[(s - 1) & 1][wib - 1];
-#pragma unroll
-				for (int q = 0; q < 9; ++q) in[q] = sl[q];
-			}
+			/* the ring entry (prefetched, -inf before the second strip) or the slot of the warp above */
+			if (w == 0) cp_async_wait_all();
+			const int32_t *p = w == 0 ? pre : sh.slot[(s - 1) & 1][wib - 1];
+			const int4 v0 = *(const int4*)p, v1 = *(const int4*)(p + 4);
+			in[0] = v0.x, in[1] = v0.y, in[2] = v0.z, in[3] = v0.w;
+			in[4] = v1.x, in[5] = v1.y, in[6] = v1.z, in[7] = v1.w, in[8] = p[8];
 		}
-		if (started && c == 0) { /* strip start: per-row constants, column -1 */
+		if (started && c == 0) { /* strip start: per-row constants from the staged block, column -1 */
 			i0 = 2 + k * HS + L * R;
+			const int b = i0 - lane * R;
+			const uint8_t *rb = &rowbuf[k & 1][0][0] + lane * R;
+			const int on = (int)((uintptr_t)(nas + b) & 15), od = (int)((uintptr_t)(donor + b - 1) & 15),
+				oa = (int)((uintptr_t)(acceptor + b - 2) & 15);
 #pragma unroll
 			for (int r = 0; r < R; ++r) {
 				const int i = i0 + r;
-				code[r] = i < nl ? nas[i] : 0;
+				code[r] = i < nl ? rb[on + r] : 0;
 				gi[r] = MODE == 0 ? -16 * (code[r] == 20 ? P.fs : P.ge) : (code[r] == 20 ? P.fs : P.ge);
 				ip[r] = lh[r] = ic[r] = hm[r] = NEG;
 			}
 #pragma unroll
 			for (int r = 0; r < R + 2; ++r) {
 				const int pd = i0 - 1 + r, pa = i0 - 2 + r;
-				const int dv = pd <= nl ? donor[pd] : 0, av = pa <= nl ? acceptor[pa] : 0;
+				const int dv = pd <= nl ? (int8_t)rb[ROWBLK + od + r] : 0, av = pa <= nl ? (int8_t)rb[2 * ROWBLK + oa + r] : 0;
 				dn[r] = MODE == 0 ? -16 * dv : dv;
 				ac[r] = MODE == 0 ? -16 * av : av;
 			}
@@ -368,12 +418,6 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 			} else {
 				cells_plain<MODE, R>(in, hm, ah1, ah2, ah3, row2, seg, first, sct_b, code, gi, dn, ac, ip, lh, ic, P,
 						o, z, hn);
-			}
-			if (c == al - 1) { /* the final score H(nl-1, al-1) */
-				const int rl = nl - 1 - i0;
-#pragma unroll
-				for (int r = 0; r < R; ++r)
-					if (r == rl) J->score = MODE == 0 ? hn[r] >> 4 : hn[r];
 			}
 			/* trace: one store of R 16-bit words per lane, contiguous across the lanes of a strip */
 			store_trace<R>(tr + (((int64_t)k * al + dcol) * NL + L) * R, z);
@@ -406,7 +450,17 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 			cp_async16(pre, e), cp_async16(pre + 4, e + 4), cp_async16(pre + 8, e + 8);
 		}
 	}
-	if (L == 0) cp_async_wait_all();
+	cp_async_wait_all();
+	/* the final score H(nl-1, al-1): the lane holding row nl-1 in the last strip keeps
+	 * that strip's last column in hm */
+	{
+		const int rl = nl - 1 - i0;
+		if (rl >= 0 && rl < R) {
+#pragma unroll
+			for (int r = 0; r < R; ++r)
+				if (r == rl) J->score = MODE == 0 ? hm[r] >> 4 : hm[r];
+		}
+	}
 }
 
 /* Persistent DP kernel: first every CTA takes cooperative jobs (a whole CTA per
