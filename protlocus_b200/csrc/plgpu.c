@@ -108,6 +108,9 @@ PL_EXPORT pl_engine_t *pl_engine_create(int32_t device, int64_t trace_budget_byt
 	e->coop_ratio = pl_coop_ratio();
 	e->r4_rows = pl_r4_rows();
 	CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+	CK(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
+	CK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+	CK(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
 	CK(cudaMemGetInfo(&free_b, &total_b));
 	if (trace_budget_bytes <= 0) { /* default: 40% of free memory, at most 72 GB */
 		trace_budget_bytes = (int64_t)(free_b * 0.4);
@@ -116,6 +119,10 @@ PL_EXPORT pl_engine_t *pl_engine_create(int32_t device, int64_t trace_budget_byt
 	e->trace_budget = trace_budget_bytes;
 	return e;
 fail:
+	if (e->stream) cudaStreamDestroy(e->stream);
+	if (e->side) cudaStreamDestroy(e->side);
+	if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+	if (e->ev_join) cudaEventDestroy(e->ev_join);
 	free(e);
 	return 0;
 }
@@ -135,6 +142,9 @@ PL_EXPORT void pl_engine_destroy(pl_engine_t *e)
 	pl_feat_engine_free(e);
 	pl_ps_engine_free(e);
 	if (e->stream) cudaStreamDestroy(e->stream);
+	if (e->side) cudaStreamDestroy(e->side);
+	if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+	if (e->ev_join) cudaEventDestroy(e->ev_join);
 	free(e->hj), free(e->horder), free(e->hwave);
 	free(e);
 }
@@ -267,14 +277,33 @@ static int pl_grow_host(pl_engine_t *e, int32_t n)
 	return 1;
 }
 
+/* length of the union of intervals [a[i], b[i]) (sorted in place by start) */
+static double pl_union_ms(double *a, double *b, int n)
+{
+	int i, j;
+	double tot = 0, lo, hi;
+	for (i = 1; i < n; ++i) /* insertion sort by start */
+		for (j = i; j > 0 && a[j - 1] > a[j]; --j) {
+			double t = a[j]; a[j] = a[j - 1], a[j - 1] = t;
+			t = b[j], b[j] = b[j - 1], b[j - 1] = t;
+		}
+	for (i = 0; i < n; i = j) {
+		lo = a[i], hi = b[i];
+		for (j = i + 1; j < n && a[j] <= hi; ++j) if (b[j] > hi) hi = b[j];
+		tot += hi - lo;
+	}
+	return tot;
+}
+
 /* Runs the whole batch on `st`.  Inputs (nt/aa/ss) and outputs (res/cig) are device pointers. */
 static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n,
 		const uint8_t *nt, const uint8_t *aa, const uint8_t *ss, pl_splice_result_t *res_dev,
 		uint32_t *cig_dev, int64_t cig_cap, int64_t *total_out, cudaStream_t st)
 {
 	plk_params_t P;
-	int32_t q, max_al = 1, n_waves = 1, w, max_sub, *sorted, wave_n_coop = 0;
-	int64_t prep_total = 0, tmp_total = 0, trace_total = 0, max_trace = 0, slots;
+	int32_t q, max_al = 1, n_waves = 1, w, max_sub, *sorted, wave_n_coop = 0, two = 0;
+	int64_t prep_total = 0, tmp_total = 0, trace_total = 0, max_trace = 0, slots, arena_budget, arena_words = 0;
+	int64_t ring_ints = 0;
 	int64_t *wave_bytes = 0, *wave_cells = 0, total_words = 0;
 	int ok = 0;
 
@@ -313,7 +342,11 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 		pl_set_error("one job needs %lld trace bytes, over the budget of %lld", (long long)max_trace, (long long)e->trace_budget);
 		return 0;
 	}
-	/* 2. waves by LPT bin packing on trace bytes */
+	/* 2. waves by LPT bin packing on trace bytes.  A batch over the budget runs its
+	 * waves alternately on two streams, each with its own arena of half the budget:
+	 * a wave's DP then starts while the one before drains instead of after it. */
+	arena_budget = e->trace_budget;
+	if (trace_total > e->trace_budget && 4 * max_trace <= e->trace_budget) two = 1, arena_budget = e->trace_budget / 2;
 	sorted = e->horder + n;
 	{
 		pl_key_t *key = (pl_key_t*)malloc(sizeof(pl_key_t) * (size_t)n);
@@ -323,9 +356,10 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 		for (q = 0; q < n; ++q) sorted[q] = key[q].idx;
 		free(key);
 	}
-	if (trace_total > e->trace_budget)
-		n_waves = (int32_t)((trace_total + (e->trace_budget - max_trace) - 1) / (e->trace_budget - max_trace));
+	if (trace_total > arena_budget)
+		n_waves = (int32_t)((trace_total + (arena_budget - max_trace) - 1) / (arena_budget - max_trace));
 	if (n_waves > n) n_waves = n;
+	if (n_waves < 2) two = 0;
 	wave_bytes = (int64_t*)calloc((size_t)n_waves, sizeof(int64_t));
 	wave_cells = (int64_t*)calloc((size_t)n_waves, sizeof(int64_t));
 	if (!wave_bytes || !wave_cells) { pl_set_error("out of host memory"); goto fail; }
@@ -351,7 +385,9 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 	{
 		int64_t need_trace = 0;
 		for (w = 0; w < n_waves; ++w) if (wave_bytes[w] > need_trace) need_trace = wave_bytes[w];
-		if (!dbuf_ensure(&e->trace, (size_t)need_trace)) goto fail;
+		need_trace = (need_trace + 255) / 256 * 256;
+		arena_words = need_trace / 2;
+		if (!dbuf_ensure(&e->trace, (size_t)need_trace * (two ? 2 : 1))) goto fail;
 	}
 	if (!dbuf_ensure(&e->jobs, sizeof(plk_job_t) * (size_t)n) || !dbuf_ensure(&e->order, sizeof(int32_t) * (size_t)n) ||
 			!dbuf_ensure(&e->counters, 64) || !dbuf_ensure(&e->prep, (size_t)prep_total + PLK_PREP_SLACK) ||
@@ -360,7 +396,8 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 	{
 		const int64_t stride = ((int64_t)max_al + 1) * PLK_RING_INTS;
 		const int64_t n_ctas = (int64_t)e->n_sm * pl_max_ctas(e);
-		if (!dbuf_ensure(&e->ring, sizeof(int32_t) * (size_t)(stride * n_ctas * PLK_WARPS_PER_CTA))) goto fail;
+		ring_ints = stride * n_ctas * PLK_WARPS_PER_CTA;
+		if (!dbuf_ensure(&e->ring, sizeof(int32_t) * (size_t)(ring_ints * (two ? 2 : 1)))) goto fail;
 	}
 	/* order array: per wave, per mode: cooperative jobs then solo jobs, each by decreasing size */
 	{
@@ -387,10 +424,16 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 	PL_TIME(e, st, 0);
 	CKK(plk_prep((const plk_job_t*)e->jobs.p, n, nt, aa, ss, (uint8_t*)e->prep.p, &P, st));
 	PL_TIME(e, st, 0);
+	if (two) { /* fork: the side stream starts after the preparation */
+		CK(cudaEventRecord(e->ev_fork, st));
+		CK(cudaStreamWaitEvent(e->side, e->ev_fork, 0));
+	}
 	{
 		int32_t pos = 0;
 		for (w = 0; w < n_waves; ++w) {
-			const int32_t wave_start = pos;
+			const int32_t wave_start = pos, a = two ? (w & 1) : 0;
+			cudaStream_t sw = a ? e->side : st;
+			uint16_t *trace_w = (uint16_t*)e->trace.p + a * arena_words;
 			int m, r;
 			for (m = 0; m < 3; ++m)
 				for (r = 0; r < 2; ++r) {
@@ -404,21 +447,25 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 						const int32_t *ord = (const int32_t*)e->order.p + pos;
 						const int64_t stride = ((int64_t)max_al + 1) * PLK_RING_INTS;
 						const int32_t ctas = e->n_sm * e->ctas_per_sm[m][r];
-						PL_TIME(e, st, 1);
-						CKK(plk_splice_dp((plk_job_t*)e->jobs.p, ord, n_coop, ord + n_coop, n_solo, (int32_t*)e->counters.p,
-								(const uint8_t*)e->prep.p, (uint16_t*)e->trace.p, (int32_t*)e->ring.p, stride, ctas, m, rows,
-								&P, st));
-						PL_TIME(e, st, 1);
+						PL_TIME(e, sw, 1);
+						CKK(plk_splice_dp((plk_job_t*)e->jobs.p, ord, n_coop, ord + n_coop, n_solo,
+								(int32_t*)e->counters.p + 8 * a, (const uint8_t*)e->prep.p, trace_w,
+								(int32_t*)e->ring.p + a * ring_ints, stride, ctas, m, rows, &P, sw));
+						PL_TIME(e, sw, 1);
 						++e->last_dp_launches;
 						wave_n_coop += n_coop;
 					}
 					pos += n_coop + n_solo;
 				}
-			PL_TIME(e, st, 2);
+			PL_TIME(e, sw, 2);
 			CKK(plk_traceback((plk_job_t*)e->jobs.p, (const int32_t*)e->order.p + wave_start, pos - wave_start,
-					(const uint16_t*)e->trace.p, (uint32_t*)e->tmp.p, st));
-			PL_TIME(e, st, 2);
+					trace_w, (uint32_t*)e->tmp.p, sw));
+			PL_TIME(e, sw, 2);
 		}
+	}
+	if (two) { /* join */
+		CK(cudaEventRecord(e->ev_join, e->side));
+		CK(cudaStreamWaitEvent(st, e->ev_join, 0));
 	}
 	PL_TIME(e, st, 3);
 	CKK(plk_scan_compact((plk_job_t*)e->jobs.p, n, (const uint32_t*)e->tmp.p, cig_dev, cig_cap,
@@ -428,15 +475,30 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 	CK(cudaStreamSynchronize(st));
 	if (total_out) *total_out = total_words;
 	e->last_waves = n_waves, e->last_coop = wave_n_coop;
-	if (e->timing) { /* event pairs in order: prep, (dp)*, per wave [(dp)* traceback], compact */
-		int k;
+	if (e->timing) {
+		/* event pairs: prep, every DP launch and every traceback (on the stream of their
+		 * wave), compaction.  DP time is the union of the DP launches' intervals, traceback
+		 * time the part of the tracebacks' intervals outside that union. */
+		int k, nd = 0, nb = 0;
 		float ms;
+		double dp0[sizeof(e->ev) / sizeof(e->ev[0]) / 2], dp1[sizeof(e->ev) / sizeof(e->ev[0]) / 2];
+		double all0[sizeof(e->ev) / sizeof(e->ev[0]) / 2], all1[sizeof(e->ev) / sizeof(e->ev[0]) / 2], u_dp, u_all;
 		e->acc_dp_launches += e->last_dp_launches;
 		for (q = 0; q < n; ++q) e->acc_cells += (int64_t)(e->hj[q].nl - 2) * e->hj[q].al;
 		for (k = 0; k + 1 < e->n_ev; k += 2) {
-			cudaEventElapsedTime(&ms, e->ev[k], e->ev[k + 1]);
-			e->acc_ms[e->ev_kind[k]] += ms;
+			if (e->ev_kind[k] == 1 || e->ev_kind[k] == 2) {
+				float a0, a1;
+				cudaEventElapsedTime(&a0, e->ev[0], e->ev[k]);
+				cudaEventElapsedTime(&a1, e->ev[0], e->ev[k + 1]);
+				if (e->ev_kind[k] == 1) dp0[nd] = a0, dp1[nd++] = a1;
+				all0[nb] = a0, all1[nb++] = a1;
+			} else {
+				cudaEventElapsedTime(&ms, e->ev[k], e->ev[k + 1]);
+				e->acc_ms[e->ev_kind[k]] += ms;
+			}
 		}
+		u_dp = pl_union_ms(dp0, dp1, nd), u_all = pl_union_ms(all0, all1, nb);
+		e->acc_ms[1] += u_dp, e->acc_ms[2] += u_all - u_dp;
 	}
 	ok = 1;
 fail:

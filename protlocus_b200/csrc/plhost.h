@@ -25,6 +25,10 @@ struct pl_engine_s {
 	int32_t r4_rows;                        /* jobs with at most this many DP rows take 4 rows per lane */
 	double coop_ratio;                      /* cooperative-job threshold (pl_coop_ratio by default) */
 	cudaStream_t stream;
+	/* second stream of the global DP: when a batch needs several waves, odd waves run
+	 * on it with their own trace arena, so a wave's DP fills the tail of the one before */
+	cudaStream_t side;
+	cudaEvent_t ev_fork, ev_join;
 	int64_t trace_budget;
 	dbuf_t jobs, order, counters, prep, trace, ring, tmp, total, nt, aa, ss, res, cig;
 	/* extension DP */
