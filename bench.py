@@ -13,7 +13,9 @@ bit-exact with the reference CPU path.
           step's inputs, all kernels, D2H of the results and CIGARs
   roofline  the DP kernel (k_splice_dp): algorithmic int16 lane-ops per cell
           (65 with traceback, counted from the reference SSE kernel) x cells,
-          divided by the DP kernel's own CUDA-event time, against the integer
+          divided by the DP kernel's own CUDA-event time (the union of the DP
+          launches' intervals: a batch over the trace budget runs its waves on two
+          streams, so launches of consecutive waves overlap), against the integer
           pipe's lane-op peak measured live on this device (pl_measure_int_peak)
   cpu_baseline  the reference's ns_global_gs_auto compiled from its own sources
           (oracle/_ref), driven by the reference's kt_for over all host cores, on

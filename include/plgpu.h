@@ -172,7 +172,9 @@ int pl_splice_batch_host(pl_engine_t *e, const ns_opt_t *opt,
 /* Device-resident inputs and outputs: nt/aa/ss/results/cigar are device
  * pointers; the job table is read on the host (it drives the planning).
  * Work is issued on `stream` (a cudaStream_t passed as void*, NULL = the
- * engine's own stream) and the call returns once it has completed.
+ * engine's own stream; a multi-wave batch forks half its waves onto the
+ * engine's second stream after the preparation and joins it back before the
+ * compaction) and the call returns once it has completed.
  * *total_cigar (optional) receives the number of CIGAR words produced; jobs
  * beyond cigar_cap get status -2.  Returns 1 on success. */
 int pl_splice_batch_device(pl_engine_t *e, const ns_opt_t *opt,
@@ -182,7 +184,10 @@ int pl_splice_batch_device(pl_engine_t *e, const ns_opt_t *opt,
 		int64_t *total_cigar, void *stream);
 
 /* Optional CUDA-event timing of every batch phase (prep, DP kernel, traceback,
- * compaction), accumulated until the next pl_engine_set_timing() call. */
+ * compaction), accumulated until the next pl_engine_set_timing() call.  A batch
+ * over the trace budget runs its waves alternately on the engine's stream and a
+ * second one; dp_ms is then the union of the DP launches' intervals and
+ * traceback_ms the part of the tracebacks outside it. */
 int pl_engine_set_timing(pl_engine_t *e, int32_t enable);
 void pl_engine_times(const pl_engine_t *e, double *prep_ms, double *dp_ms, double *traceback_ms,
 		double *compact_ms, int64_t *dp_launches, int64_t *cells);

@@ -349,7 +349,6 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 	}
 	cp_async_wait_all();
 	__syncwarp();
-	/* warp-uniform: the step at which the warp's lane 0 next starts a strip, and that strip */
 
 	for (int s = 0; s < total; ++s) {
 		if (__shfl_sync(FULL, c, 0) == 0) {
