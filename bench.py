@@ -68,12 +68,13 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the engine's default tuning instead of autotuning it on the workload (global DP)")
     ap.add_argument("--workload", default="global",
-                    choices=["global", "ext", "hmm", "gapless", "forward", "prefilter", "extra", "prescreen"],
+                    choices=["global", "ext", "hmm", "gapless", "forward", "prefilter", "extra", "prescreen", "chain"],
                     help="global: the batched global spliced DP (headline); ext: the batched extension DP; "
                          "hmm: the integer profile-HMM DP; gapless: the gapless X-drop prefilter; "
                          "forward: the recheck Forward score; prefilter: learned candidate prefilter vs the plain "
                          "batched DP over the held-out seed's candidates; extra: alignment statistics and exon "
-                         "features from the CIGAR; prescreen: banded gapped profile-ORF alignment")
+                         "features from the CIGAR; prescreen: banded gapped profile-ORF alignment; chain: anchor "
+                         "chaining (mp_chain) of the coarse mapping")
     ap.add_argument("--peptides", type=int, default=20000, help="peptides per step (--workload forward)")
     ap.add_argument("--candidates", type=int, default=131072, help="candidates of 8 anchors (--workload gapless)")
     ap.add_argument("--profiles", type=int, default=16, help="profiles per step (--workload hmm)")
@@ -230,6 +231,8 @@ def main():
         return main_extra(args)
     if args.workload == "prescreen":
         return main_prescreen(args)
+    if args.workload == "chain":
+        return main_chain(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -1335,6 +1338,125 @@ def main_prescreen(args):
                                 "traffic": None, "ops_per_cell": PS_OPS_PER_CELL,
                                 "peak_source": "measured live: pl_measure_int_peak, int32"},
                      cpu, clk, {"cells_per_step": int(cells), "positive_scores": int((sc > 0).sum())})
+    eng.close()
+    R.close()
+    return 0
+
+
+# ---------------------------------------------------------------------------- anchor chaining
+
+CHAIN_OPS_PER_PAIR = 47  # lane-ops per scored predecessor: comput_sc (chain.c:112-152) + the update (:184-199)
+
+
+def main_chain(args):
+    """One step = mp_chain (main-chain arguments of mp_map_coarse, map.c:630: bw = max intron
+    36000 for a 100 Mb genome, max_gap 1000, max_skip 25, kmer 6, bbit 8) over the seed anchors
+    of 10,000 synthetic query proteins, about 2^20 anchors.  value: the chaining DP on the device
+    with the anchors resident (pl_chain_fill_device, CUDA events); e2e: pl_chain_host with host
+    buffers (upload, DP, f and p back, backtrack and compaction on the host cores), wall clock."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    from protlocus_b200.abi import chain_opt, chain_opt_struct
+    R = Ranks("nccl")
+    if args.impl == "reference" and not R.is_root:
+        R.close()
+        return 0
+    n_q = 10000
+    qs = W.chain_anchors(n_q, seed=R.seed(21))
+    off, n, a = L.chain_pack(qs)
+    n_a = len(a)
+    opt = chain_opt("main")
+    desc = (f"mp_chain over {n_q} synthetic query proteins' seed anchors ({n_a} anchors: planted genes with "
+            "Poisson(4) introns, half with a paralog, Poisson(40) random hits; 100 Mb genome, bbit 8), main-chain "
+            "arguments of the coarse mapping")
+    metric = "anchor chaining (mp_chain, bit-exact) anchors/s at 1 B200"
+    threads = os.cpu_count() or 1
+    if args.impl == "reference":
+        O.ref_chain_batch(opt, off, n, a, threads)  # warm-up
+        t0 = time.perf_counter()
+        reps = 0
+        while reps < max(1, args.steps) or time.perf_counter() - t0 < 2.0:
+            O.ref_chain_batch(opt, off, n, a, threads)
+            reps += 1
+        v = n_a * reps / (time.perf_counter() - t0)
+        print(json.dumps({"metric": metric, "value": round(v, 1), "unit": "anchors/s", "n_gpus": args.gpus,
+                          "steps": reps, "warmup": 1, "ms_per_step": round(n_a / v * 1e3, 3), "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "int32+fp32", "data": "synthetic",
+                          "impl": "reference", "config": {"workload": desc},
+                          "cpu_baseline": {"value": round(v, 1), "unit": "anchors/s", "cores": threads,
+                                           "kind": "reference", "sample": "the whole batch, chain.c mp_chain per query "
+                                           "over kt_for threads"},
+                          "e2e": {"value": round(v, 1), "unit": "anchors/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        R.close()
+        return 0
+    eng = L.Engine(R.local)
+    o = chain_opt_struct(opt)
+    d_a = torch.from_numpy(a.view(np.int64).copy()).cuda()
+    d_f, d_p, d_v = (torch.zeros(n_a, dtype=torch.int32, device="cuda") for _ in range(3))
+    stream = torch.cuda.current_stream()
+
+    def fill():
+        if not eng.lib.pl_chain_fill_device(eng.h, C.byref(o), n_q, off.ctypes.data, n.ctypes.data, d_a.data_ptr(), n_a,
+                                            d_f.data_ptr(), d_p.data_ptr(), d_v.data_ptr(), stream.cuda_stream):
+            raise RuntimeError("pl_chain_fill_device: " + L.error())
+
+    for _ in range(max(3, args.warmup)):
+        fill()
+    clocks = Clocks(R.local)
+    eng.set_timing(True)
+    launches0 = L.load().pl_kernel_launch_count()
+    R.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        fill()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = L.load().pl_kernel_launch_count() - launches0
+    t = R.max(ev0.elapsed_time(ev1) / 1e3 / args.steps)
+    tm = eng.times()
+    k_s = tm["dp_ms"] / 1e3 / args.steps
+    pairs = int(eng.lib.pl_chain_last_pairs(eng.h))
+    int32_peak, _ = L.measure_int_peak(R.local)
+    achieved = pairs * CHAIN_OPS_PER_PAIR / k_s if k_s > 0 else 0.0
+    # end to end: pl_chain_host from host buffers
+    u = np.zeros(n_a, np.uint64)
+    a_out = np.zeros(n_a, np.uint64)
+    n_u = np.zeros(n_q, np.int32)
+    eng.set_timing(False)
+    R.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        if not eng.lib.pl_chain_host(eng.h, C.byref(o), n_q, off.ctypes.data, n.ctypes.data, a.ctypes.data, n_a,
+                                     u.ctypes.data, n_u.ctypes.data, a_out.ctypes.data):
+            raise RuntimeError("pl_chain_host: " + L.error())
+    te = R.max((time.perf_counter() - t0) / args.steps)
+    n_all = R.sum(n_a)
+    cpu = None
+    if R.is_root:
+        t1 = time.perf_counter()
+        tot = O.ref_chain_batch(opt, off, n, a, threads)
+        secs = time.perf_counter() - t1
+        ours = sum(int((u[off[q]: off[q] + n_u[q]] & np.uint64(0xFFFFFFFF)).sum()) for q in range(n_q))
+        cpu = {"value": round(n_a / secs, 1), "unit": "anchors/s", "cores": threads, "kind": "reference",
+               "sample": "the whole batch, chain.c mp_chain per query over kt_for threads"}
+        _simple_line(metric, n_all / t, "anchors/s", args, R.world, t * 1e3, "int32+fp32", desc,
+                     {"value": round(n_all / te, 1), "unit": "anchors/s", "ms_per_step": round(te * 1e3, 2),
+                      "h2d_bytes_per_step": int(a.nbytes + off.nbytes + n.nbytes),
+                      "d2h_bytes_per_step": int(8 * n_a), "api": "pl_chain_host (device DP, host backtrack on "
+                      f"{os.cpu_count()} threads), wall clock"},
+                     launches, {"bound": "int", "kernel": "k_chain_fill", "achieved": achieved, "peak": int32_peak,
+                                "unit": "lane-ops/s", "frac": achieved / int32_peak if int32_peak else None,
+                                "traffic": None, "ops_per_pair": CHAIN_OPS_PER_PAIR, "pairs_per_step": pairs,
+                                "kernel_ms_per_step": round(k_s * 1e3, 3),
+                                "peak_source": "measured live: pl_measure_int_peak, int32"},
+                     cpu, clk, {"anchors_per_step": n_a, "chains": int(n_u.sum()), "chained_anchors": ours,
+                                "chained_anchors_reference": tot})
     eng.close()
     R.close()
     return 0

@@ -501,6 +501,41 @@ typedef struct {
 int pl_ps_gapped_host(pl_engine_t *e, const pl_ps_job_t *jobs, int32_t n, const int8_t *pssm, int64_t l_pssm,
 		const uint8_t *orf, int64_t l_orf, int32_t go, int32_t ge, int32_t *scores);
 
+/* ---------------------------------------------------------------------------
+ * Anchor chaining (chain.c:160-219, mp_chain) of many queries at once.  A
+ * query's anchors are blockId << 32 | queryPos, sorted ascending, as mp_chain
+ * takes them; the arguments of mp_chain are the fields of pl_chain_opt_t.  The
+ * chaining DP (the score f, predecessor p and peak v of every anchor,
+ * chain.c:183-208) runs on the device, one warp per query; the backtrack and
+ * compaction (chain.c:8-110) run on the host's cores.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+	int32_t max_dist_x, max_dist_y, bw, max_skip, max_iter, min_cnt, min_sc;
+	float chn_coef_log;
+	int32_t is_spliced, kmer, bbit, pad;
+} pl_chain_opt_t;
+
+/* Host buffers.  Query q's anchors are a[off[q] .. off[q] + n[q]) of the n_a in
+ * `a`.  Out, per query: n_u[q] chains (score << 32 | #anchors, mp_chain's u[])
+ * at u + off[q] and the chained anchors in mp_chain's output order at
+ * a_out + off[q]; each region holds up to n[q] words.  Returns 1 on success. */
+int pl_chain_host(pl_engine_t *e, const pl_chain_opt_t *opt, int32_t n_q, const int64_t *off, const int32_t *n,
+		const uint64_t *a, int64_t n_a, uint64_t *u, int32_t *n_u, uint64_t *a_out);
+
+/* The chaining DP alone on device buffers (a_dev, f/p/v out, one int32 each per
+ * anchor; p = -1 where no predecessor), issued on `stream` (NULL = the engine's
+ * own); off and n are host arrays. */
+int pl_chain_fill_device(pl_engine_t *e, const pl_chain_opt_t *opt, int32_t n_q, const int64_t *off,
+		const int32_t *n, const uint64_t *a_dev, int64_t n_a, int32_t *f_dev, int32_t *p_dev, int32_t *v_dev,
+		void *stream);
+
+/* Predecessor pairs scored by the last fill run with engine timing on. */
+int64_t pl_chain_last_pairs(const pl_engine_t *e);
+
+/* The host half for one query: chains from a fill's f and p (no device). */
+int pl_chain_finish(const pl_chain_opt_t *opt, int64_t n, const uint64_t *a, const int32_t *f, const int32_t *p,
+		uint64_t *u, int32_t *n_u, uint64_t *a_out);
+
 #ifdef __cplusplus
 }
 #endif

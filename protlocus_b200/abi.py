@@ -229,3 +229,27 @@ class PsJob(C.Structure):
     """pl_ps_job_t"""
     _fields_ = [("pssm_off", C.c_int64), ("orf_off", C.c_int64), ("L", C.c_int32), ("n", C.c_int32),
                 ("diag", C.c_int32), ("band", C.c_int32)]
+
+
+class ChainOpt(C.Structure):
+    """pl_chain_opt_t: the arguments of mp_chain (chain.c:160)."""
+    _fields_ = [("max_dist_x", C.c_int32), ("max_dist_y", C.c_int32), ("bw", C.c_int32), ("max_skip", C.c_int32),
+                ("max_iter", C.c_int32), ("min_cnt", C.c_int32), ("min_sc", C.c_int32), ("chn_coef_log", C.c_float),
+                ("is_spliced", C.c_int32), ("kmer", C.c_int32), ("bbit", C.c_int32), ("pad", C.c_int32)]
+
+
+def chain_opt(kind: str = "main", max_intron: int = 36000, bbit: int = 8, kmer: int = 6) -> dict:
+    """mp_chain's arguments at the reference's defaults (options.c:44-60, index kmer 6, bbit 8):
+    "main" = the coarse chain of mp_map_coarse (map.c:630), "pre" = its pre-chain (map.c:618,
+    w = 1 << bbit); max_intron = bw, set from the genome size (options.c:31-38)."""
+    if kind == "pre":
+        w = 1 << bbit
+        return dict(max_dist_x=w, max_dist_y=w, bw=w, max_skip=25, max_iter=1000000, min_cnt=2, min_sc=0, coef=0.75,
+                    is_spliced=1, kmer=kmer, bbit=bbit)
+    return dict(max_dist_x=max_intron, max_dist_y=1000, bw=max_intron, max_skip=25, max_iter=1000000, min_cnt=3,
+                min_sc=0, coef=0.75, is_spliced=1, kmer=kmer, bbit=bbit)
+
+
+def chain_opt_struct(o: dict) -> ChainOpt:
+    return ChainOpt(o["max_dist_x"], o["max_dist_y"], o["bw"], o["max_skip"], o["max_iter"], o["min_cnt"], o["min_sc"],
+                    o["coef"], o["is_spliced"], o["kmer"], o["bbit"], 0)

@@ -56,6 +56,9 @@ struct pl_engine_s {
 	dbuf_t f_jobs, f_cig, f_nt, f_aa, f_pssm, f_mat, f_res, f_feat;
 	/* prescreen banded alignment */
 	dbuf_t s_jobs, s_pssm, s_orf, s_scr, s_score;
+	/* anchor chaining */
+	dbuf_t c_off, c_n, c_order, c_a, c_f, c_p, c_v, c_t, c_counter;
+	int64_t c_last_pairs;   /* predecessors scored by the last timed fill */
 	/* host planning scratch */
 	plk_job_t *hj;
 	int32_t *horder, *hwave, m_jobs;
@@ -85,6 +88,7 @@ void pl_rc_engine_free(pl_engine_t *e);
 void pl_pf_engine_free(pl_engine_t *e);
 void pl_feat_engine_free(pl_engine_t *e);
 void pl_ps_engine_free(pl_engine_t *e);
+void pl_chain_engine_free(pl_engine_t *e);
 int pl_ns_device(void);
 void pl_ns_set_error(const char *msg);
 

@@ -256,6 +256,23 @@ typedef struct {
 } plk_ps_args_t;
 int plk_ps_gapped(const plk_ps_args_t *a, void *stream);
 
+/* anchor chaining DP (chain.c:160-208): thread g takes query order[g], anchors a[off[q] ..
+ * off[q] + n[q]); f, p, v per anchor out, t per anchor scratch (mark stamps) */
+typedef struct {
+	const int64_t *off;
+	const int32_t *n, *order;
+	const uint64_t *a;
+	int32_t *f, *p, *v, *t;
+	unsigned long long *pairs;   /* optional: predecessors scored, summed over queries */
+	int32_t *err;                /* set non-zero by a query whose indices leave their ranges (then skipped) */
+	int64_t n_a;                 /* anchors in a / f / p / v / t */
+	int32_t n_q;
+	int32_t max_dist_x, max_dist_y, bw, max_skip, max_iter, is_spliced, kmer, bbit;
+	float coef;
+} plk_chain_args_t;
+int plk_chain_fill(const plk_chain_args_t *a, int32_t n_ctas, void *stream);
+int plk_chain_threads_per_cta(void);
+
 #ifdef __cplusplus
 }
 #endif

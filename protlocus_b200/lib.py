@@ -11,7 +11,8 @@ import re
 
 import numpy as np
 
-from .abi import ExtraJob, ExtraResult, Feat, PsJob, ExtJob, ExtResult, NsOpt, NsRst, SpliceJob, SpliceResult
+from .abi import (ChainOpt, ExtraJob, ExtraResult, Feat, PsJob, ExtJob, ExtResult, NsOpt, NsRst, SpliceJob,
+                  SpliceResult, chain_opt_struct)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libplgpu.so")
@@ -132,6 +133,17 @@ def load() -> C.CDLL:
     lib.pl_ps_gapped_host.argtypes = [C.c_void_p, C.POINTER(PsJob), C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
                                       C.c_int64, C.c_int32, C.c_int32, C.c_void_p]
     lib.pl_ps_gapped_host.restype = C.c_int
+    lib.pl_chain_host.argtypes = [C.c_void_p, C.POINTER(ChainOpt), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.pl_chain_host.restype = C.c_int
+    lib.pl_chain_fill_device.argtypes = [C.c_void_p, C.POINTER(ChainOpt), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.pl_chain_fill_device.restype = C.c_int
+    lib.pl_chain_finish.argtypes = [C.POINTER(ChainOpt), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.POINTER(C.c_int32), C.c_void_p]
+    lib.pl_chain_finish.restype = C.c_int
+    lib.pl_chain_last_pairs.argtypes = [C.c_void_p]
+    lib.pl_chain_last_pairs.restype = C.c_int64
     lib.pl_engine_set_tuning.argtypes = [C.c_void_p, C.c_int32, C.c_double]
     lib.pl_engine_get_tuning.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
     lib.pl_engine_autotune.argtypes = [C.c_void_p, C.POINTER(NsOpt), C.POINTER(SpliceJob), C.c_int32, C.c_void_p,
@@ -176,6 +188,44 @@ def error() -> str:
 
 _libc = C.CDLL(None)
 _libc.free.argtypes = [C.c_void_p]
+
+
+def chain_pack(queries):
+    """(off int64, n int32, anchors uint64) of a list of per-query anchor arrays."""
+    n = np.array([len(x) for x in queries], np.int32)
+    off = np.zeros(len(queries), np.int64)
+    if len(queries) > 1:
+        off[1:] = np.cumsum(n[:-1], dtype=np.int64)
+    a = np.concatenate([np.asarray(x, np.uint64) for x in queries]) if len(queries) else np.zeros(0, np.uint64)
+    return off, n, np.ascontiguousarray(a, np.uint64)
+
+
+def chain_unpack(off, n_u, u, a_out):
+    out = []
+    for q in range(len(off)):
+        k = int(n_u[q])
+        uq = u[off[q]: off[q] + k].copy()
+        tot = int((uq & np.uint64(0xFFFFFFFF)).sum()) if k else 0
+        out.append((uq, a_out[off[q]: off[q] + tot].copy()))
+    return out
+
+
+def chain_finish(opt: dict, a, f, p):
+    """The host half of mp_chain for one query from a fill's f and p (pl_chain_finish)."""
+    a = np.ascontiguousarray(a, np.uint64)
+    f = np.ascontiguousarray(f, np.int32)
+    p = np.ascontiguousarray(p, np.int32)
+    n = len(a)
+    u = np.zeros(max(n, 1), np.uint64)
+    a_out = np.zeros(max(n, 1), np.uint64)
+    n_u = C.c_int32()
+    o = chain_opt_struct(opt)
+    if not load().pl_chain_finish(C.byref(o), n, a.ctypes.data, f.ctypes.data, p.ctypes.data, u.ctypes.data,
+                                  C.byref(n_u), a_out.ctypes.data):
+        raise RuntimeError("pl_chain_finish: " + error())
+    k = n_u.value
+    tot = int((u[:k] & np.uint64(0xFFFFFFFF)).sum()) if k else 0
+    return u[:k].copy(), a_out[:tot].copy()
 
 
 class Engine:
@@ -292,6 +342,20 @@ class Engine:
                                           pk["orf"].ctypes.data, pk["n_orf"], go, ge, pk["score"].ctypes.data):
             raise RuntimeError("pl_ps_gapped_host: " + error())
         return pk["score"][: pk["n"]]
+
+    def chain(self, opt: dict, queries):
+        """mp_chain over many queries on the device (pl_chain_host).  queries: list of sorted
+        uint64 anchor arrays.  Returns per query (u words, chained anchors) as numpy arrays."""
+        off, n, a = chain_pack(queries)
+        n_q, n_a = len(queries), len(a)
+        u = np.zeros(max(n_a, 1), np.uint64)
+        a_out = np.zeros(max(n_a, 1), np.uint64)
+        n_u = np.zeros(max(n_q, 1), np.int32)
+        o = chain_opt_struct(opt)
+        if not self.lib.pl_chain_host(self.h, C.byref(o), n_q, off.ctypes.data, n.ctypes.data, a.ctypes.data, n_a,
+                                      u.ctypes.data, n_u.ctypes.data, a_out.ctypes.data):
+            raise RuntimeError("pl_chain_host: " + error())
+        return chain_unpack(off, n_u, u, a_out)
 
     def ps_gapped(self, cands, go: int = 11, ge: int = 1) -> np.ndarray:
         """Prescreen banded gapped scores of (pssm [L x 22] int8, orf codes, diag, band) candidates."""

@@ -344,3 +344,39 @@ def genome_fasta(n_genes: int, seed: int = 5, *, n_contigs: int = 4, contig_len:
 
     genome = fasta([(f"ctg{c}", "".join(contigs[c])) for c in range(n_contigs)])
     return genome, fasta(prots)
+
+
+def chain_anchors(n_q: int, seed: int = 7, *, genome_len: int = 100_000_000, bbit: int = 8, al_median: float = 350.0,
+                  hit_rate: float = 0.15, n_noise: float = 40.0, paralog: float = 0.5):
+    """Per-query seed anchors for mp_chain, as the coarse mapping collects them (blockId << 32 |
+    queryPos, sorted): for each query protein (length log-normal around al_median, 50-2500 aa)
+    the k-mer hits of its planted gene (exons split by Poisson(4) introns of log-normal length,
+    median 150 bp, at most 20 kb; a hit per residue with probability hit_rate), half the time
+    a weaker paralogous copy elsewhere, and Poisson(n_noise) random hits over the genome.
+    bbit = 0 gives nucleotide coordinates instead of blocks (the refinement's chaining)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_q):
+        al = int(np.clip(rng.lognormal(math.log(al_median), 0.6), 50, 2500))
+        anchors = []
+
+        def gene(rate):
+            n_exon = 1 + int(rng.poisson(4))
+            cuts = np.sort(rng.choice(np.arange(1, al), size=min(n_exon - 1, al - 1), replace=False)) if al > 1 else []
+            bounds = [0, *[int(c) for c in cuts], al]
+            span = 3 * al + 20000 * n_exon
+            g = int(rng.integers(0, max(1, genome_len - span)))
+            for e in range(len(bounds) - 1):
+                q0, q1 = bounds[e], bounds[e + 1]
+                hit = rng.random(q1 - q0) < rate
+                for q in np.nonzero(hit)[0]:
+                    anchors.append(((g + 3 * int(q)) >> bbit) << 32 | (q0 + int(q)))
+                g += 3 * (q1 - q0) + int(min(20000, rng.lognormal(math.log(150), 1.0)))
+
+        gene(hit_rate)
+        if rng.random() < paralog:
+            gene(hit_rate / 3)
+        for _ in range(int(rng.poisson(n_noise))):
+            anchors.append((int(rng.integers(0, genome_len)) >> bbit) << 32 | int(rng.integers(0, al)))
+        out.append(np.unique(np.array(anchors, dtype=np.uint64)))
+    return out

@@ -327,3 +327,45 @@ def ref_ps_gapped(pssm, orf, diag: int, band: int, go: int = 11, ge: int = 1) ->
     p = np.ascontiguousarray(np.asarray(pssm, np.int8).reshape(-1, 22))
     o = np.ascontiguousarray(np.asarray(orf, np.uint8))
     return int(ps_lib().ref_ps_gapped(p.ctypes.data, p.shape[0], o.ctypes.data, o.size, diag, band, go, ge))
+
+
+_chain = None
+
+
+def chain_lib():
+    """oracle/_ref/libchain_ref.so: the reference's own mp_chain, or None where it was not built."""
+    global _chain
+    if _chain is None:
+        path = os.path.join(ROOT, "oracle", "_ref", "libchain_ref.so")
+        if not os.path.exists(path):
+            return None
+        lib = C.CDLL(path)
+        lib.ref_chain.argtypes = [C.c_int32] * 7 + [C.c_float] + [C.c_int32] * 3 + [C.c_int64, C.c_void_p, C.c_void_p,
+                                                                                     C.c_void_p, C.c_void_p]
+        lib.ref_chain.restype = C.c_int64
+        _chain = lib
+    return _chain
+
+
+def ref_chain(opt: dict, a):
+    """(u words, chained anchors) of the reference's mp_chain over one query's sorted anchors."""
+    a = np.ascontiguousarray(a, np.uint64)
+    n = len(a)
+    u = np.zeros(max(n, 1), np.uint64)
+    out = np.zeros(max(n, 1), np.uint64)
+    n_u = C.c_int32()
+    tot = chain_lib().ref_chain(opt["max_dist_x"], opt["max_dist_y"], opt["bw"], opt["max_skip"], opt["max_iter"],
+                                opt["min_cnt"], opt["min_sc"], opt["coef"], opt["is_spliced"], opt["kmer"], opt["bbit"],
+                                n, a.ctypes.data, u.ctypes.data, C.byref(n_u), out.ctypes.data)
+    return u[:n_u.value].copy(), out[:tot].copy()
+
+
+def ref_chain_batch(opt: dict, off, n, a, threads: int) -> int:
+    """The reference's mp_chain over a packed batch on `threads` host threads (kt_for); the
+    total number of chained anchors."""
+    lib = chain_lib()
+    lib.ref_chain_batch.argtypes = [C.c_int32] * 7 + [C.c_float] + [C.c_int32] * 4 + [C.c_void_p] * 3 + [C.c_int32]
+    lib.ref_chain_batch.restype = C.c_int64
+    return int(lib.ref_chain_batch(opt["max_dist_x"], opt["max_dist_y"], opt["bw"], opt["max_skip"], opt["max_iter"],
+                                   opt["min_cnt"], opt["min_sc"], opt["coef"], opt["is_spliced"], opt["kmer"],
+                                   opt["bbit"], len(n), off.ctypes.data, n.ctypes.data, a.ctypes.data, threads))
