@@ -34,6 +34,33 @@ def test_struct_layouts_match_c(tmp_path):
     assert [int(x) for x in out] == want
 
 
+RECORDS = [("GaplessCandidate", "ns_gpu_gapless_candidate_t"), ("GaplessAnchor", "ns_gpu_gapless_anchor_t"),
+           ("SpliceJob", "pl_splice_job_t"), ("SpliceResult", "pl_splice_result_t"), ("ExtJob", "pl_ext_job_t"),
+           ("ExtResult", "pl_ext_result_t"), ("ExtraJob", "pl_extra_job_t"), ("Feat", "pl_feat_t"),
+           ("ExtraResult", "pl_extra_result_t"), ("PsJob", "pl_ps_job_t"), ("ChainOpt", "pl_chain_opt_t")]
+
+
+def test_every_record_field_offset_matches_c(tmp_path):
+    """sizeof and the offset of every field of each public record, as gcc lays them out
+    from include/plgpu.h, equal the ctypes mirrors the Python layer passes."""
+    from protlocus_b200 import abi
+    lines, want = [], []
+    for py, c in RECORDS:
+        cls = getattr(abi, py)
+        lines.append(f'printf("%zu\\n", sizeof({c}));')
+        want.append(C.sizeof(cls))
+        for name, _ in cls._fields_:
+            lines.append(f'printf("%zu\\n", offsetof({c}, {name}));')
+            want.append(getattr(cls, name).offset)
+    src = tmp_path / "off.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "plgpu.h"\nint main(void){\n' +
+                   "\n".join(lines) + "\nreturn 0;}\n")
+    exe = tmp_path / "off"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert out == want
+
+
 def test_no_device_is_an_error_not_a_fallback():
     """Without a GPU the entry points refuse: ns_gpu_init() returns 0 with a message."""
     torch = pytest.importorskip("torch")

@@ -72,3 +72,18 @@ def test_empty_and_single():
     for a in (np.zeros(0, np.uint64), np.array([5 << 32 | 7], np.uint64),
               np.array([5 << 32 | 7, 5 << 32 | 13], np.uint64)):
         _check(opt, a)
+
+
+def test_corrupt_predecessors_are_an_error():
+    """The host backtrack refuses a predecessor array with a forward or self link (it
+    would otherwise walk forever) instead of looping."""
+    opt = chain_opt("main")
+    a = np.array([(k // 3) << 32 | (5 * k) for k in range(40)], np.uint64)
+    f = np.arange(10, 50, dtype=np.int32)
+    p = np.arange(-1, 39, dtype=np.int32)
+    p[20] = 25  # a forward link
+    with pytest.raises(RuntimeError):
+        L.chain_finish(opt, a, f, p)
+    p[20] = 20  # a self link
+    with pytest.raises(RuntimeError):
+        L.chain_finish(opt, a, f, p)
