@@ -87,3 +87,21 @@ def test_corrupt_predecessors_are_an_error():
     p[20] = 20  # a self link
     with pytest.raises(RuntimeError):
         L.chain_finish(opt, a, f, p)
+
+
+@need
+@pytest.mark.parametrize("seed", range(6))
+def test_random_arguments(seed):
+    """mp_chain's arguments drawn at random (non-spliced penalties and max_drop = bw,
+    positive min_sc, min_cnt, small bw and max_dist_y, bbit 0 / 4 / 8, kmer, coefficient):
+    the restated fill plus the library's host half equal the reference."""
+    rng = np.random.default_rng(100 + seed)
+    bbit = int(rng.choice([0, 4, 8]))
+    opt = dict(max_dist_x=int(rng.integers(200, 40000)), max_dist_y=int(rng.integers(50, 2000)),
+               bw=int(rng.integers(100, 40000)), max_skip=int(rng.integers(1, 40)),
+               max_iter=int(rng.integers(3, 5000)), min_cnt=int(rng.integers(1, 5)), min_sc=int(rng.integers(0, 40)),
+               coef=float(rng.uniform(0.2, 1.5)), is_spliced=int(rng.integers(0, 2)), kmer=int(rng.integers(4, 8)),
+               bbit=bbit)
+    glen = 5_000_000 if bbit == 0 else 100_000_000
+    for a in W.chain_anchors(10, seed=200 + seed, genome_len=glen, bbit=bbit, al_median=180):
+        _check(opt, a)

@@ -82,3 +82,23 @@ def test_fill_arrays_match_restatement():
             assert np.array_equal(f[s], wf) and np.array_equal(p[s], wp) and np.array_equal(v[s], wv), q
     finally:
         eng.close()
+
+
+@need
+@pytest.mark.parametrize("seed", range(4))
+def test_random_arguments_match_reference(seed):
+    """The device DP plus host half under random mp_chain arguments (non-spliced
+    penalties, positive min_sc, small bw and max_dist_y, bbit 0 / 4 / 8, kmer, coefficient)."""
+    rng = np.random.default_rng(300 + seed)
+    bbit = int(rng.choice([0, 4, 8]))
+    opt = dict(max_dist_x=int(rng.integers(200, 40000)), max_dist_y=int(rng.integers(50, 2000)),
+               bw=int(rng.integers(100, 40000)), max_skip=int(rng.integers(1, 40)),
+               max_iter=int(rng.integers(3, 5000)), min_cnt=int(rng.integers(1, 5)), min_sc=int(rng.integers(0, 40)),
+               coef=float(rng.uniform(0.2, 1.5)), is_spliced=int(rng.integers(0, 2)), kmer=int(rng.integers(4, 8)),
+               bbit=bbit)
+    glen = 5_000_000 if bbit == 0 else 100_000_000
+    eng = L.Engine(0)
+    try:
+        _batch(eng, opt, W.chain_anchors(150, seed=400 + seed, genome_len=glen, bbit=bbit, al_median=180))
+    finally:
+        eng.close()
