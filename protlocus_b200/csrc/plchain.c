@@ -34,11 +34,22 @@ static void pl_kv_insertsort(pl_kv_t *beg, pl_kv_t *end)
 
 /* one pass on the byte of x at shift s: buckets placed in place by following
  * displacement cycles, then each bucket sorted on the next byte (more than 64
- * elements) or by insertion (2 to 64) */
+ * elements) or by insertion (2 to 64).  A pass whose keys all share the byte
+ * leaves the order as it is and hands the whole range to the next byte, so the
+ * passes above the highest byte in which the range's keys differ are skipped
+ * (identical permutation, without the 256-bucket work). */
 static void pl_kv_rsort(pl_kv_t *beg, pl_kv_t *end, int s)
 {
 	pl_kv_t *bb[256], *be[256], *i, tmp, swap;
 	int k, l;
+	{
+		uint64_t lo = beg->x, hi = beg->x, d;
+		for (i = beg + 1; i != end; ++i) lo = i->x < lo ? i->x : lo, hi = i->x > hi ? i->x : hi;
+		if (lo == hi) return; /* every pass is the identity */
+		d = lo ^ hi;
+		k = 63 - __builtin_clzll(d);  /* highest differing bit */
+		if (k / 8 * 8 < s) s = k / 8 * 8;
+	}
 	for (k = 0; k < 256; ++k) bb[k] = be[k] = beg;
 	for (i = beg; i != end; ++i) ++be[i->x >> s & 255];
 	for (k = 1; k < 256; ++k) be[k] += be[k - 1] - beg, bb[k] = be[k - 1];
