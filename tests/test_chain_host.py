@@ -105,3 +105,30 @@ def test_random_arguments(seed):
     glen = 5_000_000 if bbit == 0 else 100_000_000
     for a in W.chain_anchors(10, seed=200 + seed, genome_len=glen, bbit=bbit, al_median=180):
         _check(opt, a)
+
+
+def _golden_cases():
+    import json
+    import os
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "golden"))
+    import make_chain_golden as G
+    with open(os.path.join(here, "golden", "chain_golden.json")) as f:
+        data = json.load(f)
+    for case in data["cases"]:
+        qs = G.case_queries(case["gen"])
+        assert G.digest(qs) == case["sha256"], case["name"]  # the generator still makes the same anchors
+        yield case, qs
+
+
+def test_golden_fixture():
+    """The restated fill plus the library's host half reproduce the fixture the
+    reference's mp_chain wrote (tests/golden/make_chain_golden.py); no reference
+    build needed."""
+    for case, qs in _golden_cases():
+        for a, want in zip(qs, case["chains"]):
+            f, p, _v = CR.fill(a, case["opt"])
+            u, out = L.chain_finish(case["opt"], a, f, p)
+            assert [int(x) for x in u] == want["u"], case["name"]
+            assert [int(x) for x in out] == want["a"], case["name"]

@@ -102,3 +102,17 @@ def test_random_arguments_match_reference(seed):
         _batch(eng, opt, W.chain_anchors(150, seed=400 + seed, genome_len=glen, bbit=bbit, al_median=180))
     finally:
         eng.close()
+
+
+def test_golden_fixture_on_device():
+    """Device DP plus host half against the fixture the reference's mp_chain wrote."""
+    from test_chain_host import _golden_cases
+    eng = L.Engine(0)
+    try:
+        for case, qs in _golden_cases():
+            got = eng.chain(case["opt"], qs)
+            for (u, out), want in zip(got, case["chains"]):
+                assert [int(x) for x in u] == want["u"], case["name"]
+                assert [int(x) for x in out] == want["a"], case["name"]
+    finally:
+        eng.close()
