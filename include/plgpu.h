@@ -524,7 +524,8 @@ int pl_chain_host(pl_engine_t *e, const pl_chain_opt_t *opt, int32_t n_q, const 
 
 /* The chaining DP alone on device buffers (a_dev, f/p/v out, one int32 each per
  * anchor; p = -1 where no predecessor), issued on `stream` (NULL = the engine's
- * own); off and n are host arrays. */
+ * own); off and n are host arrays.  Returns once the DP has completed: the kernel
+ * checks every index it uses and the call fails when one was out of range. */
 int pl_chain_fill_device(pl_engine_t *e, const pl_chain_opt_t *opt, int32_t n_q, const int64_t *off,
 		const int32_t *n, const uint64_t *a_dev, int64_t n_a, int32_t *f_dev, int32_t *p_dev, int32_t *v_dev,
 		void *stream);
