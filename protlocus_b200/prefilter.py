@@ -9,7 +9,7 @@ MLP on the tensor cores (pl_pf_predict), drops candidates predicted to fail,
 tightens the windows of the others to the predicted alignment span plus a
 margin, and runs the same exact DP there; a kept candidate whose tightened DP
 does not pass falls back to its full window.  Every reported alignment comes
-from the exact DP; the plain path is the judge of recall.
+from the exact DP; recall is measured against the plain path.
 
 Training pairs are the plain path's own outcomes: label = pass, and for passing
 candidates the first and last aligned codon of the plain alignment (CIGAR M ops)
