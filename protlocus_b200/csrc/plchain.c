@@ -201,6 +201,25 @@ void pl_chain_engine_free(pl_engine_t *e)
 {
 	dbuf_free(&e->c_off), dbuf_free(&e->c_n), dbuf_free(&e->c_order), dbuf_free(&e->c_a), dbuf_free(&e->c_f);
 	dbuf_free(&e->c_p), dbuf_free(&e->c_v), dbuf_free(&e->c_t), dbuf_free(&e->c_counter);
+	if (e->c_host) cudaFreeHost(e->c_host);
+	e->c_host = 0, e->c_host_cap = 0;
+}
+
+/* the engine's pinned host buffer, grown to at least `need` bytes */
+static void *pl_chain_pinned(pl_engine_t *e, size_t need)
+{
+	if (need == 0) need = 16;
+	if (e->c_host_cap >= need) return e->c_host;
+	if (e->c_host) cudaFreeHost(e->c_host);
+	e->c_host = 0, e->c_host_cap = 0;
+	if (cudaHostAlloc(&e->c_host, need, cudaHostAllocDefault) != cudaSuccess) {
+		cudaGetLastError();
+		e->c_host = 0;
+		pl_set_error("cudaHostAlloc of %zu bytes failed", need);
+		return 0;
+	}
+	e->c_host_cap = need;
+	return e->c_host;
 }
 
 /* the options as mp_chain applies them before its fill (chain.c:173-175) */
@@ -211,21 +230,13 @@ static void pl_chain_norm(const pl_chain_opt_t *in, pl_chain_opt_t *o)
 	if (o->max_dist_y < o->bw && !o->is_spliced) o->max_dist_y = o->bw;
 }
 
-typedef struct { int64_t n; int32_t q; } pl_qkey_t;
-static int pl_cmp_qkey(const void *x, const void *y)
-{
-	const pl_qkey_t *a = (const pl_qkey_t*)x, *b = (const pl_qkey_t*)y;
-	if (a->n != b->n) return a->n > b->n ? -1 : 1;
-	return a->q - b->q;
-}
-
 PL_EXPORT int pl_chain_fill_device(pl_engine_t *e, const pl_chain_opt_t *opt, int32_t n_q, const int64_t *off,
 		const int32_t *n, const uint64_t *a_dev, int64_t n_a, int32_t *f_dev, int32_t *p_dev, int32_t *v_dev,
 		void *stream)
 {
 	pl_chain_opt_t o;
 	plk_chain_args_t A;
-	pl_qkey_t *key = 0;
+	int64_t *key = 0;
 	int32_t *order = 0, q;
 	int ok = 0;
 	cudaStream_t st;
@@ -235,11 +246,16 @@ PL_EXPORT int pl_chain_fill_device(pl_engine_t *e, const pl_chain_opt_t *opt, in
 		if (n[q] < 0 || off[q] < 0 || off[q] + n[q] > n_a) { pl_set_error("query %d: anchors outside the buffer", q); return 0; }
 	if (opt->bbit < 0 || opt->bbit > 31) { pl_set_error("bbit %d outside 0..31", opt->bbit); return 0; }
 	pl_chain_norm(opt, &o);
-	key = (pl_qkey_t*)malloc(sizeof(*key) * (size_t)n_q), order = (int32_t*)malloc(sizeof(int32_t) * (size_t)n_q);
-	if (!key || !order) { pl_set_error("out of host memory"); goto fail; }
-	for (q = 0; q < n_q; ++q) key[q].n = n[q], key[q].q = q;
-	qsort(key, (size_t)n_q, sizeof(*key), pl_cmp_qkey);
-	for (q = 0; q < n_q; ++q) order[q] = key[q].q;
+	{ /* longest first, ties by query index: a counting sort on n */
+		int32_t max_n = 0, m;
+		int64_t pos = 0;
+		for (q = 0; q < n_q; ++q) if (n[q] > max_n) max_n = n[q];
+		key = (int64_t*)calloc((size_t)max_n + 1, sizeof(int64_t)), order = (int32_t*)malloc(sizeof(int32_t) * (size_t)n_q);
+		if (!key || !order) { pl_set_error("out of host memory"); goto fail; }
+		for (q = 0; q < n_q; ++q) ++key[n[q]];
+		for (m = max_n; m >= 0; --m) { const int64_t c = key[m]; key[m] = pos, pos += c; }
+		for (q = 0; q < n_q; ++q) order[key[n[q]]++] = q;
+	}
 	CK(cudaSetDevice(e->device));
 	st = stream ? (cudaStream_t)stream : e->stream;
 	if (!dbuf_ensure(&e->c_off, sizeof(int64_t) * (size_t)n_q) || !dbuf_ensure(&e->c_n, sizeof(int32_t) * (size_t)n_q) ||
@@ -349,9 +365,9 @@ PL_EXPORT int pl_chain_host(pl_engine_t *e, const pl_chain_opt_t *opt, int32_t n
 			!dbuf_ensure(&e->c_p, sizeof(int32_t) * (size_t)(n_a > 0 ? n_a : 1)) ||
 			!dbuf_ensure(&e->c_v, sizeof(int32_t) * (size_t)(n_a > 0 ? n_a : 1)))
 		return 0;
-	hf = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n_a > 0 ? n_a : 1));
-	hp = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n_a > 0 ? n_a : 1));
-	if (!hf || !hp) { pl_set_error("out of host memory"); goto fail; }
+	hf = (int32_t*)pl_chain_pinned(e, 2 * sizeof(int32_t) * (size_t)(n_a > 0 ? n_a : 1));
+	if (!hf) goto fail;
+	hp = hf + (n_a > 0 ? n_a : 1);
 	if (n_a > 0) CK(cudaMemcpyAsync(e->c_a.p, a, sizeof(uint64_t) * (size_t)n_a, cudaMemcpyHostToDevice, st));
 	if (!pl_chain_fill_device(e, opt, n_q, off, n, (const uint64_t*)e->c_a.p, n_a, (int32_t*)e->c_f.p, (int32_t*)e->c_p.p,
 			(int32_t*)e->c_v.p, st))
@@ -375,7 +391,6 @@ PL_EXPORT int pl_chain_host(pl_engine_t *e, const pl_chain_opt_t *opt, int32_t n
 	}
 	ok = 1;
 fail:
-	free(hf), free(hp);
 	return ok;
 }
 

@@ -58,6 +58,8 @@ struct pl_engine_s {
 	dbuf_t s_jobs, s_pssm, s_orf, s_scr, s_score;
 	/* anchor chaining */
 	dbuf_t c_off, c_n, c_order, c_a, c_f, c_p, c_v, c_t, c_counter;
+	void *c_host;           /* pinned host buffer for the fill's f and p (grow-only) */
+	size_t c_host_cap;
 	int64_t c_last_pairs;   /* predecessors scored by the last timed fill */
 	/* host planning scratch */
 	plk_job_t *hj;
