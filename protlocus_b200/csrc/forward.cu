@@ -17,14 +17,18 @@
  * reference's order matters here: the bias is exp of a sum over all residues
  * of log-odds that are normalised by the Forward total, so a reordering that
  * moves the total by 1e-4 nats moves the bias by L x 1e-4 of itself.
- * What remains different is the device's expf / log1pf, within their ulp
- * bounds of the host libm's: a one-ulp change of the Forward total moves the
- * bias by about L ulps, so peptides scoring near 0 bits can differ by ~2e-5
- * bits; scores agree to ~1e-6 relative otherwise.
+ * The transcendental steps carry the host's bits too: rc_logsum's expf and
+ * log1pf are glibc's algorithms restated (glibc_mathf.cuh, equal to the host
+ * libm on every float), the length model's logf values come from the host with
+ * the peptide record, every float step is written in its rounded form (no
+ * contraction into FMA), and the null2 residue sum runs in the reference's
+ * order.  Only the final double-precision exp/log/log1p of the bias are the
+ * device's own; their results are rounded to float.
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "plk.h"
+#include "glibc_mathf.cuh"
 
 #define FULL 0xffffffffu
 #define RC_NEG (-1e30f)
@@ -38,8 +42,8 @@ enum { T_MM, T_IM, T_DM, T_BM, T_MI, T_II, T_MD, T_DD }; /* recheck.c:74 */
 __device__ __forceinline__ float ls(float a, float b)
 { /* rc_logsum, recheck.c:260-265 */
 	const float mx = a > b ? a : b, mn = a > b ? b : a;
-	if (mn <= RC_NEG || mx - mn > 50.0f) return mx;
-	return mx + log1pf(expf(mn - mx));
+	if (mn <= RC_NEG || __fsub_rn(mx, mn) > 50.0f) return mx;
+	return __fadd_rn(mx, gl_log1pf(gl_expf(__fsub_rn(mn, mx))));
 }
 
 struct FwdArgs {
@@ -72,8 +76,7 @@ __global__ void __launch_bounds__(256) k_rc_forward(FwdArgs A)
 		const float *msc = R.msc, *tsc = R.tsc;
 		const uint8_t *dsq = A.dsq + P.dsq_off;
 		const int C = (M + 31) / 32, lo = 1 + lane * C, hi = min(M + 1, lo + C);
-		const float pmove = (2.0f + 1.0f) / ((float)L + 2.0f + 1.0f);
-		const float lmove = logf(pmove), lloop = logf(1.0f - pmove);
+		const float lmove = P.lmove, lloop = P.lloop;
 		const float lE = -(float)RC_LN2;
 		const int do_null2 = P.null2;
 		float *FM = do_null2 ? A.scratch + P.scratch_off : 0, *FI = FM ? FM + (size_t)(L + 1) * W : 0;
@@ -126,7 +129,7 @@ __global__ void __launch_bounds__(256) k_rc_forward(FwdArgs A)
 		float bias = 0.0f;
 		/* ---- Backward + posterior null2 (recheck.c:321-431) ---- */
 		if (FM) {
-			const float logL = logf((float)L);
+			const float logL = P.logL;
 			float *BMg = xCf + (L + 1), *BIg = BMg + (size_t)(L + 1) * W;       /* Backward M / I rows */
 			float *bNg = BIg + (size_t)(L + 1) * W, *bJg = bNg + (L + 1), *bCg = bJg + (L + 1);
 			float bC = lmove, bE = bC + lE, bJ = RC_NEG, bN = RC_NEG;
@@ -226,24 +229,23 @@ __global__ void __launch_bounds__(256) k_rc_forward(FwdArgs A)
 				s_odds += exp((double)lnodds_x[x]);
 			}
 			const float lnodds_X = (float)log(s_odds / 20.0);
+			/* the residue sum in the reference's order (recheck.c:427), on lane 0 */
 			double n2 = 0.0;
-			for (int i = lane; i < L; i += 32) {
-				const int x = dsq[i];
-				float v = lnodds_X;
+			if (lane == 0)
+				for (int i = 0; i < L; ++i) {
+					const int x = dsq[i];
+					float v = lnodds_X;
 #pragma unroll
-				for (int q = 0; q < 20; ++q) if (x == q) v = lnodds_x[q];
-				n2 += (double)v;
-			}
-#pragma unroll
-			for (int o = 16; o >= 1; o >>= 1) n2 += __shfl_xor_sync(FULL, n2, o);
-			const double a = log(1.0 / 256.0) + n2;
-			bias = (float)(a > 0.0 ? a + log1p(exp(-a)) : log1p(exp(a)));
+					for (int q = 0; q < 20; ++q) if (x == q) v = lnodds_x[q];
+					n2 = __dadd_rn(n2, (double)v);
+				}
+			n2 = __shfl_sync(FULL, n2, 0);
+			const double a = __dadd_rn(log(1.0 / 256.0), n2);
+			bias = (float)(a > 0.0 ? __dadd_rn(a, log1p(exp(-a))) : log1p(exp(a)));
 		}
-		if (lane == 0) {
-			const float p1 = (float)L / (float)(L + 1);
-			const float null1 = (float)L * logf(p1) + logf(1.0f - p1);
-			A.bits[A.order[idx]] = (tot - null1 - bias) / (float)RC_LN2;
-			A.bias[A.order[idx]] = bias / (float)RC_LN2;
+		if (lane == 0) {  /* recheck.c:432-437; null1 = L*logf(p1) + logf(1-p1) comes from the host */
+			A.bits[A.order[idx]] = __fdiv_rn(__fsub_rn(__fsub_rn(tot, P.null1), bias), (float)RC_LN2);
+			A.bias[A.order[idx]] = __fdiv_rn(bias, (float)RC_LN2);
 		}
 		__syncwarp();
 	}
@@ -279,4 +281,29 @@ extern "C" int plk_rc_forward(const plk_rc_prof_t *prof, const plk_rc_pep_t *pep
 	k_rc_forward<<<(unsigned)grid, 32 * warps, smem, st>>>(A);
 	plk_add_launches(1);
 	return (int)cudaGetLastError();
+}
+
+__global__ void k_mathf_eval(int fn, uint32_t lo, uint32_t stride, int64_t n, float *out)
+{
+	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+		const float x = __uint_as_float(lo + (uint32_t)((uint64_t)i * stride));
+		out[i] = fn == 0 ? gl_expf(x) : gl_log1pf(x);
+	}
+}
+
+extern "C" __attribute__((visibility("default"))) int pl_rc_mathf_eval(int32_t device, int32_t fn, uint32_t lo,
+		uint32_t stride, int64_t n, float *out)
+{
+	float *d = 0;
+	if ((fn != 0 && fn != 1) || n < 0 || !out) return 0;
+	if (n == 0) return 1;
+	if (cudaSetDevice(device) != cudaSuccess || cudaMalloc((void**)&d, sizeof(float) * (size_t)n) != cudaSuccess) return 0;
+	int64_t grid = (n + 255) / 256;
+	if (grid > 148 * 16) grid = 148 * 16;
+	k_mathf_eval<<<(unsigned)grid, 256>>>(fn, lo, stride, n, d);
+	plk_add_launches(1);
+	cudaError_t e = cudaGetLastError();
+	if (e == cudaSuccess) e = cudaMemcpy(out, d, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost);
+	cudaFree(d);
+	return e == cudaSuccess;
 }

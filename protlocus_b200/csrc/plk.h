@@ -156,6 +156,9 @@ typedef struct {
 	int64_t dsq_off;      /* residue codes 0-20 */
 	int64_t scratch_off;  /* float offset of the null2 scratch: 4*(L+1)*(M+1) + 6*(L+1) floats */
 	int32_t len, prof, null2, pad;
+	/* the per-peptide logarithms of the length model, computed with the host's logf
+	 * (recheck.c:289-290, :321, :433-434) so that they carry the host libm's bits */
+	float lmove, lloop, logL, null1;
 } plk_rc_pep_t;
 #define PLK_RC_MAX_C 64                 /* columns per lane: profiles up to 32*64 = 2048 positions */
 #define PLK_RC_MAX_M (32 * PLK_RC_MAX_C)

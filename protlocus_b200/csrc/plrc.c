@@ -15,6 +15,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <math.h>
 #include "plhost.h"
 
 #define RC_NULL2_MAXCELLS 33554432LL
@@ -103,6 +104,16 @@ PL_EXPORT int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *pro
 		pep[q].dsq_off = off[q], pep[q].len = L, pep[q].prof = pid;
 		pep[q].null2 = do_null2 && cells <= RC_NULL2_MAXCELLS;
 		pep[q].scratch_off = 0;  /* set per wave below */
+		{ /* the length model's logarithms, with the expressions of recheck.c:289-290, :321 and :433-434
+		   * evaluated by the host's libm, so the device starts from the bits the reference computes */
+			const float pmove = (2.0f + 1.0f) / ((float)L + 2.0f + 1.0f);
+			const float p1 = (float)L / (float)(L + 1);
+			const float lp1 = logf(p1), l1p1 = logf(1.0f - p1);
+			const float l_term = (float)L * lp1;
+			pep[q].lmove = logf(pmove), pep[q].lloop = logf(1.0f - pmove);
+			pep[q].logL = logf((float)L);
+			pep[q].null1 = l_term + l1p1;
+		}
 		key[q].key = (int64_t)L * hp[pid].M, key[q].idx = q;
 		cells_total += (int64_t)L * hp[pid].M;
 	}

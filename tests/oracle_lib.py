@@ -254,6 +254,23 @@ def rc_encode(seq: bytes):
     return d
 
 
+def rc_ref_batch(handle, peptides, null2: bool = True, threads: int = 0):
+    """rc_score of every (profile index, residue codes) pair, run by the reference's kt_for over the host's
+    cores: (bits, bias) float32 arrays."""
+    import numpy as np
+    n = len(peptides)
+    pid = np.array([p for p, _ in peptides], dtype=np.int32)
+    lens = np.array([len(d) for _, d in peptides], dtype=np.int32)
+    offs = np.zeros(n, dtype=np.int64)
+    if n > 1:
+        offs[1:] = np.cumsum(lens[:-1])
+    dsq = np.ascontiguousarray(np.concatenate([np.asarray(d, dtype=np.uint8) for _, d in peptides]))
+    bits, bias = np.zeros(n, dtype=np.float32), np.zeros(n, dtype=np.float32)
+    rc_lib().ref_rc_bench(threads or (os.cpu_count() or 1), handle, n, pid.ctypes.data, dsq.ctypes.data,
+                          offs.ctypes.data, lens.ctypes.data, int(null2), bits.ctypes.data, bias.ctypes.data)
+    return bits, bias
+
+
 def rc_ref_score(handle, k: int, dsq, null2: bool = True):
     import numpy as np
     b, s = C.c_float(), C.c_float()
