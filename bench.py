@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--pairs", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-prefilter", action="store_true",
+                    help="leave the learned-prefilter loci/s sub-object out of the headline line")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the engine's default tuning instead of autotuning it on the workload (global DP)")
     ap.add_argument("--workload", default="global",
@@ -340,6 +342,24 @@ def main():
                                                                  args.cpu_seconds)
         cpu = {"value": round(gcups, 3), "unit": "GCUPS", "cores": threads, "kind": kind, "sample": sample}
 
+    # the second half of the metric: learned-prefilter loci/s against the plain path, same run
+    pf = None
+    eng.close()
+    del d_nt, d_aa, d_res, d_cig
+    torch.cuda.empty_cache()
+    if not args.no_prefilter:
+        pf = prefilter_measure(args, R, local, min(args.steps, 5), 3, 0.0)
+        if pf is not None:
+            pf = {k: pf[k] for k in ("metric", "value", "unit", "ms_per_step", "plain", "speedup_vs_plain",
+                                     "locus_recall", "plain_loci", "learned_loci", "extra_loci", "candidates_per_s",
+                                     "output_recall", "kept", "fallback", "phase_s", "e2e", "gpu_launches", "config")}
+            if cpu is not None:
+                cpc = pf["plain"]["cells_per_step"] / PF_N_PROT
+                pf["cpu_baseline"] = {"value": round(cpu["value"] * 1e9 / cpc, 2), "unit": "loci/s",
+                                      "cores": cpu["cores"], "kind": cpu["kind"],
+                                      "sample": "the headline's CPU GCUPS converted at this set's mean cells per locus "
+                                                "(plain path on the CPU)"}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
@@ -363,9 +383,9 @@ def main():
                          "phase_ms_per_step": {k: round(v / args.steps, 2) for k, v in tm.items() if k.endswith("_ms")}},
             "cpu_baseline": cpu,
             "clocks": clk,
+            "prefilter": pf,
         }
         print(json.dumps(line), flush=True)
-    eng.close()
     R.close()
     return 0
 
@@ -565,9 +585,9 @@ def main_ext(args):
                                                "dp_ms": round(tm["dp_ms"] / args.steps, 3)}},
             "cpu_baseline": cpu,
             "clocks": clk,
+            "prefilter": pf,
         }
         print(json.dumps(line), flush=True)
-    eng.close()
     R.close()
     return 0
 
@@ -1060,49 +1080,36 @@ PF_METRIC = "loci/sec learned-prefilter vs plain at >=99.5% locus recall (1 B200
 PF_MODEL = os.path.join(ROOT, "protlocus_b200", "data", "prefilter.npz")
 
 
-def main_prefilter(args):
-    """One step = the learned path over every candidate of the held-out seed (features,
-    MLP, exact DP on the tightened windows of the kept candidates, full-window fallback),
-    inputs resident on the device.  The plain batched DP over the same candidates is
-    timed beside it; recall = the learned path's share of the plain path's passing
-    candidates.  e2e adds the upload of the candidate sequences from pinned host memory
-    and the read-back of the pass flags to every step."""
+PF_N_PROT = 4096
+
+
+def prefilter_measure(args, R, local, steps, warmup, cpu_seconds):
+    """The learned prefilter against the plain batched DP on the held-out seed, inputs
+    resident on the device.  One step of each path covers every candidate of the seed:
+    the plain path runs the exact DP on every full window; the learned path computes
+    features, runs the MLP, runs the exact DP on the tightened windows of the kept
+    candidates and the full-window fallback.  Both then apply the reference's output test
+    per protein (mp_reg_will_output: score > 0, out_sim, out_cov), and a locus -- a
+    protein's planted gene -- counts as reported when a candidate on the gene passes.
+    Returns the measurement as a dict (rank 0; None elsewhere)."""
     import torch
     from protlocus_b200 import prefilter as P
-    R = Ranks("nccl")
-    rank, world, local = R.rank, R.world, R.local
+    rank, world = R.rank, R.world
     seed = R.seed(65)
-    cand = P.make_candidates(seed, 4096)
+    cand = P.make_candidates(seed, PF_N_PROT)
     n = len(cand["jobs"])
     n_all = R.sum(n)
+    loci_all = R.sum(PF_N_PROT)
     jobs = cand["jobs"]
     cells_plain = int(((jobs["nl"].astype(np.int64) - 2) * jobs["al"]).sum())
-    if args.impl == "reference":
-        if rank == 0:
-            gcups, threads, kind, sample, secs, acc = cpu_baseline(
-                None, cand["nt"], cand["aa"], jobs["nt_off"].copy(), jobs["aa_off"].copy(), jobs["nl"].copy(),
-                jobs["al"].copy(), Options(flag=NS_F_CIGAR), args.cpu_seconds / 2, steps=max(1, args.steps))
-            v = gcups * 1e9 / (cells_plain / n)
-            print(json.dumps({"metric": PF_METRIC, "value": round(v, 1), "unit": "candidates/s", "n_gpus": args.gpus,
-                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(n / v * 1e3, 1),
-                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16",
-                              "data": "synthetic", "impl": "reference",
-                              "config": {"workload": f"plain spliced DP over the {n} candidates of seed {seed}",
-                                         "step": "bounded sample, converted at the set's mean cells per candidate"},
-                              "cpu_baseline": {"value": round(v, 1), "unit": "candidates/s", "cores": threads,
-                                               "kind": kind, "sample": sample},
-                              "e2e": {"value": round(v, 1), "unit": "candidates/s", "h2d_bytes_per_step": 0,
-                                      "d2h_bytes_per_step": 0}}), flush=True)
-        R.close()
-        return 0
     eng = L.Engine(local)
     model, meta = P.load_model(PF_MODEL, local)
     tau, margin, tau_fb = float(meta["tau"]), int(meta["margin"]), float(meta["tau_fb"])
     pipe = P.Pipeline(eng, cand)
     if not args.no_autotune:
         pipe.autotune_paths(model, tau, margin, tau_fb)
-    plain, _, _ = pipe.plain()
-    for _ in range(max(3, args.warmup)):
+    plain, _ = pipe.plain()
+    for _ in range(max(3, warmup)):
         pipe.learned(model, tau, margin, 0.0, tau_fb)
     clocks = Clocks(local)
     eng.set_timing(True)
@@ -1111,80 +1118,123 @@ def main_prefilter(args):
     torch.cuda.synchronize()
     clocks.start()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         passed, st = pipe.learned(model, tau, margin, 0.0, tau_fb)
     torch.cuda.synchronize()
-    t_learned = (time.perf_counter() - t0) / args.steps
+    t_learned = (time.perf_counter() - t0) / steps
     R.barrier()
     clk = clocks.stop()
     launches = L.load().pl_kernel_launch_count() - launches0
     tm = eng.times()
     t_learned = R.max(t_learned)
-    pos = plain > 0
-    recall = float(passed[pos].mean()) if pos.any() else 1.0
-    # the plain batched DP over the same candidates
+    m = P.path_metrics(pipe, plain, passed)
+    # the plain batched DP over the same candidates, with the same output test
     R.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         pipe.plain()
     torch.cuda.synchronize()
-    t_plain = R.max((time.perf_counter() - t0) / args.steps)
+    t_plain = R.max((time.perf_counter() - t0) / steps)
     # end to end: candidate sequences from pinned host memory, pass flags back
     h_nt = torch.from_numpy(cand["nt"].copy()).pin_memory()
     h_aa = torch.from_numpy(cand["aa"].copy()).pin_memory()
     R.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         pipe.d_nt.copy_(h_nt, non_blocking=True)
         pipe.d_aa.copy_(h_aa, non_blocking=True)
-        p2, _ = pipe.learned(model, tau, margin, 0.0, tau_fb)
+        pipe.learned(model, tau, margin, 0.0, tau_fb)
     torch.cuda.synchronize()
-    t_e2e = R.max((time.perf_counter() - t0) / args.steps)
+    t_e2e = R.max((time.perf_counter() - t0) / steps)
     dp_s = tm["dp_ms"] / 1e3
     int32_peak, i16x2_peak = L.measure_int_peak(local)
     peak = max(int32_peak, i16x2_peak)
     achieved = tm["cells"] * OPS_PER_CELL / dp_s if dp_s > 0 else 0.0
-    cpu = None
+    out = None
     if rank == 0:
-        gcups, threads, kind, sample, _secs, _acc = cpu_baseline(
-            None, cand["nt"], cand["aa"], jobs["nt_off"].copy(), jobs["aa_off"].copy(), jobs["nl"].copy(),
-            jobs["al"].copy(), Options(flag=NS_F_CIGAR), args.cpu_seconds)
-        v = gcups * 1e9 / (cells_plain / n)
-        cpu = {"value": round(v, 1), "unit": "candidates/s", "cores": threads, "kind": kind,
-               "sample": sample + ", converted at the set's mean cells per candidate (plain path on the CPU)"}
-        line = {"metric": PF_METRIC, "value": round(n_all / t_learned, 1), "unit": "candidates/s", "n_gpus": world,
-                "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": round(t_learned * 1e3, 2),
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16+bf16",
-                "data": "synthetic",
-                "config": {"workload": f"{n} chained candidates of held-out seed {seed}: 4096 proteins x (own window "
-                                       "both strands, a partial window, 5 windows of other genes), windows 1-50 kb",
-                           "model": f"4-layer BF16 MLP {model.hidden} wide, trained on "
-                                    f"{int(meta['train_rows'])} plain-DP outcomes of seeds {meta['train_seeds']}",
-                           "tau": tau, "margin_nt": margin, "tau_fallback": tau_fb,
-                           "tuning_plain": pipe.tune_plain, "tuning_learned": pipe.tune_learned,
-                           "l2": "the candidate sequences (205 MB) and the DP trace arena exceed L2"},
-                "plain": {"value": round(n_all / t_plain, 1), "unit": "candidates/s", "ms_per_step": round(t_plain * 1e3, 2),
-                          "cells_per_step": cells_plain},
-                "speedup_vs_plain": round(t_plain / t_learned, 2),
-                "recall": round(recall, 5), "plain_pass": int(pos.sum()), "extra_pass": int((passed & ~pos).sum()),
-                "kept": st["kept"], "fallback": st["fallback"], "cells_tight_per_step": st["cells_tight"],
-                "phase_s": {"features_mlp": round(st["s_score"], 4), "dp_tight": round(st["s_dp"], 4),
-                            "dp_fallback": round(st["s_fallback"], 4)},
-                "e2e": {"value": round(n_all / t_e2e, 1), "unit": "candidates/s", "ms_per_step": round(t_e2e * 1e3, 2),
-                        "h2d_bytes_per_step": int(cand["nt"].nbytes + cand["aa"].nbytes + jobs.nbytes),
-                        "d2h_bytes_per_step": int(n * 16 * 4 + n * 4 * 4), "api": "prefilter.Pipeline over the C ABI "
-                        "(pl_pf_features_device, pl_pf_predict, pl_splice_batch_device), wall clock"},
-                "gpu_launches": int(launches),
-                "roofline": {"bound": "int", "kernel": "k_splice_dp (tightened windows)", "achieved": achieved,
-                             "peak": peak, "unit": "lane-ops/s", "frac": achieved / peak if peak else None,
-                             "traffic": None, "ops_per_cell": OPS_PER_CELL,
-                             "peak_source": "measured live: pl_measure_int_peak"},
-                "cpu_baseline": cpu, "clocks": clk}
-        print(json.dumps(line), flush=True)
+        cpu = None
+        if cpu_seconds > 0:
+            gcups, threads, kind, sample, _secs, _acc = cpu_baseline(
+                None, cand["nt"], cand["aa"], jobs["nt_off"].copy(), jobs["aa_off"].copy(), jobs["nl"].copy(),
+                jobs["al"].copy(), Options(flag=NS_F_CIGAR), cpu_seconds)
+            v = gcups * 1e9 / (cells_plain / PF_N_PROT)
+            cpu = {"value": round(v, 2), "unit": "loci/s", "cores": threads, "kind": kind,
+                   "sample": sample + ", converted at the set's mean cells per locus (plain path on the CPU)"}
+        out = {"metric": PF_METRIC, "value": round(loci_all / t_learned, 1), "unit": "loci/s", "n_gpus": world,
+               "steps": steps, "warmup": max(3, warmup), "ms_per_step": round(t_learned * 1e3, 2),
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16+bf16",
+               "data": "synthetic",
+               "config": {"workload": f"{PF_N_PROT} loci of held-out seed {seed}: per protein 8 chained candidates "
+                                      "(own window both strands, a partial window, 5 windows of other genes), "
+                                      f"{n} candidates, windows 1-50 kb",
+                          "model": f"4-layer BF16 MLP {model.hidden} wide, trained on "
+                                   f"{int(meta['train_rows'])} plain-path outcomes of seeds {meta['train_seeds']}, "
+                                   f"calibrated on seed {int(meta['val_seed'])}",
+                          "output_test": "mp_reg_will_output per protein: score > 0, >= 0.99 x best, "
+                                         "aligned query span >= 0.1 x length, first 1000",
+                          "tau": tau, "margin_nt": margin, "tau_fallback": tau_fb,
+                          "tuning_plain": pipe.tune_plain, "tuning_learned": pipe.tune_learned,
+                          "l2": "the candidate sequences (205 MB) and the DP trace arena exceed L2"},
+               "plain": {"value": round(loci_all / t_plain, 1), "unit": "loci/s",
+                         "ms_per_step": round(t_plain * 1e3, 2), "cells_per_step": cells_plain},
+               "speedup_vs_plain": round(t_plain / t_learned, 2),
+               "locus_recall": round(m["locus_recall"], 5), "plain_loci": m["plain_loci"],
+               "learned_loci": m["learned_loci"], "extra_loci": m["extra_loci"],
+               "candidates_per_s": round(n_all / t_learned, 1), "output_recall": round(m["out_recall"], 5),
+               "plain_outputs": m["plain_out"], "extra_outputs": m["extra_out"],
+               "kept": st["kept"], "fallback": st["fallback"], "cells_tight_per_step": st["cells_tight"],
+               "phase_s": {"features_mlp": round(st["s_score"], 4), "dp_tight": round(st["s_dp"], 4),
+                           "dp_fallback": round(st["s_fallback"], 4), "output_test": round(st["s_output"], 4)},
+               "e2e": {"value": round(loci_all / t_e2e, 1), "unit": "loci/s", "ms_per_step": round(t_e2e * 1e3, 2),
+                       "h2d_bytes_per_step": int(cand["nt"].nbytes + cand["aa"].nbytes + jobs.nbytes),
+                       "d2h_bytes_per_step": int(n * 16 * 4 + n * 4 * 4), "api": "prefilter.Pipeline over the C ABI "
+                       "(pl_pf_features_device, pl_pf_predict, pl_splice_batch_device), wall clock"},
+               "gpu_launches": int(launches),
+               "roofline": {"bound": "int", "kernel": "k_splice_dp (tightened windows)", "achieved": achieved,
+                            "peak": peak, "unit": "lane-ops/s", "frac": achieved / peak if peak else None,
+                            "traffic": None, "ops_per_cell": OPS_PER_CELL,
+                            "peak_source": "measured live: pl_measure_int_peak"},
+               "cpu_baseline": cpu, "clocks": clk}
     model.close()
     eng.close()
+    return out
+
+
+def main_prefilter(args):
+    """--workload prefilter: the learned path's loci/s line (see prefilter_measure).  The
+    reference arm times the plain spliced DP on the host cores over a bounded sample of the
+    same candidates, converted to loci/s at the set's mean cells per locus."""
+    from protlocus_b200 import prefilter as P
+    R = Ranks("nccl")
+    if args.impl == "reference":
+        if R.rank == 0:
+            seed = R.seed(65)
+            cand = P.make_candidates(seed, PF_N_PROT)
+            jobs = cand["jobs"]
+            n = len(jobs)
+            cells_plain = int(((jobs["nl"].astype(np.int64) - 2) * jobs["al"]).sum())
+            gcups, threads, kind, sample, secs, acc = cpu_baseline(
+                None, cand["nt"], cand["aa"], jobs["nt_off"].copy(), jobs["aa_off"].copy(), jobs["nl"].copy(),
+                jobs["al"].copy(), Options(flag=NS_F_CIGAR), args.cpu_seconds / 2, steps=max(1, args.steps))
+            v = gcups * 1e9 / (cells_plain / PF_N_PROT)
+            print(json.dumps({"metric": PF_METRIC, "value": round(v, 2), "unit": "loci/s", "n_gpus": args.gpus,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(PF_N_PROT / v * 1e3, 1),
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16",
+                              "data": "synthetic", "impl": "reference",
+                              "config": {"workload": f"plain spliced DP over the {n} candidates of the {PF_N_PROT} "
+                                                     f"loci of seed {seed}",
+                                         "step": "bounded sample, converted at the set's mean cells per locus"},
+                              "cpu_baseline": {"value": round(v, 2), "unit": "loci/s", "cores": threads,
+                                               "kind": kind, "sample": sample},
+                              "e2e": {"value": round(v, 2), "unit": "loci/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+        R.close()
+        return 0
+    line = prefilter_measure(args, R, R.local, args.steps, args.warmup, args.cpu_seconds)
+    if line is not None:
+        print(json.dumps(line), flush=True)
     R.close()
     return 0
 

@@ -119,7 +119,9 @@ double ns_gpu_d2h_seconds(void);
 ns_gpu_request_t *ns_gpu_submit(void *km, const char *ns, int32_t nl, const char *as, int32_t al,
 		const ns_opt_t *opt, const uint8_t *ss);
 /* nasw.h:151 -- block until done; 1 = r filled (nt_len, aa_len, score and the
- * CIGAR appended into r->cigar from the request's km), 0 = failed.  Frees the
+ * CIGAR appended into r->cigar from the request's km), 0 = failed (device
+ * failure, or the CIGAR could not be grown: host memory, or a km arena passed
+ * by a program that links no kalloc; ns_gpu_error() says which).  Frees the
  * request either way. */
 int ns_gpu_wait(ns_gpu_request_t *request, ns_rst_t *r);
 /* nasw.h:152 -- submit + wait. */
@@ -209,6 +211,14 @@ void pl_engine_get_tuning(const pl_engine_t *e, int32_t *r4_rows, double *coop_r
 int pl_engine_autotune(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n,
 		const uint8_t *nt, const uint8_t *aa, const uint8_t *ss, int32_t *r4_rows, double *coop_ratio);
 
+/* Host-side fault injection for failure tests (no counterpart in the
+ * reference): site 0 = a host allocation of the request queue or the
+ * extension batch object, 1 = a device buffer allocation of an engine, 2 = the
+ * next device batch of the extension executor; the site fails once, on its
+ * (after+1)-th pass from now (after < 0 disarms).  No device work is involved:
+ * the failure is the error path the real failure takes.  Returns 1 when armed. */
+int pl_debug_fault(int32_t site, int32_t after);
+
 /* Number of trace waves, cooperative jobs and DP launches of the last batch. */
 void pl_engine_last_plan(const pl_engine_t *e, int32_t *n_waves, int32_t *n_coop, int32_t *n_dp_launches);
 
@@ -225,7 +235,9 @@ void pl_engine_last_plan(const pl_engine_t *e, int32_t *n_waves, int32_t *n_coop
  * function returns only after its stream has finished and holds a library lock
  * for its whole duration, so calls never overlap on the GPU.  The first call on
  * a device looks up the array's address and caches it; make it before any
- * stream capture begins.  Returns 1 on success. */
+ * stream capture begins.  The cached address dies with the device's context:
+ * after cudaDeviceReset() the entry point must not be called again.  Returns 1
+ * on success. */
 int pl_splice_batch_noalloc(const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n_jobs,
 		const uint8_t *nt, const uint8_t *aa, const uint8_t *ss,
 		pl_splice_result_t *results_dev, uint32_t *cigar_dev, int64_t cigar_cap,
@@ -260,8 +272,15 @@ int ns_ext_batch_ready(ns_ext_batch_t *b, int32_t id);
 /* nasw.h:207 -- sleep until some outstanding flush of b completes. */
 void ns_ext_batch_wait(ns_ext_batch_t *b);
 /* nasw.h:208 -- block until request `id` is done; the result stays valid until
- * a later flush after every result of its flush was fetched. */
+ * a later flush after every result of its flush was fetched.  NULL when the
+ * request failed: its device batch failed, or host memory ran out while it was
+ * queued or flushed (ns_ext_batch_ready() is then 1 for it).  There is no CPU
+ * fallback, so the caller must check: the error text is in ns_gpu_error() and
+ * pl_last_error(), and pl_ext_failed_count() counts the failed requests.  The
+ * executor keeps serving later flushes after a failure. */
 const ns_rst_t *ns_ext_batch_get(ns_ext_batch_t *b, int32_t id);
+/* Requests of the batch objects that failed on the device (monotonic). */
+uint64_t pl_ext_failed_count(void);
 /* nasw.h:209 -- waits for b's outstanding flushes, then frees b. */
 void ns_ext_batch_destroy(ns_ext_batch_t *b);
 /* nasw.h:210-211 -- kernel launches of the extension path / requests run on the device. */
@@ -381,8 +400,12 @@ int64_t pl_gapless_last_steps(const pl_engine_t *e);
  * recheck.c:283-440 and runs from its kt_for worker, recheck.c:546-568).
  * Multihit-local Forward in log space, float, with the optional null2
  * (ByExpectation) bias correction: bits = (fwd - null1 - bias) / ln 2 and the
- * bias in bits, exactly the two numbers rc_score returns, to float rounding
- * (reduction order differs; agreement within 1e-5 relative).
+ * bias in bits, the two numbers rc_score returns.  Every float step follows
+ * rc_score's order, and rc_logsum's expf / log1pf are the host glibc's
+ * algorithms restated, so the results equal the reference's bit for bit
+ * whenever the reference runs on an x86-64 glibc 2.39 host with FMA (the only
+ * steps left to the device are the double-precision exp/log of the bias,
+ * whose results are rounded to float).
  * ------------------------------------------------------------------------- */
 typedef struct pl_rc_profile_s pl_rc_profile_t;
 /* A search profile as recheck.c builds it (rc_prof_t, recheck.c:66-72): msc
@@ -401,6 +424,12 @@ int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *profiles, int
 		int32_t do_null2, float *bits, float *bias);
 /* DP cells (sum of L*M) of the last recheck batch of this engine. */
 int64_t pl_rc_last_cells(const pl_engine_t *e);
+/* Self-check of the Forward's transcendental steps: evaluates on the device
+ * fn 0 = expf, 1 = log1pf (the restated glibc algorithms the Forward uses) at
+ * the n floats whose bit patterns are lo, lo + stride, lo + 2*stride, ... and
+ * copies the results to the host array out.  Allocates device memory per call;
+ * returns 1 on success. */
+int pl_rc_mathf_eval(int32_t device, int32_t fn, uint32_t lo, uint32_t stride, int64_t n, float *out);
 
 /* DP cells of the last extension batch: the rows the reference's row loop
  * visits (up to the x-drop row, nasw-sse.c:361-447) times al, and the nominal

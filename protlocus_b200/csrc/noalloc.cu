@@ -29,7 +29,9 @@
  *     several host threads run one after another;
  *   - the first call on a device looks the array's device address up
  *     (cudaGetSymbolAddress, with that device current) and caches it; make that
- *     first call before any stream capture begins;
+ *     first call before any stream capture begins.  The cached address belongs
+ *     to the device's context: a process that calls cudaDeviceReset() (or
+ *     otherwise tears that context down) must not call this entry point again;
  *   - no cudaMalloc, cudaFree or other allocating routine is called; host-side
  *     planning uses fixed static tables.
  * Host code must not pass g_noalloc_scratch itself to a kernel: in host code
@@ -184,6 +186,9 @@ static int na_run(const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n_jo
 	strcpy(g_na_err, "none");
 	return 1;
 cuda_fail:
+	/* work queued before the failing step may still be running on the array: wait for it (ignoring
+	 * the result) so that the array is idle once the lock is released */
+	cudaStreamSynchronize(st);
 	snprintf(g_na_err, sizeof(g_na_err), "pl_splice_batch_noalloc: %s", cudaGetErrorString(e));
 	return 0;
 }

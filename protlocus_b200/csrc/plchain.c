@@ -230,6 +230,14 @@ static void pl_chain_norm(const pl_chain_opt_t *in, pl_chain_opt_t *o)
 	if (o->max_dist_y < o->bw && !o->is_spliced) o->max_dist_y = o->bw;
 }
 
+static __thread const int32_t *pl_chain_sort_n;  /* the lengths pl_chain_cmp_len orders by */
+static int pl_chain_cmp_len(const void *x, const void *y)
+{
+	const int32_t a = *(const int32_t*)x, b = *(const int32_t*)y;
+	if (pl_chain_sort_n[a] != pl_chain_sort_n[b]) return pl_chain_sort_n[a] > pl_chain_sort_n[b] ? -1 : 1;
+	return a < b ? -1 : a > b;
+}
+
 PL_EXPORT int pl_chain_fill_device(pl_engine_t *e, const pl_chain_opt_t *opt, int32_t n_q, const int64_t *off,
 		const int32_t *n, const uint64_t *a_dev, int64_t n_a, int32_t *f_dev, int32_t *p_dev, int32_t *v_dev,
 		void *stream)
@@ -246,15 +254,24 @@ PL_EXPORT int pl_chain_fill_device(pl_engine_t *e, const pl_chain_opt_t *opt, in
 		if (n[q] < 0 || off[q] < 0 || off[q] + n[q] > n_a) { pl_set_error("query %d: anchors outside the buffer", q); return 0; }
 	if (opt->bbit < 0 || opt->bbit > 31) { pl_set_error("bbit %d outside 0..31", opt->bbit); return 0; }
 	pl_chain_norm(opt, &o);
-	{ /* longest first, ties by query index: a counting sort on n */
+	{ /* longest first, ties by query index: a counting sort on n while its table stays small next to
+	   * the batch, else a comparison sort (one long query must not cost a table of its length) */
 		int32_t max_n = 0, m;
 		int64_t pos = 0;
 		for (q = 0; q < n_q; ++q) if (n[q] > max_n) max_n = n[q];
-		key = (int64_t*)calloc((size_t)max_n + 1, sizeof(int64_t)), order = (int32_t*)malloc(sizeof(int32_t) * (size_t)n_q);
-		if (!key || !order) { pl_set_error("out of host memory"); goto fail; }
-		for (q = 0; q < n_q; ++q) ++key[n[q]];
-		for (m = max_n; m >= 0; --m) { const int64_t c = key[m]; key[m] = pos, pos += c; }
-		for (q = 0; q < n_q; ++q) order[key[n[q]]++] = q;
+		order = (int32_t*)malloc(sizeof(int32_t) * (size_t)n_q);
+		if (!order) { pl_set_error("out of host memory"); goto fail; }
+		if ((int64_t)max_n <= 4 * (int64_t)n_q + 65536) {
+			key = (int64_t*)calloc((size_t)max_n + 1, sizeof(int64_t));
+			if (!key) { pl_set_error("out of host memory"); goto fail; }
+			for (q = 0; q < n_q; ++q) ++key[n[q]];
+			for (m = max_n; m >= 0; --m) { const int64_t c = key[m]; key[m] = pos, pos += c; }
+			for (q = 0; q < n_q; ++q) order[key[n[q]]++] = q;
+		} else {
+			pl_chain_sort_n = n;
+			for (q = 0; q < n_q; ++q) order[q] = q;
+			qsort(order, (size_t)n_q, sizeof(int32_t), pl_chain_cmp_len);
+		}
 	}
 	CK(cudaSetDevice(e->device));
 	st = stream ? (cudaStream_t)stream : e->stream;

@@ -8,8 +8,10 @@
  * groups the requests by option set, packs them into staging buffers and runs
  * each group as one device batch (preparation, DP, results) on its own engine.
  * Results are fetched per request; get() blocks on the flush's completion.
- * There is no CPU fallback: a device failure aborts the process with the
- * error text (the reference's NS_EXT_GPU_STRICT behaviour).
+ * There is no CPU fallback and nothing aborts: a failed device batch (or a host
+ * allocation that fails) marks its requests as failed, ns_ext_batch_get()
+ * returns NULL for them and the error text is in ns_gpu_error() and
+ * pl_last_error().
  */
 #define _POSIX_C_SOURCE 200809L
 #include <limits.h>
@@ -229,8 +231,17 @@ PL_EXPORT int pl_ext_batch_host(pl_engine_t *e, const ns_opt_t *opt, const pl_ex
 		const int8_t *pssm, int64_t pssm_len, pl_ext_result_t *results)
 {
 	cudaStream_t st;
+	int32_t q;
 	if (!e) { pl_set_error("no engine"); return 0; }
 	if (n <= 0) return 1;
+	if (!jobs || !nt || !aa || !results) { pl_set_error("invalid batch arguments"); return 0; }
+	for (q = 0; q < n; ++q) { /* every span inside its host buffer: the kernels read exactly these bytes */
+		const pl_ext_job_t *x = &jobs[q];
+		if (!pl_span_ok("request", q, "nt", x->nt_off, x->nl, nt_len) || !pl_span_ok("request", q, "aa", x->aa_off, x->al, aa_len) ||
+				(ss && x->ss_off >= 0 && !pl_span_ok("request", q, "ss", x->ss_off, x->nl, ss_len)) ||
+				(x->pssm_off >= 0 && (!pssm || !pl_span_ok("request", q, "pssm", x->pssm_off, (int64_t)x->al * 22, pssm_len))))
+			return 0;
+	}
 	st = e->stream;
 	CK(cudaSetDevice(e->device));
 	if (!dbuf_ensure(&e->x_nt, (size_t)nt_len) || !dbuf_ensure(&e->x_aa, (size_t)aa_len) ||
@@ -264,6 +275,7 @@ typedef struct {
 	const uint8_t *ss;
 	const int8_t *pssm;
 	int32_t nl, al, flag, grp;
+	int32_t failed;         /* set by the executor when the device batch of the request failed */
 	ns_rst_t rst;
 } xr_req_t;
 
@@ -276,9 +288,13 @@ typedef struct xr_gen_s {   /* one flush ("generation") */
 	struct xr_gen_s *gnext; /* the batch object's flushes, oldest first */
 } xr_gen_t;
 
+#define XR_MAX_LOST 8
 struct ns_ext_batch_s {
 	void *km;
 	int32_t n, m, next_id;
+	int32_t pend_base;      /* id of the first queued request */
+	int32_t dropped;        /* a request could not be queued (host memory): the pending set fails at flush */
+	int32_t n_lost, lost[XR_MAX_LOST][2];  /* id ranges of flushes that failed before reaching the executor */
 	xr_req_t *req;
 	ns_opt_t *opts;         /* options of each queued request */
 	xr_gen_t *gens;
@@ -289,7 +305,7 @@ static pthread_cond_t xr_cv_work = PTHREAD_COND_INITIALIZER, xr_cv_done = PTHREA
 static xr_gen_t *xr_head, *xr_tail;
 static int xr_ready = -1;
 static pl_engine_t *xr_engine;
-static uint64_t xr_launches, xr_requests;
+static uint64_t xr_launches, xr_requests, xr_failed;
 
 static void *xr_executor(void *arg);
 
@@ -319,6 +335,7 @@ out:
 
 PL_EXPORT uint64_t ns_ext_gpu_launch_count(void) { return __sync_fetch_and_add(&xr_launches, 0ull); }
 PL_EXPORT uint64_t ns_ext_gpu_request_count(void) { return __sync_fetch_and_add(&xr_requests, 0ull); }
+PL_EXPORT uint64_t pl_ext_failed_count(void) { return __sync_fetch_and_add(&xr_failed, 0ull); }
 
 PL_EXPORT ns_ext_batch_t *ns_ext_batch_init(void *km)
 {
@@ -329,21 +346,33 @@ PL_EXPORT ns_ext_batch_t *ns_ext_batch_init(void *km)
 	return b;
 }
 
-static void xr_oom(void) { fprintf(stderr, "[plgpu] out of host memory in the extension batch\n"); abort(); }
+static void xr_fail(const char *what)
+{
+	pl_set_error("extension batch: %s", what);
+	pl_ns_set_error(pl_last_error());
+}
+
+static void *xr_malloc(size_t n) { return pl_fault_hit(PL_FAULT_HOST_ALLOC) ? 0 : malloc(n); }
+static void *xr_realloc(void *p, size_t n) { return pl_fault_hit(PL_FAULT_HOST_ALLOC) ? 0 : realloc(p, n); }
 
 PL_EXPORT int32_t ns_ext_batch_add(ns_ext_batch_t *b, const char *ns, int32_t nl, const char *as, int32_t al,
 		const ns_opt_t *opt, const uint8_t *ss)
 {
 	xr_req_t *q;
+	if (b->n == 0 && !b->dropped) b->pend_base = b->next_id;
+	if (b->dropped) return b->next_id++;  /* the pending set already lost a request: it fails as a whole */
 	if (b->n == b->m) {
 		const int32_t m = b->m ? b->m << 1 : 16;
-		xr_req_t *r = (xr_req_t*)realloc(b->req, sizeof(xr_req_t) * (size_t)m);
-		ns_opt_t *o;
-		if (!r) xr_oom();
-		b->req = r;
-		o = (ns_opt_t*)realloc(b->opts, sizeof(ns_opt_t) * (size_t)m);
-		if (!o) xr_oom();
-		b->opts = o, b->m = m;
+		xr_req_t *r = (xr_req_t*)xr_realloc(b->req, sizeof(xr_req_t) * (size_t)m);
+		ns_opt_t *o = r ? (ns_opt_t*)xr_realloc(b->opts, sizeof(ns_opt_t) * (size_t)m) : 0;
+		if (r) b->req = r;
+		if (o) b->opts = o;
+		if (!r || !o) {
+			xr_fail("out of host memory queueing a request");
+			b->dropped = 1;
+			return b->next_id++;
+		}
+		b->m = m;
 	}
 	q = &b->req[b->n];
 	memset(q, 0, sizeof(*q));
@@ -394,19 +423,45 @@ static void xr_reap(ns_ext_batch_t *b)
 	}
 }
 
+/* the pending requests can not reach the device: their ids are recorded as failed */
+static int32_t xr_lose_pending(ns_ext_batch_t *b)
+{
+	if (b->n_lost < XR_MAX_LOST) {
+		b->lost[b->n_lost][0] = b->pend_base, b->lost[b->n_lost][1] = b->next_id, ++b->n_lost;
+	} else { /* fold into the last range: ids between belong to flushes found first by xr_find */
+		b->lost[XR_MAX_LOST - 1][1] = b->next_id;
+	}
+	free(b->req), free(b->opts);
+	b->req = 0, b->opts = 0, b->n = b->m = 0, b->dropped = 0;
+	return 0;
+}
+
+static int xr_is_lost(const ns_ext_batch_t *b, int32_t id)
+{
+	int32_t k;
+	for (k = 0; k < b->n_lost; ++k)
+		if (id >= b->lost[k][0] && id < b->lost[k][1]) return 1;
+	return 0;
+}
+
 PL_EXPORT int32_t ns_ext_batch_flush(ns_ext_batch_t *b)
 {
 	xr_gen_t *g;
 	int32_t k, n;
 	if (!b) return 0;
 	xr_reap(b);
+	if (b->dropped) return xr_lose_pending(b);
 	if (b->n == 0) return 0;
-	g = (xr_gen_t*)calloc(1, sizeof(*g));
-	if (!g) xr_oom();
+	g = (xr_gen_t*)xr_malloc(sizeof(*g));
+	if (g) memset(g, 0, sizeof(*g));
+	if (g) g->grp = (xr_opt_t*)xr_malloc(sizeof(xr_opt_t) * (size_t)b->n);
+	if (!g || !g->grp) {
+		free(g);
+		xr_fail("out of host memory at flush");
+		return xr_lose_pending(b);
+	}
 	g->base = b->next_id - b->n, g->n = n = b->n;
 	g->req = b->req, b->req = 0;
-	g->grp = (xr_opt_t*)malloc(sizeof(xr_opt_t) * (size_t)n);
-	if (!g->grp) xr_oom();
 	for (k = 0; k < n; ++k) { /* distinct option sets */
 		int32_t t;
 		for (t = 0; t < g->n_grp; ++t) if (xr_same_opt(&g->grp[t].opt, &b->opts[k])) break;
@@ -441,7 +496,8 @@ static xr_gen_t *xr_find(const ns_ext_batch_t *b, int32_t id)
 PL_EXPORT int ns_ext_batch_ready(ns_ext_batch_t *b, int32_t id)
 {
 	xr_gen_t *g = b ? xr_find(b, id) : 0;
-	return g ? xr_released(g) : 0;
+	if (!g) return b && xr_is_lost(b, id);
+	return xr_released(g);
 }
 
 PL_EXPORT void ns_ext_batch_wait(ns_ext_batch_t *b)
@@ -465,12 +521,12 @@ PL_EXPORT void ns_ext_batch_wait(ns_ext_batch_t *b)
 PL_EXPORT const ns_rst_t *ns_ext_batch_get(ns_ext_batch_t *b, int32_t id)
 {
 	xr_gen_t *g = b ? xr_find(b, id) : 0;
-	if (!g) return 0;
+	if (!g) return 0;  /* unknown id, or a flush that failed before reaching the device */
 	pthread_mutex_lock(&xr_mu);
 	while (!g->done) pthread_cond_wait(&xr_cv_done, &xr_mu);
 	pthread_mutex_unlock(&xr_mu);
 	++g->n_got;
-	return &g->req[id - g->base].rst;
+	return g->req[id - g->base].failed ? 0 : &g->req[id - g->base].rst;
 }
 
 PL_EXPORT void ns_ext_batch_destroy(ns_ext_batch_t *b)
@@ -522,19 +578,25 @@ static int xr_run(const ns_opt_t *o, const xr_ref_t *refs, int32_t n)
 		if (r->ss) memcpy(ss + p_ss, r->ss, (size_t)r->nl), x->ss_off = p_ss, p_ss += r->nl;
 		if (r->pssm) memcpy(ps + p_ps, r->pssm, (size_t)r->al * 22), x->pssm_off = p_ps, p_ps += (int64_t)r->al * 22;
 	}
-	ok = pl_ext_batch_host(xr_engine, o, jobs, n, nt, l_nt, aa, l_aa, ss, l_ss, ps, l_ps, res);
+	ok = !pl_fault_hit(PL_FAULT_EXT_BATCH);
+	if (!ok) pl_set_error("extension DP batch failed (injected)");
+	else ok = pl_ext_batch_host(xr_engine, o, jobs, n, nt, l_nt, aa, l_aa, ss, l_ss, ps, l_ps, res);
 	if (ok) {
 		for (q = 0; q < n; ++q) {
 			xr_req_t *r = &refs[q].g->req[refs[q].k];
-			if (res[q].status != 0) { ok = 0; break; }
+			if (res[q].status != 0) { ok = 0; pl_set_error("extension request failed on the device"); break; }
 			r->rst.n_cigar = 0, r->rst.nt_len = res[q].nt_len, r->rst.aa_len = res[q].aa_len, r->rst.score = res[q].score;
 		}
 		__sync_fetch_and_add(&xr_launches, (uint64_t)xr_engine->x_last_launches);
 	}
 out:
-	if (!ok) { /* no CPU path to fall back on: fail loudly */
-		fprintf(stderr, "[plgpu] extension DP batch of %d requests failed: %s\n", n, pl_last_error());
-		abort();
+	if (!ok) { /* no CPU path to fall back on: every request of the batch reports failure */
+		char msg[1100];
+		snprintf(msg, sizeof(msg), "extension DP batch of %d requests failed: %s", n, pl_last_error());
+		pl_set_error("%s", msg);
+		pl_ns_set_error(msg);
+		for (q = 0; q < n; ++q) refs[q].g->req[refs[q].k].failed = 1;
+		__sync_fetch_and_add(&xr_failed, (uint64_t)n);
 	}
 	free(jobs), free(res), free(nt), free(aa), free(ss), free(ps);
 	return ok;
@@ -553,10 +615,15 @@ static void *xr_executor(void *arg)
 		list = xr_head, xr_head = xr_tail = 0;
 		pthread_mutex_unlock(&xr_mu);
 		for (g = list; g; g = g->qnext) total += g->n;
-		refs = (xr_ref_t*)malloc(sizeof(xr_ref_t) * (size_t)(total > 0 ? total : 1));
-		if (!refs) xr_oom();
+		refs = (xr_ref_t*)xr_malloc(sizeof(xr_ref_t) * (size_t)(total > 0 ? total : 1));
+		if (!refs) { /* every request of these flushes fails */
+			xr_fail("out of host memory in the executor");
+			for (g = list; g; g = g->qnext)
+				for (k = 0; k < g->n; ++k) g->req[k].failed = 1;
+			__sync_fetch_and_add(&xr_failed, (uint64_t)total);
+		}
 		/* every waiting flush, grouped by option set across flushes: one device batch per set */
-		for (g = list; g; g = g->qnext) {
+		for (g = refs ? list : 0; g; g = g->qnext) {
 			int32_t t;
 			for (t = 0; t < g->n_grp; ++t) {
 				const ns_opt_t *o = &g->grp[t].opt;

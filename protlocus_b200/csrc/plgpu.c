@@ -44,11 +44,53 @@
  * (Python, tests) must pass km == NULL and get plain realloc. */
 extern void *krealloc(void *km, void *ptr, size_t size) __attribute__((weak));
 
+/* NULL (with the error text set) when the allocation fails or a km arena is passed by a
+ * program that links no kalloc; the old block then stays valid */
 static void *pl_krealloc(void *km, void *ptr, size_t size)
 {
-	if (krealloc) return krealloc(km, ptr, size);
-	if (km) { fprintf(stderr, "[plgpu] a km arena was passed but the program links no kalloc\n"); abort(); }
-	return realloc(ptr, size);
+	void *q;
+	if (pl_fault_hit(PL_FAULT_HOST_ALLOC)) q = 0;
+	else if (krealloc) q = krealloc(km, ptr, size);
+	else if (km) {
+		pl_set_error("a km arena was passed but the program links no kalloc");
+		return 0;
+	} else q = realloc(ptr, size);
+	if (!q) pl_set_error("out of host memory for a CIGAR of %zu bytes", size);
+	return q;
+}
+
+/* ------------------------------------------------------------------ host-side fault injection (tests) */
+
+static int32_t pl_fault_after[PL_FAULT_N];
+static pthread_mutex_t pl_fault_mu = PTHREAD_MUTEX_INITIALIZER;
+
+int pl_fault_hit(int site)
+{
+	int hit = 0;
+	if (site < 0 || site >= PL_FAULT_N || __atomic_load_n(&pl_fault_after[site], __ATOMIC_RELAXED) <= 0) return 0;
+	pthread_mutex_lock(&pl_fault_mu);
+	if (pl_fault_after[site] > 0 && --pl_fault_after[site] == 0) hit = 1, pl_fault_after[site] = 0;
+	pthread_mutex_unlock(&pl_fault_mu);
+	return hit;
+}
+
+int pl_span_ok(const char *rec, int32_t q, const char *buf, int64_t off, int64_t len, int64_t cap)
+{
+	if (off < 0 || len < 0 || off > cap || len > cap - off) {
+		pl_set_error("%s %d: %s span [%lld, +%lld) outside the %lld-byte buffer", rec, q, buf, (long long)off,
+				(long long)len, (long long)cap);
+		return 0;
+	}
+	return 1;
+}
+
+PL_EXPORT int pl_debug_fault(int32_t site, int32_t after)
+{
+	if (site < 0 || site >= PL_FAULT_N) return 0;
+	pthread_mutex_lock(&pl_fault_mu);
+	pl_fault_after[site] = after < 0 ? 0 : after + 1;
+	pthread_mutex_unlock(&pl_fault_mu);
+	return 1;
 }
 
 /* ------------------------------------------------------------------ errors */
@@ -76,6 +118,10 @@ int dbuf_ensure(dbuf_t *b, size_t need)
 	if (b->cap >= need) return 1;
 	if (b->p) cudaFree(b->p);
 	b->p = 0, b->cap = 0;
+	if (pl_fault_hit(PL_FAULT_DEV_ALLOC)) {
+		pl_set_error("cudaMalloc of %zu bytes failed (injected)", need);
+		return 0;
+	}
 	if (cudaMalloc(&b->p, need) != cudaSuccess) {
 		cudaGetLastError();
 		pl_set_error("cudaMalloc of %zu bytes failed", need);
@@ -587,7 +633,14 @@ PL_EXPORT int pl_splice_batch_host(pl_engine_t *e, const ns_opt_t *opt, const pl
 {
 	cudaStream_t st;
 	int64_t total = 0;
+	int32_t q;
 	if (!e) { pl_set_error("no engine"); return 0; }
+	if (n < 0 || (n > 0 && (!jobs || !nt || !aa || !results))) { pl_set_error("invalid batch arguments"); return 0; }
+	for (q = 0; q < n; ++q) /* every span inside its host buffer: the kernels read exactly these bytes */
+		if (!pl_span_ok("job", q, "nt", jobs[q].nt_off, jobs[q].nl, nt_len) ||
+				!pl_span_ok("job", q, "aa", jobs[q].aa_off, jobs[q].al, aa_len) ||
+				(ss && jobs[q].ss_off >= 0 && !pl_span_ok("job", q, "ss", jobs[q].ss_off, jobs[q].nl, ss_len)))
+			return 0;
 	st = e->stream;
 	CK(cudaSetDevice(e->device));
 	if (!dbuf_ensure(&e->nt, (size_t)nt_len) || !dbuf_ensure(&e->aa, (size_t)aa_len) ||
@@ -848,8 +901,14 @@ PL_EXPORT int ns_gpu_wait(ns_gpu_request_t *r, ns_rst_t *rst)
 			const uint32_t op = r->cigar[k] & 0xf, len = r->cigar[k] >> 4;
 			if (rst->n_cigar == 0 || op != (rst->cigar[rst->n_cigar - 1] & 0xf) || op == NS_CIGAR_F || op == NS_CIGAR_G) {
 				if (rst->n_cigar == rst->m_cigar) {
-					rst->m_cigar += (rst->m_cigar >> 1) + 8;
-					rst->cigar = (uint32_t*)pl_krealloc(r->km, rst->cigar, sizeof(uint32_t) * (size_t)rst->m_cigar);
+					const int32_t m = rst->m_cigar + (rst->m_cigar >> 1) + 8;
+					uint32_t *c = (uint32_t*)pl_krealloc(r->km, rst->cigar, sizeof(uint32_t) * (size_t)m);
+					if (!c) { /* the CIGAR so far stays in rst; the request reports failure */
+						pl_ns_set_error(pl_last_error());
+						success = 0;
+						break;
+					}
+					rst->cigar = c, rst->m_cigar = m;
 				}
 				rst->cigar[rst->n_cigar++] = len << 4 | op;
 			} else rst->cigar[rst->n_cigar - 1] += len << 4;

@@ -16,6 +16,13 @@
 	pl_set_error("%s failed: %s", #call, cudaGetErrorString((cudaError_t)_e)); goto fail; } } while (0)
 
 /* grow-only device buffer */
+/* host-side fault injection for the failure tests (pl_debug_fault): a site fails once, after
+ * a set number of passes; no device work is involved */
+enum { PL_FAULT_HOST_ALLOC = 0, PL_FAULT_DEV_ALLOC = 1, PL_FAULT_EXT_BATCH = 2, PL_FAULT_N = 3 };
+int pl_fault_hit(int site);
+/* 1 when [off, off+len) lies inside a buffer of cap bytes, else 0 with the error text set */
+int pl_span_ok(const char *rec, int32_t q, const char *buf, int64_t off, int64_t len, int64_t cap);
+
 typedef struct { void *p; size_t cap; } dbuf_t;
 int dbuf_ensure(dbuf_t *b, size_t need);
 void dbuf_free(dbuf_t *b);

@@ -125,6 +125,11 @@ def load() -> C.CDLL:
     lib.pl_rc_score_host.restype = C.c_int
     lib.pl_rc_last_cells.argtypes = [C.c_void_p]
     lib.pl_rc_last_cells.restype = C.c_int64
+    lib.pl_rc_mathf_eval.argtypes = [C.c_int32, C.c_int32, C.c_uint32, C.c_uint32, C.c_int64, C.c_void_p]
+    lib.pl_rc_mathf_eval.restype = C.c_int
+    lib.pl_debug_fault.argtypes = [C.c_int32, C.c_int32]
+    lib.pl_debug_fault.restype = C.c_int
+    lib.pl_ext_failed_count.restype = C.c_uint64
     lib.pl_extra_cal_host.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.POINTER(ExtraJob), C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
                                       C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.POINTER(ExtraResult),
@@ -609,7 +614,7 @@ class ExtBatch:
     def get(self, rid: int):
         p = self.lib.ns_ext_batch_get(self.h, rid)
         if not p:
-            raise KeyError(rid)
+            raise RuntimeError(f"extension request {rid} failed: " + self.lib.ns_gpu_error().decode())
         r = p.contents
         return (r.score, r.nt_len, r.aa_len)
 

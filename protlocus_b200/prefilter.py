@@ -2,8 +2,14 @@
 
 A chained candidate is a protein and the genomic window its chain spans, on one
 strand.  The plain path runs the exact spliced DP (pl_splice_batch_device) over
-every candidate window; a candidate "passes" when the DP score is positive (the
-`sc > 0` test of mp_reg_will_output, map.c:459-461).  The learned path computes
+every candidate window; a candidate "passes" when it survives the reference's
+output test, mp_reg_will_output (map.c:442-468), applied per protein: among the
+protein's aligned candidates ranked by score, within the first out_n, score > 0,
+score >= out_sim x the best score and an aligned query span of at least
+out_cov x the protein length (options.c:63-65: out_n 1000, out_sim 0.99,
+out_cov 0.1).  A protein's locus (its planted gene) is reported when one of the
+candidates on that gene -- its own window on either strand, or the partial window
+cutting the gene -- passes.  The learned path computes
 features on the device (pl_pf_features_device), scores them with a 4-layer BF16
 MLP on the tensor cores (pl_pf_predict), drops candidates predicted to fail,
 tightens the windows of the others to the predicted alignment span plus a
@@ -13,7 +19,8 @@ from the exact DP; recall is measured against the plain path.
 
 Training pairs are the plain path's own outcomes: label = pass, and for passing
 candidates the first and last aligned codon of the plain alignment (CIGAR M ops)
-as fractions of the window.
+as fractions of the window.  Recall is measured per locus: the share of the
+loci the plain path reports that the learned path reports too.
 
 Synthetic candidates (make_candidates) follow the batched configuration: per
 protein (log-normal length, median 350 aa, 50-2500) one window of 1-50 kb holding
@@ -36,7 +43,9 @@ from .abi import NS_F_CIGAR, Options, SpliceJob, SpliceResult
 
 FDIM = 576
 JOB_DTYPE = np.dtype([("nt_off", "<i8"), ("aa_off", "<i8"), ("ss_off", "<i8"), ("nl", "<i4"), ("al", "<i4")])
+RES_DTYPE = np.dtype([("score", "<i4"), ("n_cigar", "<i4"), ("cigar_off", "<i8"), ("mode", "<i4"), ("status", "<i4")])
 KIND_OWN_PLUS, KIND_OWN_MINUS, KIND_PARTIAL, KIND_OTHER = 0, 1, 2, 3
+OUT_N, OUT_SIM, OUT_COV = 1000, 0.99, 0.1  # the reference's output defaults (options.c:63-65)
 
 
 def make_candidates(seed: int, n_prot: int = 4096, n_other: int = 5, *, win_min: int = 1000, win_max: int = 50000,
@@ -106,13 +115,13 @@ def cigar_bounds(cig: np.ndarray, res, min_run: int = 10) -> tuple[np.ndarray, n
     at the window start and a long intron, and closes the same way; the runs skip
     those."""
     n = len(res)
-    offs = np.array([r.cigar_off for r in res], np.int64)
-    cnt = np.array([r.n_cigar for r in res], np.int64)
+    offs = np.asarray(res["cigar_off"], np.int64)
+    cnt = np.asarray(res["n_cigar"], np.int64)
     start = np.full(n, -1, np.int64)
     end = np.full(n, -1, np.int64)
     if n == 0 or cnt.sum() == 0:
         return start, end
-    idx = np.concatenate([np.arange(o, o + c) for o, c in zip(offs, cnt)])
+    idx = np.repeat(offs, cnt) + (np.arange(int(cnt.sum())) - np.repeat(np.cumsum(cnt) - cnt, cnt))
     w = cig[idx].astype(np.int64)
     op, ln = w & 15, w >> 4
     ntc = np.where((op == 0) | (op == 2), 3 * ln, np.where(op == 1, 0, ln))
@@ -131,6 +140,75 @@ def cigar_bounds(cig: np.ndarray, res, min_run: int = 10) -> tuple[np.ndarray, n
     start[has] = cum[fm[has]] - ntc[fm[has]] - base[has]
     end[has] = cum[lm[has]] - base[has]
     return start, end
+
+
+def query_span(cig: np.ndarray, res: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """Aligned query span of each job: the residue where its first codon match (M op)
+    starts and the residue where its last one ends (0, 0 without one).  res is a
+    RES_DTYPE array whose CIGARs lie back to back in cig (as the compaction writes them)."""
+    n = len(res)
+    qs, qe = np.zeros(n, np.int64), np.zeros(n, np.int64)
+    cnt = res["n_cigar"].astype(np.int64)
+    if n == 0 or cnt.sum() == 0:
+        return qs, qe
+    start = res["cigar_off"].astype(np.int64)
+    total = int(cnt.sum())
+    seg = np.repeat(np.arange(n), cnt)
+    idx = start[seg] + (np.arange(total) - np.repeat(np.cumsum(cnt) - cnt, cnt))
+    w = cig[idx].astype(np.int64)
+    op, ln = w & 15, w >> 4
+    # residues consumed (align.c:173-215): M and I one per unit, G and the split codon of U/V one per op
+    aac = np.where((op == 0) | (op == 1), ln, np.where((op == 11) | (op == 12) | (op == 13), 1, 0))
+    cum = np.cumsum(aac)
+    base = np.zeros(n, np.int64)
+    has_any = cnt > 0
+    first = np.cumsum(cnt) - cnt
+    base[has_any] = cum[first[has_any]] - aac[first[has_any]]
+    isM = op == 0
+    big = total + 1
+    fm, lm = np.full(n, big), np.full(n, -1)
+    pos = np.arange(total)
+    np.minimum.at(fm, seg[isM], pos[isM])
+    np.maximum.at(lm, seg[isM], pos[isM])
+    has = lm >= 0
+    qs[has] = cum[fm[has]] - aac[fm[has]] - base[has]
+    qe[has] = cum[lm[has]] - base[has]
+    return qs, qe
+
+
+def output_set(score: np.ndarray, qs: np.ndarray, qe: np.ndarray, prot: np.ndarray, qlen: np.ndarray,
+               aligned: np.ndarray | None = None, out_n: int = OUT_N, out_sim: float = OUT_SIM,
+               out_cov: float = OUT_COV) -> np.ndarray:
+    """Candidates that mp_reg_will_output's final test (map.c:456-462) lets through, per
+    protein: among the protein's aligned candidates ranked by decreasing score (ties by
+    candidate order), the first out_n with score > 0, score >= out_sim x the best score
+    and qe - qs >= out_cov x qlen.  aligned: candidates that have a result (all when None)."""
+    n = len(score)
+    ok = np.ones(n, bool) if aligned is None else aligned.astype(bool)
+    sc = score.astype(np.int64)
+    order = np.lexsort((np.arange(n), -sc, prot))          # by protein, then score descending
+    order = order[ok[order]]
+    p_sorted = prot[order]
+    first = np.ones(len(order), bool)
+    first[1:] = p_sorted[1:] != p_sorted[:-1]
+    grp_start = np.maximum.accumulate(np.where(first, np.arange(len(order)), 0))
+    rank = np.arange(len(order)) - grp_start
+    best = sc[order][grp_start]
+    c = order
+    passes = (sc[c] > 0) & (sc[c] >= best.astype(np.float64) * out_sim) & \
+             ((qe[c] - qs[c]) >= qlen[c].astype(np.float64) * out_cov) & (rank < out_n)
+    out = np.zeros(n, bool)
+    out[c[passes]] = True
+    return out
+
+
+def loci_reported(out: np.ndarray, prot: np.ndarray, kind: np.ndarray, n_prot: int) -> np.ndarray:
+    """Per protein: its planted gene is reported (a candidate on the gene -- own window on
+    either strand or the partial window -- is in the output set)."""
+    on_gene = out & (kind != KIND_OTHER)
+    rep = np.zeros(n_prot, bool)
+    rep[prot[on_gene]] = True
+    return rep
 
 
 class PrefilterModel:
@@ -237,19 +315,42 @@ class Pipeline:
             raise RuntimeError("pl_pf_features_device: " + L.error())
         return feats, chain
 
-    def plain(self, bounds: bool = False):
-        """The plain path: the exact DP over every candidate's full window."""
+    def plain(self):
+        """The plain path: the exact DP over every candidate's full window, then the output
+        test per protein.  Returns (output mask, scores)."""
         self._use(self.tune_plain)
-        return self.dp(self.cand["jobs"], bounds)
+        score, qs, qe = self.dp(self.cand["jobs"], spans=True)
+        return self.decide(score, qs, qe), score
 
-    def dp(self, jobs: np.ndarray, bounds: bool = False):
+    def decide(self, score, qs, qe, aligned=None):
+        """The output set of a path's results (mp_reg_will_output's test, per protein)."""
+        c = self.cand
+        return output_set(score, qs, qe, c["prot"], c["jobs"]["al"], aligned)
+
+    def loci(self, out):
+        """Per protein: its planted gene is reported."""
+        c = self.cand
+        return loci_reported(out, c["prot"], c["kind"], int(c["prot"].max()) + 1 if len(c["prot"]) else 0)
+
+    def dp(self, jobs: np.ndarray, bounds: bool = False, spans: bool = False):
         """Exact spliced DP with CIGAR over `jobs` (device-resident sequences): scores, and
-        the aligned span (first/last codon match) when bounds."""
-        import torch
+        from the CIGARs either the aligned window span (first/last run of codon matches,
+        bounds) or the aligned query span (first/last codon match, spans)."""
         n = len(jobs)
         if n == 0:
             z = np.zeros(0, np.int64)
             return np.zeros(0, np.int32), z, z
+        res, cig = self.dp_raw(jobs, bounds or spans)
+        score = res["score"].copy()
+        if not bounds and not spans:
+            return score, None, None
+        s, e = query_span(cig, res) if spans else cigar_bounds(cig, res)
+        return score, s, e
+
+    def dp_raw(self, jobs: np.ndarray, cigars: bool = True):
+        """The DP results of `jobs` (RES_DTYPE) and the CIGAR words (None unless cigars)."""
+        import torch
+        n = len(jobs)
         cap = int(jobs["al"].astype(np.int64).sum() * 4 + 256 * n)
         d_res = torch.zeros(n * C.sizeof(SpliceResult), dtype=torch.uint8, device=self.dev)
         d_cig = torch.zeros(cap, dtype=torch.int32, device=self.dev)
@@ -259,18 +360,16 @@ class Pipeline:
                                                    self.d_aa.data_ptr(), None, d_res.data_ptr(), d_cig.data_ptr(),
                                                    cap, C.byref(total), stream):
             raise RuntimeError("pl_splice_batch_device: " + L.error())
-        res = (SpliceResult * n).from_buffer_copy(d_res.cpu().numpy().tobytes())
-        score = np.array([r.score for r in res], np.int32)
-        if not bounds:
-            return score, None, None
-        cig = d_cig[: int(total.value)].cpu().numpy()
-        s, e = cigar_bounds(cig, res)
-        return score, s, e
+        res = np.frombuffer(d_res.cpu().numpy().tobytes(), RES_DTYPE)
+        if (res["status"] != 0).any():
+            raise RuntimeError(f"{int((res['status'] != 0).sum())} DP jobs failed")
+        return res, (d_cig[: int(total.value)].cpu().numpy() if cigars else None)
 
-    def targets(self, score, s, e):
-        """[label, start fraction, end fraction, box weight] rows for training."""
+    def targets(self, passed, s, e):
+        """[label, start fraction, end fraction, box weight] rows for training: label = the
+        candidate is in the plain path's output set."""
         nl = self.cand["jobs"]["nl"].astype(np.float64)
-        y = (score > 0).astype(np.float32)
+        y = passed.astype(np.float32)
         T = np.zeros((self.n, 4), np.float32)
         T[:, 0] = y
         T[:, 1] = np.where(y > 0, s / nl, 0.0)
@@ -305,9 +404,10 @@ class Pipeline:
         return jobs
 
     def learned(self, model: PrefilterModel, tau: float, margin: int, rel: float = 0.0, tau_fb: float = 0.0):
-        """The learned path: (pass mask over all candidates, stats).  Candidates with
-        p >= tau run the exact DP on their tightened windows; those that do not pass
-        there and have p >= tau_fb run it again on the full window."""
+        """The learned path: (output mask over all candidates, stats).  Candidates with
+        p >= tau run the exact DP on their tightened windows; those whose score there is
+        not positive and have p >= tau_fb run it again on the full window; the output test
+        then runs per protein over the candidates that were aligned."""
         import torch
         t0 = time.perf_counter()
         feats, chain = self.features()
@@ -319,20 +419,26 @@ class Pipeline:
         keep = np.nonzero(z >= _logit(tau))[0]
         jobs = self.tightened(keep, o, ch, margin, rel)
         self._use(self.tune_learned)
-        sc, _, _ = self.dp(jobs)
+        sc, qs, qe = self.dp(jobs, spans=True)
         t2 = time.perf_counter()
-        fail = keep[sc <= 0]
-        fail = fail[z[fail] >= _logit(tau_fb)]
+        bad = sc <= 0
+        fail = keep[bad]
+        fb = z[fail] >= _logit(tau_fb)
+        fail = fail[fb]
         self._use(self.tune_plain)
-        sc2, _, _ = self.dp(self.cand["jobs"][fail])
+        sc2, qs2, qe2 = self.dp(self.cand["jobs"][fail], spans=True)
         torch.cuda.synchronize()
         t3 = time.perf_counter()
-        passed = np.zeros(self.n, bool)
-        passed[keep[sc > 0]] = True
-        passed[fail[sc2 > 0]] = True
+        score = np.zeros(self.n, np.int32)
+        qsa, qea = np.zeros(self.n, np.int64), np.zeros(self.n, np.int64)
+        aligned = np.zeros(self.n, bool)
+        score[keep], qsa[keep], qea[keep], aligned[keep] = sc, qs, qe, True
+        score[fail], qsa[fail], qea[fail] = sc2, qs2, qe2
+        passed = self.decide(score, qsa, qea, aligned)
+        t4 = time.perf_counter()
         cells_tight = int(((jobs["nl"].astype(np.int64) - 2) * jobs["al"]).sum())
         stats = {"kept": int(len(keep)), "fallback": int(len(fail)), "cells_tight": cells_tight,
-                 "s_score": t1 - t0, "s_dp": t2 - t1, "s_fallback": t3 - t2, "s_total": t3 - t0}
+                 "s_score": t1 - t0, "s_dp": t2 - t1, "s_fallback": t3 - t2, "s_output": t4 - t3, "s_total": t4 - t0}
         return passed, stats
 
 
@@ -372,9 +478,12 @@ def build_set(eng: L.Engine, seeds, n_prot: int, workers: int = 8, log=None):
         f, _ = pipe.features()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        sc, s, e = pipe.dp(cand["jobs"], bounds=True)
+        res, cig = pipe.dp_raw(cand["jobs"])
         dp_s += time.perf_counter() - t0
-        T = pipe.targets(sc, s, e)
+        sc = res["score"].copy()
+        s, e = cigar_bounds(cig, res)
+        qs, qe = query_span(cig, res)
+        T = pipe.targets(pipe.decide(sc, qs, qe), s, e)
         feats.append(f[: pipe.n])
         targets.append(torch.from_numpy(T).to(pipe.dev))
         labels.append(T[:, 0] > 0.5)
@@ -465,12 +574,12 @@ def evaluate(eng: L.Engine, model: PrefilterModel, cand: dict, tau: float, margi
     import torch
     pipe = Pipeline(eng, cand)
     pipe.autotune_paths(model, tau, margin, tau_fb)
-    plain, _, _ = pipe.plain()  # warm-up
+    plain, _ = pipe.plain()  # warm-up
     t_plain = []
     for _ in range(repeats):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        plain, _, _ = pipe.plain()
+        plain, _ = pipe.plain()
         torch.cuda.synchronize()
         t_plain.append(time.perf_counter() - t0)
     pipe.learned(model, tau, margin, 0.0, tau_fb)  # warm-up
@@ -483,14 +592,24 @@ def evaluate(eng: L.Engine, model: PrefilterModel, cand: dict, tau: float, margi
         st["wall"] = time.perf_counter() - t0
         runs.append((passed, st))
     passed, st = min(runs, key=lambda r: r[1]["wall"])
-    pos = plain > 0
+    m = path_metrics(pipe, plain, passed)
     jobs = cand["jobs"]
     cells_plain = int(((jobs["nl"].astype(np.int64) - 2) * jobs["al"]).sum())
-    return {"n": pipe.n, "plain_pass": int(pos.sum()), "recall": float(passed[pos].mean()) if pos.any() else 1.0,
-            "extra_pass": int((passed & ~pos).sum()), "plain_s": min(t_plain), "learned_s": st["wall"],
-            "plain_loci_per_s": pipe.n / min(t_plain), "learned_loci_per_s": pipe.n / st["wall"],
+    n_loci = m["loci"]
+    return {"n": pipe.n, **m, "plain_s": min(t_plain), "learned_s": st["wall"],
+            "plain_loci_per_s": n_loci / min(t_plain), "learned_loci_per_s": n_loci / st["wall"],
             "speedup": min(t_plain) / st["wall"], "cells_plain": cells_plain, "tune_plain": pipe.tune_plain,
             "tune_learned": pipe.tune_learned, **st}
+
+
+def path_metrics(pipe: Pipeline, plain_out: np.ndarray, learned_out: np.ndarray) -> dict:
+    """Locus-level and candidate-level agreement of the learned path with the plain path."""
+    lp, ll = pipe.loci(plain_out), pipe.loci(learned_out)
+    return {"loci": int(len(lp)), "plain_loci": int(lp.sum()), "learned_loci": int(ll.sum()),
+            "locus_recall": float((lp & ll).sum() / lp.sum()) if lp.any() else 1.0,
+            "extra_loci": int((ll & ~lp).sum()), "plain_out": int(plain_out.sum()),
+            "out_recall": float(learned_out[plain_out].mean()) if plain_out.any() else 1.0,
+            "extra_out": int((learned_out & ~plain_out).sum())}
 
 
 def main(argv=None):
@@ -499,8 +618,8 @@ def main(argv=None):
     import sys
     ap = argparse.ArgumentParser(description="train / evaluate the learned candidate prefilter")
     ap.add_argument("cmd", choices=["train", "calibrate", "eval"])
-    ap.add_argument("--train-seeds", default="1-63")
-    ap.add_argument("--val-seed", type=int, default=64)
+    ap.add_argument("--train-seeds", default="1-64")
+    ap.add_argument("--val-seed", type=int, default=66, help="calibration seed (held out from training and evaluation)")
     ap.add_argument("--eval-seed", type=int, default=65)
     ap.add_argument("--n-prot", type=int, default=4096)
     ap.add_argument("--epochs", type=int, default=8)
@@ -534,8 +653,8 @@ def main(argv=None):
     if a.cmd in ("train", "calibrate"):
         cand = make_candidates(a.val_seed, a.n_prot)
         pipe = Pipeline(eng, cand)
-        plain, _, _ = pipe.dp(cand["jobs"])
-        tau, margin, tau_fb, info = calibrate(model, pipe, plain > 0, a.recall)
+        plain, _ = pipe.plain()
+        tau, margin, tau_fb, info = calibrate(model, pipe, plain, a.recall)
         log(f"calibrated on seed {a.val_seed}: tau {tau:.4g}, margin {margin}, tau_fb {tau_fb:.4g}, {info}")
         meta.update(tau=tau, margin=margin, tau_fb=tau_fb, val_seed=a.val_seed, val_recall=a.recall)
         save(out, model, **meta)

@@ -70,3 +70,15 @@ def test_no_device_is_an_error_not_a_fallback():
     assert lib.ns_gpu_init(0) == 0
     assert lib.ns_gpu_error().decode() != "none"
     assert lib.ns_gpu_submit(None, b"ATG", 3, b"M", 1, None, None) is None
+
+
+def test_fault_hook_and_span_checks_without_a_device():
+    """The fault-injection hook validates its site; with no device the extension batch object is
+    refused (NULL) rather than run on the CPU."""
+    lib = L.load()
+    assert lib.pl_debug_fault(3, 0) == 0 and lib.pl_debug_fault(-1, 0) == 0
+    for site in (0, 1, 2):
+        assert lib.pl_debug_fault(site, -1) == 1
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        assert not lib.ns_ext_batch_init(None)

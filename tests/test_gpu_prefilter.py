@@ -210,12 +210,35 @@ def test_learned_path_small():
         assert losses[-10:].mean() < 0.7 * losses[:10].mean(), (losses[:10], losses[-10:])
         cand = P.make_candidates(13, n_prot=64)
         pipe = P.Pipeline(eng, cand)
-        plain, _, _ = pipe.dp(cand["jobs"])
+        plain, _ = pipe.plain()
         passed, stats = pipe.learned(model, tau=1e-4, margin=400, rel=0.2)
         assert stats["kept"] <= pipe.n
-        assert passed[plain > 0].mean() >= 0.97
-        own = (cand["kind"] == P.KIND_OWN_PLUS) & (plain > 0)
-        assert passed[own].mean() >= 0.98
+        m = P.path_metrics(pipe, plain, passed)
+        assert m["plain_loci"] >= 40 and m["locus_recall"] >= 0.97, m
+    finally:
+        model.close()
+        eng.close()
+
+
+def test_shipped_model_locus_recall():
+    """The shipped model and thresholds on 1024 proteins of the held-out seed 65 (8192
+    candidates): the learned path reports at least 99.5 % of the loci the plain path
+    reports, with every alignment from the exact DP."""
+    import os
+    from protlocus_b200 import prefilter as P
+    path = os.path.join(os.path.dirname(P.__file__), "data", "prefilter.npz")
+    eng = L.Engine(0)
+    model, meta = P.load_model(path, 0)
+    try:
+        assert "1-64" in str(meta["train_seeds"]) and int(meta["val_seed"]) not in range(1, 66)
+        cand = P.make_candidates(65, n_prot=1024)
+        pipe = P.Pipeline(eng, cand)
+        plain, _ = pipe.plain()
+        passed, stats = pipe.learned(model, float(meta["tau"]), int(meta["margin"]), 0.0, float(meta["tau_fb"]))
+        m = P.path_metrics(pipe, plain, passed)
+        print(m, stats)
+        assert m["plain_loci"] >= 500 and m["locus_recall"] >= 0.995, m
+        assert stats["cells_tight"] < 0.2 * int(((cand["jobs"]["nl"].astype(np.int64) - 2) * cand["jobs"]["al"]).sum())
     finally:
         model.close()
         eng.close()

@@ -10,13 +10,17 @@ from protlocus_b200.abi import SpliceResult, make_tables
 
 
 def _res(counts):
-    out, off = [], 0
-    for c in counts:
-        r = SpliceResult()
-        r.n_cigar, r.cigar_off = c, off
-        off += c
-        out.append(r)
+    out = np.zeros(len(counts), P.RES_DTYPE)
+    out["n_cigar"] = counts
+    out["cigar_off"] = np.concatenate([[0], np.cumsum(counts)[:-1]])
     return out
+
+
+def test_result_record_matches_the_c_struct():
+    import ctypes as C
+    assert P.RES_DTYPE.itemsize == C.sizeof(SpliceResult)
+    for name, _ in SpliceResult._fields_:
+        assert P.RES_DTYPE.fields[name][1] == getattr(SpliceResult, name).offset
 
 
 OPS = {"M": 0, "I": 1, "D": 2, "N": 3, "F": 10, "G": 11, "U": 12, "V": 13}  # nasw.h:33-41
@@ -94,3 +98,42 @@ def test_feature_restatement_hand_case():
     assert na == 12 and length == 6
     assert chain == [2 + 14, 2 + 29, 4, 9]
     assert F[512 + 17] == 1.0 and F[512 + 18] == 1.0
+
+
+def test_query_span_counts_residues_like_extra_cal():
+    # 2I 5M 300N 3G... residues: I 2, M 5, N 0, G 1, U 1 (split codon), M 4
+    cig = np.array([w(2, "I"), w(5, "M"), w(300, "N"), w(4, "G"), w(80, "U"), w(4, "M"), w(6, "D"),
+                    w(3, "I"), w(1, "M")], np.uint32)
+    qs, qe = P.query_span(cig, _res([7, 2]))
+    assert qs[0] == 2 and qe[0] == 2 + 5 + 1 + 1 + 4
+    assert qs[1] == 3 and qe[1] == 4          # 3I 1M
+    qs, qe = P.query_span(np.array([w(4, "I")], np.uint32), _res([1]))
+    assert qs[0] == 0 and qe[0] == 0          # no codon match: empty span
+
+
+def test_output_set_follows_the_reference_rule():
+    # protein 0: best 1000; 995 >= 0.99*1000 passes, 986 does not; protein 1: all scores <= 0
+    score = np.array([1000, 995, 986, 0, -5, -1], np.int32)
+    prot = np.array([0, 0, 0, 0, 1, 1])
+    qlen = np.array([100] * 6)
+    qs = np.zeros(6, np.int64)
+    qe = np.array([100, 100, 100, 100, 100, 100])
+    out = P.output_set(score, qs, qe, prot, qlen)
+    assert out.tolist() == [True, True, False, False, False, False]
+    # a short aligned span fails out_cov (< 0.1 x 100 residues)
+    qe2 = qe.copy()
+    qe2[1] = 9
+    assert P.output_set(score, qs, qe2, prot, qlen).tolist()[:2] == [True, False]
+    # a candidate without a result neither passes nor sets the best score (986 >= 0.99*995)
+    aligned = np.array([False, True, True, True, True, True])
+    out = P.output_set(score, qs, qe, prot, qlen, aligned)
+    assert out.tolist()[:3] == [False, True, True]
+    # out_n limits the ranks examined
+    assert P.output_set(score, qs, qe, prot, qlen, out_n=1).tolist()[:2] == [True, False]
+
+
+def test_loci_reported_needs_a_candidate_on_the_gene():
+    kind = np.array([P.KIND_OWN_PLUS, P.KIND_OWN_MINUS, P.KIND_PARTIAL, P.KIND_OTHER] * 2, np.int8)
+    prot = np.repeat([0, 1], 4)
+    out = np.array([False, False, True, False, False, False, False, True])
+    assert P.loci_reported(out, prot, kind, 2).tolist() == [True, False]

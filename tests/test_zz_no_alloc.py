@@ -10,6 +10,12 @@ one left behind -- and requires identical scores and CIGARs (the DP is integer
 arithmetic, so the tolerance is zero).  It also checks that a batch too large for
 the fixed array is refused with a message instead of running.
 
+Three option sets cover the three DP launches inside the entry point: the
+default scoring (16-bit jobs), a matrix with W:W = 127 (the 32-bit route of
+ns_global_gs_auto for the longer proteins, 16-bit for the shorter ones, so one
+call launches both), and W:W = 110 with a negative end bonus (16-bit with the
+upper clamp live).
+
 This file is collected last so that a run stopping at the first failure has
 already run every other test; it also passes on its own in a fresh process.
 """
@@ -20,7 +26,7 @@ import pytest
 
 from protlocus_b200 import lib as L
 from protlocus_b200 import workload as W
-from protlocus_b200.abi import NS_F_CIGAR, Options, SpliceJob, SpliceResult
+from protlocus_b200.abi import AA_I2C, BLOSUM62, NS_F_CIGAR, Options, SpliceJob, SpliceResult
 
 pytestmark = pytest.mark.gpu
 
@@ -33,6 +39,32 @@ def _batch():
         nt, aa = W.single_locus(seed=700 + q, al=al, window=int(rng.integers(3 * al + 200, 3 * al + 2500)))
         pairs += [(nt, aa), (W.revcomp(nt), aa)]
     return pairs
+
+
+def _case(kind):
+    """(options, pairs, widths the jobs must run at) of one option set."""
+    if kind == "default":
+        return Options(flag=NS_F_CIGAR), _batch(), {16}
+    rng = np.random.default_rng(32 if kind == "wide" else 33)
+    m = BLOSUM62.copy()
+    w = AA_I2C.index("W")
+    pairs = []
+    if kind == "wide":  # 32-bit for al*127 + end_bonus > 30000 (al >= 237), 16-bit below
+        m[w, w] = 127
+        opt = Options.nasw_defaults(flag=NS_F_CIGAR, matrix=m)
+        for q in range(24):
+            al = int(rng.integers(240, 420)) if q % 2 == 0 else int(rng.integers(20, 200))
+            nt, aa = W.single_locus(seed=int(rng.integers(1 << 30)), al=al, window=3 * al + int(rng.integers(50, 1500)))
+            pairs.append((nt, aa))
+        return opt, pairs, {16, 32}
+    m[w, w] = 110  # upper clamp: al*110 within 256 of 32767, end bonus -6000 keeps the 16-bit route
+    opt = Options(flag=NS_F_CIGAR, matrix=m, end_bonus=-6000)
+    for _ in range(12):
+        al = int(rng.integers(296, 320))
+        aa = rng.choice(list(b"WWWWWACDEFG"), size=al).astype(np.uint8).tobytes()
+        nt = W.random_dna(rng, int(rng.integers(3 * al, 3 * al + 400))).encode()
+        pairs.append((nt, aa))
+    return opt, pairs, {16}
 
 
 def _upload(torch, pairs):
@@ -58,12 +90,12 @@ def _read(torch, n, d_res, d_cig):
     return out
 
 
-def test_noalloc_matches_allocating_entry_point():
+@pytest.mark.parametrize("kind", ["default", "wide", "upper_clamp"])
+def test_noalloc_matches_allocating_entry_point(kind):
     torch = pytest.importorskip("torch")
     lib = L.load()
-    pairs = _batch()
+    opt, pairs, widths = _case(kind)
     n = len(pairs)
-    opt = Options(flag=NS_F_CIGAR)
     jobs, d_nt, d_aa = _upload(torch, pairs)
     cap = sum(len(a) + len(b) + 8 for a, b in pairs)
     stream = torch.cuda.current_stream().cuda_stream
@@ -76,6 +108,7 @@ def test_noalloc_matches_allocating_entry_point():
                                           d_res.data_ptr(), d_cig.data_ptr(), cap, C.byref(total), stream), L.error()
     want = _read(torch, n, d_res, d_cig)
     eng.close()
+    assert {w for _, w, _ in want} == widths
 
     for call in range(2):  # the second call starts from the array the first one left behind
         d_res2 = torch.full((n * C.sizeof(SpliceResult),), 0xA5, dtype=torch.uint8, device="cuda")
