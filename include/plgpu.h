@@ -222,6 +222,35 @@ int pl_debug_fault(int32_t site, int32_t after);
 /* Number of trace waves, cooperative jobs and DP launches of the last batch. */
 void pl_engine_last_plan(const pl_engine_t *e, int32_t *n_waves, int32_t *n_coop, int32_t *n_dp_launches);
 
+/* ---------------------------------------------------------------------------
+ * Several GPUs for one batch (no counterpart in the reference, whose queue
+ * drives one device, nasw-cuda.cu:516-576).  Jobs are independent, so a batch
+ * shards with no exchange inside a DP: pl_group_plan assigns each job to a
+ * device slot (by decreasing DP cells, each to the slot with the fewest cells
+ * so far), one host thread per device runs its share on that device's engine,
+ * and pl_group_gather writes results and CIGARs back in the caller's job order,
+ * CIGARs dense from cigar[0] as pl_splice_batch_host writes them (a job whose
+ * words pass cigar_cap gets status -2).  The planner and the gather are plain
+ * host functions.
+ * ------------------------------------------------------------------------- */
+typedef struct pl_group_s pl_group_t;
+pl_group_t *pl_group_create(const int32_t *devices, int32_t n_devices, int64_t trace_budget_bytes);
+void pl_group_destroy(pl_group_t *g);
+/* The engine of device slot `slot` (for tuning or timing), NULL outside the group. */
+pl_engine_t *pl_group_engine(pl_group_t *g, int32_t slot);
+/* pl_splice_batch_host over the group; *total_cigar (optional) = words written. */
+int pl_group_splice_host(pl_group_t *g, const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n_jobs,
+		const uint8_t *nt, int64_t nt_len, const uint8_t *aa, int64_t aa_len, const uint8_t *ss, int64_t ss_len,
+		pl_splice_result_t *results, uint32_t *cigar, int64_t cigar_cap, int64_t *total_cigar);
+/* dev_of_job[q] = device slot of job q; cells_of_dev (optional, n_devices) = DP cells per slot. */
+int pl_group_plan(const pl_splice_job_t *jobs, int32_t n_jobs, int32_t n_devices, int32_t *dev_of_job,
+		int64_t *cells_of_dev);
+/* Reassembly: dev_results[d] holds slot d's results in the order of its jobs
+ * (cigar_off into dev_cigar[d]); writes results/cigar in job order. */
+int pl_group_gather(int32_t n_jobs, const int32_t *dev_of_job, int32_t n_devices,
+		const pl_splice_result_t *const *dev_results, const uint32_t *const *dev_cigar,
+		pl_splice_result_t *results, uint32_t *cigar, int64_t cigar_cap, int64_t *total_cigar);
+
 /* Allocation-free variant of pl_splice_batch_device() -- no counterpart in the
  * reference.  For callers that cannot allocate device memory on this path: a
  * program that gives all free device memory to its own pool and runs under that

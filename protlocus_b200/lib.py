@@ -127,6 +127,20 @@ def load() -> C.CDLL:
     lib.pl_rc_last_cells.restype = C.c_int64
     lib.pl_rc_mathf_eval.argtypes = [C.c_int32, C.c_int32, C.c_uint32, C.c_uint32, C.c_int64, C.c_void_p]
     lib.pl_rc_mathf_eval.restype = C.c_int
+    lib.pl_group_create.argtypes = [C.c_void_p, C.c_int32, C.c_int64]
+    lib.pl_group_create.restype = C.c_void_p
+    lib.pl_group_destroy.argtypes = [C.c_void_p]
+    lib.pl_group_engine.argtypes = [C.c_void_p, C.c_int32]
+    lib.pl_group_engine.restype = C.c_void_p
+    lib.pl_group_splice_host.argtypes = [C.c_void_p, C.POINTER(NsOpt), C.POINTER(SpliceJob), C.c_int32,
+                                         C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                         C.POINTER(SpliceResult), C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
+    lib.pl_group_splice_host.restype = C.c_int
+    lib.pl_group_plan.argtypes = [C.POINTER(SpliceJob), C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]
+    lib.pl_group_plan.restype = C.c_int
+    lib.pl_group_gather.argtypes = [C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                    C.POINTER(SpliceResult), C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
+    lib.pl_group_gather.restype = C.c_int
     lib.pl_debug_fault.argtypes = [C.c_int32, C.c_int32]
     lib.pl_debug_fault.restype = C.c_int
     lib.pl_ext_failed_count.restype = C.c_uint64
@@ -628,6 +642,46 @@ class ExtBatch:
             self.close()
         except Exception:
             pass
+
+
+def group_plan(jobs, n_devices: int):
+    """pl_group_plan over a SpliceJob array: (device slot of each job, DP cells per slot)."""
+    n = len(jobs)
+    dev = np.zeros(max(n, 1), np.int32)
+    cells = np.zeros(n_devices, np.int64)
+    if not load().pl_group_plan(jobs, n, n_devices, dev.ctypes.data, cells.ctypes.data):
+        raise RuntimeError("pl_group_plan: " + error())
+    return dev[:n], cells
+
+
+def group_gather(dev_of_job, per_device, cigar_cap: int | None = None):
+    """pl_group_gather: per_device[d] = (list of (score, cigar words) in the order of slot d's
+    jobs).  Returns (SpliceResult array in job order, dense CIGAR words, total words)."""
+    n = len(dev_of_job)
+    n_dev = len(per_device)
+    keep = []
+    res_ptrs = (C.c_void_p * n_dev)()
+    cig_ptrs = (C.c_void_p * n_dev)()
+    for d, items in enumerate(per_device):
+        r = (SpliceResult * max(len(items), 1))()
+        words, off = [], 0
+        for k, (score, cig) in enumerate(items):
+            r[k].score, r[k].n_cigar, r[k].cigar_off, r[k].mode, r[k].status = score, len(cig), off, 16, 0
+            words += list(cig)
+            off += len(cig)
+        w = np.array(words + [0], np.uint32)
+        keep += [r, w]
+        res_ptrs[d] = C.cast(r, C.c_void_p)
+        cig_ptrs[d] = w.ctypes.data
+    cap = cigar_cap if cigar_cap is not None else sum(len(c) for items in per_device for _, c in items)
+    out = (SpliceResult * max(n, 1))()
+    cig = np.zeros(max(cap, 1), np.uint32)
+    total = C.c_int64()
+    dv = np.ascontiguousarray(dev_of_job, np.int32)
+    if not load().pl_group_gather(n, dv.ctypes.data, n_dev, res_ptrs, cig_ptrs, out, cig.ctypes.data, cap,
+                                  C.byref(total)):
+        raise RuntimeError("pl_group_gather: " + error())
+    return out, cig, total.value
 
 
 def measure_int_peak(device: int = 0):

@@ -6,7 +6,10 @@ per-rank seeding that gives each rank its own batch.  Two processes with the
 gloo backend check each of these, then check that each rank's own batch is
 processed correctly: every rank runs the oracle restatement of the spliced DP
 on its shard and the whole-job checksum, gathered over ranks, equals the
-single-process result over the union of the shards.
+single-process result over the union of the shards.  A second test splits ONE
+batch with the group planner (pl_group_plan), each rank aligns its share, rank 0
+gathers the shares (the only exchange, on the host) and reassembles them with
+pl_group_gather: the result equals a single process's over the whole batch.
 """
 import os
 import socket
@@ -96,3 +99,69 @@ def test_single_process_needs_no_process_group(monkeypatch):
     R.barrier()
     R.close()
     assert job_rate(10, 0) == 0.0
+
+
+def _batch_pairs():
+    from protlocus_b200 import workload as W
+    rng = np.random.default_rng(77)
+    return [W.random_pair(rng, max_al=40) for _ in range(14)]
+
+
+def _align(pairs):
+    import oracle_lib as O
+    from protlocus_b200.abi import NS_F_CIGAR, Options
+    opt = Options(flag=NS_F_CIGAR)
+    out = []
+    for nt, aa in pairs:
+        score, _ntl, _aal, cig = O.run("gs_auto", nt, aa, opt)
+        out.append((score, [int(x) for x in cig]))
+    return out
+
+
+def _job_table(pairs):
+    from protlocus_b200.abi import SpliceJob
+    jobs = (SpliceJob * len(pairs))()
+    pn = pa = 0
+    for q, (nt, aa) in enumerate(pairs):
+        jobs[q].nt_off, jobs[q].aa_off, jobs[q].ss_off, jobs[q].nl, jobs[q].al = pn, pa, -1, len(nt), len(aa)
+        pn += len(nt)
+        pa += len(aa)
+    return jobs
+
+
+def _shard_worker(rank, world, port, out):
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, here)
+    sys.path.insert(0, os.path.dirname(here))
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    from protlocus_b200 import lib as L
+    from protlocus_b200.ranks import Ranks
+    R = Ranks("gloo", timeout_s=60)
+    try:
+        pairs = _batch_pairs()                       # every rank holds the same job table
+        dev, _cells = L.group_plan(_job_table(pairs), world)
+        mine = _align([pairs[q] for q in range(len(pairs)) if dev[q] == rank])
+        shares = [None] * world
+        dist.all_gather_object(shares, mine)         # the host-side gather of results
+        if rank == 0:
+            res, cig, total = L.group_gather(dev, shares)
+            out[0] = ([(res[q].score, cig[res[q].cigar_off:res[q].cigar_off + res[q].n_cigar].tolist())
+                       for q in range(len(pairs))], dev.tolist())
+        R.barrier()
+    finally:
+        R.close()
+
+
+@pytest.mark.timeout(300)
+def test_two_gloo_ranks_shard_one_batch():
+    world = 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        mp.start_processes(_shard_worker, args=(world, port, out), nprocs=world, join=True, start_method="spawn")
+        got, dev = out[0]
+    assert set(dev) == {0, 1}                        # both ranks took a share
+    assert got == _align(_batch_pairs())             # job order and CIGARs as one process
