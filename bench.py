@@ -67,10 +67,14 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-prefilter", action="store_true",
                     help="leave the learned-prefilter loci/s sub-object out of the headline line")
+    ap.add_argument("--no-refgpu", action="store_true",
+                    help="leave the reference's own CUDA global DP (timed in a child process) out of the headline")
+    ap.add_argument("--ref-jobs", type=int, default=256, help="jobs of the reference GPU queue sample (--workload refgpu)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the engine's default tuning instead of autotuning it on the workload (global DP)")
     ap.add_argument("--workload", default="global",
-                    choices=["global", "ext", "hmm", "gapless", "forward", "prefilter", "extra", "prescreen", "chain"],
+                    choices=["global", "ext", "hmm", "gapless", "forward", "prefilter", "extra", "prescreen", "chain",
+                             "refgpu"],
                     help="global: the batched global spliced DP (headline); ext: the batched extension DP; "
                          "hmm: the integer profile-HMM DP; gapless: the gapless X-drop prefilter; "
                          "forward: the recheck Forward score; prefilter: learned candidate prefilter vs the plain "
@@ -81,6 +85,11 @@ def parse():
     ap.add_argument("--candidates", type=int, default=131072, help="candidates of 8 anchors (--workload gapless)")
     ap.add_argument("--profiles", type=int, default=16, help="profiles per step (--workload hmm)")
     ap.add_argument("--regions", type=int, default=4096, help="regions per profile (--workload hmm)")
+    ap.add_argument("--hmm-shape", default="regions", choices=["regions", "genome"],
+                    help="--workload hmm: 'regions' = synthetic regions per profile; 'genome' = the profile-HMM "
+                         "configuration (use --profiles 1000): every profile against a six-frame genome slice")
+    ap.add_argument("--genome-slice-mb", type=float, default=2.0, help="Mb of the 100 Mb genome scanned per step")
+    ap.add_argument("--genome-region-kb", type=int, default=12, help="region window of the genome scan (kb)")
     ap.add_argument("--requests", type=int, default=65536, help="extension requests per step (--workload ext)")
     ap.add_argument("--uniform", default=None, metavar="N:NL:AL",
                     help="profiling case instead of the batched workload: N planted loci of window NL and protein AL")
@@ -95,15 +104,23 @@ def make_jobs(args, seed):
 
 
 def pack(jobs):
+    """Packed inputs and job table; a protein searched on both strands is stored once and both
+    jobs point at it (the jobs of one protein and window length then run as int16x2 pairs)."""
     n = len(jobs)
     nl = np.array([len(a) for a, _ in jobs], dtype=np.int32)
     al = np.array([len(b) for _, b in jobs], dtype=np.int32)
     nt_off = np.zeros(n, dtype=np.int64)
     aa_off = np.zeros(n, dtype=np.int64)
     nt_off[1:] = np.cumsum(nl[:-1])
-    aa_off[1:] = np.cumsum(al[:-1])
+    prot_off, parts, pos = {}, [], 0
+    for q, (_, b) in enumerate(jobs):
+        if b not in prot_off:
+            prot_off[b] = pos
+            parts.append(b)
+            pos += len(b)
+        aa_off[q] = prot_off[b]
     nt = np.frombuffer(b"".join(a for a, _ in jobs), dtype=np.uint8)
-    aa = np.frombuffer(b"".join(b for _, b in jobs), dtype=np.uint8)
+    aa = np.frombuffer(b"".join(parts), dtype=np.uint8)
     tab = (SpliceJob * n)()
     for q in range(n):
         tab[q].nt_off, tab[q].aa_off, tab[q].ss_off, tab[q].nl, tab[q].al = nt_off[q], aa_off[q], -1, nl[q], al[q]
@@ -217,8 +234,105 @@ def run_reference(args):
     return 0
 
 
+REF_CUDA_SO = os.path.join(ROOT, "oracle", "_ref", "libnscuda_ref.so")
+
+
+def main_refgpu(args):
+    """The reference's own CUDA global DP (nasw-cuda.cu compiled for sm_100a from its sources,
+    oracle/_ref/libnscuda_ref.so) on this GPU: its request queue over a bounded seeded sample of
+    the headline jobs (ns_gpu_submit from 16 host threads, then ns_gpu_wait, which includes its
+    host backtrack from the full trace copied back), and the latency of ns_gpu_global on the
+    single-locus job (500 aa, 20 kb).  Runs in its own process (its own CUDA context); prints
+    one JSON object."""
+    if not os.path.exists(REF_CUDA_SO):
+        print(json.dumps({"unavailable": "oracle/_ref/libnscuda_ref.so not built"}), flush=True)
+        return 0
+    lib = C.CDLL(REF_CUDA_SO)
+    lib.ref_gpu_queue_bench.restype = C.c_double
+    lib.ref_gpu_queue_bench.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_int32] + [C.c_void_p] * 8
+    lib.ref_gpu_global_latency.restype = C.c_int32
+    lib.ref_gpu_global_latency.argtypes = [C.c_int32, C.c_void_p, C.c_char_p, C.c_int32, C.c_char_p, C.c_int32,
+                                           C.c_int32, C.c_void_p]
+    opt = Options(flag=NS_F_CIGAR)
+    jobs = make_jobs(args, 1)
+    rng = np.random.default_rng(777)
+    take = np.sort(rng.permutation(len(jobs))[: args.ref_jobs])
+    sub = [jobs[q] for q in take]
+    nt, aa, nt_off, aa_off, nl, al, _ = pack(sub)
+    n = len(sub)
+    score = np.zeros(n, np.int32)
+    taken = np.zeros(n, np.int32)
+    # warm-up: the queue's threads, the module load and the device buffers
+    w = min(n, 8)
+    lib.ref_gpu_queue_bench(0, 16, C.addressof(opt.c), w, nt.ctypes.data, nt_off.ctypes.data, nl.ctypes.data,
+                            aa.ctypes.data, aa_off.ctypes.data, al.ctypes.data, score.ctypes.data, taken.ctypes.data)
+    secs = lib.ref_gpu_queue_bench(0, 16, C.addressof(opt.c), n, nt.ctypes.data, nt_off.ctypes.data,
+                                   nl.ctypes.data, aa.ctypes.data, aa_off.ctypes.data, al.ctypes.data,
+                                   score.ctypes.data, taken.ctypes.data)
+    if secs <= 0:
+        print(json.dumps({"unavailable": "the reference's ns_gpu_init failed"}), flush=True)
+        return 0
+    cells = (nl.astype(np.int64) - 2) * al
+    ok = taken > 0
+    c_nt, c_aa = W.single_locus(seed=0)
+    lat = np.zeros(20, np.float64)
+    lib.ref_gpu_global_latency(0, C.addressof(opt.c), c_nt, len(c_nt), c_aa, len(c_aa), 20, lat.ctypes.data)
+    print(json.dumps({"gcups": round(float(cells[ok].sum()) / secs / 1e9, 3), "jobs": int(n), "taken": int(ok.sum()),
+                      "cells": int(cells[ok].sum()), "seconds": round(secs, 3),
+                      "config0_ms_median": round(float(np.median(lat[2:])) * 1e3, 3),
+                      "sample": f"{n} of {len(jobs)} DP jobs of the headline batch (seeded random subset), "
+                                "ns_gpu_submit from 16 threads then ns_gpu_wait (kernel, D2H of the full trace, "
+                                "host backtrack)"}), flush=True)
+    return 0
+
+
+def config0_latency(local):
+    """Latency of one DP on the single-locus job (500 aa protein, 20 kb window, CIGAR): this
+    library's bulk entry point with one job and its request queue (ns_gpu_global), and the
+    reference's SSE kernel on one host core.  Medians of 20 calls after 3 warm-up calls."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    opt = Options(flag=NS_F_CIGAR)
+    c_nt, c_aa = W.single_locus(seed=0)
+    out = {"job": f"single locus: protein {len(c_aa)} aa, window {len(c_nt)} nt, "
+                  f"{(len(c_nt) - 2) * len(c_aa) / 1e6:.1f} M cells, with CIGAR"}
+    eng = L.Engine(local)
+    t = []
+    for k in range(23):
+        t0 = time.perf_counter()
+        eng.align_host(opt, [(c_nt, c_aa)])
+        t.append(time.perf_counter() - t0)
+    eng.close()
+    out["ours_ms"] = round(statistics.median(t[3:]) * 1e3, 3)
+    if L.gpu_init(local):
+        t = []
+        for k in range(23):
+            t0 = time.perf_counter()
+            L.gpu_global(c_nt, c_aa, opt)
+            t.append(time.perf_counter() - t0)
+        out["ours_queue_ms"] = round(statistics.median(t[3:]) * 1e3, 3)
+    ref = O.ref_lib()
+    if ref is not None:
+        fn = ref.ref_bench_global
+        fn.restype = C.c_double
+        fn.argtypes = [C.c_int32, C.c_int32] + [C.c_void_p] * 9
+        ntb = np.frombuffer(c_nt, np.uint8)
+        aab = np.frombuffer(c_aa, np.uint8)
+        z64 = np.zeros(1, np.int64)
+        nl1 = np.array([len(c_nt)], np.int32)
+        al1 = np.array([len(c_aa)], np.int32)
+        sc = np.zeros(1, np.int32)
+        nc = np.zeros(1, np.int32)
+        t = [fn(1, 1, ntb.ctypes.data, z64.ctypes.data, nl1.ctypes.data, aab.ctypes.data, z64.ctypes.data,
+                al1.ctypes.data, C.addressof(opt.c), sc.ctypes.data, nc.ctypes.data) for _ in range(23)]
+        out["reference_sse_1core_ms"] = round(statistics.median(t[3:]) * 1e3, 3)
+    return out
+
+
 def main():
     args = parse()
+    if args.workload == "refgpu":
+        return main_refgpu(args)
     if args.workload == "ext":
         return run_reference_ext(args) if args.impl == "reference" else main_ext(args)
     if args.workload == "hmm":
@@ -347,6 +461,19 @@ def main():
     eng.close()
     del d_nt, d_aa, d_res, d_cig
     torch.cuda.empty_cache()
+    lat = config0_latency(local) if rank == 0 else None
+    refgpu = None
+    if rank == 0 and not args.no_refgpu:  # the reference's CUDA kernel as the GPU bar, in its own process
+        try:
+            pr = subprocess.run([sys.executable, os.path.abspath(__file__), "--workload", "refgpu", "--ref-jobs",
+                                 str(args.ref_jobs), "--pairs", str(args.pairs)], capture_output=True, text=True,
+                                timeout=600)
+            refgpu = json.loads(pr.stdout.strip().splitlines()[-1]) if pr.returncode == 0 and pr.stdout.strip() \
+                else {"unavailable": f"child exited {pr.returncode}: {pr.stderr.strip()[-200:]}"}
+        except Exception as ex:  # a timeout or a parse error: report it, keep the line
+            refgpu = {"unavailable": f"{type(ex).__name__}: {str(ex)[:200]}"}
+        if lat is not None and "config0_ms_median" in refgpu:
+            lat["reference_gpu_queue_ms"] = refgpu.pop("config0_ms_median")
     if not args.no_prefilter:
         pf = prefilter_measure(args, R, local, min(args.steps, 5), 3, 0.0)
         if pf is not None:
@@ -384,6 +511,8 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clk,
             "prefilter": pf,
+            "reference_gpu": refgpu,
+            "config0_latency": lat,
         }
         print(json.dumps(line), flush=True)
     R.close()
@@ -586,6 +715,8 @@ def main_ext(args):
             "cpu_baseline": cpu,
             "clocks": clk,
             "prefilter": pf,
+            "reference_gpu": refgpu,
+            "config0_latency": lat,
         }
         print(json.dumps(line), flush=True)
     R.close()
@@ -600,6 +731,19 @@ HMM_OPS_PER_CELL = 17  # int32 ops per cell of mp_hmm_dp_score's inner loop (hmm
 
 def hmm_workload(args, seed):
     from protlocus_b200 import hmm as H
+    if args.hmm_shape == "genome":  # the profile-HMM configuration: profiles x six frames of a genome slice
+        texts, probs = H.synthetic_profiles(args.profiles, seed=seed, m_min=50, m_max=800)
+        profs = H.parse_hmmer3("".join(texts))
+        nt, offs, lens, inside = H.genome_scan(probs, seed + 1000, slice_mb=args.genome_slice_mb,
+                                               region_nt=args.genome_region_kb * 1000)
+        batch = (nt, offs, lens)  # one region set, scored against every profile
+        desc = (f"profile-HMM genome scan: {args.profiles} synthetic Plan7 profiles (m uniform 50-800, "
+                "Dirichlet-perturbed background, M->M ~0.95, HMMER3 text through the parser) against the six-frame "
+                f"translation of a 100 Mb 45%-GC genome with 1000 planted profile-sampled domains; each step scans "
+                f"the first {args.genome_slice_mb:g} Mb ({args.genome_slice_mb:g}% of the genome, {inside} planted "
+                f"domains) as {len(lens)} regions of {args.genome_region_kb} kb overlapping by 2.4 kb (a domain of "
+                "up to 800 codons lies inside one), both strands, frames 0-2; cells = the regions' codons x m")
+        return texts, profs, [batch] * len(profs), desc
     texts, probs = H.synthetic_profiles(args.profiles, seed=seed, m_min=50, m_max=800)
     profs = H.parse_hmmer3("".join(texts))
     rng = np.random.default_rng(seed + 1000)
@@ -689,7 +833,8 @@ def main_hmm(args):
     hp = [L.HmmProfile(p["emit"], p["trans"], ca, local) for p in profs]
     cells = sum(int((ln // 3).astype(np.int64).sum()) * p["m"] for p, (_, _, ln) in zip(profs, batches))
     cells_all = R.sum(cells)  # whole job (every rank takes this collective)
-    d_nt = [torch.from_numpy(nt).to("cuda") for nt, _, _ in batches]
+    dev_nt = {}  # one device copy per distinct region set (the genome scan shares one across profiles)
+    d_nt = [dev_nt.setdefault(id(nt), torch.from_numpy(nt).to("cuda")) for nt, _, _ in batches]
     d_sc = [torch.zeros(len(ln), dtype=torch.int32, device="cuda") for _, _, ln in batches]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
@@ -729,7 +874,8 @@ def main_hmm(args):
 
     e2e = None
     if not args.no_e2e:
-        h_nt = [torch.from_numpy(nt).pin_memory() for nt, _, _ in batches]
+        pin_nt = {}
+        h_nt = [pin_nt.setdefault(id(nt), torch.from_numpy(nt).pin_memory()) for nt, _, _ in batches]
         h_sc = [np.zeros(len(ln), dtype=np.int32) for _, _, ln in batches]
         est = torch.cuda.ExternalStream(eng.stream)
 

@@ -221,6 +221,13 @@ int pl_debug_fault(int32_t site, int32_t after);
 
 /* Number of trace waves, cooperative jobs and DP launches of the last batch. */
 void pl_engine_last_plan(const pl_engine_t *e, int32_t *n_waves, int32_t *n_coop, int32_t *n_dp_launches);
+/* Two 16-bit jobs that share one protein (the same aa_off in the job table) and one
+ * window length -- the two strands of a locus -- run as a pair in the two halves of
+ * the int16x2 DP kernel when their score range fits its 15-bit domain (on by
+ * default; PLGPU_PAIR=0 or pl_engine_set_pairing(e, 0) turns it off).  Results are
+ * the same either way.  pl_engine_last_pairs: pairs formed in the last batch. */
+void pl_engine_set_pairing(pl_engine_t *e, int32_t enable);
+int32_t pl_engine_last_pairs(const pl_engine_t *e);
 
 /* ---------------------------------------------------------------------------
  * Several GPUs for one batch (no counterpart in the reference, whose queue

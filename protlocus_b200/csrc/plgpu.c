@@ -144,7 +144,7 @@ PL_EXPORT pl_engine_t *pl_engine_create(int32_t device, int64_t trace_budget_byt
 	e->device = device;
 	CK(cudaSetDevice(device));
 	CK(cudaDeviceGetAttribute(&e->n_sm, cudaDevAttrMultiProcessorCount, device));
-	for (m = 0; m < 3; ++m) {
+	for (m = 0; m < 4; ++m) {
 		int r;
 		for (r = 0; r < 2; ++r) {
 			e->ctas_per_sm[m][r] = plk_dp_ctas_per_sm(m, r == 0 ? 8 : 4);
@@ -153,6 +153,10 @@ PL_EXPORT pl_engine_t *pl_engine_create(int32_t device, int64_t trace_budget_byt
 	}
 	e->coop_ratio = pl_coop_ratio();
 	e->r4_rows = pl_r4_rows();
+	{
+		const char *v = getenv("PLGPU_PAIR");
+		e->pairing = !(v && *v && atoi(v) == 0);
+	}
 	CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
 	CK(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
 	CK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
@@ -307,7 +311,7 @@ static int pl_cmp_cells_desc(const void *a, const void *b)
 static int pl_max_ctas(const pl_engine_t *e)
 {
 	int m, r, c = 0;
-	for (m = 0; m < 3; ++m)
+	for (m = 0; m < 4; ++m)
 		for (r = 0; r < 2; ++r) if (e->ctas_per_sm[m][r] > c) c = e->ctas_per_sm[m][r];
 	return c;
 }
@@ -342,6 +346,78 @@ static double pl_union_ms(double *a, double *b, int n)
 	return tot;
 }
 
+/* The paired int16x2 DP (mode 3) keeps values v + B in 15 bits per half with the
+ * saturation floor at F.  Its admission bound, from the recurrences: a real H value
+ * is at least the cost of one path to it (the diagonal out of column -1 at row 2,
+ * insertions along row 2, one intron down the column: s_min - go - ge*al - io -
+ * 256), every state derived from H values is at most two penalised steps below
+ * (P1 = go + ge + io + fs + 256 each), and no value exceeds al*max(sc) + 256.  A
+ * job of protein length al is admitted when [low bound, high bound] fits between
+ * F + 512 and 0x7fff - 512 after biasing; every penalty stays below F so that the
+ * floor never wraps under a subtraction. */
+#define PL_PAIR_F 512
+static int pl_pair_limits(const ns_opt_t *opt, int max_sub, int32_t *al_cap, int32_t *bias)
+{
+	int i, s_min = 0;
+	int64_t c_low, per_al, cap;
+	if (opt->go + opt->ge > 256 || opt->io > 256 || opt->fs > 256 || opt->go < 0 || opt->ge < 0 || opt->io < 0 ||
+			opt->fs < 0 || opt->asize != 22)
+		return 0;
+	for (i = 0; i < 22 * 22; ++i) if (opt->sc[i] < s_min) s_min = opt->sc[i];
+	c_low = -s_min + opt->go + opt->io + 256 + 2 * (opt->go + opt->ge + opt->io + opt->fs + 256);
+	per_al = opt->ge + (max_sub > 0 ? max_sub : 0);
+	cap = (32767 - PL_PAIR_F - 512 - 512 - 256 - c_low) / (per_al > 0 ? per_al : 1);
+	if (cap < 1) return 0;
+	*al_cap = cap > 65535 ? 65535 : (int32_t)cap;
+	*bias = (int32_t)(PL_PAIR_F + 512 + c_low + (int64_t)opt->ge * *al_cap);
+	return 1;
+}
+
+/* launch group of a job: its mode, with the second jobs of pairs in group 4 */
+static int pl_group_of(const plk_job_t *J) { return J->mode == 3 && J->pair < 0 ? 4 : J->mode; }
+
+typedef struct { int64_t aa_off; int32_t al, nl, idx; } pl_pkey_t;
+static int pl_cmp_pair(const void *a, const void *b)
+{
+	const pl_pkey_t *x = (const pl_pkey_t*)a, *y = (const pl_pkey_t*)b;
+	if (x->aa_off != y->aa_off) return x->aa_off < y->aa_off ? -1 : 1;
+	if (x->al != y->al) return x->al - y->al;
+	if (x->nl != y->nl) return x->nl - y->nl;
+	return x->idx - y->idx;
+}
+
+/* Pairs of 16-bit jobs with one protein (the same aa_off) and one window length run as
+ * mode 3; returns the number of pairs formed (0 on a host allocation failure too). */
+static int32_t pl_form_pairs(pl_engine_t *e, const ns_opt_t *opt, int32_t n, int max_sub, plk_params_t *P)
+{
+	pl_pkey_t *key;
+	int32_t q, m = 0, n_pairs = 0, al_cap = 0, bias = 0;
+	if (!e->pairing || n < 2 || !pl_pair_limits(opt, max_sub, &al_cap, &bias)) return 0;
+	key = (pl_pkey_t*)malloc(sizeof(*key) * (size_t)n);
+	if (!key) return 0;
+	for (q = 0; q < n; ++q) {
+		const plk_job_t *J = &e->hj[q];
+		if (J->mode != 0 || J->al > al_cap) continue;
+		key[m].aa_off = J->aa_off, key[m].al = J->al, key[m].nl = J->nl, key[m].idx = q, ++m;
+	}
+	qsort(key, (size_t)m, sizeof(*key), pl_cmp_pair);
+	for (q = 0; q + 1 < m; ++q) {
+		if (key[q].aa_off != key[q + 1].aa_off || key[q].al != key[q + 1].al || key[q].nl != key[q + 1].nl) continue;
+		/* a pair shares one wave: both traces must fit the budget together */
+		if (2 * plk_trace_words(key[q].nl, key[q].al, PLK_WARPS_PER_CTA, e->hj[key[q].idx].rows) * 2 > e->trace_budget)
+			continue;
+		{
+			plk_job_t *A = &e->hj[key[q].idx], *B = &e->hj[key[q + 1].idx];
+			A->mode = B->mode = 3;
+			A->pair = key[q + 1].idx, B->pair = -1;
+			++n_pairs, ++q;
+		}
+	}
+	free(key);
+	P->pair_b = bias, P->pair_f = PL_PAIR_F;
+	return n_pairs;
+}
+
 /* Runs the whole batch on `st`.  Inputs (nt/aa/ss) and outputs (res/cig) are device pointers. */
 static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n,
 		const uint8_t *nt, const uint8_t *aa, const uint8_t *ss, pl_splice_result_t *res_dev,
@@ -354,7 +430,7 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 	int64_t *wave_bytes = 0, *wave_cells = 0, total_words = 0;
 	int ok = 0;
 
-	e->last_waves = e->last_coop = e->last_dp_launches = 0;
+	e->last_waves = e->last_coop = e->last_dp_launches = e->last_pairs = 0;
 	if (n <= 0) { if (total_out) *total_out = 0; return 1; }
 	if (!pl_params(opt, &P, 0)) return 0;
 	if (!pl_grow_host(e, n)) return 0;
@@ -389,6 +465,12 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 		pl_set_error("one job needs %lld trace bytes, over the budget of %lld", (long long)max_trace, (long long)e->trace_budget);
 		return 0;
 	}
+	e->last_pairs = pl_form_pairs(e, opt, n, max_sub, &P);
+	if (e->last_pairs > 0) /* the unit the waves are packed by is a pair: twice a job's trace */
+		for (q = 0; q < n; ++q)
+			if (e->hj[q].mode == 3 && e->hj[q].pair >= 0 &&
+					2 * plk_trace_words(e->hj[q].nl, e->hj[q].al, PLK_WARPS_PER_CTA, e->hj[q].rows) * 2 > max_trace)
+				max_trace = 2 * plk_trace_words(e->hj[q].nl, e->hj[q].al, PLK_WARPS_PER_CTA, e->hj[q].rows) * 2;
 	/* 2. waves by LPT bin packing on trace bytes.  A batch over the budget runs its
 	 * waves alternately on two streams, each with its own arena of half the budget:
 	 * a wave's DP then starts while the one before drains instead of after it. */
@@ -412,11 +494,16 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 	if (!wave_bytes || !wave_cells) { pl_set_error("out of host memory"); goto fail; }
 	for (q = 0; q < n; ++q) {
 		const int32_t j = sorted[q];
-		int32_t best = 0;
+		const plk_job_t *J = &e->hj[j];
+		int32_t best = 0, t;
+		if (J->mode == 3 && J->pair < 0) continue;  /* the second job of a pair goes with the first */
 		for (w = 1; w < n_waves; ++w) if (wave_bytes[w] < wave_bytes[best]) best = w;
-		e->hwave[j] = best;
-		wave_bytes[best] += plk_trace_words(e->hj[j].nl, e->hj[j].al, PLK_WARPS_PER_CTA, e->hj[j].rows) * 2;
-		wave_cells[best] += (int64_t)(e->hj[j].nl - 2) * e->hj[j].al;
+		for (t = 0; t < (J->mode == 3 ? 2 : 1); ++t) {
+			const int32_t jj = t == 0 ? j : J->pair;
+			e->hwave[jj] = best;
+			wave_bytes[best] += plk_trace_words(e->hj[jj].nl, e->hj[jj].al, PLK_WARPS_PER_CTA, e->hj[jj].rows) * 2;
+			wave_cells[best] += (int64_t)(e->hj[jj].nl - 2) * e->hj[jj].al;
+		}
 	}
 	/* 3. cooperative or solo, trace offsets inside each wave's arena */
 	memset(wave_bytes, 0, sizeof(int64_t) * (size_t)n_waves);
@@ -426,6 +513,7 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 		const int64_t cells = (int64_t)(J->nl - 2) * J->al, share = wave_cells[e->hwave[j]] / slots;
 		if (J->al >= 200 && J->nl - 2 >= 32 * PLK_WARPS_PER_CTA * J->rows && (double)cells > share * e->coop_ratio)
 			J->nw = PLK_WARPS_PER_CTA;
+		if (J->mode == 3 && J->pair >= 0) e->hj[J->pair].nw = J->nw;  /* a pair shares one wavefront */
 		J->trace_off = wave_bytes[e->hwave[j]] / 2;
 		wave_bytes[e->hwave[j]] += (plk_trace_words(J->nl, J->al, J->nw, J->rows) * 2 + 15) / 16 * 16;
 	}
@@ -451,7 +539,7 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 		int32_t pos = 0;
 		for (w = 0; w < n_waves; ++w) {
 			int m, r;
-			for (m = 0; m < 3; ++m)
+			for (m = 0; m < 5; ++m)
 				for (r = 0; r < 2; ++r) {
 					const int rows = r == 0 ? 8 : 4;
 					int pass;
@@ -459,7 +547,7 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 						for (q = 0; q < n; ++q) {
 							const int32_t j = sorted[q];
 							const plk_job_t *J = &e->hj[j];
-							if (e->hwave[j] == w && J->mode == m && J->rows == rows && (J->nw > 1) == (pass == 0))
+							if (e->hwave[j] == w && pl_group_of(J) == m && J->rows == rows && (J->nw > 1) == (pass == 0))
 								e->horder[pos++] = j;
 						}
 				}
@@ -482,15 +570,15 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 			cudaStream_t sw = a ? e->side : st;
 			uint16_t *trace_w = (uint16_t*)e->trace.p + a * arena_words;
 			int m, r;
-			for (m = 0; m < 3; ++m)
+			for (m = 0; m < 5; ++m)
 				for (r = 0; r < 2; ++r) {
 					const int rows = r == 0 ? 8 : 4;
 					int32_t n_coop = 0, n_solo = 0;
-#define PL_IN_GROUP(x) (e->hwave[e->horder[(x)]] == w && e->hj[e->horder[(x)]].mode == m && e->hj[e->horder[(x)]].rows == rows)
+#define PL_IN_GROUP(x) (e->hwave[e->horder[(x)]] == w && pl_group_of(&e->hj[e->horder[(x)]]) == m && e->hj[e->horder[(x)]].rows == rows)
 					while (pos + n_coop < n && PL_IN_GROUP(pos + n_coop) && e->hj[e->horder[pos + n_coop]].nw > 1) ++n_coop;
 					while (pos + n_coop + n_solo < n && PL_IN_GROUP(pos + n_coop + n_solo)) ++n_solo;
 #undef PL_IN_GROUP
-					if (n_coop + n_solo > 0) {
+					if (n_coop + n_solo > 0 && m < 4) {  /* group 4: second jobs of pairs, run with their first */
 						const int32_t *ord = (const int32_t*)e->order.p + pos;
 						const int64_t stride = ((int64_t)max_al + 1) * PLK_RING_INTS;
 						const int32_t ctas = e->n_sm * e->ctas_per_sm[m][r];
@@ -552,6 +640,10 @@ fail:
 	free(wave_bytes), free(wave_cells);
 	return ok;
 }
+
+PL_EXPORT int32_t pl_engine_last_pairs(const pl_engine_t *e) { return e ? e->last_pairs : 0; }
+
+PL_EXPORT void pl_engine_set_pairing(pl_engine_t *e, int32_t enable) { if (e) e->pairing = enable != 0; }
 
 PL_EXPORT void pl_engine_set_tuning(pl_engine_t *e, int32_t r4_rows, double coop_ratio)
 {

@@ -28,7 +28,8 @@ int dbuf_ensure(dbuf_t *b, size_t need);
 void dbuf_free(dbuf_t *b);
 
 struct pl_engine_s {
-	int device, n_sm, ctas_per_sm[3][2];   /* per DP width mode, per rows per lane (8, 4) */
+	int device, n_sm, ctas_per_sm[4][2];   /* per DP mode (3: paired int16x2), per rows per lane (8, 4) */
+	int pairing;                            /* form int16x2 pairs (PLGPU_PAIR=0 turns it off) */
 	int32_t r4_rows;                        /* jobs with at most this many DP rows take 4 rows per lane */
 	double coop_ratio;                      /* cooperative-job threshold (pl_coop_ratio by default) */
 	cudaStream_t stream;
@@ -71,7 +72,7 @@ struct pl_engine_s {
 	/* host planning scratch */
 	plk_job_t *hj;
 	int32_t *horder, *hwave, m_jobs;
-	int32_t last_waves, last_coop, last_dp_launches;
+	int32_t last_waves, last_coop, last_dp_launches, last_pairs;
 	/* optional CUDA-event timing of the phases: prep, DP, traceback, compaction */
 	int timing;
 	cudaEvent_t ev[2 + 4 * 64];

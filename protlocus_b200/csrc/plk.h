@@ -33,6 +33,9 @@ typedef struct {
 	 * kernel reads them as constants): go, ge, io, -fs + 9/8/7/6 (frameshift
 	 * candidates 6-9 with their tags), -fs, go + ge */
 	int32_t s16[9];
+	/* the paired int16x2 DP (mode 3): bias B of its 15-bit domain and the floor F that
+	 * stands for the reference's -32768 (set by the host when it forms pairs) */
+	int32_t pair_b, pair_f;
 } plk_params_t;
 
 /* fills plk_params_t.s16 from go/ge/io/fs (every host path that builds parameters calls it) */
@@ -52,12 +55,14 @@ typedef struct {
 	int64_t tmp_off;                 /* reversed CIGAR scratch (uint32 words), capacity nl+al+8 */
 	int64_t out_off;                 /* final CIGAR offset in the output buffer (filled by the scan) */
 	int32_t nl, al;
-	int32_t mode;                    /* 0: int16 (lower clamp suffices), 1: int32 (gs32b), 2: int16 both clamps */
+	int32_t mode;                    /* 0: int16 (lower clamp suffices), 1: int32 (gs32b), 2: int16 both clamps,
+	                                  * 3: int16 paired with a job of the same protein and window length */
 	int32_t slen;                    /* segment length of the striping being reproduced */
 	int32_t nw;                      /* warps cooperating on the job: 1 or PLK_WARPS_PER_CTA */
 	int32_t rows;                    /* DP rows per lane of a strip: 8 or 4 */
 	int32_t score, n_tmp;            /* outputs of the DP / traceback */
-	int32_t status, pad;
+	int32_t status;
+	int32_t pair;                    /* mode 3: the partner job's index in the first job of a pair, -1 in the second */
 } plk_job_t;
 
 /* per-request metadata of the extension DP, device resident */

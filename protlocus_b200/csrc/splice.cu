@@ -500,6 +500,321 @@ k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop
 	}
 }
 
+/* ------------------------------------------------------------------ paired int16x2 DP (mode 3) */
+
+/*
+ * Two jobs with one protein and windows of one length -- the two strands of a
+ * locus -- run in the two 16-bit halves of every 32-bit register, so one DPX
+ * instruction (__viaddmax_u16x2: max(a + b, c); __vimax3_u16x2) updates the same
+ * cell of both.  Values live in a biased 15-bit domain per half: v -> v + B, with
+ * the reference's saturation floor (-32768) mapped to F.  The host admits a pair
+ * only when every value the DP can reach provably stays within [F + 512,
+ * 0x7fff - 512] after biasing: the 16-bit adds then never wrap, values at the
+ * floor never meet real ones, and every clamp at F is exactly the reference's
+ * _mm_subs_epi16 saturation.
+ *
+ * The first-winning candidate cannot ride in the low bits of the value as in the
+ * 32-bit kernel.  Each cell stores ten bits "candidate k is below the maximum"
+ * (the traceback takes the first clear one: first wins, nasw-sse.c:517-530) and the
+ * six extension / lazy-F comparisons.  Each bit is one add: with both operands
+ * below 0x8000 per half, (a + 0x8000 - b) has bit 15 set exactly when a >= b and
+ * never borrows across the halves.  Byte permutes with sign replication gather the
+ * bit-15 / bit-31 answers into bytes, and a tree of bit-selects merges them into
+ * the trace word of each job (low half: the first job, high half: the second):
+ *   bits 0-4  s0 s2 s4 s6 s8     bits 8-12  s1 s3 s5 s7 s9   (s_k: candidate k < max)
+ *   bits 5-7  g4 g6 g8           bits 13-15 g5 g7 g9         (g4: not I-extended,
+ *   g5: not D-extended, g6/g7/g8: not A/B/C-extended, g9: not raised by the carried
+ *   insertion); the traceback converts such a word to the layout of the other modes.
+ */
+struct DpSharedPair {
+	int32_t slot[2][PLK_WARPS_PER_CTA][PLK_RING_INTS];
+	int32_t job;
+	int32_t pre[PLK_WARPS_PER_CTA][PLK_RING_INTS] __attribute__((aligned(16)));
+	uint8_t rows[PLK_WARPS_PER_CTA][2][2][3][ROWBLK] __attribute__((aligned(16)));  /* [warp][job][parity][array] */
+};
+#define PAIR_SCT_WORDS (22 * 22 * 22)   /* [protein residue][codon residue of job 1][of job 2] */
+
+__device__ __forceinline__ unsigned pk16(int a, int b) { return ((unsigned)a & 0xffffu) | ((unsigned)b << 16); }
+/* bytes: sign of x's bit 15, of y's bit 15, of x's bit 31, of y's bit 31 */
+__device__ __forceinline__ unsigned sign_pairs(unsigned x, unsigned y)
+{
+	unsigned d;
+	asm("prmt.b32 %0, %1, %2, 0xFBD9;" : "=r"(d) : "r"(x), "r"(y));
+	return d;
+}
+__device__ __forceinline__ unsigned sel_bits(unsigned a, unsigned b, unsigned m) { return (a & m) | (b & ~m); }
+/* per-half unsigned maximum of two, as one add+max instruction (there is no two-input form) */
+__device__ __forceinline__ unsigned vmax2u(unsigned a, unsigned b) { return __viaddmax_u16x2(a, 0u, b); }
+
+struct PairK { unsigned F2, GOn, GEn, IOn, FSn, FSp, GOEn; };
+
+template <int R>
+__device__ __forceinline__ void cells_pair(const unsigned (&in)[9], unsigned (&hm)[R], const unsigned ah1,
+		const unsigned ah2, const unsigned ah3, const bool row2, const unsigned r2h, const unsigned r2f,
+		const uint32_t *__restrict__ srow, const int (&cp)[R], const unsigned (&gi)[R], const unsigned (&dn)[R + 2],
+		const unsigned (&ac)[R + 2], unsigned (&ip)[R], unsigned (&lh)[R], const unsigned (&ic)[R], const PairK &K,
+		unsigned (&o)[9], unsigned (&z)[R], unsigned (&hn)[R])
+{
+	unsigned h1 = in[0], h2 = in[1], h3 = in[2], d1 = in[3], d2 = in[4], d3 = in[5], va = in[6], vb = in[7], vc = in[8];
+#pragma unroll
+	for (int r = 0; r < R; ++r) {
+		unsigned h1m1 = r >= 1 ? hm[r - 1] : ah1;
+		unsigned h2m1 = r >= 2 ? hm[r - 2] : (r == 1 ? ah1 : ah2);
+		unsigned h3m1 = r >= 3 ? hm[r - 3] : (r == 2 ? ah1 : (r == 1 ? ah2 : ah3));
+		if (r == 0 && row2) h1m1 = r2f, h2m1 = r2f, h3m1 = r2h; /* column -1 while row 2 is computed: {0, -fs, -fs} */
+		/* 1: I -- g4 = H'(c-1) - go >= I(c-1) */
+		const unsigned t4 = __viaddmax_u16x2(lh[r], K.GOn, K.F2);
+		const unsigned g4 = t4 + 0x80008000u - ip[r];
+		const unsigned ipn = __viaddmax_u16x2(vmax2u(t4, ip[r]), K.GEn, K.F2);
+		ip[r] = ipn;
+		/* 2: D -- g5 = H(i-3) - go >= D(i-3) */
+		const unsigned u5 = __viaddmax_u16x2(h3, K.GOn, K.F2);
+		const unsigned g5 = u5 + 0x80008000u - d3;
+		const unsigned dnew = __viaddmax_u16x2(vmax2u(u5, d3), gi[r], K.F2);
+		/* 3-5: phase-0/1/2 introns */
+		const unsigned ua = __viaddmax_u16x2(h1, K.IOn, K.F2);
+		const unsigned t6 = __viaddmax_u16x2(ua, dn[r], K.F2);
+		const unsigned g6 = t6 + 0x80008000u - va;
+		const unsigned anew = vmax2u(t6, va);
+		const unsigned ub = __viaddmax_u16x2(h1m1, K.IOn, K.F2);
+		const unsigned t7 = __viaddmax_u16x2(ub, dn[r + 1], K.F2);
+		const unsigned g7 = t7 + 0x80008000u - vb;
+		const unsigned bnew = vmax2u(t7, vb);
+		const unsigned t8 = __viaddmax_u16x2(ub, dn[r + 2], K.F2);
+		const unsigned g8 = t8 + 0x80008000u - vc;
+		const unsigned cnew = vmax2u(t8, vc);
+		/* candidates 0-5 (floored at F, where none of them can win), 6-9 folded */
+		const unsigned c0 = __viaddmax_u16x2(h3m1, srow[cp[r]], K.F2);  /* H(i-3,j-1) + s(i,j) */
+		const unsigned c3 = __viaddmax_u16x2(anew, ac[r + 2], K.F2);    /* A - a(i) */
+		const unsigned c4 = __viaddmax_u16x2(bnew, ac[r], K.F2);        /* B - a(i-2) */
+		const unsigned c5 = __viaddmax_u16x2(cnew, ac[r + 1], K.F2);    /* C - a(i-1) */
+		unsigned he = __vimax3_u16x2(c0, ipn, dnew);
+		he = __vimax3_u16x2(he, c3, c4);
+		const unsigned fsm = vmax2u(__vimax3_u16x2(h1, h2, h1m1), h2m1);
+		he = __viaddmax_u16x2(fsm, K.FSn, vmax2u(he, c5));     /* 6-9: H(i-1|i-2, j|j-1) - fs */
+		/* s_k: candidate k < max, the bit 15 of max + 0x7fff - c_k (no borrow: c_k <= max) */
+		const unsigned m1 = he + 0x7fff7fffu;
+		const unsigned s0 = m1 - c0, s1 = m1 - ipn, s2 = m1 - dnew, s3 = m1 - c3, s4 = m1 - c4, s5 = m1 - c5;
+		const unsigned s6 = m1 - h1 + K.FSp, s7 = m1 - h2 + K.FSp, s8 = m1 - h1m1 + K.FSp, s9 = m1 - h2m1 + K.FSp;
+		lh[r] = he;
+		/* the carried insertion: g9 = H' >= ic */
+		const unsigned g9 = he + 0x80008000u - ic[r];
+		const unsigned h = vmax2u(he, ic[r]);
+		/* gather the sixteen bits of both cells */
+		const unsigned p0 = sign_pairs(s0, s1), p1 = sign_pairs(s2, s3), p2 = sign_pairs(s4, s5), p3 = sign_pairs(s6, s7);
+		const unsigned p4 = sign_pairs(s8, s9), p5 = sign_pairs(g4, g5), p6 = sign_pairs(g6, g7), p7 = sign_pairs(g8, g9);
+		const unsigned q01 = sel_bits(p0, p1, 0x01010101u), q23 = sel_bits(p2, p3, 0x04040404u);
+		const unsigned q45 = sel_bits(p4, p5, 0x10101010u), q67 = sel_bits(p6, p7, 0x40404040u);
+		z[r] = sel_bits(sel_bits(q01, q23, 0x03030303u), sel_bits(q45, q67, 0x30303030u), 0x0f0f0f0fu);
+		hn[r] = h;
+		h3 = h2, h2 = h1, h1 = h;
+		d3 = d2, d2 = d1, d1 = dnew;
+		va = anew, vb = bnew, vc = cnew;
+	}
+	o[0] = h1, o[1] = h2, o[2] = h3, o[3] = d1, o[4] = d2, o[5] = d3, o[6] = va, o[7] = vb, o[8] = vc;
+}
+
+template <int R>
+__device__ __forceinline__ void store_trace_pair(uint16_t *pa, uint16_t *pb, const unsigned (&z)[R])
+{ /* low halves to the first job's trace, high halves to the second's */
+	uint32_t wa[R / 2], wb[R / 2];
+#pragma unroll
+	for (int q = 0; q < R / 2; ++q) wa[q] = __byte_perm(z[2 * q], z[2 * q + 1], 0x5410), wb[q] = __byte_perm(z[2 * q], z[2 * q + 1], 0x7632);
+	*(typename TraceVec<R>::T*)pa = *(const typename TraceVec<R>::T*)wa;
+	*(typename TraceVec<R>::T*)pb = *(const typename TraceVec<R>::T*)wb;
+}
+
+/* One pair of jobs on a wavefront of NW warps; the structure of dp_job with packed values. */
+template <int NW, int R>
+__device__ __forceinline__ void dp_pair(plk_job_t *__restrict__ JA, plk_job_t *__restrict__ JB,
+		const uint8_t *__restrict__ prep, uint16_t *__restrict__ trace, int32_t *__restrict__ myring,
+		DpSharedPair &sh, const uint32_t *__restrict__ sct2, const PairK &K, const plk_params_t &P,
+		const int L, const int wib)
+{
+	constexpr int NL = 32 * NW, HS = NL * R;
+	const unsigned NEG = K.F2;
+	const int lane = L & 31, w = L >> 5;
+	const int nl = JA->nl, al = JA->al, slen = JA->slen;
+	const uint8_t *nasA = prep + JA->prep_off, *aas = nasA + nl;
+	const int8_t *donA = (const int8_t*)(aas + al), *accA = donA + nl + 1;
+	const uint8_t *nasB = prep + JB->prep_off;
+	const int8_t *donB = (const int8_t*)(nasB + nl + al), *accB = donB + nl + 1;
+	uint16_t *trA = trace + JA->trace_off, *trB = trace + JB->trace_off;
+	const int nr = nl - 2, nstrip = (nr + HS - 1) / HS;
+	const int Pc = al > NL ? al : NL + 1;
+	const int total = nstrip * Pc + NL - 1;
+	int32_t *pre = sh.pre[wib];
+	uint8_t (*rowA)[3][ROWBLK] = sh.rows[wib][0], (*rowB)[3][ROWBLK] = sh.rows[wib][1];
+	const unsigned r2h = P.pair_b * 0x10001u, r2f = (unsigned)(P.pair_b - P.fs) * 0x10001u;
+
+	int c = -L, k = 0, cs = 0, dcol = 0, i0 = 0;
+	unsigned ip[R], lh[R], ic[R], hm[R], gi[R], dn[R + 2], ac[R + 2];
+	int cp[R];
+	unsigned ah1 = NEG, ah2 = NEG, ah3 = NEG;
+	unsigned o[9];
+#pragma unroll
+	for (int q = 0; q < 9; ++q) o[q] = NEG;
+#pragma unroll
+	for (int r = 0; r < R; ++r) ip[r] = lh[r] = ic[r] = hm[r] = NEG, cp[r] = 0, gi[r] = 0;
+#pragma unroll
+	for (int r = 0; r < R + 2; ++r) dn[r] = ac[r] = 0;
+	stage_rows<R>(rowA[0], nasA, donA, accA, nl, 2 + w * 32 * R, lane);
+	stage_rows<R>(rowB[0], nasB, donB, accB, nl, 2 + w * 32 * R, lane);
+	if (L == 0) {
+#pragma unroll
+		for (int q = 0; q < 9; ++q) pre[q] = (int32_t)NEG;
+	}
+	cp_async_wait_all();
+	__syncwarp();
+
+	for (int s = 0; s < total; ++s) {
+		if (__shfl_sync(FULL, c, 0) == 0) {
+			cp_async_wait_all();
+			__syncwarp();
+			const int kn = (s - 32 * w) / Pc + 1;
+			if (kn < nstrip) {
+				stage_rows<R>(rowA[kn & 1], nasA, donA, accA, nl, 2 + kn * HS + w * 32 * R, lane);
+				stage_rows<R>(rowB[kn & 1], nasB, donB, accB, nl, 2 + kn * HS + w * 32 * R, lane);
+			}
+		}
+		unsigned in[9];
+#pragma unroll
+		for (int q = 0; q < 9; ++q) in[q] = __shfl_up_sync(FULL, o[q], 1);
+		const bool started = c >= 0 && k < nstrip;
+		if (lane == 0 && started) {
+			if (w == 0) cp_async_wait_all();
+			const int32_t *p = w == 0 ? pre : sh.slot[(s - 1) & 1][wib - 1];
+			const int4 v0 = *(const int4*)p, v1 = *(const int4*)(p + 4);
+			in[0] = v0.x, in[1] = v0.y, in[2] = v0.z, in[3] = v0.w;
+			in[4] = v1.x, in[5] = v1.y, in[6] = v1.z, in[7] = v1.w, in[8] = p[8];
+		}
+		if (started && c == 0) { /* strip start: per-row constants of both jobs, column -1 */
+			i0 = 2 + k * HS + L * R;
+			const int b = i0 - lane * R;
+			const uint8_t *ra = &rowA[k & 1][0][0] + lane * R, *rb = &rowB[k & 1][0][0] + lane * R;
+			const int onA = (int)((uintptr_t)(nasA + b) & 15), odA = (int)((uintptr_t)(donA + b - 1) & 15),
+				oaA = (int)((uintptr_t)(accA + b - 2) & 15);
+			const int onB = (int)((uintptr_t)(nasB + b) & 15), odB = (int)((uintptr_t)(donB + b - 1) & 15),
+				oaB = (int)((uintptr_t)(accB + b - 2) & 15);
+#pragma unroll
+			for (int r = 0; r < R; ++r) {
+				const int i = i0 + r;
+				const int ca = i < nl ? ra[onA + r] : 0, cb = i < nl ? rb[onB + r] : 0;
+				cp[r] = ca * 22 + cb;
+				gi[r] = pk16(-(ca == 20 ? P.fs : P.ge), -(cb == 20 ? P.fs : P.ge));
+				ip[r] = lh[r] = ic[r] = hm[r] = NEG;
+			}
+#pragma unroll
+			for (int r = 0; r < R + 2; ++r) {
+				const int pd = i0 - 1 + r, pa = i0 - 2 + r;
+				const int dva = pd <= nl ? (int8_t)ra[ROWBLK + odA + r] : 0, dvb = pd <= nl ? (int8_t)rb[ROWBLK + odB + r] : 0;
+				const int ava = pa <= nl ? (int8_t)ra[2 * ROWBLK + oaA + r] : 0, avb = pa <= nl ? (int8_t)rb[2 * ROWBLK + oaB + r] : 0;
+				dn[r] = pk16(-dva, -dvb);
+				ac[r] = pk16(-ava, -avb);
+			}
+			ah1 = ah2 = ah3 = NEG;
+			cs = 0, dcol = L % al;
+		}
+		if (started && c < al && i0 < nl) {
+			const bool seg = cs == 0, first = c == 0, row2 = first && i0 == 2;
+			const uint32_t *srow = sct2 + 484 * aas[c];
+			unsigned hn[R], z[R];
+			/* the striped schedule's segment hand-over (nasw-sse.c:537-553) */
+			if (seg) {
+#pragma unroll
+				for (int r = 0; r < R; ++r) {
+					const unsigned hop = __viaddmax_u16x2(lh[r], K.GOEn, NEG), iext = __viaddmax_u16x2(ip[r], K.GEn, NEG);
+					ic[r] = __vimax3_u16x2(hop, iext, __viaddmax_u16x2(ic[r], K.GEn, NEG));
+					ip[r] = NEG, lh[r] = NEG;
+				}
+			} else {
+#pragma unroll
+				for (int r = 0; r < R; ++r) ic[r] = __viaddmax_u16x2(ic[r], K.GEn, NEG);
+			}
+			cells_pair<R>(in, hm, ah1, ah2, ah3, row2, r2h, r2f, srow, cp, gi, dn, ac, ip, lh, ic, K, o, z, hn);
+			const int64_t toff = (((int64_t)k * al + dcol) * NL + L) * R;
+			store_trace_pair<R>(trA + toff, trB + toff, z);
+			if (L == NL - 1) {
+				int32_t *e = myring + (int64_t)c * PLK_RING_INTS;
+#pragma unroll
+				for (int q = 0; q < 9; ++q) __stcg(e + q, (int32_t)o[q]);
+			}
+#pragma unroll
+			for (int r = 0; r < R; ++r) hm[r] = hn[r];
+			ah1 = in[0], ah2 = in[1], ah3 = in[2];
+		}
+		if (NW > 1) {
+			if (lane == 31) {
+				int32_t *sl = sh.slot[s & 1][wib];
+#pragma unroll
+				for (int q = 0; q < 9; ++q) sl[q] = (int32_t)o[q];
+			}
+			__syncthreads();
+		} else __syncwarp();
+		++c;
+		if (c > 0) {
+			if (++cs == slen) cs = 0;
+			if (++dcol >= al) dcol = 0;
+		}
+		if (c == Pc) c = 0, ++k;
+		if (L == 0 && k >= 1 && k < nstrip && c < al) {
+			const int32_t *e = myring + (int64_t)c * PLK_RING_INTS;
+			cp_async16(pre, e), cp_async16(pre + 4, e + 4), cp_async16(pre + 8, e + 8);
+		}
+	}
+	cp_async_wait_all();
+	{ /* H(nl-1, al-1) of both jobs, unbiased */
+		const int rl = nl - 1 - i0;
+		if (rl >= 0 && rl < R) {
+#pragma unroll
+			for (int r = 0; r < R; ++r)
+				if (r == rl) JA->score = (int)(hm[r] & 0xffffu) - P.pair_b, JB->score = (int)(hm[r] >> 16) - P.pair_b;
+		}
+	}
+}
+
+template <int R>
+__global__ void __launch_bounds__(32 * PLK_WARPS_PER_CTA, R == 8 ? 2 : 3)
+k_splice_pair(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop, int n_coop,
+		const int32_t *__restrict__ order_solo, int n_solo, int32_t *counters,
+		const uint8_t *__restrict__ prep, uint16_t *__restrict__ trace, int32_t *__restrict__ ring,
+		int64_t ring_stride, plk_params_t P)
+{
+	__shared__ DpSharedPair sh;
+	extern __shared__ __align__(16) uint32_t pair_sct[];  /* [a][ca][cb] = s(ca, a) | s(cb, a) << 16 */
+	for (int x = threadIdx.x; x < PAIR_SCT_WORDS; x += blockDim.x) {
+		const int a = x / 484, ca = (x / 22) % 22, cb = x % 22;
+		pair_sct[x] = pk16(P.sc[ca * 22 + a], P.sc[cb * 22 + a]);
+	}
+	PairK K;
+	K.F2 = (unsigned)P.pair_f * 0x10001u;
+	K.GOn = pk16(-P.go, -P.go), K.GEn = pk16(-P.ge, -P.ge), K.IOn = pk16(-P.io, -P.io);
+	K.FSn = pk16(-P.fs, -P.fs), K.FSp = pk16(P.fs, P.fs), K.GOEn = pk16(-(P.go + P.ge), -(P.go + P.ge));
+	__syncthreads();
+	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+	for (;;) {
+		if (threadIdx.x == 0) sh.job = atomicAdd(&counters[0], 1);
+		__syncthreads();
+		const int idx = sh.job;
+		__syncthreads();
+		if (idx >= n_coop) break;
+		plk_job_t *J = jobs + order_coop[idx];
+		dp_pair<PLK_WARPS_PER_CTA, R>(J, jobs + J->pair, prep, trace,
+				ring + (int64_t)blockIdx.x * PLK_WARPS_PER_CTA * ring_stride, sh, pair_sct, K, P, threadIdx.x, wib);
+		__syncthreads();
+	}
+	int32_t *myring = ring + ((int64_t)blockIdx.x * PLK_WARPS_PER_CTA + wib) * ring_stride;
+	for (;;) {
+		int idx = 0;
+		if (lane == 0) idx = atomicAdd(&counters[1], 1);
+		idx = __shfl_sync(FULL, idx, 0);
+		if (idx >= n_solo) break;
+		plk_job_t *J = jobs + order_solo[idx];
+		dp_pair<1, R>(J, jobs + J->pair, prep, trace, myring, sh, pair_sct, K, P, lane, wib);
+		__syncwarp();
+	}
+}
+
 /* ------------------------------------------------------------------ traceback */
 
 /* trace-word bit of the extension flag of state 1..5 (I, D, A, B, C) */
@@ -536,6 +851,25 @@ __device__ __forceinline__ void tb_load_chunk(const uint16_t *__restrict__ tr, i
 	}
 }
 
+/* a trace word of the paired kernel in the layout of the other modes (15 - state in
+ * bits 0-3, extension bits I 4, D 5, C 6, A 12, B 13, carried-insertion bit 14) */
+__device__ __forceinline__ uint16_t tb_pair_norm(unsigned x)
+{
+	const unsigned s = (x & 1u) | (x >> 7 & 2u) | (x << 1 & 4u) | (x >> 6 & 8u) | (x << 2 & 16u) | (x >> 5 & 32u) |
+		(x << 3 & 64u) | (x >> 4 & 128u) | (x << 4 & 256u) | (x >> 3 & 512u);
+	const unsigned state = __ffs(~s) - 1;  /* the first candidate equal to the maximum */
+	const unsigned n = ~x;                 /* the g bits are negated flags */
+	return (uint16_t)((15u - state) | (n >> 5 & 1u) << 4 | (n >> 13 & 1u) << 5 | (n >> 7 & 1u) << 6 |
+		(n >> 6 & 1u) << 12 | (n >> 14 & 1u) << 13 | (n >> 15 & 1u) << 14);
+}
+
+__device__ __forceinline__ void tb_norm8(uint16_t (&w)[8], const bool pair)
+{
+	if (!pair) return;
+#pragma unroll
+	for (int r = 0; r < 8; ++r) w[r] = tb_pair_norm(w[r]);
+}
+
 __global__ void __launch_bounds__(32 * TB_WARPS) k_traceback(plk_job_t *__restrict__ jobs,
 		const int32_t *__restrict__ order, int n_order, const uint16_t *__restrict__ trace, uint32_t *__restrict__ tmp)
 {
@@ -548,6 +882,7 @@ __global__ void __launch_bounds__(32 * TB_WARPS) k_traceback(plk_job_t *__restri
 	const uint16_t *tr = trace + J->trace_off;
 	uint32_t *out = tmp + J->tmp_off;
 	const int nlanes = 32 * J->nw;
+	const bool pair = J->mode == 3;
 	int i = nl - 1, j = al - 1, last = 0, n = 0;
 	while (i >= 2 && j >= 0) {
 		/* stage the tile whose top-right corner holds (i, j): 8-row groups, one or two chunks each */
@@ -566,6 +901,7 @@ __global__ void __launch_bounds__(32 * TB_WARPS) k_traceback(plk_job_t *__restri
 					tb_load_chunk(tr, 4, nlanes, al, 2 * g + 1, col, w2);
 					*(uint2*)(w + 4) = *(const uint2*)w2;
 				}
+				tb_norm8(w, pair);
 				s_tile[wib][dq][dc] = *(const uint4*)w;
 			}
 		}
@@ -608,6 +944,7 @@ __global__ void __launch_bounds__(32 * TB_WARPS) k_traceback(plk_job_t *__restri
 			if (ch >= 0) {
 				__align__(16) uint16_t w[8];
 				tb_load_chunk(tr, R, nlanes, al, ch, j, w);
+				tb_norm8(w, pair);
 				const int ra = ch * R;
 #pragma unroll
 				for (int r = 7; r >= 0; --r) {
@@ -705,8 +1042,20 @@ static int dp_occupancy()
 	return e == cudaSuccess ? n : -1;
 }
 
+#define PAIR_SMEM (PAIR_SCT_WORDS * 4)
+
+template <int R>
+static int pair_occupancy()
+{
+	int n = 0;
+	if (cudaFuncSetAttribute(k_splice_pair<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM) != cudaSuccess) return -1;
+	const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_splice_pair<R>, 32 * PLK_WARPS_PER_CTA, PAIR_SMEM);
+	return e == cudaSuccess ? n : -1;
+}
+
 extern "C" int plk_dp_ctas_per_sm(int32_t mode, int32_t rows)
 {
+	if (mode == 3) return rows == 4 ? pair_occupancy<4>() : pair_occupancy<8>();
 	if (rows == 4) return mode == 1 ? dp_occupancy<1, 4>() : mode == 2 ? dp_occupancy<2, 4>() : dp_occupancy<0, 4>();
 	return mode == 1 ? dp_occupancy<1, 8>() : mode == 2 ? dp_occupancy<2, 8>() : dp_occupancy<0, 8>();
 }
@@ -723,7 +1072,12 @@ extern "C" int plk_splice_dp(plk_job_t *jobs, const int32_t *order_coop, int32_t
 	const dim3 grid(n_ctas), block(32 * PLK_WARPS_PER_CTA);
 #define DP_LAUNCH(M, RR) k_splice_dp<M, RR><<<grid, block, 0, st>>>(jobs, order_coop, n_coop, order_solo, n_solo, \
 		counters, prep, trace, ring, ring_stride_ints, *p)
-	if (rows == 4) {
+	if (mode == 3) { /* pairs: order_* hold the first job of each pair (jobs[q].pair: the second) */
+		if (rows == 4) k_splice_pair<4><<<grid, block, PAIR_SMEM, st>>>(jobs, order_coop, n_coop, order_solo, n_solo,
+				counters, prep, trace, ring, ring_stride_ints, *p);
+		else k_splice_pair<8><<<grid, block, PAIR_SMEM, st>>>(jobs, order_coop, n_coop, order_solo, n_solo,
+				counters, prep, trace, ring, ring_stride_ints, *p);
+	} else if (rows == 4) {
 		if (mode == 1) DP_LAUNCH(1, 4); else if (mode == 2) DP_LAUNCH(2, 4); else DP_LAUNCH(0, 4);
 	} else {
 		if (mode == 1) DP_LAUNCH(1, 8); else if (mode == 2) DP_LAUNCH(2, 8); else DP_LAUNCH(0, 8);

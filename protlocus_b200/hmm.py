@@ -169,3 +169,50 @@ def regions(rng: np.random.Generator, probs: np.ndarray, n: int, len_min: int = 
 
 
 assert AA_I2C[:20] != ALPHABET  # the two alphabet orders differ: emissions are indexed in HMMER order
+
+
+def genome_scan(probs, seed: int, genome_mb: float = 100.0, n_domains: int = 1000, slice_mb: float = 2.0,
+                region_nt: int = 30000, overlap_nt: int = 2400, gc: float = 0.45):
+    """The profile-HMM configuration's genome: genome_mb of 45% GC sequence (nt4 codes) with
+    n_domains domains sampled from the profiles' match emissions, reverse-translated and planted
+    on random strands; and the regions of a scan of its first slice_mb in six frames -- the slice
+    and its reverse complement cut into region_nt windows overlapping by overlap_nt (a domain of
+    up to 800 codons is inside one window), each window in frames 0, 1, 2.  Returns (nt4 regions
+    concatenated, offsets, lengths, planted domains inside the slice)."""
+    rng = np.random.default_rng(seed)
+    n = int(genome_mb * 1e6)
+    p = np.array([(1 - gc) / 2, gc / 2, gc / 2, (1 - gc) / 2])
+    g = rng.choice(4, size=n, p=p).astype(np.uint8)
+    comp = np.array([3, 2, 1, 0, 4], np.uint8)
+    slice_nt = min(n, int(slice_mb * 1e6))
+    inside = 0
+    for _ in range(n_domains):
+        k = int(rng.integers(0, len(probs)))
+        pr = probs[k]
+        m = pr.shape[0]
+        a, b = sorted(int(x) for x in rng.integers(0, m + 1, size=2))
+        if b - a < 10:
+            a, b = 0, m
+        cdf = np.cumsum(pr[a:b] / pr[a:b].sum(axis=1, keepdims=True), axis=1)
+        pick = (rng.random(b - a)[:, None] > cdf).sum(axis=1).clip(0, 19)
+        cds = nt4(reverse_translate(rng, "".join(ALPHABET[int(x)] for x in pick)).encode())
+        pos = int(rng.integers(0, n - len(cds)))
+        if rng.random() < 0.5:
+            cds = comp[cds[::-1]]
+        g[pos:pos + len(cds)] = cds
+        inside += pos + len(cds) <= slice_nt
+    fwd = g[:slice_nt]
+    rev = comp[fwd[::-1]]
+    parts, offs, lens = [], [], []
+    pos = 0
+    step = region_nt - overlap_nt
+    for strand in (fwd, rev):
+        for st in range(0, max(1, len(strand) - overlap_nt), step):
+            w = strand[st:st + region_nt]
+            for f in range(3):
+                r = w[f:]
+                parts.append(r)
+                offs.append(pos)
+                lens.append(len(r))
+                pos += len(r)
+    return (np.concatenate(parts), np.array(offs, np.int32), np.array(lens, np.int32), inside)

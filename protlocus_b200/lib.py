@@ -127,6 +127,9 @@ def load() -> C.CDLL:
     lib.pl_rc_last_cells.restype = C.c_int64
     lib.pl_rc_mathf_eval.argtypes = [C.c_int32, C.c_int32, C.c_uint32, C.c_uint32, C.c_int64, C.c_void_p]
     lib.pl_rc_mathf_eval.restype = C.c_int
+    lib.pl_engine_last_pairs.argtypes = [C.c_void_p]
+    lib.pl_engine_last_pairs.restype = C.c_int32
+    lib.pl_engine_set_pairing.argtypes = [C.c_void_p, C.c_int32]
     lib.pl_group_create.argtypes = [C.c_void_p, C.c_int32, C.c_int64]
     lib.pl_group_create.restype = C.c_void_p
     lib.pl_group_destroy.argtypes = [C.c_void_p]
@@ -260,6 +263,12 @@ class Engine:
         if self.h:
             self.lib.pl_engine_destroy(self.h)
             self.h = None
+
+    def set_pairing(self, on: bool):
+        self.lib.pl_engine_set_pairing(self.h, int(on))
+
+    def last_pairs(self) -> int:
+        return int(self.lib.pl_engine_last_pairs(self.h))
 
     def __del__(self):
         try:
@@ -401,15 +410,18 @@ class Engine:
         jobs = (SpliceJob * n)()
         nt_parts, aa_parts, ss_parts = [], [], []
         pos_nt = pos_aa = 0
+        prot_off = {}  # one copy of each protein: jobs that share it (both strands) can run as int16x2 pairs
         for q, (nt, aa) in enumerate(pairs):
-            jobs[q].nt_off, jobs[q].aa_off, jobs[q].nl, jobs[q].al = pos_nt, pos_aa, len(nt), len(aa)
+            if aa not in prot_off:
+                prot_off[aa] = pos_aa
+                aa_parts.append(aa)
+                pos_aa += len(aa)
+            jobs[q].nt_off, jobs[q].aa_off, jobs[q].nl, jobs[q].al = pos_nt, prot_off[aa], len(nt), len(aa)
             s = ss[q] if ss is not None else None
             jobs[q].ss_off = pos_nt if s is not None else -1
             nt_parts.append(nt)
-            aa_parts.append(aa)
             ss_parts.append(s if s is not None else bytes(len(nt)))
             pos_nt += len(nt)
-            pos_aa += len(aa)
         ntb = np.frombuffer(b"".join(nt_parts), dtype=np.uint8)
         aab = np.frombuffer(b"".join(aa_parts), dtype=np.uint8)
         ssb = np.frombuffer(b"".join(ss_parts), dtype=np.uint8) if ss is not None else None

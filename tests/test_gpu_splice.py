@@ -321,3 +321,91 @@ def test_queue_async_submits(queue_ready, oracle):
         libc.free(C.cast(r.cigar, C.c_void_p))
     assert lib.ns_gpu_dispatch_count() - d0 == 129
     assert lib.ns_gpu_launch_count() - l0 >= 2
+
+
+def _paired_batch(rng, n, max_al=80):
+    """Random loci on both strands plus exact duplicates: every job has a partner with the same
+    protein and window length, so the engine runs them as int16x2 pairs."""
+    pairs = []
+    for q in range(n):
+        nt, aa = W.random_pair(rng, max_al=max_al)
+        pairs += [(nt, aa), (W.revcomp(nt), aa)] if q % 3 else [(nt, aa), (nt, aa)]
+    return pairs
+
+
+@pytest.mark.parametrize("seed", [21, 22])
+def test_paired_int16x2_bit_exact(engine, oracle, seed):
+    """The paired kernel (two jobs per 32-bit lane) against the oracle: random pairs on both
+    strands, planted loci, and the golden vectors with a duplicate strand; pairing on and off
+    give identical results."""
+    rng = np.random.default_rng(seed)
+    opt = Options(flag=NS_F_CIGAR)
+    pairs = _paired_batch(rng, 150)
+    for q in range(6):
+        nt, aa = W.single_locus(seed=seed * 100 + q, al=int(rng.integers(120, 600)),
+                                window=int(rng.integers(2000, 9000)))
+        pairs += [(nt, aa), (W.revcomp(nt), aa)]
+    got = _check(engine, oracle, opt, pairs)
+    assert engine.last_pairs() == len(pairs) // 2
+    engine.set_pairing(False)
+    try:
+        plain = engine.align_host(opt, pairs)
+        assert engine.last_pairs() == 0
+    finally:
+        engine.set_pairing(True)
+    assert [(s, c) for s, c, _ in got] == [(s, c) for s, c, _ in plain]
+
+
+def test_paired_golden_vectors_with_twins(engine, oracle, golden):
+    """Each 16-bit golden vector next to its own twin (same protein, same window)."""
+    by_opt = {}
+    for c in golden["cases"]:
+        if c["opt"].get("flag", NS_F_CIGAR) & (NS_F_EXT_LEFT | NS_F_EXT_RIGHT) or c["fn"] != "ns_global_gs16b":
+            continue
+        if c["ss"]:
+            continue
+        by_opt.setdefault(repr(sorted(c["opt"].items())), []).append(c)
+    n = 0
+    for cases in by_opt.values():
+        opt = oracle.make_options(cases[0]["opt"])
+        if oracle.port_lib().port_needs_wide(opt.ptr, max(len(c["aa"]) for c in cases)):
+            continue
+        pairs = []
+        for c in cases:
+            pairs += [(c["nt"].encode(), c["aa"].encode())] * 2
+        got = engine.align_host(opt, pairs)
+        for k, c in enumerate(cases):
+            for t in range(2):
+                score, cig, _ = got[2 * k + t]
+                assert (score, cig) == (c["score"], c["cigar"]), (c["group"], len(c["nt"]), len(c["aa"]), score)
+                n += 1
+    assert n >= 200
+
+
+def test_paired_cooperative_and_waves(oracle):
+    """Long pairs on whole-CTA wavefronts, in a batch split into several trace waves."""
+    rng = np.random.default_rng(23)
+    opt = Options(flag=NS_F_CIGAR)
+    pairs = []
+    for q in range(10):
+        al = int(rng.integers(250, 700))
+        nt, aa = W.single_locus(seed=2300 + q, al=al, window=int(rng.integers(12000, 30000)))
+        pairs += [(nt, aa), (W.revcomp(nt), aa)]
+    pairs += _paired_batch(rng, 60, max_al=50)
+    eng = L.Engine(0, trace_budget_bytes=96 << 20)
+    try:
+        eng.set_tuning(0, 0.1)
+        got = _check(eng, oracle, opt, pairs)
+        plan = eng.last_plan()
+        assert plan["waves"] >= 2 and plan["coop"] >= 2 and eng.last_pairs() == len(pairs) // 2, plan
+    finally:
+        eng.close()
+
+
+def test_pairs_not_formed_outside_the_15_bit_range(engine, oracle):
+    """Penalties large enough to reach the int16 floor keep jobs unpaired (32-bit lanes)."""
+    rng = np.random.default_rng(24)
+    opt = Options(flag=NS_F_CIGAR, go=3000, ge=200, io=9000, fs=5000, stop_pen=23)
+    pairs = _paired_batch(rng, 40, max_al=40)
+    _check(engine, oracle, opt, pairs)
+    assert engine.last_pairs() == 0
