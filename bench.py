@@ -92,14 +92,19 @@ def parse():
     ap.add_argument("--genome-region-kb", type=int, default=12, help="region window of the genome scan (kb)")
     ap.add_argument("--requests", type=int, default=65536, help="extension requests per step (--workload ext)")
     ap.add_argument("--uniform", default=None, metavar="N:NL:AL",
-                    help="profiling case instead of the batched workload: N planted loci of window NL and protein AL")
+                    help="profiling case instead of the batched workload: N jobs, N/2 planted loci of window NL "
+                         "and protein AL on both strands")
     return ap.parse_args()
 
 
 def make_jobs(args, seed):
-    if args.uniform:
+    if args.uniform:  # n jobs: n/2 planted loci of window nl and protein al, each on both strands
         n, nl, al = (int(x) for x in args.uniform.split(":"))
-        return [W.single_locus(seed=seed * 100003 + q, al=al, window=nl) for q in range(n)]
+        out = []
+        for q in range((n + 1) // 2):
+            nt, aa = W.single_locus(seed=seed * 100003 + q, al=al, window=nl)
+            out += [(nt, aa), (W.revcomp(nt), aa)]
+        return out[:n]
     return W.batch_pairs(args.pairs, seed=seed)
 
 

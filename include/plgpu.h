@@ -499,6 +499,25 @@ int pl_pf_features_device(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_j
 		const uint8_t *nt, const uint8_t *aa, void *feats, int32_t *chain, void *stream);
 /* Scores of n candidates: out f32 [ceil(n/128)*128 x 16] device, from feats as above. */
 int pl_pf_predict(pl_pf_model_t *m, const void *feats, int64_t n, float *out, void *stream);
+/* The learned selector in one call (the hook it serves is the candidate selection
+ * of mp_gpu_prefilter_select, map.c:511-532, run from mp_gpu_prefilter_batch,
+ * map.c:1014-1089): features and the MLP over n candidates (host job table, nt/aa
+ * device buffers), then pl_pf_decide.  prob (optional, host): sigmoid of column 0.
+ * Host outputs: keep, fallback, out_jobs.  Returns 1 on success. */
+int pl_pf_select_device(pl_pf_model_t *m, pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jobs,
+		int32_t n, const uint8_t *nt, const uint8_t *aa, double tau, int32_t margin, double tau_fb,
+		uint8_t *keep, uint8_t *fallback, pl_splice_job_t *out_jobs, float *prob, void *stream);
+/* The decision (host only): keep[q] = logit >= logit(tau); a kept candidate's window
+ * becomes the union of the predicted span (columns 1-2 of out, clipped to [0, 1],
+ * times nl) and the span its best anchor chain implies (chain[4q] minus 3x the
+ * residues before chain[4q+2], chain[4q+1] plus 3x those after chain[4q+3]),
+ * widened by margin + rel x its length on each side, cut to the window; a span
+ * under 3 nt keeps the full window (out_jobs[q]: nt_off / nl moved, the rest
+ * copied).  fallback[q] = logit >= logit(tau_fb): a kept candidate whose DP on
+ * the cut window does not pass reruns on the full window. */
+int pl_pf_decide(int32_t n, const pl_splice_job_t *jobs, const float *out, int64_t out_stride, const int32_t *chain,
+		double tau, int32_t margin, double rel, double tau_fb, uint8_t *keep, uint8_t *fallback,
+		pl_splice_job_t *out_jobs);
 /* `steps` Adam steps on minibatches perm[s*batch .. (s+1)*batch) (s counts steps
  * modulo n_perm / batch) of feats (bf16 rows) and targets (f32 [label, start,
  * end, box weight] rows), device buffers; batch a multiple of 128.  Loss per step

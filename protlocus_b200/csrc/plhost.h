@@ -59,7 +59,9 @@ struct pl_engine_s {
 	dbuf_t r_prof, r_pep, r_dsq, r_order, r_counter, r_scratch, r_bits, r_bias;
 	int64_t r_last_cells;
 	/* learned-prefilter features */
-	dbuf_t pf_cand;
+	dbuf_t pf_cand, pf_feats, pf_chain, pf_out;
+	void *pf_host;          /* the selector's chain and score rows read back (grow-only) */
+	size_t pf_host_cap;
 	/* alignment statistics / exon features */
 	dbuf_t f_jobs, f_cig, f_nt, f_aa, f_pssm, f_mat, f_res, f_feat;
 	/* prescreen banded alignment */

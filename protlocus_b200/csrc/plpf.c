@@ -428,7 +428,9 @@ PL_EXPORT int pl_pf_gemm(int32_t device, const void *A, int64_t lda, const void 
 
 void pl_pf_engine_free(pl_engine_t *e)
 {
-	dbuf_free(&e->pf_cand);
+	dbuf_free(&e->pf_cand), dbuf_free(&e->pf_feats), dbuf_free(&e->pf_chain), dbuf_free(&e->pf_out);
+	free(e->pf_host);
+	e->pf_host = 0, e->pf_host_cap = 0;
 }
 
 PL_EXPORT int pl_pf_features_device(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n,
@@ -464,4 +466,75 @@ PL_EXPORT int pl_pf_features_device(pl_engine_t *e, const ns_opt_t *opt, const p
 fail:
 	free(hc);
 	return ok;
+}
+
+/* ------------------------------------------------------------------ the selector's decision */
+
+PL_EXPORT int pl_pf_decide(int32_t n, const pl_splice_job_t *jobs, const float *out, int64_t out_stride,
+		const int32_t *chain, double tau, int32_t margin, double rel, double tau_fb, uint8_t *keep, uint8_t *fallback,
+		pl_splice_job_t *out_jobs)
+{
+	const double z_keep = tau <= 0.0 ? -INFINITY : tau >= 1.0 ? INFINITY : log(tau / (1.0 - tau));
+	const double z_fb = tau_fb <= 0.0 ? -INFINITY : tau_fb >= 1.0 ? INFINITY : log(tau_fb / (1.0 - tau_fb));
+	int32_t q;
+	if (n < 0 || (n > 0 && (!jobs || !out || !keep || !out_jobs))) { pl_set_error("pf decide: bad arguments"); return 0; }
+	for (q = 0; q < n; ++q) {
+		const float *o = out + (int64_t)q * out_stride;
+		const pl_splice_job_t *x = &jobs[q];
+		const double nl = (double)x->nl, al = (double)x->al, z = (double)o[0];
+		double ps, pe, lo, hi, pad, s, e;
+		out_jobs[q] = *x;
+		keep[q] = z >= z_keep;
+		if (fallback) fallback[q] = z >= z_fb;
+		if (!keep[q]) continue;
+		/* the predicted span, window fractions clipped to [0, 1] */
+		ps = (double)fminf(fmaxf(o[1], 0.0f), 1.0f) * nl, pe = (double)fminf(fmaxf(o[2], 0.0f), 1.0f) * nl;
+		lo = ps < pe ? ps : pe, hi = ps < pe ? pe : ps;
+		if (chain && chain[4 * q] >= 0) { /* united with the span the best anchor chain implies */
+			const double c_lo = (double)chain[4 * q] - 3.0 * chain[4 * q + 2] - 2.0;
+			const double c_hi = (double)chain[4 * q + 1] + 3.0 * (al - 1.0 - chain[4 * q + 3]) + 1.0;
+			if (c_lo < lo) lo = c_lo;
+			if (c_hi > hi) hi = c_hi;
+		}
+		pad = (double)margin + rel * (hi - lo);
+		s = floor(lo - pad), e = ceil(hi + pad);
+		s = s < 0.0 ? 0.0 : s > nl ? nl : s;
+		e = e < 0.0 ? 0.0 : e > nl ? nl : e;
+		if (e - s < 3.0) s = 0.0, e = nl;
+		out_jobs[q].nt_off = x->nt_off + (int64_t)s;
+		out_jobs[q].nl = (int32_t)(e - s);
+	}
+	return 1;
+}
+
+PL_EXPORT int pl_pf_select_device(pl_pf_model_t *m, pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jobs,
+		int32_t n, const uint8_t *nt, const uint8_t *aa, double tau, int32_t margin, double tau_fb, uint8_t *keep,
+		uint8_t *fallback, pl_splice_job_t *out_jobs, float *prob, void *stream)
+{
+	cudaStream_t st = stream ? (cudaStream_t)stream : (e ? e->stream : 0);
+	const int64_t npad = ((int64_t)n + 127) / 128 * 128;
+	float *ho;
+	int32_t *hc, q;
+	if (!m || !e || n < 0) { pl_set_error("pf select: missing model or engine"); return 0; }
+	if (n == 0) return 1;
+	if (m->device != e->device || m->in_dim != PLK_PF_FDIM) { pl_set_error("pf select: model on another device or of another width"); return 0; }
+	CK(cudaSetDevice(e->device));
+	if (!dbuf_ensure(&e->pf_feats, 2 * (size_t)npad * PLK_PF_FDIM) || !dbuf_ensure(&e->pf_chain, 16 * (size_t)n) ||
+			!dbuf_ensure(&e->pf_out, 4 * 16 * (size_t)npad))
+		return 0;
+	if (e->pf_host_cap < (size_t)n) {
+		void *h = realloc(e->pf_host, (size_t)n * (16 + 16 * 4));
+		if (!h) { pl_set_error("out of host memory"); return 0; }
+		e->pf_host = h, e->pf_host_cap = (size_t)n;
+	}
+	hc = (int32_t*)e->pf_host, ho = (float*)((char*)e->pf_host + 16 * (size_t)n);
+	if (!pl_pf_features_device(e, opt, jobs, n, nt, aa, e->pf_feats.p, (int32_t*)e->pf_chain.p, st)) return 0;
+	if (!pl_pf_predict(m, e->pf_feats.p, n, (float*)e->pf_out.p, st)) return 0;
+	CK(cudaMemcpyAsync(hc, e->pf_chain.p, 16 * (size_t)n, cudaMemcpyDeviceToHost, st));
+	CK(cudaMemcpyAsync(ho, e->pf_out.p, 4 * 16 * (size_t)n, cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	if (prob) for (q = 0; q < n; ++q) prob[q] = 1.0f / (1.0f + expf(-ho[16 * q]));
+	return pl_pf_decide(n, jobs, ho, 16, hc, tau, margin, 0.0, tau_fb, keep, fallback, out_jobs);
+fail:
+	return 0;
 }

@@ -127,6 +127,13 @@ def load() -> C.CDLL:
     lib.pl_rc_last_cells.restype = C.c_int64
     lib.pl_rc_mathf_eval.argtypes = [C.c_int32, C.c_int32, C.c_uint32, C.c_uint32, C.c_int64, C.c_void_p]
     lib.pl_rc_mathf_eval.restype = C.c_int
+    lib.pl_pf_decide.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_double, C.c_int32,
+                                 C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.pl_pf_decide.restype = C.c_int
+    lib.pl_pf_select_device.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(NsOpt), C.c_void_p, C.c_int32, C.c_void_p,
+                                        C.c_void_p, C.c_double, C.c_int32, C.c_double, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.pl_pf_select_device.restype = C.c_int
     lib.pl_engine_last_pairs.argtypes = [C.c_void_p]
     lib.pl_engine_last_pairs.restype = C.c_int32
     lib.pl_engine_set_pairing.argtypes = [C.c_void_p, C.c_int32]

@@ -383,25 +383,17 @@ class Pipeline:
         alignment span and the span the best anchor chain implies (its first anchor
         minus 3x the residues before it, its last plus 3x the residues after it), plus
         margin + rel * span on both sides (at least 3 nt, within the window)."""
-        jobs = self.cand["jobs"][keep].copy()
-        nl = jobs["nl"].astype(np.int64)
-        al = jobs["al"].astype(np.int64)
-        ps = np.clip(out[keep, 1], 0.0, 1.0) * nl
-        pe = np.clip(out[keep, 2], 0.0, 1.0) * nl
-        lo, hi = np.minimum(ps, pe), np.maximum(ps, pe)
-        if chain is not None:
-            c = chain[keep].astype(np.int64)
-            has = c[:, 0] >= 0
-            lo = np.where(has, np.minimum(lo, c[:, 0] - 3 * c[:, 2] - 2), lo)
-            hi = np.where(has, np.maximum(hi, c[:, 1] + 3 * (al - 1 - c[:, 3]) + 1), hi)
-        pad = margin + rel * (hi - lo)
-        s = np.clip(np.floor(lo - pad), 0, nl).astype(np.int64)
-        e = np.clip(np.ceil(hi + pad), 0, nl).astype(np.int64)
-        short = e - s < 3
-        s[short], e[short] = 0, nl[short]
-        jobs["nt_off"] += s
-        jobs["nl"] = (e - s).astype(np.int32)
-        return jobs
+        jobs = np.ascontiguousarray(self.cand["jobs"][keep])
+        n = len(jobs)
+        o = np.ascontiguousarray(out[keep, :3], np.float32)
+        ch = np.ascontiguousarray(chain[keep], np.int32) if chain is not None else None
+        k = np.zeros(max(n, 1), np.uint8)
+        tight = np.zeros(n, JOB_DTYPE)
+        if n and not L.load().pl_pf_decide(n, jobs.ctypes.data, o.ctypes.data, 3,
+                                           ch.ctypes.data if ch is not None else None, 0.0, int(margin), float(rel),
+                                           1.0, k.ctypes.data, None, tight.ctypes.data):
+            raise RuntimeError("pl_pf_decide: " + L.error())
+        return tight
 
     def learned(self, model: PrefilterModel, tau: float, margin: int, rel: float = 0.0, tau_fb: float = 0.0):
         """The learned path: (output mask over all candidates, stats).  Candidates with
@@ -410,21 +402,36 @@ class Pipeline:
         then runs per protein over the candidates that were aligned."""
         import torch
         t0 = time.perf_counter()
-        feats, chain = self.features()
-        out = model.predict(feats, self.n)
-        o = out[: self.n, :3].cpu().numpy()
-        ch = chain[: self.n].cpu().numpy()
+        if rel == 0.0:  # features, MLP and the decision in one C call (pl_pf_select_device)
+            n = self.n
+            k = np.zeros(n, np.uint8)
+            fbk = np.zeros(n, np.uint8)
+            tight = np.zeros(n, JOB_DTYPE)
+            stream = torch.cuda.current_stream().cuda_stream
+            if not self.eng.lib.pl_pf_select_device(model.h, self.eng.h, self.opt.ptr, self.cand["jobs"].ctypes.data,
+                                                    n, self.d_nt.data_ptr(), self.d_aa.data_ptr(), float(tau),
+                                                    int(margin), float(tau_fb), k.ctypes.data, fbk.ctypes.data,
+                                                    tight.ctypes.data, None, stream):
+                raise RuntimeError("pl_pf_select_device: " + L.error())
+            keep = np.nonzero(k)[0]
+            jobs = tight[keep]
+            fb_mask = fbk.astype(bool)
+        else:
+            feats, chain = self.features()
+            out = model.predict(feats, self.n)
+            o = out[: self.n, :3].cpu().numpy()
+            ch = chain[: self.n].cpu().numpy()
+            z = o[:, 0]
+            keep = np.nonzero(z >= _logit(tau))[0]
+            jobs = self.tightened(keep, o, ch, margin, rel)
+            fb_mask = z >= _logit(tau_fb)
         t1 = time.perf_counter()
-        z = o[:, 0]
-        keep = np.nonzero(z >= _logit(tau))[0]
-        jobs = self.tightened(keep, o, ch, margin, rel)
         self._use(self.tune_learned)
         sc, qs, qe = self.dp(jobs, spans=True)
         t2 = time.perf_counter()
         bad = sc <= 0
         fail = keep[bad]
-        fb = z[fail] >= _logit(tau_fb)
-        fail = fail[fb]
+        fail = fail[fb_mask[fail]]
         self._use(self.tune_plain)
         sc2, qs2, qe2 = self.dp(self.cand["jobs"][fail], spans=True)
         torch.cuda.synchronize()

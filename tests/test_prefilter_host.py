@@ -137,3 +137,25 @@ def test_loci_reported_needs_a_candidate_on_the_gene():
     prot = np.repeat([0, 1], 4)
     out = np.array([False, False, True, False, False, False, False, True])
     assert P.loci_reported(out, prot, kind, 2).tolist() == [True, False]
+
+
+def test_decision_thresholds_in_c():
+    """pl_pf_decide keeps logit >= logit(tau) and marks fallback at logit >= logit(tau_fb)."""
+    from protlocus_b200 import lib as L
+    jobs = np.zeros(4, P.JOB_DTYPE)
+    jobs["nt_off"] = [0, 100, 200, 300]
+    jobs["nl"] = [90, 90, 90, 90]
+    jobs["al"] = [10, 10, 10, 10]
+    z = np.array([P._logit(0.2) - 1e-3, P._logit(0.2), P._logit(0.9), 5.0], np.float32)
+    out = np.zeros((4, 3), np.float32)
+    out[:, 0], out[:, 1], out[:, 2] = z, 0.1, 0.9
+    keep = np.zeros(4, np.uint8)
+    fb = np.zeros(4, np.uint8)
+    tight = np.zeros(4, P.JOB_DTYPE)
+    assert L.load().pl_pf_decide(4, jobs.ctypes.data, out.ctypes.data, 3, None, 0.2, 5, 0.0, 0.9, keep.ctypes.data,
+                                 fb.ctypes.data, tight.ctypes.data)
+    # float32 rounding of the logits decides the borderline case exactly as the comparison in C does
+    assert keep.tolist() == [int(np.float64(x) >= P._logit(0.2)) for x in z]
+    assert fb.tolist() == [int(np.float64(x) >= P._logit(0.9)) for x in z]
+    assert tight["nt_off"][3] == 300 + 4 and tight["nl"][3] == 81 + 5 - 4   # [9 - 5, 81 + 5] of 90
+    assert tight["nt_off"][0] == 0 and tight["nl"][0] == 90                 # dropped: copied unchanged
