@@ -401,22 +401,28 @@ def main():
     peak = max(int32_peak, i16x2_peak)
 
     clocks = Clocks(local)
-    eng.set_timing(True)
     launches0 = L.load().pl_kernel_launch_count()
+    replays0 = int(eng.lib.pl_engine_graph_replays(eng.h))
     barrier()
     torch.cuda.synchronize()
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
-        step_device()
+        step_device()  # a repeated batch: replayed from the engine's captured graph
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
     launches = L.load().pl_kernel_launch_count() - launches0
+    replays = int(eng.lib.pl_engine_graph_replays(eng.h)) - replays0
     t = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
     value = cells_all * args.steps / t / 1e9
+    # the phase times of the roofline: the same steps again with the engine's CUDA events between the launches
+    eng.set_timing(True)
+    for _ in range(max(1, min(args.steps, 3))):
+        step_device()
+    torch.cuda.synchronize()
     tm = eng.times()
     plan = eng.last_plan()
     dp_s = tm["dp_ms"] / 1e3
@@ -500,7 +506,8 @@ def main():
             "config": {"workload": WORKLOAD if not args.uniform else "profiling case " + args.uniform, "n_jobs": n, "cells_per_step": cells, "seed": "1+rank",
                        "l2": "inputs and the per-step traceback arena (tens of GB) are far larger than L2",
                        "waves": plan["waves"], "coop_jobs": plan["coop"], "parallelism": f"{world} independent ranks",
-                       "tuning": tuning},
+                       "tuning": tuning, "int16x2_pairs": eng.last_pairs(),
+                       "graph_replays_in_timed_steps": replays},
             "e2e": e2e,
             "gpu_launches": int(launches),
             "roofline": {"bound": "int", "kernel": "k_splice_dp", "achieved": achieved, "peak": peak,
@@ -512,7 +519,9 @@ def main():
                          "ops_per_cell": OPS_PER_CELL, "dp_kernel_gcups": round(dp_gcups, 3),
                          "peak_source": "measured live: pl_measure_int_peak (int32 %.3g, int16x2 %.3g lane-ops/s)"
                                         % (int32_peak, i16x2_peak),
-                         "phase_ms_per_step": {k: round(v / args.steps, 2) for k, v in tm.items() if k.endswith("_ms")}},
+                         "phase_ms_per_step": {k: round(v / max(1, min(args.steps, 3)), 2) for k, v in tm.items()
+                                               if k.endswith("_ms")},
+                         "phase_source": "engine CUDA events over separate steps after the timed region"},
             "cpu_baseline": cpu,
             "clocks": clk,
             "prefilter": pf,

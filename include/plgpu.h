@@ -228,6 +228,14 @@ void pl_engine_last_plan(const pl_engine_t *e, int32_t *n_waves, int32_t *n_coop
  * the same either way.  pl_engine_last_pairs: pairs formed in the last batch. */
 void pl_engine_set_pairing(pl_engine_t *e, int32_t enable);
 int32_t pl_engine_last_pairs(const pl_engine_t *e);
+/* A batch whose launch plan has the same shape as the previous batch's (the same
+ * job count, waves, launch groups, buffers and options: a repeated batch, or one
+ * batch size fed again and again) is captured into a CUDA graph and, while the
+ * shape recurs, replayed from it; untimed calls only (on by default;
+ * PLGPU_GRAPHS=0 or pl_engine_set_graphs(e, 0) turns it off).
+ * pl_engine_graph_replays: batches launched from a captured graph so far. */
+void pl_engine_set_graphs(pl_engine_t *e, int32_t enable);
+int64_t pl_engine_graph_replays(const pl_engine_t *e);
 
 /* ---------------------------------------------------------------------------
  * Several GPUs for one batch (no counterpart in the reference, whose queue

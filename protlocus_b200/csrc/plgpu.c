@@ -154,8 +154,9 @@ PL_EXPORT pl_engine_t *pl_engine_create(int32_t device, int64_t trace_budget_byt
 	e->coop_ratio = pl_coop_ratio();
 	e->r4_rows = pl_r4_rows();
 	{
-		const char *v = getenv("PLGPU_PAIR");
+		const char *v = getenv("PLGPU_PAIR"), *g = getenv("PLGPU_GRAPHS");
 		e->pairing = !(v && *v && atoi(v) == 0);
+		e->graphs = !(g && *g && atoi(g) == 0);
 	}
 	CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
 	CK(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
@@ -181,6 +182,7 @@ PL_EXPORT void pl_engine_destroy(pl_engine_t *e)
 {
 	if (!e) return;
 	cudaSetDevice(e->device);
+	if (e->g_exec) cudaGraphExecDestroy(e->g_exec);
 	dbuf_free(&e->jobs), dbuf_free(&e->order), dbuf_free(&e->counters), dbuf_free(&e->prep);
 	dbuf_free(&e->trace), dbuf_free(&e->ring), dbuf_free(&e->tmp), dbuf_free(&e->total);
 	dbuf_free(&e->nt), dbuf_free(&e->aa), dbuf_free(&e->ss), dbuf_free(&e->res), dbuf_free(&e->cig);
@@ -418,6 +420,39 @@ static int32_t pl_form_pairs(pl_engine_t *e, const ns_opt_t *opt, int32_t n, int
 	return n_pairs;
 }
 
+/* FNV-1a of the launch sequence's shape: sizes, buffers, parameters and, per position of
+ * the order array, the wave / launch group / rows / cooperative flag of its job */
+static uint64_t pl_fnv(uint64_t h, const void *p, size_t n)
+{
+	const unsigned char *b = (const unsigned char*)p;
+	size_t i;
+	for (i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+	return h;
+}
+
+static int pl_group_of(const plk_job_t *J);
+
+static uint64_t pl_plan_key(const pl_engine_t *e, int32_t n, int32_t n_waves, int32_t two, int64_t arena_words,
+		int64_t ring_ints, int32_t max_al, const void *nt, const void *aa, const void *ss, const void *res,
+		const void *cig, int64_t cig_cap, cudaStream_t st, const plk_params_t *P)
+{
+	uint64_t h = 1469598103934665603ull;
+	const void *ptr[14];
+	int64_t v[7];
+	int32_t i;
+	v[0] = n, v[1] = n_waves, v[2] = two, v[3] = arena_words, v[4] = ring_ints, v[5] = max_al, v[6] = cig_cap;
+	ptr[0] = nt, ptr[1] = aa, ptr[2] = ss, ptr[3] = res, ptr[4] = cig, ptr[5] = (const void*)st, ptr[6] = e->jobs.p;
+	ptr[7] = e->order.p, ptr[8] = e->counters.p, ptr[9] = e->prep.p, ptr[10] = e->trace.p, ptr[11] = e->ring.p;
+	ptr[12] = e->tmp.p, ptr[13] = e->total.p;
+	h = pl_fnv(h, v, sizeof(v)), h = pl_fnv(h, ptr, sizeof(ptr)), h = pl_fnv(h, P, sizeof(*P));
+	for (i = 0; i < n; ++i) {
+		const plk_job_t *J = &e->hj[e->horder[i]];
+		const int32_t t = e->hwave[e->horder[i]] << 8 | pl_group_of(J) << 4 | J->rows << 1 | (J->nw > 1);
+		h = pl_fnv(h, &t, sizeof(t));
+	}
+	return h ? h : 1;
+}
+
 /* Runs the whole batch on `st`.  Inputs (nt/aa/ss) and outputs (res/cig) are device pointers. */
 static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jobs, int32_t n,
 		const uint8_t *nt, const uint8_t *aa, const uint8_t *ss, pl_splice_result_t *res_dev,
@@ -428,7 +463,8 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 	int64_t prep_total = 0, tmp_total = 0, trace_total = 0, max_trace = 0, slots, arena_budget, arena_words = 0;
 	int64_t ring_ints = 0;
 	int64_t *wave_bytes = 0, *wave_cells = 0, total_words = 0;
-	int ok = 0;
+	int ok = 0, capturing = 0;
+	uint64_t g_launch0 = 0, g_key = 0;
 
 	e->last_waves = e->last_coop = e->last_dp_launches = e->last_pairs = 0;
 	if (n <= 0) { if (total_out) *total_out = 0; return 1; }
@@ -556,6 +592,32 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 	CK(cudaMemcpyAsync(e->jobs.p, e->hj, sizeof(plk_job_t) * (size_t)n, cudaMemcpyHostToDevice, st));
 	CK(cudaMemcpyAsync(e->order.p, e->horder, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
 	e->n_ev = 0;
+	{ /* Graph replay: the launches below depend only on the plan's shape (the groups of the
+	   * order array, the waves, the buffers and the parameters), not on the job table's
+	   * contents, which the copies above refresh.  A shape seen on the previous call is
+	   * captured into a CUDA graph on this one and replayed while it recurs (timed runs
+	   * launch directly: their events sit between the launches). */
+		const uint64_t key = pl_plan_key(e, n, n_waves, two, arena_words, ring_ints, max_al, nt, aa, ss, res_dev,
+				cig_dev, cig_cap, st, &P);
+		const int use = e->graphs && !e->timing;
+		if (use && e->g_exec && key == e->g_key) {
+			CK(cudaGraphLaunch(e->g_exec, st));
+			plk_add_launches((uint64_t)e->g_nlaunch);
+			e->last_dp_launches = e->g_dp_launches, wave_n_coop = e->g_coop;
+			++e->g_replays;
+			goto launched;
+		}
+		capturing = use && key == e->g_prev_key;
+		e->g_prev_key = key;
+		if (capturing) {
+			g_launch0 = plk_launches();
+			if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+				cudaGetLastError();  /* a stream that cannot be captured (the legacy stream): launch directly */
+				capturing = 0;
+			}
+			g_key = key;
+		}
+	}
 	PL_TIME(e, st, 0);
 	CKK(plk_prep((const plk_job_t*)e->jobs.p, n, nt, aa, ss, (uint8_t*)e->prep.p, &P, st));
 	PL_TIME(e, st, 0);
@@ -606,6 +668,21 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 	CKK(plk_scan_compact((plk_job_t*)e->jobs.p, n, (const uint32_t*)e->tmp.p, cig_dev, cig_cap,
 			(int64_t*)e->total.p, res_dev, st));
 	PL_TIME(e, st, 3);
+	if (capturing) {
+		cudaGraph_t g = 0;
+		capturing = 0;
+		CK(cudaStreamEndCapture(st, &g));
+		if (e->g_exec) cudaGraphExecDestroy(e->g_exec), e->g_exec = 0;
+		{
+			const cudaError_t ie = cudaGraphInstantiate(&e->g_exec, g, 0);
+			cudaGraphDestroy(g);
+			CK(ie);
+		}
+		e->g_key = g_key, e->g_nlaunch = (int64_t)(plk_launches() - g_launch0);
+		e->g_dp_launches = e->last_dp_launches, e->g_coop = wave_n_coop;
+		CK(cudaGraphLaunch(e->g_exec, st));
+	}
+launched:
 	CK(cudaMemcpyAsync(&total_words, e->total.p, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
 	CK(cudaStreamSynchronize(st));
 	if (total_out) *total_out = total_words;
@@ -637,11 +714,22 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 	}
 	ok = 1;
 fail:
+	if (capturing) { /* a launch failed during the capture: end it, keep the stream usable */
+		cudaGraph_t g = 0;
+		cudaStreamEndCapture(st, &g);
+		if (g) cudaGraphDestroy(g);
+		cudaGetLastError();
+		e->g_prev_key = 0;
+	}
 	free(wave_bytes), free(wave_cells);
 	return ok;
 }
 
 PL_EXPORT int32_t pl_engine_last_pairs(const pl_engine_t *e) { return e ? e->last_pairs : 0; }
+
+PL_EXPORT void pl_engine_set_graphs(pl_engine_t *e, int32_t enable) { if (e) e->graphs = enable != 0; }
+
+PL_EXPORT int64_t pl_engine_graph_replays(const pl_engine_t *e) { return e ? e->g_replays : 0; }
 
 PL_EXPORT void pl_engine_set_pairing(pl_engine_t *e, int32_t enable) { if (e) e->pairing = enable != 0; }
 

@@ -30,6 +30,11 @@ void dbuf_free(dbuf_t *b);
 struct pl_engine_s {
 	int device, n_sm, ctas_per_sm[4][2];   /* per DP mode (3: paired int16x2), per rows per lane (8, 4) */
 	int pairing;                            /* form int16x2 pairs (PLGPU_PAIR=0 turns it off) */
+	int graphs;                             /* capture and replay recurring launch plans (PLGPU_GRAPHS=0: off) */
+	uint64_t g_key, g_prev_key;             /* shape of the captured plan, of the previous call's plan */
+	cudaGraphExec_t g_exec;
+	int64_t g_nlaunch, g_replays;           /* kernel launches in the graph; replays so far */
+	int32_t g_dp_launches, g_coop;
 	int32_t r4_rows;                        /* jobs with at most this many DP rows take 4 rows per lane */
 	double coop_ratio;                      /* cooperative-job threshold (pl_coop_ratio by default) */
 	cudaStream_t stream;

@@ -137,6 +137,9 @@ def load() -> C.CDLL:
     lib.pl_engine_last_pairs.argtypes = [C.c_void_p]
     lib.pl_engine_last_pairs.restype = C.c_int32
     lib.pl_engine_set_pairing.argtypes = [C.c_void_p, C.c_int32]
+    lib.pl_engine_set_graphs.argtypes = [C.c_void_p, C.c_int32]
+    lib.pl_engine_graph_replays.argtypes = [C.c_void_p]
+    lib.pl_engine_graph_replays.restype = C.c_int64
     lib.pl_group_create.argtypes = [C.c_void_p, C.c_int32, C.c_int64]
     lib.pl_group_create.restype = C.c_void_p
     lib.pl_group_destroy.argtypes = [C.c_void_p]

@@ -409,3 +409,21 @@ def test_pairs_not_formed_outside_the_15_bit_range(engine, oracle):
     pairs = _paired_batch(rng, 40, max_al=40)
     _check(engine, oracle, opt, pairs)
     assert engine.last_pairs() == 0
+
+
+def test_graph_replay_bit_exact(oracle):
+    """A batch fed again and again: the second call captures the launch plan into a CUDA graph,
+    later calls replay it; every call's results equal the oracle's, and with graphs off too."""
+    rng = np.random.default_rng(25)
+    opt = Options(flag=NS_F_CIGAR)
+    pairs = _paired_batch(rng, 40, max_al=60) + [W.random_pair(rng, max_al=60) for _ in range(30)]
+    eng = L.Engine(0)
+    try:
+        r0 = int(eng.lib.pl_engine_graph_replays(eng.h))
+        outs = [_check(eng, oracle, opt, pairs) for _ in range(4)]
+        assert int(eng.lib.pl_engine_graph_replays(eng.h)) - r0 >= 2
+        eng.lib.pl_engine_set_graphs(eng.h, 0)
+        outs.append(_check(eng, oracle, opt, pairs))
+        assert all(o == outs[0] for o in outs)
+    finally:
+        eng.close()
