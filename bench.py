@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--no-refgpu", action="store_true",
                     help="leave the reference's own CUDA global DP (timed in a child process) out of the headline")
     ap.add_argument("--ref-jobs", type=int, default=256, help="jobs of the reference GPU queue sample (--workload refgpu)")
+    ap.add_argument("--tuning-json", default=None,
+                    help="per-shape-class tuning file (default: $PLGPU_TUNING_JSON or ~/.cache/protlocus_b200/tuning.json)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the engine's default tuning instead of autotuning it on the workload (global DP)")
     ap.add_argument("--workload", default="global",
@@ -384,11 +386,25 @@ def main():
 
     tuning = {"r4_rows": None, "coop_ratio": None, "autotuned": False}
     if not args.no_autotune:
-        r4, ratio = C.c_int32(), C.c_double()
-        if not eng.lib.pl_engine_autotune(eng.h, opt.ptr, tab, n, d_nt.data_ptr(), d_aa.data_ptr(), None,
-                                          C.byref(r4), C.byref(ratio)):
-            raise RuntimeError("pl_engine_autotune: " + L.error())
-        tuning = {"r4_rows": r4.value, "coop_ratio": ratio.value, "autotuned": True}
+        from protlocus_b200 import tuning as TU
+        tf = TU.TuningFile(args.tuning_json)
+        klass = TU.shape_class(nl, al)
+        hit = tf.get(klass)
+        if hit is not None:  # this shape class was tuned before: no search
+            eng.set_tuning(hit["r4_rows"], hit["coop_ratio"])
+            tuning = {**hit, "autotuned": False, "shape_class": klass, "from": tf.path}
+        else:
+            r4, ratio = C.c_int32(), C.c_double()
+            if not eng.lib.pl_engine_autotune(eng.h, opt.ptr, tab, n, d_nt.data_ptr(), d_aa.data_ptr(), None,
+                                              C.byref(r4), C.byref(ratio)):
+                raise RuntimeError("pl_engine_autotune: " + L.error())
+            tuning = {"r4_rows": r4.value, "coop_ratio": ratio.value, "autotuned": True, "shape_class": klass}
+            try:
+                tf.put(klass, r4.value, ratio.value, jobs=int(n), device=torch.cuda.get_device_name(local))
+                tf.save()
+                tuning["saved_to"] = tf.path
+            except OSError:
+                pass
     else:
         tuning.update(eng.tuning())
     for _ in range(args.warmup):
