@@ -854,6 +854,7 @@ def run_reference_hmm(args):
 
 def main_hmm(args):
     import torch
+    from protlocus_b200 import hmm as H
     R = Ranks("nccl")
     rank, world, local, barrier, max_over_ranks = R.rank, R.world, R.local, R.barrier, R.max
 

@@ -505,13 +505,14 @@ k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop
 /*
  * Two jobs with one protein and windows of one length -- the two strands of a
  * locus -- run in the two 16-bit halves of every 32-bit register, so one DPX
- * instruction (__viaddmax_u16x2: max(a + b, c); __vimax3_u16x2) updates the same
+ * instruction (__viaddmax_s16x2: max(a + b, c); __vimax3_s16x2) updates the same
  * cell of both.  Values live in a biased 15-bit domain per half: v -> v + B, with
  * the reference's saturation floor (-32768) mapped to F.  The host admits a pair
  * only when every value the DP can reach provably stays within [F + 512,
  * 0x7fff - 512] after biasing: the 16-bit adds then never wrap, values at the
  * floor never meet real ones, and every clamp at F is exactly the reference's
- * _mm_subs_epi16 saturation.
+ * _mm_subs_epi16 saturation.  Every value, and every sum formed on the way, lies in
+ * [0, 0x7fff] per half, so the signed 16-bit forms order them as unsigned numbers.
  *
  * The first-winning candidate cannot ride in the low bits of the value as in the
  * 32-bit kernel.  Each cell stores ten bits "candidate k is below the maximum"
@@ -544,7 +545,7 @@ __device__ __forceinline__ unsigned sign_pairs(unsigned x, unsigned y)
 }
 __device__ __forceinline__ unsigned sel_bits(unsigned a, unsigned b, unsigned m) { return (a & m) | (b & ~m); }
 /* per-half unsigned maximum of two, as one add+max instruction (there is no two-input form) */
-__device__ __forceinline__ unsigned vmax2u(unsigned a, unsigned b) { return __viaddmax_u16x2(a, 0u, b); }
+__device__ __forceinline__ unsigned vmax2u(unsigned a, unsigned b) { return __viaddmax_s16x2(a, 0u, b); }
 
 struct PairK { unsigned F2, GOn, GEn, IOn, FSn, FSp, GOEn; };
 
@@ -563,35 +564,35 @@ __device__ __forceinline__ void cells_pair(const unsigned (&in)[9], unsigned (&h
 		unsigned h3m1 = r >= 3 ? hm[r - 3] : (r == 2 ? ah1 : (r == 1 ? ah2 : ah3));
 		if (r == 0 && row2) h1m1 = r2f, h2m1 = r2f, h3m1 = r2h; /* column -1 while row 2 is computed: {0, -fs, -fs} */
 		/* 1: I -- g4 = H'(c-1) - go >= I(c-1) */
-		const unsigned t4 = __viaddmax_u16x2(lh[r], K.GOn, K.F2);
+		const unsigned t4 = __viaddmax_s16x2(lh[r], K.GOn, K.F2);
 		const unsigned g4 = t4 + 0x80008000u - ip[r];
-		const unsigned ipn = __viaddmax_u16x2(vmax2u(t4, ip[r]), K.GEn, K.F2);
+		const unsigned ipn = __viaddmax_s16x2(vmax2u(t4, ip[r]), K.GEn, K.F2);
 		ip[r] = ipn;
 		/* 2: D -- g5 = H(i-3) - go >= D(i-3) */
-		const unsigned u5 = __viaddmax_u16x2(h3, K.GOn, K.F2);
+		const unsigned u5 = __viaddmax_s16x2(h3, K.GOn, K.F2);
 		const unsigned g5 = u5 + 0x80008000u - d3;
-		const unsigned dnew = __viaddmax_u16x2(vmax2u(u5, d3), gi[r], K.F2);
+		const unsigned dnew = __viaddmax_s16x2(vmax2u(u5, d3), gi[r], K.F2);
 		/* 3-5: phase-0/1/2 introns */
-		const unsigned ua = __viaddmax_u16x2(h1, K.IOn, K.F2);
-		const unsigned t6 = __viaddmax_u16x2(ua, dn[r], K.F2);
+		const unsigned ua = __viaddmax_s16x2(h1, K.IOn, K.F2);
+		const unsigned t6 = __viaddmax_s16x2(ua, dn[r], K.F2);
 		const unsigned g6 = t6 + 0x80008000u - va;
 		const unsigned anew = vmax2u(t6, va);
-		const unsigned ub = __viaddmax_u16x2(h1m1, K.IOn, K.F2);
-		const unsigned t7 = __viaddmax_u16x2(ub, dn[r + 1], K.F2);
+		const unsigned ub = __viaddmax_s16x2(h1m1, K.IOn, K.F2);
+		const unsigned t7 = __viaddmax_s16x2(ub, dn[r + 1], K.F2);
 		const unsigned g7 = t7 + 0x80008000u - vb;
 		const unsigned bnew = vmax2u(t7, vb);
-		const unsigned t8 = __viaddmax_u16x2(ub, dn[r + 2], K.F2);
+		const unsigned t8 = __viaddmax_s16x2(ub, dn[r + 2], K.F2);
 		const unsigned g8 = t8 + 0x80008000u - vc;
 		const unsigned cnew = vmax2u(t8, vc);
 		/* candidates 0-5 (floored at F, where none of them can win), 6-9 folded */
-		const unsigned c0 = __viaddmax_u16x2(h3m1, srow[cp[r]], K.F2);  /* H(i-3,j-1) + s(i,j) */
-		const unsigned c3 = __viaddmax_u16x2(anew, ac[r + 2], K.F2);    /* A - a(i) */
-		const unsigned c4 = __viaddmax_u16x2(bnew, ac[r], K.F2);        /* B - a(i-2) */
-		const unsigned c5 = __viaddmax_u16x2(cnew, ac[r + 1], K.F2);    /* C - a(i-1) */
-		unsigned he = __vimax3_u16x2(c0, ipn, dnew);
-		he = __vimax3_u16x2(he, c3, c4);
-		const unsigned fsm = vmax2u(__vimax3_u16x2(h1, h2, h1m1), h2m1);
-		he = __viaddmax_u16x2(fsm, K.FSn, vmax2u(he, c5));     /* 6-9: H(i-1|i-2, j|j-1) - fs */
+		const unsigned c0 = __viaddmax_s16x2(h3m1, srow[cp[r]], K.F2);  /* H(i-3,j-1) + s(i,j) */
+		const unsigned c3 = __viaddmax_s16x2(anew, ac[r + 2], K.F2);    /* A - a(i) */
+		const unsigned c4 = __viaddmax_s16x2(bnew, ac[r], K.F2);        /* B - a(i-2) */
+		const unsigned c5 = __viaddmax_s16x2(cnew, ac[r + 1], K.F2);    /* C - a(i-1) */
+		unsigned he = __vimax3_s16x2(c0, ipn, dnew);
+		he = __vimax3_s16x2(he, c3, c4);
+		const unsigned fsm = vmax2u(__vimax3_s16x2(h1, h2, h1m1), h2m1);
+		he = __viaddmax_s16x2(fsm, K.FSn, vmax2u(he, c5));     /* 6-9: H(i-1|i-2, j|j-1) - fs */
 		/* s_k: candidate k < max, the bit 15 of max + 0x7fff - c_k (no borrow: c_k <= max) */
 		const unsigned m1 = he + 0x7fff7fffu;
 		const unsigned s0 = m1 - c0, s1 = m1 - ipn, s2 = m1 - dnew, s3 = m1 - c3, s4 = m1 - c4, s5 = m1 - c5;
@@ -723,13 +724,13 @@ __device__ __forceinline__ void dp_pair(plk_job_t *__restrict__ JA, plk_job_t *_
 			if (seg) {
 #pragma unroll
 				for (int r = 0; r < R; ++r) {
-					const unsigned hop = __viaddmax_u16x2(lh[r], K.GOEn, NEG), iext = __viaddmax_u16x2(ip[r], K.GEn, NEG);
-					ic[r] = __vimax3_u16x2(hop, iext, __viaddmax_u16x2(ic[r], K.GEn, NEG));
+					const unsigned hop = __viaddmax_s16x2(lh[r], K.GOEn, NEG), iext = __viaddmax_s16x2(ip[r], K.GEn, NEG);
+					ic[r] = __vimax3_s16x2(hop, iext, __viaddmax_s16x2(ic[r], K.GEn, NEG));
 					ip[r] = NEG, lh[r] = NEG;
 				}
 			} else {
 #pragma unroll
-				for (int r = 0; r < R; ++r) ic[r] = __viaddmax_u16x2(ic[r], K.GEn, NEG);
+				for (int r = 0; r < R; ++r) ic[r] = __viaddmax_s16x2(ic[r], K.GEn, NEG);
 			}
 			cells_pair<R>(in, hm, ah1, ah2, ah3, row2, r2h, r2f, srow, cp, gi, dn, ac, ip, lh, ic, K, o, z, hn);
 			const int64_t toff = (((int64_t)k * al + dcol) * NL + L) * R;
