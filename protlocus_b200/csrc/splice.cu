@@ -594,9 +594,9 @@ __device__ __forceinline__ void cells_pair(const unsigned (&in)[9], unsigned (&h
 		const unsigned fsm = vmax2u(__vimax3_s16x2(h1, h2, h1m1), h2m1);
 		he = __viaddmax_s16x2(fsm, K.FSn, vmax2u(he, c5));     /* 6-9: H(i-1|i-2, j|j-1) - fs */
 		/* s_k: candidate k < max, the bit 15 of max + 0x7fff - c_k (no borrow: c_k <= max) */
-		const unsigned m1 = he + 0x7fff7fffu;
+		const unsigned m1 = he + 0x7fff7fffu, m1f = m1 + K.FSp;  /* two-operand forms: the adder of the FMA pipe */
 		const unsigned s0 = m1 - c0, s1 = m1 - ipn, s2 = m1 - dnew, s3 = m1 - c3, s4 = m1 - c4, s5 = m1 - c5;
-		const unsigned s6 = m1 - h1 + K.FSp, s7 = m1 - h2 + K.FSp, s8 = m1 - h1m1 + K.FSp, s9 = m1 - h2m1 + K.FSp;
+		const unsigned s6 = m1f - h1, s7 = m1f - h2, s8 = m1f - h1m1, s9 = m1f - h2m1;
 		lh[r] = he;
 		/* the carried insertion: g9 = H' >= ic */
 		const unsigned g9 = he + 0x80008000u - ic[r];
