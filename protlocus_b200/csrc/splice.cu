@@ -544,7 +544,8 @@ __device__ __forceinline__ unsigned sign_pairs(unsigned x, unsigned y)
 	return d;
 }
 __device__ __forceinline__ unsigned sel_bits(unsigned a, unsigned b, unsigned m) { return (a & m) | (b & ~m); }
-/* per-half unsigned maximum of two, as one add+max instruction (there is no two-input form) */
+/* per-half maximum of two, as one add+max instruction (there is no two-input intrinsic; an
+ * inline max.s16x2 cost registers) */
 __device__ __forceinline__ unsigned vmax2u(unsigned a, unsigned b) { return __viaddmax_s16x2(a, 0u, b); }
 
 struct PairK { unsigned F2, GOn, GEn, IOn, FSn, FSp, GOEn; };
