@@ -577,6 +577,15 @@ int pl_extra_cal_host(pl_engine_t *e, int32_t go, int32_t ge, int32_t fs, int32_
 		const uint8_t *codon, const uint8_t *aa20, const pl_extra_job_t *jobs, int32_t n,
 		const uint32_t *cigar, int64_t n_cigar_words, const uint8_t *nt, int64_t l_nt, const uint8_t *aa, int64_t l_aa,
 		const int8_t *pssm, int64_t l_pssm, pl_extra_result_t *results, pl_feat_t *feats, int64_t n_feat_slots);
+/* Device-resident variant: cigar, nt, aa, pssm, results and feats are device
+ * pointers (the offsets of jobs index them as in the host call; the caller
+ * guarantees that every job's spans lie inside its buffers); the job table and the
+ * tables are host memory.  Work is issued on `stream` (NULL = the engine's) and the
+ * call returns when it has completed. */
+int pl_extra_cal_device(pl_engine_t *e, int32_t go, int32_t ge, int32_t fs, int32_t asize, const int8_t *mat,
+		const uint8_t *codon, const uint8_t *aa20, const pl_extra_job_t *jobs, int32_t n, const uint32_t *cigar,
+		const uint8_t *nt, const uint8_t *aa, const int8_t *pssm, pl_extra_result_t *results, pl_feat_t *feats,
+		void *stream);
 
 /* ---------------------------------------------------------------------------
  * Prescreen banded gapped alignment (prescreen.c:346-382, ps_gapped) of many
@@ -592,6 +601,11 @@ typedef struct {
 } pl_ps_job_t;
 int pl_ps_gapped_host(pl_engine_t *e, const pl_ps_job_t *jobs, int32_t n, const int8_t *pssm, int64_t l_pssm,
 		const uint8_t *orf, int64_t l_orf, int32_t go, int32_t ge, int32_t *scores);
+/* Device-resident variant: pssm, orf and scores are device pointers; the caller
+ * guarantees the spans and that every residue code is 0..21 (the host call checks
+ * both).  The job table is host memory; returns when the work has completed. */
+int pl_ps_gapped_device(pl_engine_t *e, const pl_ps_job_t *jobs, int32_t n, const int8_t *pssm, const uint8_t *orf,
+		int32_t go, int32_t ge, int32_t *scores, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Anchor chaining (chain.c:160-219, mp_chain) of many queries at once.  A

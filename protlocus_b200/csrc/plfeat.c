@@ -158,3 +158,99 @@ fail:
 	free(hj);
 	return ok;
 }
+
+/* ------------------------------------------------------------------ device-resident variants */
+
+PL_EXPORT int pl_extra_cal_device(pl_engine_t *e, int32_t go, int32_t ge, int32_t fs, int32_t asize, const int8_t *mat,
+		const uint8_t *codon, const uint8_t *aa20, const pl_extra_job_t *jobs, int32_t n, const uint32_t *cigar,
+		const uint8_t *nt, const uint8_t *aa, const int8_t *pssm, pl_extra_result_t *results, pl_feat_t *feats,
+		void *stream)
+{
+	plk_extra_args_t a;
+	cudaStream_t st;
+	int32_t q;
+	if (!e || !mat || !codon || !aa20 || asize <= 0 || asize > 32) { pl_set_error("extra: missing tables"); return 0; }
+	if (n <= 0) return 1;
+	for (q = 0; q < n; ++q) {
+		const pl_extra_job_t *J = &jobs[q];
+		if (J->n_cigar < 0 || J->cigar_off < 0 || J->nt_off < 0 || J->l_nt < 0 || J->aa_off < 0 || J->qe < J->qs ||
+				J->feat_off < 0 || J->feat_cap < 0 || (J->pssm_off >= 0 && !pssm)) {
+			pl_set_error("alignment %d: negative offsets or sizes", q);
+			return 0;
+		}
+	}
+	CK(cudaSetDevice(e->device));
+	st = stream ? (cudaStream_t)stream : e->stream;
+	if (!dbuf_ensure(&e->f_jobs, sizeof(plk_extra_job_t) * (size_t)n) || !dbuf_ensure(&e->f_mat, (size_t)asize * asize))
+		goto fail;
+	CK(cudaMemcpyAsync(e->f_jobs.p, jobs, sizeof(plk_extra_job_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+	CK(cudaMemcpyAsync(e->f_mat.p, mat, (size_t)asize * asize, cudaMemcpyHostToDevice, st));
+	memset(&a, 0, sizeof(a));
+	a.jobs = (const plk_extra_job_t*)e->f_jobs.p, a.n = n, a.cigar = cigar, a.nt = nt, a.aa = aa, a.pssm = pssm;
+	a.mat = (const int8_t*)e->f_mat.p, a.go = go, a.ge = ge, a.fs = fs, a.asize = asize;
+	memcpy(a.codon, codon, 64), memcpy(a.aa20, aa20, 256);
+	a.res = (plk_extra_res_t*)results, a.feat = (plk_feat_t*)feats;
+	e->n_ev = 0;
+	PL_TIME(e, st, 1);
+	CKK(plk_extra(&a, st));
+	PL_TIME(e, st, 1);
+	CK(cudaStreamSynchronize(st));  /* the job table is reused by the next call */
+	{
+		int64_t codons = 0;
+		for (q = 0; q < n; ++q) codons += jobs[q].qe - jobs[q].qs;
+		pl_feat_times(e, codons);
+	}
+	return 1;
+fail:
+	return 0;
+}
+
+PL_EXPORT int pl_ps_gapped_device(pl_engine_t *e, const pl_ps_job_t *jobs, int32_t n, const int8_t *pssm,
+		const uint8_t *orf, int32_t go, int32_t ge, int32_t *scores, void *stream)
+{
+	plk_ps_job_t *hj = 0;
+	plk_ps_args_t a;
+	cudaStream_t st;
+	int64_t scr = 0, cells = 0;
+	int32_t q;
+	int ok = 0;
+	if (!e) { pl_set_error("no engine"); return 0; }
+	if (n <= 0) return 1;
+	hj = (plk_ps_job_t*)malloc(sizeof(*hj) * (size_t)n);
+	if (!hj) { pl_set_error("out of host memory"); return 0; }
+	for (q = 0; q < n; ++q) {
+		const pl_ps_job_t *J = &jobs[q];
+		int32_t i;
+		if (J->L < 0 || J->n < 0 || J->pssm_off < 0 || J->orf_off < 0) {
+			pl_set_error("candidate %d: negative offsets or sizes", q);
+			goto fail;
+		}
+		hj[q].pssm_off = J->pssm_off, hj[q].orf_off = J->orf_off, hj[q].scratch_off = scr;
+		hj[q].L = J->L, hj[q].n = J->n, hj[q].diag = J->diag, hj[q].band = J->band;
+		scr += (int64_t)J->n + 1;
+		for (i = 0; i < J->L; ++i) {
+			int32_t lo = J->band > 0 ? i + J->diag - J->band : 0, hi = J->band > 0 ? i + J->diag + J->band : J->n - 1;
+			if (lo < 0) lo = 0;
+			if (hi > J->n - 1) hi = J->n - 1;
+			if (hi >= lo) cells += hi - lo + 1;
+		}
+	}
+	CK(cudaSetDevice(e->device));
+	st = stream ? (cudaStream_t)stream : e->stream;
+	if (!dbuf_ensure(&e->s_jobs, sizeof(*hj) * (size_t)n) || !dbuf_ensure(&e->s_scr, sizeof(int) * 2 * (size_t)(scr > 0 ? scr : 1)))
+		goto fail;
+	CK(cudaMemcpyAsync(e->s_jobs.p, hj, sizeof(*hj) * (size_t)n, cudaMemcpyHostToDevice, st));
+	memset(&a, 0, sizeof(a));
+	a.jobs = (const plk_ps_job_t*)e->s_jobs.p, a.n = n, a.pssm = pssm, a.orf = orf, a.go = go, a.ge = ge;
+	a.scratch = (int*)e->s_scr.p, a.score = scores;
+	e->n_ev = 0;
+	PL_TIME(e, st, 1);
+	CKK(plk_ps_gapped(&a, st));
+	PL_TIME(e, st, 1);
+	CK(cudaStreamSynchronize(st));  /* the job table and scratch are reused by the next call */
+	pl_feat_times(e, cells);
+	ok = 1;
+fail:
+	free(hj);
+	return ok;
+}

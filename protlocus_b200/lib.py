@@ -165,6 +165,13 @@ def load() -> C.CDLL:
     lib.pl_ps_gapped_host.argtypes = [C.c_void_p, C.POINTER(PsJob), C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
                                       C.c_int64, C.c_int32, C.c_int32, C.c_void_p]
     lib.pl_ps_gapped_host.restype = C.c_int
+    lib.pl_extra_cal_device.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.POINTER(ExtraJob), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.pl_extra_cal_device.restype = C.c_int
+    lib.pl_ps_gapped_device.argtypes = [C.c_void_p, C.POINTER(PsJob), C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                        C.c_int32, C.c_void_p, C.c_void_p]
+    lib.pl_ps_gapped_device.restype = C.c_int
     lib.pl_chain_host.argtypes = [C.c_void_p, C.POINTER(ChainOpt), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.pl_chain_host.restype = C.c_int
@@ -346,6 +353,32 @@ class Engine:
                                           pk["res"], pk["feats"], pk["n_feat"]):
             raise RuntimeError("pl_extra_cal_host: " + error())
         return pk
+
+    def extra_upload(self, pk):
+        """Device copies (torch tensors) of a packed batch's inputs and outputs, for extra_run_device."""
+        import torch
+        d = {k: torch.from_numpy(np.ascontiguousarray(pk[k])).to("cuda") for k in ("cig", "nt", "aa")}
+        d["pssm"] = torch.from_numpy(pk["pssm"]).to("cuda") if pk["pssm"] is not None else None
+        d["res"] = torch.zeros(max(pk["n"], 1) * C.sizeof(ExtraResult), dtype=torch.uint8, device="cuda")
+        d["feats"] = torch.zeros(max(pk["n_feat"], 1) * C.sizeof(Feat), dtype=torch.uint8, device="cuda")
+        return d
+
+    def extra_run_device(self, pk, d, go: int, ge: int, fs: int, mat, codon, aa20, stream=None):
+        """pl_extra_cal_device over a packed batch whose buffers are on the device (extra_upload)."""
+        m = np.ascontiguousarray(np.asarray(mat, np.int8))
+        cd = np.ascontiguousarray(np.asarray(codon, np.uint8))
+        a20 = np.ascontiguousarray(np.asarray(aa20, np.uint8))
+        if not self.lib.pl_extra_cal_device(self.h, go, ge, fs, 22, m.ctypes.data, cd.ctypes.data, a20.ctypes.data,
+                                            pk["jobs"], pk["n"], d["cig"].data_ptr(), d["nt"].data_ptr(),
+                                            d["aa"].data_ptr(), d["pssm"].data_ptr() if d["pssm"] is not None else None,
+                                            d["res"].data_ptr(), d["feats"].data_ptr(), stream):
+            raise RuntimeError("pl_extra_cal_device: " + error())
+
+    def ps_run_device(self, pk, d_pssm, d_orf, d_score, go: int = 11, ge: int = 1, stream=None):
+        """pl_ps_gapped_device: pssm / orf / score buffers already on the device (torch tensors)."""
+        if not self.lib.pl_ps_gapped_device(self.h, pk["jobs"], pk["n"], d_pssm.data_ptr(), d_orf.data_ptr(), go, ge,
+                                            d_score.data_ptr(), stream):
+            raise RuntimeError("pl_ps_gapped_device: " + error())
 
     def extra_cal(self, alns, go: int, ge: int, fs: int, mat, codon, aa20):
         """Alignment statistics and exon features on the device (see extra_pack).

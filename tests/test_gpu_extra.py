@@ -97,3 +97,27 @@ def test_extra_pssm_and_span_mismatch():
         _compare(alns, eng.extra_cal(alns, GO, GE, FS, MAT, CODON, AA20))
     finally:
         eng.close()
+
+
+@pytest.mark.gpu
+def test_extra_device_entry_equals_host_entry():
+    """pl_extra_cal_device on device-resident buffers gives the host entry point's records."""
+    import ctypes as C
+    from protlocus_b200.abi import ExtraResult, Feat
+    alns, rng = _alignments(9, n_planted=6, n_random=20)
+    for a in alns[::3]:
+        a["pssm"] = rng.integers(-6, 10, size=(a["qe"] - a["qs"], 22)).astype(np.int8)
+    eng = L.Engine(0)
+    try:
+        pk = eng.extra_run(eng.extra_pack(alns), GO, GE, FS, MAT, CODON, AA20)
+        d = eng.extra_upload(pk)
+        eng.extra_run_device(pk, d, GO, GE, FS, MAT, CODON, AA20)
+        res = (ExtraResult * max(pk["n"], 1)).from_buffer_copy(d["res"].cpu().numpy().tobytes())
+        feats = (Feat * max(pk["n_feat"], 1)).from_buffer_copy(d["feats"].cpu().numpy().tobytes())
+        assert bytes(res)[: C.sizeof(ExtraResult) * pk["n"]] == bytes(pk["res"])[: C.sizeof(ExtraResult) * pk["n"]]
+        for q in range(pk["n"]):
+            J, r = pk["jobs"][q], pk["res"][q]
+            for k in range(min(r.n_feat, J.feat_cap)):
+                assert bytes(feats[J.feat_off + k]) == bytes(pk["feats"][J.feat_off + k]), (q, k)
+    finally:
+        eng.close()

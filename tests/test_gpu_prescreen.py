@@ -60,3 +60,21 @@ def test_ps_gapped_matches_reference():
     assert len(bad) == 0, [(int(i), cands[i][0].shape[0], cands[i][1].size, cands[i][2], cands[i][3], int(got[i]),
                             int(want[i])) for i in bad[:5]]
     assert (want > 0).mean() > 0.5
+
+
+@pytest.mark.gpu
+def test_ps_gapped_device_entry_equals_host_entry():
+    """pl_ps_gapped_device on device-resident PSSMs and ORFs gives the host entry point's scores."""
+    import torch
+    cands = _cases(4, 400)
+    eng = L.Engine(0)
+    try:
+        pk = eng.ps_pack(cands)
+        want = eng.ps_run(pk).copy()
+        d_pssm = torch.from_numpy(pk["pssm"]).to("cuda")
+        d_orf = torch.from_numpy(pk["orf"]).to("cuda")
+        d_score = torch.zeros(max(pk["n"], 1), dtype=torch.int32, device="cuda")
+        eng.ps_run_device(pk, d_pssm, d_orf, d_score)
+        assert np.array_equal(d_score.cpu().numpy()[: pk["n"]], want)
+    finally:
+        eng.close()
