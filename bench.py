@@ -1427,12 +1427,14 @@ def _simple_line(metric, value, unit, args, world, ms, dtype, desc, e2e, launche
 
 
 def main_extra(args):
-    """One step = pl_extra_cal_host over the alignments of the batched global DP (4096 pairs x 2
-    strands): mp_extra_cal's counts and exon features for each, host buffers in and out."""
+    """One step = mp_extra_cal's counts and exon features over the alignments of the batched
+    global DP (4096 pairs x 2 strands).  `value` times pl_extra_cal_device on device-resident
+    CIGARs, bases and residues (CUDA events, a 256 MB buffer written between steps); `e2e`
+    times pl_extra_cal_host, host buffers in and out, on the wall clock."""
     import torch
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as O
-    from protlocus_b200.abi import BLOSUM62, make_tables
+    from protlocus_b200.abi import BLOSUM62, ExtraResult, make_tables
     R = Ranks("nccl")
     jobs = make_jobs(args, R.seed(1))
     nt, aa, nt_off, aa_off, nl, al, tab = pack(jobs)
@@ -1449,21 +1451,38 @@ def main_extra(args):
     pk = eng.extra_pack(alns)
     for _ in range(max(3, args.warmup)):
         eng.extra_run(pk, 11, 1, 23, mat, codon, aa20)
+    d = eng.extra_upload(pk)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > L2 (126 MB): written between steps
+    for _ in range(max(3, args.warmup)):
+        eng.extra_run_device(pk, d, 11, 1, 23, mat, codon, aa20, stream=stream.cuda_stream)
     clocks = Clocks(R.local)
     eng.set_timing(True)
     launches0 = L.load().pl_kernel_launch_count()
     R.barrier()
     torch.cuda.synchronize()
     clocks.start()
+    t = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.extra_run_device(pk, d, 11, 1, 23, mat, codon, aa20, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t += e0.elapsed_time(e1) / 1e3
+    t = R.max(t / args.steps)
+    clk = clocks.stop()
+    launches = L.load().pl_kernel_launch_count() - launches0
+    k_s = eng.times()["dp_ms"] / 1e3 / args.steps
+    R.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         eng.extra_run(pk, 11, 1, 23, mat, codon, aa20)
     te = R.max((time.perf_counter() - t0) / args.steps)
     res = [(pk["res"][q], None) for q in range(n)]
-    clk = clocks.stop()
-    launches = L.load().pl_kernel_launch_count() - launches0
-    k_s = eng.times()["dp_ms"] / 1e3 / args.steps
     bad = sum(1 for r, _ in res if not r.ok)
+    same = bytes(d["res"].cpu().numpy().tobytes())[: C.sizeof(ExtraResult) * n] == bytes(pk["res"])[: C.sizeof(ExtraResult) * n]
     n_all = R.sum(n)
     ncig = sum(len(a["cigar"]) for a in alns)
     nfeat = sum(r.n_feat for r, _ in res)
@@ -1480,16 +1499,19 @@ def main_extra(args):
         v = k / (time.perf_counter() - t1)
         cpu = {"value": round(v, 1), "unit": "alignments/s", "cores": 1, "kind": "reference",
                "sample": f"{k} alignments, align.c mp_extra_cal (compiled from the reference) called one by one"}
-        _simple_line("alignment statistics + exon features (mp_extra_cal) alignments/s at 1 B200", n_all / k_s,
-                     "alignments/s", args, R.world, k_s * 1e3, "int32",
+        _simple_line("alignment statistics + exon features (mp_extra_cal) alignments/s at 1 B200", n_all / t,
+                     "alignments/s", args, R.world, t * 1e3, "int32",
                      f"{n} global spliced alignments of the batched DP (4096 pairs x 2 strands), {ncig} CIGAR ops",
                      {"value": round(n_all / te, 1), "unit": "alignments/s", "ms_per_step": round(te * 1e3, 2),
                       "h2d_bytes_per_step": int(sum(len(a["nt4"]) + a["qe"] for a in alns) + 4 * ncig + 64 * n),
                       "d2h_bytes_per_step": int(40 * n + 56 * (ncig + 2 * n)), "api": "pl_extra_cal_host, wall clock"},
                      launches, {"bound": "hbm", "kernel": "k_extra", "achieved": alg / k_s / 1e9, "peak": peak,
                                 "unit": "GB/s", "frac": alg / k_s / 1e9 / peak, "traffic": None,
+                                "kernel_ms": round(k_s * 1e3, 4),
                                 "note": "algorithmic bytes: 4 B per aligned residue, 4 B per CIGAR op, the records"},
-                     cpu, clk, {"span_mismatches": bad, "features": nfeat})
+                     cpu, clk, {"span_mismatches": bad, "features": nfeat, "device_equals_host_records": same,
+                                "api": "pl_extra_cal_device (device-resident inputs and outputs)",
+                                "l2": "a 256 MB buffer is written between timed steps"})
     eng.close()
     R.close()
     return 0
@@ -1499,9 +1521,11 @@ PS_OPS_PER_CELL = 11  # int32 ops per banded cell (prescreen.c:368-378): add, 2 
 
 
 def main_prescreen(args):
-    """One step = pl_ps_gapped_host over 20,000 (profile, ORF, diagonal) candidates: PSSMs of
-    50-800 rows, ORFs of 100-1500 residues with a planted profile-favoured stretch on half of
-    them, band 32 (the default), host buffers in and out."""
+    """One step = the banded gapped alignment of 20,000 (profile, ORF, diagonal) candidates:
+    PSSMs of 50-800 rows, ORFs of 100-1500 residues with a planted profile-favoured stretch on
+    half of them, band 32 (the default).  `value` times pl_ps_gapped_device on device-resident
+    PSSMs and ORFs (CUDA events, a 256 MB buffer written between steps); `e2e` times
+    pl_ps_gapped_host, host buffers in and out, on the wall clock."""
     import torch
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as O
@@ -1525,22 +1549,41 @@ def main_prescreen(args):
     pk = eng.ps_pack(cands)
     for _ in range(max(3, args.warmup)):
         eng.ps_run(pk)
+    stream = torch.cuda.current_stream()
+    d_pssm = torch.from_numpy(pk["pssm"]).to("cuda")
+    d_orf = torch.from_numpy(pk["orf"]).to("cuda")
+    d_score = torch.zeros(max(n, 1), dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > L2 (126 MB): written between steps
+    for _ in range(max(3, args.warmup)):
+        eng.ps_run_device(pk, d_pssm, d_orf, d_score, stream=stream.cuda_stream)
     clocks = Clocks(R.local)
     eng.set_timing(True)
     launches0 = L.load().pl_kernel_launch_count()
     R.barrier()
     torch.cuda.synchronize()
     clocks.start()
-    t0 = time.perf_counter()
+    t = 0.0
     for _ in range(args.steps):
-        sc = eng.ps_run(pk)
-    te = R.max((time.perf_counter() - t0) / args.steps)
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.ps_run_device(pk, d_pssm, d_orf, d_score, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t += e0.elapsed_time(e1) / 1e3
+    t = R.max(t / args.steps)
     clk = clocks.stop()
     launches = L.load().pl_kernel_launch_count() - launches0
     tm = eng.times()
     k_s = tm["dp_ms"] / 1e3 / args.steps
     cells = tm["cells"] // args.steps
     cells_all = R.sum(cells)
+    R.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sc = eng.ps_run(pk)
+    te = R.max((time.perf_counter() - t0) / args.steps)
+    same = bool(np.array_equal(d_score.cpu().numpy()[:n], sc))
     int32_peak, _ = L.measure_int_peak(R.local)
     achieved = cells * PS_OPS_PER_CELL / k_s
     cpu = None
@@ -1554,17 +1597,20 @@ def main_prescreen(args):
                   for b_lo, b_hi in [(i + d - 32, i + d + 32) for i in range(p.shape[0])] if min(b_hi, o.size - 1) >= max(b_lo, 0))
         cpu = {"value": round(c_k / secs / 1e9, 4), "unit": "GCUPS", "cores": 1, "kind": "reference",
                "sample": f"{k} candidates, prescreen.c ps_gapped (compiled from the reference) called one by one"}
-        _simple_line("prescreen banded gapped alignment GCUPS at 1 B200", cells_all / k_s / 1e9, "GCUPS", args, R.world,
-                     k_s * 1e3, "int32",
+        _simple_line("prescreen banded gapped alignment GCUPS at 1 B200", cells_all / t / 1e9, "GCUPS", args, R.world,
+                     t * 1e3, "int32",
                      f"{n} profile x ORF candidates: PSSM 50-800 rows, ORF 100-1500 aa, band 32, half planted",
                      {"value": round(cells_all / te / 1e9, 3), "unit": "GCUPS", "ms_per_step": round(te * 1e3, 2),
                       "h2d_bytes_per_step": int(sum(p.size + o.size for p, o, _, _ in cands) + 24 * n),
                       "d2h_bytes_per_step": 4 * n, "api": "pl_ps_gapped_host, wall clock"},
                      launches, {"bound": "int", "kernel": "k_ps_gapped", "achieved": achieved, "peak": int32_peak,
                                 "unit": "lane-ops/s", "frac": achieved / int32_peak if int32_peak else None,
-                                "traffic": None, "ops_per_cell": PS_OPS_PER_CELL,
+                                "traffic": None, "ops_per_cell": PS_OPS_PER_CELL, "kernel_ms": round(k_s * 1e3, 4),
                                 "peak_source": "measured live: pl_measure_int_peak, int32"},
-                     cpu, clk, {"cells_per_step": int(cells), "positive_scores": int((sc > 0).sum())})
+                     cpu, clk, {"cells_per_step": int(cells), "positive_scores": int((sc > 0).sum()),
+                                "device_equals_host_scores": same,
+                                "api": "pl_ps_gapped_device (device-resident PSSMs, ORFs and scores)",
+                                "l2": "a 256 MB buffer is written between timed steps"})
     eng.close()
     R.close()
     return 0
