@@ -441,6 +441,7 @@ def main():
     torch.cuda.synchronize()
     tm = eng.times()
     plan = eng.last_plan()
+    n_pairs = eng.last_pairs()
     dp_s = tm["dp_ms"] / 1e3
     achieved = tm["cells"] * OPS_PER_CELL / dp_s if dp_s > 0 else 0.0
     dp_gcups = tm["cells"] / dp_s / 1e9 if dp_s > 0 else 0.0
@@ -522,7 +523,7 @@ def main():
             "config": {"workload": WORKLOAD if not args.uniform else "profiling case " + args.uniform, "n_jobs": n, "cells_per_step": cells, "seed": "1+rank",
                        "l2": "inputs and the per-step traceback arena (tens of GB) are far larger than L2",
                        "waves": plan["waves"], "coop_jobs": plan["coop"], "parallelism": f"{world} independent ranks",
-                       "tuning": tuning, "int16x2_pairs": eng.last_pairs(),
+                       "tuning": tuning, "int16x2_pairs": n_pairs,
                        "graph_replays_in_timed_steps": replays},
             "e2e": e2e,
             "gpu_launches": int(launches),

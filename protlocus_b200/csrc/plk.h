@@ -36,6 +36,9 @@ typedef struct {
 	/* the paired int16x2 DP (mode 3): bias B of its 15-bit domain and the floor F that
 	 * stands for the reference's -32768 (set by the host when it forms pairs) */
 	int32_t pair_b, pair_f;
+	/* the paired DP's trace-bit gather runs as multiply-adds on the FMA pipe, its
+	 * multipliers read as kernel constants: 2^0 .. 2^15, and -(2^10 - 1), -2^10 .. -2^15 */
+	int32_t pair_pw[16], pair_nw[7];
 } plk_params_t;
 
 /* fills plk_params_t.s16 from go/ge/io/fs (every host path that builds parameters calls it) */
@@ -45,6 +48,9 @@ static inline void plk_fill_scaled(plk_params_t *p)
 	p->s16[0] = 16 * p->go, p->s16[1] = 16 * p->ge, p->s16[2] = 16 * p->io;
 	for (i = 0; i < 4; ++i) p->s16[3 + i] = -16 * p->fs + 9 - i;
 	p->s16[7] = -16 * p->fs, p->s16[8] = 16 * (p->go + p->ge);
+	for (i = 0; i < 16; ++i) p->pair_pw[i] = 1 << i;
+	p->pair_nw[0] = -((1 << 10) - 1);
+	for (i = 0; i < 6; ++i) p->pair_nw[1 + i] = -(1 << (10 + i));
 }
 
 /* per-job metadata, device resident */

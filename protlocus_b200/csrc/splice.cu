@@ -87,31 +87,99 @@ struct DpShared {
 	/* per warp, double-buffered by strip parity: the codons, donor and acceptor
 	 * penalties of the warp's 32*R rows of a strip, staged ahead of the strip */
 	uint8_t rows[PLK_WARPS_PER_CTA][2][3][ROWBLK] __attribute__((aligned(16)));
+	uint64_t bar[PLK_WARPS_PER_CTA][2];                 /* per warp and buffer: completion of its bulk copies */
 };
 
-/* Stage the row inputs of the warp's block of a strip, rows [b, b + 32R): codons
- * nas[b..], donor[b-1..] and acceptor[b-2..], 32R+2 bytes each.  Each block is
- * copied as 16-byte cp.async chunks from the 16-byte boundary at or below its
- * start; chunks that start past the end of their array are skipped (their bytes
- * are never read: the readers apply the row bounds).  Lanes 1-31 issue the
- * copies; lane 0 keeps its own cp.async queue for the strip hand-off ring.  The
- * preparation arrays sit inside a 16-byte aligned allocation with at least 16
- * bytes after the last one. */
-template <int R>
-__device__ __forceinline__ void stage_rows(uint8_t (*buf)[ROWBLK], const uint8_t *nas, const int8_t *donor,
-		const int8_t *acceptor, const int nl, const int b, const int lane)
+/* Row-input staging by the tensor memory accelerator.  The row inputs of the warp's
+ * block of a strip, rows [b, b + 32R) -- codons nas[b..], donor[b-1..] and
+ * acceptor[b-2..], 32R+2 bytes each -- are copied by lane 0 as 1-D bulk copies
+ * (cp.async.bulk, global -> this CTA's shared memory) from the 16-byte boundary at
+ * or below each start, cut at the first 16-byte boundary at or past the end of the
+ * array (bytes past the end are never read: the readers apply the row bounds).
+ * The preparation arrays sit inside a 16-byte aligned allocation with at least 16
+ * bytes after the last one.  The copies of a buffer complete on the warp's mbarrier
+ * of that buffer; the other 31 lanes issue nothing.
+ *
+ * `st` (per warp, in registers, kept across the jobs of a kernel): bits 0-1 the
+ * parity of the next phase of each buffer's mbarrier, bits 2-3 the buffers with
+ * copies in flight, bit 4 once a wait ran out (every later wait is skipped and the
+ * jobs of the warp report status -3: the DP did not run on its inputs). */
+#define ROW_WAIT_NS 1000000000ull   /* a staging wait gives up after one second */
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void row_bar_init(uint64_t *bar)
 {
-	constexpr int CH = (32 * R + 2 + 15 + 15) / 16;  /* chunks per block */
-	static_assert(CH * 16 <= ROWBLK, "row block");
-	if (lane == 0) return;
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(bar)), "r"(1) : "memory");
+}
+__device__ __forceinline__ void row_bar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+/* 16-byte aligned source and byte count (a multiple of 16, at most cap) of one array's block */
+__device__ __forceinline__ uint32_t row_span(const void *start, const void *end, uint32_t cap, const uint8_t *&src)
+{
+	src = (const uint8_t*)((uintptr_t)start & ~(uintptr_t)15);
+	const long long left = (long long)((const uint8_t*)end - src);
+	if (left <= 0) return 0u;
+	const uint32_t up = (uint32_t)((left + 15) & ~15ll);
+	return up < cap ? up : cap;
+}
+
+__device__ __forceinline__ void row_bulk(void *dst, const uint8_t *src, uint32_t bytes, uint64_t *bar)
+{
+	if (bytes) asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+			:: "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+
+/* lane 0: the blocks of NJ jobs (one window length) into buffers buf[j], completing on bar;
+ * the arrays' addresses come from the job table (J[j]->prep_off, nl, al) */
+template <int R, int NJ>
+__device__ __noinline__ void stage_rows(uint8_t (*const *buf)[ROWBLK], uint64_t *bar, const uint8_t *prep,
+		plk_job_t *const *J, const int b)
+{
+	constexpr uint32_t CB = ((32 * R + 2 + 15 + 15) / 16) * 16;
+	static_assert(CB <= ROWBLK, "row block");
+	const uint8_t *src[3 * NJ];
+	uint32_t n[3 * NJ], total = 0;
 #pragma unroll
-	for (int g = lane - 1; g < 3 * CH; g += 31) {
-		const int a = g / CH, j = g - a * CH;
-		const uint8_t *s = a == 0 ? nas + b : (const uint8_t*)(a == 1 ? donor + b - 1 : acceptor + b - 2);
-		const uint8_t *end = a == 0 ? nas + nl : (const uint8_t*)(a == 1 ? donor : acceptor) + nl + 1;
-		const uint8_t *src = (const uint8_t*)((uintptr_t)s & ~(uintptr_t)15) + 16 * j;
-		if (src < end) cp_async16(buf[a] + 16 * j, src);
+	for (int j = 0; j < NJ; ++j) {
+		const int nl = J[j]->nl, al = J[j]->al;
+		const uint8_t *nas = prep + J[j]->prep_off, *donor = nas + nl + al, *acceptor = donor + nl + 1;
+		n[3 * j] = row_span(nas + b, nas + nl, CB, src[3 * j]);
+		n[3 * j + 1] = row_span(donor + b - 1, donor + nl + 1, CB, src[3 * j + 1]);
+		n[3 * j + 2] = row_span(acceptor + b - 2, acceptor + nl + 1, CB, src[3 * j + 2]);
+		total += n[3 * j] + n[3 * j + 1] + n[3 * j + 2];
 	}
+	/* the buffer's earlier reads (generic proxy) before the copies' writes (async proxy) */
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_addr(bar)), "r"(total) : "memory");
+#pragma unroll
+	for (int j = 0; j < NJ; ++j)
+#pragma unroll
+		for (int a = 0; a < 3; ++a) row_bulk(buf[j][a], src[3 * j + a], n[3 * j + a], bar);
+}
+
+/* every lane: waits (bounded) for the copies into buffer q when they are in flight */
+__device__ __forceinline__ void rows_ready(uint64_t *bar, unsigned &st, const int q, plk_job_t *JA, plk_job_t *JB)
+{
+	if (!(st >> (2 + q) & 1u)) return;
+	st &= ~(4u << q);
+	if (st & 16u) return;
+	const uint32_t a = smem_addr(bar + q), parity = st >> q & 1u;
+	uint64_t t0;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+	for (;;) {
+		uint32_t done;
+		asm volatile("{\n\t.reg .pred p;\n\t"
+		             "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+		             "selp.u32 %0, 1, 0, p;\n\t}"
+		             : "=r"(done) : "r"(a), "r"(parity) : "memory");
+		if (done) { st ^= 1u << q; return; }
+		uint64_t t;
+		asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+		if (t - t0 > ROW_WAIT_NS) break;
+	}
+	st |= 16u;
+	JA->status = -3;
+	if (JB) JB->status = -3;
 }
 
 
@@ -313,7 +381,7 @@ __device__ __forceinline__ void cells_plain(const int (&in)[9], int (&hm)[R], co
 template <int MODE, int NW, int R>
 __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t *__restrict__ prep,
 		uint16_t *__restrict__ trace, int32_t *__restrict__ myring, DpShared &sh, const plk_params_t &P,
-		const int L, const int wib)
+		const int L, const int wib, unsigned &st)
 {
 	constexpr int NL = 32 * NW, HS = NL * R;
 	constexpr int SC = MODE == 0 ? 16 : 1;                  /* value scale of the mode */
@@ -341,23 +409,36 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 	for (int r = 0; r < R; ++r) ip[r] = lh[r] = ic[r] = hm[r] = NEG, code[r] = 0, gi[r] = 0;
 #pragma unroll
 	for (int r = 0; r < R + 2; ++r) dn[r] = ac[r] = 0;
+	uint64_t *bar = sh.bar[wib];
 	/* the first strip's row inputs, and the ring entry of the first strip (the -inf row) */
-	stage_rows<R>(rowbuf[0], nas, donor, acceptor, nl, 2 + w * 32 * R, lane);
+	if (lane == 0) {
+		uint8_t (*const b0[1])[ROWBLK] = {rowbuf[0]};
+		plk_job_t *const JP[1] = {J};
+		stage_rows<R, 1>(b0, &bar[0], prep, JP, 2 + w * 32 * R);
+	}
+	st |= 4u;
 	if (L == 0) {
 #pragma unroll
 		for (int q = 0; q < 9; ++q) pre[q] = NEG;
 	}
-	cp_async_wait_all();
+	rows_ready(bar, st, 0, J, nullptr);
 	__syncwarp();
 
 	for (int s = 0; s < total; ++s) {
 		if (__shfl_sync(FULL, c, 0) == 0) {
 			/* lane 0 of the warp starts a strip: the strip's row inputs (staged one
 			 * period ago) are visible after the wait; stage those of the next strip */
-			cp_async_wait_all();
-			__syncwarp();
 			const int kn = (s - 32 * w) / Pc + 1;
-			if (kn < nstrip) stage_rows<R>(rowbuf[kn & 1], nas, donor, acceptor, nl, 2 + kn * HS + w * 32 * R, lane);
+			rows_ready(bar, st, (kn - 1) & 1, J, nullptr);
+			__syncwarp();
+			if (kn < nstrip) {
+				if (lane == 0) {
+					uint8_t (*const bn[1])[ROWBLK] = {rowbuf[kn & 1]};
+					plk_job_t *const JP[1] = {J};
+					stage_rows<R, 1>(bn, &bar[kn & 1], prep, JP, 2 + kn * HS + w * 32 * R);
+				}
+				st |= 4u << (kn & 1);
+			}
 		}
 		/* column state of the rows above: lane-1's output of the previous step */
 		int in[9];
@@ -450,6 +531,8 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 		}
 	}
 	cp_async_wait_all();
+	rows_ready(bar, st, 0, J, nullptr);  /* no copies are in flight here; kept as a guard */
+	rows_ready(bar, st, 1, J, nullptr);
 	/* the final score H(nl-1, al-1): the lane holding row nl-1 in the last strip keeps
 	 * that strip's last column in hm */
 	{
@@ -477,8 +560,10 @@ k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop
 		const int b = x / 22, a = x % 22, v = P.sc[a * 22 + b];
 		sh.sct[x] = MODE == 0 ? v * 16 + 15 : v;
 	}
-	__syncthreads();
 	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+	if (lane == 0) row_bar_init(&sh.bar[wib][0]), row_bar_init(&sh.bar[wib][1]), row_bar_init_fence();
+	__syncthreads();
+	unsigned st = 0;
 	for (;;) {
 		if (threadIdx.x == 0) sh.job = atomicAdd(&counters[0], 1);
 		__syncthreads();
@@ -486,7 +571,7 @@ k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop
 		__syncthreads();
 		if (idx >= n_coop) break;
 		dp_job<MODE, PLK_WARPS_PER_CTA, R>(jobs + order_coop[idx], prep, trace,
-				ring + (int64_t)blockIdx.x * PLK_WARPS_PER_CTA * ring_stride, sh, P, threadIdx.x, wib);
+				ring + (int64_t)blockIdx.x * PLK_WARPS_PER_CTA * ring_stride, sh, P, threadIdx.x, wib, st);
 		__syncthreads();
 	}
 	int32_t *myring = ring + ((int64_t)blockIdx.x * PLK_WARPS_PER_CTA + wib) * ring_stride;
@@ -495,7 +580,7 @@ k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop
 		if (lane == 0) idx = atomicAdd(&counters[1], 1);
 		idx = __shfl_sync(FULL, idx, 0);
 		if (idx >= n_solo) break;
-		dp_job<MODE, 1, R>(jobs + order_solo[idx], prep, trace, myring, sh, P, lane, wib);
+		dp_job<MODE, 1, R>(jobs + order_solo[idx], prep, trace, myring, sh, P, lane, wib, st);
 		__syncwarp();
 	}
 }
@@ -515,47 +600,43 @@ k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop
  * [0, 0x7fff] per half, so the signed 16-bit forms order them as unsigned numbers.
  *
  * The first-winning candidate cannot ride in the low bits of the value as in the
- * 32-bit kernel.  Each cell stores ten bits "candidate k is below the maximum"
- * (the traceback takes the first clear one: first wins, nasw-sse.c:517-530) and the
- * six extension / lazy-F comparisons.  Each bit is one add: with both operands
- * below 0x8000 per half, (a + 0x8000 - b) has bit 15 set exactly when a >= b and
- * never borrows across the halves.  Byte permutes with sign replication gather the
- * bit-15 / bit-31 answers into bytes, and a tree of bit-selects merges them into
- * the trace word of each job (low half: the first job, high half: the second):
- *   bits 0-4  s0 s2 s4 s6 s8     bits 8-12  s1 s3 s5 s7 s9   (s_k: candidate k < max)
- *   bits 5-7  g4 g6 g8           bits 13-15 g5 g7 g9         (g4: not I-extended,
- *   g5: not D-extended, g6/g7/g8: not A/B/C-extended, g9: not raised by the carried
- *   insertion); the traceback converts such a word to the layout of the other modes.
+ * 32-bit kernel.  Each cell stores ten bits "candidate k equals the maximum" (the
+ * traceback takes the first set one: first wins, nasw-sse.c:517-530) and the six
+ * extension / lazy-F comparisons.  Each bit comes out clean from one DPX step: for
+ * c <= m per half, max(c + 1, m) - m is 1 exactly when c == m and 0 otherwise, in
+ * both halves at once with no borrow between them.  The subtraction and the
+ * placement of the bit are linear, so the whole word is one sum of multiply-adds,
+ *   z = sum_k max(c_k + 1, m_k) * 2^p_k  -  sum_k m_k * 2^p_k   (mod 2^32),
+ * which runs on the FMA pipe (the multipliers are kernel constants) while the DPX
+ * steps keep the ALU pipe.  Bit p of each half: p = k for candidates 0-9 (m = the
+ * cell's maximum) and p = 10-15 for g4-g9 with m = the maximum the compared value
+ * entered:
+ *   g4: I opened from H' (not I-extended)   g5: D opened (not D-extended)
+ *   g6/g7/g8: A/B/C opened (not extended)   g9: H' >= the carried insertion;
+ * the traceback converts such a word to the layout of the other modes.
  */
 struct DpSharedPair {
 	int32_t slot[2][PLK_WARPS_PER_CTA][PLK_RING_INTS];
 	int32_t job;
 	int32_t pre[PLK_WARPS_PER_CTA][PLK_RING_INTS] __attribute__((aligned(16)));
 	uint8_t rows[PLK_WARPS_PER_CTA][2][2][3][ROWBLK] __attribute__((aligned(16)));  /* [warp][job][parity][array] */
+	uint64_t bar[PLK_WARPS_PER_CTA][2];  /* per warp and buffer parity: both jobs' copies */
 };
 #define PAIR_SCT_WORDS (22 * 22 * 22)   /* [protein residue][codon residue of job 1][of job 2] */
 
 __device__ __forceinline__ unsigned pk16(int a, int b) { return ((unsigned)a & 0xffffu) | ((unsigned)b << 16); }
-/* bytes: sign of x's bit 15, of y's bit 15, of x's bit 31, of y's bit 31 */
-__device__ __forceinline__ unsigned sign_pairs(unsigned x, unsigned y)
-{
-	unsigned d;
-	asm("prmt.b32 %0, %1, %2, 0xFBD9;" : "=r"(d) : "r"(x), "r"(y));
-	return d;
-}
-__device__ __forceinline__ unsigned sel_bits(unsigned a, unsigned b, unsigned m) { return (a & m) | (b & ~m); }
 /* per-half maximum of two, as one add+max instruction (there is no two-input intrinsic; an
  * inline max.s16x2 cost registers) */
 __device__ __forceinline__ unsigned vmax2u(unsigned a, unsigned b) { return __viaddmax_s16x2(a, 0u, b); }
 
-struct PairK { unsigned F2, GOn, GEn, IOn, FSn, FSp, GOEn; };
+struct PairK { unsigned F2, GOn, GEn, IOn, FSn, GOEn, ONE, ONEFS; };
 
 template <int R>
 __device__ __forceinline__ void cells_pair(const unsigned (&in)[9], unsigned (&hm)[R], const unsigned ah1,
 		const unsigned ah2, const unsigned ah3, const bool row2, const unsigned r2h, const unsigned r2f,
 		const uint32_t *__restrict__ srow, const int (&cp)[R], const unsigned (&gi)[R], const unsigned (&dn)[R + 2],
 		const unsigned (&ac)[R + 2], unsigned (&ip)[R], unsigned (&lh)[R], const unsigned (&ic)[R], const PairK &K,
-		unsigned (&o)[9], unsigned (&z)[R], unsigned (&hn)[R])
+		const plk_params_t &P, unsigned (&o)[9], unsigned (&z)[R], unsigned (&hn)[R])
 {
 	unsigned h1 = in[0], h2 = in[1], h3 = in[2], d1 = in[3], d2 = in[4], d3 = in[5], va = in[6], vb = in[7], vc = in[8];
 #pragma unroll
@@ -566,24 +647,21 @@ __device__ __forceinline__ void cells_pair(const unsigned (&in)[9], unsigned (&h
 		if (r == 0 && row2) h1m1 = r2f, h2m1 = r2f, h3m1 = r2h; /* column -1 while row 2 is computed: {0, -fs, -fs} */
 		/* 1: I -- g4 = H'(c-1) - go >= I(c-1) */
 		const unsigned t4 = __viaddmax_s16x2(lh[r], K.GOn, K.F2);
-		const unsigned g4 = t4 + 0x80008000u - ip[r];
-		const unsigned ipn = __viaddmax_s16x2(vmax2u(t4, ip[r]), K.GEn, K.F2);
+		const unsigned m4 = vmax2u(t4, ip[r]);
+		const unsigned ipn = __viaddmax_s16x2(m4, K.GEn, K.F2);
 		ip[r] = ipn;
 		/* 2: D -- g5 = H(i-3) - go >= D(i-3) */
 		const unsigned u5 = __viaddmax_s16x2(h3, K.GOn, K.F2);
-		const unsigned g5 = u5 + 0x80008000u - d3;
-		const unsigned dnew = __viaddmax_s16x2(vmax2u(u5, d3), gi[r], K.F2);
+		const unsigned m5 = vmax2u(u5, d3);
+		const unsigned dnew = __viaddmax_s16x2(m5, gi[r], K.F2);
 		/* 3-5: phase-0/1/2 introns */
 		const unsigned ua = __viaddmax_s16x2(h1, K.IOn, K.F2);
 		const unsigned t6 = __viaddmax_s16x2(ua, dn[r], K.F2);
-		const unsigned g6 = t6 + 0x80008000u - va;
 		const unsigned anew = vmax2u(t6, va);
 		const unsigned ub = __viaddmax_s16x2(h1m1, K.IOn, K.F2);
 		const unsigned t7 = __viaddmax_s16x2(ub, dn[r + 1], K.F2);
-		const unsigned g7 = t7 + 0x80008000u - vb;
 		const unsigned bnew = vmax2u(t7, vb);
 		const unsigned t8 = __viaddmax_s16x2(ub, dn[r + 2], K.F2);
-		const unsigned g8 = t8 + 0x80008000u - vc;
 		const unsigned cnew = vmax2u(t8, vc);
 		/* candidates 0-5 (floored at F, where none of them can win), 6-9 folded */
 		const unsigned c0 = __viaddmax_s16x2(h3m1, srow[cp[r]], K.F2);  /* H(i-3,j-1) + s(i,j) */
@@ -594,20 +672,27 @@ __device__ __forceinline__ void cells_pair(const unsigned (&in)[9], unsigned (&h
 		he = __vimax3_s16x2(he, c3, c4);
 		const unsigned fsm = vmax2u(__vimax3_s16x2(h1, h2, h1m1), h2m1);
 		he = __viaddmax_s16x2(fsm, K.FSn, vmax2u(he, c5));     /* 6-9: H(i-1|i-2, j|j-1) - fs */
-		/* s_k: candidate k < max, the bit 15 of max + 0x7fff - c_k (no borrow: c_k <= max) */
-		const unsigned m1 = he + 0x7fff7fffu, m1f = m1 + K.FSp;  /* two-operand forms: the adder of the FMA pipe */
-		const unsigned s0 = m1 - c0, s1 = m1 - ipn, s2 = m1 - dnew, s3 = m1 - c3, s4 = m1 - c4, s5 = m1 - c5;
-		const unsigned s6 = m1f - h1, s7 = m1f - h2, s8 = m1f - h1m1, s9 = m1f - h2m1;
 		lh[r] = he;
-		/* the carried insertion: g9 = H' >= ic */
-		const unsigned g9 = he + 0x80008000u - ic[r];
-		const unsigned h = vmax2u(he, ic[r]);
-		/* gather the sixteen bits of both cells */
-		const unsigned p0 = sign_pairs(s0, s1), p1 = sign_pairs(s2, s3), p2 = sign_pairs(s4, s5), p3 = sign_pairs(s6, s7);
-		const unsigned p4 = sign_pairs(s8, s9), p5 = sign_pairs(g4, g5), p6 = sign_pairs(g6, g7), p7 = sign_pairs(g8, g9);
-		const unsigned q01 = sel_bits(p0, p1, 0x01010101u), q23 = sel_bits(p2, p3, 0x04040404u);
-		const unsigned q45 = sel_bits(p4, p5, 0x10101010u), q67 = sel_bits(p6, p7, 0x40404040u);
-		z[r] = sel_bits(sel_bits(q01, q23, 0x03030303u), sel_bits(q45, q67, 0x30303030u), 0x0f0f0f0fu);
+		const unsigned h = vmax2u(he, ic[r]);                  /* the carried insertion */
+		/* the sixteen bits of both cells: max(c + 1, m) on the ALU pipe, the sum on the FMA pipe */
+		unsigned zz = __viaddmax_s16x2(c0, K.ONE, he);
+		zz += __viaddmax_s16x2(ipn, K.ONE, he) * (unsigned)P.pair_pw[1];
+		zz += __viaddmax_s16x2(dnew, K.ONE, he) * (unsigned)P.pair_pw[2];
+		zz += __viaddmax_s16x2(c3, K.ONE, he) * (unsigned)P.pair_pw[3];
+		zz += __viaddmax_s16x2(c4, K.ONE, he) * (unsigned)P.pair_pw[4];
+		zz += __viaddmax_s16x2(c5, K.ONE, he) * (unsigned)P.pair_pw[5];
+		zz += __viaddmax_s16x2(h1, K.ONEFS, he) * (unsigned)P.pair_pw[6];
+		zz += __viaddmax_s16x2(h2, K.ONEFS, he) * (unsigned)P.pair_pw[7];
+		zz += __viaddmax_s16x2(h1m1, K.ONEFS, he) * (unsigned)P.pair_pw[8];
+		zz += __viaddmax_s16x2(h2m1, K.ONEFS, he) * (unsigned)P.pair_pw[9];
+		zz += he * (unsigned)P.pair_nw[0];
+		zz += __viaddmax_s16x2(t4, K.ONE, m4) * (unsigned)P.pair_pw[10] + m4 * (unsigned)P.pair_nw[1];
+		zz += __viaddmax_s16x2(u5, K.ONE, m5) * (unsigned)P.pair_pw[11] + m5 * (unsigned)P.pair_nw[2];
+		zz += __viaddmax_s16x2(t6, K.ONE, anew) * (unsigned)P.pair_pw[12] + anew * (unsigned)P.pair_nw[3];
+		zz += __viaddmax_s16x2(t7, K.ONE, bnew) * (unsigned)P.pair_pw[13] + bnew * (unsigned)P.pair_nw[4];
+		zz += __viaddmax_s16x2(t8, K.ONE, cnew) * (unsigned)P.pair_pw[14] + cnew * (unsigned)P.pair_nw[5];
+		zz += __viaddmax_s16x2(he, K.ONE, h) * (unsigned)P.pair_pw[15] + h * (unsigned)P.pair_nw[6];
+		z[r] = zz;
 		hn[r] = h;
 		h3 = h2, h2 = h1, h1 = h;
 		d3 = d2, d2 = d1, d1 = dnew;
@@ -631,7 +716,7 @@ template <int NW, int R>
 __device__ __forceinline__ void dp_pair(plk_job_t *__restrict__ JA, plk_job_t *__restrict__ JB,
 		const uint8_t *__restrict__ prep, uint16_t *__restrict__ trace, int32_t *__restrict__ myring,
 		DpSharedPair &sh, const uint32_t *__restrict__ sct2, const PairK &K, const plk_params_t &P,
-		const int L, const int wib)
+		const int L, const int wib, unsigned &st)
 {
 	constexpr int NL = 32 * NW, HS = NL * R;
 	const unsigned NEG = K.F2;
@@ -660,23 +745,31 @@ __device__ __forceinline__ void dp_pair(plk_job_t *__restrict__ JA, plk_job_t *_
 	for (int r = 0; r < R; ++r) ip[r] = lh[r] = ic[r] = hm[r] = NEG, cp[r] = 0, gi[r] = 0;
 #pragma unroll
 	for (int r = 0; r < R + 2; ++r) dn[r] = ac[r] = 0;
-	stage_rows<R>(rowA[0], nasA, donA, accA, nl, 2 + w * 32 * R, lane);
-	stage_rows<R>(rowB[0], nasB, donB, accB, nl, 2 + w * 32 * R, lane);
+	uint64_t *bar = sh.bar[wib];
+	plk_job_t *const JP[2] = {JA, JB};
+	if (lane == 0) {
+		uint8_t (*const b0[2])[ROWBLK] = {rowA[0], rowB[0]};
+		stage_rows<R, 2>(b0, &bar[0], prep, JP, 2 + w * 32 * R);
+	}
+	st |= 4u;
 	if (L == 0) {
 #pragma unroll
 		for (int q = 0; q < 9; ++q) pre[q] = (int32_t)NEG;
 	}
-	cp_async_wait_all();
+	rows_ready(bar, st, 0, JA, JB);
 	__syncwarp();
 
 	for (int s = 0; s < total; ++s) {
 		if (__shfl_sync(FULL, c, 0) == 0) {
-			cp_async_wait_all();
-			__syncwarp();
 			const int kn = (s - 32 * w) / Pc + 1;
+			rows_ready(bar, st, (kn - 1) & 1, JA, JB);
+			__syncwarp();
 			if (kn < nstrip) {
-				stage_rows<R>(rowA[kn & 1], nasA, donA, accA, nl, 2 + kn * HS + w * 32 * R, lane);
-				stage_rows<R>(rowB[kn & 1], nasB, donB, accB, nl, 2 + kn * HS + w * 32 * R, lane);
+				if (lane == 0) {
+					uint8_t (*const bn[2])[ROWBLK] = {rowA[kn & 1], rowB[kn & 1]};
+					stage_rows<R, 2>(bn, &bar[kn & 1], prep, JP, 2 + kn * HS + w * 32 * R);
+				}
+				st |= 4u << (kn & 1);
 			}
 		}
 		unsigned in[9];
@@ -733,7 +826,7 @@ __device__ __forceinline__ void dp_pair(plk_job_t *__restrict__ JA, plk_job_t *_
 #pragma unroll
 				for (int r = 0; r < R; ++r) ic[r] = __viaddmax_s16x2(ic[r], K.GEn, NEG);
 			}
-			cells_pair<R>(in, hm, ah1, ah2, ah3, row2, r2h, r2f, srow, cp, gi, dn, ac, ip, lh, ic, K, o, z, hn);
+			cells_pair<R>(in, hm, ah1, ah2, ah3, row2, r2h, r2f, srow, cp, gi, dn, ac, ip, lh, ic, K, P, o, z, hn);
 			const int64_t toff = (((int64_t)k * al + dcol) * NL + L) * R;
 			store_trace_pair<R>(trA + toff, trB + toff, z);
 			if (L == NL - 1) {
@@ -765,6 +858,8 @@ __device__ __forceinline__ void dp_pair(plk_job_t *__restrict__ JA, plk_job_t *_
 		}
 	}
 	cp_async_wait_all();
+	rows_ready(bar, st, 0, JA, JB);  /* no copies are in flight here; kept as a guard */
+	rows_ready(bar, st, 1, JA, JB);
 	{ /* H(nl-1, al-1) of both jobs, unbiased */
 		const int rl = nl - 1 - i0;
 		if (rl >= 0 && rl < R) {
@@ -791,9 +886,12 @@ k_splice_pair(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_co
 	PairK K;
 	K.F2 = (unsigned)P.pair_f * 0x10001u;
 	K.GOn = pk16(-P.go, -P.go), K.GEn = pk16(-P.ge, -P.ge), K.IOn = pk16(-P.io, -P.io);
-	K.FSn = pk16(-P.fs, -P.fs), K.FSp = pk16(P.fs, P.fs), K.GOEn = pk16(-(P.go + P.ge), -(P.go + P.ge));
-	__syncthreads();
+	K.FSn = pk16(-P.fs, -P.fs), K.GOEn = pk16(-(P.go + P.ge), -(P.go + P.ge));
+	K.ONE = 0x00010001u, K.ONEFS = pk16(1 - P.fs, 1 - P.fs);
 	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+	if (lane == 0) row_bar_init(&sh.bar[wib][0]), row_bar_init(&sh.bar[wib][1]), row_bar_init_fence();
+	__syncthreads();
+	unsigned st = 0;
 	for (;;) {
 		if (threadIdx.x == 0) sh.job = atomicAdd(&counters[0], 1);
 		__syncthreads();
@@ -802,7 +900,7 @@ k_splice_pair(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_co
 		if (idx >= n_coop) break;
 		plk_job_t *J = jobs + order_coop[idx];
 		dp_pair<PLK_WARPS_PER_CTA, R>(J, jobs + J->pair, prep, trace,
-				ring + (int64_t)blockIdx.x * PLK_WARPS_PER_CTA * ring_stride, sh, pair_sct, K, P, threadIdx.x, wib);
+				ring + (int64_t)blockIdx.x * PLK_WARPS_PER_CTA * ring_stride, sh, pair_sct, K, P, threadIdx.x, wib, st);
 		__syncthreads();
 	}
 	int32_t *myring = ring + ((int64_t)blockIdx.x * PLK_WARPS_PER_CTA + wib) * ring_stride;
@@ -812,7 +910,7 @@ k_splice_pair(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_co
 		idx = __shfl_sync(FULL, idx, 0);
 		if (idx >= n_solo) break;
 		plk_job_t *J = jobs + order_solo[idx];
-		dp_pair<1, R>(J, jobs + J->pair, prep, trace, myring, sh, pair_sct, K, P, lane, wib);
+		dp_pair<1, R>(J, jobs + J->pair, prep, trace, myring, sh, pair_sct, K, P, lane, wib, st);
 		__syncwarp();
 	}
 }
@@ -857,12 +955,9 @@ __device__ __forceinline__ void tb_load_chunk(const uint16_t *__restrict__ tr, i
  * bits 0-3, extension bits I 4, D 5, C 6, A 12, B 13, carried-insertion bit 14) */
 __device__ __forceinline__ uint16_t tb_pair_norm(unsigned x)
 {
-	const unsigned s = (x & 1u) | (x >> 7 & 2u) | (x << 1 & 4u) | (x >> 6 & 8u) | (x << 2 & 16u) | (x >> 5 & 32u) |
-		(x << 3 & 64u) | (x >> 4 & 128u) | (x << 4 & 256u) | (x >> 3 & 512u);
-	const unsigned state = __ffs(~s) - 1;  /* the first candidate equal to the maximum */
-	const unsigned n = ~x;                 /* the g bits are negated flags */
-	return (uint16_t)((15u - state) | (n >> 5 & 1u) << 4 | (n >> 13 & 1u) << 5 | (n >> 7 & 1u) << 6 |
-		(n >> 6 & 1u) << 12 | (n >> 14 & 1u) << 13 | (n >> 15 & 1u) << 14);
+	const unsigned state = __ffs(x & 0x3ffu) - 1;  /* the first candidate equal to the maximum */
+	const unsigned n = ~x;                         /* the g bits are negated flags */
+	return (uint16_t)((15u - state) | (n >> 6 & 0x30u) | (n >> 8 & 0x40u) | (n & 0x3000u) | (n >> 1 & 0x4000u));
 }
 
 __device__ __forceinline__ void tb_norm8(uint16_t (&w)[8], const bool pair)

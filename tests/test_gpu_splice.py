@@ -357,10 +357,12 @@ def test_paired_int16x2_bit_exact(engine, oracle, seed):
 
 
 def test_paired_golden_vectors_with_twins(engine, oracle, golden):
-    """Each 16-bit golden vector next to its own twin (same protein, same window)."""
+    """Each golden vector the 16-bit DP answers (ns_global_gs16b, and ns_global_gs_auto where
+    it dispatches to 16 bits) next to its own twin (same protein, same window)."""
     by_opt = {}
     for c in golden["cases"]:
-        if c["opt"].get("flag", NS_F_CIGAR) & (NS_F_EXT_LEFT | NS_F_EXT_RIGHT) or c["fn"] != "ns_global_gs16b":
+        if c["opt"].get("flag", NS_F_CIGAR) & (NS_F_EXT_LEFT | NS_F_EXT_RIGHT) or \
+                c["fn"] not in ("ns_global_gs16b", "ns_global_gs_auto"):
             continue
         if c["ss"]:
             continue
