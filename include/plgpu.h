@@ -224,8 +224,12 @@ void pl_engine_last_plan(const pl_engine_t *e, int32_t *n_waves, int32_t *n_coop
 /* Two 16-bit jobs that share one protein (the same aa_off in the job table) and one
  * window length -- the two strands of a locus -- run as a pair in the two halves of
  * the int16x2 DP kernel when their score range fits its 15-bit domain (on by
- * default; PLGPU_PAIR=0 or pl_engine_set_pairing(e, 0) turns it off).  Results are
- * the same either way.  pl_engine_last_pairs: pairs formed in the last batch. */
+ * default; PLGPU_PAIR=0 or pl_engine_set_pairing(e, 0) turns it off).  With
+ * enable = 1 a job pairs only when the pair's cells are at most PLGPU_PAIR_SHARE
+ * (default 1) times the batch's cells per CTA and trace wave, so that a pair never
+ * becomes a launch's longest unit (a batch too small to fill the GPU forms none);
+ * enable = 2 pairs every eligible job.  Results are the same either way.
+ * pl_engine_last_pairs: pairs formed in the last batch. */
 void pl_engine_set_pairing(pl_engine_t *e, int32_t enable);
 int32_t pl_engine_last_pairs(const pl_engine_t *e);
 /* A batch whose launch plan has the same shape as the previous batch's (the same
@@ -599,6 +603,10 @@ typedef struct {
 	int32_t L, n;        /* profile length, ORF length */
 	int32_t diag, band;  /* ps_cand_t.diag, mp_psopt_t.band */
 } pl_ps_job_t;
+/* Cells of one candidate's banded DP (rows [0, L), ORF positions within band of
+ * row + diag, clipped to [0, n); the whole L x n matrix when band <= 0): the count
+ * the timing counters report. */
+int64_t pl_ps_band_cells(int32_t L, int32_t n, int32_t diag, int32_t band);
 int pl_ps_gapped_host(pl_engine_t *e, const pl_ps_job_t *jobs, int32_t n, const int8_t *pssm, int64_t l_pssm,
 		const uint8_t *orf, int64_t l_orf, int32_t go, int32_t ge, int32_t *scores);
 /* Device-resident variant: pssm, orf and scores are device pointers; the caller

@@ -93,6 +93,34 @@ void pl_ps_engine_free(pl_engine_t *e)
 	dbuf_free(&e->s_jobs), dbuf_free(&e->s_pssm), dbuf_free(&e->s_orf), dbuf_free(&e->s_scr), dbuf_free(&e->s_score);
 }
 
+/* Cells of one candidate's banded DP: rows i in [0, L) cover ORF positions
+ * [max(i + diag - band, 0), min(i + diag + band, n - 1)] (every position when band <= 0),
+ * summed in closed form: with x = i + diag the width is linear in x between the two
+ * breakpoints x = band and x = n - 1 - band, and positive exactly on [-band, n - 1 + band]. */
+PL_EXPORT int64_t pl_ps_band_cells(int32_t L, int32_t n, int32_t diag, int32_t band)
+{
+	int64_t x0, x1, cut[2], tot = 0;
+	int k;
+	if (L <= 0 || n <= 0) return 0;
+	if (band <= 0) return (int64_t)L * n;
+	x0 = diag > -(int64_t)band ? diag : -(int64_t)band;
+	x1 = (int64_t)diag + L - 1 < (int64_t)n - 1 + band ? (int64_t)diag + L - 1 : (int64_t)n - 1 + band;
+	cut[0] = band < (int64_t)n - 1 - band ? band : (int64_t)n - 1 - band;
+	cut[1] = band < (int64_t)n - 1 - band ? (int64_t)n - 1 - band : band;
+	for (k = 0; k < 3 && x0 <= x1; ++k) {
+		const int64_t s = x0, t = k < 2 && cut[k] < x1 ? cut[k] : x1;
+		if (t >= s) {
+			/* lo = 0 (x <= band) or x - band; hi = x + band (x <= n - 1 - band) or n - 1 */
+			const int64_t la = s <= band ? 0 : 1, lc = s <= band ? 0 : -(int64_t)band;
+			const int64_t ha = s <= (int64_t)n - 1 - band ? 1 : 0, hc = s <= (int64_t)n - 1 - band ? band : (int64_t)n - 1;
+			const int64_t a = ha - la, c = hc - lc + 1, m = t - s + 1;
+			tot += a * (s + t) * m / 2 + c * m;
+			x0 = t + 1;
+		}
+	}
+	return tot;
+}
+
 PL_EXPORT int pl_ps_gapped_host(pl_engine_t *e, const pl_ps_job_t *jobs, int32_t n, const int8_t *pssm, int64_t l_pssm,
 		const uint8_t *orf, int64_t l_orf, int32_t go, int32_t ge, int32_t *scores)
 {
@@ -141,16 +169,7 @@ PL_EXPORT int pl_ps_gapped_host(pl_engine_t *e, const pl_ps_job_t *jobs, int32_t
 	CK(cudaStreamSynchronize(st));
 	{ /* cells: the banded (or full) rows inside the ORF */
 		int64_t cells = 0;
-		for (q = 0; q < n; ++q) {
-			int32_t i;
-			const pl_ps_job_t *J = &jobs[q];
-			for (i = 0; i < J->L; ++i) {
-				int32_t lo = J->band > 0 ? i + J->diag - J->band : 0, hi = J->band > 0 ? i + J->diag + J->band : J->n - 1;
-				if (lo < 0) lo = 0;
-				if (hi > J->n - 1) hi = J->n - 1;
-				if (hi >= lo) cells += hi - lo + 1;
-			}
-		}
+		for (q = 0; q < n; ++q) cells += pl_ps_band_cells(jobs[q].L, jobs[q].n, jobs[q].diag, jobs[q].band);
 		pl_feat_times(e, cells);
 	}
 	ok = 1;
@@ -220,7 +239,6 @@ PL_EXPORT int pl_ps_gapped_device(pl_engine_t *e, const pl_ps_job_t *jobs, int32
 	if (!hj) { pl_set_error("out of host memory"); return 0; }
 	for (q = 0; q < n; ++q) {
 		const pl_ps_job_t *J = &jobs[q];
-		int32_t i;
 		if (J->L < 0 || J->n < 0 || J->pssm_off < 0 || J->orf_off < 0) {
 			pl_set_error("candidate %d: negative offsets or sizes", q);
 			goto fail;
@@ -228,12 +246,7 @@ PL_EXPORT int pl_ps_gapped_device(pl_engine_t *e, const pl_ps_job_t *jobs, int32
 		hj[q].pssm_off = J->pssm_off, hj[q].orf_off = J->orf_off, hj[q].scratch_off = scr;
 		hj[q].L = J->L, hj[q].n = J->n, hj[q].diag = J->diag, hj[q].band = J->band;
 		scr += (int64_t)J->n + 1;
-		for (i = 0; i < J->L; ++i) {
-			int32_t lo = J->band > 0 ? i + J->diag - J->band : 0, hi = J->band > 0 ? i + J->diag + J->band : J->n - 1;
-			if (lo < 0) lo = 0;
-			if (hi > J->n - 1) hi = J->n - 1;
-			if (hi >= lo) cells += hi - lo + 1;
-		}
+		cells += pl_ps_band_cells(J->L, J->n, J->diag, J->band);
 	}
 	CK(cudaSetDevice(e->device));
 	st = stream ? (cudaStream_t)stream : e->stream;

@@ -388,18 +388,36 @@ static int pl_cmp_pair(const void *a, const void *b)
 	return x->idx - y->idx;
 }
 
+/* A pair is one unit of a persistent launch, twice a job's cells: pairing the largest jobs
+ * of a batch would lengthen the launch's critical path (its longest unit), so a job pairs
+ * only when the pair's cells stay within PLGPU_PAIR_SHARE (default 1) times the cells per
+ * CTA of a wave: total cells / (CTAs x the waves the trace budget implies). */
+static double g_pair_share = 1.0;
+static pthread_once_t g_pair_share_once = PTHREAD_ONCE_INIT;
+static void pl_pair_share_init(void)
+{
+	const char *v = getenv("PLGPU_PAIR_SHARE");
+	if (v && *v) {
+		const double x = atof(v);
+		if (x > 0.0) g_pair_share = x;
+	}
+}
+
 /* Pairs of 16-bit jobs with one protein (the same aa_off) and one window length run as
- * mode 3; returns the number of pairs formed (0 on a host allocation failure too). */
-static int32_t pl_form_pairs(pl_engine_t *e, const ns_opt_t *opt, int32_t n, int max_sub, plk_params_t *P)
+ * mode 3 when each pair's cells are at most max_pair_cells; returns the number of pairs
+ * formed (0 on a host allocation failure too). */
+static int32_t pl_form_pairs(pl_engine_t *e, const ns_opt_t *opt, int32_t n, int max_sub, int64_t max_pair_cells,
+		plk_params_t *P)
 {
 	pl_pkey_t *key;
 	int32_t q, m = 0, n_pairs = 0, al_cap = 0, bias = 0;
 	if (!e->pairing || n < 2 || !pl_pair_limits(opt, max_sub, &al_cap, &bias)) return 0;
+	if (e->pairing == 2) max_pair_cells = INT64_MAX;  /* every eligible job */
 	key = (pl_pkey_t*)malloc(sizeof(*key) * (size_t)n);
 	if (!key) return 0;
 	for (q = 0; q < n; ++q) {
 		const plk_job_t *J = &e->hj[q];
-		if (J->mode != 0 || J->al > al_cap) continue;
+		if (J->mode != 0 || J->al > al_cap || 2 * (int64_t)(J->nl - 2) * J->al > max_pair_cells) continue;
 		key[m].aa_off = J->aa_off, key[m].al = J->al, key[m].nl = J->nl, key[m].idx = q, ++m;
 	}
 	qsort(key, (size_t)m, sizeof(*key), pl_cmp_pair);
@@ -501,7 +519,14 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 		pl_set_error("one job needs %lld trace bytes, over the budget of %lld", (long long)max_trace, (long long)e->trace_budget);
 		return 0;
 	}
-	e->last_pairs = pl_form_pairs(e, opt, n, max_sub, &P);
+	{
+		int64_t cells = 0, waves = 1;
+		for (q = 0; q < n; ++q) cells += (int64_t)(e->hj[q].nl - 2) * e->hj[q].al;
+		if (trace_total > e->trace_budget) waves = (2 * trace_total + e->trace_budget - 1) / e->trace_budget;
+		pthread_once(&g_pair_share_once, pl_pair_share_init);
+		e->last_pairs = pl_form_pairs(e, opt, n, max_sub,
+				(int64_t)(g_pair_share * (double)cells / ((double)e->n_sm * e->ctas_per_sm[3][0] * (double)waves)), &P);
+	}
 	if (e->last_pairs > 0) /* the unit the waves are packed by is a pair: twice a job's trace */
 		for (q = 0; q < n; ++q)
 			if (e->hj[q].mode == 3 && e->hj[q].pair >= 0 &&
@@ -731,7 +756,7 @@ PL_EXPORT void pl_engine_set_graphs(pl_engine_t *e, int32_t enable) { if (e) e->
 
 PL_EXPORT int64_t pl_engine_graph_replays(const pl_engine_t *e) { return e ? e->g_replays : 0; }
 
-PL_EXPORT void pl_engine_set_pairing(pl_engine_t *e, int32_t enable) { if (e) e->pairing = enable != 0; }
+PL_EXPORT void pl_engine_set_pairing(pl_engine_t *e, int32_t enable) { if (e) e->pairing = enable == 2 ? 2 : enable != 0; }
 
 PL_EXPORT void pl_engine_set_tuning(pl_engine_t *e, int32_t r4_rows, double coop_ratio)
 {

@@ -87,99 +87,31 @@ struct DpShared {
 	/* per warp, double-buffered by strip parity: the codons, donor and acceptor
 	 * penalties of the warp's 32*R rows of a strip, staged ahead of the strip */
 	uint8_t rows[PLK_WARPS_PER_CTA][2][3][ROWBLK] __attribute__((aligned(16)));
-	uint64_t bar[PLK_WARPS_PER_CTA][2];                 /* per warp and buffer: completion of its bulk copies */
 };
 
-/* Row-input staging by the tensor memory accelerator.  The row inputs of the warp's
- * block of a strip, rows [b, b + 32R) -- codons nas[b..], donor[b-1..] and
- * acceptor[b-2..], 32R+2 bytes each -- are copied by lane 0 as 1-D bulk copies
- * (cp.async.bulk, global -> this CTA's shared memory) from the 16-byte boundary at
- * or below each start, cut at the first 16-byte boundary at or past the end of the
- * array (bytes past the end are never read: the readers apply the row bounds).
- * The preparation arrays sit inside a 16-byte aligned allocation with at least 16
- * bytes after the last one.  The copies of a buffer complete on the warp's mbarrier
- * of that buffer; the other 31 lanes issue nothing.
- *
- * `st` (per warp, in registers, kept across the jobs of a kernel): bits 0-1 the
- * parity of the next phase of each buffer's mbarrier, bits 2-3 the buffers with
- * copies in flight, bit 4 once a wait ran out (every later wait is skipped and the
- * jobs of the warp report status -3: the DP did not run on its inputs). */
-#define ROW_WAIT_NS 1000000000ull   /* a staging wait gives up after one second */
-
-__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void row_bar_init(uint64_t *bar)
+/* Stage the row inputs of the warp's block of a strip, rows [b, b + 32R): codons
+ * nas[b..], donor[b-1..] and acceptor[b-2..], 32R+2 bytes each.  Each block is
+ * copied as 16-byte cp.async chunks from the 16-byte boundary at or below its
+ * start; chunks that start past the end of their array are skipped (their bytes
+ * are never read: the readers apply the row bounds).  Lanes 1-31 issue the
+ * copies; lane 0 keeps its own cp.async queue for the strip hand-off ring.  The
+ * preparation arrays sit inside a 16-byte aligned allocation with at least 16
+ * bytes after the last one. */
+template <int R>
+__device__ __forceinline__ void stage_rows(uint8_t (*buf)[ROWBLK], const uint8_t *nas, const int8_t *donor,
+		const int8_t *acceptor, const int nl, const int b, const int lane)
 {
-	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(bar)), "r"(1) : "memory");
-}
-__device__ __forceinline__ void row_bar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-
-/* 16-byte aligned source and byte count (a multiple of 16, at most cap) of one array's block */
-__device__ __forceinline__ uint32_t row_span(const void *start, const void *end, uint32_t cap, const uint8_t *&src)
-{
-	src = (const uint8_t*)((uintptr_t)start & ~(uintptr_t)15);
-	const long long left = (long long)((const uint8_t*)end - src);
-	if (left <= 0) return 0u;
-	const uint32_t up = (uint32_t)((left + 15) & ~15ll);
-	return up < cap ? up : cap;
-}
-
-__device__ __forceinline__ void row_bulk(void *dst, const uint8_t *src, uint32_t bytes, uint64_t *bar)
-{
-	if (bytes) asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-			:: "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
-}
-
-/* lane 0: the blocks of NJ jobs (one window length) into buffers buf[j], completing on bar;
- * the arrays' addresses come from the job table (J[j]->prep_off, nl, al) */
-template <int R, int NJ>
-__device__ __noinline__ void stage_rows(uint8_t (*const *buf)[ROWBLK], uint64_t *bar, const uint8_t *prep,
-		plk_job_t *const *J, const int b)
-{
-	constexpr uint32_t CB = ((32 * R + 2 + 15 + 15) / 16) * 16;
-	static_assert(CB <= ROWBLK, "row block");
-	const uint8_t *src[3 * NJ];
-	uint32_t n[3 * NJ], total = 0;
+	constexpr int CH = (32 * R + 2 + 15 + 15) / 16;  /* chunks per block */
+	static_assert(CH * 16 <= ROWBLK, "row block");
+	if (lane == 0) return;
 #pragma unroll
-	for (int j = 0; j < NJ; ++j) {
-		const int nl = J[j]->nl, al = J[j]->al;
-		const uint8_t *nas = prep + J[j]->prep_off, *donor = nas + nl + al, *acceptor = donor + nl + 1;
-		n[3 * j] = row_span(nas + b, nas + nl, CB, src[3 * j]);
-		n[3 * j + 1] = row_span(donor + b - 1, donor + nl + 1, CB, src[3 * j + 1]);
-		n[3 * j + 2] = row_span(acceptor + b - 2, acceptor + nl + 1, CB, src[3 * j + 2]);
-		total += n[3 * j] + n[3 * j + 1] + n[3 * j + 2];
+	for (int g = lane - 1; g < 3 * CH; g += 31) {
+		const int a = g / CH, j = g - a * CH;
+		const uint8_t *s = a == 0 ? nas + b : (const uint8_t*)(a == 1 ? donor + b - 1 : acceptor + b - 2);
+		const uint8_t *end = a == 0 ? nas + nl : (const uint8_t*)(a == 1 ? donor : acceptor) + nl + 1;
+		const uint8_t *src = (const uint8_t*)((uintptr_t)s & ~(uintptr_t)15) + 16 * j;
+		if (src < end) cp_async16(buf[a] + 16 * j, src);
 	}
-	/* the buffer's earlier reads (generic proxy) before the copies' writes (async proxy) */
-	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_addr(bar)), "r"(total) : "memory");
-#pragma unroll
-	for (int j = 0; j < NJ; ++j)
-#pragma unroll
-		for (int a = 0; a < 3; ++a) row_bulk(buf[j][a], src[3 * j + a], n[3 * j + a], bar);
-}
-
-/* every lane: waits (bounded) for the copies into buffer q when they are in flight */
-__device__ __forceinline__ void rows_ready(uint64_t *bar, unsigned &st, const int q, plk_job_t *JA, plk_job_t *JB)
-{
-	if (!(st >> (2 + q) & 1u)) return;
-	st &= ~(4u << q);
-	if (st & 16u) return;
-	const uint32_t a = smem_addr(bar + q), parity = st >> q & 1u;
-	uint64_t t0;
-	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-	for (;;) {
-		uint32_t done;
-		asm volatile("{\n\t.reg .pred p;\n\t"
-		             "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-		             "selp.u32 %0, 1, 0, p;\n\t}"
-		             : "=r"(done) : "r"(a), "r"(parity) : "memory");
-		if (done) { st ^= 1u << q; return; }
-		uint64_t t;
-		asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-		if (t - t0 > ROW_WAIT_NS) break;
-	}
-	st |= 16u;
-	JA->status = -3;
-	if (JB) JB->status = -3;
 }
 
 
@@ -215,7 +147,7 @@ template <int NW, int R>
 __device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[R], const int ah1, const int ah2,
 		const int ah3, const bool row2, const int *__restrict__ sct_b, const int (&code)[R],
 		const int (&gi)[R], const int (&dn)[R + 2], const int (&ac)[R + 2],
-		int (&ip)[R], int (&lh)[R], const int (&ic)[R], const int *__restrict__ c16,
+		int (&ip)[R], int (&lh)[R], const int (&ic)[R], const int *__restrict__ c16, const int go_e, const int seg_i,
 		int (&o)[9], unsigned (&z)[R], int (&hn)[R])
 {
 	/* The integer pipe is the bound, so the update is written in the DPX forms that
@@ -237,9 +169,9 @@ __device__ __forceinline__ void cells_scaled(const int (&in)[9], int (&hm)[R], c
 		/* each extension flag is the sign of a difference: x > y exactly when y - x < 0
 		 * (|values| < 2^21, no overflow) */
 		/* 1: I -- p4 = I(c-1) > H'(c-1) - go */
-		const int t4 = __viaddmax_s32(lh[r], -GO, N16);
-		const int d4 = t4 - ip[r];
-		ip[r] = __vimax3_s32(t4 - GE, ip[r] - GE, N16);  /* max(max(t4, ip) - ge, floor) */
+		const int t4 = __viaddmax_s32(lh[r], go_e, N16);     /* go_e: -go, or below the floor at a segment start */
+		const int d4 = t4 - ip[r] - seg_i;
+		ip[r] = __vimax3_s32(t4 - GE, ip[r] + seg_i - GE, N16);  /* max(max(t4, ip) - ge, floor) */
 		/* 2: D -- p5 = D(i-3) > H(i-3) - go */
 		const int u5 = __viaddmax_s32(h3, -GO, N16);
 		const int d5 = u5 - d3;
@@ -381,7 +313,7 @@ __device__ __forceinline__ void cells_plain(const int (&in)[9], int (&hm)[R], co
 template <int MODE, int NW, int R>
 __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t *__restrict__ prep,
 		uint16_t *__restrict__ trace, int32_t *__restrict__ myring, DpShared &sh, const plk_params_t &P,
-		const int L, const int wib, unsigned &st)
+		const int L, const int wib)
 {
 	constexpr int NL = 32 * NW, HS = NL * R;
 	constexpr int SC = MODE == 0 ? 16 : 1;                  /* value scale of the mode */
@@ -409,36 +341,23 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 	for (int r = 0; r < R; ++r) ip[r] = lh[r] = ic[r] = hm[r] = NEG, code[r] = 0, gi[r] = 0;
 #pragma unroll
 	for (int r = 0; r < R + 2; ++r) dn[r] = ac[r] = 0;
-	uint64_t *bar = sh.bar[wib];
 	/* the first strip's row inputs, and the ring entry of the first strip (the -inf row) */
-	if (lane == 0) {
-		uint8_t (*const b0[1])[ROWBLK] = {rowbuf[0]};
-		plk_job_t *const JP[1] = {J};
-		stage_rows<R, 1>(b0, &bar[0], prep, JP, 2 + w * 32 * R);
-	}
-	st |= 4u;
+	stage_rows<R>(rowbuf[0], nas, donor, acceptor, nl, 2 + w * 32 * R, lane);
 	if (L == 0) {
 #pragma unroll
 		for (int q = 0; q < 9; ++q) pre[q] = NEG;
 	}
-	rows_ready(bar, st, 0, J, nullptr);
+	cp_async_wait_all();
 	__syncwarp();
 
 	for (int s = 0; s < total; ++s) {
 		if (__shfl_sync(FULL, c, 0) == 0) {
 			/* lane 0 of the warp starts a strip: the strip's row inputs (staged one
 			 * period ago) are visible after the wait; stage those of the next strip */
-			const int kn = (s - 32 * w) / Pc + 1;
-			rows_ready(bar, st, (kn - 1) & 1, J, nullptr);
+			cp_async_wait_all();
 			__syncwarp();
-			if (kn < nstrip) {
-				if (lane == 0) {
-					uint8_t (*const bn[1])[ROWBLK] = {rowbuf[kn & 1]};
-					plk_job_t *const JP[1] = {J};
-					stage_rows<R, 1>(bn, &bar[kn & 1], prep, JP, 2 + kn * HS + w * 32 * R);
-				}
-				st |= 4u << (kn & 1);
-			}
+			const int kn = (s - 32 * w) / Pc + 1;
+			if (kn < nstrip) stage_rows<R>(rowbuf[kn & 1], nas, donor, acceptor, nl, 2 + kn * HS + w * 32 * R, lane);
 		}
 		/* column state of the rows above: lane-1's output of the previous step */
 		int in[9];
@@ -476,25 +395,30 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 			ah1 = ah2 = ah3 = NEG;
 			cs = 0, dcol = L % al;
 		}
-		if (started && c < al && i0 < nl) {
+		const bool live = started && c < al && i0 < nl;
+		const bool any_seg = __any_sync(FULL, live && cs == 0);  /* some lane starts a segment this step */
+		if (live) {
 			const bool seg = cs == 0, first = c == 0, row2 = first && i0 == 2;
 			const int *sct_b = sh.sct + 22 * aas[c];
 			int hn[R];
 			unsigned z[R];
 			if (MODE == 0) {
-				/* the striped schedule's segment hand-over (nasw-sse.c:537-553): rare, so branched */
-				if (seg) {
+				/* the striped schedule's segment hand-over (nasw-sse.c:537-553): at a segment start
+				 * the carried insertion takes the hand-over candidates, and the first-pass H' and I
+				 * restart at -inf -- the cell reads them through go_e / seg_i, which push them below
+				 * the floor, so no lane branches on its own segment start */
+				const int go_e = seg ? -(1 << 28) : -c16[0], seg_i = seg ? -(1 << 28) : 0;
+				if (any_seg) {
+					const int goe_e = seg ? -GOE : -(1 << 28), ge_e = seg ? -GE16 : -(1 << 28);
 #pragma unroll
-					for (int r = 0; r < R; ++r) {
-						const int hop = max(lh[r] - GOE, NEG), iext = max(ip[r] - GE16, NEG);
-						ic[r] = max(max(hop, iext), max(ic[r] - GE16, NEG));
-						ip[r] = NEG, lh[r] = NEG;
-					}
+					for (int r = 0; r < R; ++r)
+						ic[r] = __viaddmax_s32(ic[r], -GE16, __viaddmax_s32(ip[r], ge_e, __viaddmax_s32(lh[r], goe_e, NEG)));
 				} else {
 #pragma unroll
 					for (int r = 0; r < R; ++r) ic[r] = max(ic[r] - GE16, NEG);
 				}
-				cells_scaled<NW, R>(in, hm, ah1, ah2, ah3, row2, sct_b, code, gi, dn, ac, ip, lh, ic, c16, o, z, hn);
+				cells_scaled<NW, R>(in, hm, ah1, ah2, ah3, row2, sct_b, code, gi, dn, ac, ip, lh, ic, c16, go_e, seg_i,
+						o, z, hn);
 			} else {
 				cells_plain<MODE, R>(in, hm, ah1, ah2, ah3, row2, seg, first, sct_b, code, gi, dn, ac, ip, lh, ic, P,
 						o, z, hn);
@@ -531,8 +455,6 @@ __device__ __forceinline__ void dp_job(plk_job_t *__restrict__ J, const uint8_t 
 		}
 	}
 	cp_async_wait_all();
-	rows_ready(bar, st, 0, J, nullptr);  /* no copies are in flight here; kept as a guard */
-	rows_ready(bar, st, 1, J, nullptr);
 	/* the final score H(nl-1, al-1): the lane holding row nl-1 in the last strip keeps
 	 * that strip's last column in hm */
 	{
@@ -560,10 +482,8 @@ k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop
 		const int b = x / 22, a = x % 22, v = P.sc[a * 22 + b];
 		sh.sct[x] = MODE == 0 ? v * 16 + 15 : v;
 	}
-	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-	if (lane == 0) row_bar_init(&sh.bar[wib][0]), row_bar_init(&sh.bar[wib][1]), row_bar_init_fence();
 	__syncthreads();
-	unsigned st = 0;
+	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
 	for (;;) {
 		if (threadIdx.x == 0) sh.job = atomicAdd(&counters[0], 1);
 		__syncthreads();
@@ -571,7 +491,7 @@ k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop
 		__syncthreads();
 		if (idx >= n_coop) break;
 		dp_job<MODE, PLK_WARPS_PER_CTA, R>(jobs + order_coop[idx], prep, trace,
-				ring + (int64_t)blockIdx.x * PLK_WARPS_PER_CTA * ring_stride, sh, P, threadIdx.x, wib, st);
+				ring + (int64_t)blockIdx.x * PLK_WARPS_PER_CTA * ring_stride, sh, P, threadIdx.x, wib);
 		__syncthreads();
 	}
 	int32_t *myring = ring + ((int64_t)blockIdx.x * PLK_WARPS_PER_CTA + wib) * ring_stride;
@@ -580,7 +500,7 @@ k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop
 		if (lane == 0) idx = atomicAdd(&counters[1], 1);
 		idx = __shfl_sync(FULL, idx, 0);
 		if (idx >= n_solo) break;
-		dp_job<MODE, 1, R>(jobs + order_solo[idx], prep, trace, myring, sh, P, lane, wib, st);
+		dp_job<MODE, 1, R>(jobs + order_solo[idx], prep, trace, myring, sh, P, lane, wib);
 		__syncwarp();
 	}
 }
@@ -620,14 +540,17 @@ struct DpSharedPair {
 	int32_t job;
 	int32_t pre[PLK_WARPS_PER_CTA][PLK_RING_INTS] __attribute__((aligned(16)));
 	uint8_t rows[PLK_WARPS_PER_CTA][2][2][3][ROWBLK] __attribute__((aligned(16)));  /* [warp][job][parity][array] */
-	uint64_t bar[PLK_WARPS_PER_CTA][2];  /* per warp and buffer parity: both jobs' copies */
 };
 #define PAIR_SCT_WORDS (22 * 22 * 22)   /* [protein residue][codon residue of job 1][of job 2] */
 
 __device__ __forceinline__ unsigned pk16(int a, int b) { return ((unsigned)a & 0xffffu) | ((unsigned)b << 16); }
-/* per-half maximum of two, as one add+max instruction (there is no two-input intrinsic; an
- * inline max.s16x2 cost registers) */
-__device__ __forceinline__ unsigned vmax2u(unsigned a, unsigned b) { return __viaddmax_s16x2(a, 0u, b); }
+/* per-half signed maximum of two */
+__device__ __forceinline__ unsigned vmax2u(unsigned a, unsigned b)
+{
+	unsigned d;
+	asm("max.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+	return d;
+}
 
 struct PairK { unsigned F2, GOn, GEn, IOn, FSn, GOEn, ONE, ONEFS; };
 
@@ -636,7 +559,8 @@ __device__ __forceinline__ void cells_pair(const unsigned (&in)[9], unsigned (&h
 		const unsigned ah2, const unsigned ah3, const bool row2, const unsigned r2h, const unsigned r2f,
 		const uint32_t *__restrict__ srow, const int (&cp)[R], const unsigned (&gi)[R], const unsigned (&dn)[R + 2],
 		const unsigned (&ac)[R + 2], unsigned (&ip)[R], unsigned (&lh)[R], const unsigned (&ic)[R], const PairK &K,
-		const plk_params_t &P, unsigned (&o)[9], unsigned (&z)[R], unsigned (&hn)[R])
+		const plk_params_t &P, const unsigned go_e, const unsigned seg_i, unsigned (&o)[9], unsigned (&z)[R],
+		unsigned (&hn)[R])
 {
 	unsigned h1 = in[0], h2 = in[1], h3 = in[2], d1 = in[3], d2 = in[4], d3 = in[5], va = in[6], vb = in[7], vc = in[8];
 #pragma unroll
@@ -646,8 +570,8 @@ __device__ __forceinline__ void cells_pair(const unsigned (&in)[9], unsigned (&h
 		unsigned h3m1 = r >= 3 ? hm[r - 3] : (r == 2 ? ah1 : (r == 1 ? ah2 : ah3));
 		if (r == 0 && row2) h1m1 = r2f, h2m1 = r2f, h3m1 = r2h; /* column -1 while row 2 is computed: {0, -fs, -fs} */
 		/* 1: I -- g4 = H'(c-1) - go >= I(c-1) */
-		const unsigned t4 = __viaddmax_s16x2(lh[r], K.GOn, K.F2);
-		const unsigned m4 = vmax2u(t4, ip[r]);
+		const unsigned t4 = __viaddmax_s16x2(lh[r], go_e, K.F2);  /* go_e: -go, or below the floor at a segment start */
+		const unsigned m4 = __viaddmax_s16x2(ip[r], seg_i, t4);
 		const unsigned ipn = __viaddmax_s16x2(m4, K.GEn, K.F2);
 		ip[r] = ipn;
 		/* 2: D -- g5 = H(i-3) - go >= D(i-3) */
@@ -716,7 +640,7 @@ template <int NW, int R>
 __device__ __forceinline__ void dp_pair(plk_job_t *__restrict__ JA, plk_job_t *__restrict__ JB,
 		const uint8_t *__restrict__ prep, uint16_t *__restrict__ trace, int32_t *__restrict__ myring,
 		DpSharedPair &sh, const uint32_t *__restrict__ sct2, const PairK &K, const plk_params_t &P,
-		const int L, const int wib, unsigned &st)
+		const int L, const int wib)
 {
 	constexpr int NL = 32 * NW, HS = NL * R;
 	const unsigned NEG = K.F2;
@@ -745,31 +669,23 @@ __device__ __forceinline__ void dp_pair(plk_job_t *__restrict__ JA, plk_job_t *_
 	for (int r = 0; r < R; ++r) ip[r] = lh[r] = ic[r] = hm[r] = NEG, cp[r] = 0, gi[r] = 0;
 #pragma unroll
 	for (int r = 0; r < R + 2; ++r) dn[r] = ac[r] = 0;
-	uint64_t *bar = sh.bar[wib];
-	plk_job_t *const JP[2] = {JA, JB};
-	if (lane == 0) {
-		uint8_t (*const b0[2])[ROWBLK] = {rowA[0], rowB[0]};
-		stage_rows<R, 2>(b0, &bar[0], prep, JP, 2 + w * 32 * R);
-	}
-	st |= 4u;
+	stage_rows<R>(rowA[0], nasA, donA, accA, nl, 2 + w * 32 * R, lane);
+	stage_rows<R>(rowB[0], nasB, donB, accB, nl, 2 + w * 32 * R, lane);
 	if (L == 0) {
 #pragma unroll
 		for (int q = 0; q < 9; ++q) pre[q] = (int32_t)NEG;
 	}
-	rows_ready(bar, st, 0, JA, JB);
+	cp_async_wait_all();
 	__syncwarp();
 
 	for (int s = 0; s < total; ++s) {
 		if (__shfl_sync(FULL, c, 0) == 0) {
-			const int kn = (s - 32 * w) / Pc + 1;
-			rows_ready(bar, st, (kn - 1) & 1, JA, JB);
+			cp_async_wait_all();
 			__syncwarp();
+			const int kn = (s - 32 * w) / Pc + 1;
 			if (kn < nstrip) {
-				if (lane == 0) {
-					uint8_t (*const bn[2])[ROWBLK] = {rowA[kn & 1], rowB[kn & 1]};
-					stage_rows<R, 2>(bn, &bar[kn & 1], prep, JP, 2 + kn * HS + w * 32 * R);
-				}
-				st |= 4u << (kn & 1);
+				stage_rows<R>(rowA[kn & 1], nasA, donA, accA, nl, 2 + kn * HS + w * 32 * R, lane);
+				stage_rows<R>(rowB[kn & 1], nasB, donB, accB, nl, 2 + kn * HS + w * 32 * R, lane);
 			}
 		}
 		unsigned in[9];
@@ -810,23 +726,27 @@ __device__ __forceinline__ void dp_pair(plk_job_t *__restrict__ JA, plk_job_t *_
 			ah1 = ah2 = ah3 = NEG;
 			cs = 0, dcol = L % al;
 		}
-		if (started && c < al && i0 < nl) {
+		const bool live = started && c < al && i0 < nl;
+		const bool any_seg = __any_sync(FULL, live && cs == 0);  /* some lane starts a segment this step */
+		if (live) {
 			const bool seg = cs == 0, first = c == 0, row2 = first && i0 == 2;
 			const uint32_t *srow = sct2 + 484 * aas[c];
 			unsigned hn[R], z[R];
-			/* the striped schedule's segment hand-over (nasw-sse.c:537-553) */
-			if (seg) {
+			/* the striped schedule's segment hand-over (nasw-sse.c:537-553), as in the 32-bit
+			 * kernel: an addend of 0x8000 per half sends a value below the floor (every value
+			 * is in [0, 0x7fff], so the sum is negative as a signed half) */
+			const unsigned go_e = seg ? 0x80008000u : K.GOn, seg_i = seg ? 0x80008000u : 0u;
+			if (any_seg) {
+				const unsigned goe_e = seg ? K.GOEn : 0x80008000u, ge_e = seg ? K.GEn : 0x80008000u;
 #pragma unroll
-				for (int r = 0; r < R; ++r) {
-					const unsigned hop = __viaddmax_s16x2(lh[r], K.GOEn, NEG), iext = __viaddmax_s16x2(ip[r], K.GEn, NEG);
-					ic[r] = __vimax3_s16x2(hop, iext, __viaddmax_s16x2(ic[r], K.GEn, NEG));
-					ip[r] = NEG, lh[r] = NEG;
-				}
+				for (int r = 0; r < R; ++r)
+					ic[r] = __viaddmax_s16x2(ic[r], K.GEn, __viaddmax_s16x2(ip[r], ge_e, __viaddmax_s16x2(lh[r], goe_e, NEG)));
 			} else {
 #pragma unroll
 				for (int r = 0; r < R; ++r) ic[r] = __viaddmax_s16x2(ic[r], K.GEn, NEG);
 			}
-			cells_pair<R>(in, hm, ah1, ah2, ah3, row2, r2h, r2f, srow, cp, gi, dn, ac, ip, lh, ic, K, P, o, z, hn);
+			cells_pair<R>(in, hm, ah1, ah2, ah3, row2, r2h, r2f, srow, cp, gi, dn, ac, ip, lh, ic, K, P, go_e, seg_i,
+					o, z, hn);
 			const int64_t toff = (((int64_t)k * al + dcol) * NL + L) * R;
 			store_trace_pair<R>(trA + toff, trB + toff, z);
 			if (L == NL - 1) {
@@ -858,8 +778,6 @@ __device__ __forceinline__ void dp_pair(plk_job_t *__restrict__ JA, plk_job_t *_
 		}
 	}
 	cp_async_wait_all();
-	rows_ready(bar, st, 0, JA, JB);  /* no copies are in flight here; kept as a guard */
-	rows_ready(bar, st, 1, JA, JB);
 	{ /* H(nl-1, al-1) of both jobs, unbiased */
 		const int rl = nl - 1 - i0;
 		if (rl >= 0 && rl < R) {
@@ -888,10 +806,8 @@ k_splice_pair(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_co
 	K.GOn = pk16(-P.go, -P.go), K.GEn = pk16(-P.ge, -P.ge), K.IOn = pk16(-P.io, -P.io);
 	K.FSn = pk16(-P.fs, -P.fs), K.GOEn = pk16(-(P.go + P.ge), -(P.go + P.ge));
 	K.ONE = 0x00010001u, K.ONEFS = pk16(1 - P.fs, 1 - P.fs);
-	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-	if (lane == 0) row_bar_init(&sh.bar[wib][0]), row_bar_init(&sh.bar[wib][1]), row_bar_init_fence();
 	__syncthreads();
-	unsigned st = 0;
+	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
 	for (;;) {
 		if (threadIdx.x == 0) sh.job = atomicAdd(&counters[0], 1);
 		__syncthreads();
@@ -900,7 +816,7 @@ k_splice_pair(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_co
 		if (idx >= n_coop) break;
 		plk_job_t *J = jobs + order_coop[idx];
 		dp_pair<PLK_WARPS_PER_CTA, R>(J, jobs + J->pair, prep, trace,
-				ring + (int64_t)blockIdx.x * PLK_WARPS_PER_CTA * ring_stride, sh, pair_sct, K, P, threadIdx.x, wib, st);
+				ring + (int64_t)blockIdx.x * PLK_WARPS_PER_CTA * ring_stride, sh, pair_sct, K, P, threadIdx.x, wib);
 		__syncthreads();
 	}
 	int32_t *myring = ring + ((int64_t)blockIdx.x * PLK_WARPS_PER_CTA + wib) * ring_stride;
@@ -910,7 +826,7 @@ k_splice_pair(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_co
 		idx = __shfl_sync(FULL, idx, 0);
 		if (idx >= n_solo) break;
 		plk_job_t *J = jobs + order_solo[idx];
-		dp_pair<1, R>(J, jobs + J->pair, prep, trace, myring, sh, pair_sct, K, P, lane, wib, st);
+		dp_pair<1, R>(J, jobs + J->pair, prep, trace, myring, sh, pair_sct, K, P, lane, wib);
 		__syncwarp();
 	}
 }

@@ -162,6 +162,8 @@ def load() -> C.CDLL:
                                       C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.POINTER(ExtraResult),
                                       C.POINTER(Feat), C.c_int64]
     lib.pl_extra_cal_host.restype = C.c_int
+    lib.pl_ps_band_cells.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+    lib.pl_ps_band_cells.restype = C.c_int64
     lib.pl_ps_gapped_host.argtypes = [C.c_void_p, C.POINTER(PsJob), C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
                                       C.c_int64, C.c_int32, C.c_int32, C.c_void_p]
     lib.pl_ps_gapped_host.restype = C.c_int
@@ -281,8 +283,9 @@ class Engine:
             self.lib.pl_engine_destroy(self.h)
             self.h = None
 
-    def set_pairing(self, on: bool):
-        self.lib.pl_engine_set_pairing(self.h, int(on))
+    def set_pairing(self, on):
+        """False: off; True: pairs within the per-CTA share of the batch; 2: every eligible job."""
+        self.lib.pl_engine_set_pairing(self.h, 2 if on == 2 else int(bool(on)))
 
     def last_pairs(self) -> int:
         return int(self.lib.pl_engine_last_pairs(self.h))

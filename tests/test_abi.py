@@ -82,3 +82,22 @@ def test_fault_hook_and_span_checks_without_a_device():
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         assert not lib.ns_ext_batch_init(None)
+
+
+def test_band_cells_closed_form_matches_the_row_sum():
+    """pl_ps_band_cells (the prescreen's cell count, summed in closed form) equals the sum of
+    the clipped band widths row by row, over bands, diagonals far left / right of the ORF and
+    tiny matrices."""
+    import numpy as np
+    lib = L.load()
+    rng = np.random.default_rng(5)
+    cases = [(1, 1, 0, 1), (5, 3, -10, 2), (5, 3, 10, 2), (0, 7, 0, 3), (7, 0, 0, 3), (9, 4, 2, 0), (9, 4, 2, -1)]
+    cases += [(int(rng.integers(0, 300)), int(rng.integers(0, 500)), int(rng.integers(-400, 600)),
+               int(rng.choice([1, 2, 8, 32, 64, 0, -3, 700]))) for _ in range(3000)]
+    for L_, n, d, b in cases:
+        want = 0
+        for i in range(L_):
+            lo, hi = (i + d - b, i + d + b) if b > 0 else (0, n - 1)
+            lo, hi = max(lo, 0), min(hi, n - 1)
+            want += max(0, hi - lo + 1)
+        assert lib.pl_ps_band_cells(L_, n, d, b) == want, (L_, n, d, b)

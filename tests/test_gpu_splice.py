@@ -345,10 +345,11 @@ def test_paired_int16x2_bit_exact(engine, oracle, seed):
         nt, aa = W.single_locus(seed=seed * 100 + q, al=int(rng.integers(120, 600)),
                                 window=int(rng.integers(2000, 9000)))
         pairs += [(nt, aa), (W.revcomp(nt), aa)]
-    got = _check(engine, oracle, opt, pairs)
-    assert engine.last_pairs() == len(pairs) // 2
-    engine.set_pairing(False)
+    engine.set_pairing(2)  # every eligible job, whatever the batch's size
     try:
+        got = _check(engine, oracle, opt, pairs)
+        assert engine.last_pairs() == len(pairs) // 2
+        engine.set_pairing(False)
         plain = engine.align_host(opt, pairs)
         assert engine.last_pairs() == 0
     finally:
@@ -367,20 +368,25 @@ def test_paired_golden_vectors_with_twins(engine, oracle, golden):
         if c["ss"]:
             continue
         by_opt.setdefault(repr(sorted(c["opt"].items())), []).append(c)
-    n = 0
-    for cases in by_opt.values():
-        opt = oracle.make_options(cases[0]["opt"])
-        cases = [c for c in cases if not oracle.port_lib().port_needs_wide(opt.ptr, len(c["aa"]))]
-        pairs = []
-        for c in cases:
-            pairs += [(c["nt"].encode(), c["aa"].encode())] * 2
-        got = engine.align_host(opt, pairs)
-        for k, c in enumerate(cases):
-            for t in range(2):
-                score, cig, _ = got[2 * k + t]
-                assert (score, cig) == (c["score"], c["cigar"]), (c["group"], len(c["nt"]), len(c["aa"]), score)
-                n += 1
-    assert n >= 300
+    n = n_pairs = 0
+    engine.set_pairing(2)
+    try:
+        for cases in by_opt.values():
+            opt = oracle.make_options(cases[0]["opt"])
+            cases = [c for c in cases if not oracle.port_lib().port_needs_wide(opt.ptr, len(c["aa"]))]
+            pairs = []
+            for c in cases:
+                pairs += [(c["nt"].encode(), c["aa"].encode())] * 2
+            got = engine.align_host(opt, pairs)
+            n_pairs += engine.last_pairs()
+            for k, c in enumerate(cases):
+                for t in range(2):
+                    score, cig, _ = got[2 * k + t]
+                    assert (score, cig) == (c["score"], c["cigar"]), (c["group"], len(c["nt"]), len(c["aa"]), score)
+                    n += 1
+    finally:
+        engine.set_pairing(True)
+    assert n >= 300 and n_pairs >= 100, (n, n_pairs)
 
 
 def test_paired_cooperative_and_waves(oracle):
@@ -396,9 +402,34 @@ def test_paired_cooperative_and_waves(oracle):
     eng = L.Engine(0, trace_budget_bytes=96 << 20)
     try:
         eng.set_tuning(0, 0.1)
+        eng.set_pairing(2)
         got = _check(eng, oracle, opt, pairs)
         plan = eng.last_plan()
         assert plan["waves"] >= 2 and plan["coop"] >= 2 and eng.last_pairs() == len(pairs) // 2, plan
+    finally:
+        eng.close()
+
+
+def test_pairs_within_the_per_cta_share(oracle):
+    """Default pairing: a batch of many small loci pairs them, while the two large loci whose
+    pair would exceed the batch's cells per CTA stay unpaired; a batch of a few large loci
+    forms no pairs.  Results equal the oracle's in both."""
+    rng = np.random.default_rng(26)
+    opt = Options(flag=NS_F_CIGAR)
+    small = []
+    for q in range(600):
+        nt, aa = W.random_pair(rng, max_al=30)
+        small += [(nt, aa), (W.revcomp(nt), aa)]
+    big = []
+    for q in range(2):
+        nt, aa = W.single_locus(seed=2600 + q, al=500, window=16000)
+        big += [(nt, aa), (W.revcomp(nt), aa)]
+    eng = L.Engine(0)
+    try:
+        _check(eng, oracle, opt, small + big)
+        assert eng.last_pairs() == len(small) // 2
+        _check(eng, oracle, opt, big)  # four jobs: each pair would be half the batch
+        assert eng.last_pairs() == 0
     finally:
         eng.close()
 
