@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--pairs", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--trace-budget-gb", type=float, default=0.0,
+                    help="traceback arena of the global DP's engine (0: the engine's default, 40%% of free memory "
+                         "up to 72 GB); a batch whose trace exceeds it runs in waves")
     ap.add_argument("--no-prefilter", action="store_true",
                     help="leave the learned-prefilter loci/s sub-object out of the headline line")
     ap.add_argument("--no-refgpu", action="store_true",
@@ -368,7 +371,7 @@ def main():
     cells = int(((nl.astype(np.int64) - 2) * al).sum())
     cells_all = R.sum(cells)  # units of the whole job (every rank takes this collective)
     opt = Options(flag=NS_F_CIGAR)
-    eng = L.Engine(local)
+    eng = L.Engine(local, int(args.trace_budget_gb * (1 << 30)))
     cap = n * 4096
     d_nt = torch.from_numpy(nt.copy()).to("cuda")
     d_aa = torch.from_numpy(aa.copy()).to("cuda")
@@ -524,6 +527,7 @@ def main():
                        "l2": "inputs and the per-step traceback arena (tens of GB) are far larger than L2",
                        "waves": plan["waves"], "coop_jobs": plan["coop"], "parallelism": f"{world} independent ranks",
                        "tuning": tuning, "int16x2_pairs": n_pairs,
+                       "trace_budget_gb": args.trace_budget_gb or "engine default (40% of free memory, <= 72)",
                        "graph_replays_in_timed_steps": replays},
             "e2e": e2e,
             "gpu_launches": int(launches),
@@ -745,9 +749,6 @@ def main_ext(args):
                                                "dp_ms": round(tm["dp_ms"] / args.steps, 3)}},
             "cpu_baseline": cpu,
             "clocks": clk,
-            "prefilter": pf,
-            "reference_gpu": refgpu,
-            "config0_latency": lat,
         }
         print(json.dumps(line), flush=True)
     R.close()

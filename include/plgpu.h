@@ -225,10 +225,10 @@ void pl_engine_last_plan(const pl_engine_t *e, int32_t *n_waves, int32_t *n_coop
  * window length -- the two strands of a locus -- run as a pair in the two halves of
  * the int16x2 DP kernel when their score range fits its 15-bit domain (on by
  * default; PLGPU_PAIR=0 or pl_engine_set_pairing(e, 0) turns it off).  With
- * enable = 1 a job pairs only when the pair's cells are at most PLGPU_PAIR_SHARE
- * (default 1) times the batch's cells per CTA and trace wave, so that a pair never
- * becomes a launch's longest unit (a batch too small to fill the GPU forms none);
- * enable = 2 pairs every eligible job.  Results are the same either way.
+ * enable = 1 the eligible jobs pair when they make at least PLGPU_PAIR_MIN (default 1)
+ * times as many pairs as the DP launch has warps (a batch too small to fill the GPU
+ * keeps its jobs single: a pair's unit of work is longer than a job's); enable = 2
+ * pairs every eligible job.  Results are the same either way.
  * pl_engine_last_pairs: pairs formed in the last batch. */
 void pl_engine_set_pairing(pl_engine_t *e, int32_t enable);
 int32_t pl_engine_last_pairs(const pl_engine_t *e);

@@ -99,7 +99,7 @@ template <int MODE>
 __device__ __forceinline__ void cells_ext(const int (&in)[9], const int (&hm)[PLK_ROWS], const int ah1, const int ah2,
 		const int ah3, const bool row2, const int (&sv)[PLK_ROWS], const int (&gim)[PLK_ROWS],
 		const int (&dnn)[PLK_ROWS + 2], const int (&acn)[PLK_ROWS + 2], int (&ip)[PLK_ROWS], int (&lh)[PLK_ROWS],
-		const int (&ic)[PLK_ROWS], const int NGO, const int NGE, const int NIO, const int NFS,
+		const int (&ic)[PLK_ROWS], const int GOI, const int NGO, const int NGE, const int NIO, const int NFS,
 		int (&o)[9], int (&hn)[PLK_ROWS])
 {
 	constexpr int R = PLK_ROWS, NEG = -32768;
@@ -113,26 +113,24 @@ __device__ __forceinline__ void cells_ext(const int (&in)[9], const int (&hm)[PL
 		if (r == 0 && row2) h1m1 = NFS, h2m1 = NFS, h3m1 = 0; /* column -1 while row 2 is computed: {0, -fs, -fs} */
 		int he, dnew, anew, bnew, cnew;
 		if (MODE == 0) {
-			he = max(h3m1 + sv[r], NEG);
-			ip[r] = max(max(lh[r] + NGO, ip[r]) + NGE, NEG);
-			he = max(he, ip[r]);
-			dnew = max(max(h3 + NGO, d3) + gim[r], NEG);
-			he = max(he, dnew);
-			const int u = max(h1 + NIO, NEG);
-			anew = max(u + dnn[r], va);
-			he = max(he, anew + acn[r + 2]);
-			const int u2 = max(h1m1 + NIO, NEG);
-			bnew = max(u2 + dnn[r + 1], vb);
-			he = max(he, bnew + acn[r]);
-			cnew = max(u2 + dnn[r + 2], vc);
-			he = max(he, cnew + acn[r + 1]);
-			he = max(he, h1 + NFS);
-			he = max(he, h2 + NFS);
-			he = max(he, h1m1 + NFS);
-			he = max(he, h2m1 + NFS);
+			/* one fused add+max (or three-way max) per step; the four frameshift
+			 * candidates share their penalty, so their maximum is taken first */
+			const int c0 = __viaddmax_s32(h3m1, sv[r], NEG);
+			ip[r] = __viaddmax_s32(__viaddmax_s32(lh[r], GOI, ip[r]), NGE, NEG);  /* GOI: -go, or -inf at a segment start */
+			dnew = __viaddmax_s32(__viaddmax_s32(h3, NGO, d3), gim[r], NEG);
+			he = __vimax3_s32(c0, ip[r], dnew);
+			const int u = __viaddmax_s32(h1, NIO, NEG);
+			anew = __viaddmax_s32(u, dnn[r], va);
+			const int u2 = __viaddmax_s32(h1m1, NIO, NEG);
+			bnew = __viaddmax_s32(u2, dnn[r + 1], vb);
+			cnew = __viaddmax_s32(u2, dnn[r + 2], vc);
+			he = __viaddmax_s32(anew, acn[r + 2], he);
+			he = __viaddmax_s32(bnew, acn[r], he);
+			he = __viaddmax_s32(cnew, acn[r + 1], he);
+			he = __viaddmax_s32(max(__vimax3_s32(h1, h2, h1m1), h2m1), NFS, he);
 		} else {
 			he = A::add(h3m1, sv[r]);
-			ip[r] = A::add(max(A::add(lh[r], NGO), ip[r]), NGE);
+			ip[r] = A::add(max(A::add(lh[r], GOI), ip[r]), NGE);
 			he = max(he, ip[r]);
 			dnew = A::add(max(A::add(h3, NGO), d3), gim[r]);
 			he = max(he, dnew);
@@ -244,14 +242,25 @@ __device__ __forceinline__ void ext_job(plk_ext_job_t *__restrict__ J, const uin
 			ah1 = ah2 = ah3 = NEG;
 			cs = 0;
 		}
-		if (started && c < ncol && i0 < nl) {
-			/* segment hand-over of the striped schedule (nasw-sse.c:432-433 and the lazy-F loop) */
-			if (cs == 0) {
+		const bool live = started && c < ncol && i0 < nl;
+		const bool any_seg = __any_sync(FULL, live && cs == 0);  /* some lane starts a segment this step */
+		/* the row maximum over the padding columns: with end_bonus >= 0 the real columns'
+		 * maximum is already in the key, so it is kept only on steps where some lane pads */
+		const bool track_rmax = __any_sync(FULL, live && c >= al) || P.end_bonus < 0;
+		if (live) {
+			/* segment hand-over of the striped schedule (nasw-sse.c:432-433 and the lazy-F loop):
+			 * the carried insertion takes the hand-over candidates, and the first-pass H' and I
+			 * restart at -inf -- H' through the cell's open penalty go_e, I by an addend that
+			 * sends it below every candidate -- with one warp-uniform branch per step (a strip's
+			 * first column needs no case of its own: its H', I and carried insertion are -inf) */
+			const bool seg = cs == 0;
+			const int go_e = seg ? -(1 << 28) : NGO;
+			if (any_seg) {
+				const int goe_e = seg ? NGOE : -(1 << 28), ge_e = seg ? NGE : -(1 << 28), seg_i = seg ? -(1 << 28) : 0;
 #pragma unroll
 				for (int r = 0; r < R; ++r) {
-					if (c == 0) ic[r] = NEG;
-					else ic[r] = max(max(Ar<MODE>::add(lh[r], NGOE), Ar<MODE>::add(ip[r], NGE)), Ar<MODE>::add(ic[r], NGE));
-					ip[r] = NEG, lh[r] = NEG;
+					ic[r] = max(Ar<MODE>::add(ic[r], NGE), max(Ar<MODE>::add(lh[r], goe_e), Ar<MODE>::add(ip[r], ge_e)));
+					ip[r] += seg_i;
 				}
 			} else {
 #pragma unroll
@@ -274,14 +283,15 @@ __device__ __forceinline__ void ext_job(plk_ext_job_t *__restrict__ J, const uin
 			}
 			int hn[R];
 			cells_ext<MODE>(in, hm, ah1, ah2, ah3, c == 0 && i0 == 2, sv, gim, dnn, acn, ip, lh, ic,
-					NGO, NGE, NIO, NFS, o, hn);
+					go_e, NGO, NGE, NIO, NFS, o, hn);
 			const KeyT kc = c < al - 1 ? (KeyT)(K::KW - 1 - c)
 				: c == al - 1 ? (KeyT)P.end_bonus * K::KW + (KeyT)(K::KW - 1 - c) : (KeyT)K::PAD;
+			if (track_rmax) {
 #pragma unroll
-			for (int r = 0; r < R; ++r) {
-				rmax[r] = max(rmax[r], hn[r]);
-				key[r] = max(key[r], (KeyT)hn[r] * K::KW + kc);
+				for (int r = 0; r < R; ++r) rmax[r] = max(rmax[r], hn[r]);
 			}
+#pragma unroll
+			for (int r = 0; r < R; ++r) key[r] = max(key[r], (KeyT)hn[r] * K::KW + kc);
 			if (glob && c == al - 1) { /* the global score H(nl-1, al-1) (nasw-sse.c:559) */
 				const int rl = nl - 1 - i0;
 #pragma unroll

@@ -388,36 +388,36 @@ static int pl_cmp_pair(const void *a, const void *b)
 	return x->idx - y->idx;
 }
 
-/* A pair is one unit of a persistent launch, twice a job's cells: pairing the largest jobs
- * of a batch would lengthen the launch's critical path (its longest unit), so a job pairs
- * only when the pair's cells stay within PLGPU_PAIR_SHARE (default 1) times the cells per
- * CTA of a wave: total cells / (CTAs x the waves the trace budget implies). */
-static double g_pair_share = 1.0;
-static pthread_once_t g_pair_share_once = PTHREAD_ONCE_INIT;
-static void pl_pair_share_init(void)
+/* A pair runs as one unit of work: one step of a pair costs about 1.7 steps of a single
+ * job and does two jobs' cells.  While a batch's units fill the GPU that is a gain;
+ * a batch with fewer units than the DP launch has warps would only make its units
+ * longer.  So pairs are formed only when there are at least PLGPU_PAIR_MIN (default 1)
+ * times as many of them as warps of a launch -- for every eligible job or none, since a
+ * single job and a pair run in different launches, one after the other.  pairing = 2
+ * pairs every eligible job. */
+static double g_pair_min = 1.0;
+static pthread_once_t g_pair_min_once = PTHREAD_ONCE_INIT;
+static void pl_pair_min_init(void)
 {
-	const char *v = getenv("PLGPU_PAIR_SHARE");
+	const char *v = getenv("PLGPU_PAIR_MIN");
 	if (v && *v) {
 		const double x = atof(v);
-		if (x > 0.0) g_pair_share = x;
+		if (x >= 0.0) g_pair_min = x;
 	}
 }
 
 /* Pairs of 16-bit jobs with one protein (the same aa_off) and one window length run as
- * mode 3 when each pair's cells are at most max_pair_cells; returns the number of pairs
- * formed (0 on a host allocation failure too). */
-static int32_t pl_form_pairs(pl_engine_t *e, const ns_opt_t *opt, int32_t n, int max_sub, int64_t max_pair_cells,
-		plk_params_t *P)
+ * mode 3; returns the number of pairs formed (0 on a host allocation failure too). */
+static int32_t pl_form_pairs(pl_engine_t *e, const ns_opt_t *opt, int32_t n, int max_sub, plk_params_t *P)
 {
 	pl_pkey_t *key;
 	int32_t q, m = 0, n_pairs = 0, al_cap = 0, bias = 0;
 	if (!e->pairing || n < 2 || !pl_pair_limits(opt, max_sub, &al_cap, &bias)) return 0;
-	if (e->pairing == 2) max_pair_cells = INT64_MAX;  /* every eligible job */
 	key = (pl_pkey_t*)malloc(sizeof(*key) * (size_t)n);
 	if (!key) return 0;
 	for (q = 0; q < n; ++q) {
 		const plk_job_t *J = &e->hj[q];
-		if (J->mode != 0 || J->al > al_cap || 2 * (int64_t)(J->nl - 2) * J->al > max_pair_cells) continue;
+		if (J->mode != 0 || J->al > al_cap) continue;
 		key[m].aa_off = J->aa_off, key[m].al = J->al, key[m].nl = J->nl, key[m].idx = q, ++m;
 	}
 	qsort(key, (size_t)m, sizeof(*key), pl_cmp_pair);
@@ -434,6 +434,13 @@ static int32_t pl_form_pairs(pl_engine_t *e, const ns_opt_t *opt, int32_t n, int
 		}
 	}
 	free(key);
+	pthread_once(&g_pair_min_once, pl_pair_min_init);
+	if (e->pairing == 1 && n_pairs > 0 &&
+			(double)n_pairs < g_pair_min * e->n_sm * e->ctas_per_sm[3][0] * PLK_WARPS_PER_CTA) {
+		for (q = 0; q < n; ++q)  /* too few to fill the GPU: every job single */
+			if (e->hj[q].mode == 3) e->hj[q].mode = 0, e->hj[q].pair = 0;
+		return 0;
+	}
 	P->pair_b = bias, P->pair_f = PL_PAIR_F;
 	return n_pairs;
 }
@@ -519,14 +526,7 @@ static int pl_run(pl_engine_t *e, const ns_opt_t *opt, const pl_splice_job_t *jo
 		pl_set_error("one job needs %lld trace bytes, over the budget of %lld", (long long)max_trace, (long long)e->trace_budget);
 		return 0;
 	}
-	{
-		int64_t cells = 0, waves = 1;
-		for (q = 0; q < n; ++q) cells += (int64_t)(e->hj[q].nl - 2) * e->hj[q].al;
-		if (trace_total > e->trace_budget) waves = (2 * trace_total + e->trace_budget - 1) / e->trace_budget;
-		pthread_once(&g_pair_share_once, pl_pair_share_init);
-		e->last_pairs = pl_form_pairs(e, opt, n, max_sub,
-				(int64_t)(g_pair_share * (double)cells / ((double)e->n_sm * e->ctas_per_sm[3][0] * (double)waves)), &P);
-	}
+	e->last_pairs = pl_form_pairs(e, opt, n, max_sub, &P);
 	if (e->last_pairs > 0) /* the unit the waves are packed by is a pair: twice a job's trace */
 		for (q = 0; q < n; ++q)
 			if (e->hj[q].mode == 3 && e->hj[q].pair >= 0 &&

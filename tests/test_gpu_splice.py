@@ -410,14 +410,14 @@ def test_paired_cooperative_and_waves(oracle):
         eng.close()
 
 
-def test_pairs_within_the_per_cta_share(oracle):
-    """Default pairing: a batch of many small loci pairs them, while the two large loci whose
-    pair would exceed the batch's cells per CTA stay unpaired; a batch of a few large loci
-    forms no pairs.  Results equal the oracle's in both."""
+def test_pairs_only_when_they_fill_the_gpu(oracle):
+    """Default pairing: 3000 small loci on both strands (more pairs than the DP launch has
+    warps) all pair; a batch of a few large loci keeps its jobs single.  Results equal the
+    oracle's in both."""
     rng = np.random.default_rng(26)
     opt = Options(flag=NS_F_CIGAR)
     small = []
-    for q in range(600):
+    for q in range(3000):
         nt, aa = W.random_pair(rng, max_al=30)
         small += [(nt, aa), (W.revcomp(nt), aa)]
     big = []
@@ -427,8 +427,8 @@ def test_pairs_within_the_per_cta_share(oracle):
     eng = L.Engine(0)
     try:
         _check(eng, oracle, opt, small + big)
-        assert eng.last_pairs() == len(small) // 2
-        _check(eng, oracle, opt, big)  # four jobs: each pair would be half the batch
+        assert eng.last_pairs() == len(small + big) // 2
+        _check(eng, oracle, opt, big)
         assert eng.last_pairs() == 0
     finally:
         eng.close()
