@@ -65,9 +65,10 @@ def parse():
     ap.add_argument("--pairs", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--trace-budget-gb", type=float, default=0.0,
-                    help="traceback arena of the global DP's engine (0: the engine's default, 40%% of free memory "
-                         "up to 72 GB); a batch whose trace exceeds it runs in waves")
+    ap.add_argument("--trace-budget-gb", type=float, default=110.0,
+                    help="traceback arena of the headline's engine (0: the engine's default, 40%% of free memory up to "
+                         "72 GB); the batch's 175 GB of trace runs in waves of half the arena on two streams: 110 GB "
+                         "gives four waves on a 180 GB B200")
     ap.add_argument("--no-prefilter", action="store_true",
                     help="leave the learned-prefilter loci/s sub-object out of the headline line")
     ap.add_argument("--no-refgpu", action="store_true",
