@@ -50,6 +50,7 @@ from protlocus_b200.ranks import Ranks, job_rate  # noqa: E402
 
 METRIC = "spliced-DP GCUPS (bit-exact) at 1 B200"
 DP_DRAM_BYTES_PER_CELL = 2.08  # ncu: k_splice_dp dram__bytes_read+write per cell (trace words are 2.0 B/cell)
+PAIR_DRAM_BYTES_PER_CELL = 2.20  # ncu: k_splice_pair<8>, uniform 4736x2000x250 (0.41 GB read + 6.54 GB written)
 OPS_PER_CELL = 65  # int16 lane-ops per cell with traceback bits, counted from nasw-sse.c:465-553
 WORKLOAD = ("batched global spliced DP: 4096 protein/window pairs x 2 strands = 8192 DPs with CIGAR; "
             "protein log-normal median 350 aa (50-2500), window uniform 1-50 kb, Poisson(4) introns, "
@@ -65,6 +66,8 @@ def parse():
     ap.add_argument("--pairs", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-hmm", action="store_true",
+                    help="headline: skip the profile-HMM genome-scan sub-object (1000 profiles, six frames)")
     ap.add_argument("--trace-budget-gb", type=float, default=110.0,
                     help="traceback arena of the headline's engine (0: the engine's default, 40%% of free memory up to "
                          "72 GB); the batch's 175 GB of trace runs in waves of half the arena on two streams: 110 GB "
@@ -519,6 +522,22 @@ def main():
                                       "sample": "the headline's CPU GCUPS converted at this set's mean cells per locus "
                                                 "(plain path on the CPU)"}
 
+    hmm = None
+    if rank == 0 and world == 1 and not args.no_hmm:  # the profile-HMM configuration, in its own process
+        try:
+            pr = subprocess.run([sys.executable, os.path.abspath(__file__), "--workload", "hmm", "--hmm-shape", "genome",
+                                 "--profiles", "1000", "--steps", "2", "--warmup", "1"], capture_output=True, text=True,
+                                timeout=900)
+            h = json.loads(pr.stdout.strip().splitlines()[-1]) if pr.returncode == 0 and pr.stdout.strip() else None
+            hmm = {k: h.get(k) for k in ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "e2e",
+                                         "gpu_launches", "cpu_baseline", "clocks")} if h else \
+                {"unavailable": f"child exited {pr.returncode}: {pr.stderr.strip()[-200:]}"}
+            if h:
+                hmm["roofline"] = {k: h["roofline"].get(k) for k in ("kernel", "achieved", "peak", "unit", "frac")}
+                hmm["config"] = {"workload": h["config"].get("workload")}
+        except Exception as ex:
+            hmm = {"unavailable": f"{type(ex).__name__}: {str(ex)[:200]}"}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
@@ -532,12 +551,14 @@ def main():
                        "graph_replays_in_timed_steps": replays},
             "e2e": e2e,
             "gpu_launches": int(launches),
-            "roofline": {"bound": "int", "kernel": "k_splice_dp", "achieved": achieved, "peak": peak,
-                         "unit": "lane-ops/s", "frac": achieved / peak if peak else None,
-                         "traffic": (int(DP_DRAM_BYTES_PER_CELL * tm["cells"] / tm["dp_launches"])
-                                     if tm["dp_launches"] else None),
-                         "traffic_source": "ncu dram bytes read+write of one k_splice_dp launch on the uniform "
-                                           "2400x2000x350 case (2.08 B/cell), scaled by this run's cells per launch",
+            "roofline": {"bound": "int", "kernel": "k_splice_pair" if n_pairs else "k_splice_dp", "achieved": achieved,
+                         "peak": peak, "unit": "lane-ops/s", "frac": achieved / peak if peak else None,
+                         "traffic": (int((PAIR_DRAM_BYTES_PER_CELL if n_pairs else DP_DRAM_BYTES_PER_CELL)
+                                         * tm["cells"] / tm["dp_launches"]) if tm["dp_launches"] else None),
+                         "traffic_source": ("ncu dram bytes read+write of one k_splice_pair launch on the uniform "
+                                            "4736x2000x250 case (2.20 B/cell)" if n_pairs else
+                                            "ncu dram bytes read+write of one k_splice_dp launch on the uniform "
+                                            "2400x2000x350 case (2.08 B/cell)") + ", scaled by this run's cells per launch",
                          "ops_per_cell": OPS_PER_CELL, "dp_kernel_gcups": round(dp_gcups, 3),
                          "peak_source": "measured live: pl_measure_int_peak (int32 %.3g, int16x2 %.3g lane-ops/s)"
                                         % (int32_peak, i16x2_peak),
@@ -548,6 +569,7 @@ def main():
             "clocks": clk,
             "prefilter": pf,
             "reference_gpu": refgpu,
+            "hmm": hmm,
             "config0_latency": lat,
         }
         print(json.dumps(line), flush=True)

@@ -13,6 +13,10 @@ hmm-gpu.o replaced by libplgpu) and protlocus_cuda (the reference's
   libplgpu: the PAF (with cs/cg tags) and GFF3 outputs must equal the CPU
   build's byte for byte, on protein and on HMM-profile queries (the profile
   path also reaches mp_hmm_dp_score_gpu_batch, hmm.c:324);
+* protlocus_learned (oracle/map_learned_hook.c) runs libplgpu's learned selector at
+  the mapper's candidate selection (`--gpu-prefilter` with PL_PF_MODEL set): keeping
+  every candidate it must print the plain mapper's output byte for byte, and with the
+  shipped model it must keep at least 99.5 % of the plain mapper's PAF lines verbatim;
 * `--gpu-prefilter` ranks candidates with the gapless X-drop score
   (map.c:1014-1090); there is no CPU build of it, so the reference's CUDA build
   is the reference: both programs keep the DP on the CPU and must print the
@@ -35,7 +39,8 @@ pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF = os.path.join(ROOT, "oracle", "_ref")
-CPU, PLGPU, CUDA = (os.path.join(REF, n) for n in ("protlocus_cpu", "protlocus_plgpu", "protlocus_cuda"))
+CPU, PLGPU, CUDA, LEARNED = (os.path.join(REF, n) for n in ("protlocus_cpu", "protlocus_plgpu", "protlocus_cuda",
+                                                            "protlocus_learned"))
 need = pytest.mark.skipif(not (os.path.exists(CPU) and os.path.exists(PLGPU)),
                           reason="oracle/_ref programs not built (needs the reference tree)")
 AA = "ACDEFGHIKLMNPQRSTVWY"
@@ -106,3 +111,39 @@ def test_program_gpu_prefilter(protein_inputs, topk):
     assert got == want
     got_dp, _ = run(PLGPU, ["--gpu", "--gpu-min-cells=0", *args, genome, prot])
     assert got_dp == want
+
+
+def _model_file(path, tau=None):
+    """The shipped prefilter model as the hook reads it: "hidden tau margin tau_fb n" then
+    n float32 parameters."""
+    z = np.load(os.path.join(ROOT, "protlocus_b200", "data", "prefilter.npz"))
+    p = np.ascontiguousarray(z["params"], np.float32)
+    t = float(z["tau"]) if tau is None else tau
+    with open(path, "wb") as f:
+        f.write(f"{int(z['hidden'])} {t!r} {int(z['margin'])} {float(z['tau_fb'])!r} {p.size}\n".encode())
+        f.write(p.tobytes())
+
+
+@need
+@pytest.mark.skipif(not os.path.exists(LEARNED), reason="oracle/_ref/protlocus_learned not built")
+def test_program_learned_selector(protein_inputs, tmp_path):
+    """The reference mapper with libplgpu's learned selector in place of its candidate
+    selection (map.c:1014-1089): every reported alignment is still the exact DP's, so a
+    threshold that keeps every candidate prints the plain mapper's output (no prefilter,
+    every coarse candidate aligned) byte for byte, and the shipped model keeps at least
+    99.5 % of the plain mapper's PAF lines verbatim while dropping candidates."""
+    genome, prot = protein_inputs
+    want, _ = run(PLGPU, [genome, prot])
+    keep_all = tmp_path / "keep_all.bin"
+    _model_file(keep_all, tau=0.0)
+    got_all, prof_all = run(LEARNED, ["--gpu-prefilter", genome, prot], env={"PL_PF_MODEL": str(keep_all)})
+    assert int(prof_all["prefilter_candidate"]) > 0
+    assert prof_all["prefilter_survivor"] == prof_all["prefilter_candidate"]
+    assert got_all == want
+    shipped = tmp_path / "shipped.bin"
+    _model_file(shipped)
+    got, prof = run(LEARNED, ["--gpu-prefilter", genome, prot], env={"PL_PF_MODEL": str(shipped)})
+    lines, out = want.splitlines(), set(got.splitlines())
+    kept = sum(1 for line in lines if line in out)
+    assert len(lines) >= 80 and kept >= 0.995 * len(lines), (kept, len(lines))
+    assert int(prof["prefilter_survivor"]) < int(prof["prefilter_candidate"]), prof
