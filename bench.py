@@ -895,7 +895,19 @@ def main_hmm(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
 
+    shared = len(dev_nt) == 1 and len(hp) > 1  # one region set for every profile: one call for all of them
+    if shared:
+        _, offs0, lens0 = batches[0]
+        d_all = torch.zeros(len(hp) * len(lens0), dtype=torch.int32, device="cuda")
+        handles = (C.c_void_p * len(hp))(*[p.h for p in hp])
+
     def step_device():
+        if shared:  # planned and translated once, the profiles' launches side by side (pl_hmm_score_many_device)
+            if not eng.lib.pl_hmm_score_many_device(eng.h, handles, len(hp), len(lens0), d_nt[0].data_ptr(),
+                                                    offs0.ctypes.data, lens0.ctypes.data, d_all.data_ptr(),
+                                                    stream.cuda_stream):
+                raise RuntimeError("pl_hmm_score_many_device: " + L.error())
+            return
         for p, (nt, offs, lens), dn, ds in zip(hp, batches, d_nt, d_sc):
             if not eng.lib.pl_hmm_score_device(eng.h, p.h, len(lens), dn.data_ptr(), offs.ctypes.data,
                                                lens.ctypes.data, ds.data_ptr(), stream.cuda_stream):
@@ -958,7 +970,7 @@ def main_hmm(args):
                "d2h_bytes_per_step": int(sum(4 * len(ln) for _, _, ln in batches)),
                "ms_per_step": round(te / args.steps * 1e3, 2), "api": "pl_hmm_score_host (C ABI, pinned host buffers)"}
         # parity of this run's scores with the device path
-        ref_sc = [ds.cpu().numpy() for ds in d_sc]
+        ref_sc = (list(d_all.cpu().numpy().reshape(len(hp), -1)) if shared else [ds.cpu().numpy() for ds in d_sc])
         if any((a != b).any() for a, b in zip(ref_sc, h_sc)):
             raise RuntimeError("host and device HMM scores differ")
 
@@ -982,7 +994,10 @@ def main_hmm(args):
                          "peak_source": "measured live: pl_measure_int_peak, int32 add+max chains (%.3g lane-ops/s)"
                                         % int32_peak,
                          "phase_ms_per_step": {"codons_ms": round(tm["prep_ms"] / args.steps, 3),
-                                               "dp_ms": round(tm["dp_ms"] / args.steps, 3)}},
+                                               "dp_ms": round(tm["dp_ms"] / args.steps, 3)},
+                         "api": "pl_hmm_score_many_device: every profile's launch side by side on the engine's HMM "
+                                "streams (dp_ms spans the translation and every launch)" if shared else
+                                "pl_hmm_score_device per profile"},
             "cpu_baseline": cpu,
             "clocks": clk,
         }

@@ -401,6 +401,13 @@ int pl_hmm_score_host(pl_engine_t *e, const pl_hmm_profile_t *p, int32_t n, cons
  * `stream` (NULL = the engine's); returns when done.  Returns 1 on success. */
 int pl_hmm_score_device(pl_engine_t *e, const pl_hmm_profile_t *p, int32_t n, const uint8_t *nt,
 		const int32_t *off, const int32_t *len, int32_t *score_dev, void *stream);
+/* n_prof profiles against one set of n regions (device nt; off/len on the host):
+ * score_dev[k * n + q] = profile k on region q.  The region tables are planned, uploaded
+ * and translated once, and the profiles' launches run side by side on the engine's HMM
+ * streams (a region set that fills only part of the GPU per profile then keeps it busy).
+ * Returns when done; 1 on success. */
+int pl_hmm_score_many_device(pl_engine_t *e, const pl_hmm_profile_t *const *ps, int32_t n_prof, int32_t n,
+		const uint8_t *nt, const int32_t *off, const int32_t *len, int32_t *score_dev, void *stream);
 /* DP cells (codon rows x m) of the last HMM batch of this engine. */
 int64_t pl_hmm_last_cells(const pl_engine_t *e);
 

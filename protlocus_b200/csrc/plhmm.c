@@ -23,6 +23,7 @@ struct pl_hmm_profile_s {
 	int device;
 	plk_hmm_prof_t k;      /* device tables */
 	uint8_t *codon_dev;    /* codon index -> HMMER column, 20 = no emission */
+	uint8_t codon[64];     /* the same, on the host */
 };
 
 PL_EXPORT pl_hmm_profile_t *pl_hmm_profile_create(int32_t device, int32_t m, const int16_t *emit,
@@ -45,6 +46,7 @@ PL_EXPORT pl_hmm_profile_t *pl_hmm_profile_create(int32_t device, int32_t m, con
 	for (k = 0; k < 7; ++k)
 		for (j = 0; j < mpad; ++j) t[(size_t)k * mpad + j] = j < m ? trans[(size_t)j * 7 + k] : -(1 << 28);
 	p->device = device, p->k.m = m, p->k.mpad = mpad;
+	memcpy(p->codon, codon_alpha, 64);
 	CK(cudaSetDevice(device));
 	CK(cudaMalloc((void**)&p->k.emit_t, sizeof(int16_t) * 21 * (size_t)mpad));
 	CK(cudaMalloc((void**)&p->k.trans_t, sizeof(int32_t) * 7 * (size_t)mpad));
@@ -78,6 +80,15 @@ void pl_hmm_engine_free(pl_engine_t *e)
 	dbuf_free(&e->h_off), dbuf_free(&e->h_len), dbuf_free(&e->h_rowoff), dbuf_free(&e->h_rows);
 	dbuf_free(&e->h_order), dbuf_free(&e->h_counter), dbuf_free(&e->h_edge), dbuf_free(&e->h_nt);
 	dbuf_free(&e->h_score);
+	{
+		int s;
+		for (s = 0; s < PL_HMM_STREAMS; ++s) {
+			dbuf_free(&e->h_edge_s[s]);
+			if (e->h_st[s]) cudaStreamDestroy(e->h_st[s]), e->h_st[s] = 0;
+		}
+		for (s = 0; s <= PL_HMM_STREAMS; ++s)
+			if (e->h_ev[s]) cudaEventDestroy(e->h_ev[s]), e->h_ev[s] = 0;
+	}
 	free(e->h_hbuf);
 	e->h_hbuf = 0, e->h_hcap = 0;
 }
@@ -173,6 +184,87 @@ PL_EXPORT int pl_hmm_score_device(pl_engine_t *e, const pl_hmm_profile_t *p, int
 	if (!e) { pl_set_error("no engine"); return 0; }
 	if (cudaSetDevice(e->device) != cudaSuccess) { pl_set_error("cudaSetDevice failed"); return 0; }
 	return pl_hmm_run(e, p, n, nt, off, len, score_dev, stream ? (cudaStream_t)stream : e->stream);
+}
+
+/* Many profiles against one region set: the planning, the upload of the region tables and
+ * the codon translation once (again only when a profile's codon table differs from the
+ * previous one's), then one DP launch per profile, round-robin on PL_HMM_STREAMS streams
+ * with their own queue counters and edge buffers, so that the launches of a region set too
+ * small to fill the GPU run side by side. */
+PL_EXPORT int pl_hmm_score_many_device(pl_engine_t *e, const pl_hmm_profile_t *const *ps, int32_t n_prof, int32_t n,
+		const uint8_t *nt, const int32_t *off, const int32_t *len, int32_t *score_dev, void *stream)
+{
+	int64_t *row_off, rows_total, cells = 0, rows_sum = 0;
+	int32_t *order, max_rows, q, k, s, warps;
+	const uint8_t *codon = 0;
+	cudaStream_t st;
+	if (!e) { pl_set_error("no engine"); return 0; }
+	if (n <= 0 || n_prof <= 0) return 1;
+	if (!ps || !off || !len || !nt || !score_dev) { pl_set_error("pl_hmm_score_many_device: missing argument"); return 0; }
+	for (k = 0; k < n_prof; ++k)
+		if (!ps[k] || ps[k]->device != e->device) { pl_set_error("profile %d missing or on another device", k); return 0; }
+	CK(cudaSetDevice(e->device));
+	st = stream ? (cudaStream_t)stream : e->stream;
+	if (!pl_hmm_plan(e, n, len, &row_off, &order, &rows_total, &max_rows)) return 0;
+	for (q = 0; q < n; ++q) rows_sum += len[q] >= 3 ? len[q] / 3 : 0;
+	warps = plk_hmm_warps_per_cta();
+	for (s = 0; s < PL_HMM_STREAMS; ++s)
+		if (!e->h_st[s]) CK(cudaStreamCreateWithFlags(&e->h_st[s], cudaStreamNonBlocking));
+	for (s = 0; s <= PL_HMM_STREAMS; ++s)
+		if (!e->h_ev[s]) CK(cudaEventCreateWithFlags(&e->h_ev[s], cudaEventDisableTiming));
+	if (!dbuf_ensure(&e->h_off, sizeof(int32_t) * (size_t)n) || !dbuf_ensure(&e->h_len, sizeof(int32_t) * (size_t)n) ||
+			!dbuf_ensure(&e->h_rowoff, sizeof(int64_t) * (size_t)n) || !dbuf_ensure(&e->h_order, sizeof(int32_t) * (size_t)n) ||
+			!dbuf_ensure(&e->h_rows, (size_t)(rows_total > 0 ? rows_total : 16)) ||
+			!dbuf_ensure(&e->h_counter, 64 * PL_HMM_STREAMS))
+		return 0;
+	CK(cudaMemcpyAsync(e->h_off.p, off, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+	CK(cudaMemcpyAsync(e->h_len.p, len, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+	CK(cudaMemcpyAsync(e->h_rowoff.p, row_off, sizeof(int64_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+	CK(cudaMemcpyAsync(e->h_order.p, order, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+	e->n_ev = 0;
+	PL_TIME(e, st, 1);
+	for (k = 0; k < n_prof; ++k) {
+		const pl_hmm_profile_t *p = ps[k];
+		int32_t ctas = plk_hmm_ctas_per_sm(p->k.mpad);
+		cudaStream_t sk;
+		if (ctas < 1) { pl_set_error("HMM DP kernel does not fit on an SM"); return 0; }
+		ctas *= e->n_sm;
+		if ((int64_t)ctas * warps > n) ctas = (n + warps - 1) / warps;
+		if (!codon || memcmp(codon, p->codon, 64) != 0) {  /* the rows of this codon table, then fork again */
+			if (codon) {  /* every launch reading the previous rows has finished */
+				for (s = 0; s < PL_HMM_STREAMS; ++s) {
+					CK(cudaEventRecord(e->h_ev[s], e->h_st[s]));
+					CK(cudaStreamWaitEvent(st, e->h_ev[s], 0));
+				}
+			}
+			CKK(plk_hmm_codons(nt, (const int32_t*)e->h_off.p, (const int32_t*)e->h_len.p, (const int64_t*)e->h_rowoff.p,
+					n, p->codon_dev, (uint8_t*)e->h_rows.p, st));
+			CK(cudaEventRecord(e->h_ev[PL_HMM_STREAMS], st));
+			for (s = 0; s < PL_HMM_STREAMS; ++s) CK(cudaStreamWaitEvent(e->h_st[s], e->h_ev[PL_HMM_STREAMS], 0));
+			codon = p->codon;
+		}
+		s = k % PL_HMM_STREAMS, sk = e->h_st[s];
+		if (!dbuf_ensure(&e->h_edge_s[s], (size_t)16 * 2 * (size_t)(max_rows + 1) * (size_t)ctas * warps)) return 0;
+		CKK(plk_hmm_dp(&p->k, (const uint8_t*)e->h_rows.p, (const int64_t*)e->h_rowoff.p, (const int32_t*)e->h_len.p,
+				(const int32_t*)e->h_order.p, n, (int32_t*)e->h_counter.p + 16 * s, e->h_edge_s[s].p,
+				(int64_t)max_rows + 1, ctas, score_dev + (int64_t)k * n, sk));
+		cells += rows_sum * p->k.m;
+	}
+	for (s = 0; s < PL_HMM_STREAMS; ++s) {  /* join */
+		CK(cudaEventRecord(e->h_ev[s], e->h_st[s]));
+		CK(cudaStreamWaitEvent(st, e->h_ev[s], 0));
+	}
+	PL_TIME(e, st, 1);
+	CK(cudaStreamSynchronize(st));
+	if (e->timing) {
+		float ms;
+		if (e->n_ev >= 2 && cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]) == cudaSuccess) e->acc_ms[1] += ms;
+		e->acc_dp_launches += n_prof, e->acc_cells += cells;
+	}
+	e->h_last_cells = cells;
+	return 1;
+fail:
+	return 0;
 }
 
 PL_EXPORT int pl_hmm_score_host(pl_engine_t *e, const pl_hmm_profile_t *p, int32_t n, const uint8_t *nt,

@@ -52,6 +52,12 @@ struct pl_engine_s {
 	int64_t x_cells_run, x_cells_nominal;
 	/* integer HMM DP */
 	dbuf_t h_off, h_len, h_rowoff, h_rows, h_order, h_counter, h_edge, h_nt, h_score;
+	/* several profiles at once: concurrent launches on PL_HMM_STREAMS streams, each with its
+	 * own queue counter and edge buffer */
+#define PL_HMM_STREAMS 4
+	cudaStream_t h_st[PL_HMM_STREAMS];
+	cudaEvent_t h_ev[PL_HMM_STREAMS + 1];
+	dbuf_t h_edge_s[PL_HMM_STREAMS];
 	void *h_hbuf;
 	size_t h_hcap;
 	int64_t h_last_cells;

@@ -101,6 +101,9 @@ def load() -> C.CDLL:
     lib.pl_hmm_score_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_void_p]
     lib.pl_hmm_score_device.restype = C.c_int
+    lib.pl_hmm_score_many_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.pl_hmm_score_many_device.restype = C.c_int
     lib.pl_hmm_last_cells.argtypes = [C.c_void_p]
     lib.pl_hmm_last_cells.restype = C.c_int64
     lib.mp_hmm_dp_score_gpu.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
@@ -555,6 +558,24 @@ class Engine:
                                           lens.ctypes.data, score.ctypes.data):
             raise RuntimeError("pl_hmm_score_host failed: " + error())
         return score[:n].tolist()
+
+    def hmm_score_many(self, profiles, regions) -> np.ndarray:
+        """pl_hmm_score_many_device: every profile against one region set (nt4 code arrays);
+        returns an int32 array [profile, region]."""
+        import torch
+        n = len(regions)
+        lens = np.array([len(r) for r in regions], dtype=np.int32)
+        offs = np.zeros(n, dtype=np.int32)
+        if n > 1:
+            offs[1:] = np.cumsum(lens[:-1])
+        nt = np.concatenate([np.asarray(r, dtype=np.uint8) for r in regions]) if n else np.zeros(1, np.uint8)
+        d_nt = torch.from_numpy(np.ascontiguousarray(nt)).to("cuda")
+        d_sc = torch.zeros(max(1, len(profiles) * n), dtype=torch.int32, device="cuda")
+        handles = (C.c_void_p * len(profiles))(*[p.h for p in profiles])
+        if not self.lib.pl_hmm_score_many_device(self.h, handles, len(profiles), n, d_nt.data_ptr(), offs.ctypes.data,
+                                                 lens.ctypes.data, d_sc.data_ptr(), None):
+            raise RuntimeError("pl_hmm_score_many_device failed: " + error())
+        return d_sc.cpu().numpy()[: len(profiles) * n].reshape(len(profiles), n)
 
     def gapless_score(self, w: dict, block_width: int, kmer: int, xdrop: int, mat, codon) -> np.ndarray:
         """pl_gapless_score_host on workload dict w: one int32 score per candidate."""

@@ -52,3 +52,26 @@ def test_hmm_reference_entry_without_hmm_c():
     """mp_hmm_dp_score_gpu reports "not taken" (INT32_MIN) when the program links no hmm.c accessors."""
     nt = np.zeros(30, dtype=np.uint8)
     assert L.load().mp_hmm_dp_score_gpu(None, nt.ctypes.data, 30) == -2 ** 31
+
+
+def test_hmm_many_profiles_equal_one_by_one(engine):
+    """pl_hmm_score_many_device (the region set planned and translated once, the profiles'
+    launches side by side on the engine's HMM streams) gives every profile's per-call scores:
+    nine profiles of 1-4 tiles (more than there are streams, so streams are reused), one
+    with another codon table (the rows are translated again), 60 regions of 0-2500 nt."""
+    ca = H.codon_alpha()
+    texts, probs = H.synthetic_profiles(9, seed=31, m_min=20, m_max=1000)
+    tabs = H.parse_hmmer3("".join(texts))
+    ca2 = ca.copy()
+    ca2[[3, 7, 11]] = 20  # three more codons without emission
+    profs = [L.HmmProfile(t["emit"], t["trans"], ca2 if k == 5 else ca) for k, t in enumerate(tabs)]
+    rng = np.random.default_rng(32)
+    regions = H.regions(rng, probs[0], 60, 0, 2500)
+    try:
+        many = engine.hmm_score_many(profs, regions)
+        for k, prof in enumerate(profs):
+            assert many[k].tolist() == engine.hmm_score(prof, regions), k
+        assert engine.lib.pl_hmm_last_cells(engine.h) == sum(len(r) // 3 for r in regions) * tabs[-1]["m"]
+    finally:
+        for prof in profs:
+            prof.close()

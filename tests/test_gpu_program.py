@@ -145,5 +145,7 @@ def test_program_learned_selector(protein_inputs, tmp_path):
     got, prof = run(LEARNED, ["--gpu-prefilter", genome, prot], env={"PL_PF_MODEL": str(shipped)})
     lines, out = want.splitlines(), set(got.splitlines())
     kept = sum(1 for line in lines if line in out)
+    print(f"learned selector: {kept} of {len(lines)} plain PAF lines kept verbatim, {len(out)} lines out; "
+          f"candidates {prof['prefilter_candidate']} -> {prof['prefilter_survivor']}")
     assert len(lines) >= 80 and kept >= 0.995 * len(lines), (kept, len(lines))
     assert int(prof["prefilter_survivor"]) < int(prof["prefilter_candidate"]), prof
