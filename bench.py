@@ -947,7 +947,18 @@ def main_hmm(args):
         h_sc = [np.zeros(len(ln), dtype=np.int32) for _, _, ln in batches]
         est = torch.cuda.ExternalStream(eng.stream)
 
+        if shared:
+            h_all = np.zeros((len(hp), len(lens0)), dtype=np.int32)
+
         def step_host():
+            if shared:  # the region set uploaded once for every profile (pl_hmm_score_many_host)
+                if not eng.lib.pl_hmm_score_many_host(eng.h, handles, len(hp), len(lens0), h_nt[0].data_ptr(),
+                                                      h_nt[0].numel(), offs0.ctypes.data, lens0.ctypes.data,
+                                                      h_all.ctypes.data):
+                    raise RuntimeError("pl_hmm_score_many_host: " + L.error())
+                for k in range(len(hp)):
+                    h_sc[k][:] = h_all[k]
+                return
             for p, (nt, offs, lens), hn, hs in zip(hp, batches, h_nt, h_sc):
                 if not eng.lib.pl_hmm_score_host(eng.h, p.h, len(lens), hn.data_ptr(), hn.numel(), offs.ctypes.data,
                                                  lens.ctypes.data, hs.ctypes.data):
@@ -965,10 +976,12 @@ def main_hmm(args):
         torch.cuda.synchronize()
         barrier()
         te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+        h2d = (batches[0][0].nbytes + 8 * len(lens0)) if shared else sum(nt.nbytes + 8 * len(ln) for nt, _, ln in batches)
         e2e = {"value": round(cells_all * args.steps / te / 1e9, 3), "unit": "GCUPS",
-               "h2d_bytes_per_step": int(sum(nt.nbytes + 8 * len(ln) for nt, _, ln in batches)),
+               "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(sum(4 * len(ln) for _, _, ln in batches)),
-               "ms_per_step": round(te / args.steps * 1e3, 2), "api": "pl_hmm_score_host (C ABI, pinned host buffers)"}
+               "ms_per_step": round(te / args.steps * 1e3, 2),
+               "api": ("pl_hmm_score_many_host" if shared else "pl_hmm_score_host") + " (C ABI, pinned host buffers)"}
         # parity of this run's scores with the device path
         ref_sc = (list(d_all.cpu().numpy().reshape(len(hp), -1)) if shared else [ds.cpu().numpy() for ds in d_sc])
         if any((a != b).any() for a, b in zip(ref_sc, h_sc)):

@@ -408,6 +408,9 @@ int pl_hmm_score_device(pl_engine_t *e, const pl_hmm_profile_t *p, int32_t n, co
  * Returns when done; 1 on success. */
 int pl_hmm_score_many_device(pl_engine_t *e, const pl_hmm_profile_t *const *ps, int32_t n_prof, int32_t n,
 		const uint8_t *nt, const int32_t *off, const int32_t *len, int32_t *score_dev, void *stream);
+/* The same from host buffers (nt of l_nt bytes uploaded once; score: n_prof x n). */
+int pl_hmm_score_many_host(pl_engine_t *e, const pl_hmm_profile_t *const *ps, int32_t n_prof, int32_t n,
+		const uint8_t *nt, int64_t l_nt, const int32_t *off, const int32_t *len, int32_t *score);
 /* DP cells (codon rows x m) of the last HMM batch of this engine. */
 int64_t pl_hmm_last_cells(const pl_engine_t *e);
 

@@ -267,6 +267,35 @@ fail:
 	return 0;
 }
 
+/* pl_hmm_score_many_device from host buffers: the region set uploaded once, the
+ * n_prof x n scores copied back. */
+PL_EXPORT int pl_hmm_score_many_host(pl_engine_t *e, const pl_hmm_profile_t *const *ps, int32_t n_prof, int32_t n,
+		const uint8_t *nt, int64_t l_nt, const int32_t *off, const int32_t *len, int32_t *score)
+{
+	cudaStream_t st;
+	int32_t q;
+	if (!e) { pl_set_error("no engine"); return 0; }
+	if (n <= 0 || n_prof <= 0) return 1;
+	for (q = 0; q < n; ++q)
+		if (off[q] < 0 || len[q] < 0 || (int64_t)off[q] + len[q] > l_nt) {
+			pl_set_error("region %d [%d, +%d) outside the %lld-byte buffer", q, off[q], len[q], (long long)l_nt);
+			return 0;
+		}
+	st = e->stream;
+	CK(cudaSetDevice(e->device));
+	if (!dbuf_ensure(&e->h_nt, (size_t)(l_nt > 0 ? l_nt : 1)) ||
+			!dbuf_ensure(&e->h_score, sizeof(int32_t) * (size_t)n * (size_t)n_prof))
+		return 0;
+	if (l_nt > 0) CK(cudaMemcpyAsync(e->h_nt.p, nt, (size_t)l_nt, cudaMemcpyHostToDevice, st));
+	if (!pl_hmm_score_many_device(e, ps, n_prof, n, (const uint8_t*)e->h_nt.p, off, len, (int32_t*)e->h_score.p, st))
+		return 0;
+	CK(cudaMemcpyAsync(score, e->h_score.p, sizeof(int32_t) * (size_t)n * (size_t)n_prof, cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	return 1;
+fail:
+	return 0;
+}
+
 PL_EXPORT int pl_hmm_score_host(pl_engine_t *e, const pl_hmm_profile_t *p, int32_t n, const uint8_t *nt,
 		int64_t l_nt, const int32_t *off, const int32_t *len, int32_t *score)
 {

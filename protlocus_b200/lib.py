@@ -104,6 +104,9 @@ def load() -> C.CDLL:
     lib.pl_hmm_score_many_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p]
     lib.pl_hmm_score_many_device.restype = C.c_int
+    lib.pl_hmm_score_many_host.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int64,
+                                           C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.pl_hmm_score_many_host.restype = C.c_int
     lib.pl_hmm_last_cells.argtypes = [C.c_void_p]
     lib.pl_hmm_last_cells.restype = C.c_int64
     lib.mp_hmm_dp_score_gpu.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]

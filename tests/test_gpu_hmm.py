@@ -8,6 +8,8 @@ library in test_gpu_dropin.py.  Added here: profiles of one to three 256-column
 tiles, regions with ambiguous codes, stop codons, lengths 0-5 and many regions
 per batch.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -69,6 +71,14 @@ def test_hmm_many_profiles_equal_one_by_one(engine):
     regions = H.regions(rng, probs[0], 60, 0, 2500)
     try:
         many = engine.hmm_score_many(profs, regions)
+        lens = np.array([len(r) for r in regions], dtype=np.int32)
+        offs = np.concatenate([[0], np.cumsum(lens[:-1])]).astype(np.int32)
+        nt = np.ascontiguousarray(np.concatenate(regions).astype(np.uint8))
+        host = np.zeros((len(profs), len(regions)), dtype=np.int32)
+        handles = (ctypes.c_void_p * len(profs))(*[p.h for p in profs])
+        assert engine.lib.pl_hmm_score_many_host(engine.h, handles, len(profs), len(regions), nt.ctypes.data, nt.size,
+                                                 offs.ctypes.data, lens.ctypes.data, host.ctypes.data), L.error()
+        assert np.array_equal(host, many)
         for k, prof in enumerate(profs):
             assert many[k].tolist() == engine.hmm_score(prof, regions), k
         assert engine.lib.pl_hmm_last_cells(engine.h) == sum(len(r) // 3 for r in regions) * tabs[-1]["m"]
