@@ -91,6 +91,38 @@ fail:
 void pl_ps_engine_free(pl_engine_t *e)
 {
 	dbuf_free(&e->s_jobs), dbuf_free(&e->s_pssm), dbuf_free(&e->s_orf), dbuf_free(&e->s_scr), dbuf_free(&e->s_score);
+	dbuf_free(&e->s_order);
+}
+
+/* The candidates the band kernel takes (plk_ps_band_ok), longest profile first (a counting
+ * sort on the profile length in 16-row buckets) so that the two candidates sharing a warp run
+ * about as many rows; key holds n int64 of host scratch and must outlive the upload (the
+ * callers free it after their final synchronisation). */
+#define PL_PS_BUCKETS 1024
+static int pl_ps_band_plan(pl_engine_t *e, const plk_ps_job_t *hj, int32_t n, int32_t go, int32_t ge, int64_t *key,
+		cudaStream_t st, plk_ps_args_t *a)
+{
+	int32_t q, m = 0, *ord = (int32_t*)key, cnt[PL_PS_BUCKETS + 1];
+	memset(cnt, 0, sizeof(cnt));
+	for (q = 0; q < n; ++q)
+		if (plk_ps_band_ok(hj[q].L, hj[q].n, hj[q].band, go, ge)) {
+			const int32_t b = hj[q].L >> 4 < PL_PS_BUCKETS - 1 ? hj[q].L >> 4 : PL_PS_BUCKETS - 1;
+			++cnt[PL_PS_BUCKETS - 1 - b + 1], ++m;
+		}
+	a->band_order = 0, a->n_band = m;
+	if (m == 0) return 1;
+	for (q = 0; q < PL_PS_BUCKETS; ++q) cnt[q + 1] += cnt[q];
+	for (q = 0; q < n; ++q)
+		if (plk_ps_band_ok(hj[q].L, hj[q].n, hj[q].band, go, ge)) {
+			const int32_t b = hj[q].L >> 4 < PL_PS_BUCKETS - 1 ? hj[q].L >> 4 : PL_PS_BUCKETS - 1;
+			ord[cnt[PL_PS_BUCKETS - 1 - b]++] = q;
+		}
+	if (!dbuf_ensure(&e->s_order, sizeof(int32_t) * (size_t)m)) return 0;
+	CK(cudaMemcpyAsync(e->s_order.p, ord, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, st));
+	a->band_order = (const int32_t*)e->s_order.p;
+	return 1;
+fail:
+	return 0;
 }
 
 /* Cells of one candidate's banded DP: rows i in [0, L) cover ORF positions
@@ -132,7 +164,7 @@ PL_EXPORT int pl_ps_gapped_host(pl_engine_t *e, const pl_ps_job_t *jobs, int32_t
 	int ok = 0;
 	if (!e) { pl_set_error("no engine"); return 0; }
 	if (n <= 0) return 1;
-	hj = (plk_ps_job_t*)malloc(sizeof(*hj) * (size_t)n);
+	hj = (plk_ps_job_t*)malloc((sizeof(*hj) + sizeof(int64_t)) * (size_t)n);  /* the job table, then the band plan's keys */
 	if (!hj) { pl_set_error("out of host memory"); return 0; }
 	for (q = 0; q < n; ++q) {
 		const pl_ps_job_t *J = &jobs[q];
@@ -161,6 +193,7 @@ PL_EXPORT int pl_ps_gapped_host(pl_engine_t *e, const pl_ps_job_t *jobs, int32_t
 	memset(&a, 0, sizeof(a));
 	a.jobs = (const plk_ps_job_t*)e->s_jobs.p, a.n = n, a.pssm = (const int8_t*)e->s_pssm.p;
 	a.orf = (const uint8_t*)e->s_orf.p, a.go = go, a.ge = ge, a.scratch = (int*)e->s_scr.p, a.score = (int32_t*)e->s_score.p;
+	if (!pl_ps_band_plan(e, hj, n, go, ge, (int64_t*)(hj + n), st, &a)) goto fail;
 	e->n_ev = 0;
 	PL_TIME(e, st, 1);
 	CKK(plk_ps_gapped(&a, st));
@@ -235,7 +268,7 @@ PL_EXPORT int pl_ps_gapped_device(pl_engine_t *e, const pl_ps_job_t *jobs, int32
 	int ok = 0;
 	if (!e) { pl_set_error("no engine"); return 0; }
 	if (n <= 0) return 1;
-	hj = (plk_ps_job_t*)malloc(sizeof(*hj) * (size_t)n);
+	hj = (plk_ps_job_t*)malloc((sizeof(*hj) + sizeof(int64_t)) * (size_t)n);  /* the job table, then the band plan's keys */
 	if (!hj) { pl_set_error("out of host memory"); return 0; }
 	for (q = 0; q < n; ++q) {
 		const pl_ps_job_t *J = &jobs[q];
@@ -256,6 +289,7 @@ PL_EXPORT int pl_ps_gapped_device(pl_engine_t *e, const pl_ps_job_t *jobs, int32
 	memset(&a, 0, sizeof(a));
 	a.jobs = (const plk_ps_job_t*)e->s_jobs.p, a.n = n, a.pssm = pssm, a.orf = orf, a.go = go, a.ge = ge;
 	a.scratch = (int*)e->s_scr.p, a.score = scores;
+	if (!pl_ps_band_plan(e, hj, n, go, ge, (int64_t*)(hj + n), st, &a)) goto fail;
 	e->n_ev = 0;
 	PL_TIME(e, st, 1);
 	CKK(plk_ps_gapped(&a, st));

@@ -76,7 +76,7 @@ struct pl_engine_s {
 	/* alignment statistics / exon features */
 	dbuf_t f_jobs, f_cig, f_nt, f_aa, f_pssm, f_mat, f_res, f_feat;
 	/* prescreen banded alignment */
-	dbuf_t s_jobs, s_pssm, s_orf, s_scr, s_score;
+	dbuf_t s_jobs, s_pssm, s_orf, s_scr, s_score, s_order;
 	/* anchor chaining */
 	dbuf_t c_off, c_n, c_order, c_a, c_f, c_p, c_v, c_t, c_counter;
 	void *c_host;           /* pinned host buffer for the fill's f and p (grow-only) */

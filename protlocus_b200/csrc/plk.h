@@ -267,8 +267,25 @@ typedef struct {
 	int32_t go, ge;
 	int *scratch;
 	int32_t *score;
+	/* the candidates the band kernel takes (plk_ps_band_ok), longest profile first; the
+	 * wavefront kernel skips them.  n_band = 0: the wavefront kernel takes every one. */
+	const int32_t *band_order;
+	int64_t n_band;
 } plk_ps_args_t;
 int plk_ps_gapped(const plk_ps_args_t *a, void *stream);
+/* the band kernel's candidates: a band of at most PLK_PS_BAND_W cells per row (16 lanes x 5),
+ * a profile and an ORF, and gap penalties with go >= ge >= 0 (its horizontal-gap scan relies
+ * on an open costing at least an extension) */
+#define PLK_PS_BAND_W 80
+#ifdef __CUDACC__
+#define PLK_HD __host__ __device__
+#else
+#define PLK_HD
+#endif
+static inline PLK_HD int plk_ps_band_ok(int32_t L, int32_t n, int32_t band, int32_t go, int32_t ge)
+{
+	return L > 0 && n > 0 && band > 0 && 2 * band + 1 <= PLK_PS_BAND_W && go >= ge && ge >= 0;
+}
 
 /* anchor chaining DP (chain.c:160-208): thread g takes query order[g], anchors a[off[q] ..
  * off[q] + n[q]); f, p, v per anchor out, t per anchor scratch (mark stamps) */

@@ -45,6 +45,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_ps_gapped(plk_ps_args_t A)
 	const int64_t q = (int64_t)blockIdx.x * WARPS + wib;
 	if (q >= A.n) return;
 	const plk_ps_job_t J = A.jobs[q];
+	if (A.n_band > 0 && plk_ps_band_ok(J.L, J.n, J.band, A.go, A.ge)) return;  /* the band kernel's */
 	const int8_t *pssm = A.pssm + J.pssm_off;
 	const uint8_t *orf = A.orf + J.orf_off;
 	const int L = J.L, n = J.n, diag = J.diag, band = J.band, go = A.go, ge = A.ge;
@@ -107,6 +108,94 @@ __global__ void __launch_bounds__(32 * WARPS) k_ps_gapped(plk_ps_args_t A)
 	if (lane == 0) A.score[q] = best;
 }
 
+/*
+ * Band kernel: 16 lanes per candidate (two per warp, consecutive in the longest-first
+ * order, so the halves of a warp run about as many rows), the band of a row across the
+ * lanes, rows in turn.  In band coordinates (u = t - (i + diag - band), 0 <= u < 2*band+1)
+ * the cell (i, u) needs row i-1's H at u (the diagonal) and its H and F at u+1 (above),
+ * so lane l keeps, for its five slots u = 5l..5l+4, the H/F the reference's row arrays
+ * hold at column i + diag - band - 1 + u before row i: one shuffle brings slot u+1 of the
+ * lane's last cell, and slots past the band hold the arrays' untouched 0 / -inf.  A cell
+ * outside the ORF is not computed and takes the value from u+1 (the arrays keep it).  The
+ * horizontal gap of a row is a prefix maximum across the band: with go >= ge a gap opened
+ * from a cell whose H came from a horizontal gap never beats extending that gap, so
+ *   e(u) = max over computed v < u of (max(H'(v), 0) + v*ge) - go - (u-1)*ge,
+ * H' being the cell's value before the horizontal gap, exactly the reference's e of
+ * prescreen.c:373; the row's first cell gets -inf as there.
+ */
+constexpr int BC = 5;                  /* band cells per lane */
+constexpr int BL = 16;                 /* lanes per candidate */
+static_assert(BC * BL == PLK_PS_BAND_W, "band width");
+
+__global__ void __launch_bounds__(32 * WARPS) k_ps_band(plk_ps_args_t A)
+{
+	const int lane = threadIdx.x & 31, half = lane >> 4, l = lane & 15;
+	const unsigned hm = 0xffffu << (16 * half);
+	const int64_t slot = ((int64_t)blockIdx.x * WARPS + (threadIdx.x >> 5)) * 2 + half;
+	if (slot >= A.n_band) return;  /* the whole half-warp leaves together */
+	const int q = A.band_order[slot];
+	const plk_ps_job_t J = A.jobs[q];
+	const int8_t *pssm = A.pssm + J.pssm_off;
+	const uint8_t *orf = A.orf + J.orf_off;
+	const int L = J.L, n = J.n, diag = J.diag, band = J.band, go = A.go, ge = A.ge, W = 2 * band + 1;
+	int SH[BC], SF[BC], ug[BC];  /* ug: u * ge of the lane's slots */
+#pragma unroll
+	for (int c = 0; c < BC; ++c) SH[c] = 0, SF[c] = NEG, ug[c] = (BC * l + c) * ge;
+	const int goe = go - ge;
+	int best = 0;
+	for (int i = 0; i < L; ++i) {
+		const int base = i + diag - band;
+		if (base > n - 1) break;          /* this band and every later one lie right of the ORF */
+		if (base + W - 1 < 0) continue;   /* left of the ORF: nothing computed yet, the slots hold 0 / -inf */
+		int nh = __shfl_down_sync(hm, SH[0], 1, BL), nf = __shfl_down_sync(hm, SF[0], 1, BL);
+		if (l == BL - 1) nh = 0, nf = NEG;
+		const int8_t *prow = pssm + (int64_t)i * 22;
+		const int t0 = base + BC * l;                    /* the lane's first column */
+		const int c_lo = -t0, c_hi = min(W - 1 - BC * l, n - 1 - t0);  /* its valid slots: c_lo <= c <= c_hi */
+		const uint8_t *orow = orf + t0;
+		int hh[BC], fc[BC], P[BC];
+		bool v[BC];
+#pragma unroll
+		for (int c = 0; c < BC; ++c) {
+			const int hup = c + 1 < BC ? SH[c + 1] : nh, fup = c + 1 < BC ? SF[c + 1] : nf;
+			v[c] = c >= c_lo && c <= c_hi;
+			int g = NEG;
+			hh[c] = 0, fc[c] = NEG;
+			if (v[c]) {
+				const int h0 = SH[c] + __ldg(prow + __ldg(orow + c));
+				fc[c] = max(fup - ge, hup - go);
+				hh[c] = max(h0, fc[c]);
+				g = max(hh[c], 0) + ug[c];
+			}
+			P[c] = c == 0 ? g : max(P[c - 1], g);  /* inclusive prefix inside the lane */
+		}
+		/* exclusive prefix maximum of the lanes' totals across the half-warp */
+		int x = P[BC - 1];
+#pragma unroll
+		for (int off = 1; off < BL; off <<= 1) {
+			const int y = __shfl_up_sync(hm, x, off, BL);
+			if (l >= off) x = max(x, y);
+		}
+		int ex = __shfl_up_sync(hm, x, 1, BL);
+		if (l == 0) ex = NEG;
+		int nSH[BC], nSF[BC];
+#pragma unroll
+		for (int c = 0; c < BC; ++c) {
+			const int pre = c == 0 ? ex : max(ex, P[c - 1]);
+			const int e = pre - goe - ug[c];  /* pre - go - (u - 1) * ge */
+			const int h = max(max(hh[c], e), 0);
+			if (v[c]) best = max(best, h);
+			nSH[c] = v[c] ? h : (c + 1 < BC ? SH[c + 1] : nh);
+			nSF[c] = v[c] ? fc[c] : (c + 1 < BC ? SF[c + 1] : nf);
+		}
+#pragma unroll
+		for (int c = 0; c < BC; ++c) SH[c] = nSH[c], SF[c] = nSF[c];
+	}
+#pragma unroll
+	for (int o = 8; o >= 1; o >>= 1) best = max(best, __shfl_xor_sync(hm, best, o, BL));
+	if (l == 0) A.score[q] = best;
+}
+
 }  // namespace
 
 extern "C" int plk_ps_gapped(const plk_ps_args_t *a, void *stream)
@@ -114,5 +203,10 @@ extern "C" int plk_ps_gapped(const plk_ps_args_t *a, void *stream)
 	if (a->n <= 0) return 0;
 	k_ps_gapped<<<(unsigned)((a->n + WARPS - 1) / WARPS), 32 * WARPS, 0, (cudaStream_t)stream>>>(*a);
 	plk_add_launches(1);
+	if (a->n_band > 0) {
+		const int64_t warps = (a->n_band + 1) / 2;
+		k_ps_band<<<(unsigned)((warps + WARPS - 1) / WARPS), 32 * WARPS, 0, (cudaStream_t)stream>>>(*a);
+		plk_add_launches(1);
+	}
 	return (int)cudaGetLastError();
 }

@@ -78,3 +78,37 @@ def test_ps_gapped_device_entry_equals_host_entry():
         assert np.array_equal(d_score.cpu().numpy()[: pk["n"]], want)
     finally:
         eng.close()
+
+
+@pytest.mark.gpu
+@need_ref
+@pytest.mark.parametrize("go,ge", [(11, 1), (5, 2), (3, 3), (4, 0), (2, 5)])
+def test_ps_band_kernel_matches_reference(go, ge):
+    """Bands of at most 80 cells go to the 16-lane band kernel when go >= ge >= 0 (the others,
+    and go < ge, to the wavefront kernel): 2000 candidates of every band width up to 39 and
+    beyond, diagonals from far left of the ORF to far right, against the reference."""
+    rng = np.random.default_rng(40 + go * 7 + ge)
+    cands = []
+    for q in range(2000):
+        Lq = int(rng.integers(1, 300))
+        pssm = rng.integers(-9, 8, size=(Lq, 22)).astype(np.int8)
+        nq = int(rng.integers(1, 500))
+        orf = rng.integers(0, 22, size=nq).astype(np.uint8)
+        diag = int(rng.integers(-Lq - 60, nq + 60))
+        if q % 2 == 0 and nq > 40 and Lq > 40:
+            d0 = int(rng.integers(-Lq // 2, nq // 2))
+            t = np.arange(Lq) + d0
+            ok = (t >= 0) & (t < nq) & (rng.random(Lq) < 0.8)
+            orf[t[ok]] = np.argmax(pssm[np.arange(Lq)[ok]], axis=1).astype(np.uint8)
+            diag = d0 + int(rng.integers(-3, 4))
+        band = int(rng.choice([1, 2, 8, 16, 32, 32, 39, 40, 0]))
+        cands.append((pssm, orf, diag, band))
+    eng = L.Engine(0)
+    try:
+        got = eng.ps_gapped(cands, go, ge)
+    finally:
+        eng.close()
+    want = np.array([O.ref_ps_gapped(p, o, d, b, go, ge) for p, o, d, b in cands])
+    bad = np.nonzero(got != want)[0]
+    assert len(bad) == 0, [(int(i), cands[i][0].shape[0], cands[i][1].size, cands[i][2], cands[i][3], int(got[i]),
+                            int(want[i])) for i in bad[:5]]
