@@ -17,6 +17,9 @@ hmm-gpu.o replaced by libplgpu) and protlocus_cuda (the reference's
   the mapper's candidate selection (`--gpu-prefilter` with PL_PF_MODEL set): keeping
   every candidate it must print the plain mapper's output byte for byte, and with the
   shipped model it must keep at least 99.5 % of the plain mapper's PAF lines verbatim;
+* protlocus_recheck_gpu (oracle/recheck_gpu_hook.c) is the reference's recheck program
+  scoring its peptides through libplgpu's Forward: its output and per-candidate table
+  must equal the stock program's byte for byte;
 * `--gpu-prefilter` ranks candidates with the gapless X-drop score
   (map.c:1014-1090); there is no CPU build of it, so the reference's CUDA build
   is the reference: both programs keep the DP on the CPU and must print the
@@ -41,6 +44,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF = os.path.join(ROOT, "oracle", "_ref")
 CPU, PLGPU, CUDA, LEARNED = (os.path.join(REF, n) for n in ("protlocus_cpu", "protlocus_plgpu", "protlocus_cuda",
                                                             "protlocus_learned"))
+RC_CPU, RC_GPU = (os.path.join(REF, n) for n in ("protlocus_recheck_cpu", "protlocus_recheck_gpu"))
 need = pytest.mark.skipif(not (os.path.exists(CPU) and os.path.exists(PLGPU)),
                           reason="oracle/_ref programs not built (needs the reference tree)")
 AA = "ACDEFGHIKLMNPQRSTVWY"
@@ -149,3 +153,53 @@ def test_program_learned_selector(protein_inputs, tmp_path):
           f"candidates {prof['prefilter_candidate']} -> {prof['prefilter_survivor']}")
     assert len(lines) >= 80 and kept >= 0.995 * len(lines), (kept, len(lines))
     assert int(prof["prefilter_survivor"]) < int(prof["prefilter_candidate"]), prof
+
+
+@pytest.fixture(scope="module")
+def recheck_inputs(tmp_path_factory):
+    """Candidates of an HMM-library mapping run with --trans (PAF + ##STA peptide lines) of 40
+    synthetic profiles against a genome holding one planted copy of each, and the profiles
+    with a STATS LOCAL FORWARD calibration on two of every three (the rest get no E-value)."""
+    d = tmp_path_factory.mktemp("recheck")
+    texts, probs = H.synthetic_profiles(40, seed=41, m_min=60, m_max=500, concentration=1.0)
+    rng = np.random.default_rng(42)
+    prots = ["".join(AA[rng.choice(20, p=row / row.sum())] for row in pm) for pm in probs]
+    g, _ = W.genome_fasta(0, seed=43, n_contigs=6, contig_len=200_000, proteins=prots, divergence=0.15)
+    (d / "genome.fa").write_text(g)
+    (d / "q.hmm").write_text("".join(texts))
+    out, k = [], 0
+    for line in "".join(texts).splitlines(True):
+        out.append(line)
+        if line.startswith("ALPH"):
+            if k % 3 != 2:
+                out.append(f"STATS LOCAL FORWARD    {60 + 4 * k:.4f}  0.0{5 + k % 5}\n")
+            k += 1
+    (d / "q_stats.hmm").write_text("".join(out))
+    p = subprocess.run([CPU, "-t8", "--trans", str(d / "genome.fa"), str(d / "q.hmm")], capture_output=True,
+                       text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    (d / "cand.paf").write_text(p.stdout)
+    return str(d / "q_stats.hmm"), str(d / "cand.paf"), d
+
+
+@need
+@pytest.mark.skipif(not (os.path.exists(RC_CPU) and os.path.exists(RC_GPU)), reason="recheck programs not built")
+@pytest.mark.parametrize("extra", [[], ["-n"], ["-e", "1e-30"]])
+def test_program_recheck_gpu(recheck_inputs, extra):
+    """The reference's recheck program with its Forward scoring on libplgpu prints the stock
+    program's passing lines (and, with -a, the failing ones with their scores) and writes
+    its per-candidate table (bits, bias, E-value, pass) byte for byte; with the null2
+    correction off too, and at a threshold that fails part of the candidates."""
+    hmm, cand, d = recheck_inputs
+    outs = []
+    for prog in (RC_CPU, RC_GPU):
+        tsv = d / (os.path.basename(prog) + "".join(extra) + ".tsv")
+        p = subprocess.run([prog, "-t", "8", "-a", "-T", str(tsv), *extra, hmm, cand], capture_output=True, text=True,
+                           timeout=600)
+        assert p.returncode == 0, p.stderr[-2000:]
+        outs.append((p.stdout, tsv.read_text()))
+    (want, want_tsv), (got, got_tsv) = outs
+    rows = want_tsv.splitlines()[1:]
+    assert len(rows) >= 30 and sum(1 for r in rows if r.split("\t")[4] != ".") >= 30, want_tsv[:500]
+    assert got_tsv == want_tsv
+    assert got == want
