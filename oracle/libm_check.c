@@ -3,7 +3,8 @@
  * checker of the restated glibc algorithms in protlocus_b200/csrc/glibc_mathf.cuh
  * (which the device's recheck Forward uses in rc_logsum, recheck.c:260-265).
  *
- *   lm_mismatch: runs the header's host build and the host libm over float bit
+ *   lm_mismatch: runs the header's host build (fn 0 expf, 1 log1pf, 2 and 3 their
+ *                branch-free forms for rc_logsum's ranges) and the host libm over float bit
  *                patterns lo, lo+stride, ... < hi and counts the results that differ
  *                in any bit (NaN results compare equal to NaN);
  *   lm_host:     fills out[] with the host libm's values at n bit patterns, for the
@@ -17,8 +18,13 @@
 
 #define LM_EXPORT __attribute__((visibility("default")))
 
-static float lm_host_fn(int fn, float x) { return fn == 0 ? expf(x) : log1pf(x); }
-static float lm_port_fn(int fn, float x) { return fn == 0 ? gl_expf(x) : gl_log1pf(x); }
+/* fn 0 / 1: gl_expf / gl_log1pf; fn 2 / 3: their branch-free forms for rc_logsum's ranges,
+ * gl_expf_rng (|x| < 88) and gl_log1pf_unit (0 <= x <= 1), checked on those ranges */
+static float lm_host_fn(int fn, float x) { return (fn & 1) == 0 ? expf(x) : log1pf(x); }
+static float lm_port_fn(int fn, float x)
+{
+	return fn == 0 ? gl_expf(x) : fn == 1 ? gl_log1pf(x) : fn == 2 ? gl_expf_rng(x) : gl_log1pf_unit(x);
+}
 
 LM_EXPORT int64_t lm_mismatch(int fn, uint32_t lo, uint32_t hi, uint32_t stride, uint32_t *first_bad)
 {

@@ -193,4 +193,118 @@ GLM_FN float gl_log1pf(float x)
 	                GLM_FSUB(GLM_FSUB(hfsq, GLM_FADD(GLM_FMUL(s, GLM_FADD(hfsq, R)), GLM_FADD(GLM_FMUL(kf, ln2_lo), c))), f));
 }
 
+/*
+ * Branch-free forms for rc_logsum's arguments, which lie in narrow ranges: expf of
+ * mn - mx in [-50, 0] and log1pf of its result in [0, 1].  Without branches, lanes
+ * with different arguments do not diverge and a thread can keep several logsums in
+ * flight.  Each returns the same bits as the function above on its range (every
+ * path's value is formed by the same operations, then selected); the checks cover
+ * every float of both ranges, on the host and on the device.
+ */
+
+/* a / b for 1 <= b <= 2.5 and |a| <= 1 (a zero or normal), correctly rounded, with no
+ * branch and no conversion on the device: a reciprocal estimate refined by one Newton
+ * step, the quotient, and Markstein's correction with a fused multiply-add (the
+ * remainder a - q*b is exact for q this close to a/b; P. Markstein, IBM J. Res. Dev.
+ * 34(1), 1990).  gl_log1pf_unit's two quotients (f / (2 + f) and c / (1 + x)) are
+ * checked equal to the correctly rounded ones at every float x of [0, 1] through
+ * the function's whole result, against the host libm. */
+GLM_FN float glm_div(float a, float b)
+{
+#if defined(__CUDA_ARCH__)
+	float r;
+	asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
+	r = __fmaf_rn(__fmaf_rn(-b, r, 1.0f), r, r);
+	const float q = __fmul_rn(a, r);
+	return __fmaf_rn(__fmaf_rn(-q, b, a), r, q);
+#else
+	return a / b;
+#endif
+}
+
+/* c ? a : b for floats, as a select on the device (both operands are computed, so no
+ * branch splits independent evaluations) */
+GLM_FN float glm_self(int c, float a, float b)
+{
+#if defined(__CUDA_ARCH__)
+	float r;
+	asm("{\n\t.reg .pred p;\n\tsetp.ne.s32 p, %1, 0;\n\tselp.f32 %0, %2, %3, p;\n\t}" : "=f"(r) : "r"(c), "f"(a), "f"(b));
+	return r;
+#else
+	return c ? a : b;
+#endif
+}
+
+/* gl_expf for |x| < 88 (rc_logsum: [-50, 0]), where its special cases never apply;
+ * tab is the 2^(j/32) table (a copy in shared memory on the device) */
+GLM_FN float gl_expf_rng_t(float x, const uint64_t *tab)
+{
+	const double inv_ln2_32 = 0x1.71547652b82fep+0 * 32, shift = 0x1.8p+52;
+	const double c0 = 0x1.c6af84b912394p-5 / 32 / 32 / 32, c1 = 0x1.ebfce50fac4f3p-3 / 32 / 32,
+	             c2 = 0x1.62e42ff0c52d6p-1 / 32;
+	const double xd = (double)x;
+	double kd = GLM_DFMA(inv_ln2_32, xd, shift);
+	const uint64_t ki = glm_d2u(kd);
+	kd = GLM_DSUB(kd, shift);
+	const double r = GLM_DFMA(inv_ln2_32, xd, -kd);
+	const uint64_t t = tab[ki % 32] + (ki << 47);
+	const double s = glm_u2d(t);
+	const double z = GLM_DFMA(c0, r, c1), r2 = GLM_DMUL(r, r);
+	double y = GLM_DFMA(c2, r, 1.0);
+	y = GLM_DFMA(z, r2, y);
+	y = GLM_DMUL(y, s);
+	return GLM_D2F(y);
+}
+
+GLM_FN float gl_expf_rng(float x)
+{
+#if defined(__CUDA_ARCH__)
+	return gl_expf_rng_t(x, glm_exp2_tab_dev);
+#else
+	return gl_expf_rng_t(x, glm_exp2_tab_host);
+#endif
+}
+
+/* gl_log1pf for 0 <= x <= 1: the paths of gl_log1pf that this range reaches (x below
+ * 2^-29; k = 0 below 0.41422; 1+x = 2^k (1+f) above, with the |f| < 2^-20 cases),
+ * each evaluated with gl_log1pf's operations, the result selected */
+GLM_FN float gl_log1pf_unit(float x)
+{
+	const float ln2_hi = 6.9313812256e-01f, ln2_lo = 9.0580006145e-06f;
+	const float lp1 = 6.6666668653e-01f, lp2 = 4.0000000596e-01f, lp3 = 2.8571429849e-01f,
+	            lp4 = 2.2222198546e-01f, lp5 = 1.8183572590e-01f, lp6 = 1.5313838422e-01f,
+	            lp7 = 1.4798198640e-01f;
+	const int32_t hx = (int32_t)glm_f2u(x);
+	const int small = hx < 0x3ed413d7, tiny = hx < 0x31000000;
+	const float r_tiny = glm_self(hx < 0x24800000, x, GLM_FSUB(x, GLM_FMUL(GLM_FMUL(x, x), 0.5f)));
+	/* 1 + x = 2^k (1 + f) with the rounding correction c / u */
+	const float u1 = GLM_FADD(1.0f, x);
+	const int32_t hu1 = (int32_t)glm_f2u(u1), k1 = (hu1 >> 23) - 127, m = hu1 & 0x007fffff;
+	const float c1 = glm_div(k1 > 0 ? GLM_FSUB(1.0f, GLM_FSUB(u1, x)) : GLM_FSUB(x, GLM_FSUB(u1, 1.0f)), u1);
+	const int hi_m = m >= 0x3504f7;
+	const float uL = glm_u2f((uint32_t)m | (hi_m ? 0x3f000000u : 0x3f800000u));
+	const int32_t k = small ? 0 : (hi_m ? k1 + 1 : k1), hu = small ? 1 : (hi_m ? (0x00800000 - m) >> 2 : m);
+	const float f = glm_self(small, x, GLM_FSUB(uL, 1.0f)), c = glm_self(small, 0.0f, c1);
+	const float hfsq = GLM_FMUL(GLM_FMUL(0.5f, f), f), kf = k == 0 ? 0.0f : (k == 1 ? 1.0f : 2.0f);  /* k <= 2 */
+	/* |f| < 2^-20 */
+	const float r_f0 = glm_self(k == 0, 0.0f, GLM_FADD(GLM_FMUL(kf, ln2_hi), GLM_FADD(c, GLM_FMUL(kf, ln2_lo))));
+	const float R0 = GLM_FMUL(hfsq, GLM_FSUB(1.0f, GLM_FMUL(0.66666666666666666f, f)));
+	const float r_fs = glm_self(k == 0, GLM_FSUB(f, R0),
+	                            GLM_FSUB(GLM_FMUL(kf, ln2_hi), GLM_FSUB(GLM_FSUB(R0, GLM_FADD(GLM_FMUL(kf, ln2_lo), c)), f)));
+	/* the polynomial */
+	const float s = glm_div(f, GLM_FADD(2.0f, f)), z = GLM_FMUL(s, s);
+	float R = GLM_FMUL(lp7, z);
+	R = GLM_FMUL(z, GLM_FADD(lp6, R));
+	R = GLM_FMUL(z, GLM_FADD(lp5, R));
+	R = GLM_FMUL(z, GLM_FADD(lp4, R));
+	R = GLM_FMUL(z, GLM_FADD(lp3, R));
+	R = GLM_FMUL(z, GLM_FADD(lp2, R));
+	R = GLM_FMUL(z, GLM_FADD(lp1, R));
+	const float sR = GLM_FMUL(s, GLM_FADD(hfsq, R));
+	const float r_p = glm_self(k == 0, GLM_FSUB(f, GLM_FSUB(hfsq, sR)),
+	                           GLM_FSUB(GLM_FMUL(kf, ln2_hi), GLM_FSUB(GLM_FSUB(hfsq, GLM_FADD(sR, GLM_FADD(GLM_FMUL(kf, ln2_lo), c))), f)));
+	const float r = glm_self(hu == 0, glm_self(f == 0.0f, r_f0, r_fs), r_p);
+	return glm_self(tiny, r_tiny, r);
+}
+
 #endif

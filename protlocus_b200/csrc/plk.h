@@ -165,18 +165,23 @@ typedef struct {
 /* one peptide */
 typedef struct {
 	int64_t dsq_off;      /* residue codes 0-20 */
-	int64_t scratch_off;  /* float offset of the null2 scratch: 4*(L+1)*(M+1) + 6*(L+1) floats */
 	int32_t len, prof, null2, pad;
 	/* the per-peptide logarithms of the length model, computed with the host's logf
 	 * (recheck.c:289-290, :321, :433-434) so that they carry the host libm's bits */
 	float lmove, lloop, logL, null1;
 } plk_rc_pep_t;
-#define PLK_RC_MAX_C 64                 /* columns per lane: profiles up to 32*64 = 2048 positions */
-#define PLK_RC_MAX_M (32 * PLK_RC_MAX_C)
+/* a group: up to 32 peptides of one profile, one per lane of a warp, their DP
+ * matrices interleaved by lane in a scratch region of plk_rc_group_floats floats */
+typedef struct {
+	int64_t scratch_off;  /* float offset of the region, a multiple of 4 */
+	int32_t first, count; /* its peptides: order[first .. first + count) */
+	int32_t prof, lmax;   /* the profile and the longest peptide */
+	int32_t full, pad;    /* full: some peptide takes null2, so every M/I row is kept */
+} plk_rc_grp_t;
+#define PLK_RC_MAX_M 2048
+int64_t plk_rc_group_floats(int32_t lmax, int32_t M, int32_t full);
 int plk_rc_forward(const plk_rc_prof_t *prof, const plk_rc_pep_t *pep, const uint8_t *dsq, const int32_t *order,
-		int32_t n, int32_t *counter, float *scratch, float *bits, float *bias, int32_t max_m, int32_t n_sm,
-		void *stream);
-int plk_rc_smem_per_warp(int32_t max_m);
+		const plk_rc_grp_t *grp, int32_t n_grp, float *scratch, float *bits, float *bias, void *stream);
 /* CTAs of the DP kernel that fit on one SM at once (occupancy) */
 int plk_dp_ctas_per_sm(int32_t mode, int32_t rows);
 uint64_t plk_launches(void);

@@ -4,11 +4,13 @@
  *
  * Profiles are the search profiles recheck.c builds (rc_prof_t's msc / tsc,
  * recheck.c:66-72 and :197-249), uploaded once with pl_rc_profile_create.  A
- * batch scores peptides against their own profiles; with null2 every peptide
- * needs scratch of 4*(L+1)*(M+1) + 6*(L+1) floats (the Forward and Backward M/I
- * rows and the special states of every row), and a batch whose
- * scratch exceeds the engine's budget runs in waves.  As in recheck.c, the
- * null2 correction is skipped for a pair above 2^25 DP cells
+ * batch scores peptides against their own profiles, one peptide per lane: the
+ * peptides of a profile, longest first, go in groups of up to 32 (one warp each),
+ * and the groups run longest first.  A group's DP matrices are interleaved by lane
+ * in one scratch region (plk_rc_group_floats: with null2 the Forward and Backward
+ * M/I rows of every row, 4*(lmax+1)*(M+1) floats per lane, else two rows), and a
+ * batch whose groups exceed the engine's budget runs in waves on the stream.  As
+ * in recheck.c, the null2 correction is skipped for a pair above 2^25 DP cells
  * (RC_NULL2_MAXCELLS, recheck.c:273).
  */
 #define _POSIX_C_SOURCE 200809L
@@ -59,7 +61,7 @@ PL_EXPORT void pl_rc_profile_destroy(pl_rc_profile_t *p)
 void pl_rc_engine_free(pl_engine_t *e)
 {
 	dbuf_free(&e->r_prof), dbuf_free(&e->r_pep), dbuf_free(&e->r_dsq), dbuf_free(&e->r_order);
-	dbuf_free(&e->r_counter), dbuf_free(&e->r_scratch), dbuf_free(&e->r_bits), dbuf_free(&e->r_bias);
+	dbuf_free(&e->r_grp), dbuf_free(&e->r_scratch), dbuf_free(&e->r_bits), dbuf_free(&e->r_bias);
 }
 
 typedef struct { int64_t key; int32_t idx; } pl_rkey_t;
@@ -70,14 +72,27 @@ static int pl_rkey_cmp(const void *a, const void *b)
 	return x->idx - y->idx;
 }
 
+/* peptides by profile, longest first within a profile (the lanes of a group then run
+ * about as many rows) */
+typedef struct { int32_t prof, len, idx; } pl_rpep_t;
+static int pl_rpep_cmp(const void *a, const void *b)
+{
+	const pl_rpep_t *x = (const pl_rpep_t*)a, *y = (const pl_rpep_t*)b;
+	if (x->prof != y->prof) return x->prof - y->prof;
+	if (x->len != y->len) return y->len - x->len;
+	return x->idx - y->idx;
+}
+
 PL_EXPORT int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *profiles, int32_t n_prof, int32_t n,
 		const int32_t *prof_id, const uint8_t *dsq, int64_t dsq_len, const int64_t *off, const int32_t *len,
 		int32_t do_null2, float *bits, float *bias)
 {
 	plk_rc_prof_t *hp = 0;
 	plk_rc_pep_t *pep = 0;
-	pl_rkey_t *key = 0;
-	int32_t *order = 0, q, max_m = 1;
+	pl_rpep_t *rp = 0;
+	pl_rkey_t *gk = 0;
+	plk_rc_grp_t *grp = 0, *gs = 0;
+	int32_t *order = 0, q, n_grp = 0;
 	int64_t budget, cells_total = 0;
 	cudaStream_t st;
 	int ok = 0;
@@ -87,13 +102,15 @@ PL_EXPORT int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *pro
 	CK(cudaSetDevice(e->device));
 	hp = (plk_rc_prof_t*)malloc(sizeof(*hp) * (size_t)(n_prof > 0 ? n_prof : 1));
 	pep = (plk_rc_pep_t*)calloc((size_t)n, sizeof(*pep));
-	key = (pl_rkey_t*)malloc(sizeof(*key) * (size_t)n);
+	rp = (pl_rpep_t*)malloc(sizeof(*rp) * (size_t)n);
 	order = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
-	if (!hp || !pep || !key || !order) { pl_set_error("out of host memory"); goto fail; }
+	grp = (plk_rc_grp_t*)calloc((size_t)n, sizeof(*grp));
+	gs = (plk_rc_grp_t*)calloc((size_t)n, sizeof(*gs));
+	gk = (pl_rkey_t*)malloc(sizeof(*gk) * (size_t)n);
+	if (!hp || !pep || !rp || !order || !grp || !gs || !gk) { pl_set_error("out of host memory"); goto fail; }
 	for (q = 0; q < n_prof; ++q) {
 		if (!profiles[q] || profiles[q]->device != e->device) { pl_set_error("profile %d missing or on another device", q); goto fail; }
 		hp[q] = profiles[q]->k;
-		if (hp[q].M > max_m) max_m = hp[q].M;
 	}
 	for (q = 0; q < n; ++q) {
 		const int32_t pid = prof_id[q], L = len[q];
@@ -103,7 +120,6 @@ PL_EXPORT int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *pro
 		cells = (int64_t)(L + 1) * (hp[pid].M + 1);
 		pep[q].dsq_off = off[q], pep[q].len = L, pep[q].prof = pid;
 		pep[q].null2 = do_null2 && cells <= RC_NULL2_MAXCELLS;
-		pep[q].scratch_off = 0;  /* set per wave below */
 		{ /* the length model's logarithms, with the expressions of recheck.c:289-290, :321 and :433-434
 		   * evaluated by the host's libm, so the device starts from the bits the reference computes */
 			const float pmove = (2.0f + 1.0f) / ((float)L + 2.0f + 1.0f);
@@ -114,7 +130,7 @@ PL_EXPORT int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *pro
 			pep[q].logL = logf((float)L);
 			pep[q].null1 = l_term + l1p1;
 		}
-		key[q].key = (int64_t)L * hp[pid].M, key[q].idx = q;
+		rp[q].prof = pid, rp[q].len = L, rp[q].idx = q;
 		cells_total += (int64_t)L * hp[pid].M;
 	}
 	{ /* residue codes index the 21-column score rows */
@@ -122,41 +138,63 @@ PL_EXPORT int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *pro
 		for (j = 0; j < dsq_len; ++j)
 			if (dsq[j] > 20) { pl_set_error("residue code %d at %lld (0-20 expected)", dsq[j], (long long)j); goto fail; }
 	}
-	qsort(key, (size_t)n, sizeof(*key), pl_rkey_cmp);
+	/* groups: up to 32 consecutive peptides of one profile, in the longest-first order */
+	qsort(rp, (size_t)n, sizeof(*rp), pl_rpep_cmp);
+	for (q = 0; q < n; ++q) order[q] = rp[q].idx;
+	for (q = 0; q < n;) {
+		plk_rc_grp_t *G = &grp[n_grp];
+		int32_t j = q;
+		G->first = q, G->prof = rp[q].prof, G->lmax = rp[q].len, G->full = 0;
+		while (j < n && j - q < 32 && rp[j].prof == G->prof) G->full |= pep[rp[j].idx].null2, ++j;
+		G->count = j - q;
+		gk[n_grp].key = (int64_t)G->lmax * hp[G->prof].M, gk[n_grp].idx = n_grp;
+		++n_grp, q = j;
+	}
+	qsort(gk, (size_t)n_grp, sizeof(*gk), pl_rkey_cmp);  /* the longest groups first */
+	for (q = 0; q < n_grp; ++q) gs[q] = grp[gk[q].idx];
 	if (!dbuf_ensure(&e->r_prof, sizeof(*hp) * (size_t)(n_prof > 0 ? n_prof : 1)) ||
 			!dbuf_ensure(&e->r_pep, sizeof(*pep) * (size_t)n) || !dbuf_ensure(&e->r_dsq, (size_t)dsq_len) ||
-			!dbuf_ensure(&e->r_order, sizeof(int32_t) * (size_t)n) || !dbuf_ensure(&e->r_counter, 64) ||
+			!dbuf_ensure(&e->r_order, sizeof(int32_t) * (size_t)n) ||
+			!dbuf_ensure(&e->r_grp, sizeof(*gs) * (size_t)n_grp) ||
 			!dbuf_ensure(&e->r_bits, sizeof(float) * (size_t)n) || !dbuf_ensure(&e->r_bias, sizeof(float) * (size_t)n))
 		goto fail;
+	/* waves of groups, each within the scratch budget (the first group of a wave always
+	 * goes, so the budget only has to hold the largest group) */
+	budget = e->trace_budget;
+	{
+		int32_t w0 = 0;
+		int64_t peak = 0;
+		while (w0 < n_grp) {
+			int32_t w1 = w0;
+			int64_t used = 0;
+			while (w1 < n_grp) {
+				const int64_t need = plk_rc_group_floats(gs[w1].lmax, hp[gs[w1].prof].M, gs[w1].full);
+				if (w1 > w0 && (used + need) * (int64_t)sizeof(float) > budget) break;
+				gs[w1].scratch_off = used, used += need;
+				++w1;
+			}
+			if (used > peak) peak = used;
+			w0 = w1;
+		}
+		if (!dbuf_ensure(&e->r_scratch, (size_t)(peak > 0 ? peak : 4) * sizeof(float))) goto fail;
+	}
 	CK(cudaMemcpyAsync(e->r_prof.p, hp, sizeof(*hp) * (size_t)n_prof, cudaMemcpyHostToDevice, st));
 	CK(cudaMemcpyAsync(e->r_dsq.p, dsq, (size_t)dsq_len, cudaMemcpyHostToDevice, st));
-	/* waves: longest first, scratch within the budget (the largest single peptide always fits) */
-	budget = e->trace_budget;
+	CK(cudaMemcpyAsync(e->r_pep.p, pep, sizeof(*pep) * (size_t)n, cudaMemcpyHostToDevice, st));
+	CK(cudaMemcpyAsync(e->r_order.p, order, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+	CK(cudaMemcpyAsync(e->r_grp.p, gs, sizeof(*gs) * (size_t)n_grp, cudaMemcpyHostToDevice, st));
 	e->n_ev = 0;
 	{
 		int32_t w0 = 0;
-		while (w0 < n) {
-			int32_t w1 = w0;
-			int64_t used = 0;
-			while (w1 < n) {
-				plk_rc_pep_t *p = &pep[key[w1].idx];
-				const int64_t need = p->null2 ? 4 * (int64_t)(p->len + 1) * (hp[p->prof].M + 1) + 6 * (int64_t)(p->len + 1) : 0;
-				if (w1 > w0 && (used + need) * (int64_t)sizeof(float) > budget) break;
-				p->scratch_off = used, used += (need + 3) / 4 * 4;
-				order[w1] = key[w1].idx;
-				++w1;
-			}
-			if (!dbuf_ensure(&e->r_scratch, (size_t)(used > 0 ? used : 4) * sizeof(float))) goto fail;
-			CK(cudaMemcpyAsync(e->r_pep.p, pep, sizeof(*pep) * (size_t)n, cudaMemcpyHostToDevice, st));
-			CK(cudaMemcpyAsync((int32_t*)e->r_order.p + w0, order + w0, sizeof(int32_t) * (size_t)(w1 - w0),
-					cudaMemcpyHostToDevice, st));
+		while (w0 < n_grp) {
+			int32_t w1 = w0 + 1;
+			while (w1 < n_grp && gs[w1].scratch_off > 0) ++w1;  /* a wave ends where the offsets restart */
 			PL_TIME(e, st, 1);
 			CKK(plk_rc_forward((const plk_rc_prof_t*)e->r_prof.p, (const plk_rc_pep_t*)e->r_pep.p,
-					(const uint8_t*)e->r_dsq.p, (const int32_t*)e->r_order.p + w0, w1 - w0, (int32_t*)e->r_counter.p,
-					(float*)e->r_scratch.p, (float*)e->r_bits.p, (float*)e->r_bias.p, max_m, e->n_sm, st));
+					(const uint8_t*)e->r_dsq.p, (const int32_t*)e->r_order.p, (const plk_rc_grp_t*)e->r_grp.p + w0,
+					w1 - w0, (float*)e->r_scratch.p, (float*)e->r_bits.p, (float*)e->r_bias.p, st));
 			PL_TIME(e, st, 1);
-			CK(cudaStreamSynchronize(st));  /* the next wave reuses the scratch and the job table */
-			w0 = w1;
+			w0 = w1;  /* waves run in stream order, so the next one may reuse the scratch */
 		}
 	}
 	CK(cudaMemcpyAsync(bits, e->r_bits.p, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, st));
@@ -174,7 +212,7 @@ PL_EXPORT int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *pro
 	e->r_last_cells = cells_total;
 	ok = 1;
 fail:
-	free(hp), free(pep), free(key), free(order);
+	free(hp), free(pep), free(rp), free(order), free(grp), free(gs), free(gk);
 	return ok;
 }
 

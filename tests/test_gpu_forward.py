@@ -118,6 +118,8 @@ def _bits_of(f):
 @pytest.mark.parametrize("fn,lo,hi", [
     (0, 0x80000000, _bits_of(-50.0) + 1),  # expf at every float in [-50, -0], the arguments rc_logsum passes
     (1, 0x00000000, _bits_of(1.0) + 1),    # log1pf at every float in [0, 1], the values expf returns there
+    (2, 0x80000000, _bits_of(-50.0) + 1),  # the branch-free forms rc_logsum runs on the device, same ranges
+    (3, 0x00000000, _bits_of(1.0) + 1),    # (log1pf's includes the branch-free division)
 ])
 def test_device_libm_equals_host(fn, lo, hi):
     """The device build of the restated expf / log1pf against the host libm at every float bit pattern

@@ -5,7 +5,9 @@ mn - mx in [-50, 0], so expf is swept densely over [-50, 0] and log1pf over
 [0, 1]; both are also swept sparsely over every float (infinities, NaN,
 overflow, underflow, subnormals).  Exhaustive runs over all 4.28e9 floats gave
 0 mismatches for both; the device build is checked over the full Forward range
-in tests/test_gpu_forward.py.
+in tests/test_gpu_forward.py.  The branch-free forms rc_logsum uses on the device
+(gl_expf_rng, gl_log1pf_unit) equal the host libm on every float of [-50, 50] and
+[0, 1] (exhaustive runs, 0 mismatches); the sweeps below repeat that densely.
 """
 import ctypes as C
 import os
@@ -36,6 +38,10 @@ def _bits(f):
     (1, 0x00000000, 0xffffffff, 4099),
     (0, _bits(-0.4), _bits(-0.5) + 1, 1),   # a dense window of each, every pattern
     (1, _bits(0.40), _bits(0.45) + 1, 1),   # around log1pf's 0.41422 branch
+    (2, 0x80000000, _bits(-50.0) + 1, 7),   # the branch-free forms on rc_logsum's ranges
+    (3, 0x00000000, _bits(1.0) + 1, 7),
+    (3, _bits(0.40), _bits(0.45) + 1, 1),
+    (3, _bits(0.99), _bits(1.0) + 1, 1),    # |f| < 2^-20 near 1 + x = 2
 ])
 def test_restated_libm_equals_host(fn, lo, hi, stride):
     bad = C.c_uint32()
