@@ -524,8 +524,10 @@ k_splice_dp(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_coop
  * traceback takes the first set one: first wins, nasw-sse.c:517-530) and the six
  * extension / lazy-F comparisons.  Each bit comes out clean from one DPX step: for
  * c <= m per half, max(c + 1, m) - m is 1 exactly when c == m and 0 otherwise, in
- * both halves at once with no borrow between them.  The subtraction and the
- * placement of the bit are linear, so the whole word is one sum of multiply-adds,
+ * both halves at once with no borrow between them; the candidates use the form
+ * max(c, m - 1) - (m - 1), which takes a candidate that is a sum c = a + b in the
+ * same step.  The subtraction and the placement of the bit are linear, so the whole
+ * word is one sum of multiply-adds,
  *   z = sum_k max(c_k + 1, m_k) * 2^p_k  -  sum_k m_k * 2^p_k   (mod 2^32),
  * which runs on the FMA pipe (the multipliers are kernel constants) while the DPX
  * steps keep the ALU pipe.  Bit p of each half: p = k for candidates 0-9 (m = the
@@ -552,7 +554,7 @@ __device__ __forceinline__ unsigned vmax2u(unsigned a, unsigned b)
 	return d;
 }
 
-struct PairK { unsigned F2, GOn, GEn, IOn, FSn, GOEn, ONE, ONEFS; };
+struct PairK { unsigned F2, GOn, GEn, IOn, FSn, GOEn, ONE; };
 
 template <int R>
 __device__ __forceinline__ void cells_pair(const unsigned (&in)[9], unsigned (&hm)[R], const unsigned ah1,
@@ -587,29 +589,36 @@ __device__ __forceinline__ void cells_pair(const unsigned (&in)[9], unsigned (&h
 		const unsigned bnew = vmax2u(t7, vb);
 		const unsigned t8 = __viaddmax_s16x2(ub, dn[r + 2], K.F2);
 		const unsigned cnew = vmax2u(t8, vc);
-		/* candidates 0-5 (floored at F, where none of them can win), 6-9 folded */
+		/* candidates 0-5 and the frameshifts 6-9 into the maximum he.  c0 keeps its floor F;
+		 * c3-c5 (A - a(i), B - a(i-2), C - a(i-1)) are folded in as sums: he >= c0 >= F, so
+		 * their floors cannot change he (every sum stays in [0, 0x7fff]) */
 		const unsigned c0 = __viaddmax_s16x2(h3m1, srow[cp[r]], K.F2);  /* H(i-3,j-1) + s(i,j) */
-		const unsigned c3 = __viaddmax_s16x2(anew, ac[r + 2], K.F2);    /* A - a(i) */
-		const unsigned c4 = __viaddmax_s16x2(bnew, ac[r], K.F2);        /* B - a(i-2) */
-		const unsigned c5 = __viaddmax_s16x2(cnew, ac[r + 1], K.F2);    /* C - a(i-1) */
-		unsigned he = __vimax3_s16x2(c0, ipn, dnew);
-		he = __vimax3_s16x2(he, c3, c4);
+		unsigned x = __vimax3_s16x2(c0, ipn, dnew);
+		x = __viaddmax_s16x2(anew, ac[r + 2], x);
+		x = __viaddmax_s16x2(bnew, ac[r], x);
+		x = __viaddmax_s16x2(cnew, ac[r + 1], x);
 		const unsigned fsm = vmax2u(__vimax3_s16x2(h1, h2, h1m1), h2m1);
-		he = __viaddmax_s16x2(fsm, K.FSn, vmax2u(he, c5));     /* 6-9: H(i-1|i-2, j|j-1) - fs */
+		const unsigned he = __viaddmax_s16x2(fsm, K.FSn, x);     /* 6-9: H(i-1|i-2, j|j-1) - fs */
 		lh[r] = he;
 		const unsigned h = vmax2u(he, ic[r]);                  /* the carried insertion */
-		/* the sixteen bits of both cells: max(c + 1, m) on the ALU pipe, the sum on the FMA pipe */
-		unsigned zz = __viaddmax_s16x2(c0, K.ONE, he);
-		zz += __viaddmax_s16x2(ipn, K.ONE, he) * (unsigned)P.pair_pw[1];
-		zz += __viaddmax_s16x2(dnew, K.ONE, he) * (unsigned)P.pair_pw[2];
-		zz += __viaddmax_s16x2(c3, K.ONE, he) * (unsigned)P.pair_pw[3];
-		zz += __viaddmax_s16x2(c4, K.ONE, he) * (unsigned)P.pair_pw[4];
-		zz += __viaddmax_s16x2(c5, K.ONE, he) * (unsigned)P.pair_pw[5];
-		zz += __viaddmax_s16x2(h1, K.ONEFS, he) * (unsigned)P.pair_pw[6];
-		zz += __viaddmax_s16x2(h2, K.ONEFS, he) * (unsigned)P.pair_pw[7];
-		zz += __viaddmax_s16x2(h1m1, K.ONEFS, he) * (unsigned)P.pair_pw[8];
-		zz += __viaddmax_s16x2(h2m1, K.ONEFS, he) * (unsigned)P.pair_pw[9];
-		zz += he * (unsigned)P.pair_nw[0];
+		/* the sixteen bits of both cells.  Candidate k's bit is max(c_k, he - 1) - (he - 1),
+		 * 1 exactly when c_k == he (c_k <= he; he - 1 per half has no borrow, he >= F); a
+		 * floor cell (he == F) sets bit 0, c0 == F, so its first set bit, the state the
+		 * traceback reads, is the reference's 0 whatever the unfloored sums give.  The g
+		 * bits are max(c + 1, m) - m with m the maximum the value entered.  The maxima run
+		 * on the ALU pipe, the sum on the FMA pipe. */
+		const unsigned hm1 = he * (unsigned)P.pair_pw[0] - 0x00010001u;
+		unsigned zz = vmax2u(c0, hm1);
+		zz += vmax2u(ipn, hm1) * (unsigned)P.pair_pw[1];
+		zz += vmax2u(dnew, hm1) * (unsigned)P.pair_pw[2];
+		zz += __viaddmax_s16x2(anew, ac[r + 2], hm1) * (unsigned)P.pair_pw[3];
+		zz += __viaddmax_s16x2(bnew, ac[r], hm1) * (unsigned)P.pair_pw[4];
+		zz += __viaddmax_s16x2(cnew, ac[r + 1], hm1) * (unsigned)P.pair_pw[5];
+		zz += __viaddmax_s16x2(h1, K.FSn, hm1) * (unsigned)P.pair_pw[6];
+		zz += __viaddmax_s16x2(h2, K.FSn, hm1) * (unsigned)P.pair_pw[7];
+		zz += __viaddmax_s16x2(h1m1, K.FSn, hm1) * (unsigned)P.pair_pw[8];
+		zz += __viaddmax_s16x2(h2m1, K.FSn, hm1) * (unsigned)P.pair_pw[9];
+		zz += hm1 * (unsigned)P.pair_nw[0];
 		zz += __viaddmax_s16x2(t4, K.ONE, m4) * (unsigned)P.pair_pw[10] + m4 * (unsigned)P.pair_nw[1];
 		zz += __viaddmax_s16x2(u5, K.ONE, m5) * (unsigned)P.pair_pw[11] + m5 * (unsigned)P.pair_nw[2];
 		zz += __viaddmax_s16x2(t6, K.ONE, anew) * (unsigned)P.pair_pw[12] + anew * (unsigned)P.pair_nw[3];
@@ -805,7 +814,7 @@ k_splice_pair(plk_job_t *__restrict__ jobs, const int32_t *__restrict__ order_co
 	K.F2 = (unsigned)P.pair_f * 0x10001u;
 	K.GOn = pk16(-P.go, -P.go), K.GEn = pk16(-P.ge, -P.ge), K.IOn = pk16(-P.io, -P.io);
 	K.FSn = pk16(-P.fs, -P.fs), K.GOEn = pk16(-(P.go + P.ge), -(P.go + P.ge));
-	K.ONE = 0x00010001u, K.ONEFS = pk16(1 - P.fs, 1 - P.fs);
+	K.ONE = 0x00010001u;
 	__syncthreads();
 	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
 	for (;;) {
