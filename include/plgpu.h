@@ -483,10 +483,11 @@ int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *profiles, int
 /* DP cells (sum of L*M) of the last recheck batch of this engine. */
 int64_t pl_rc_last_cells(const pl_engine_t *e);
 /* Self-check of the Forward's transcendental steps: evaluates on the device
- * fn 0 = expf, 1 = log1pf (the restated glibc algorithms the Forward uses) at
- * the n floats whose bit patterns are lo, lo + stride, lo + 2*stride, ... and
- * copies the results to the host array out.  Allocates device memory per call;
- * returns 1 on success. */
+ * fn 0 = expf, 1 = log1pf (the restated glibc algorithms), 2 / 3 = their
+ * branch-free forms for rc_logsum's ranges (|x| < 88, 0 <= x <= 1) and 4 / 5 =
+ * the four-wide forms of those, which the Forward runs, at the n floats whose bit
+ * patterns are lo, lo + stride, lo + 2*stride, ... and copies the results to the
+ * host array out.  Allocates device memory per call; returns 1 on success. */
 int pl_rc_mathf_eval(int32_t device, int32_t fn, uint32_t lo, uint32_t stride, int64_t n, float *out);
 
 /* DP cells of the last extension batch: the rows the reference's row loop

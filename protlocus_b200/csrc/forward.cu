@@ -58,6 +58,26 @@ __device__ __forceinline__ float ls(float a, float b)
 	return glm_self(mn <= RC_NEG || d < -50.0f, mx, r);
 }
 
+/* N independent logsums, each exactly ls(a[j], b[j]), written across the N arguments
+ * statement by statement so that their dependence chains interleave */
+template <int N>
+__device__ __forceinline__ void lsn(const float (&a)[N], const float (&b)[N], float (&r)[N])
+{
+	float mx[N], x[N], ex[N], lg[N];
+	int keep[N];
+#pragma unroll
+	for (int j = 0; j < N; ++j) {
+		mx[j] = a[j] > b[j] ? a[j] : b[j];
+		const float mn = a[j] > b[j] ? b[j] : a[j], d = __fsub_rn(mn, mx[j]);
+		keep[j] = mn <= RC_NEG || d < -50.0f;
+		x[j] = fmaxf(d, -50.0f);
+	}
+	gl_expf_rng_n<N>(x, ex, s_exp2);
+	gl_log1pf_unit_n<N>(ex, lg);
+#pragma unroll
+	for (int j = 0; j < N; ++j) r[j] = glm_self(keep[j], mx[j], __fadd_rn(mx[j], lg[j]));
+}
+
 /* a group's region, every array interleaved by lane:
  *   FMI float2 {M, I} [rows][M+1]: rows = lmax+1 when full, else rows i-1 and i at (i & 1)
  *   BMI float2 {M, I} [lmax+1][M+1]: the Backward rows (full groups only)
@@ -84,67 +104,179 @@ __device__ __forceinline__ float ldr(const float *p) { return __ldcg(p); }
 __device__ __forceinline__ void str2(float2 *p, float2 v) { __stcg(p, v); }
 __device__ __forceinline__ void str(float *p, float v) { __stcg(p, v); }
 
-/* Forward (recheck.c:298-318) of one lane's peptide; returns the total tot (nats).
- * Step k of a row's loop forms M(k) from the first-level sums taken in step k-1,
- * the first-level sums of M(k+1), I(k), D(k), the exit term ls(M(k-1), D(k-1)),
- * and adds column k-2's term to E: the same operations on the same operands as the
- * reference's column loop, with E's terms added in column order. */
-__device__ float rc_forward_lane(const RcLane &S, const plk_rc_pep_t &P, const plk_rc_prof_t &R,
-		const uint8_t *__restrict__ dsq)
+/*
+ * The passes run on four warps of a group's CTA, each pass split in two along its
+ * dependences: the Forward's M/I warp (M(k), I(k): they read only the row above) and
+ * its chain warp (D and the exit sum E along the row, one column behind, then the
+ * row's special states, whose xB the M/I warp needs for the next row); the
+ * Backward's chain warp (the B sum over the row below, then D along the row from the
+ * last column) and its M/I warp (M(k), I(k), one column behind the D it needs).
+ * Per column, a value crosses between the two warps of a pass through a ring in
+ * shared memory whose slots are 64-bit words holding the value and a tag (the pass
+ * step t and column count c as t * (M + 2) + c), written and read whole, so the
+ * consumer lane waits for its slot to carry the tag and needs no fence; the consumer
+ * hands its progress back the same way, and the producer does not overwrite a slot
+ * the consumer has not taken.  Once per row, where a warp reads rows the other wrote
+ * to global memory, a counter is advanced after a block fence.  Every wait is bounded
+ * by a clock limit: on expiry the CTA's abort flag and the launch's error word are
+ * set and every warp leaves its loops (the barriers that follow are still met).
+ */
+#define RC_Q 32                        /* ring depth, columns */
+#define RC_SPIN_LIMIT 10000000000LL    /* clock cycles, some seconds */
+#define FULL 0xffffffffu
+
+struct RcSync {
+	volatile int fc, bc, bp, abort;             /* row hand-offs: Forward chain row done, Backward M/I row done, row L */
+	volatile unsigned long long m[RC_Q][32];    /* M(i, k) of the Forward's M/I warp, tagged */
+	volatile unsigned long long dn[RC_Q][32];   /* D(i, k+1) of the Backward's chain warp, tagged */
+	volatile unsigned long long fcons[32], bcons[32], bE[32];  /* consumer progress; bE of a Backward row */
+	float xB[32], tot[32], u[3][32];
+};
+
+__device__ __forceinline__ unsigned long long rc_pack(const int tag, const float v)
 {
-	const int M = R.M, W = M + 1, L = P.len;
+	return ((unsigned long long)(unsigned)tag << 32) | __float_as_uint(v);
+}
+
+/* the value of a slot once it carries tag (exactly, or at least tag when ge); false in
+ * ok when the wait ran out or the CTA aborted */
+__device__ __forceinline__ float rc_take(RcSync &Y, volatile unsigned long long &slot, const int tag, const bool ge,
+		int *err, bool &ok)
+{
+	unsigned long long v = slot;
+	if (ge ? (int)(v >> 32) < tag : (int)(v >> 32) != tag) {
+		const long long t0 = clock64();
+		for (;;) {
+			v = slot;
+			if (ge ? (int)(v >> 32) >= tag : (int)(v >> 32) == tag) break;
+			if (Y.abort) { ok = false; break; }
+			if (clock64() - t0 > RC_SPIN_LIMIT) { Y.abort = 1; atomicExch(err, 1); ok = false; break; }
+		}
+	}
+	return __uint_as_float((unsigned)v);
+}
+
+/* warp-wide wait until ctr >= target, then a block fence (the rows the other warp wrote
+ * before its matching rc_publish are visible); false when it ran out or the CTA aborted */
+__device__ __forceinline__ bool rc_wait(RcSync &Y, volatile int &ctr, const int target, int *err)
+{
+	int ok = 1;
+	if ((threadIdx.x & 31) == 0 && ctr < target) {
+		const long long t0 = clock64();
+		while (ctr < target) {
+			if (Y.abort) { ok = 0; break; }
+			if (clock64() - t0 > RC_SPIN_LIMIT) { Y.abort = 1; atomicExch(err, 1); ok = 0; break; }
+			__nanosleep(32);
+		}
+	}
+	ok = __shfl_sync(FULL, ok, 0);
+	__threadfence_block();
+	return ok != 0;
+}
+
+/* make the warp's writes so far visible to the CTA, then set ctr = v */
+__device__ __forceinline__ void rc_publish(volatile int &ctr, const int v)
+{
+	__syncwarp();
+	__threadfence_block();
+	if ((threadIdx.x & 31) == 0) ctr = v;
+}
+
+#define NEG2 make_float2(RC_NEG, RC_NEG)
+
+/* Forward M/I warp (recheck.c:305-311): for row i, M(k) = ls(ls(M'(k-1) + MM, I'(k-1) +
+ * IM), ls(xB' + BM, D'(k-1) + DM)) + e(k) and I(k) = ls(M'(k) + MI, I'(k) + II) from the
+ * row above ('); the first level of M(k+1) is taken in step k. */
+__device__ bool rc_fwd_mi(const RcLane &S, const plk_rc_pep_t &P, const plk_rc_prof_t &R,
+		const uint8_t *__restrict__ dsq, const bool on, RcSync &Y, int *err)
+{
+	const int M = R.M, W = M + 1, W2 = M + 2, lane = threadIdx.x & 31, L = on ? P.len : 0;
 	const float4 *T4 = (const float4*)R.tsc;
-	const float *msc = R.msc;
-	const float lmove = P.lmove, lloop = P.lloop, lE = -(float)RC_LN2;
-	const size_t sps = (size_t)(S.lmax + 1) << 5;
-	float *xNf = S.sp, *xJf = xNf + sps, *xCf = xJf + sps;
-	for (int k = 0; k <= M; ++k) str2(S.fmi + rc_ix(0, k, W), make_float2(RC_NEG, RC_NEG)), str(S.d + ((size_t)k << 5), RC_NEG);
-	float xN = 0.0f, xB = lmove, xJ = RC_NEG, xC = RC_NEG;
-	if (P.null2) str(xNf, 0.0f), str(xJf, RC_NEG), str(xCf, RC_NEG);
-	for (int i = 1; i <= L; ++i) {
+	if (on)
+		for (int k = 0; k <= M; ++k) str2(S.fmi + rc_ix(0, k, W), NEG2), str(S.d + ((size_t)k << 5), RC_NEG);
+	float xB = P.lmove;
+	for (int i = 1; i <= S.lmax; ++i) {
+		if (i >= 2) {  /* the chain warp's row i-1: its D row and xB */
+			if (!rc_wait(Y, Y.fc, (i - 1) * W2 + M + 1, err)) return false;
+			xB = Y.xB[lane];
+		}
+		const bool act = i <= L;
 		const int rp = S.full ? i - 1 : (i - 1) & 1, rc = S.full ? i : i & 1;
 		const float2 *pr = S.fmi + rc_ix(rp, 0, W);
 		float2 *cr = S.fmi + rc_ix(rc, 0, W);
 		const float *dp = S.d + ((i & 1) ? 0 : ((size_t)W << 5));   /* recheck.c:303 */
-		float *dr = S.d + ((i & 1) ? ((size_t)W << 5) : 0);
-		const int xr = dsq[i - 1];
-		const float *mcol = msc + xr;  /* M(k)'s emission at mcol[(k-1)*21] */
-		str2(cr, make_float2(RC_NEG, RC_NEG)), str(dr, RC_NEG);
-		/* step 1's first-level sums read column 0 of the previous row (-inf) and tsc row 0 */
-		float4 t0 = __ldg(T4), t1 = __ldg(T4 + 1);   /* tsc row k-1 in step k */
+		const float *mcol = R.msc + (act ? dsq[i - 1] : 0);
+		if (act) str2(cr, NEG2);
+		const float4 t0 = __ldg(T4);
+		float4 t1 = __ldg(T4 + 1);                      /* tsc row k-1 in step k */
 		float a = ls(RC_NEG + t0.x, RC_NEG + t0.y), b = ls(xB + t0.w, RC_NEG + t0.z);
-		float2 cur = ldr2(pr + ((size_t)1 << 5));      /* M, I of the previous row at column k */
-		float cd = ldr(dp + ((size_t)1 << 5));          /* its D at column k */
-		float4 n0 = t0, n1 = t1;                        /* tsc row k */
-		if (M > 1) n0 = __ldg(T4 + 2), n1 = __ldg(T4 + 3);
-		float ms = __ldg(mcol);                         /* emission of column k */
+		float2 cur = act ? ldr2(pr + ((size_t)1 << 5)) : NEG2;  /* M, I of the row above at column k */
+		float cd = act ? ldr(dp + ((size_t)1 << 5)) : RC_NEG;   /* its D */
+		float4 n0 = __ldg(T4 + 2 * (M > 1 ? 1 : 0)), n1 = __ldg(T4 + 2 * (M > 1 ? 1 : 0) + 1);  /* tsc row k */
+		float ms = __ldg(mcol);
+#pragma unroll 1
+		for (int k = 1; k <= M; ++k) {
+			if (k > RC_Q) {  /* the chain warp has taken column k - Q from this slot */
+				bool ok = true;
+				rc_take(Y, Y.fcons[lane], i * W2 + k - RC_Q, true, err, ok);
+				if (!__all_sync(FULL, ok)) return false;
+			}
+			const int kn = k + 1 <= M ? k + 1 : M, kt = k + 1 < M ? k + 1 : (M > 1 ? M - 1 : 0);
+			const float2 nxt = act ? ldr2(pr + ((size_t)kn << 5)) : NEG2;
+			const float nd = act ? ldr(dp + ((size_t)kn << 5)) : RC_NEG;
+			const float4 p0 = __ldg(T4 + 2 * kt), p1 = __ldg(T4 + 2 * kt + 1);  /* tsc row k+1 */
+			const float msn = __ldg(mcol + (size_t)(kn - 1) * RC_NCODE);
+			/* M(k)'s second level, I(k), M(k+1)'s first level */
+			const float la[4] = {a, cur.x + t1.x, cur.x + n0.x, xB + n0.w}, lb[4] = {b, cur.y + t1.y, cur.y + n0.y, cd + n0.z};
+			float lr[4];
+			lsn<4>(la, lb, lr);
+			const float mrk = lr[0] + ms;                    /* M(k) */
+			const float irk = glm_self(k < M, lr[1], RC_NEG); /* I(k) */
+			a = lr[2], b = lr[3];
+			if (act) str2(cr + ((size_t)k << 5), make_float2(mrk, irk));
+			Y.m[k % RC_Q][lane] = rc_pack(i * W2 + k, mrk);
+			t1 = n1, n0 = p0, n1 = p1, cur = nxt, cd = nd, ms = msn;
+		}
+	}
+	return true;
+}
+
+/* Forward chain warp (recheck.c:312-317): D(k) = ls(M(k-1) + MD, D(k-1) + DD) and
+ * E = ls(E, ls(M(k), D(k))) in column order from the M/I warp's M, then xJ, xC, xN and
+ * xB of the row; tot = xC(L) + lmove. */
+__device__ bool rc_fwd_chain(const RcLane &S, const plk_rc_pep_t &P, const plk_rc_prof_t &R, const bool on,
+		RcSync &Y, int *err)
+{
+	const int M = R.M, W = M + 1, W2 = M + 2, lane = threadIdx.x & 31, L = on ? P.len : 0;
+	const float4 *T4 = (const float4*)R.tsc;
+	const float lmove = P.lmove, lloop = P.lloop, lE = -(float)RC_LN2;
+	const size_t sps = (size_t)(S.lmax + 1) << 5;
+	float *xNf = S.sp, *xJf = xNf + sps, *xCf = xJf + sps;
+	const bool keep = on && P.null2;
+	float xN = 0.0f, xB = lmove, xJ = RC_NEG, xC = RC_NEG;
+	if (keep) str(xNf, 0.0f), str(xJf, RC_NEG), str(xCf, RC_NEG);
+	for (int i = 1; i <= S.lmax; ++i) {
+		const bool act = i <= L;
+		float *dr = S.d + ((i & 1) ? ((size_t)W << 5) : 0);
+		if (act) str(dr, RC_NEG);
 		/* D(1) = ls(M(0) + 0, D(0) + 0) = -inf exactly, as the reference's D(1) */
 		float mr1 = RC_NEG, dr1 = RC_NEG, tq = RC_NEG, e = RC_NEG, mdq = 0.0f, ddq = 0.0f;
+		float4 tr = __ldg(T4 + 1);  /* tsc row k-1 in step k: MD, DD */
 #pragma unroll 1
-		for (int k = 1; k < M; ++k) {
-			/* loads for step k+1, used after this step's logsums */
-			const float2 nxt = ldr2(pr + ((size_t)(k + 1) << 5));
-			const float nd = ldr(dp + ((size_t)(k + 1) << 5));
-			const int kn = k + 1 < M ? k + 1 : k;
-			const float4 p0 = __ldg(T4 + 2 * kn), p1 = __ldg(T4 + 2 * kn + 1);  /* tsc row k+1 */
-			const float msn = __ldg(mcol + (size_t)k * RC_NCODE);
-			const float mrk = ls(a, b) + ms;                            /* M(k) */
-			const float irk = ls(cur.x + t1.x, cur.y + t1.y);           /* I(k): tsc row k-1 */
-			const float drk = ls(mr1 + mdq, dr1 + ddq);                 /* D(k): tsc row k-2 */
-			const float tk1 = ls(mr1, dr1);                             /* E's term of column k-1 */
-			e = ls(e, tq);                                             /* E += column k-2's */
-			a = ls(cur.x + n0.x, cur.y + n0.y), b = ls(xB + n0.w, cd + n0.z);  /* M(k+1)'s first level */
-			str2(cr + ((size_t)k << 5), make_float2(mrk, irk)), str(dr + ((size_t)k << 5), drk);
-			tq = tk1, mr1 = mrk, dr1 = drk, mdq = t1.z, ddq = t1.w;
-			t0 = n0, t1 = n1, n0 = p0, n1 = p1, cur = nxt, cd = nd, ms = msn;
-		}
-		{ /* column M: I(M) = -inf */
-			const float mrk = ls(a, b) + ms;
-			const float drk = M >= 2 ? ls(mr1 + mdq, dr1 + ddq) : RC_NEG;
-			const float tk1 = ls(mr1, dr1);
-			e = ls(e, tq);
-			str2(cr + ((size_t)M << 5), make_float2(mrk, RC_NEG)), str(dr + ((size_t)M << 5), drk);
-			tq = tk1, mr1 = mrk, dr1 = drk;
+		for (int k = 1; k <= M; ++k) {
+			const float4 tn = __ldg(T4 + 2 * (k < M ? k : k - 1) + 1);
+			bool ok = true;
+			const float mrk = rc_take(Y, Y.m[k % RC_Q][lane], i * W2 + k, false, err, ok);
+			if (!__all_sync(FULL, ok)) return false;
+			Y.fcons[lane] = rc_pack(i * W2 + k, 0.0f);
+			/* D(k) (tsc row k-2), E's term of column k-1, E += column k-2's term */
+			const float la[3] = {mr1 + mdq, mr1, e}, lb[3] = {dr1 + ddq, dr1, tq};
+			float lr[3];
+			lsn<3>(la, lb, lr);
+			const float drk = lr[0], tk1 = lr[1];
+			e = lr[2];
+			if (act) str(dr + ((size_t)k << 5), drk);
+			tq = tk1, mr1 = mrk, dr1 = drk, mdq = tr.z, ddq = tr.w, tr = tn;
 		}
 		e = ls(e, tq);            /* column M-1 */
 		e = ls(e, ls(mr1, dr1));  /* column M */
@@ -152,24 +284,29 @@ __device__ float rc_forward_lane(const RcLane &S, const plk_rc_pep_t &P, const p
 		xC = ls(xC + lloop, e + lE);
 		xN = xN + lloop;
 		xB = ls(xN + lmove, xJ + lmove);
-		if (P.null2) str(xNf + ((size_t)i << 5), xN), str(xJf + ((size_t)i << 5), xJ), str(xCf + ((size_t)i << 5), xC);
+		if (keep && act) str(xNf + ((size_t)i << 5), xN), str(xJf + ((size_t)i << 5), xJ), str(xCf + ((size_t)i << 5), xC);
+		if (act) Y.tot[lane] = xC + lmove;  /* C->T after the peptide's last row */
+		Y.xB[lane] = xB;
+		rc_publish(Y.fc, i * W2 + M + 1);
 	}
-	return xC + lmove;  /* C->T */
+	return true;
 }
 
-/* Backward (recheck.c:321-375) of one lane's peptide: its M/I rows and special states.
- * It reads neither the Forward's rows nor its total, so it runs beside the Forward. */
-__device__ void rc_backward_lane(const RcLane &S, const plk_rc_pep_t &P, const plk_rc_prof_t &R,
-		const uint8_t *__restrict__ dsq)
+/* Backward chain warp (recheck.c:323-375 without M and I): row L, then for each row i
+ * (step t = L-1-i of the lane's rows) B = the sum over the columns of M(i+1, k) +
+ * t[k-1].BM + e(k, x(i+1)) in column order, the special states, and D along the row
+ * from the last column, D(k) = ls(M(i+1, k+1) + e(k+1) + DM, ls(D(k+1) + DD, bE)), handing
+ * D(k+1) and bE to the M/I warp. */
+__device__ bool rc_bwd_chain(const RcLane &S, const plk_rc_pep_t &P, const plk_rc_prof_t &R,
+		const uint8_t *__restrict__ dsq, const bool n2, RcSync &Y, int *err)
 {
-	const int M = R.M, W = M + 1, L = P.len;
+	const int M = R.M, W = M + 1, W2 = M + 2, lane = threadIdx.x & 31, L = n2 ? P.len : 1;
 	const float4 *T4 = (const float4*)R.tsc;
-	const float *msc = R.msc;
 	const float lmove = P.lmove, lloop = P.lloop, lE = -(float)RC_LN2;
 	const size_t sps = (size_t)(S.lmax + 1) << 5;
 	float *bNg = S.sp + 3 * sps, *bJg = bNg + sps, *bCg = bJg + sps;
 	float bC = lmove, bE = bC + lE, bJ = RC_NEG, bN = RC_NEG;
-	{ /* row L: M(M) = D(M) = bE; M(k) = ls(bE, D(k+1) + t[k-1].MD), D(k) = ls(bE, D(k+1) + t[k-1].DD) */
+	if (n2) { /* row L: M(M) = D(M) = bE; M(k) = ls(bE, D(k+1) + t[k-1].MD), D(k) = ls(bE, D(k+1) + t[k-1].DD) */
 		float2 *rw = S.bmi + rc_ix(L, 0, W);
 		float dn = bE;
 		str2(rw + ((size_t)M << 5), make_float2(bE, RC_NEG));
@@ -181,57 +318,113 @@ __device__ void rc_backward_lane(const RcLane &S, const plk_rc_pep_t &P, const p
 			str2(rw + ((size_t)k << 5), make_float2(m, RC_NEG));
 			t1 = tn;
 		}
-		str2(rw, make_float2(RC_NEG, RC_NEG));
+		str2(rw, NEG2);
 		str(bNg + ((size_t)L << 5), bN), str(bJg + ((size_t)L << 5), bJ), str(bCg + ((size_t)L << 5), bC);
 	}
-	for (int i = L - 1; i >= 1; --i) {
-		const float2 *nx = S.bmi + rc_ix(i + 1, 0, W);  /* row i+1 */
-		float2 *rw = S.bmi + rc_ix(i, 0, W);
-		const int xn = dsq[i];                           /* residue i+1 */
-		const float *mcol = msc + xn;
-		/* B = sum over the columns of M(i+1, k) + t[k-1].BM + e(k, x(i+1)), in column order;
-		 * the next column's operands are loaded a step ahead */
+	rc_publish(Y.bp, 0);  /* row L */
+	for (int t = 0; t + 2 <= S.lmax; ++t) {
+		const int i = L - 1 - t;
+		const bool act = n2 && i >= 1;
+		if (t >= 1 && !rc_wait(Y, Y.bc, (t - 1) * W2 + M + 1, err)) return false;  /* row i+1's M */
+		const float2 *nx = S.bmi + rc_ix(act ? i + 1 : 0, 0, W);
+		const float *mcol = R.msc + (act ? dsq[i] : 0);  /* residue i+1 */
 		float bB = RC_NEG;
-		float um = ldr2(nx + ((size_t)1 << 5)).x, ut = __ldg(R.tsc + T_BM), ue = __ldg(mcol);
+		{ /* the next column's operands a step ahead */
+			float um = act ? ldr2(nx + ((size_t)1 << 5)).x : RC_NEG, ut = __ldg(R.tsc + T_BM), ue = __ldg(mcol);
 #pragma unroll 1
-		for (int k = 1; k <= M; ++k) {
-			const int kn = k < M ? k + 1 : k;
-			const float vm = ldr2(nx + ((size_t)kn << 5)).x, vt = __ldg(R.tsc + (size_t)(kn - 1) * 8 + T_BM),
-			            ve = __ldg(mcol + (size_t)(kn - 1) * RC_NCODE);
-			bB = ls(bB, um + ut + ue);
-			um = vm, ut = vt, ue = ve;
+			for (int k = 1; k <= M; ++k) {
+				const int kn = k < M ? k + 1 : k;
+				const float vm = act ? ldr2(nx + ((size_t)kn << 5)).x : RC_NEG,
+				            vt = __ldg(R.tsc + (size_t)(kn - 1) * 8 + T_BM), ve = __ldg(mcol + (size_t)(kn - 1) * RC_NCODE);
+				bB = ls(bB, um + ut + ue);
+				um = vm, ut = vt, ue = ve;
+			}
 		}
-		const float bJn = bJ, bCn = bC, bNn = bN;
-		bJ = ls(bJn + lloop, bB + lmove);
-		bC = bCn + lloop;
-		bE = ls(bJ + lE, bC + lE);
-		bN = ls(bNn + lloop, bB + lmove);
-		str(bNg + ((size_t)i << 5), bN), str(bJg + ((size_t)i << 5), bJ), str(bCg + ((size_t)i << 5), bC);
-		/* M, I and D of row i, last column first (recheck.c:359-370); D(k+1) is the previous
-		 * step's; the next step's operands are loaded a step ahead */
-		str2(rw + ((size_t)M << 5), make_float2(bE, RC_NEG));
+		if (act) {
+			const float bJn = bJ, bCn = bC, bNn = bN;
+			bJ = ls(bJn + lloop, bB + lmove);
+			bC = bCn + lloop;
+			bE = ls(bJ + lE, bC + lE);
+			bN = ls(bNn + lloop, bB + lmove);
+			str(bNg + ((size_t)i << 5), bN), str(bJg + ((size_t)i << 5), bJ), str(bCg + ((size_t)i << 5), bC);
+		}
+		Y.bE[lane] = rc_pack(t * W2, bE);
+		/* D along the row, last column first; D(k+1) goes to the ring before D(k) is formed */
 		float dn = bE;
-		float mup = ldr2(nx + ((size_t)M << 5)).x;           /* M(i+1, k+1) */
-		const int k1 = M - 1 > 0 ? M - 1 : 0;
-		float4 tk = __ldg(T4 + 2 * k1);                       /* tsc row k: MM, IM, DM */
-		float4 r0 = __ldg(T4 + 2 * (k1 > 0 ? k1 - 1 : 0)), r1 = __ldg(T4 + 2 * (k1 > 0 ? k1 - 1 : 0) + 1);  /* row k-1 */
-		float2 here = ldr2(nx + ((size_t)k1 << 5));          /* M, I of row i+1 at column k */
-		float me = __ldg(mcol + (size_t)k1 * RC_NCODE);       /* e(k+1, x(i+1)) */
+		float mup = act ? ldr2(nx + ((size_t)M << 5)).x : RC_NEG;   /* M(i+1, k+1) */
+		float me = __ldg(mcol + (size_t)(M >= 2 ? M - 1 : 0) * RC_NCODE);  /* e(k+1, x(i+1)) */
+		float dm = __ldg(R.tsc + (size_t)(M >= 2 ? M - 1 : 0) * 8 + T_DM);  /* tsc row k: DM */
+		float dd = __ldg(R.tsc + (size_t)(M >= 2 ? M - 2 : 0) * 8 + T_DD);  /* tsc row k-1: DD */
 #pragma unroll 1
 		for (int k = M - 1; k >= 1; --k) {
+			const int c = M - k;  /* columns handed over so far, this one included */
+			if (c > RC_Q) {  /* the M/I warp has taken column count c - Q from this slot */
+				bool ok = true;
+				rc_take(Y, Y.bcons[lane], t * W2 + c - RC_Q, true, err, ok);
+				if (!__all_sync(FULL, ok)) return false;
+			}
+			const int kp = k >= 2 ? k - 1 : 0;
+			const float nmup = act ? ldr2(nx + ((size_t)k << 5)).x : RC_NEG;
+			const float nme = __ldg(mcol + (size_t)kp * RC_NCODE), ndm = __ldg(R.tsc + (size_t)kp * 8 + T_DM),
+			            ndd = __ldg(R.tsc + (size_t)(kp >= 1 ? kp - 1 : 0) * 8 + T_DD);
+			Y.dn[k % RC_Q][lane] = rc_pack(t * W2 + c, dn);
+			const float mn1 = mup + me;
+			dn = ls(mn1 + dm, ls(dn + dd, bE));
+			mup = nmup, me = nme, dm = ndm, dd = ndd;
+		}
+	}
+	return true;
+}
+
+/* Backward M/I warp (recheck.c:362-366): for row i, M(k) = ls(ls(mn1 + MM, I(i+1, k) + MI),
+ * ls(bE, D(k+1) + MD)) and I(k) = ls(mn1 + IM, I(i+1, k) + II), mn1 = M(i+1, k+1) + e(k+1),
+ * from the chain warp's bE and D(k+1). */
+__device__ bool rc_bwd_mi(const RcLane &S, const plk_rc_pep_t &P, const plk_rc_prof_t &R,
+		const uint8_t *__restrict__ dsq, const bool n2, RcSync &Y, int *err)
+{
+	const int M = R.M, W = M + 1, W2 = M + 2, lane = threadIdx.x & 31, L = n2 ? P.len : 1;
+	const float4 *T4 = (const float4*)R.tsc;
+	for (int t = 0; t + 2 <= S.lmax; ++t) {
+		const int i = L - 1 - t;
+		const bool act = n2 && i >= 1;
+		if (t == 0 && !rc_wait(Y, Y.bp, 0, err)) return false;  /* row L, written by the chain warp */
+		bool ok = true;
+		const float bE = rc_take(Y, Y.bE[lane], t * W2, false, err, ok);
+		if (!__all_sync(FULL, ok)) return false;
+		const float2 *nx = S.bmi + rc_ix(act ? i + 1 : 0, 0, W);
+		float2 *rw = S.bmi + rc_ix(act ? i : 0, 0, W);
+		const float *mcol = R.msc + (act ? dsq[i] : 0);
+		if (act) str2(rw + ((size_t)M << 5), make_float2(bE, RC_NEG));
+		const int k1 = M - 1 > 0 ? M - 1 : 0;
+		float mup = act ? ldr2(nx + ((size_t)M << 5)).x : RC_NEG;    /* M(i+1, k+1) */
+		float4 tk = __ldg(T4 + 2 * k1);                               /* tsc row k: MM, IM */
+		float4 r1 = __ldg(T4 + 2 * (k1 > 0 ? k1 - 1 : 0) + 1);         /* tsc row k-1: MI, II, MD */
+		float4 r0 = __ldg(T4 + 2 * (k1 > 0 ? k1 - 1 : 0));
+		float2 here = act ? ldr2(nx + ((size_t)k1 << 5)) : NEG2;      /* M, I of row i+1 at column k */
+		float me = __ldg(mcol + (size_t)k1 * RC_NCODE);
+#pragma unroll 1
+		for (int k = M - 1; k >= 1; --k) {
+			const int c = M - k;
+
 			const int kp = k >= 2 ? k - 2 : 0;
 			const float4 q0 = __ldg(T4 + 2 * kp), q1 = __ldg(T4 + 2 * kp + 1);  /* tsc row k-2 */
-			const float2 nh = ldr2(nx + ((size_t)(k - 1) << 5));                /* column k-1 */
+			const float2 nh = act ? ldr2(nx + ((size_t)(k - 1) << 5)) : NEG2;
 			const float mne = __ldg(mcol + (size_t)(k - 1) * RC_NCODE);
+			const float dk1 = rc_take(Y, Y.dn[k % RC_Q][lane], t * W2 + c, false, err, ok);
+			if (!__all_sync(FULL, ok)) return false;
+			Y.bcons[lane] = rc_pack(t * W2 + c, 0.0f);
 			const float mn1 = mup + me;
-			const float m = ls(ls(mn1 + tk.x, here.y + r1.x), ls(bE, dn + r1.z));
-			const float ii = ls(mn1 + tk.y, here.y + r1.y);
-			dn = ls(mn1 + tk.z, ls(dn + r1.w, bE));
-			str2(rw + ((size_t)k << 5), make_float2(m, ii));
+			const float la[3] = {mn1 + tk.x, bE, mn1 + tk.y}, lb[3] = {here.y + r1.x, dk1 + r1.z, here.y + r1.y};
+			float lr[3];
+			lsn<3>(la, lb, lr);
+			const float m = ls(lr[0], lr[1]), ii = lr[2];
+			if (act) str2(rw + ((size_t)k << 5), make_float2(m, ii));
 			mup = here.x, tk = r0, r0 = q0, r1 = q1, here = nh, me = mne;
 		}
-		str2(rw, make_float2(RC_NEG, RC_NEG));
+		if (act) str2(rw, NEG2);
+		rc_publish(Y.bc, t * W2 + M + 1);
 	}
+	return true;
 }
 
 /* posterior usage of columns [k_lo, k_hi] in log space, rows in ascending order
@@ -258,12 +451,13 @@ __device__ void rc_usage_lane(const RcLane &S, const plk_rc_pep_t &P, const int 
 			float2 fn[RC_UB], gn[RC_UB];
 #pragma unroll
 			for (int j = 0; j < RC_UB; ++j) fn[j] = ldr2(S.fmi + rc_ix(in, kk[j], W)), gn[j] = ldr2(S.bmi + rc_ix(in, kk[j], W));
+			float sa[RC_UB], sb[RC_UB];
 #pragma unroll
-			for (int j = 0; j < RC_UB; ++j) {
-				um[j] = ls(um[j], f[j].x + g[j].x);
-				ui[j] = ls(ui[j], f[j].y + g[j].y);
-				f[j] = fn[j], g[j] = gn[j];
-			}
+			for (int j = 0; j < RC_UB; ++j) sa[j] = f[j].x + g[j].x, sb[j] = f[j].y + g[j].y;
+			lsn<RC_UB>(um, sa, um);
+			lsn<RC_UB>(ui, sb, ui);
+#pragma unroll
+			for (int j = 0; j < RC_UB; ++j) f[j] = fn[j], g[j] = gn[j];
 		}
 #pragma unroll
 		for (int j = 0; j < RC_UB; ++j)
@@ -279,9 +473,13 @@ __device__ void rc_special_usage(const RcLane &S, const plk_rc_pep_t &P, float &
 	const float lloop = P.lloop;
 	uN = uJ = uC = RC_NEG;
 	for (int i = 1; i <= P.len; ++i) {
-		uN = ls(uN, ldr(xNf + ((size_t)(i - 1) << 5)) + ldr(bNg + ((size_t)i << 5)) + lloop);
-		uJ = ls(uJ, ldr(xJf + ((size_t)(i - 1) << 5)) + ldr(bJg + ((size_t)i << 5)) + lloop);
-		uC = ls(uC, ldr(xCf + ((size_t)(i - 1) << 5)) + ldr(bCg + ((size_t)i << 5)) + lloop);
+		const float ua[3] = {uN, uJ, uC};
+		const float ub[3] = {ldr(xNf + ((size_t)(i - 1) << 5)) + ldr(bNg + ((size_t)i << 5)) + lloop,
+		                     ldr(xJf + ((size_t)(i - 1) << 5)) + ldr(bJg + ((size_t)i << 5)) + lloop,
+		                     ldr(xCf + ((size_t)(i - 1) << 5)) + ldr(bCg + ((size_t)i << 5)) + lloop};
+		float ur[3];
+		lsn<3>(ua, ub, ur);
+		uN = ur[0], uJ = ur[1], uC = ur[2];
 	}
 }
 
@@ -303,7 +501,13 @@ __device__ float rc_null2_bias(const RcLane &S, const plk_rc_pep_t &P, const plk
 		const float u = ldr(lum + ((size_t)k << 5)) - tot - logL;
 		const float *mr = msc + (size_t)(k - 1) * RC_NCODE;
 #pragma unroll
-		for (int x = 0; x < 20; ++x) v[x] = ls(v[x], u + __ldg(mr + x));
+		for (int x0 = 0; x0 < 20; x0 += 4) {
+			const float va[4] = {v[x0], v[x0 + 1], v[x0 + 2], v[x0 + 3]};
+			const float vb[4] = {u + __ldg(mr + x0), u + __ldg(mr + x0 + 1), u + __ldg(mr + x0 + 2), u + __ldg(mr + x0 + 3)};
+			float vr[4];
+			lsn<4>(va, vb, vr);
+			v[x0] = vr[0], v[x0 + 1] = vr[1], v[x0 + 2] = vr[2], v[x0 + 3] = vr[3];
+		}
 	}
 	double s_odds = 0.0;
 #pragma unroll
@@ -330,21 +534,26 @@ struct RcArgs {
 	const plk_rc_grp_t *grp;
 	int32_t n_grp;
 	float *scratch, *bits, *bias;
+	int *err;  /* set when a wait between warps ran out */
 };
 
-/* one CTA per group, two warps (the hardware hands the groups, longest first, to the
- * SMs as they free up); lane l of both warps takes the group's l-th peptide.  Warp 0
- * runs the Forward, warp 1 the Backward (null2 peptides), side by side; then each
- * takes half of the columns' usage sums, warp 1 the special states' too, and warp 0
- * the bias and the score. */
-__global__ void __launch_bounds__(64, 1) k_rc_lanes(RcArgs A)
+/* one CTA per group, four warps (the hardware hands the groups, longest first, to the
+ * SMs as they free up); lane l of every warp takes the group's l-th peptide.  Warps 0/1
+ * run the Forward, warps 2/3 the Backward (null2 peptides); then each warp takes a
+ * quarter of the columns' usage sums, warp 3 the special states' too, and warp 0 the
+ * bias and the score. */
+__global__ void __launch_bounds__(128, 1) k_rc_lanes(RcArgs A)
 {
-	__shared__ float s_u[3][32];
+	__shared__ RcSync Y;
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	if (threadIdx.x < 32) s_exp2[threadIdx.x] = glm_exp2_tab_dev[threadIdx.x];
+	if (threadIdx.x == 0) Y.fc = Y.bp = Y.bc = -1, Y.abort = 0;
+	for (int x = threadIdx.x; x < RC_Q * 32; x += blockDim.x)  /* no slot carries a tag yet */
+		Y.m[x >> 5][x & 31] = Y.dn[x >> 5][x & 31] = rc_pack(-1, 0.0f);
+	if (threadIdx.x < 32) Y.fcons[threadIdx.x] = Y.bcons[threadIdx.x] = Y.bE[threadIdx.x] = rc_pack(-1, 0.0f);
 	__syncthreads();
 	const plk_rc_grp_t G = A.grp[blockIdx.x];
-	const bool on = lane < G.count;  /* every thread stays for the barriers */
+	const bool on = lane < G.count;  /* every thread stays for the barriers and the warp-wide steps */
 	const int q = on ? A.order[G.first + lane] : 0;
 	const plk_rc_pep_t P = A.pep[q];
 	const plk_rc_prof_t R = A.prof[G.prof];
@@ -359,23 +568,26 @@ __global__ void __launch_bounds__(64, 1) k_rc_lanes(RcArgs A)
 	S.full = G.full, S.lmax = G.lmax;
 	const uint8_t *dsq = A.dsq + P.dsq_off;
 	const bool n2 = on && P.null2;
-	float tot = 0.0f;
-	if (w == 0 && on) tot = rc_forward_lane(S, P, R, dsq);
-	if (w == 1 && n2) rc_backward_lane(S, P, R, dsq);
-	float bias = 0.0f;
-	if (G.full) {  /* the same for the whole CTA */
-		__syncthreads();
-		const int half = (M + 1) / 2;
-		if (n2) rc_usage_lane(S, P, M, w == 0 ? 1 : half + 1, w == 0 ? half : M);
-		if (w == 1 && n2) {
+	if (w == 0) rc_fwd_mi(S, P, R, dsq, on, Y, A.err);
+	else if (w == 1) rc_fwd_chain(S, P, R, on, Y, A.err);
+	else if (G.full && w == 2) rc_bwd_chain(S, P, R, dsq, n2, Y, A.err);
+	else if (G.full && w == 3) rc_bwd_mi(S, P, R, dsq, n2, Y, A.err);
+	__syncthreads();
+	const bool ok = !Y.abort;
+	if (G.full && ok) {  /* the same for the whole CTA */
+		const int k0 = 1 + (M * w) / 4, k1 = (M * (w + 1)) / 4;
+		if (n2 && k0 <= k1) rc_usage_lane(S, P, M, k0, k1);
+		if (w == 3 && n2) {
 			float uN, uJ, uC;
 			rc_special_usage(S, P, uN, uJ, uC);
-			s_u[0][lane] = uN, s_u[1][lane] = uJ, s_u[2][lane] = uC;
+			Y.u[0][lane] = uN, Y.u[1][lane] = uJ, Y.u[2][lane] = uC;
 		}
-		__syncthreads();
-		if (w == 0 && n2) bias = rc_null2_bias(S, P, R, dsq, tot, s_u[0][lane], s_u[1][lane], s_u[2][lane]);
 	}
-	if (w == 0 && on) {  /* recheck.c:432-437; null1 = L*logf(p1) + logf(1-p1) comes from the host */
+	__syncthreads();
+	if (w == 0 && on && ok) {
+		const float tot = Y.tot[lane];
+		const float bias = n2 ? rc_null2_bias(S, P, R, dsq, tot, Y.u[0][lane], Y.u[1][lane], Y.u[2][lane]) : 0.0f;
+		/* recheck.c:432-437; null1 = L*logf(p1) + logf(1-p1) comes from the host */
 		A.bits[q] = __fdiv_rn(__fsub_rn(__fsub_rn(tot, P.null1), bias), (float)RC_LN2);
 		A.bias[q] = __fdiv_rn(bias, (float)RC_LN2);
 	}
@@ -383,19 +595,31 @@ __global__ void __launch_bounds__(64, 1) k_rc_lanes(RcArgs A)
 
 extern "C" int plk_rc_forward(const plk_rc_prof_t *prof, const plk_rc_pep_t *pep, const uint8_t *dsq,
 		const int32_t *order, const plk_rc_grp_t *grp, int32_t n_grp, float *scratch, float *bits, float *bias,
-		void *stream)
+		int *err, void *stream)
 {
 	if (n_grp <= 0) return 0;
 	RcArgs A;
 	A.prof = prof, A.pep = pep, A.dsq = dsq, A.order = order, A.grp = grp, A.n_grp = n_grp;
-	A.scratch = scratch, A.bits = bits, A.bias = bias;
-	k_rc_lanes<<<(unsigned)n_grp, 64, 0, (cudaStream_t)stream>>>(A);
+	A.scratch = scratch, A.bits = bits, A.bias = bias, A.err = err;
+	k_rc_lanes<<<(unsigned)n_grp, 128, 0, (cudaStream_t)stream>>>(A);
 	plk_add_launches(1);
 	return (int)cudaGetLastError();
 }
 
 __global__ void k_mathf_eval(int fn, uint32_t lo, uint32_t stride, int64_t n, float *out)
 {
+	if (fn >= 4) {  /* the N-wide forms, four consecutive arguments per thread */
+		for (int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x * 4) {
+			float x[4], y[4];
+#pragma unroll
+			for (int j = 0; j < 4; ++j) x[j] = __uint_as_float(lo + (uint32_t)((uint64_t)(i0 + j < n ? i0 + j : i0) * stride));
+			if (fn == 4) gl_expf_rng_n<4>(x, y, glm_exp2_tab_dev);
+			else gl_log1pf_unit_n<4>(x, y);
+#pragma unroll
+			for (int j = 0; j < 4; ++j) if (i0 + j < n) out[i0 + j] = y[j];
+		}
+		return;
+	}
 	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
 		const float x = __uint_as_float(lo + (uint32_t)((uint64_t)i * stride));
 		out[i] = fn == 0 ? gl_expf(x) : fn == 1 ? gl_log1pf(x) : fn == 2 ? gl_expf_rng(x) : gl_log1pf_unit(x);
@@ -406,7 +630,7 @@ extern "C" __attribute__((visibility("default"))) int pl_rc_mathf_eval(int32_t d
 		uint32_t stride, int64_t n, float *out)
 {
 	float *d = 0;
-	if (fn < 0 || fn > 3 || n < 0 || !out) return 0;
+	if (fn < 0 || fn > 5 || n < 0 || !out) return 0;
 	if (n == 0) return 1;
 	if (cudaSetDevice(device) != cudaSuccess || cudaMalloc((void**)&d, sizeof(float) * (size_t)n) != cudaSuccess) return 0;
 	int64_t grid = (n + 255) / 256;

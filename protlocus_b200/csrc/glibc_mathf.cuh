@@ -307,4 +307,118 @@ GLM_FN float gl_log1pf_unit(float x)
 	return glm_self(tiny, r_tiny, r);
 }
 
+#if defined(__CUDACC__)
+/*
+ * N independent evaluations of gl_expf_rng_t / gl_log1pf_unit, written statement by
+ * statement across the N arguments so that the N dependence chains interleave in the
+ * instruction stream (the compiler does not interleave N separate calls).  Every
+ * element goes through exactly the operations of the scalar form.
+ */
+#define GLM_N for (int j = 0; j < N; ++j)
+template <int N>
+static __device__ __forceinline__ void gl_expf_rng_n(const float (&x)[N], float (&out)[N], const uint64_t *tab)
+{
+	const double inv_ln2_32 = 0x1.71547652b82fep+0 * 32, shift = 0x1.8p+52;
+	const double c0 = 0x1.c6af84b912394p-5 / 32 / 32 / 32, c1 = 0x1.ebfce50fac4f3p-3 / 32 / 32,
+	             c2 = 0x1.62e42ff0c52d6p-1 / 32;
+	double xd[N], kd[N], r[N], s[N], z[N], r2[N], y[N];
+	uint64_t ki[N];
+#pragma unroll
+	GLM_N xd[j] = (double)x[j];
+#pragma unroll
+	GLM_N kd[j] = GLM_DFMA(inv_ln2_32, xd[j], shift);
+#pragma unroll
+	GLM_N ki[j] = glm_d2u(kd[j]);
+#pragma unroll
+	GLM_N kd[j] = GLM_DSUB(kd[j], shift);
+#pragma unroll
+	GLM_N r[j] = GLM_DFMA(inv_ln2_32, xd[j], -kd[j]);
+#pragma unroll
+	GLM_N s[j] = glm_u2d(tab[ki[j] % 32] + (ki[j] << 47));
+#pragma unroll
+	GLM_N z[j] = GLM_DFMA(c0, r[j], c1), r2[j] = GLM_DMUL(r[j], r[j]);
+#pragma unroll
+	GLM_N y[j] = GLM_DFMA(c2, r[j], 1.0);
+#pragma unroll
+	GLM_N y[j] = GLM_DFMA(z[j], r2[j], y[j]);
+#pragma unroll
+	GLM_N y[j] = GLM_DMUL(y[j], s[j]);
+#pragma unroll
+	GLM_N out[j] = GLM_D2F(y[j]);
+}
+
+template <int N>
+static __device__ __forceinline__ void gl_log1pf_unit_n(const float (&x)[N], float (&out)[N])
+{
+	const float ln2_hi = 6.9313812256e-01f, ln2_lo = 9.0580006145e-06f;
+	const float lp1 = 6.6666668653e-01f, lp2 = 4.0000000596e-01f, lp3 = 2.8571429849e-01f,
+	            lp4 = 2.2222198546e-01f, lp5 = 1.8183572590e-01f, lp6 = 1.5313838422e-01f,
+	            lp7 = 1.4798198640e-01f;
+	int32_t hx[N], k1[N], m[N], k[N], hu[N];
+	int small[N], tiny[N], hi_m[N];
+	float r_tiny[N], u1[N], c1[N], uL[N], f[N], c[N], hfsq[N], kf[N], r_f0[N], R0[N], r_fs[N], s[N], zz[N], R[N],
+	      sR[N], r_p[N], t2[N];
+#pragma unroll
+	GLM_N hx[j] = (int32_t)glm_f2u(x[j]), small[j] = hx[j] < 0x3ed413d7, tiny[j] = hx[j] < 0x31000000;
+#pragma unroll
+	GLM_N r_tiny[j] = glm_self(hx[j] < 0x24800000, x[j], GLM_FSUB(x[j], GLM_FMUL(GLM_FMUL(x[j], x[j]), 0.5f)));
+#pragma unroll
+	GLM_N u1[j] = GLM_FADD(1.0f, x[j]);
+#pragma unroll
+	GLM_N {
+		const int32_t hu1 = (int32_t)glm_f2u(u1[j]);
+		k1[j] = (hu1 >> 23) - 127, m[j] = hu1 & 0x007fffff;
+	}
+#pragma unroll
+	GLM_N t2[j] = k1[j] > 0 ? GLM_FSUB(1.0f, GLM_FSUB(u1[j], x[j])) : GLM_FSUB(x[j], GLM_FSUB(u1[j], 1.0f));
+#pragma unroll
+	GLM_N c1[j] = glm_div(t2[j], u1[j]);
+#pragma unroll
+	GLM_N {
+		hi_m[j] = m[j] >= 0x3504f7;
+		uL[j] = glm_u2f((uint32_t)m[j] | (hi_m[j] ? 0x3f000000u : 0x3f800000u));
+		k[j] = small[j] ? 0 : (hi_m[j] ? k1[j] + 1 : k1[j]);
+		hu[j] = small[j] ? 1 : (hi_m[j] ? (0x00800000 - m[j]) >> 2 : m[j]);
+	}
+#pragma unroll
+	GLM_N f[j] = glm_self(small[j], x[j], GLM_FSUB(uL[j], 1.0f)), c[j] = glm_self(small[j], 0.0f, c1[j]);
+#pragma unroll
+	GLM_N hfsq[j] = GLM_FMUL(GLM_FMUL(0.5f, f[j]), f[j]), kf[j] = k[j] == 0 ? 0.0f : (k[j] == 1 ? 1.0f : 2.0f);
+#pragma unroll
+	GLM_N r_f0[j] = glm_self(k[j] == 0, 0.0f, GLM_FADD(GLM_FMUL(kf[j], ln2_hi), GLM_FADD(c[j], GLM_FMUL(kf[j], ln2_lo))));
+#pragma unroll
+	GLM_N R0[j] = GLM_FMUL(hfsq[j], GLM_FSUB(1.0f, GLM_FMUL(0.66666666666666666f, f[j])));
+#pragma unroll
+	GLM_N r_fs[j] = glm_self(k[j] == 0, GLM_FSUB(f[j], R0[j]),
+	                         GLM_FSUB(GLM_FMUL(kf[j], ln2_hi), GLM_FSUB(GLM_FSUB(R0[j], GLM_FADD(GLM_FMUL(kf[j], ln2_lo), c[j])), f[j])));
+#pragma unroll
+	GLM_N s[j] = glm_div(f[j], GLM_FADD(2.0f, f[j]));
+#pragma unroll
+	GLM_N zz[j] = GLM_FMUL(s[j], s[j]);
+#pragma unroll
+	GLM_N R[j] = GLM_FMUL(lp7, zz[j]);
+#pragma unroll
+	GLM_N R[j] = GLM_FMUL(zz[j], GLM_FADD(lp6, R[j]));
+#pragma unroll
+	GLM_N R[j] = GLM_FMUL(zz[j], GLM_FADD(lp5, R[j]));
+#pragma unroll
+	GLM_N R[j] = GLM_FMUL(zz[j], GLM_FADD(lp4, R[j]));
+#pragma unroll
+	GLM_N R[j] = GLM_FMUL(zz[j], GLM_FADD(lp3, R[j]));
+#pragma unroll
+	GLM_N R[j] = GLM_FMUL(zz[j], GLM_FADD(lp2, R[j]));
+#pragma unroll
+	GLM_N R[j] = GLM_FMUL(zz[j], GLM_FADD(lp1, R[j]));
+#pragma unroll
+	GLM_N sR[j] = GLM_FMUL(s[j], GLM_FADD(hfsq[j], R[j]));
+#pragma unroll
+	GLM_N r_p[j] = glm_self(k[j] == 0, GLM_FSUB(f[j], GLM_FSUB(hfsq[j], sR[j])),
+	                        GLM_FSUB(GLM_FMUL(kf[j], ln2_hi),
+	                                 GLM_FSUB(GLM_FSUB(hfsq[j], GLM_FADD(sR[j], GLM_FADD(GLM_FMUL(kf[j], ln2_lo), c[j]))), f[j])));
+#pragma unroll
+	GLM_N out[j] = glm_self(tiny[j], r_tiny[j], glm_self(hu[j] == 0, glm_self(f[j] == 0.0f, r_f0[j], r_fs[j]), r_p[j]));
+}
+#undef GLM_N
+#endif
+
 #endif

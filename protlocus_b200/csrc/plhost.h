@@ -67,7 +67,7 @@ struct pl_engine_s {
 	int64_t g_cached_bases;
 	int64_t g_last_steps;
 	/* recheck Forward */
-	dbuf_t r_prof, r_pep, r_dsq, r_order, r_grp, r_scratch, r_bits, r_bias;
+	dbuf_t r_prof, r_pep, r_dsq, r_order, r_grp, r_err, r_scratch, r_bits, r_bias;
 	int64_t r_last_cells;
 	/* learned-prefilter features */
 	dbuf_t pf_cand, pf_feats, pf_chain, pf_out;

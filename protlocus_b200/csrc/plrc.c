@@ -61,7 +61,7 @@ PL_EXPORT void pl_rc_profile_destroy(pl_rc_profile_t *p)
 void pl_rc_engine_free(pl_engine_t *e)
 {
 	dbuf_free(&e->r_prof), dbuf_free(&e->r_pep), dbuf_free(&e->r_dsq), dbuf_free(&e->r_order);
-	dbuf_free(&e->r_grp), dbuf_free(&e->r_scratch), dbuf_free(&e->r_bits), dbuf_free(&e->r_bias);
+	dbuf_free(&e->r_grp), dbuf_free(&e->r_err), dbuf_free(&e->r_scratch), dbuf_free(&e->r_bits), dbuf_free(&e->r_bias);
 }
 
 typedef struct { int64_t key; int32_t idx; } pl_rkey_t;
@@ -155,7 +155,7 @@ PL_EXPORT int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *pro
 	if (!dbuf_ensure(&e->r_prof, sizeof(*hp) * (size_t)(n_prof > 0 ? n_prof : 1)) ||
 			!dbuf_ensure(&e->r_pep, sizeof(*pep) * (size_t)n) || !dbuf_ensure(&e->r_dsq, (size_t)dsq_len) ||
 			!dbuf_ensure(&e->r_order, sizeof(int32_t) * (size_t)n) ||
-			!dbuf_ensure(&e->r_grp, sizeof(*gs) * (size_t)n_grp) ||
+			!dbuf_ensure(&e->r_grp, sizeof(*gs) * (size_t)n_grp) || !dbuf_ensure(&e->r_err, 64) ||
 			!dbuf_ensure(&e->r_bits, sizeof(float) * (size_t)n) || !dbuf_ensure(&e->r_bias, sizeof(float) * (size_t)n))
 		goto fail;
 	/* waves of groups, each within the scratch budget (the first group of a wave always
@@ -183,6 +183,7 @@ PL_EXPORT int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *pro
 	CK(cudaMemcpyAsync(e->r_pep.p, pep, sizeof(*pep) * (size_t)n, cudaMemcpyHostToDevice, st));
 	CK(cudaMemcpyAsync(e->r_order.p, order, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
 	CK(cudaMemcpyAsync(e->r_grp.p, gs, sizeof(*gs) * (size_t)n_grp, cudaMemcpyHostToDevice, st));
+	CK(cudaMemsetAsync(e->r_err.p, 0, sizeof(int), st));
 	e->n_ev = 0;
 	{
 		int32_t w0 = 0;
@@ -192,14 +193,19 @@ PL_EXPORT int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *pro
 			PL_TIME(e, st, 1);
 			CKK(plk_rc_forward((const plk_rc_prof_t*)e->r_prof.p, (const plk_rc_pep_t*)e->r_pep.p,
 					(const uint8_t*)e->r_dsq.p, (const int32_t*)e->r_order.p, (const plk_rc_grp_t*)e->r_grp.p + w0,
-					w1 - w0, (float*)e->r_scratch.p, (float*)e->r_bits.p, (float*)e->r_bias.p, st));
+					w1 - w0, (float*)e->r_scratch.p, (float*)e->r_bits.p, (float*)e->r_bias.p, (int*)e->r_err.p, st));
 			PL_TIME(e, st, 1);
 			w0 = w1;  /* waves run in stream order, so the next one may reuse the scratch */
 		}
 	}
 	CK(cudaMemcpyAsync(bits, e->r_bits.p, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, st));
 	CK(cudaMemcpyAsync(bias, e->r_bias.p, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, st));
-	CK(cudaStreamSynchronize(st));
+	{
+		int derr = 0;
+		CK(cudaMemcpyAsync(&derr, e->r_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+		CK(cudaStreamSynchronize(st));
+		if (derr) { pl_set_error("recheck Forward: a wait between the warps of a group ran out"); goto fail; }
+	}
 	if (e->timing) {
 		int k;
 		float ms;

@@ -120,6 +120,8 @@ def _bits_of(f):
     (1, 0x00000000, _bits_of(1.0) + 1),    # log1pf at every float in [0, 1], the values expf returns there
     (2, 0x80000000, _bits_of(-50.0) + 1),  # the branch-free forms rc_logsum runs on the device, same ranges
     (3, 0x00000000, _bits_of(1.0) + 1),    # (log1pf's includes the branch-free division)
+    (4, 0x80000000, _bits_of(-50.0) + 1),  # their four-wide forms (four arguments per evaluation)
+    (5, 0x00000000, _bits_of(1.0) + 1),
 ])
 def test_device_libm_equals_host(fn, lo, hi):
     """The device build of the restated expf / log1pf against the host libm at every float bit pattern
