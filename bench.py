@@ -1293,8 +1293,9 @@ def main_forward(args):
                     "h2d_bytes_per_step": int(dsq.nbytes + 20 * len(pid)), "d2h_bytes_per_step": int(8 * len(pid)),
                     "api": "pl_rc_score_host (C ABI, host buffers), wall clock"},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "mufu/fp32", "kernel": "k_rc_forward", "achieved": None, "peak": None, "frac": None,
-                         "note": "transcendental-bound (expf + log1pf per logsum); row chains serial by design"},
+            "roofline": {"bound": "latency", "kernel": "k_rc_lanes", "achieved": None, "peak": None, "frac": None,
+                         "note": "one peptide per lane; the longest peptide's chains (three dependent logsums per "
+                                 "Backward cell, each a restated glibc expf + log1pf) bound the step"},
             "cpu_baseline": {"value": round(c / secs / 1e9, 4), "unit": "GCUPS", "cores": threads, "kind": "reference",
                              "sample": f"{k} peptides, recheck.c rc_score via kt_for"}}
     print(json.dumps(line), flush=True)
