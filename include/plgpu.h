@@ -489,6 +489,12 @@ int64_t pl_rc_last_cells(const pl_engine_t *e);
  * patterns are lo, lo + stride, lo + 2*stride, ... and copies the results to the
  * host array out.  Allocates device memory per call; returns 1 on success. */
 int pl_rc_mathf_eval(int32_t device, int32_t fn, uint32_t lo, uint32_t stride, int64_t n, float *out);
+/* Test hook (no counterpart in the reference): the clock-cycle limit of the waits
+ * between the warps of a recheck Forward group, for every later call of the process;
+ * 0 restores the default (some seconds).  A wait that runs out makes the call fail
+ * (pl_rc_score_host returns 0, pl_last_error says so) without faulting the device:
+ * the group's warps leave their loops and the kernel ends.  Returns 1. */
+int pl_rc_debug_wait_limit(int64_t cycles);
 
 /* DP cells of the last extension batch: the rows the reference's row loop
  * visits (up to the x-drop row, nasw-sse.c:361-447) times al, and the nominal

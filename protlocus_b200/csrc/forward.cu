@@ -122,11 +122,12 @@ __device__ __forceinline__ void str(float *p, float v) { __stcg(p, v); }
  * set and every warp leaves its loops (the barriers that follow are still met).
  */
 #define RC_Q 32                        /* ring depth, columns */
-#define RC_SPIN_LIMIT 10000000000LL    /* clock cycles, some seconds */
+#define RC_SPIN_LIMIT 10000000000LL    /* clock cycles, some seconds: the default limit of a wait */
 #define FULL 0xffffffffu
 
 struct RcSync {
 	volatile int fc, bc, bp, abort;             /* row hand-offs: Forward chain row done, Backward M/I row done, row L */
+	long long lim;                              /* clock cycles a wait may take */
 	volatile unsigned long long m[RC_Q][32];    /* M(i, k) of the Forward's M/I warp, tagged */
 	volatile unsigned long long dn[RC_Q][32];   /* D(i, k+1) of the Backward's chain warp, tagged */
 	volatile unsigned long long fcons[32], bcons[32], bE[32];  /* consumer progress; bE of a Backward row */
@@ -150,7 +151,7 @@ __device__ __forceinline__ float rc_take(RcSync &Y, volatile unsigned long long 
 			v = slot;
 			if (ge ? (int)(v >> 32) >= tag : (int)(v >> 32) == tag) break;
 			if (Y.abort) { ok = false; break; }
-			if (clock64() - t0 > RC_SPIN_LIMIT) { Y.abort = 1; atomicExch(err, 1); ok = false; break; }
+			if (clock64() - t0 > Y.lim) { Y.abort = 1; atomicExch(err, 1); ok = false; break; }
 		}
 	}
 	return __uint_as_float((unsigned)v);
@@ -165,7 +166,7 @@ __device__ __forceinline__ bool rc_wait(RcSync &Y, volatile int &ctr, const int 
 		const long long t0 = clock64();
 		while (ctr < target) {
 			if (Y.abort) { ok = 0; break; }
-			if (clock64() - t0 > RC_SPIN_LIMIT) { Y.abort = 1; atomicExch(err, 1); ok = 0; break; }
+			if (clock64() - t0 > Y.lim) { Y.abort = 1; atomicExch(err, 1); ok = 0; break; }
 			__nanosleep(32);
 		}
 	}
@@ -535,6 +536,7 @@ struct RcArgs {
 	int32_t n_grp;
 	float *scratch, *bits, *bias;
 	int *err;  /* set when a wait between warps ran out */
+	long long spin_limit;
 };
 
 /* one CTA per group, four warps (the hardware hands the groups, longest first, to the
@@ -547,7 +549,7 @@ __global__ void __launch_bounds__(128, 1) k_rc_lanes(RcArgs A)
 	__shared__ RcSync Y;
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	if (threadIdx.x < 32) s_exp2[threadIdx.x] = glm_exp2_tab_dev[threadIdx.x];
-	if (threadIdx.x == 0) Y.fc = Y.bp = Y.bc = -1, Y.abort = 0;
+	if (threadIdx.x == 0) Y.fc = Y.bp = Y.bc = -1, Y.abort = 0, Y.lim = A.spin_limit;
 	for (int x = threadIdx.x; x < RC_Q * 32; x += blockDim.x)  /* no slot carries a tag yet */
 		Y.m[x >> 5][x & 31] = Y.dn[x >> 5][x & 31] = rc_pack(-1, 0.0f);
 	if (threadIdx.x < 32) Y.fcons[threadIdx.x] = Y.bcons[threadIdx.x] = Y.bE[threadIdx.x] = rc_pack(-1, 0.0f);
@@ -595,10 +597,11 @@ __global__ void __launch_bounds__(128, 1) k_rc_lanes(RcArgs A)
 
 extern "C" int plk_rc_forward(const plk_rc_prof_t *prof, const plk_rc_pep_t *pep, const uint8_t *dsq,
 		const int32_t *order, const plk_rc_grp_t *grp, int32_t n_grp, float *scratch, float *bits, float *bias,
-		int *err, void *stream)
+		int *err, int64_t spin_limit, void *stream)
 {
 	if (n_grp <= 0) return 0;
 	RcArgs A;
+	A.spin_limit = spin_limit > 0 ? spin_limit : RC_SPIN_LIMIT;
 	A.prof = prof, A.pep = pep, A.dsq = dsq, A.order = order, A.grp = grp, A.n_grp = n_grp;
 	A.scratch = scratch, A.bits = bits, A.bias = bias, A.err = err;
 	k_rc_lanes<<<(unsigned)n_grp, 128, 0, (cudaStream_t)stream>>>(A);

@@ -181,9 +181,11 @@ typedef struct {
 #define PLK_RC_MAX_M 2048
 int64_t plk_rc_group_floats(int32_t lmax, int32_t M, int32_t full);
 /* err: a device int, set to 1 when a wait between the warps of a group ran out (the
- * launch's results are then invalid) */
+ * launch's results are then invalid); spin_limit: clock cycles a wait may take, 0 the
+ * default */
 int plk_rc_forward(const plk_rc_prof_t *prof, const plk_rc_pep_t *pep, const uint8_t *dsq, const int32_t *order,
-		const plk_rc_grp_t *grp, int32_t n_grp, float *scratch, float *bits, float *bias, int *err, void *stream);
+		const plk_rc_grp_t *grp, int32_t n_grp, float *scratch, float *bits, float *bias, int *err,
+		int64_t spin_limit, void *stream);
 /* CTAs of the DP kernel that fit on one SM at once (occupancy) */
 int plk_dp_ctas_per_sm(int32_t mode, int32_t rows);
 uint64_t plk_launches(void);

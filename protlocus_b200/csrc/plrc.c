@@ -64,6 +64,15 @@ void pl_rc_engine_free(pl_engine_t *e)
 	dbuf_free(&e->r_grp), dbuf_free(&e->r_err), dbuf_free(&e->r_scratch), dbuf_free(&e->r_bits), dbuf_free(&e->r_bias);
 }
 
+/* the limit of the waits between a group's warps (pl_rc_debug_wait_limit), 0: the kernel's default */
+static int64_t g_rc_wait_limit = 0;
+
+PL_EXPORT int pl_rc_debug_wait_limit(int64_t cycles)
+{
+	__atomic_store_n(&g_rc_wait_limit, cycles > 0 ? cycles : 0, __ATOMIC_RELAXED);
+	return 1;
+}
+
 typedef struct { int64_t key; int32_t idx; } pl_rkey_t;
 static int pl_rkey_cmp(const void *a, const void *b)
 {
@@ -193,7 +202,8 @@ PL_EXPORT int pl_rc_score_host(pl_engine_t *e, const pl_rc_profile_t *const *pro
 			PL_TIME(e, st, 1);
 			CKK(plk_rc_forward((const plk_rc_prof_t*)e->r_prof.p, (const plk_rc_pep_t*)e->r_pep.p,
 					(const uint8_t*)e->r_dsq.p, (const int32_t*)e->r_order.p, (const plk_rc_grp_t*)e->r_grp.p + w0,
-					w1 - w0, (float*)e->r_scratch.p, (float*)e->r_bits.p, (float*)e->r_bias.p, (int*)e->r_err.p, st));
+					w1 - w0, (float*)e->r_scratch.p, (float*)e->r_bits.p, (float*)e->r_bias.p, (int*)e->r_err.p,
+					__atomic_load_n(&g_rc_wait_limit, __ATOMIC_RELAXED), st));
 			PL_TIME(e, st, 1);
 			w0 = w1;  /* waves run in stream order, so the next one may reuse the scratch */
 		}

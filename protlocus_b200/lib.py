@@ -133,6 +133,8 @@ def load() -> C.CDLL:
     lib.pl_rc_last_cells.restype = C.c_int64
     lib.pl_rc_mathf_eval.argtypes = [C.c_int32, C.c_int32, C.c_uint32, C.c_uint32, C.c_int64, C.c_void_p]
     lib.pl_rc_mathf_eval.restype = C.c_int
+    lib.pl_rc_debug_wait_limit.argtypes = [C.c_int64]
+    lib.pl_rc_debug_wait_limit.restype = C.c_int
     lib.pl_pf_decide.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_double, C.c_int32,
                                  C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.pl_pf_decide.restype = C.c_int

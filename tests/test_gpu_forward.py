@@ -111,6 +111,31 @@ def test_forward_sweep_bit_exact(engine, null2):
         p.close()
 
 
+def test_wait_between_warps_runs_out_cleanly(engine):
+    """A Forward group's warps hand values over through bounded waits.  With the limit
+    cut to a few cycles a wait runs out: the call fails with the reason (no fault, no
+    hang: the warps leave their loops and the kernel ends), and with the default limit
+    back the same engine scores the batch bit for bit."""
+    texts, probs = H.synthetic_profiles(2, seed=53, m_min=300, m_max=400)
+    handle, profs = O.rc_load("".join(texts))
+    gp = [L.RcProfile(msc, tsc) for _, msc, tsc in profs]
+    rng = np.random.default_rng(13)
+    peps = [(k, O.rc_encode(s)) for k in range(len(profs)) for s in _peptides(rng, probs[k], 8, 300)]
+    lib = engine.lib
+    try:
+        assert lib.pl_rc_debug_wait_limit(4) == 1
+        with pytest.raises(RuntimeError, match="wait between the warps"):
+            engine.rc_score(gp, peps, True)
+    finally:
+        lib.pl_rc_debug_wait_limit(0)
+    bits, bias = engine.rc_score(gp, peps, True)
+    for (k, d), b, s in zip(peps, bits, bias):
+        rb, rs = O.rc_ref_score(handle, k, d, True)
+        assert (b, s) == (np.float32(rb), np.float32(rs)), (k, len(d), b, rb, s, rs)
+    for p in gp:
+        p.close()
+
+
 def _bits_of(f):
     return int(np.array([f], dtype=np.float32).view(np.uint32)[0])
 
