@@ -465,6 +465,25 @@ int64_t pl_gapless_last_steps(const pl_engine_t *e);
  * steps left to the device are the double-precision exp/log of the bias,
  * whose results are rounded to float).
  * ------------------------------------------------------------------------- */
+/* ---- Seeding (the sketch and anchor stages of mp_map_coarse, map.c:565-572) ----
+ * The mapper's k-mer index (mp_idx_t's ki: the first kb entry of every bucket, n_bucket
+ * = 1 << (4 kmer - mod_bit) of them; kb: the block ids, index.c:74-98) copied to a
+ * device.  NULL on bad sizes or a device failure (pl_last_error). */
+typedef struct pl_seed_index_s pl_seed_index_t;
+pl_seed_index_t *pl_seed_index_create(int32_t device, const int64_t *ki, int64_t n_bucket, const uint32_t *kb,
+		int64_t n_kb, int32_t kmer, int32_t mod_bit);
+void pl_seed_index_destroy(pl_seed_index_t *x);
+/* The anchors of n proteins (seq: letters or residue codes 0-21, protein q at seq[off[q]],
+ * len[q] bytes) in the mapper's default mode: mp_sketch_prot's seeds (sketch.c:18-37), the
+ * occurrence cap of mp_cal_max_occ limited by max_occ (map.c:304-320, :566-569), every
+ * block of every seed whose bucket holds at most the cap (mp_collect_anchors without the
+ * accuracy mode's repeat rescue, map.c:346-397), sorted ascending (map.c:571).  Fills
+ * a_off[0..n] (protein q's anchors at a[a_off[q] .. a_off[q+1]), block << 32 | position)
+ * and returns the total; a is written only when the total fits a_cap (call again with a
+ * larger array otherwise).  -1 on a bad argument or a device failure (pl_last_error). */
+int64_t pl_seed_anchors_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq, int64_t seq_len,
+		const int64_t *off, const int32_t *len, int32_t max_occ, int64_t *a_off, uint64_t *a, int64_t a_cap);
+
 typedef struct pl_rc_profile_s pl_rc_profile_t;
 /* A search profile as recheck.c builds it (rc_prof_t, recheck.c:66-72): msc
  * M x 21 match log-odds in nats (column 20 = degenerate residue), tsc M x 8

@@ -1,0 +1,121 @@
+/*
+ * seed_port.c -- test infrastructure: a plain C restatement of the coarse mapper's
+ * seeding (the checker of protlocus_b200/csrc/seed.cu), in the default mode (no
+ * profile-derived seeds, no repeat rescue):
+ *
+ *   sketch    mp_sketch_prot (sketch.c:18-37): residues in the 13-letter alphabet of
+ *             nasw-tab.c:12 (codes 14 and 15, '*', 'X' and other bytes, restart the
+ *             k-mer), 4 bits per residue, the masked integer hash of sketch.c:7-16,
+ *             a seed (hash >> mod_bit) << 32 | position where the hash's low mod_bit
+ *             bits are 0;
+ *   max_occ   mp_cal_max_occ (map.c:304-320): from 8 seeds on, the box-plot bound
+ *             q75 + 1.5 (q75 - q25) + 10 over the seeds' bucket sizes, capped by the
+ *             option (map.c:566-569);
+ *   anchors   mp_collect_anchors (map.c:346-397) without the rescue: every block of
+ *             every seed whose bucket holds at most max_occ, as block << 32 | position;
+ *   order     radix_sort_mp64 of the anchors (map.c:571): ascending.
+ * The index is the reference's (index.c:74-98): ki[b] the first entry of bucket b in
+ * kb, the bucket's end ki[b+1] (n_kb for the last bucket).
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define SP_EXPORT __attribute__((visibility("default")))
+
+/* nasw-tab.c:9-12: the residue letters and their 13-letter groups */
+static const char *sp_aa = "ARNDCQEGHILKMFPSTWYV*X";
+static const uint8_t sp_a2r[22] = { 0, 2, 4, 4, 6, 5, 5, 8, 3, 10, 11, 2, 11, 12, 7, 1, 1, 13, 12, 10, 14, 15 };
+
+SP_EXPORT void sp_aa13_table(uint8_t *tab)
+{
+	int i;
+	memset(tab, 15, 256);
+	for (i = 0; sp_aa[i]; ++i) {
+		const uint8_t c = (uint8_t)sp_aa[i];
+		tab[i] = tab[c] = sp_a2r[i];
+		if (c >= 'A' && c <= 'Z') tab[c + 32] = sp_a2r[i];
+	}
+}
+
+static uint32_t sp_hash(uint32_t key, uint32_t mask)
+{ /* sketch.c:7-16 */
+	key = (key + ~(key << 15)) & mask;
+	key ^= key >> 10;
+	key = (key + (key << 3)) & mask;
+	key ^= key >> 6;
+	key = (key + ~(key << 11)) & mask;
+	key ^= key >> 16;
+	return key;
+}
+
+static int sp_cmp64(const void *a, const void *b)
+{
+	const uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;
+	return x < y ? -1 : x > y;
+}
+
+/* the seeds of one protein; returns their number (at most len) */
+SP_EXPORT int32_t sp_sketch(const uint8_t *seq, int32_t len, int32_t kmer, int32_t mod_bit, uint64_t *seeds)
+{
+	uint8_t tab[256];
+	int32_t i, l = 0, n = 0;
+	const uint32_t mask_k = (1U << kmer * 4) - 1, mask_mod = (1U << mod_bit) - 1;
+	uint32_t x = 0;
+	sp_aa13_table(tab);
+	for (i = 0; i < len; ++i) {
+		const uint32_t c = tab[seq[i]];
+		if (c < 14) {
+			x = (x << 4 | c) & mask_k;
+			if (++l >= kmer) {
+				const uint32_t y = sp_hash(x, mask_k);
+				if ((y & mask_mod) == 0) seeds[n++] = (uint64_t)(y >> mod_bit) << 32 | (uint32_t)i;
+			}
+		} else x = 0, l = 0;
+	}
+	return n;
+}
+
+/* the anchors of one protein into *out (malloc'd, sorted); returns their number, -1 on
+ * a host allocation failure */
+SP_EXPORT int64_t sp_anchors(const int64_t *ki, int64_t n_bucket, const uint32_t *kb, int64_t n_kb, int32_t kmer,
+		int32_t mod_bit, int32_t max_occ_opt, const uint8_t *seq, int32_t len, uint64_t **out)
+{
+	uint64_t *sd = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(len > 0 ? len : 1)), *cnt, *a;
+	int32_t n, i, max_occ = max_occ_opt;
+	int64_t n_a = 0, k = 0, j;
+	*out = 0;
+	if (!sd) return -1;
+	n = sp_sketch(seq, len, kmer, mod_bit, sd);
+	if (n >= 8) {
+		uint64_t q25, q75;
+		cnt = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)n);
+		if (!cnt) { free(sd); return -1; }
+		for (i = 0; i < n; ++i) {
+			const int64_t b = (int64_t)(sd[i] >> 32), en = b + 1 < n_bucket ? ki[b + 1] : n_kb;
+			cnt[i] = (uint64_t)(en - ki[b]);
+		}
+		qsort(cnt, (size_t)n, sizeof(uint64_t), sp_cmp64);
+		q25 = cnt[(int64_t)(n * .25 + .499)], q75 = cnt[(int64_t)(n * .75 + .499)];
+		max_occ = (int32_t)(q75 + (q75 - q25) * 1.5 + 10.);
+		free(cnt);
+		if (max_occ > max_occ_opt) max_occ = max_occ_opt;
+	}
+	for (i = 0; i < n; ++i) {
+		const int64_t b = (int64_t)(sd[i] >> 32), en = b + 1 < n_bucket ? ki[b + 1] : n_kb;
+		if (en - ki[b] <= max_occ) n_a += en - ki[b];
+	}
+	a = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(n_a > 0 ? n_a : 1));
+	if (!a) { free(sd); return -1; }
+	for (i = 0; i < n; ++i) {
+		const int64_t b = (int64_t)(sd[i] >> 32), st = ki[b], en = b + 1 < n_bucket ? ki[b + 1] : n_kb;
+		if (en - st > max_occ) continue;
+		for (j = st; j < en; ++j) a[k++] = (uint64_t)kb[j] << 32 | (uint32_t)sd[i];
+	}
+	qsort(a, (size_t)n_a, sizeof(uint64_t), sp_cmp64);
+	free(sd);
+	*out = a;
+	return n_a;
+}
+
+SP_EXPORT void sp_free(void *p) { free(p); }

@@ -1,0 +1,36 @@
+/*
+ * seed_ref_hook.c -- test infrastructure: appended to a copy of the reference's map.c
+ * (oracle/Makefile, target seedref -> oracle/_ref/libseed_ref.so) so that its static
+ * seeding steps can be called on a given index: mp_sketch_query (map.c:332-343),
+ * mp_cal_max_occ (map.c:304-320), mp_collect_anchors (map.c:346-397) and the anchor
+ * sort (map.c:571), as mp_map_coarse strings them together (map.c:565-572) in the
+ * default mode (options from mp_mapopt_init, no profile).  The checker of
+ * oracle/seed_port.c and of the device seeding.
+ */
+__attribute__((visibility("default")))
+int64_t ref_seed_anchors(const int64_t *ki, const uint32_t *kb, int64_t n_kb, int32_t kmer, int32_t mod_bit,
+		int32_t max_occ_opt, const char *seq, int32_t len, uint64_t **out)
+{
+	mp_idx_t mi;
+	mp_mapopt_t opt;
+	mp64_v sd = {0, 0, 0};
+	int32_t max_occ;
+	int64_t n_a = 0, n_rescued = 0;
+	memset(&mi, 0, sizeof(mi));
+	mp_idxopt_init(&mi.opt);
+	mi.opt.kmer = kmer, mi.opt.mod_bit = mod_bit;
+	mi.ki = (int64_t*)ki, mi.kb = (uint32_t*)kb, mi.n_kb = n_kb;
+	mp_mapopt_init(&opt);
+	opt.max_occ = max_occ_opt;
+	mp_sketch_query(0, &opt, seq, len, kmer, mod_bit, opt.hmm_seed_max, &sd);
+	if (sd.n >= 8) {
+		max_occ = mp_cal_max_occ(0, &mi, sd.n, sd.a);
+		if (max_occ > opt.max_occ) max_occ = opt.max_occ;
+	} else max_occ = opt.max_occ;
+	*out = mp_collect_anchors(0, &mi, &opt, &sd, max_occ, "q", &n_a, &n_rescued);
+	kfree(0, sd.a);
+	radix_sort_mp64(*out, *out + n_a);
+	return n_a;
+}
+
+__attribute__((visibility("default"))) void ref_seed_free(void *p) { kfree(0, p); }

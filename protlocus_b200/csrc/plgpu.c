@@ -194,6 +194,7 @@ PL_EXPORT void pl_engine_destroy(pl_engine_t *e)
 	pl_feat_engine_free(e);
 	pl_ps_engine_free(e);
 	pl_chain_engine_free(e);
+	pl_seed_engine_free(e);
 	if (e->stream) cudaStreamDestroy(e->stream);
 	if (e->side) cudaStreamDestroy(e->side);
 	if (e->ev_fork) cudaEventDestroy(e->ev_fork);

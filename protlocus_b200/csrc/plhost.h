@@ -68,6 +68,8 @@ struct pl_engine_s {
 	int64_t g_last_steps;
 	/* recheck Forward */
 	dbuf_t r_prof, r_pep, r_dsq, r_order, r_grp, r_err, r_scratch, r_bits, r_bias;
+	/* seeding (plseed.c) */
+	dbuf_t s_seq, s_off, s_len, s_seed, s_cnt, s_nseed, s_cap, s_nanc, s_aoff, s_anc, s_anc2, s_tmp;
 	int64_t r_last_cells;
 	/* learned-prefilter features */
 	dbuf_t pf_cand, pf_feats, pf_chain, pf_out;
@@ -108,6 +110,7 @@ void pl_ext_engine_free(pl_engine_t *e);
 void pl_hmm_engine_free(pl_engine_t *e);
 void pl_gapless_engine_free(pl_engine_t *e);
 void pl_rc_engine_free(pl_engine_t *e);
+void pl_seed_engine_free(pl_engine_t *e);
 void pl_pf_engine_free(pl_engine_t *e);
 void pl_feat_engine_free(pl_engine_t *e);
 void pl_ps_engine_free(pl_engine_t *e);

@@ -178,6 +178,28 @@ typedef struct {
 	int32_t prof, lmax;   /* the profile and the longest peptide */
 	int32_t full, pad;    /* full: some peptide takes null2, so every M/I row is kept */
 } plk_rc_grp_t;
+/* seeding of a batch of proteins (seed.cu) */
+typedef struct {
+	const uint8_t *seq;          /* the proteins, concatenated (letters or codes 0-21) */
+	const int64_t *off;          /* protein q at seq[off[q]], len[q] bytes; also its seed slots */
+	const int32_t *len;
+	int32_t n;
+	const int64_t *ki;           /* the index: bucket starts (n_bucket) and block ids (n_kb) */
+	int64_t n_bucket;
+	const uint32_t *kb;
+	int64_t n_kb;
+	int32_t kmer, mod_bit, max_occ;
+	uint64_t *seeds;             /* per residue slot: the seeds, in position order */
+	uint32_t *cnt;               /* per residue slot: the seeds' bucket sizes (reordered) */
+	int32_t *n_seed, *cap;       /* per protein: seeds, occurrence cap */
+	int64_t *n_anchor;           /* per protein: anchors */
+	const int64_t *a_off;        /* per protein: first anchor (n + 1 entries) */
+	uint64_t *anchors;
+} plk_seed_args_t;
+int plk_seed_sketch(const plk_seed_args_t *a, void *stream);
+int plk_seed_emit(const plk_seed_args_t *a, void *stream);
+int plk_seed_sort(const uint64_t *keys_in, uint64_t *keys_out, int64_t n_items, int32_t n_seg, const int64_t *seg_off,
+		void *tmp, size_t *tmp_bytes, void *stream);
 #define PLK_RC_MAX_M 2048
 int64_t plk_rc_group_floats(int32_t lmax, int32_t M, int32_t full);
 /* err: a device int, set to 1 when a wait between the warps of a group ran out (the

@@ -1,0 +1,144 @@
+/*
+ * plseed.c -- host layer of the coarse mapper's seeding on the device (the sketch and
+ * anchor stages of mp_map_coarse, map.c:565-572, default mode; seed.cu).
+ *
+ * The index is the mapper's own (mp_idx_t's ki / kb, index.c:74-98), uploaded once with
+ * pl_seed_index_create.  A batch takes proteins (letters or residue codes 0-21) and
+ * returns, per protein, its anchors (block << 32 | position) sorted ascending, as
+ * mp_collect_anchors and the following radix sort leave them.  The accuracy mode's
+ * repeat rescue (map.c:360-384) and the profile-derived seeds of mp_sketch_hmm are not
+ * done here: a caller in those modes keeps the reference's path.
+ */
+#define _POSIX_C_SOURCE 200809L
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "plhost.h"
+
+struct pl_seed_index_s {
+	int device;
+	int32_t kmer, mod_bit;
+	int64_t n_bucket, n_kb;
+	int64_t *ki;
+	uint32_t *kb;
+};
+
+PL_EXPORT pl_seed_index_t *pl_seed_index_create(int32_t device, const int64_t *ki, int64_t n_bucket, const uint32_t *kb,
+		int64_t n_kb, int32_t kmer, int32_t mod_bit)
+{
+	pl_seed_index_t *x;
+	if (kmer < 1 || kmer > 8 || mod_bit < 0 || mod_bit >= kmer * 4 || n_bucket != (int64_t)1 << (kmer * 4 - mod_bit) ||
+			n_kb < 0 || n_kb > (int64_t)UINT32_MAX || !ki || (n_kb > 0 && !kb)) {
+		pl_set_error("seed index: kmer %d, mod_bit %d, %lld buckets, %lld entries (kmer 1-8, 1 << (4 kmer - mod_bit) buckets)",
+				kmer, mod_bit, (long long)n_bucket, (long long)n_kb);
+		return 0;
+	}
+	x = (pl_seed_index_t*)calloc(1, sizeof(*x));
+	if (!x) { pl_set_error("out of host memory"); return 0; }
+	x->device = device, x->kmer = kmer, x->mod_bit = mod_bit, x->n_bucket = n_bucket, x->n_kb = n_kb;
+	CK(cudaSetDevice(device));
+	CK(cudaMalloc((void**)&x->ki, sizeof(int64_t) * (size_t)n_bucket));
+	CK(cudaMalloc((void**)&x->kb, sizeof(uint32_t) * (size_t)(n_kb > 0 ? n_kb : 1)));
+	CK(cudaMemcpy(x->ki, ki, sizeof(int64_t) * (size_t)n_bucket, cudaMemcpyHostToDevice));
+	if (n_kb > 0) CK(cudaMemcpy(x->kb, kb, sizeof(uint32_t) * (size_t)n_kb, cudaMemcpyHostToDevice));
+	return x;
+fail:
+	if (x->ki) cudaFree(x->ki);
+	if (x->kb) cudaFree(x->kb);
+	free(x);
+	return 0;
+}
+
+PL_EXPORT void pl_seed_index_destroy(pl_seed_index_t *x)
+{
+	if (!x) return;
+	cudaSetDevice(x->device);
+	cudaFree(x->ki), cudaFree(x->kb);
+	free(x);
+}
+
+void pl_seed_engine_free(pl_engine_t *e)
+{
+	dbuf_free(&e->s_seq), dbuf_free(&e->s_off), dbuf_free(&e->s_len), dbuf_free(&e->s_seed), dbuf_free(&e->s_cnt);
+	dbuf_free(&e->s_nseed), dbuf_free(&e->s_cap), dbuf_free(&e->s_nanc), dbuf_free(&e->s_aoff);
+	dbuf_free(&e->s_anc), dbuf_free(&e->s_anc2), dbuf_free(&e->s_tmp);
+}
+
+PL_EXPORT int64_t pl_seed_anchors_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
+		int64_t seq_len, const int64_t *off, const int32_t *len, int32_t max_occ, int64_t *a_off, uint64_t *a,
+		int64_t a_cap)
+{
+	plk_seed_args_t A;
+	int64_t *na = 0, total = 0, ret = -1;
+	int32_t q;
+	size_t tmp_bytes = 0;
+	cudaStream_t st;
+	if (!e || !x) { pl_set_error("no engine or index"); return -1; }
+	if (x->device != e->device) { pl_set_error("seed index on device %d, engine on %d", x->device, e->device); return -1; }
+	if (n < 0 || !a_off || (n > 0 && (!seq || !off || !len))) { pl_set_error("seed batch: bad arguments"); return -1; }
+	a_off[0] = 0;
+	if (n == 0) return 0;
+	for (q = 0; q < n; ++q)
+		if (len[q] < 0 || off[q] < 0 || off[q] + len[q] > seq_len) {
+			pl_set_error("protein %d: length %d at %lld of %lld", q, len[q], (long long)off[q], (long long)seq_len);
+			return -1;
+		}
+	st = e->stream;
+	CK(cudaSetDevice(e->device));
+	na = (int64_t*)malloc(sizeof(int64_t) * (size_t)n);
+	if (!na) { pl_set_error("out of host memory"); return -1; }
+	if (!dbuf_ensure(&e->s_seq, (size_t)(seq_len > 0 ? seq_len : 1)) || !dbuf_ensure(&e->s_off, sizeof(int64_t) * (size_t)n) ||
+			!dbuf_ensure(&e->s_len, sizeof(int32_t) * (size_t)n) ||
+			!dbuf_ensure(&e->s_seed, sizeof(uint64_t) * (size_t)(seq_len > 0 ? seq_len : 1)) ||
+			!dbuf_ensure(&e->s_cnt, sizeof(uint32_t) * (size_t)(seq_len > 0 ? seq_len : 1)) ||
+			!dbuf_ensure(&e->s_nseed, sizeof(int32_t) * (size_t)n) || !dbuf_ensure(&e->s_cap, sizeof(int32_t) * (size_t)n) ||
+			!dbuf_ensure(&e->s_nanc, sizeof(int64_t) * (size_t)n) || !dbuf_ensure(&e->s_aoff, sizeof(int64_t) * (size_t)(n + 1)))
+		goto fail;
+	if (seq_len > 0) CK(cudaMemcpyAsync(e->s_seq.p, seq, (size_t)seq_len, cudaMemcpyHostToDevice, st));
+	CK(cudaMemcpyAsync(e->s_off.p, off, sizeof(int64_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+	CK(cudaMemcpyAsync(e->s_len.p, len, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+	memset(&A, 0, sizeof(A));
+	A.seq = (const uint8_t*)e->s_seq.p, A.off = (const int64_t*)e->s_off.p, A.len = (const int32_t*)e->s_len.p, A.n = n;
+	A.ki = x->ki, A.n_bucket = x->n_bucket, A.kb = x->kb, A.n_kb = x->n_kb;
+	A.kmer = x->kmer, A.mod_bit = x->mod_bit, A.max_occ = max_occ;
+	A.seeds = (uint64_t*)e->s_seed.p, A.cnt = (uint32_t*)e->s_cnt.p;
+	A.n_seed = (int32_t*)e->s_nseed.p, A.cap = (int32_t*)e->s_cap.p, A.n_anchor = (int64_t*)e->s_nanc.p;
+	e->n_ev = 0;
+	PL_TIME(e, st, 1);
+	CKK(plk_seed_sketch(&A, st));
+	PL_TIME(e, st, 1);
+	CK(cudaMemcpyAsync(na, e->s_nanc.p, sizeof(int64_t) * (size_t)n, cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	for (q = 0; q < n; ++q) total += na[q], a_off[q + 1] = total;
+	ret = total;
+	if (total > a_cap || total == 0) goto done;  /* a_off only: the caller grows a to a_off[n] */
+	if (!dbuf_ensure(&e->s_anc, sizeof(uint64_t) * (size_t)total) || !dbuf_ensure(&e->s_anc2, sizeof(uint64_t) * (size_t)total))
+		goto fail;
+	CK(cudaMemcpyAsync(e->s_aoff.p, a_off, sizeof(int64_t) * (size_t)(n + 1), cudaMemcpyHostToDevice, st));
+	A.a_off = (const int64_t*)e->s_aoff.p, A.anchors = (uint64_t*)e->s_anc.p;
+	PL_TIME(e, st, 1);
+	CKK(plk_seed_emit(&A, st));
+	CKK(plk_seed_sort((const uint64_t*)e->s_anc.p, (uint64_t*)e->s_anc2.p, total, n, (const int64_t*)e->s_aoff.p, 0,
+			&tmp_bytes, st));
+	if (!dbuf_ensure(&e->s_tmp, tmp_bytes > 0 ? tmp_bytes : 16)) goto fail;
+	CKK(plk_seed_sort((const uint64_t*)e->s_anc.p, (uint64_t*)e->s_anc2.p, total, n, (const int64_t*)e->s_aoff.p,
+			e->s_tmp.p, &tmp_bytes, st));
+	PL_TIME(e, st, 1);
+	CK(cudaMemcpyAsync(a, e->s_anc2.p, sizeof(uint64_t) * (size_t)total, cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+done:
+	if (e->timing) {  /* the sketch, and the emission with the sort */
+		int k;
+		float ms;
+		for (k = 0; k + 1 < e->n_ev; k += 2) {
+			cudaEventElapsedTime(&ms, e->ev[k], e->ev[k + 1]);
+			e->acc_ms[e->ev_kind[k]] += ms;
+		}
+		e->acc_dp_launches += e->n_ev / 2;
+	}
+	free(na);
+	return ret;
+fail:
+	free(na);
+	return -1;
+}

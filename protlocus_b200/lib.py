@@ -135,6 +135,12 @@ def load() -> C.CDLL:
     lib.pl_rc_mathf_eval.restype = C.c_int
     lib.pl_rc_debug_wait_limit.argtypes = [C.c_int64]
     lib.pl_rc_debug_wait_limit.restype = C.c_int
+    lib.pl_seed_index_create.argtypes = [C.c_int32, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32, C.c_int32]
+    lib.pl_seed_index_create.restype = C.c_void_p
+    lib.pl_seed_index_destroy.argtypes = [C.c_void_p]
+    lib.pl_seed_anchors_host.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
+                                         C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64]
+    lib.pl_seed_anchors_host.restype = C.c_int64
     lib.pl_pf_decide.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_double, C.c_int32,
                                  C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.pl_pf_decide.restype = C.c_int
@@ -609,6 +615,46 @@ class Engine:
                                          bias.ctypes.data):
             raise RuntimeError("pl_rc_score_host failed: " + error())
         return bits, bias
+
+
+class SeedIndex:
+    """A pl_seed_index_t: the mapper's k-mer index (ki int64 bucket starts, kb uint32 block ids) on a device."""
+
+    def __init__(self, ki, kb, kmer: int, mod_bit: int, device: int = 0):
+        self.lib = load()
+        ki = np.ascontiguousarray(ki, dtype=np.int64)
+        kb = np.ascontiguousarray(kb, dtype=np.uint32)
+        self.h = self.lib.pl_seed_index_create(device, ki.ctypes.data, ki.size, kb.ctypes.data, kb.size, kmer, mod_bit)
+        if not self.h:
+            raise RuntimeError("pl_seed_index_create: " + error())
+
+    def close(self):
+        if self.h:
+            self.lib.pl_seed_index_destroy(self.h)
+            self.h = None
+
+
+def seed_anchors(eng, index: SeedIndex, proteins, max_occ: int):
+    """Anchors of a list of proteins (bytes) through pl_seed_anchors_host: a list of sorted uint64 arrays."""
+    n = len(proteins)
+    lens = np.array([len(p) for p in proteins], dtype=np.int32)
+    offs = np.zeros(n, dtype=np.int64)
+    if n > 1:
+        offs[1:] = np.cumsum(lens[:-1])
+    seq = np.frombuffer(b"".join(proteins), dtype=np.uint8) if n else np.zeros(1, np.uint8)
+    seq = np.ascontiguousarray(seq if seq.size else np.zeros(1, np.uint8))
+    a_off = np.zeros(n + 1, dtype=np.int64)
+    cap = 1 << 20
+    for _ in range(2):
+        a = np.zeros(max(cap, 1), dtype=np.uint64)
+        tot = eng.lib.pl_seed_anchors_host(eng.h, index.h, n, seq.ctypes.data, int(lens.sum()), offs.ctypes.data,
+                                           lens.ctypes.data, max_occ, a_off.ctypes.data, a.ctypes.data, cap)
+        if tot < 0:
+            raise RuntimeError("pl_seed_anchors_host: " + error())
+        if tot <= cap:
+            return [a[a_off[q]:a_off[q + 1]].copy() for q in range(n)]
+        cap = int(tot)
+    raise RuntimeError("pl_seed_anchors_host: capacity")
 
 
 class RcProfile:

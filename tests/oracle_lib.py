@@ -386,3 +386,72 @@ def ref_chain_batch(opt: dict, off, n, a, threads: int) -> int:
     return int(lib.ref_chain_batch(opt["max_dist_x"], opt["max_dist_y"], opt["bw"], opt["max_skip"], opt["max_iter"],
                                    opt["min_cnt"], opt["min_sc"], opt["coef"], opt["is_spliced"], opt["kmer"],
                                    opt["bbit"], len(n), off.ctypes.data, n.ctypes.data, a.ctypes.data, threads))
+
+
+# ---------------------------------------------------------------- seeding (map.c:304-397, sketch.c:18-37)
+
+SEED_REF_SO = os.path.join(ORACLE, "_ref", "libseed_ref.so")
+_seed_ref = None
+
+
+def seed_ref_lib():
+    """The reference's own seeding steps (map.c with oracle/seed_ref_hook.c), or None."""
+    global _seed_ref
+    if _seed_ref is None and os.path.exists(SEED_REF_SO):
+        lib = C.CDLL(SEED_REF_SO)
+        lib.ns_make_tables(1)
+        lib.ref_seed_anchors.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
+                                         C.c_char_p, C.c_int32, C.POINTER(C.POINTER(C.c_uint64))]
+        lib.ref_seed_anchors.restype = C.c_int64
+        lib.ref_seed_free.argtypes = [C.c_void_p]
+        _seed_ref = lib
+    return _seed_ref
+
+
+def _seed_port():
+    lib = port_lib()
+    if not hasattr(lib, "_seed_ready"):
+        lib.sp_anchors.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
+                                   C.c_char_p, C.c_int32, C.POINTER(C.POINTER(C.c_uint64))]
+        lib.sp_anchors.restype = C.c_int64
+        lib.sp_free.argtypes = [C.c_void_p]
+        lib._seed_ready = True
+    return lib
+
+
+def seed_index(rng, kmer: int = 6, mod_bit: int = 1, mean_occ: float = 3.0, n_block: int = 400_000,
+               hot: int = 64, hot_occ: int = 30_000):
+    """A synthetic index in the reference's layout (index.c:74-98): ki[b] = first entry of bucket
+    b in kb (int64), kb = block ids (uint32).  Bucket sizes are Poisson(mean_occ) with `hot`
+    buckets of about hot_occ entries (repeats, which the occurrence cap drops)."""
+    n_bucket = 1 << (kmer * 4 - mod_bit)
+    cnt = rng.poisson(mean_occ, size=n_bucket).astype(np.int64)
+    cnt[rng.choice(n_bucket, size=hot, replace=False)] = rng.integers(hot_occ // 2, hot_occ, size=hot)
+    ki = np.zeros(n_bucket, dtype=np.int64)
+    ki[1:] = np.cumsum(cnt[:-1])
+    kb = rng.integers(0, n_block, size=int(cnt.sum()), dtype=np.uint32)
+    return ki, kb
+
+
+def _seed_take(fn, free, *args):
+    out = C.POINTER(C.c_uint64)()
+    n = fn(*args, C.byref(out))
+    if n < 0:
+        raise MemoryError("seeding checker out of host memory")
+    a = np.ctypeslib.as_array(out, shape=(max(n, 1),))[:n].copy() if n > 0 else np.zeros(0, np.uint64)
+    free(out)
+    return a
+
+
+def seed_anchors(ki, kb, kmer: int, mod_bit: int, max_occ: int, seq: bytes, use_ref: bool | None = None):
+    """Sorted anchors (block << 32 | position, uint64) of one protein: the reference's own
+    steps when oracle/_ref/libseed_ref.so is built (or use_ref), else the port."""
+    lib = seed_ref_lib() if use_ref is not False else None
+    if use_ref and lib is None:
+        raise RuntimeError("oracle/_ref/libseed_ref.so not built")
+    if lib is not None:
+        return _seed_take(lib.ref_seed_anchors, lib.ref_seed_free, ki.ctypes.data, kb.ctypes.data, kb.size, kmer,
+                          mod_bit, max_occ, seq, len(seq))
+    p = _seed_port()
+    return _seed_take(p.sp_anchors, p.sp_free, ki.ctypes.data, ki.size, kb.ctypes.data, kb.size, kmer, mod_bit,
+                      max_occ, seq, len(seq))

@@ -1,0 +1,73 @@
+"""Seeding on the device (seed.cu, pl_seed_anchors_host) against the reference's own
+steps (map.c's mp_sketch_query, mp_cal_max_occ, mp_collect_anchors and the anchor sort,
+oracle/_ref/libseed_ref.so; the restatement oracle/seed_port.c where that is not built):
+the same sorted anchors per protein, bit for bit, on synthetic indexes in the mapper's
+layout with hot (repeat) buckets, for several sampling rates and occurrence caps;
+proteins with stops, X, lowercase letters, residue codes, repeats, and fewer than 8 seeds.
+Also: an empty batch, an empty index, and the capacity rule (a_off filled, anchors not)."""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from protlocus_b200 import lib as L
+from test_seed import seed_proteins
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def engine():
+    e = L.Engine(0)
+    yield e
+    e.close()
+
+
+@pytest.mark.parametrize("mod_bit,max_occ", [(1, 20000), (1, 40), (2, 500), (0, 200)])
+def test_seed_anchors_match_reference(engine, mod_bit, max_occ):
+    rng = np.random.default_rng(200 + mod_bit * 7 + max_occ)
+    ki, kb = O.seed_index(rng, kmer=6, mod_bit=mod_bit, n_block=300_000)
+    idx = L.SeedIndex(ki, kb, 6, mod_bit)
+    try:
+        prots = seed_proteins(rng, 300)
+        got = L.seed_anchors(engine, idx, prots, max_occ)
+        for q, seq in enumerate(prots):
+            want = O.seed_anchors(ki, kb, 6, mod_bit, max_occ, seq)
+            assert np.array_equal(got[q], want), (q, len(seq), got[q].size, want.size)
+    finally:
+        idx.close()
+
+
+def test_seed_edges(engine):
+    rng = np.random.default_rng(7)
+    ki, kb = O.seed_index(rng, kmer=6, mod_bit=1, n_block=1000)
+    idx = L.SeedIndex(ki, kb, 6, 1)
+    lib = engine.lib
+    import ctypes as C
+    try:
+        assert L.seed_anchors(engine, idx, [], 100) == []
+        prots = seed_proteins(rng, 20)
+        want = [O.seed_anchors(ki, kb, 6, 1, 20000, s) for s in prots]
+        # the capacity rule: a too small array gets the offsets only
+        n = len(prots)
+        lens = np.array([len(p) for p in prots], np.int32)
+        offs = np.zeros(n, np.int64)
+        offs[1:] = np.cumsum(lens[:-1])
+        seq = np.frombuffer(b"".join(prots), np.uint8).copy()
+        a_off = np.zeros(n + 1, np.int64)
+        a = np.zeros(1, np.uint64)
+        tot = lib.pl_seed_anchors_host(engine.h, idx.h, n, seq.ctypes.data, seq.size, offs.ctypes.data,
+                                       lens.ctypes.data, 20000, a_off.ctypes.data, a.ctypes.data, 0)
+        assert tot == sum(w.size for w in want) and list(np.diff(a_off)) == [w.size for w in want]
+        # a protein span past the sequence is refused
+        bad = lens.copy()
+        bad[-1] += 5
+        assert lib.pl_seed_anchors_host(engine.h, idx.h, n, seq.ctypes.data, seq.size, offs.ctypes.data,
+                                        bad.ctypes.data, 20000, a_off.ctypes.data, a.ctypes.data, 0) == -1
+    finally:
+        idx.close()
+    empty = L.SeedIndex(np.zeros(1 << 23, np.int64), np.zeros(0, np.uint32), 6, 1)
+    try:
+        got = L.seed_anchors(engine, empty, [b"ARNDCQEGHILK" * 5], 100)
+        assert got[0].size == 0
+    finally:
+        empty.close()

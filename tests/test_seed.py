@@ -1,0 +1,70 @@
+"""The seeding restatement (oracle/seed_port.c) against the reference's own steps
+(map.c's mp_sketch_query, mp_cal_max_occ, mp_collect_anchors and the anchor sort,
+map.c:304-397 and :565-572, sketch.c:18-37; oracle/_ref/libseed_ref.so built from the
+reference's sources with oracle/seed_ref_hook.c): the same sorted anchors, on
+synthetic indexes in the reference's layout.  Proteins: random residues, repeats of a
+short motif (hot buckets), stop and X runs (k-mer restarts), lowercase letters,
+residue codes, very short ones (fewer than 8 seeds: the option's cap alone)."""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+
+need_ref = pytest.mark.skipif(O.seed_ref_lib() is None, reason="oracle/_ref/libseed_ref.so not built")
+AA = b"ARNDCQEGHILKMFPSTWYV"
+
+
+def seed_proteins(rng, n):
+    out = []
+    for q in range(n):
+        L = int(rng.integers(1, 1200))
+        s = bytearray(AA[int(x)] for x in rng.integers(0, 20, size=L))
+        kind = q % 6
+        if kind == 1 and L > 40:  # a repeated motif: the same k-mers many times
+            m = bytes(s[:7])
+            for p in range(0, L - 7, 9):
+                s[p:p + 7] = m
+        elif kind == 2:  # stops and X restart the k-mer
+            for p in rng.integers(0, L, size=max(1, L // 30)):
+                s[p] = ord("*") if rng.random() < 0.5 else ord("X")
+        elif kind == 3:
+            s = bytearray(s.lower())
+        elif kind == 4:  # residue codes 0-21 instead of letters
+            s = bytearray(int(x) for x in rng.integers(0, 22, size=L))
+        elif kind == 5:
+            s = s[: int(rng.integers(1, 12))]
+        out.append(bytes(s))
+    return out
+
+
+@need_ref
+@pytest.mark.parametrize("mod_bit,max_occ", [(1, 20000), (1, 40), (2, 20000), (0, 200)])
+def test_seed_port_equals_reference(mod_bit, max_occ):
+    rng = np.random.default_rng(100 + mod_bit * 7 + max_occ)
+    ki, kb = O.seed_index(rng, kmer=6, mod_bit=mod_bit, n_block=200_000)
+    for seq in seed_proteins(rng, 60):
+        ref = O.seed_anchors(ki, kb, 6, mod_bit, max_occ, seq, use_ref=True)
+        port = O.seed_anchors(ki, kb, 6, mod_bit, max_occ, seq, use_ref=False)
+        assert np.array_equal(ref, port), (len(seq), ref.size, port.size)
+
+
+def test_seed_port_hand_case():
+    """ARNDCQ (six residues, kmer 6): one k-mer, a seed iff its hash has mod_bit zero low bits;
+    with mod_bit 0 every k-mer is a seed, and a bucket of three blocks gives three anchors."""
+    kmer, mod_bit = 6, 0
+    n_bucket = 1 << (kmer * 4)
+    ki = np.zeros(n_bucket, dtype=np.int64)
+    kb = np.zeros(0, dtype=np.uint32)
+    a = O.seed_anchors(ki, kb, kmer, mod_bit, 100, b"ARNDCQ", use_ref=False)
+    assert a.size == 0  # empty index
+    # the seed's bucket, from the port's sketch: give it three blocks
+    import ctypes as C
+    lib = O.port_lib()
+    lib.sp_sketch.argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
+    sd = np.zeros(8, np.uint64)
+    assert lib.sp_sketch(b"ARNDCQ", 6, kmer, mod_bit, sd.ctypes.data) == 1
+    b = int(sd[0] >> np.uint64(32))
+    ki[b + 1:] = 3
+    kb = np.array([7, 5, 9], dtype=np.uint32)
+    a = O.seed_anchors(ki, kb, kmer, mod_bit, 100, b"ARNDCQ", use_ref=False)
+    assert [int(x >> np.uint64(32)) for x in a] == [5, 7, 9] and all(int(x) & 0xffffffff == 5 for x in a)
