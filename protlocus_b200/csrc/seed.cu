@@ -7,10 +7,11 @@
  * (map.c:571).  The index is the reference's own (index.c:74-98), on the device:
  * ki[b] the first entry of bucket b in kb, the bucket's end ki[b+1] (n_kb for the last).
  *
- *   k_seed_sketch  one thread per protein: the rolling 4-bit k-mer over the 13-letter
- *                  alphabet, the masked integer hash, the seeds in position order, each
- *                  seed's bucket size, and the cap (the 25 % and 75 % order statistics
- *                  of the sizes by an in-place selection) and the anchor count.
+ *   k_seed_sketch  one warp per protein: the 4-bit k-mers over the 13-letter alphabet of
+ *                  32 positions at a time, the masked integer hash, the seeds compacted
+ *                  in position order, their bucket sizes (32 lookups in flight), the cap
+ *                  (the 25 % and 75 % order statistics of the sizes by a warp radix
+ *                  select) and the anchor count.
  *   k_seed_emit    one warp per protein: for each seed in order whose bucket is within
  *                  the cap, the lanes copy the bucket's blocks as block << 32 | position.
  * The anchors of each protein are then sorted (cub::DeviceSegmentedSort, ascending 64-bit
@@ -40,35 +41,38 @@ __device__ __forceinline__ uint32_t sd_hash(uint32_t key, const uint32_t mask)
 	return key;
 }
 
-/* the k-th smallest of v[0..n) (0-based), reordering v: Hoare partitions */
-__device__ uint32_t sd_select(uint32_t *v, int64_t n, const int64_t k)
-{
-	int64_t lo = 0, hi = n - 1;
-	while (lo < hi) {
-		const uint32_t pivot = v[lo + (hi - lo) / 2];
-		int64_t i = lo, j = hi;
-		while (i <= j) {
-			while (v[i] < pivot) ++i;
-			while (v[j] > pivot) --j;
-			if (i <= j) {
-				const uint32_t t = v[i];
-				v[i] = v[j], v[j] = t;
-				++i, --j;
-			}
-		}
-		if (k <= j) hi = j;
-		else if (k >= i) lo = i;
-		else return v[k];
-	}
-	return v[k];
-}
-
 __device__ __forceinline__ int64_t sd_bucket_size(const int64_t *ki, const int64_t n_bucket, const int64_t n_kb, const int64_t b)
 {
 	return (b + 1 < n_bucket ? ki[b + 1] : n_kb) - ki[b];
 }
 
-__global__ void __launch_bounds__(128) k_seed_sketch(plk_seed_args_t A)
+__device__ __forceinline__ int64_t sd_warp_sum(int64_t v)
+{
+#pragma unroll
+	for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+
+/* the k-th smallest (0-based) of v[0..n), the whole warp: bit by bit from the top, the
+ * values that share the bits chosen so far and have a 0 next are counted */
+__device__ uint32_t sd_select(const uint32_t *v, const int32_t n, int64_t k, const int lane)
+{
+	uint32_t prefix = 0, mask = 0;
+	for (int bit = 31; bit >= 0; --bit) {
+		const uint32_t m = mask | 1u << bit;
+		int64_t c = 0;
+		for (int32_t j = lane; j < n; j += 32) c += (v[j] & m) == prefix;
+		c = sd_warp_sum(c);
+		if (k >= c) k -= c, prefix |= 1u << bit;
+		mask = m;
+	}
+	return prefix;
+}
+
+/* one warp per protein: the seeds in position order (a position's k-mer is its last kmer
+ * residues when none of them restarts the k-mer, which is what the reference's rolling
+ * k-mer holds), their bucket sizes, the cap and the anchor count */
+__global__ void __launch_bounds__(256) k_seed_sketch(plk_seed_args_t A)
 {
 	__shared__ uint8_t tab[256];
 	for (int x = threadIdx.x; x < 256; x += blockDim.x) tab[x] = 15;
@@ -79,43 +83,53 @@ __global__ void __launch_bounds__(128) k_seed_sketch(plk_seed_args_t A)
 		if (c >= 'A' && c <= 'Z') tab[c + 32] = g;
 	}
 	__syncthreads();
-	const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	if (q >= A.n) return;
+	const int lane = threadIdx.x & 31;
+	const int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	if (q >= A.n) return;  /* whole warps */
 	const uint8_t *seq = A.seq + A.off[q];
-	const int32_t len = A.len[q];
+	const int32_t len = A.len[q], kmer = A.kmer;
 	uint64_t *sd = A.seeds + A.off[q];
 	uint32_t *cnt = A.cnt + A.off[q];
-	const uint32_t mask_k = (1U << A.kmer * 4) - 1, mask_mod = (1U << A.mod_bit) - 1;
-	uint32_t x = 0;
-	int32_t l = 0, n = 0;
-	for (int32_t i = 0; i < len; ++i) {
-		const uint32_t c = tab[seq[i]];
-		if (c < 14) {
-			x = (x << 4 | c) & mask_k;
-			if (++l >= A.kmer) {
-				const uint32_t y = sd_hash(x, mask_k);
-				if ((y & mask_mod) == 0) {
-					sd[n] = (uint64_t)(y >> A.mod_bit) << 32 | (uint32_t)i;
-					cnt[n] = (uint32_t)sd_bucket_size(A.ki, A.n_bucket, A.n_kb, (int64_t)(y >> A.mod_bit));
-					++n;
-				}
+	const uint32_t mask_k = (1U << kmer * 4) - 1, mask_mod = (1U << A.mod_bit) - 1;
+	int32_t n = 0;
+	for (int32_t i0 = 0; i0 < len; i0 += 32) {
+		const int32_t i = i0 + lane;
+		bool is_seed = false;
+		uint64_t key = 0;
+		if (i < len && i >= kmer - 1) {
+			uint32_t x = 0;
+			bool ok = true;
+			for (int32_t t = i - kmer + 1; t <= i; ++t) {
+				const uint32_t c = tab[seq[t]];
+				ok = ok && c < 14;
+				x = (x << 4 | c) & mask_k;
 			}
-		} else x = 0, l = 0;
+			if (ok) {
+				const uint32_t y = sd_hash(x, mask_k);
+				if ((y & mask_mod) == 0) is_seed = true, key = (uint64_t)(y >> A.mod_bit) << 32 | (uint32_t)i;
+			}
+		}
+		const unsigned bal = __ballot_sync(0xffffffffu, is_seed);
+		if (is_seed) {
+			const int32_t j = n + __popc(bal & ((1u << lane) - 1));
+			sd[j] = key;
+			cnt[j] = (uint32_t)sd_bucket_size(A.ki, A.n_bucket, A.n_kb, (int64_t)(key >> 32));
+		}
+		n += __popc(bal);
 	}
+	__syncwarp();
 	int32_t max_occ = A.max_occ;
-	if (n >= 8) {  /* map.c:310-319: sizes sorted, q25 and q75 picked by index */
+	if (n >= 8) {  /* map.c:310-319: the sizes' order statistics at these indices */
 		const int64_t k25 = (int64_t)(n * .25 + .499), k75 = (int64_t)(n * .75 + .499);
-		const uint64_t q75 = sd_select(cnt, n, k75);
-		const uint64_t q25 = sd_select(cnt, k75 + 1, k25);  /* the k75+1 smallest are in cnt[0..k75] now */
+		const uint64_t q75 = sd_select(cnt, n, k75, lane), q25 = sd_select(cnt, n, k25, lane);
 		max_occ = (int32_t)__dadd_rn(__dadd_rn((double)q75, __dmul_rn((double)(q75 - q25), 1.5)), 10.);
 		if (max_occ > A.max_occ) max_occ = A.max_occ;
 	}
 	int64_t n_a = 0;
-	for (int32_t j = 0; j < n; ++j) {
-		const int64_t sz = sd_bucket_size(A.ki, A.n_bucket, A.n_kb, (int64_t)(sd[j] >> 32));
-		if (sz <= max_occ) n_a += sz;
-	}
-	A.n_seed[q] = n, A.cap[q] = max_occ, A.n_anchor[q] = n_a;
+	for (int32_t j = lane; j < n; j += 32)
+		if ((int64_t)cnt[j] <= max_occ) n_a += cnt[j];
+	n_a = sd_warp_sum(n_a);
+	if (lane == 0) A.n_seed[q] = n, A.cap[q] = max_occ, A.n_anchor[q] = n_a;
 }
 
 __global__ void __launch_bounds__(256) k_seed_emit(plk_seed_args_t A)
@@ -142,7 +156,7 @@ __global__ void __launch_bounds__(256) k_seed_emit(plk_seed_args_t A)
 extern "C" int plk_seed_sketch(const plk_seed_args_t *a, void *stream)
 {
 	if (a->n <= 0) return 0;
-	k_seed_sketch<<<(unsigned)((a->n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(*a);
+	k_seed_sketch<<<(unsigned)((a->n * 32 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*a);
 	plk_add_launches(1);
 	return (int)cudaGetLastError();
 }
