@@ -12,8 +12,8 @@
  *                  in position order, their bucket sizes (32 lookups in flight), the cap
  *                  (the 25 % and 75 % order statistics of the sizes by a warp radix
  *                  select) and the anchor count.
- *   k_seed_emit    one warp per protein: for each seed in order whose bucket is within
- *                  the cap, the lanes copy the bucket's blocks as block << 32 | position.
+ *   k_seed_emit    one warp per protein: 32 seeds at a time, their kept buckets laid out by
+ *                  a warp scan, the lanes copy the blocks as block << 32 | position.
  * The anchors of each protein are then sorted (cub::DeviceSegmentedSort, ascending 64-bit
  * keys: equal keys are equal values, so any sort leaves the reference's array).
  */
@@ -132,22 +132,53 @@ __global__ void __launch_bounds__(256) k_seed_sketch(plk_seed_args_t A)
 	if (lane == 0) A.n_seed[q] = n, A.cap[q] = max_occ, A.n_anchor[q] = n_a;
 }
 
-__global__ void __launch_bounds__(256) k_seed_emit(plk_seed_args_t A)
+#define SD_EMIT_WARPS 8
+__global__ void __launch_bounds__(32 * SD_EMIT_WARPS) k_seed_emit(plk_seed_args_t A)
 {
-	const int lane = threadIdx.x & 31;
+	__shared__ int64_t s_pre[SD_EMIT_WARPS][33], s_st[SD_EMIT_WARPS][32];
+	__shared__ uint32_t s_pos[SD_EMIT_WARPS][32];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	const int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	if (q >= A.n) return;
+	if (q >= A.n) return;  /* whole warps */
 	const uint64_t *sd = A.seeds + A.off[q];
 	const int32_t n = A.n_seed[q], max_occ = A.cap[q];
 	uint64_t *a = A.anchors + A.a_off[q];
 	int64_t k = 0;
-	for (int32_t j = 0; j < n; ++j) {
-		const int64_t b = (int64_t)(sd[j] >> 32), st = A.ki[b];
-		const int64_t sz = (b + 1 < A.n_bucket ? A.ki[b + 1] : A.n_kb) - st;
-		if (sz > max_occ) continue;
-		const uint64_t pos = (uint32_t)sd[j];
-		for (int64_t t = lane; t < sz; t += 32) a[k + t] = (uint64_t)A.kb[st + t] << 32 | pos;
-		k += sz;
+	/* 32 seeds at a time: their buckets' starts and sizes (0 past the cap) side by side, an
+	 * exclusive scan of the sizes, then every lane copies blocks of any of the 32 seeds
+	 * (the seed of output t: the last one whose offset is at most t) */
+	for (int32_t j0 = 0; j0 < n; j0 += 32) {
+		const int32_t j = j0 + lane;
+		int64_t st = 0, sz = 0;
+		uint32_t pos = 0;
+		if (j < n) {
+			const int64_t b = (int64_t)(sd[j] >> 32);
+			st = A.ki[b];
+			sz = (b + 1 < A.n_bucket ? A.ki[b + 1] : A.n_kb) - st;
+			if (sz > max_occ) sz = 0;
+			pos = (uint32_t)sd[j];
+		}
+		int64_t inc = sz;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const int64_t t = __shfl_up_sync(0xffffffffu, inc, o);
+			if (lane >= o) inc += t;
+		}
+		const int64_t total = __shfl_sync(0xffffffffu, inc, 31);
+		s_pre[w][lane] = inc - sz, s_st[w][lane] = st, s_pos[w][lane] = pos;
+		if (lane == 31) s_pre[w][32] = total;
+		__syncwarp();
+		for (int64_t t = lane; t < total; t += 32) {
+			int lo = 0, hi = 31;
+			while (lo < hi) {
+				const int mid = (lo + hi + 1) >> 1;
+				if (s_pre[w][mid] <= t) lo = mid;
+				else hi = mid - 1;
+			}
+			a[k + t] = (uint64_t)A.kb[s_st[w][lo] + (t - s_pre[w][lo])] << 32 | s_pos[w][lo];
+		}
+		k += total;
+		__syncwarp();
 	}
 }
 
@@ -164,7 +195,8 @@ extern "C" int plk_seed_sketch(const plk_seed_args_t *a, void *stream)
 extern "C" int plk_seed_emit(const plk_seed_args_t *a, void *stream)
 {
 	if (a->n <= 0) return 0;
-	k_seed_emit<<<(unsigned)((a->n * 32 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*a);
+	k_seed_emit<<<(unsigned)((a->n * 32 + 32 * SD_EMIT_WARPS - 1) / (32 * SD_EMIT_WARPS)), 32 * SD_EMIT_WARPS, 0,
+			(cudaStream_t)stream>>>(*a);
 	plk_add_launches(1);
 	return (int)cudaGetLastError();
 }
