@@ -483,6 +483,20 @@ void pl_seed_index_destroy(pl_seed_index_t *x);
  * larger array otherwise).  -1 on a bad argument or a device failure (pl_last_error). */
 int64_t pl_seed_anchors_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq, int64_t seq_len,
 		const int64_t *off, const int32_t *len, int32_t max_occ, int64_t *a_off, uint64_t *a, int64_t a_cap);
+/* The same with the options of mp_collect_anchors (map.c:346-397): max_occ (opt->max_occ);
+ * repeat_cap > 0 turns on the accuracy mode's repeat rescue (MP_F_ACCURACY with
+ * MP_ACC_REPEAT_RESCUE: opt->acc_repeat_cap, opt->acc_anchor_budget), which needs every
+ * protein's query-name hash (pl_seed_qname_hash of its name, as mp_hash_qname). */
+typedef struct {
+	int32_t max_occ, repeat_cap;
+	int64_t anchor_budget;
+	const uint32_t *qname_hash;
+} pl_seed_opt_t;
+int64_t pl_seed_anchors_opt_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
+		int64_t seq_len, const int64_t *off, const int32_t *len, const pl_seed_opt_t *opt, int64_t *a_off, uint64_t *a,
+		int64_t a_cap);
+/* mp_hash_qname (map.c:322-329) of a query name */
+uint32_t pl_seed_qname_hash(const char *qname);
 
 typedef struct pl_rc_profile_s pl_rc_profile_t;
 /* A search profile as recheck.c builds it (rc_prof_t, recheck.c:66-72): msc

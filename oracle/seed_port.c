@@ -11,8 +11,12 @@
  *   max_occ   mp_cal_max_occ (map.c:304-320): from 8 seeds on, the box-plot bound
  *             q75 + 1.5 (q75 - q25) + 10 over the seeds' bucket sizes, capped by the
  *             option (map.c:566-569);
- *   anchors   mp_collect_anchors (map.c:346-397) without the rescue: every block of
- *             every seed whose bucket holds at most max_occ, as block << 32 | position;
+ *   anchors   mp_collect_anchors (map.c:346-397): every block of every seed whose bucket
+ *             holds at most max_occ, as block << 32 | position; with the accuracy mode's
+ *             repeat rescue (sp_anchors_acc), up to repeat_cap evenly spaced blocks of the
+ *             other buckets, within anchor_budget: the seeds' shares scaled down, then the
+ *             rest handed out one at a time from the query name's hash onwards, over the
+ *             seeds in their sorted order (map.c:360-384);
  *   order     radix_sort_mp64 of the anchors (map.c:571): ascending.
  * The index is the reference's (index.c:74-98): ki[b] the first entry of bucket b in
  * kb, the bucket's end ki[b+1] (n_kb for the last bucket).
@@ -76,17 +80,30 @@ SP_EXPORT int32_t sp_sketch(const uint8_t *seq, int32_t len, int32_t kmer, int32
 	return n;
 }
 
+/* mp_hash_qname (map.c:322-329): FNV-1a over the name's bytes */
+SP_EXPORT uint32_t sp_qname_hash(const char *qname)
+{
+	uint32_t h = 2166136261U;
+	if (!qname) return h;
+	for (; *qname; ++qname) h = (h ^ (uint8_t)*qname) * 16777619U;
+	return h;
+}
+
 /* the anchors of one protein into *out (malloc'd, sorted); returns their number, -1 on
- * a host allocation failure */
-SP_EXPORT int64_t sp_anchors(const int64_t *ki, int64_t n_bucket, const uint32_t *kb, int64_t n_kb, int32_t kmer,
-		int32_t mod_bit, int32_t max_occ_opt, const uint8_t *seq, int32_t len, uint64_t **out)
+ * a host allocation failure.  repeat_cap > 0: the accuracy mode's repeat rescue with
+ * anchor_budget and the query name's hash qhash */
+SP_EXPORT int64_t sp_anchors_acc(const int64_t *ki, int64_t n_bucket, const uint32_t *kb, int64_t n_kb, int32_t kmer,
+		int32_t mod_bit, int32_t max_occ_opt, int32_t repeat_cap, int64_t anchor_budget, uint32_t qhash,
+		const uint8_t *seq, int32_t len, uint64_t **out)
 {
 	uint64_t *sd = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(len > 0 ? len : 1)), *cnt, *a;
+	int64_t *take;
 	int32_t n, i, max_occ = max_occ_opt;
-	int64_t n_a = 0, k = 0, j;
+	int64_t n_a = 0, n_res = 0, k = 0, j;
 	*out = 0;
 	if (!sd) return -1;
 	n = sp_sketch(seq, len, kmer, mod_bit, sd);
+	qsort(sd, (size_t)n, sizeof(uint64_t), sp_cmp64);  /* mp_sketch_query's order */
 	if (n >= 8) {
 		uint64_t q25, q75;
 		cnt = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)n);
@@ -101,21 +118,50 @@ SP_EXPORT int64_t sp_anchors(const int64_t *ki, int64_t n_bucket, const uint32_t
 		free(cnt);
 		if (max_occ > max_occ_opt) max_occ = max_occ_opt;
 	}
+	take = (int64_t*)calloc((size_t)(n > 0 ? n : 1), sizeof(int64_t));
+	if (!take) { free(sd); return -1; }
 	for (i = 0; i < n; ++i) {
-		const int64_t b = (int64_t)(sd[i] >> 32), en = b + 1 < n_bucket ? ki[b + 1] : n_kb;
-		if (en - ki[b] <= max_occ) n_a += en - ki[b];
+		const int64_t b = (int64_t)(sd[i] >> 32), sz = (b + 1 < n_bucket ? ki[b + 1] : n_kb) - ki[b];
+		if (sz <= max_occ) take[i] = sz, n_a += sz;
+		else if (repeat_cap > 0) take[i] = sz < repeat_cap ? sz : repeat_cap, n_res += take[i];
 	}
+	if (n_res > anchor_budget) {
+		int64_t used = 0;
+		const uint32_t start = n > 0 ? qhash % (uint32_t)n : 0;
+		for (i = 0; i < n; ++i) {
+			const int64_t b = (int64_t)(sd[i] >> 32), sz = (b + 1 < n_bucket ? ki[b + 1] : n_kb) - ki[b];
+			if (sz > max_occ && take[i] > 0) take[i] = take[i] * anchor_budget / n_res, used += take[i];
+		}
+		for (i = 0; i < n && used < anchor_budget; ++i) {
+			const int32_t jj = (int32_t)((start + (uint32_t)i) % (uint32_t)n);
+			const int64_t b = (int64_t)(sd[jj] >> 32), sz = (b + 1 < n_bucket ? ki[b + 1] : n_kb) - ki[b];
+			const int64_t cap = sz < repeat_cap ? sz : repeat_cap;
+			if (sz > max_occ && take[jj] < cap) ++take[jj], ++used;
+		}
+		n_res = used;
+	}
+	n_a += n_res;
 	a = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(n_a > 0 ? n_a : 1));
-	if (!a) { free(sd); return -1; }
+	if (!a) { free(sd), free(take); return -1; }
 	for (i = 0; i < n; ++i) {
-		const int64_t b = (int64_t)(sd[i] >> 32), st = ki[b], en = b + 1 < n_bucket ? ki[b + 1] : n_kb;
-		if (en - st > max_occ) continue;
-		for (j = st; j < en; ++j) a[k++] = (uint64_t)kb[j] << 32 | (uint32_t)sd[i];
+		const int64_t b = (int64_t)(sd[i] >> 32), st = ki[b], sz = (b + 1 < n_bucket ? ki[b + 1] : n_kb) - st;
+		if (take[i] == sz) {
+			for (j = 0; j < sz; ++j) a[k++] = (uint64_t)kb[st + j] << 32 | (uint32_t)sd[i];
+		} else if (take[i] > 0) {
+			const int64_t mid = sz / (2 * take[i]);
+			for (j = 0; j < take[i]; ++j) a[k++] = (uint64_t)kb[st + j * sz / take[i] + mid] << 32 | (uint32_t)sd[i];
+		}
 	}
 	qsort(a, (size_t)n_a, sizeof(uint64_t), sp_cmp64);
-	free(sd);
+	free(sd), free(take);
 	*out = a;
 	return n_a;
+}
+
+SP_EXPORT int64_t sp_anchors(const int64_t *ki, int64_t n_bucket, const uint32_t *kb, int64_t n_kb, int32_t kmer,
+		int32_t mod_bit, int32_t max_occ_opt, const uint8_t *seq, int32_t len, uint64_t **out)
+{
+	return sp_anchors_acc(ki, n_bucket, kb, n_kb, kmer, mod_bit, max_occ_opt, 0, 0, 0, seq, len, out);
 }
 
 SP_EXPORT void sp_free(void *p) { free(p); }

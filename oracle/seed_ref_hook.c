@@ -34,3 +34,36 @@ int64_t ref_seed_anchors(const int64_t *ki, const uint32_t *kb, int64_t n_kb, in
 }
 
 __attribute__((visibility("default"))) void ref_seed_free(void *p) { kfree(0, p); }
+
+/* the same with the accuracy mode's repeat rescue (map.c:360-384): repeat_cap blocks at
+ * most per over-cap bucket, anchor_budget in all, qname for the round-robin start */
+__attribute__((visibility("default")))
+int64_t ref_seed_anchors_acc(const int64_t *ki, const uint32_t *kb, int64_t n_kb, int32_t kmer, int32_t mod_bit,
+		int32_t max_occ_opt, int32_t repeat_cap, int64_t anchor_budget, const char *qname, const char *seq,
+		int32_t len, uint64_t **out)
+{
+	mp_idx_t mi;
+	mp_mapopt_t opt;
+	mp64_v sd = {0, 0, 0};
+	int32_t max_occ;
+	int64_t n_a = 0, n_rescued = 0;
+	memset(&mi, 0, sizeof(mi));
+	mp_idxopt_init(&mi.opt);
+	mi.opt.kmer = kmer, mi.opt.mod_bit = mod_bit;
+	mi.ki = (int64_t*)ki, mi.kb = (uint32_t*)kb, mi.n_kb = n_kb;
+	mp_mapopt_init(&opt);
+	opt.max_occ = max_occ_opt;
+	opt.flag |= MP_F_ACCURACY, opt.acc_flags |= MP_ACC_REPEAT_RESCUE;
+	opt.acc_repeat_cap = repeat_cap, opt.acc_anchor_budget = anchor_budget;
+	mp_sketch_query(0, &opt, seq, len, kmer, mod_bit, opt.hmm_seed_max, &sd);
+	if (sd.n >= 8) {
+		max_occ = mp_cal_max_occ(0, &mi, sd.n, sd.a);
+		if (max_occ > opt.max_occ) max_occ = opt.max_occ;
+	} else max_occ = opt.max_occ;
+	*out = mp_collect_anchors(0, &mi, &opt, &sd, max_occ, qname, &n_a, &n_rescued);
+	kfree(0, sd.a);
+	radix_sort_mp64(*out, *out + n_a);
+	return n_a;
+}
+
+__attribute__((visibility("default"))) uint32_t ref_seed_qname_hash(const char *qname) { return mp_hash_qname(qname); }

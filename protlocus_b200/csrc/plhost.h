@@ -70,6 +70,7 @@ struct pl_engine_s {
 	dbuf_t r_prof, r_pep, r_dsq, r_order, r_grp, r_err, r_scratch, r_bits, r_bias;
 	/* seeding (plseed.c) */
 	dbuf_t s_seq, s_off, s_len, s_seed, s_cnt, s_nseed, s_cap, s_nanc, s_aoff, s_anc, s_anc2, s_tmp;
+	dbuf_t s_take, s_send, s_seed2, s_qh;
 	int64_t r_last_cells;
 	/* learned-prefilter features */
 	dbuf_t pf_cand, pf_feats, pf_chain, pf_out;

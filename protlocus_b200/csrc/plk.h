@@ -189,17 +189,23 @@ typedef struct {
 	const uint32_t *kb;
 	int64_t n_kb;
 	int32_t kmer, mod_bit, max_occ;
-	uint64_t *seeds;             /* per residue slot: the seeds, in position order */
-	uint32_t *cnt;               /* per residue slot: the seeds' bucket sizes (reordered) */
+	int32_t repeat_cap;          /* > 0: the accuracy mode's repeat rescue (map.c:360-384) */
+	int64_t budget;              /* its anchor budget */
+	const uint32_t *qhash;       /* per protein: the query name's hash (the rescue's start) */
+	uint64_t *seeds;             /* per residue slot: the seeds (position order; sorted for the rescue) */
+	uint32_t *cnt;               /* per residue slot: the seeds' bucket sizes */
+	int32_t *take;               /* per residue slot: the anchors each seed gives */
 	int32_t *n_seed, *cap;       /* per protein: seeds, occurrence cap */
+	int64_t *seed_end;           /* per protein: off + n_seed (the seeds' segment for a sort) */
 	int64_t *n_anchor;           /* per protein: anchors */
 	const int64_t *a_off;        /* per protein: first anchor (n + 1 entries) */
 	uint64_t *anchors;
 } plk_seed_args_t;
 int plk_seed_sketch(const plk_seed_args_t *a, void *stream);
+int plk_seed_take(const plk_seed_args_t *a, void *stream);
 int plk_seed_emit(const plk_seed_args_t *a, void *stream);
 int plk_seed_sort(const uint64_t *keys_in, uint64_t *keys_out, int64_t n_items, int32_t n_seg, const int64_t *seg_off,
-		void *tmp, size_t *tmp_bytes, void *stream);
+		const int64_t *seg_end, void *tmp, size_t *tmp_bytes, void *stream);
 #define PLK_RC_MAX_M 2048
 int64_t plk_rc_group_floats(int32_t lmax, int32_t M, int32_t full);
 /* err: a device int, set to 1 when a wait between the warps of a group ran out (the

@@ -5,9 +5,10 @@
  * The index is the mapper's own (mp_idx_t's ki / kb, index.c:74-98), uploaded once with
  * pl_seed_index_create.  A batch takes proteins (letters or residue codes 0-21) and
  * returns, per protein, its anchors (block << 32 | position) sorted ascending, as
- * mp_collect_anchors and the following radix sort leave them.  The accuracy mode's
- * repeat rescue (map.c:360-384) and the profile-derived seeds of mp_sketch_hmm are not
- * done here: a caller in those modes keeps the reference's path.
+ * mp_collect_anchors and the following radix sort leave them, with the accuracy mode's
+ * repeat rescue (map.c:360-384) when asked (pl_seed_anchors_opt_host).  The
+ * profile-derived seeds of mp_sketch_hmm are not done here: a caller with a profile keeps
+ * the reference's path.
  */
 #define _POSIX_C_SOURCE 200809L
 #include <stdio.h>
@@ -62,12 +63,23 @@ void pl_seed_engine_free(pl_engine_t *e)
 	dbuf_free(&e->s_seq), dbuf_free(&e->s_off), dbuf_free(&e->s_len), dbuf_free(&e->s_seed), dbuf_free(&e->s_cnt);
 	dbuf_free(&e->s_nseed), dbuf_free(&e->s_cap), dbuf_free(&e->s_nanc), dbuf_free(&e->s_aoff);
 	dbuf_free(&e->s_anc), dbuf_free(&e->s_anc2), dbuf_free(&e->s_tmp);
+	dbuf_free(&e->s_take), dbuf_free(&e->s_send), dbuf_free(&e->s_seed2), dbuf_free(&e->s_qh);
 }
 
-PL_EXPORT int64_t pl_seed_anchors_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
-		int64_t seq_len, const int64_t *off, const int32_t *len, int32_t max_occ, int64_t *a_off, uint64_t *a,
+PL_EXPORT uint32_t pl_seed_qname_hash(const char *qname)
+{ /* mp_hash_qname (map.c:322-329): FNV-1a over the name's bytes */
+	uint32_t h = 2166136261U;
+	if (!qname) return h;
+	for (; *qname; ++qname) h = (h ^ (uint8_t)*qname) * 16777619U;
+	return h;
+}
+
+PL_EXPORT int64_t pl_seed_anchors_opt_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
+		int64_t seq_len, const int64_t *off, const int32_t *len, const pl_seed_opt_t *o, int64_t *a_off, uint64_t *a,
 		int64_t a_cap)
 {
+	const int rescue = o && o->repeat_cap > 0;
+	const int32_t max_occ = o ? o->max_occ : 0;
 	plk_seed_args_t A;
 	int64_t *na = 0, total = 0, ret = -1;
 	int32_t q;
@@ -75,7 +87,10 @@ PL_EXPORT int64_t pl_seed_anchors_host(pl_engine_t *e, const pl_seed_index_t *x,
 	cudaStream_t st;
 	if (!e || !x) { pl_set_error("no engine or index"); return -1; }
 	if (x->device != e->device) { pl_set_error("seed index on device %d, engine on %d", x->device, e->device); return -1; }
-	if (n < 0 || !a_off || (n > 0 && (!seq || !off || !len))) { pl_set_error("seed batch: bad arguments"); return -1; }
+	if (n < 0 || !o || !a_off || (n > 0 && (!seq || !off || !len)) || (rescue && (o->anchor_budget < 0 || !o->qname_hash))) {
+		pl_set_error("seed batch: bad arguments");
+		return -1;
+	}
 	a_off[0] = 0;
 	if (n == 0) return 0;
 	for (q = 0; q < n; ++q)
@@ -92,7 +107,11 @@ PL_EXPORT int64_t pl_seed_anchors_host(pl_engine_t *e, const pl_seed_index_t *x,
 			!dbuf_ensure(&e->s_seed, sizeof(uint64_t) * (size_t)(seq_len > 0 ? seq_len : 1)) ||
 			!dbuf_ensure(&e->s_cnt, sizeof(uint32_t) * (size_t)(seq_len > 0 ? seq_len : 1)) ||
 			!dbuf_ensure(&e->s_nseed, sizeof(int32_t) * (size_t)n) || !dbuf_ensure(&e->s_cap, sizeof(int32_t) * (size_t)n) ||
-			!dbuf_ensure(&e->s_nanc, sizeof(int64_t) * (size_t)n) || !dbuf_ensure(&e->s_aoff, sizeof(int64_t) * (size_t)(n + 1)))
+			!dbuf_ensure(&e->s_nanc, sizeof(int64_t) * (size_t)n) || !dbuf_ensure(&e->s_aoff, sizeof(int64_t) * (size_t)(n + 1)) ||
+			!dbuf_ensure(&e->s_take, sizeof(int32_t) * (size_t)(seq_len > 0 ? seq_len : 1)) ||
+			!dbuf_ensure(&e->s_send, sizeof(int64_t) * (size_t)n) ||
+			(rescue && (!dbuf_ensure(&e->s_seed2, sizeof(uint64_t) * (size_t)(seq_len > 0 ? seq_len : 1)) ||
+			            !dbuf_ensure(&e->s_qh, sizeof(uint32_t) * (size_t)n))))
 		goto fail;
 	if (seq_len > 0) CK(cudaMemcpyAsync(e->s_seq.p, seq, (size_t)seq_len, cudaMemcpyHostToDevice, st));
 	CK(cudaMemcpyAsync(e->s_off.p, off, sizeof(int64_t) * (size_t)n, cudaMemcpyHostToDevice, st));
@@ -101,11 +120,27 @@ PL_EXPORT int64_t pl_seed_anchors_host(pl_engine_t *e, const pl_seed_index_t *x,
 	A.seq = (const uint8_t*)e->s_seq.p, A.off = (const int64_t*)e->s_off.p, A.len = (const int32_t*)e->s_len.p, A.n = n;
 	A.ki = x->ki, A.n_bucket = x->n_bucket, A.kb = x->kb, A.n_kb = x->n_kb;
 	A.kmer = x->kmer, A.mod_bit = x->mod_bit, A.max_occ = max_occ;
-	A.seeds = (uint64_t*)e->s_seed.p, A.cnt = (uint32_t*)e->s_cnt.p;
+	A.repeat_cap = rescue ? o->repeat_cap : 0, A.budget = rescue ? o->anchor_budget : 0;
+	A.seeds = (uint64_t*)e->s_seed.p, A.cnt = (uint32_t*)e->s_cnt.p, A.take = (int32_t*)e->s_take.p;
 	A.n_seed = (int32_t*)e->s_nseed.p, A.cap = (int32_t*)e->s_cap.p, A.n_anchor = (int64_t*)e->s_nanc.p;
+	A.seed_end = (int64_t*)e->s_send.p;
+	if (rescue) {
+		CK(cudaMemcpyAsync(e->s_qh.p, o->qname_hash, sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+		A.qhash = (const uint32_t*)e->s_qh.p;
+	}
 	e->n_ev = 0;
 	PL_TIME(e, st, 1);
 	CKK(plk_seed_sketch(&A, st));
+	if (rescue) { /* the rescue hands its budget out over the seeds in mp_sketch_query's sorted order */
+		size_t tb = 0;
+		CKK(plk_seed_sort((const uint64_t*)e->s_seed.p, (uint64_t*)e->s_seed2.p, seq_len, n, (const int64_t*)e->s_off.p,
+				(const int64_t*)e->s_send.p, 0, &tb, st));
+		if (!dbuf_ensure(&e->s_tmp, tb > 0 ? tb : 16)) goto fail;
+		CKK(plk_seed_sort((const uint64_t*)e->s_seed.p, (uint64_t*)e->s_seed2.p, seq_len, n, (const int64_t*)e->s_off.p,
+				(const int64_t*)e->s_send.p, e->s_tmp.p, &tb, st));
+		A.seeds = (uint64_t*)e->s_seed2.p;
+	}
+	CKK(plk_seed_take(&A, st));
 	PL_TIME(e, st, 1);
 	CK(cudaMemcpyAsync(na, e->s_nanc.p, sizeof(int64_t) * (size_t)n, cudaMemcpyDeviceToHost, st));
 	CK(cudaStreamSynchronize(st));
@@ -118,10 +153,10 @@ PL_EXPORT int64_t pl_seed_anchors_host(pl_engine_t *e, const pl_seed_index_t *x,
 	A.a_off = (const int64_t*)e->s_aoff.p, A.anchors = (uint64_t*)e->s_anc.p;
 	PL_TIME(e, st, 1);
 	CKK(plk_seed_emit(&A, st));
-	CKK(plk_seed_sort((const uint64_t*)e->s_anc.p, (uint64_t*)e->s_anc2.p, total, n, (const int64_t*)e->s_aoff.p, 0,
+	CKK(plk_seed_sort((const uint64_t*)e->s_anc.p, (uint64_t*)e->s_anc2.p, total, n, (const int64_t*)e->s_aoff.p, 0, 0,
 			&tmp_bytes, st));
 	if (!dbuf_ensure(&e->s_tmp, tmp_bytes > 0 ? tmp_bytes : 16)) goto fail;
-	CKK(plk_seed_sort((const uint64_t*)e->s_anc.p, (uint64_t*)e->s_anc2.p, total, n, (const int64_t*)e->s_aoff.p,
+	CKK(plk_seed_sort((const uint64_t*)e->s_anc.p, (uint64_t*)e->s_anc2.p, total, n, (const int64_t*)e->s_aoff.p, 0,
 			e->s_tmp.p, &tmp_bytes, st));
 	PL_TIME(e, st, 1);
 	CK(cudaMemcpyAsync(a, e->s_anc2.p, sizeof(uint64_t) * (size_t)total, cudaMemcpyDeviceToHost, st));
@@ -141,4 +176,14 @@ done:
 fail:
 	free(na);
 	return -1;
+}
+
+PL_EXPORT int64_t pl_seed_anchors_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
+		int64_t seq_len, const int64_t *off, const int32_t *len, int32_t max_occ, int64_t *a_off, uint64_t *a,
+		int64_t a_cap)
+{
+	pl_seed_opt_t o;
+	memset(&o, 0, sizeof(o));
+	o.max_occ = max_occ;
+	return pl_seed_anchors_opt_host(e, x, n, seq, seq_len, off, len, &o, a_off, a, a_cap);
 }

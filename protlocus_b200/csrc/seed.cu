@@ -125,11 +125,52 @@ __global__ void __launch_bounds__(256) k_seed_sketch(plk_seed_args_t A)
 		max_occ = (int32_t)__dadd_rn(__dadd_rn((double)q75, __dmul_rn((double)(q75 - q25), 1.5)), 10.);
 		if (max_occ > A.max_occ) max_occ = A.max_occ;
 	}
-	int64_t n_a = 0;
-	for (int32_t j = lane; j < n; j += 32)
-		if ((int64_t)cnt[j] <= max_occ) n_a += cnt[j];
-	n_a = sd_warp_sum(n_a);
-	if (lane == 0) A.n_seed[q] = n, A.cap[q] = max_occ, A.n_anchor[q] = n_a;
+	if (lane == 0) A.n_seed[q] = n, A.cap[q] = max_occ, A.seed_end[q] = A.off[q] + n;
+}
+
+/* one warp per protein: the anchors each seed gives (mp_collect_anchors, map.c:352-384):
+ * a bucket within the cap whole; with the repeat rescue, up to repeat_cap blocks of a
+ * bucket over it, and when those exceed the budget, every share scaled down, then the rest
+ * of the budget handed out one block at a time over the seeds in their sorted order from
+ * the query name's hash onwards (lane 0, as the reference's loop) */
+__global__ void __launch_bounds__(256) k_seed_take(plk_seed_args_t A)
+{
+	const int lane = threadIdx.x & 31;
+	const int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	if (q >= A.n) return;  /* whole warps */
+	const uint64_t *sd = A.seeds + A.off[q];
+	int32_t *take = A.take + A.off[q];
+	const int32_t n = A.n_seed[q], max_occ = A.cap[q], rcap = A.repeat_cap;
+	int64_t n_base = 0, n_res = 0;
+	for (int32_t j = lane; j < n; j += 32) {
+		const int64_t sz = sd_bucket_size(A.ki, A.n_bucket, A.n_kb, (int64_t)(sd[j] >> 32));
+		int32_t t = 0;
+		if (sz <= max_occ) t = (int32_t)sz, n_base += sz;
+		else if (rcap > 0) t = (int32_t)(sz < rcap ? sz : rcap), n_res += t;
+		take[j] = t;
+	}
+	n_base = sd_warp_sum(n_base), n_res = sd_warp_sum(n_res);
+	if (n_res > A.budget) {
+		int64_t used = 0;
+		for (int32_t j = lane; j < n; j += 32) {
+			const int64_t sz = sd_bucket_size(A.ki, A.n_bucket, A.n_kb, (int64_t)(sd[j] >> 32));
+			if (sz > max_occ && take[j] > 0) take[j] = (int32_t)((int64_t)take[j] * A.budget / n_res), used += take[j];
+		}
+		used = sd_warp_sum(used);
+		__syncwarp();
+		if (lane == 0) {
+			const uint32_t start = n > 0 ? A.qhash[q] % (uint32_t)n : 0;
+			for (int32_t i = 0; i < n && used < A.budget; ++i) {
+				const int32_t j = (int32_t)((start + (uint32_t)i) % (uint32_t)n);
+				const int64_t sz = sd_bucket_size(A.ki, A.n_bucket, A.n_kb, (int64_t)(sd[j] >> 32));
+				const int64_t cap = sz < rcap ? sz : rcap;
+				if (sz > max_occ && take[j] < cap) ++take[j], ++used;
+			}
+		}
+		n_res = __shfl_sync(0xffffffffu, used, 0);
+		__syncwarp();
+	}
+	if (lane == 0) A.n_anchor[q] = n_base + n_res;
 }
 
 #define SD_EMIT_WARPS 8
@@ -137,11 +178,13 @@ __global__ void __launch_bounds__(32 * SD_EMIT_WARPS) k_seed_emit(plk_seed_args_
 {
 	__shared__ int64_t s_pre[SD_EMIT_WARPS][33], s_st[SD_EMIT_WARPS][32];
 	__shared__ uint32_t s_pos[SD_EMIT_WARPS][32];
+	__shared__ int64_t s_sz[SD_EMIT_WARPS][32];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	const int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	if (q >= A.n) return;  /* whole warps */
 	const uint64_t *sd = A.seeds + A.off[q];
-	const int32_t n = A.n_seed[q], max_occ = A.cap[q];
+	const int32_t n = A.n_seed[q];
+	const int32_t *take = A.take + A.off[q];
 	uint64_t *a = A.anchors + A.a_off[q];
 	int64_t k = 0;
 	/* 32 seeds at a time: their buckets' starts and sizes (0 past the cap) side by side, an
@@ -149,24 +192,24 @@ __global__ void __launch_bounds__(32 * SD_EMIT_WARPS) k_seed_emit(plk_seed_args_
 	 * (the seed of output t: the last one whose offset is at most t) */
 	for (int32_t j0 = 0; j0 < n; j0 += 32) {
 		const int32_t j = j0 + lane;
-		int64_t st = 0, sz = 0;
+		int64_t st = 0, sz = 0, tk = 0;
 		uint32_t pos = 0;
 		if (j < n) {
 			const int64_t b = (int64_t)(sd[j] >> 32);
 			st = A.ki[b];
 			sz = (b + 1 < A.n_bucket ? A.ki[b + 1] : A.n_kb) - st;
-			if (sz > max_occ) sz = 0;
+			tk = take[j];
 			pos = (uint32_t)sd[j];
 		}
-		int64_t inc = sz;
+		int64_t inc = tk;
 #pragma unroll
 		for (int o = 1; o < 32; o <<= 1) {
 			const int64_t t = __shfl_up_sync(0xffffffffu, inc, o);
 			if (lane >= o) inc += t;
 		}
 		const int64_t total = __shfl_sync(0xffffffffu, inc, 31);
-		s_pre[w][lane] = inc - sz, s_st[w][lane] = st, s_pos[w][lane] = pos;
-		if (lane == 31) s_pre[w][32] = total;
+		s_pre[w][lane] = inc - tk, s_st[w][lane] = st, s_pos[w][lane] = pos, s_sz[w][lane] = sz;
+		if (lane == 31) s_pre[w][32] = total;  /* s_pre[lo + 1] - s_pre[lo]: seed lo's take */
 		__syncwarp();
 		for (int64_t t = lane; t < total; t += 32) {
 			int lo = 0, hi = 31;
@@ -175,7 +218,10 @@ __global__ void __launch_bounds__(32 * SD_EMIT_WARPS) k_seed_emit(plk_seed_args_
 				if (s_pre[w][mid] <= t) lo = mid;
 				else hi = mid - 1;
 			}
-			a[k + t] = (uint64_t)A.kb[s_st[w][lo] + (t - s_pre[w][lo])] << 32 | s_pos[w][lo];
+			const int64_t u = t - s_pre[w][lo], bsz = s_sz[w][lo], btk = s_pre[w][lo + 1] - s_pre[w][lo];
+			/* a whole bucket, or take of its blocks evenly spaced (map.c:390-393) */
+			const int64_t o = btk == bsz ? u : u * bsz / btk + bsz / (2 * btk);
+			a[k + t] = (uint64_t)A.kb[s_st[w][lo] + o] << 32 | s_pos[w][lo];
 		}
 		k += total;
 		__syncwarp();
@@ -192,6 +238,14 @@ extern "C" int plk_seed_sketch(const plk_seed_args_t *a, void *stream)
 	return (int)cudaGetLastError();
 }
 
+extern "C" int plk_seed_take(const plk_seed_args_t *a, void *stream)
+{
+	if (a->n <= 0) return 0;
+	k_seed_take<<<(unsigned)((a->n * 32 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*a);
+	plk_add_launches(1);
+	return (int)cudaGetLastError();
+}
+
 extern "C" int plk_seed_emit(const plk_seed_args_t *a, void *stream)
 {
 	if (a->n <= 0) return 0;
@@ -201,13 +255,13 @@ extern "C" int plk_seed_emit(const plk_seed_args_t *a, void *stream)
 	return (int)cudaGetLastError();
 }
 
-/* per-protein ascending sort of the anchors from keys_in into keys_out; tmp == 0 asks for
- * the scratch size in *tmp_bytes */
+/* per-segment ascending sort of keys_in into keys_out, segment i at [seg_off[i],
+ * seg_end[i]) (seg_end 0: up to seg_off[i + 1]); tmp == 0 asks for the scratch size */
 extern "C" int plk_seed_sort(const uint64_t *keys_in, uint64_t *keys_out, int64_t n_items, int32_t n_seg,
-		const int64_t *seg_off, void *tmp, size_t *tmp_bytes, void *stream)
+		const int64_t *seg_off, const int64_t *seg_end, void *tmp, size_t *tmp_bytes, void *stream)
 {
 	cudaError_t e = cub::DeviceSegmentedSort::SortKeys(tmp, *tmp_bytes, keys_in, keys_out, n_items, n_seg, seg_off,
-			seg_off + 1, (cudaStream_t)stream);
+			seg_end ? seg_end : seg_off + 1, (cudaStream_t)stream);
 	if (tmp) plk_add_launches(1);
 	return (int)e;
 }

@@ -141,6 +141,11 @@ def load() -> C.CDLL:
     lib.pl_seed_anchors_host.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
                                          C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64]
     lib.pl_seed_anchors_host.restype = C.c_int64
+    lib.pl_seed_anchors_opt_host.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
+                                             C.c_void_p, C.POINTER(SeedOpt), C.c_void_p, C.c_void_p, C.c_int64]
+    lib.pl_seed_anchors_opt_host.restype = C.c_int64
+    lib.pl_seed_qname_hash.argtypes = [C.c_char_p]
+    lib.pl_seed_qname_hash.restype = C.c_uint32
     lib.pl_pf_decide.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_double, C.c_int32,
                                  C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.pl_pf_decide.restype = C.c_int
@@ -617,6 +622,12 @@ class Engine:
         return bits, bias
 
 
+class SeedOpt(C.Structure):
+    """pl_seed_opt_t"""
+    _fields_ = [("max_occ", C.c_int32), ("repeat_cap", C.c_int32), ("anchor_budget", C.c_int64),
+                ("qname_hash", C.c_void_p)]
+
+
 class SeedIndex:
     """A pl_seed_index_t: the mapper's k-mer index (ki int64 bucket starts, kb uint32 block ids) on a device."""
 
@@ -634,9 +645,12 @@ class SeedIndex:
             self.h = None
 
 
-def seed_anchors(eng, index: SeedIndex, proteins, max_occ: int):
-    """Anchors of a list of proteins (bytes) through pl_seed_anchors_host: a list of sorted uint64 arrays."""
+def seed_anchors(eng, index: SeedIndex, proteins, max_occ: int, repeat_cap: int = 0, budget: int = 0, names=None):
+    """Anchors of a list of proteins (bytes) through pl_seed_anchors_opt_host: a list of sorted uint64 arrays.
+    repeat_cap > 0: the accuracy mode's repeat rescue, with the proteins' names (bytes)."""
     n = len(proteins)
+    qh = np.array([eng.lib.pl_seed_qname_hash(nm) for nm in (names or [b""] * n)], dtype=np.uint32)
+    opt = SeedOpt(max_occ, repeat_cap, budget, qh.ctypes.data if n else None)
     lens = np.array([len(p) for p in proteins], dtype=np.int32)
     offs = np.zeros(n, dtype=np.int64)
     if n > 1:
@@ -647,8 +661,8 @@ def seed_anchors(eng, index: SeedIndex, proteins, max_occ: int):
     cap = 1 << 20
     for _ in range(2):
         a = np.zeros(max(cap, 1), dtype=np.uint64)
-        tot = eng.lib.pl_seed_anchors_host(eng.h, index.h, n, seq.ctypes.data, int(lens.sum()), offs.ctypes.data,
-                                           lens.ctypes.data, max_occ, a_off.ctypes.data, a.ctypes.data, cap)
+        tot = eng.lib.pl_seed_anchors_opt_host(eng.h, index.h, n, seq.ctypes.data, int(lens.sum()), offs.ctypes.data,
+                                               lens.ctypes.data, C.byref(opt), a_off.ctypes.data, a.ctypes.data, cap)
         if tot < 0:
             raise RuntimeError("pl_seed_anchors_host: " + error())
         if tot <= cap:

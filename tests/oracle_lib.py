@@ -455,3 +455,35 @@ def seed_anchors(ki, kb, kmer: int, mod_bit: int, max_occ: int, seq: bytes, use_
     p = _seed_port()
     return _seed_take(p.sp_anchors, p.sp_free, ki.ctypes.data, ki.size, kb.ctypes.data, kb.size, kmer, mod_bit,
                       max_occ, seq, len(seq))
+
+
+def seed_anchors_acc(ki, kb, kmer: int, mod_bit: int, max_occ: int, repeat_cap: int, budget: int, qname: bytes,
+                     seq: bytes, use_ref: bool | None = None):
+    """seed_anchors with the accuracy mode's repeat rescue (map.c:360-384) for a query named qname."""
+    lib = seed_ref_lib() if use_ref is not False else None
+    if use_ref and lib is None:
+        raise RuntimeError("oracle/_ref/libseed_ref.so not built")
+    if lib is not None:
+        f = lib.ref_seed_anchors_acc
+        f.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int64,
+                      C.c_char_p, C.c_char_p, C.c_int32, C.POINTER(C.POINTER(C.c_uint64))]
+        f.restype = C.c_int64
+        return _seed_take(f, lib.ref_seed_free, ki.ctypes.data, kb.ctypes.data, kb.size, kmer, mod_bit, max_occ,
+                          repeat_cap, budget, qname, seq, len(seq))
+    p = _seed_port()
+    p.sp_qname_hash.argtypes = [C.c_char_p]
+    p.sp_qname_hash.restype = C.c_uint32
+    p.sp_anchors_acc.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
+                                 C.c_int32, C.c_int64, C.c_uint32, C.c_char_p, C.c_int32,
+                                 C.POINTER(C.POINTER(C.c_uint64))]
+    p.sp_anchors_acc.restype = C.c_int64
+    return _seed_take(p.sp_anchors_acc, p.sp_free, ki.ctypes.data, ki.size, kb.ctypes.data, kb.size, kmer, mod_bit,
+                      max_occ, repeat_cap, budget, p.sp_qname_hash(qname), seq, len(seq))
+
+
+def seed_qname_hash(qname: bytes) -> int:
+    """mp_hash_qname (map.c:322-329), from the restatement."""
+    p = _seed_port()
+    p.sp_qname_hash.argtypes = [C.c_char_p]
+    p.sp_qname_hash.restype = C.c_uint32
+    return int(p.sp_qname_hash(qname))

@@ -71,3 +71,24 @@ def test_seed_edges(engine):
         assert got[0].size == 0
     finally:
         empty.close()
+
+
+@pytest.mark.parametrize("max_occ,cap,budget", [(40, 64, 250000), (40, 64, 300), (20, 200, 50), (20, 5, 7), (20, 5, 0)])
+def test_seed_rescue_matches_reference(engine, max_occ, cap, budget):
+    """The accuracy mode's repeat rescue on an index with 5 % repeat buckets: evenly spaced
+    blocks of the over-cap buckets, the budget's scaled shares and round-robin from the query
+    name's hash, over the seeds in their sorted order."""
+    from test_seed import rescue_index
+    rng = np.random.default_rng(400 + cap + budget)
+    ki, kb = rescue_index(rng)
+    idx = L.SeedIndex(ki, kb, 5, 1)
+    try:
+        prots = seed_proteins(rng, 200)
+        names = [b"query_%d" % q for q in range(len(prots))]
+        assert all(engine.lib.pl_seed_qname_hash(nm) == O.seed_qname_hash(nm) for nm in names)
+        got = L.seed_anchors(engine, idx, prots, max_occ, cap, budget, names)
+        for q, seq in enumerate(prots):
+            want = O.seed_anchors_acc(ki, kb, 5, 1, max_occ, cap, budget, names[q], seq)
+            assert np.array_equal(got[q], want), (q, len(seq), got[q].size, want.size)
+    finally:
+        idx.close()

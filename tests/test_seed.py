@@ -68,3 +68,32 @@ def test_seed_port_hand_case():
     kb = np.array([7, 5, 9], dtype=np.uint32)
     a = O.seed_anchors(ki, kb, kmer, mod_bit, 100, b"ARNDCQ", use_ref=False)
     assert [int(x >> np.uint64(32)) for x in a] == [5, 7, 9] and all(int(x) & 0xffffffff == 5 for x in a)
+
+
+@need_ref
+@pytest.mark.parametrize("max_occ,cap,budget", [(40, 64, 250000), (40, 64, 300), (20, 200, 50), (20, 5, 7),
+                                                (20, 5, 0)])
+def test_seed_port_rescue_equals_reference(max_occ, cap, budget):
+    """The accuracy mode's repeat rescue: evenly spaced blocks of the over-cap buckets, and with
+    a small budget the scaled shares plus the round-robin from the query name's hash."""
+    rng = np.random.default_rng(300 + cap + budget)
+    ki, kb = rescue_index(rng)
+    lib = O.seed_ref_lib()
+    import ctypes as C
+    lib.ref_seed_qname_hash.argtypes = [C.c_char_p]
+    lib.ref_seed_qname_hash.restype = C.c_uint32
+    rescued = 0
+    for q, seq in enumerate(seed_proteins(rng, 60)):
+        name = b"query_%d" % q
+        assert O.seed_qname_hash(name) == lib.ref_seed_qname_hash(name)
+        ref = O.seed_anchors_acc(ki, kb, 5, 1, max_occ, cap, budget, name, seq, use_ref=True)
+        port = O.seed_anchors_acc(ki, kb, 5, 1, max_occ, cap, budget, name, seq, use_ref=False)
+        assert np.array_equal(ref, port), (q, len(seq), ref.size, port.size)
+        rescued += ref.size != O.seed_anchors(ki, kb, 5, 1, max_occ, seq, use_ref=False).size
+    assert rescued >= 10 if budget > 0 else rescued == 0  # a zero budget takes nothing (map.c:365-383)
+
+
+def rescue_index(rng):
+    """kmer 5 (2^19 buckets) with 5 % repeat buckets of 150-300 blocks, so that proteins meet
+    buckets over the occurrence cap"""
+    return O.seed_index(rng, kmer=5, mod_bit=1, n_block=100_000, hot=1 << 19 >> 4, hot_occ=300)
