@@ -495,6 +495,13 @@ typedef struct {
 int64_t pl_seed_anchors_opt_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
 		int64_t seq_len, const int64_t *off, const int32_t *len, const pl_seed_opt_t *opt, int64_t *a_off, uint64_t *a,
 		int64_t a_cap);
+/* The same with the anchors left on the device: *a_dev points at them (engine memory,
+ * valid until the engine's next seeding call; NULL when there are none), a_off is filled
+ * on the host.  They can go to pl_chain_fill_device as they are (its off = a_off, n =
+ * a_off[q+1] - a_off[q]). */
+int64_t pl_seed_anchors_opt_device(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
+		int64_t seq_len, const int64_t *off, const int32_t *len, const pl_seed_opt_t *opt, int64_t *a_off,
+		const uint64_t **a_dev);
 /* mp_hash_qname (map.c:322-329) of a query name */
 uint32_t pl_seed_qname_hash(const char *qname);
 

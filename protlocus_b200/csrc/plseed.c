@@ -74,9 +74,11 @@ PL_EXPORT uint32_t pl_seed_qname_hash(const char *qname)
 	return h;
 }
 
-PL_EXPORT int64_t pl_seed_anchors_opt_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
-		int64_t seq_len, const int64_t *off, const int32_t *len, const pl_seed_opt_t *o, int64_t *a_off, uint64_t *a,
-		int64_t a_cap)
+/* the batch's anchors: into the host array a (when they fit a_cap), or left on the device
+ * (a_dev != 0: *a_dev at the engine's sorted array) */
+static int64_t pl_seed_run(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq, int64_t seq_len,
+		const int64_t *off, const int32_t *len, const pl_seed_opt_t *o, int64_t *a_off, uint64_t *a, int64_t a_cap,
+		const uint64_t **a_dev)
 {
 	const int rescue = o && o->repeat_cap > 0;
 	const int32_t max_occ = o ? o->max_occ : 0;
@@ -146,7 +148,8 @@ PL_EXPORT int64_t pl_seed_anchors_opt_host(pl_engine_t *e, const pl_seed_index_t
 	CK(cudaStreamSynchronize(st));
 	for (q = 0; q < n; ++q) total += na[q], a_off[q + 1] = total;
 	ret = total;
-	if (total > a_cap || total == 0) goto done;  /* a_off only: the caller grows a to a_off[n] */
+	if (a_dev) *a_dev = 0;
+	if (total == 0 || (!a_dev && total > a_cap)) goto done;  /* a_off only: the caller grows a to a_off[n] */
 	if (!dbuf_ensure(&e->s_anc, sizeof(uint64_t) * (size_t)total) || !dbuf_ensure(&e->s_anc2, sizeof(uint64_t) * (size_t)total))
 		goto fail;
 	CK(cudaMemcpyAsync(e->s_aoff.p, a_off, sizeof(int64_t) * (size_t)(n + 1), cudaMemcpyHostToDevice, st));
@@ -159,7 +162,8 @@ PL_EXPORT int64_t pl_seed_anchors_opt_host(pl_engine_t *e, const pl_seed_index_t
 	CKK(plk_seed_sort((const uint64_t*)e->s_anc.p, (uint64_t*)e->s_anc2.p, total, n, (const int64_t*)e->s_aoff.p, 0,
 			e->s_tmp.p, &tmp_bytes, st));
 	PL_TIME(e, st, 1);
-	CK(cudaMemcpyAsync(a, e->s_anc2.p, sizeof(uint64_t) * (size_t)total, cudaMemcpyDeviceToHost, st));
+	if (a_dev) *a_dev = (const uint64_t*)e->s_anc2.p;
+	else CK(cudaMemcpyAsync(a, e->s_anc2.p, sizeof(uint64_t) * (size_t)total, cudaMemcpyDeviceToHost, st));
 	CK(cudaStreamSynchronize(st));
 done:
 	if (e->timing) {  /* the sketch, and the emission with the sort */
@@ -176,6 +180,21 @@ done:
 fail:
 	free(na);
 	return -1;
+}
+
+PL_EXPORT int64_t pl_seed_anchors_opt_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
+		int64_t seq_len, const int64_t *off, const int32_t *len, const pl_seed_opt_t *o, int64_t *a_off, uint64_t *a,
+		int64_t a_cap)
+{
+	return pl_seed_run(e, x, n, seq, seq_len, off, len, o, a_off, a, a_cap, 0);
+}
+
+PL_EXPORT int64_t pl_seed_anchors_opt_device(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
+		int64_t seq_len, const int64_t *off, const int32_t *len, const pl_seed_opt_t *o, int64_t *a_off,
+		const uint64_t **a_dev)
+{
+	if (!a_dev) { pl_set_error("seed batch: no output pointer"); return -1; }
+	return pl_seed_run(e, x, n, seq, seq_len, off, len, o, a_off, 0, 0, a_dev);
 }
 
 PL_EXPORT int64_t pl_seed_anchors_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,

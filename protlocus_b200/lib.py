@@ -144,6 +144,9 @@ def load() -> C.CDLL:
     lib.pl_seed_anchors_opt_host.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
                                              C.c_void_p, C.POINTER(SeedOpt), C.c_void_p, C.c_void_p, C.c_int64]
     lib.pl_seed_anchors_opt_host.restype = C.c_int64
+    lib.pl_seed_anchors_opt_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
+                                               C.c_void_p, C.POINTER(SeedOpt), C.c_void_p, C.POINTER(C.c_void_p)]
+    lib.pl_seed_anchors_opt_device.restype = C.c_int64
     lib.pl_seed_qname_hash.argtypes = [C.c_char_p]
     lib.pl_seed_qname_hash.restype = C.c_uint32
     lib.pl_pf_decide.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_double, C.c_int32,

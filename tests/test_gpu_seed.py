@@ -92,3 +92,44 @@ def test_seed_rescue_matches_reference(engine, max_occ, cap, budget):
             assert np.array_equal(got[q], want), (q, len(seq), got[q].size, want.size)
     finally:
         idx.close()
+
+
+def test_seed_anchors_on_device_feed_chaining(engine):
+    """pl_seed_anchors_opt_device leaves the anchors on the device with the same offsets; the
+    chaining DP runs on them in place (pl_chain_fill_device) and, finished on the host, gives the
+    chains pl_chain_host gives from the host anchors."""
+    import ctypes as C
+    import torch
+    from protlocus_b200.abi import chain_opt, chain_opt_struct
+    rng = np.random.default_rng(77)
+    ki, kb = O.seed_index(rng, kmer=6, mod_bit=1, n_block=4000)
+    idx = L.SeedIndex(ki, kb, 6, 1)
+    try:
+        prots = seed_proteins(rng, 120)
+        host = L.seed_anchors(engine, idx, prots, 20000)
+        n = len(prots)
+        lens = np.array([len(p) for p in prots], np.int32)
+        offs = np.zeros(n, np.int64)
+        offs[1:] = np.cumsum(lens[:-1])
+        seq = np.frombuffer(b"".join(prots), np.uint8).copy()
+        a_off = np.zeros(n + 1, np.int64)
+        a_dev = C.c_void_p()
+        so = L.SeedOpt(20000, 0, 0, None)
+        tot = engine.lib.pl_seed_anchors_opt_device(engine.h, idx.h, n, seq.ctypes.data, seq.size, offs.ctypes.data,
+                                                    lens.ctypes.data, C.byref(so), a_off.ctypes.data, C.byref(a_dev))
+        assert tot == sum(h.size for h in host) > 0 and list(np.diff(a_off)) == [h.size for h in host]
+        opt = chain_opt("main")
+        o = chain_opt_struct(opt)
+        off, nq = a_off[:-1].copy(), np.diff(a_off).astype(np.int32)
+        d_f, d_p, d_v = (torch.zeros(int(tot), dtype=torch.int32, device="cuda") for _ in range(3))
+        assert engine.lib.pl_chain_fill_device(engine.h, C.byref(o), n, off.ctypes.data, nq.ctypes.data, a_dev.value,
+                                               int(tot), d_f.data_ptr(), d_p.data_ptr(), d_v.data_ptr(), None), L.error()
+        torch.cuda.synchronize()
+        f, p = d_f.cpu().numpy(), d_p.cpu().numpy()
+        want = engine.chain(opt, host)
+        for q in range(n):
+            s = slice(int(off[q]), int(off[q]) + int(nq[q]))
+            u, a_out = L.chain_finish(opt, host[q], f[s], p[s])
+            assert np.array_equal(u, want[q][0]) and np.array_equal(a_out, want[q][1]), q
+    finally:
+        idx.close()
