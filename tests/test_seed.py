@@ -97,3 +97,29 @@ def rescue_index(rng):
     """kmer 5 (2^19 buckets) with 5 % repeat buckets of 150-300 blocks, so that proteins meet
     buckets over the occurrence cap"""
     return O.seed_index(rng, kmer=5, mod_bit=1, n_block=100_000, hot=1 << 19 >> 4, hot_occ=300)
+
+
+def test_seed_boundary_host_checks():
+    """The library's host logic for seeding, no device touched: the query-name hash equals the
+    reference's mp_hash_qname (and the restatement's), and an index of the wrong shape or a
+    missing engine is refused with a reason."""
+    import ctypes as C
+    from protlocus_b200 import lib as L
+    lib = L.load()
+    ref = O.seed_ref_lib()
+    for name in [b"", b"q", b"sp|P12345|TITIN_HUMAN", bytes(range(1, 200))]:
+        h = lib.pl_seed_qname_hash(name)
+        assert h == O.seed_qname_hash(name)
+        if ref is not None:
+            ref.ref_seed_qname_hash.argtypes = [C.c_char_p]
+            ref.ref_seed_qname_hash.restype = C.c_uint32
+            assert h == ref.ref_seed_qname_hash(name)
+    ki = np.zeros(8, np.int64)
+    kb = np.zeros(1, np.uint32)
+    # 8 buckets do not fit kmer 6, mod_bit 1 (2^23 buckets); kmer 9 is over the 32-bit k-mer
+    assert not lib.pl_seed_index_create(0, ki.ctypes.data, 8, kb.ctypes.data, 1, 6, 1)
+    assert "buckets" in L.error()
+    assert not lib.pl_seed_index_create(0, ki.ctypes.data, 8, kb.ctypes.data, 1, 9, 33)
+    a_off = np.zeros(2, np.int64)
+    so = L.SeedOpt(100, 0, 0, None)
+    assert lib.pl_seed_anchors_opt_host(None, None, 1, None, 0, None, None, C.byref(so), a_off.ctypes.data, None, 0) == -1
