@@ -133,3 +133,24 @@ def test_seed_anchors_on_device_feed_chaining(engine):
             assert np.array_equal(u, want[q][0]) and np.array_equal(a_out, want[q][1]), q
     finally:
         idx.close()
+
+
+def test_seed_device_equals_golden(engine):
+    """The device against the anchors the reference's own steps wrote (tests/golden/seed_golden.json)."""
+    import json
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_seed_golden as G
+    with open(os.path.join(os.path.dirname(__file__), "golden", "seed_golden.json")) as f:
+        cases = json.load(f)["cases"]
+    for c in cases:
+        ki, kb, ps, names = G.case_inputs(tuple(c["index"]), tuple(c["proteins"]))
+        assert G.digest(ki, kb, ps) == c["digest"], c["name"]
+        idx = L.SeedIndex(ki, kb, c["index"][0], c["index"][1])
+        try:
+            got = L.seed_anchors(engine, idx, ps, c["max_occ"], c["repeat_cap"], c["budget"], names)
+        finally:
+            idx.close()
+        for q in range(len(ps)):
+            assert [int(x) for x in got[q]] == c["anchors"][q], (c["name"], q)

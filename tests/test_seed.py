@@ -123,3 +123,33 @@ def test_seed_boundary_host_checks():
     a_off = np.zeros(2, np.int64)
     so = L.SeedOpt(100, 0, 0, None)
     assert lib.pl_seed_anchors_opt_host(None, None, 1, None, 0, None, None, C.byref(so), a_off.ctypes.data, None, 0) == -1
+
+
+def _golden():
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "seed_golden.json")) as f:
+        return json.load(f)["cases"]
+
+
+def test_seed_port_equals_golden():
+    """The restatement against the anchors the reference's own steps wrote
+    (tests/golden/make_seed_golden.py); no reference tree needed."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_seed_golden as G
+    rescued = 0
+    for c in _golden():
+        ki, kb, ps, names = G.case_inputs(tuple(c["index"]), tuple(c["proteins"]))
+        assert G.digest(ki, kb, ps) == c["digest"], c["name"]
+        kmer, mod_bit = c["index"][0], c["index"][1]
+        for q, (p, nm) in enumerate(zip(ps, names)):
+            if c["repeat_cap"] > 0:
+                a = O.seed_anchors_acc(ki, kb, kmer, mod_bit, c["max_occ"], c["repeat_cap"], c["budget"], nm, p,
+                                       use_ref=False)
+                rescued += a.size != O.seed_anchors(ki, kb, kmer, mod_bit, c["max_occ"], p, use_ref=False).size
+            else:
+                a = O.seed_anchors(ki, kb, kmer, mod_bit, c["max_occ"], p, use_ref=False)
+            assert [int(x) for x in a] == c["anchors"][q], (c["name"], q)
+    assert rescued >= 10
