@@ -480,7 +480,8 @@ void pl_seed_index_destroy(pl_seed_index_t *x);
  * accuracy mode's repeat rescue, map.c:346-397), sorted ascending (map.c:571).  Fills
  * a_off[0..n] (protein q's anchors at a[a_off[q] .. a_off[q+1]), block << 32 | position)
  * and returns the total; a is written only when the total fits a_cap (call again with a
- * larger array otherwise).  -1 on a bad argument or a device failure (pl_last_error). */
+ * larger array otherwise).  -1 on a bad argument or a device failure (pl_last_error); a batch
+ * is limited to 2^31 - 1 residues and as many anchors. */
 int64_t pl_seed_anchors_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq, int64_t seq_len,
 		const int64_t *off, const int32_t *len, int32_t max_occ, int64_t *a_off, uint64_t *a, int64_t a_cap);
 /* The same with the options of mp_collect_anchors (map.c:346-397): max_occ (opt->max_occ);

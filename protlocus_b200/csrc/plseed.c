@@ -14,6 +14,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <stdint.h>
 #include "plhost.h"
 
 struct pl_seed_index_s {
@@ -95,6 +96,10 @@ static int64_t pl_seed_run(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, 
 	}
 	a_off[0] = 0;
 	if (n == 0) return 0;
+	if (seq_len > INT32_MAX) {  /* the segmented sorts count items in an int */
+		pl_set_error("seed batch of %lld residues: at most %d per call", (long long)seq_len, INT32_MAX);
+		return -1;
+	}
 	for (q = 0; q < n; ++q)
 		if (len[q] < 0 || off[q] < 0 || off[q] + len[q] > seq_len) {
 			pl_set_error("protein %d: length %d at %lld of %lld", q, len[q], (long long)off[q], (long long)seq_len);
@@ -147,6 +152,10 @@ static int64_t pl_seed_run(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, 
 	CK(cudaMemcpyAsync(na, e->s_nanc.p, sizeof(int64_t) * (size_t)n, cudaMemcpyDeviceToHost, st));
 	CK(cudaStreamSynchronize(st));
 	for (q = 0; q < n; ++q) total += na[q], a_off[q + 1] = total;
+	if (total > INT32_MAX) {  /* the anchors' segmented sort counts items in an int */
+		pl_set_error("seed batch with %lld anchors: at most %d per call, split the batch", (long long)total, INT32_MAX);
+		goto fail;
+	}
 	ret = total;
 	if (a_dev) *a_dev = 0;
 	if (total == 0 || (!a_dev && total > a_cap)) goto done;  /* a_off only: the caller grows a to a_off[n] */
