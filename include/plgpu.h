@@ -468,7 +468,8 @@ int64_t pl_gapless_last_steps(const pl_engine_t *e);
 /* ---- Seeding (the sketch and anchor stages of mp_map_coarse, map.c:565-572) ----
  * The mapper's k-mer index (mp_idx_t's ki: the first kb entry of every bucket, n_bucket
  * = 1 << (4 kmer - mod_bit) of them; kb: the block ids, index.c:74-98) copied to a
- * device.  NULL on bad sizes or a device failure (pl_last_error). */
+ * device; kmer 1-7 (at 8 the reference's 32-bit k-mer mask is an undefined shift).  NULL
+ * on bad sizes or a device failure (pl_last_error). */
 typedef struct pl_seed_index_s pl_seed_index_t;
 pl_seed_index_t *pl_seed_index_create(int32_t device, const int64_t *ki, int64_t n_bucket, const uint32_t *kb,
 		int64_t n_kb, int32_t kmer, int32_t mod_bit);

@@ -29,9 +29,11 @@ PL_EXPORT pl_seed_index_t *pl_seed_index_create(int32_t device, const int64_t *k
 		int64_t n_kb, int32_t kmer, int32_t mod_bit)
 {
 	pl_seed_index_t *x;
-	if (kmer < 1 || kmer > 8 || mod_bit < 0 || mod_bit >= kmer * 4 || n_bucket != (int64_t)1 << (kmer * 4 - mod_bit) ||
+	/* kmer 8 would need the 32-bit shift 1U << 32 for the k-mer mask, which C leaves undefined
+	 * (sketch.c:21): the reference's mask then depends on its compiler, so it is refused */
+	if (kmer < 1 || kmer > 7 || mod_bit < 0 || mod_bit >= kmer * 4 || n_bucket != (int64_t)1 << (kmer * 4 - mod_bit) ||
 			n_kb < 0 || n_kb > (int64_t)UINT32_MAX || !ki || (n_kb > 0 && !kb)) {
-		pl_set_error("seed index: kmer %d, mod_bit %d, %lld buckets, %lld entries (kmer 1-8, 1 << (4 kmer - mod_bit) buckets)",
+		pl_set_error("seed index: kmer %d, mod_bit %d, %lld buckets, %lld entries (kmer 1-7, 1 << (4 kmer - mod_bit) buckets)",
 				kmer, mod_bit, (long long)n_bucket, (long long)n_kb);
 		return 0;
 	}

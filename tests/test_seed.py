@@ -120,6 +120,9 @@ def test_seed_boundary_host_checks():
     assert not lib.pl_seed_index_create(0, ki.ctypes.data, 8, kb.ctypes.data, 1, 6, 1)
     assert "buckets" in L.error()
     assert not lib.pl_seed_index_create(0, ki.ctypes.data, 8, kb.ctypes.data, 1, 9, 33)
+    # kmer 8: the reference's mask (1U << 32) - 1 is an undefined shift, so no parity to keep
+    assert not lib.pl_seed_index_create(0, ki.ctypes.data, 8, kb.ctypes.data, 1, 8, 29)
+    assert "kmer 1-7" in L.error()
     a_off = np.zeros(2, np.int64)
     so = L.SeedOpt(100, 0, 0, None)
     assert lib.pl_seed_anchors_opt_host(None, None, 1, None, 0, None, None, C.byref(so), a_off.ctypes.data, None, 0) == -1
