@@ -89,21 +89,17 @@ SP_EXPORT uint32_t sp_qname_hash(const char *qname)
 	return h;
 }
 
-/* the anchors of one protein into *out (malloc'd, sorted); returns their number, -1 on
- * a host allocation failure.  repeat_cap > 0: the accuracy mode's repeat rescue with
- * anchor_budget and the query name's hash qhash */
-SP_EXPORT int64_t sp_anchors_acc(const int64_t *ki, int64_t n_bucket, const uint32_t *kb, int64_t n_kb, int32_t kmer,
-		int32_t mod_bit, int32_t max_occ_opt, int32_t repeat_cap, int64_t anchor_budget, uint32_t qhash,
-		const uint8_t *seq, int32_t len, uint64_t **out)
+/* the anchors of n seeds sd (sorted; freed here) into *out (malloc'd, sorted); returns
+ * their number, -1 on a host allocation failure.  repeat_cap > 0: the accuracy mode's
+ * repeat rescue with anchor_budget and the query name's hash qhash */
+static int64_t sp_anchors_of(const int64_t *ki, int64_t n_bucket, const uint32_t *kb, int64_t n_kb, int32_t max_occ_opt,
+		int32_t repeat_cap, int64_t anchor_budget, uint32_t qhash, uint64_t *sd, int32_t n, uint64_t **out)
 {
-	uint64_t *sd = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(len > 0 ? len : 1)), *cnt, *a;
+	uint64_t *cnt, *a;
 	int64_t *take;
-	int32_t n, i, max_occ = max_occ_opt;
+	int32_t i, max_occ = max_occ_opt;
 	int64_t n_a = 0, n_res = 0, k = 0, j;
 	*out = 0;
-	if (!sd) return -1;
-	n = sp_sketch(seq, len, kmer, mod_bit, sd);
-	qsort(sd, (size_t)n, sizeof(uint64_t), sp_cmp64);  /* mp_sketch_query's order */
 	if (n >= 8) {
 		uint64_t q25, q75;
 		cnt = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)n);
@@ -156,6 +152,143 @@ SP_EXPORT int64_t sp_anchors_acc(const int64_t *ki, int64_t n_bucket, const uint
 	free(sd), free(take);
 	*out = a;
 	return n_a;
+}
+
+SP_EXPORT int64_t sp_anchors_acc(const int64_t *ki, int64_t n_bucket, const uint32_t *kb, int64_t n_kb, int32_t kmer,
+		int32_t mod_bit, int32_t max_occ_opt, int32_t repeat_cap, int64_t anchor_budget, uint32_t qhash,
+		const uint8_t *seq, int32_t len, uint64_t **out)
+{
+	uint64_t *sd = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(len > 0 ? len : 1));
+	int32_t n;
+	*out = 0;
+	if (!sd) return -1;
+	n = sp_sketch(seq, len, kmer, mod_bit, sd);
+	qsort(sd, (size_t)n, sizeof(uint64_t), sp_cmp64);  /* mp_sketch_query's order */
+	return sp_anchors_of(ki, n_bucket, kb, n_kb, max_occ_opt, repeat_cap, anchor_budget, qhash, sd, n, out);
+}
+
+/* ---- HMM-profile queries: mp_sketch_hmm (sketch.c:40-118) and mp_sketch_query's merge
+ * (map.c:332-343) ---- */
+
+#define SP_HMM_ALT 4  /* MP_HMM_MAX_ALT (sketch.c:40) */
+
+typedef struct { int32_t n, loss[SP_HMM_ALT]; uint8_t code[SP_HMM_ALT]; } sp_alt_t;
+
+/* one match state's alternatives: every 13-letter group takes the best emission of its
+ * residues (20 columns in HMMER order ACDEFGHIKLMNPQRSTVWY; a group none of them maps to,
+ * or whose best is INT16_MIN, offers nothing); the groups whose loss against the state's
+ * best group is at most pos_loss, smallest loss first and the lower group first among
+ * equal losses, four at most */
+static void sp_hmm_alts(const int16_t *e20, int32_t pos_loss, const uint8_t *tab, sp_alt_t *al)
+{
+	static const char col[] = "ACDEFGHIKLMNPQRSTVWY";
+	int32_t gs[14], best = INT16_MIN, g, j, r;
+	uint8_t used[14];
+	for (g = 0; g < 14; ++g) gs[g] = INT16_MIN, used[g] = 0;
+	for (j = 0; j < 20; ++j) {
+		g = tab[(uint8_t)col[j]];
+		if (e20[j] > gs[g]) gs[g] = e20[j];
+	}
+	for (g = 0; g < 14; ++g) if (gs[g] > best) best = gs[g];
+	al->n = 0;
+	for (r = 0; r < SP_HMM_ALT; ++r) {  /* selection of the r-th smallest (loss, group) */
+		int32_t pick = -1, pl = 0;
+		for (g = 0; g < 14; ++g) {
+			if (used[g] || gs[g] == INT16_MIN || best - gs[g] > pos_loss) continue;
+			if (pick < 0 || best - gs[g] < pl) pick = g, pl = best - gs[g];
+		}
+		if (pick < 0) break;
+		used[pick] = 1, al->code[r] = (uint8_t)pick, al->loss[r] = pl, ++al->n;
+	}
+}
+
+typedef struct {
+	const sp_alt_t *al;
+	int32_t kmer, mod_bit, left_max, n_emit, max_per_win, end;
+	uint32_t mask_k, mask_mod;
+	uint64_t *out;
+	int64_t n_out;
+} sp_walk_t;
+
+/* the k-mers of one window in lexicographic order of their alternatives' ranks, each
+ * position's alternative within the loss still left (losses are >= 0 and ascending, so
+ * the first that does not fit ends the position); every whole k-mer counts towards
+ * max_per_win, a seed is kept where its hash passes the sampling */
+static void sp_hmm_walk(sp_walk_t *w, int32_t d, int32_t left, uint32_t x)
+{
+	int32_t r;
+	if (d == w->kmer) {
+		const uint32_t y = sp_hash(x, w->mask_k);
+		if ((y & w->mask_mod) == 0) w->out[w->n_out++] = (uint64_t)(y >> w->mod_bit) << 32 | (uint32_t)w->end;
+		++w->n_emit;
+		return;
+	}
+	for (r = 0; r < w->al[d].n && w->n_emit < w->max_per_win && w->al[d].loss[r] <= left; ++r)
+		sp_hmm_walk(w, d + 1, left - w->al[d].loss[r], (x << 4 | w->al[d].code[r]) & w->mask_k);
+}
+
+/* mp_sketch_hmm: the profile-derived seeds of every window of kmer match states (emit:
+ * len x 20), appended to out (room for (len - kmer + 1) * max_per_win); returns their
+ * number, -1 on a host allocation failure */
+SP_EXPORT int64_t sp_sketch_hmm(const int16_t *emit, int32_t len, int32_t kmer, int32_t mod_bit, int32_t pos_loss,
+		int32_t win_loss, int32_t max_per_win, uint64_t *out)
+{
+	uint8_t tab[256];
+	sp_alt_t *al;
+	sp_walk_t w;
+	int32_t i;
+	if (!emit || len < kmer || max_per_win <= 0) return 0;
+	al = (sp_alt_t*)malloc(sizeof(sp_alt_t) * (size_t)len);
+	if (!al) return -1;
+	sp_aa13_table(tab);
+	for (i = 0; i < len; ++i) sp_hmm_alts(emit + (size_t)i * 20, pos_loss, tab, &al[i]);
+	memset(&w, 0, sizeof(w));
+	w.kmer = kmer, w.mod_bit = mod_bit, w.max_per_win = max_per_win, w.out = out;
+	w.mask_k = (1U << kmer * 4) - 1, w.mask_mod = (1U << mod_bit) - 1;
+	for (i = kmer - 1; i < len; ++i) {
+		w.al = al + (i - kmer + 1), w.end = i, w.n_emit = 0;
+		sp_hmm_walk(&w, 0, win_loss, 0);
+	}
+	free(al);
+	return w.n_out;
+}
+
+/* an HMM-profile query's seeds (mp_sketch_query with a profile): the sequence's own (the
+ * parser's consensus, in the mapper) and, when seed_max > 0, the profile-derived ones,
+ * sorted with the duplicates removed; *out malloc'd, returns the number, -1 on a host
+ * allocation failure */
+SP_EXPORT int64_t sp_seeds_hmm_query(const uint8_t *seq, int32_t len, const int16_t *emit, int32_t hmm_len, int32_t kmer,
+		int32_t mod_bit, int32_t pos_loss, int32_t win_loss, int32_t seed_max, uint64_t **out)
+{
+	const int64_t n_win = seed_max > 0 && hmm_len >= kmer ? (int64_t)(hmm_len - kmer + 1) * seed_max : 0;
+	uint64_t *sd = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(len + n_win > 0 ? len + n_win : 1));
+	int64_t n, m, i, k;
+	*out = 0;
+	if (!sd) return -1;
+	n = sp_sketch(seq, len, kmer, mod_bit, sd);
+	if (seed_max > 0) {
+		m = sp_sketch_hmm(emit, hmm_len, kmer, mod_bit, pos_loss, win_loss, seed_max, sd + n);
+		if (m < 0) { free(sd); return -1; }
+		n += m;
+	}
+	qsort(sd, (size_t)n, sizeof(uint64_t), sp_cmp64);
+	for (i = k = 0; i < n; ++i)
+		if (k == 0 || sd[i] != sd[k - 1]) sd[k++] = sd[i];
+	*out = sd;
+	return k;
+}
+
+/* the anchors of an HMM-profile query: its seeds (sp_seeds_hmm_query), then the default
+ * mode's cap and collection (map.c:565-572) */
+SP_EXPORT int64_t sp_anchors_hmm(const int64_t *ki, int64_t n_bucket, const uint32_t *kb, int64_t n_kb, int32_t kmer,
+		int32_t mod_bit, int32_t max_occ_opt, const uint8_t *seq, int32_t len, const int16_t *emit, int32_t hmm_len,
+		int32_t pos_loss, int32_t win_loss, int32_t seed_max, uint64_t **out)
+{
+	uint64_t *sd;
+	const int64_t n = sp_seeds_hmm_query(seq, len, emit, hmm_len, kmer, mod_bit, pos_loss, win_loss, seed_max, &sd);
+	*out = 0;
+	if (n < 0) return -1;
+	return sp_anchors_of(ki, n_bucket, kb, n_kb, max_occ_opt, 0, 0, 0, sd, (int32_t)n, out);
 }
 
 SP_EXPORT int64_t sp_anchors(const int64_t *ki, int64_t n_bucket, const uint32_t *kb, int64_t n_kb, int32_t kmer,

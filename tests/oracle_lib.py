@@ -487,3 +487,106 @@ def seed_qname_hash(qname: bytes) -> int:
     p.sp_qname_hash.argtypes = [C.c_char_p]
     p.sp_qname_hash.restype = C.c_uint32
     return int(p.sp_qname_hash(qname))
+
+
+# ---------------------------------------------------------------- HMM-profile seeds (sketch.c:40-118, map.c:332-343)
+
+def _i16p(a):
+    return np.ascontiguousarray(a, dtype=np.int16)
+
+
+def sketch_hmm(emit, kmer: int, mod_bit: int, pos_loss: int, win_loss: int, max_per_win: int,
+               use_ref: bool | None = None):
+    """mp_sketch_hmm's seeds of an emission table (len x 20 int16, HMMER column order) in the
+    order the reference appends them (window by window); the reference's own function when
+    oracle/_ref/libseed_ref.so is built (or use_ref), else the restatement."""
+    e = _i16p(emit).reshape(-1, 20)
+    n = e.shape[0]
+    lib = seed_ref_lib() if use_ref is not False else None
+    if use_ref and lib is None:
+        raise RuntimeError("oracle/_ref/libseed_ref.so not built")
+    if lib is not None:
+        f = lib.ref_sketch_hmm
+        f.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                      C.POINTER(C.POINTER(C.c_uint64))]
+        f.restype = C.c_int64
+        return _seed_take(f, lib.ref_seed_free, e.ctypes.data, n, kmer, mod_bit, pos_loss, win_loss, max_per_win)
+    p = _seed_port()
+    p.sp_sketch_hmm.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                C.c_void_p]
+    p.sp_sketch_hmm.restype = C.c_int64
+    cap = max(n - kmer + 1, 0) * max(max_per_win, 0)
+    out = np.zeros(max(cap, 1), np.uint64)
+    m = p.sp_sketch_hmm(e.ctypes.data, n, kmer, mod_bit, pos_loss, win_loss, max_per_win, out.ctypes.data)
+    if m < 0:
+        raise MemoryError("seeding checker out of host memory")
+    return out[:m].copy()
+
+
+def hmm_consensus(emit) -> bytes:
+    """The parser's consensus (hmm.c:181-189): per match state the first column of the
+    largest emission, as its HMMER letter."""
+    e = _i16p(emit).reshape(-1, 20)
+    return bytes(b"ACDEFGHIKLMNPQRSTVWY"[int(j)] for j in np.argmax(e, axis=1))
+
+
+def seeds_hmm_query(seq: bytes, emit, kmer: int, mod_bit: int, pos_loss: int, win_loss: int, seed_max: int):
+    """mp_sketch_query with a profile (map.c:332-343), from the restatement: the sequence's
+    seeds and the profile-derived ones, sorted, duplicates removed."""
+    e = _i16p(emit).reshape(-1, 20)
+    p = _seed_port()
+    p.sp_seeds_hmm_query.argtypes = [C.c_char_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                     C.c_int32, C.c_int32, C.POINTER(C.POINTER(C.c_uint64))]
+    p.sp_seeds_hmm_query.restype = C.c_int64
+    return _seed_take(p.sp_seeds_hmm_query, p.sp_free, seq, len(seq), e.ctypes.data, e.shape[0], kmer, mod_bit,
+                      pos_loss, win_loss, seed_max)
+
+
+def anchors_hmm(ki, kb, kmer: int, mod_bit: int, max_occ: int, seq: bytes, emit, pos_loss: int, win_loss: int,
+                seed_max: int):
+    """The anchors of an HMM-profile query (seeds_hmm_query, then the default cap and
+    collection), from the restatement."""
+    e = _i16p(emit).reshape(-1, 20)
+    p = _seed_port()
+    p.sp_anchors_hmm.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
+                                 C.c_char_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                 C.POINTER(C.POINTER(C.c_uint64))]
+    p.sp_anchors_hmm.restype = C.c_int64
+    return _seed_take(p.sp_anchors_hmm, p.sp_free, ki.ctypes.data, ki.size, kb.ctypes.data, kb.size, kmer, mod_bit,
+                      max_occ, seq, len(seq), e.ctypes.data, e.shape[0], pos_loss, win_loss, seed_max)
+
+
+def ref_hmm_query(path: str, kmer: int, mod_bit: int, pos_loss: int, win_loss: int, seed_max: int,
+                  ki=None, kb=None, max_occ: int = 20000):
+    """The reference on an HMMER3 file: its parser, the consensus as the query, and
+    mp_sketch_query's seeds (ki None) or mp_map_coarse's anchors; None when
+    oracle/_ref/libseed_ref.so is not built."""
+    lib = seed_ref_lib()
+    if lib is None:
+        return None
+    f = lib.ref_seed_hmm_query
+    f.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                  C.c_int32, C.c_int32, C.POINTER(C.POINTER(C.c_uint64))]
+    f.restype = C.c_int64
+    return _seed_take(f, lib.ref_seed_free, path.encode(), None if ki is None else ki.ctypes.data,
+                      None if kb is None else kb.ctypes.data, 0 if kb is None else kb.size, kmer, mod_bit, max_occ,
+                      pos_loss, win_loss, seed_max)
+
+
+def ref_hmm_tables(path: str):
+    """The reference parser's consensus and emission table of an HMMER3 file, or None."""
+    lib = seed_ref_lib()
+    if lib is None:
+        return None
+    lib.ref_hmm_consensus.argtypes = [C.c_char_p, C.c_char_p, C.c_int32]
+    lib.ref_hmm_consensus.restype = C.c_int32
+    lib.ref_hmm_emissions.argtypes = [C.c_char_p, C.c_void_p, C.c_int32]
+    lib.ref_hmm_emissions.restype = C.c_int32
+    n = lib.ref_hmm_consensus(path.encode(), None, 0)
+    if n < 0:
+        raise ValueError(f"{path}: the reference parser refused it")
+    buf = C.create_string_buffer(n + 1)
+    lib.ref_hmm_consensus(path.encode(), buf, n + 1)
+    e = np.zeros((n, 20), np.int16)
+    lib.ref_hmm_emissions(path.encode(), e.ctypes.data, n * 20)
+    return buf.raw[:n], e
