@@ -590,3 +590,22 @@ def ref_hmm_tables(path: str):
     e = np.zeros((n, 20), np.int16)
     lib.ref_hmm_emissions(path.encode(), e.ctypes.data, n * 20)
     return buf.raw[:n], e
+
+
+def device_seed_fns_host(emit, kmer: int, mod_bit: int, pos_loss: int, win_loss: int, max_per_win: int):
+    """The device's profile-derived seeding functions (protlocus_b200/csrc/seed_hmm.cuh) built
+    for the host (oracle/_build/libseedhmmcheck.so), window by window as the kernel runs them."""
+    so = os.path.join(ORACLE, "_build", "libseedhmmcheck.so")
+    if not os.path.exists(so):
+        subprocess.run(["make", "-C", ORACLE, "port"], check=True, capture_output=True)
+    lib = C.CDLL(so)
+    lib.shc_sketch_hmm.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                   C.c_void_p]
+    lib.shc_sketch_hmm.restype = C.c_int64
+    e = _i16p(emit).reshape(-1, 20)
+    n = e.shape[0]
+    out = np.zeros(max(max(n - kmer + 1, 0) * max(max_per_win, 0), 1), np.uint64)
+    m = lib.shc_sketch_hmm(e.ctypes.data, n, kmer, mod_bit, pos_loss, win_loss, max_per_win, out.ctypes.data)
+    if m < 0:
+        raise MemoryError("out of host memory")
+    return out[:m].copy()

@@ -193,3 +193,21 @@ def test_seed_hmm_port_equals_golden():
         a = O.anchors_hmm(ki, kb, 6, 1, max_occ, cons, emit, pos_loss, win_loss, mx)
         assert s.size == q["seeds"]["n"] and sha(s) == q["seeds"]["sha256"], q["params"]
         assert a.size == q["anchors"]["n"] and sha(a) == q["anchors"]["sha256"], q["params"]
+
+
+@pytest.mark.parametrize("kind", ["dirichlet", "ties", "stars", "flat"])
+def test_device_functions_host_build_equal_restatement_and_reference(kind):
+    """protlocus_b200/csrc/seed_hmm.cuh, the functions the device kernel runs per state and
+    per window, built for the host: the same seeds in the same order as the restatement and,
+    when built, the reference's mp_sketch_hmm, for every parameter set and table length."""
+    rng = np.random.default_rng({"dirichlet": 21, "ties": 22, "stars": 23, "flat": 24}[kind])
+    ref_lib = O.seed_ref_lib()
+    for kmer, mod_bit, pos_loss, win_loss, mx in PARAMS:
+        for n in sorted({0, 1, kmer - 1, kmer, 53, 300}):
+            e = emission_table(rng, n, kind)
+            dev = O.device_seed_fns_host(e, kmer, mod_bit, pos_loss, win_loss, mx)
+            port = O.sketch_hmm(e, kmer, mod_bit, pos_loss, win_loss, mx, use_ref=False)
+            assert np.array_equal(dev, port), (kind, kmer, mod_bit, pos_loss, win_loss, mx, n)
+            if ref_lib is not None:
+                ref = O.sketch_hmm(e, kmer, mod_bit, pos_loss, win_loss, mx, use_ref=True)
+                assert np.array_equal(dev, ref)
