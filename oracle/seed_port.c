@@ -172,49 +172,55 @@ SP_EXPORT int64_t sp_anchors_acc(const int64_t *ki, int64_t n_bucket, const uint
 
 #define SP_HMM_ALT 4  /* MP_HMM_MAX_ALT (sketch.c:40) */
 
-typedef struct { int32_t n, loss[SP_HMM_ALT]; uint8_t code[SP_HMM_ALT]; } sp_alt_t;
+typedef struct { int32_t n; int16_t loss[SP_HMM_ALT]; uint8_t code[SP_HMM_ALT]; } sp_alt_t;
 
-/* one match state's alternatives: every 13-letter group takes the best emission of its
- * residues (20 columns in HMMER order ACDEFGHIKLMNPQRSTVWY; a group none of them maps to,
- * or whose best is INT16_MIN, offers nothing); the groups whose loss against the state's
- * best group is at most pos_loss, smallest loss first and the lower group first among
- * equal losses, four at most */
+/* one match state's alternatives (sketch.c:57-76): every 13-letter group takes the best
+ * emission of its residues (20 columns in HMMER order ACDEFGHIKLMNPQRSTVWY; a group none of
+ * them maps to, or whose best is INT16_MIN, offers nothing); the groups within pos_loss of
+ * the state's best are offered in group order to a list of four kept in ascending order by
+ * insertion: a full list takes a group only below its last entry, which drops out, and a
+ * group goes after the kept entries not above it.  Losses are stored in 16 bits as the
+ * reference's alt_loss (a loss over 32767 wraps; the comparisons then see the wrapped
+ * entries against the new group's full loss) */
 static void sp_hmm_alts(const int16_t *e20, int32_t pos_loss, const uint8_t *tab, sp_alt_t *al)
 {
 	static const char col[] = "ACDEFGHIKLMNPQRSTVWY";
-	int32_t gs[14], best = INT16_MIN, g, j, r;
-	uint8_t used[14];
-	for (g = 0; g < 14; ++g) gs[g] = INT16_MIN, used[g] = 0;
+	int32_t gs[14], best = INT16_MIN, g, j;
+	for (g = 0; g < 14; ++g) gs[g] = INT16_MIN;
 	for (j = 0; j < 20; ++j) {
 		g = tab[(uint8_t)col[j]];
 		if (e20[j] > gs[g]) gs[g] = e20[j];
 	}
 	for (g = 0; g < 14; ++g) if (gs[g] > best) best = gs[g];
-	al->n = 0;
-	for (r = 0; r < SP_HMM_ALT; ++r) {  /* selection of the r-th smallest (loss, group) */
-		int32_t pick = -1, pl = 0;
-		for (g = 0; g < 14; ++g) {
-			if (used[g] || gs[g] == INT16_MIN || best - gs[g] > pos_loss) continue;
-			if (pick < 0 || best - gs[g] < pl) pick = g, pl = best - gs[g];
-		}
-		if (pick < 0) break;
-		used[pick] = 1, al->code[r] = (uint8_t)pick, al->loss[r] = pl, ++al->n;
+	memset(al, 0, sizeof(*al));
+	for (g = 0; g < 14; ++g) {
+		const int32_t loss = best - gs[g];
+		int32_t stay, at;
+		if (gs[g] == INT16_MIN || loss > pos_loss) continue;
+		if (al->n == SP_HMM_ALT && loss >= al->loss[SP_HMM_ALT - 1]) continue;
+		stay = al->n < SP_HMM_ALT ? al->n : SP_HMM_ALT - 1;
+		at = stay;
+		while (at > 0 && al->loss[at - 1] > loss) --at;
+		memmove(&al->loss[at + 1], &al->loss[at], sizeof(int16_t) * (size_t)(stay - at));
+		memmove(&al->code[at + 1], &al->code[at], (size_t)(stay - at));
+		al->loss[at] = (int16_t)loss, al->code[at] = (uint8_t)g;
+		al->n = stay + 1;
 	}
 }
 
 typedef struct {
 	const sp_alt_t *al;
-	int32_t kmer, mod_bit, left_max, n_emit, max_per_win, end;
+	int32_t kmer, mod_bit, win_loss, n_emit, max_per_win, end;
 	uint32_t mask_k, mask_mod;
 	uint64_t *out;
 	int64_t n_out;
 } sp_walk_t;
 
-/* the k-mers of one window in lexicographic order of their alternatives' ranks, each
- * position's alternative within the loss still left (losses are >= 0 and ascending, so
- * the first that does not fit ends the position); every whole k-mer counts towards
- * max_per_win, a seed is kept where its hash passes the sampling */
-static void sp_hmm_walk(sp_walk_t *w, int32_t d, int32_t left, uint32_t x)
+/* the k-mers of one window in lexicographic order of their alternatives' ranks (sketch.c:
+ * 78-110): a position's next alternative is taken while the losses so far (acc) plus its
+ * own stay within win_loss, the first that does not ends the position; every whole k-mer
+ * counts towards max_per_win, a seed is kept where its hash passes the sampling */
+static void sp_hmm_walk(sp_walk_t *w, int32_t d, int32_t acc, uint32_t x)
 {
 	int32_t r;
 	if (d == w->kmer) {
@@ -223,8 +229,8 @@ static void sp_hmm_walk(sp_walk_t *w, int32_t d, int32_t left, uint32_t x)
 		++w->n_emit;
 		return;
 	}
-	for (r = 0; r < w->al[d].n && w->n_emit < w->max_per_win && w->al[d].loss[r] <= left; ++r)
-		sp_hmm_walk(w, d + 1, left - w->al[d].loss[r], (x << 4 | w->al[d].code[r]) & w->mask_k);
+	for (r = 0; r < w->al[d].n && w->n_emit < w->max_per_win && acc + w->al[d].loss[r] <= w->win_loss; ++r)
+		sp_hmm_walk(w, d + 1, acc + w->al[d].loss[r], (x << 4 | w->al[d].code[r]) & w->mask_k);
 }
 
 /* mp_sketch_hmm: the profile-derived seeds of every window of kmer match states (emit:
@@ -243,11 +249,11 @@ SP_EXPORT int64_t sp_sketch_hmm(const int16_t *emit, int32_t len, int32_t kmer, 
 	sp_aa13_table(tab);
 	for (i = 0; i < len; ++i) sp_hmm_alts(emit + (size_t)i * 20, pos_loss, tab, &al[i]);
 	memset(&w, 0, sizeof(w));
-	w.kmer = kmer, w.mod_bit = mod_bit, w.max_per_win = max_per_win, w.out = out;
+	w.kmer = kmer, w.mod_bit = mod_bit, w.win_loss = win_loss, w.max_per_win = max_per_win, w.out = out;
 	w.mask_k = (1U << kmer * 4) - 1, w.mask_mod = (1U << mod_bit) - 1;
 	for (i = kmer - 1; i < len; ++i) {
 		w.al = al + (i - kmer + 1), w.end = i, w.n_emit = 0;
-		sp_hmm_walk(&w, 0, win_loss, 0);
+		sp_hmm_walk(&w, 0, 0, 0);
 	}
 	free(al);
 	return w.n_out;

@@ -181,9 +181,11 @@ typedef struct {
 /* seeding of a batch of proteins (seed.cu) */
 typedef struct {
 	const uint8_t *seq;          /* the proteins, concatenated (letters or codes 0-21) */
-	const int64_t *off;          /* protein q at seq[off[q]], len[q] bytes; also its seed slots */
+	const int64_t *off;          /* protein q at seq[off[q]], len[q] bytes */
 	const int32_t *len;
 	int32_t n;
+	const int64_t *soff;         /* protein q's seed slots from soff[q] (n + 1 entries; off when
+	                                the slots are the residues') */
 	const int64_t *ki;           /* the index: bucket starts (n_bucket) and block ids (n_kb) */
 	int64_t n_bucket;
 	const uint32_t *kb;
@@ -192,11 +194,21 @@ typedef struct {
 	int32_t repeat_cap;          /* > 0: the accuracy mode's repeat rescue (map.c:360-384) */
 	int64_t budget;              /* its anchor budget */
 	const uint32_t *qhash;       /* per protein: the query name's hash (the rescue's start) */
-	uint64_t *seeds;             /* per residue slot: the seeds (position order; sorted for the rescue) */
-	uint32_t *cnt;               /* per residue slot: the seeds' bucket sizes */
-	int32_t *take;               /* per residue slot: the anchors each seed gives */
+	uint64_t *seeds;             /* per seed slot: the seeds (position order; sorted for the rescue
+	                                and for profiles) */
+	uint32_t *cnt;               /* per seed slot: the seeds' bucket sizes */
+	int32_t *take;               /* per seed slot: the anchors each seed gives */
 	int32_t *n_seed, *cap;       /* per protein: seeds, occurrence cap */
-	int64_t *seed_end;           /* per protein: off + n_seed (the seeds' segment for a sort) */
+	int64_t *seed_end;           /* per protein: soff + n_seed (the seeds' segment for a sort) */
+	/* HMM-profile queries (mp_sketch_hmm, sketch.c:40-118): per protein its profile's match
+	 * states e_off[q] .. e_off[q] + e_len[q] - 1 of emit (20 int16 each), their offered
+	 * groups in alts (sh_alts_t of seed_hmm.cuh, n_state of them) */
+	const int16_t *emit;
+	int64_t n_state;
+	const int64_t *e_off;
+	const int32_t *e_len;
+	void *alts;
+	int32_t pos_loss, win_loss, seed_max, pad1;
 	int64_t *n_anchor;           /* per protein: anchors */
 	const int64_t *a_off;        /* per protein: first anchor (n + 1 entries) */
 	uint64_t *anchors;
@@ -204,6 +216,13 @@ typedef struct {
 int plk_seed_sketch(const plk_seed_args_t *a, void *stream);
 int plk_seed_take(const plk_seed_args_t *a, void *stream);
 int plk_seed_emit(const plk_seed_args_t *a, void *stream);
+/* profiles: every state's offered groups; the windows' seeds appended to each protein's own */
+int plk_seed_hmm_alts(const plk_seed_args_t *a, void *stream);
+int plk_seed_hmm_enum(const plk_seed_args_t *a, void *stream);
+/* the seeds sorted (sorted, soff..seed_end) without duplicates into seeds, their bucket
+ * sizes, counts and the occurrence cap (the rest of mp_sketch_query with a profile and
+ * mp_cal_max_occ) */
+int plk_seed_unique(const plk_seed_args_t *a, const uint64_t *sorted, void *stream);
 int plk_seed_sort(const uint64_t *keys_in, uint64_t *keys_out, int64_t n_items, int32_t n_seg, const int64_t *seg_off,
 		const int64_t *seg_end, void *tmp, size_t *tmp_bytes, void *stream);
 #define PLK_RC_MAX_M 2048

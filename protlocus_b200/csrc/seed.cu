@@ -69,6 +69,24 @@ __device__ uint32_t sd_select(const uint32_t *v, const int32_t n, int64_t k, con
 	return prefix;
 }
 
+/* the end of a protein's sketch, the whole warp: its n seeds' bucket sizes cnt (written
+ * by the warp's lanes) give the occurrence cap, from 8 seeds on the box-plot bound over
+ * the sizes' order statistics at these indices (map.c:310-319) limited by the option
+ * (map.c:566-569); lane 0 records the count, the cap and the seeds' segment end */
+__device__ __forceinline__ void sd_finish(const plk_seed_args_t &A, const int64_t q, const uint32_t *cnt, const int32_t n,
+		const int lane)
+{
+	__syncwarp();
+	int32_t max_occ = A.max_occ;
+	if (n >= 8) {
+		const int64_t k25 = (int64_t)(n * .25 + .499), k75 = (int64_t)(n * .75 + .499);
+		const uint64_t q75 = sd_select(cnt, n, k75, lane), q25 = sd_select(cnt, n, k25, lane);
+		max_occ = (int32_t)__dadd_rn(__dadd_rn((double)q75, __dmul_rn((double)(q75 - q25), 1.5)), 10.);
+		if (max_occ > A.max_occ) max_occ = A.max_occ;
+	}
+	if (lane == 0) A.n_seed[q] = n, A.cap[q] = max_occ, A.seed_end[q] = A.soff[q] + n;
+}
+
 /* one warp per protein: the seeds in position order (a position's k-mer is its last kmer
  * residues when none of them restarts the k-mer, which is what the reference's rolling
  * k-mer holds), their bucket sizes, the cap and the anchor count */
@@ -88,8 +106,8 @@ __global__ void __launch_bounds__(256) k_seed_sketch(plk_seed_args_t A)
 	if (q >= A.n) return;  /* whole warps */
 	const uint8_t *seq = A.seq + A.off[q];
 	const int32_t len = A.len[q], kmer = A.kmer;
-	uint64_t *sd = A.seeds + A.off[q];
-	uint32_t *cnt = A.cnt + A.off[q];
+	uint64_t *sd = A.seeds + A.soff[q];
+	uint32_t *cnt = A.cnt + A.soff[q];
 	const uint32_t mask_k = (1U << kmer * 4) - 1, mask_mod = (1U << A.mod_bit) - 1;
 	int32_t n = 0;
 	for (int32_t i0 = 0; i0 < len; i0 += 32) {
@@ -117,15 +135,7 @@ __global__ void __launch_bounds__(256) k_seed_sketch(plk_seed_args_t A)
 		}
 		n += __popc(bal);
 	}
-	__syncwarp();
-	int32_t max_occ = A.max_occ;
-	if (n >= 8) {  /* map.c:310-319: the sizes' order statistics at these indices */
-		const int64_t k25 = (int64_t)(n * .25 + .499), k75 = (int64_t)(n * .75 + .499);
-		const uint64_t q75 = sd_select(cnt, n, k75, lane), q25 = sd_select(cnt, n, k25, lane);
-		max_occ = (int32_t)__dadd_rn(__dadd_rn((double)q75, __dmul_rn((double)(q75 - q25), 1.5)), 10.);
-		if (max_occ > A.max_occ) max_occ = A.max_occ;
-	}
-	if (lane == 0) A.n_seed[q] = n, A.cap[q] = max_occ, A.seed_end[q] = A.off[q] + n;
+	sd_finish(A, q, cnt, n, lane);
 }
 
 /* one warp per protein: the anchors each seed gives (mp_collect_anchors, map.c:352-384):
@@ -138,8 +148,8 @@ __global__ void __launch_bounds__(256) k_seed_take(plk_seed_args_t A)
 	const int lane = threadIdx.x & 31;
 	const int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	if (q >= A.n) return;  /* whole warps */
-	const uint64_t *sd = A.seeds + A.off[q];
-	int32_t *take = A.take + A.off[q];
+	const uint64_t *sd = A.seeds + A.soff[q];
+	int32_t *take = A.take + A.soff[q];
 	const int32_t n = A.n_seed[q], max_occ = A.cap[q], rcap = A.repeat_cap;
 	int64_t n_base = 0, n_res = 0;
 	for (int32_t j = lane; j < n; j += 32) {
@@ -182,9 +192,9 @@ __global__ void __launch_bounds__(32 * SD_EMIT_WARPS) k_seed_emit(plk_seed_args_
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	const int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	if (q >= A.n) return;  /* whole warps */
-	const uint64_t *sd = A.seeds + A.off[q];
+	const uint64_t *sd = A.seeds + A.soff[q];
 	const int32_t n = A.n_seed[q];
-	const int32_t *take = A.take + A.off[q];
+	const int32_t *take = A.take + A.soff[q];
 	uint64_t *a = A.anchors + A.a_off[q];
 	int64_t k = 0;
 	/* 32 seeds at a time: their buckets' starts and sizes (0 past the cap) side by side, an

@@ -7,14 +7,18 @@
  * A match state's emissions are 20 int16 in HMMER column order ACDEFGHIKLMNPQRSTVWY
  * (mp_hmm_emissions).  Each of the 13-letter groups (nasw-tab.c:12) takes the best
  * emission of its residues; the state offers the groups whose loss (best group's emission
- * minus the group's) is at most pos_loss, smallest loss first and the lower group first
- * among equal losses, four at most (MP_HMM_MAX_ALT).  A group none of the 20 residues
- * maps to (9), or whose best emission is INT16_MIN, offers nothing.
+ * minus the group's) is at most pos_loss, four at most (MP_HMM_MAX_ALT), placed in group
+ * order into a list kept in ascending loss order by insertion (a new group goes after
+ * every kept entry not above it; when the list is full it enters only below the last
+ * entry, which then drops out).  A group none of the 20 residues maps to (9), or whose
+ * best emission is INT16_MIN, offers nothing.  The list keeps its losses in 16 bits, as
+ * the reference does (a loss over 32767, reachable only with pos_loss over 32767, wraps,
+ * and the later comparisons and the window sums see the wrapped value).
  *
  * A window of kmer states ending at state `end` yields the k-mers of the states' offered
- * groups in lexicographic order of their ranks whose summed loss stays within win_loss
- * (losses are >= 0 and each state's ascending, so the first rank that does not fit ends
- * that state's choices); the first max_per_win such k-mers count, and each whose masked
+ * groups in lexicographic order of their ranks, walked depth first: a state's next rank is
+ * tried while the losses so far plus its loss stay within win_loss, the first that does not
+ * ends that state's choices; the first max_per_win whole k-mers count, and each whose masked
  * hash (sketch.c:7-16) has mod_bit zero low bits gives the seed
  * (hash >> mod_bit) << 32 | end.
  */
@@ -32,7 +36,8 @@
 #define SH_ALT 4       /* MP_HMM_MAX_ALT */
 #define SH_MAX_KMER 7  /* the index's largest k-mer (4 bits per residue in 32) */
 
-/* a state's offered groups: n in bits 0-3, group r in bits 4 + 4r .. 7 + 4r */
+/* a state's offered groups: n in bits 0-3, group r in bits 4 + 4r .. 7 + 4r; loss[r] the
+ * loss as a 16-bit value (sign-extended) */
 typedef struct { uint32_t code_n; int32_t loss[SH_ALT]; } sh_alts_t;
 
 /* the 13-letter group of HMMER column j (A C D E F G H I K L M N P Q R S T V W Y) */
@@ -59,8 +64,7 @@ SH_FN uint32_t sh_hash(uint32_t key, uint32_t mask)
 /* one match state's offered groups */
 SH_FN sh_alts_t sh_state_alts(const int16_t *e20, int32_t pos_loss)
 {
-	int32_t gs[14], best = INT16_MIN, g, j, r;
-	uint32_t taken = 0;
+	int32_t gs[14], best = INT16_MIN, code[SH_ALT], g, j, n = 0;
 	sh_alts_t a;
 	for (g = 0; g < 14; ++g) gs[g] = INT16_MIN;
 	for (j = 0; j < 20; ++j) {
@@ -68,40 +72,40 @@ SH_FN sh_alts_t sh_state_alts(const int16_t *e20, int32_t pos_loss)
 		gs[c] = v > gs[c] ? v : gs[c];
 	}
 	for (g = 0; g < 14; ++g) best = gs[g] > best ? gs[g] : best;
-	a.code_n = 0;
-	for (r = 0; r < SH_ALT; ++r) a.loss[r] = 0;
-	for (r = 0; r < SH_ALT; ++r) {  /* the r-th smallest (loss, group) not yet taken */
-		int32_t pick = -1, pl = 0;
-		for (g = 0; g < 14; ++g) {
-			const int32_t l = best - gs[g];
-			const int ok = !((taken >> g) & 1u) && gs[g] != INT16_MIN && l <= pos_loss;
-			if (ok && (pick < 0 || l < pl)) pick = g, pl = l;
-		}
-		if (pick < 0) break;
-		taken |= 1u << pick;
-		a.code_n |= (uint32_t)pick << (4 + 4 * r);
-		a.loss[r] = pl;
-		a.code_n = (a.code_n & ~15u) | (uint32_t)(r + 1);
+	for (j = 0; j < SH_ALT; ++j) a.loss[j] = 0, code[j] = 0;
+	for (g = 0; g < 14; ++g) {
+		const int32_t l = best - gs[g];
+		int32_t keep, p;
+		if (gs[g] == INT16_MIN || l > pos_loss) continue;
+		if (n == SH_ALT && l >= a.loss[SH_ALT - 1]) continue;  /* full, and not below the last */
+		keep = n < SH_ALT ? n : SH_ALT - 1;                   /* the entries that stay */
+		for (p = keep; p > 0 && a.loss[p - 1] > l; --p) {}    /* after the last one not above l */
+		for (j = keep; j > p; --j) a.loss[j] = a.loss[j - 1], code[j] = code[j - 1];
+		a.loss[p] = (int16_t)l, code[p] = g;
+		n = keep + 1;
 	}
+	a.code_n = (uint32_t)n;
+	for (j = 0; j < n; ++j) a.code_n |= (uint32_t)code[j] << (4 + 4 * j);
 	return a;
 }
 
 /* the seeds of the window of states al[0 .. kmer-1] ending at state `end`, into out
- * (room for max_per_win); returns their number */
+ * (room for max_per_win; NULL: only counted); returns their number */
 SH_FN int32_t sh_window_seeds(const sh_alts_t *al, int32_t kmer, int32_t mod_bit, int32_t win_loss,
 		int32_t max_per_win, int32_t end, uint64_t *out)
 {
 	const uint32_t mask_k = (1U << kmer * 4) - 1, mask_mod = (1U << mod_bit) - 1;
-	int32_t rank[SH_MAX_KMER], left[SH_MAX_KMER + 1], d = 0, n_kmer = 0, n_out = 0;
+	/* acc: the states' summed 16-bit losses, within 7 x 32768 of 0, so no sum overflows */
+	int32_t rank[SH_MAX_KMER], acc[SH_MAX_KMER + 1], d = 0, n_kmer = 0, n_out = 0;
 	uint32_t pre[SH_MAX_KMER + 1];
 	if (kmer < 1 || kmer > SH_MAX_KMER || max_per_win <= 0) return 0;
-	rank[0] = 0, left[0] = win_loss, pre[0] = 0;
-	/* depth-first over the ranks: at depth d, state d's choice rank[d] within the loss left
-	 * by the states before it; a whole k-mer at depth kmer - 1 */
+	rank[0] = 0, acc[0] = 0, pre[0] = 0;
+	/* depth-first over the ranks: at depth d, state d's choice rank[d] with the losses of
+	 * the states before it in acc[d]; a whole k-mer at depth kmer - 1 */
 	while (d >= 0) {
 		const uint32_t cn = al[d].code_n;
 		const int32_t r = rank[d];
-		if (r >= (int32_t)(cn & 15u) || al[d].loss[r] > left[d]) {  /* state d has nothing more within budget */
+		if (r >= (int32_t)(cn & 15u) || acc[d] + al[d].loss[r] > win_loss) {  /* state d has no more choices */
 			if (--d >= 0) ++rank[d];
 			continue;
 		}
@@ -109,11 +113,14 @@ SH_FN int32_t sh_window_seeds(const sh_alts_t *al, int32_t kmer, int32_t mod_bit
 			const uint32_t x = (pre[d] << 4 | ((cn >> (4 + 4 * r)) & 15u)) & mask_k;
 			if (d + 1 == kmer) {
 				const uint32_t y = sh_hash(x, mask_k);
-				if ((y & mask_mod) == 0) out[n_out++] = (uint64_t)(y >> mod_bit) << 32 | (uint32_t)end;
+				if ((y & mask_mod) == 0) {
+					if (out) out[n_out] = (uint64_t)(y >> mod_bit) << 32 | (uint32_t)end;
+					++n_out;
+				}
 				if (++n_kmer >= max_per_win) break;
 				++rank[d];
 			} else {
-				pre[d + 1] = x, left[d + 1] = left[d] - al[d].loss[r];
+				pre[d + 1] = x, acc[d + 1] = acc[d] + al[d].loss[r];
 				rank[++d] = 0;
 			}
 		}

@@ -5,7 +5,8 @@ seeding steps, and hmm.c's parser (oracle/_ref/libseed_ref.so, `make -C oracle s
 run on
   * emission tables regenerated from seeds (tests/test_seed_hmm.emission_table: Dirichlet
     profiles, ties, unreadable entries, flat rows) under several parameter sets: the
-    profile-derived seeds in the reference's order;
+    profile-derived seeds in the reference's order (with a pos_loss that lets losses over
+    32767 into the lists, which the reference keeps in 16 bits);
   * synthetic HMMER3 profiles (protlocus_b200.hmm.synthetic_profiles) read by the
     reference's parser: the query's merged seeds and its anchors on a seeded synthetic index
     (tests/oracle_lib.seed_index).
@@ -31,8 +32,9 @@ sys.path.insert(0, os.path.dirname(HERE))
 import numpy as np  # noqa: E402
 
 # emission table (kind, n, seed) x (kmer, mod_bit, pos_loss, win_loss, max_per_win)
-TABLES = [("dirichlet", 300, 901), ("ties", 120, 902), ("stars", 150, 903), ("flat", 40, 904)]
-TABLE_PARAMS = [(6, 1, 6, 8, 16), (5, 0, 6, 8, 16), (6, 2, 12, 20, 64), (4, 0, 100, 1000, 300)]
+TABLES = [("dirichlet", 300, 901), ("ties", 120, 902), ("stars", 150, 903), ("flat", 40, 904), ("wide", 200, 905)]
+TABLE_PARAMS = [(6, 1, 6, 8, 16), (5, 0, 6, 8, 16), (6, 2, 12, 20, 64), (4, 0, 100, 1000, 300),
+                (6, 1, 40000, 40000, 16)]  # the last: losses over 32767 kept in 16 bits
 # profiles (n, seed) x index (kmer 6, mod_bit 1, seed) x (pos_loss, win_loss, seed_max, max_occ)
 PROFILES = (4, 911)
 INDEX_SEED = 912

@@ -32,6 +32,12 @@ PARAMS = [(6, 1, 6, 8, 16), (5, 0, 6, 8, 16), (7, 1, 6, 8, 16), (6, 2, 12, 20, 6
           (6, 1, 6, 8, 1), (6, 1, 6, 8, 0), (1, 0, 6, 8, 16), (4, 0, 100, 1000, 300)]
 
 
+# budgets past 16 bits: a state's losses over 32767 are kept wrapped to 16 bits, as the
+# reference's alt_loss keeps them; window budgets at the int32 limits and below 0
+WIDE_PARAMS = [(6, 1, 40000, 40000, 16), (6, 1, 70000, 2 ** 31 - 1, 16), (5, 0, 100000, -5, 16),
+               (6, 1, 32767, 65534, 16), (4, 0, 65535, 0, 300), (3, 0, 2 ** 31 - 1, -(2 ** 31), 64)]
+
+
 def emission_table(rng, n: int, kind: str) -> np.ndarray:
     """n match states x 20 columns of int16 emissions of the given kind."""
     if kind == "dirichlet":
@@ -45,6 +51,11 @@ def emission_table(rng, n: int, kind: str) -> np.ndarray:
         e[rng.random((n, 20)) < 0.3] = -32768
         if n:
             e[rng.integers(0, n, size=max(1, n // 10))] = -32768  # rows the parser read as all '*'
+    elif kind == "wide":  # one to three columns high, the rest far below: losses over 32767 kept
+        e = rng.integers(-32767, 0, size=(n, 20))
+        for i in range(n):
+            e[i, rng.choice(20, size=int(rng.integers(1, 4)), replace=False)] = rng.integers(20000, 32768)
+        e[rng.random((n, 20)) < 0.05] = -32768
     elif kind == "flat":
         e = np.full((n, 20), 4)
         if n > 4:
@@ -211,3 +222,25 @@ def test_device_functions_host_build_equal_restatement_and_reference(kind):
             if ref_lib is not None:
                 ref = O.sketch_hmm(e, kmer, mod_bit, pos_loss, win_loss, mx, use_ref=True)
                 assert np.array_equal(dev, ref)
+
+
+@pytest.mark.parametrize("kind", ["wide", "stars", "dirichlet"])
+def test_sketch_hmm_losses_past_16_bits(kind):
+    """pos_loss over 32767 lets losses over 32767 into a state's list, where the reference
+    keeps them in 16 bits (wrapped): the restatement and the device functions' host build
+    follow it, checked against the reference where it is built (else the two against each
+    other); window budgets at the int32 limits and negative."""
+    rng = np.random.default_rng({"wide": 31, "stars": 32, "dirichlet": 33}[kind])
+    ref_lib = O.seed_ref_lib()
+    total = 0
+    for kmer, mod_bit, pos_loss, win_loss, mx in WIDE_PARAMS:
+        for n in (kmer, 60, 250):
+            e = emission_table(rng, n, kind)
+            port = O.sketch_hmm(e, kmer, mod_bit, pos_loss, win_loss, mx, use_ref=False)
+            dev = O.device_seed_fns_host(e, kmer, mod_bit, pos_loss, win_loss, mx)
+            assert np.array_equal(dev, port), (kind, kmer, mod_bit, pos_loss, win_loss, mx, n)
+            if ref_lib is not None:
+                ref = O.sketch_hmm(e, kmer, mod_bit, pos_loss, win_loss, mx, use_ref=True)
+                assert np.array_equal(ref, port), (kind, kmer, mod_bit, pos_loss, win_loss, mx, n, ref.size, port.size)
+            total += port.size
+    assert total > 0
