@@ -504,6 +504,32 @@ int64_t pl_seed_anchors_opt_host(pl_engine_t *e, const pl_seed_index_t *x, int32
 int64_t pl_seed_anchors_opt_device(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
 		int64_t seq_len, const int64_t *off, const int32_t *len, const pl_seed_opt_t *opt, int64_t *a_off,
 		const uint64_t **a_dev);
+/* HMM-profile queries, as mp_map_hmm_file maps one (map.c:1184-1196): the protein is the
+ * profile's consensus (hmm.c:181-189, the first column of the largest emission per match
+ * state), and per protein its profile's match emissions give the profile-derived seeds of
+ * mp_sketch_hmm (sketch.c:40-118), merged with the protein's own, sorted and deduplicated
+ * (mp_sketch_query with a profile, map.c:332-343) before the cap and the anchors.
+ * seed_max <= 0: the protein's own seeds only (as the reference, which then has nothing to
+ * merge).  The rescue of opt applies as in pl_seed_anchors_opt_host. */
+typedef struct {
+	const int16_t *emit;    /* 20 int16 per match state, HMMER column order ACDEFGHIKLMNPQRSTVWY
+	                           (mp_hmm_emissions) */
+	int64_t n_state;        /* match states in emit */
+	const int64_t *e_off;   /* protein q's profile: states e_off[q] .. e_off[q] + e_len[q] - 1 */
+	const int32_t *e_len;
+	int32_t pos_loss;       /* hmm_seed_pos_loss (options.c:112: 6) */
+	int32_t win_loss;       /* hmm_seed_win_loss (options.c:113: 8) */
+	int32_t seed_max;       /* hmm_seed_max for the coarse stage (options.c:114: 16) */
+	int32_t pad;
+} pl_seed_hmm_t;
+/* as pl_seed_anchors_opt_host / _device; a batch's seed slots (each protein's length plus
+ * min(seed_max, 4^kmer) per window of its profile) must stay within INT32_MAX */
+int64_t pl_seed_anchors_hmm_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
+		int64_t seq_len, const int64_t *off, const int32_t *len, const pl_seed_opt_t *opt, const pl_seed_hmm_t *h,
+		int64_t *a_off, uint64_t *a, int64_t a_cap);
+int64_t pl_seed_anchors_hmm_device(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
+		int64_t seq_len, const int64_t *off, const int32_t *len, const pl_seed_opt_t *opt, const pl_seed_hmm_t *h,
+		int64_t *a_off, const uint64_t **a_dev);
 /* mp_hash_qname (map.c:322-329) of a query name */
 uint32_t pl_seed_qname_hash(const char *qname);
 

@@ -284,17 +284,18 @@ SP_EXPORT int64_t sp_seeds_hmm_query(const uint8_t *seq, int32_t len, const int1
 	return k;
 }
 
-/* the anchors of an HMM-profile query: its seeds (sp_seeds_hmm_query), then the default
- * mode's cap and collection (map.c:565-572) */
+/* the anchors of an HMM-profile query: its seeds (sp_seeds_hmm_query), then the cap and
+ * the collection (map.c:565-572), with the repeat rescue when repeat_cap > 0 */
 SP_EXPORT int64_t sp_anchors_hmm(const int64_t *ki, int64_t n_bucket, const uint32_t *kb, int64_t n_kb, int32_t kmer,
-		int32_t mod_bit, int32_t max_occ_opt, const uint8_t *seq, int32_t len, const int16_t *emit, int32_t hmm_len,
-		int32_t pos_loss, int32_t win_loss, int32_t seed_max, uint64_t **out)
+		int32_t mod_bit, int32_t max_occ_opt, int32_t repeat_cap, int64_t anchor_budget, uint32_t qhash,
+		const uint8_t *seq, int32_t len, const int16_t *emit, int32_t hmm_len, int32_t pos_loss, int32_t win_loss,
+		int32_t seed_max, uint64_t **out)
 {
 	uint64_t *sd;
 	const int64_t n = sp_seeds_hmm_query(seq, len, emit, hmm_len, kmer, mod_bit, pos_loss, win_loss, seed_max, &sd);
 	*out = 0;
 	if (n < 0) return -1;
-	return sp_anchors_of(ki, n_bucket, kb, n_kb, max_occ_opt, 0, 0, 0, sd, (int32_t)n, out);
+	return sp_anchors_of(ki, n_bucket, kb, n_kb, max_occ_opt, repeat_cap, anchor_budget, qhash, sd, (int32_t)n, out);
 }
 
 SP_EXPORT int64_t sp_anchors(const int64_t *ki, int64_t n_bucket, const uint32_t *kb, int64_t n_kb, int32_t kmer,

@@ -85,12 +85,15 @@ int64_t ref_sketch_hmm(const int16_t *emit, int32_t len, int32_t kmer, int32_t m
 }
 
 /* a profile read from an HMMER3 text file by the reference's parser (hmm.c:112-195), its
- * consensus the query, as mp_map_hmm_file runs it (map.c:1184-1196): the seeds of
- * mp_sketch_query (consensus and profile-derived, sorted and deduplicated, map.c:332-343)
- * when ki is NULL, else the anchors of mp_map_coarse's seeding steps (map.c:565-572) */
+ * consensus the query and its name the query name, as mp_map_hmm_file runs it
+ * (map.c:1184-1196): the seeds of mp_sketch_query (consensus and profile-derived, sorted
+ * and deduplicated, map.c:332-343) when ki is NULL, else the anchors of mp_map_coarse's
+ * seeding steps (map.c:565-572), with the accuracy mode's repeat rescue when
+ * repeat_cap > 0 */
 __attribute__((visibility("default")))
 int64_t ref_seed_hmm_query(const char *hmm_path, const int64_t *ki, const uint32_t *kb, int64_t n_kb, int32_t kmer,
-		int32_t mod_bit, int32_t max_occ_opt, int32_t pos_loss, int32_t win_loss, int32_t seed_max, uint64_t **out)
+		int32_t mod_bit, int32_t max_occ_opt, int32_t repeat_cap, int64_t anchor_budget, int32_t pos_loss,
+		int32_t win_loss, int32_t seed_max, uint64_t **out)
 {
 	mp_idx_t mi;
 	mp_mapopt_t opt;
@@ -105,6 +108,10 @@ int64_t ref_seed_hmm_query(const char *hmm_path, const int64_t *ki, const uint32
 	mp_mapopt_init(&opt);
 	opt.hmm = h, opt.max_occ = max_occ_opt;
 	opt.hmm_seed_pos_loss = pos_loss, opt.hmm_seed_win_loss = win_loss;
+	if (repeat_cap > 0) {
+		opt.flag |= MP_F_ACCURACY, opt.acc_flags |= MP_ACC_REPEAT_RESCUE;
+		opt.acc_repeat_cap = repeat_cap, opt.acc_anchor_budget = anchor_budget;
+	}
 	mp_sketch_query(0, &opt, cons, qlen, kmer, mod_bit, seed_max, &sd);
 	if (!ki) {
 		mp_hmm_destroy(h);

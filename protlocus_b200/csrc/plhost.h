@@ -71,6 +71,7 @@ struct pl_engine_s {
 	/* seeding (plseed.c) */
 	dbuf_t s_seq, s_off, s_len, s_seed, s_cnt, s_nseed, s_cap, s_nanc, s_aoff, s_anc, s_anc2, s_tmp;
 	dbuf_t s_take, s_send, s_seed2, s_qh;
+	dbuf_t s_soff, s_emit, s_eoff, s_elen, s_alts;  /* HMM-profile queries' seed slots and profiles */
 	int64_t r_last_cells;
 	/* learned-prefilter features */
 	dbuf_t pf_cand, pf_feats, pf_chain, pf_out;

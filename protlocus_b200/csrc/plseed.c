@@ -6,9 +6,9 @@
  * pl_seed_index_create.  A batch takes proteins (letters or residue codes 0-21) and
  * returns, per protein, its anchors (block << 32 | position) sorted ascending, as
  * mp_collect_anchors and the following radix sort leave them, with the accuracy mode's
- * repeat rescue (map.c:360-384) when asked (pl_seed_anchors_opt_host).  The
- * profile-derived seeds of mp_sketch_hmm are not done here: a caller with a profile keeps
- * the reference's path.
+ * repeat rescue (map.c:360-384) when asked (pl_seed_anchors_opt_host), and for
+ * HMM-profile queries (pl_seed_anchors_hmm_host: the profile-derived seeds of
+ * mp_sketch_hmm merged with the query's own, map.c:332-343).
  */
 #define _POSIX_C_SOURCE 200809L
 #include <stdio.h>
@@ -16,6 +16,7 @@
 #include <string.h>
 #include <stdint.h>
 #include "plhost.h"
+#include "seed_hmm.cuh"
 
 struct pl_seed_index_s {
 	int device;
@@ -67,6 +68,7 @@ void pl_seed_engine_free(pl_engine_t *e)
 	dbuf_free(&e->s_nseed), dbuf_free(&e->s_cap), dbuf_free(&e->s_nanc), dbuf_free(&e->s_aoff);
 	dbuf_free(&e->s_anc), dbuf_free(&e->s_anc2), dbuf_free(&e->s_tmp);
 	dbuf_free(&e->s_take), dbuf_free(&e->s_send), dbuf_free(&e->s_seed2), dbuf_free(&e->s_qh);
+	dbuf_free(&e->s_soff), dbuf_free(&e->s_emit), dbuf_free(&e->s_eoff), dbuf_free(&e->s_elen), dbuf_free(&e->s_alts);
 }
 
 PL_EXPORT uint32_t pl_seed_qname_hash(const char *qname)
@@ -77,22 +79,49 @@ PL_EXPORT uint32_t pl_seed_qname_hash(const char *qname)
 	return h;
 }
 
-/* the batch's anchors: into the host array a (when they fit a_cap), or left on the device
- * (a_dev != 0: *a_dev at the engine's sorted array) */
-static int64_t pl_seed_run(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq, int64_t seq_len,
-		const int64_t *off, const int32_t *len, const pl_seed_opt_t *o, int64_t *a_off, uint64_t *a, int64_t a_cap,
-		const uint64_t **a_dev)
+/* the seed slots of an HMM-profile batch: protein q's from soff[q], its own seeds (at most
+ * len[q]) and at most min(seed_max, 4^kmer) per window of its profile (a window has no
+ * more distinct k-mers); soff[n] the total, or -1 with the error set */
+static int64_t pl_seed_hmm_slots(int32_t n, const int32_t *len, const pl_seed_hmm_t *h, int32_t kmer, int64_t *soff)
 {
-	const int rescue = o && o->repeat_cap > 0;
+	const int64_t per_win = h->seed_max < ((int64_t)1 << (2 * kmer)) ? h->seed_max : (int64_t)1 << (2 * kmer);
+	int64_t t = 0;
+	int32_t q;
+	for (q = 0; q < n; ++q) {
+		if (h->e_len[q] < 0 || h->e_off[q] < 0 || h->e_off[q] + h->e_len[q] > h->n_state) {
+			pl_set_error("protein %d: profile of %d states at %lld of %lld", q, h->e_len[q], (long long)h->e_off[q],
+					(long long)h->n_state);
+			return -1;
+		}
+		soff[q] = t;
+		t += len[q] + (h->e_len[q] >= kmer ? (int64_t)(h->e_len[q] - kmer + 1) * per_win : 0);
+		if (t > INT32_MAX) {  /* the segmented sorts count items in an int */
+			pl_set_error("seed batch with room for %lld seeds at protein %d: at most %d per call, split the batch",
+					(long long)t, q, INT32_MAX);
+			return -1;
+		}
+	}
+	soff[n] = t;
+	return t;
+}
+
+/* the batch's anchors: into the host array a (when they fit a_cap), or left on the device
+ * (a_dev != 0: *a_dev at the engine's sorted array); h with seed_max > 0: HMM-profile queries */
+static int64_t pl_seed_run(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq, int64_t seq_len,
+		const int64_t *off, const int32_t *len, const pl_seed_opt_t *o, const pl_seed_hmm_t *h, int64_t *a_off,
+		uint64_t *a, int64_t a_cap, const uint64_t **a_dev)
+{
+	const int rescue = o && o->repeat_cap > 0, hmm = h && h->seed_max > 0;
 	const int32_t max_occ = o ? o->max_occ : 0;
 	plk_seed_args_t A;
-	int64_t *na = 0, total = 0, ret = -1;
+	int64_t *na = 0, *soff = 0, total = 0, ret = -1, n_slot;
 	int32_t q;
 	size_t tmp_bytes = 0;
 	cudaStream_t st;
 	if (!e || !x) { pl_set_error("no engine or index"); return -1; }
 	if (x->device != e->device) { pl_set_error("seed index on device %d, engine on %d", x->device, e->device); return -1; }
-	if (n < 0 || !o || !a_off || (n > 0 && (!seq || !off || !len)) || (rescue && (o->anchor_budget < 0 || !o->qname_hash))) {
+	if (n < 0 || !o || !a_off || (n > 0 && (!seq || !off || !len)) || (rescue && (o->anchor_budget < 0 || !o->qname_hash)) ||
+			(hmm && (h->n_state < 0 || (h->n_state > 0 && !h->emit) || (n > 0 && (!h->e_off || !h->e_len))))) {
 		pl_set_error("seed batch: bad arguments");
 		return -1;
 	}
@@ -107,26 +136,48 @@ static int64_t pl_seed_run(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, 
 			pl_set_error("protein %d: length %d at %lld of %lld", q, len[q], (long long)off[q], (long long)seq_len);
 			return -1;
 		}
+	n_slot = seq_len;
+	if (hmm) {
+		soff = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n + 1));
+		if (!soff) { pl_set_error("out of host memory"); return -1; }
+		if ((n_slot = pl_seed_hmm_slots(n, len, h, x->kmer, soff)) < 0) { free(soff); return -1; }
+	}
 	st = e->stream;
 	CK(cudaSetDevice(e->device));
 	na = (int64_t*)malloc(sizeof(int64_t) * (size_t)n);
-	if (!na) { pl_set_error("out of host memory"); return -1; }
+	if (!na) { pl_set_error("out of host memory"); free(soff); return -1; }
 	if (!dbuf_ensure(&e->s_seq, (size_t)(seq_len > 0 ? seq_len : 1)) || !dbuf_ensure(&e->s_off, sizeof(int64_t) * (size_t)n) ||
 			!dbuf_ensure(&e->s_len, sizeof(int32_t) * (size_t)n) ||
-			!dbuf_ensure(&e->s_seed, sizeof(uint64_t) * (size_t)(seq_len > 0 ? seq_len : 1)) ||
-			!dbuf_ensure(&e->s_cnt, sizeof(uint32_t) * (size_t)(seq_len > 0 ? seq_len : 1)) ||
+			!dbuf_ensure(&e->s_seed, sizeof(uint64_t) * (size_t)(n_slot > 0 ? n_slot : 1)) ||
+			!dbuf_ensure(&e->s_cnt, sizeof(uint32_t) * (size_t)(n_slot > 0 ? n_slot : 1)) ||
 			!dbuf_ensure(&e->s_nseed, sizeof(int32_t) * (size_t)n) || !dbuf_ensure(&e->s_cap, sizeof(int32_t) * (size_t)n) ||
 			!dbuf_ensure(&e->s_nanc, sizeof(int64_t) * (size_t)n) || !dbuf_ensure(&e->s_aoff, sizeof(int64_t) * (size_t)(n + 1)) ||
-			!dbuf_ensure(&e->s_take, sizeof(int32_t) * (size_t)(seq_len > 0 ? seq_len : 1)) ||
+			!dbuf_ensure(&e->s_take, sizeof(int32_t) * (size_t)(n_slot > 0 ? n_slot : 1)) ||
 			!dbuf_ensure(&e->s_send, sizeof(int64_t) * (size_t)n) ||
-			(rescue && (!dbuf_ensure(&e->s_seed2, sizeof(uint64_t) * (size_t)(seq_len > 0 ? seq_len : 1)) ||
-			            !dbuf_ensure(&e->s_qh, sizeof(uint32_t) * (size_t)n))))
+			((rescue || hmm) && !dbuf_ensure(&e->s_seed2, sizeof(uint64_t) * (size_t)(n_slot > 0 ? n_slot : 1))) ||
+			(rescue && !dbuf_ensure(&e->s_qh, sizeof(uint32_t) * (size_t)n)) ||
+			(hmm && (!dbuf_ensure(&e->s_soff, sizeof(int64_t) * (size_t)(n + 1)) ||
+			         !dbuf_ensure(&e->s_emit, sizeof(int16_t) * 20 * (size_t)(h->n_state > 0 ? h->n_state : 1)) ||
+			         !dbuf_ensure(&e->s_eoff, sizeof(int64_t) * (size_t)n) || !dbuf_ensure(&e->s_elen, sizeof(int32_t) * (size_t)n) ||
+			         !dbuf_ensure(&e->s_alts, sizeof(sh_alts_t) * (size_t)(h->n_state > 0 ? h->n_state : 1)))))
 		goto fail;
 	if (seq_len > 0) CK(cudaMemcpyAsync(e->s_seq.p, seq, (size_t)seq_len, cudaMemcpyHostToDevice, st));
 	CK(cudaMemcpyAsync(e->s_off.p, off, sizeof(int64_t) * (size_t)n, cudaMemcpyHostToDevice, st));
 	CK(cudaMemcpyAsync(e->s_len.p, len, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
 	memset(&A, 0, sizeof(A));
 	A.seq = (const uint8_t*)e->s_seq.p, A.off = (const int64_t*)e->s_off.p, A.len = (const int32_t*)e->s_len.p, A.n = n;
+	A.soff = A.off;  /* the default slots: one per residue */
+	if (hmm) {
+		CK(cudaMemcpyAsync(e->s_soff.p, soff, sizeof(int64_t) * (size_t)(n + 1), cudaMemcpyHostToDevice, st));
+		if (h->n_state > 0)
+			CK(cudaMemcpyAsync(e->s_emit.p, h->emit, sizeof(int16_t) * 20 * (size_t)h->n_state, cudaMemcpyHostToDevice, st));
+		CK(cudaMemcpyAsync(e->s_eoff.p, h->e_off, sizeof(int64_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+		CK(cudaMemcpyAsync(e->s_elen.p, h->e_len, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+		A.soff = (const int64_t*)e->s_soff.p;
+		A.emit = (const int16_t*)e->s_emit.p, A.n_state = h->n_state;
+		A.e_off = (const int64_t*)e->s_eoff.p, A.e_len = (const int32_t*)e->s_elen.p, A.alts = e->s_alts.p;
+		A.pos_loss = h->pos_loss, A.win_loss = h->win_loss, A.seed_max = h->seed_max;
+	}
 	A.ki = x->ki, A.n_bucket = x->n_bucket, A.kb = x->kb, A.n_kb = x->n_kb;
 	A.kmer = x->kmer, A.mod_bit = x->mod_bit, A.max_occ = max_occ;
 	A.repeat_cap = rescue ? o->repeat_cap : 0, A.budget = rescue ? o->anchor_budget : 0;
@@ -139,8 +190,18 @@ static int64_t pl_seed_run(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, 
 	}
 	e->n_ev = 0;
 	PL_TIME(e, st, 1);
+	if (hmm) CKK(plk_seed_hmm_alts(&A, st));
 	CKK(plk_seed_sketch(&A, st));
-	if (rescue) { /* the rescue hands its budget out over the seeds in mp_sketch_query's sorted order */
+	if (hmm) {  /* the profile's seeds after the query's own, then sorted without duplicates */
+		size_t tb = 0;
+		CKK(plk_seed_hmm_enum(&A, st));
+		CKK(plk_seed_sort((const uint64_t*)e->s_seed.p, (uint64_t*)e->s_seed2.p, n_slot, n, A.soff,
+				(const int64_t*)e->s_send.p, 0, &tb, st));
+		if (!dbuf_ensure(&e->s_tmp, tb > 0 ? tb : 16)) goto fail;
+		CKK(plk_seed_sort((const uint64_t*)e->s_seed.p, (uint64_t*)e->s_seed2.p, n_slot, n, A.soff,
+				(const int64_t*)e->s_send.p, e->s_tmp.p, &tb, st));
+		CKK(plk_seed_unique(&A, (const uint64_t*)e->s_seed2.p, st));
+	} else if (rescue) { /* the rescue hands its budget out over the seeds in mp_sketch_query's sorted order */
 		size_t tb = 0;
 		CKK(plk_seed_sort((const uint64_t*)e->s_seed.p, (uint64_t*)e->s_seed2.p, seq_len, n, (const int64_t*)e->s_off.p,
 				(const int64_t*)e->s_send.p, 0, &tb, st));
@@ -186,10 +247,10 @@ done:
 		}
 		e->acc_dp_launches += e->n_ev / 2;
 	}
-	free(na);
+	free(na), free(soff);
 	return ret;
 fail:
-	free(na);
+	free(na), free(soff);
 	return -1;
 }
 
@@ -197,7 +258,7 @@ PL_EXPORT int64_t pl_seed_anchors_opt_host(pl_engine_t *e, const pl_seed_index_t
 		int64_t seq_len, const int64_t *off, const int32_t *len, const pl_seed_opt_t *o, int64_t *a_off, uint64_t *a,
 		int64_t a_cap)
 {
-	return pl_seed_run(e, x, n, seq, seq_len, off, len, o, a_off, a, a_cap, 0);
+	return pl_seed_run(e, x, n, seq, seq_len, off, len, o, 0, a_off, a, a_cap, 0);
 }
 
 PL_EXPORT int64_t pl_seed_anchors_opt_device(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
@@ -205,7 +266,23 @@ PL_EXPORT int64_t pl_seed_anchors_opt_device(pl_engine_t *e, const pl_seed_index
 		const uint64_t **a_dev)
 {
 	if (!a_dev) { pl_set_error("seed batch: no output pointer"); return -1; }
-	return pl_seed_run(e, x, n, seq, seq_len, off, len, o, a_off, 0, 0, a_dev);
+	return pl_seed_run(e, x, n, seq, seq_len, off, len, o, 0, a_off, 0, 0, a_dev);
+}
+
+PL_EXPORT int64_t pl_seed_anchors_hmm_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
+		int64_t seq_len, const int64_t *off, const int32_t *len, const pl_seed_opt_t *o, const pl_seed_hmm_t *h,
+		int64_t *a_off, uint64_t *a, int64_t a_cap)
+{
+	if (!h) { pl_set_error("seed batch: no profiles"); return -1; }
+	return pl_seed_run(e, x, n, seq, seq_len, off, len, o, h, a_off, a, a_cap, 0);
+}
+
+PL_EXPORT int64_t pl_seed_anchors_hmm_device(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,
+		int64_t seq_len, const int64_t *off, const int32_t *len, const pl_seed_opt_t *o, const pl_seed_hmm_t *h,
+		int64_t *a_off, const uint64_t **a_dev)
+{
+	if (!h || !a_dev) { pl_set_error("seed batch: no profiles or no output pointer"); return -1; }
+	return pl_seed_run(e, x, n, seq, seq_len, off, len, o, h, a_off, 0, 0, a_dev);
 }
 
 PL_EXPORT int64_t pl_seed_anchors_host(pl_engine_t *e, const pl_seed_index_t *x, int32_t n, const uint8_t *seq,

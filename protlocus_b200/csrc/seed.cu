@@ -14,6 +14,11 @@
  *                  select) and the anchor count.
  *   k_seed_emit    one warp per protein: 32 seeds at a time, their kept buckets laid out by
  *                  a warp scan, the lanes copy the blocks as block << 32 | position.
+ * HMM-profile queries (the query the profile's consensus, mp_sketch_query with a profile,
+ * map.c:332-343) add the profile-derived seeds of mp_sketch_hmm (sketch.c:40-118) before
+ * the cap: k_seed_hmm_alts (a thread per match state: its offered groups), k_seed_hmm_enum
+ * (a warp per protein, a lane per window: the seeds appended after the protein's own), a
+ * segmented sort and k_seed_unique (duplicates removed, then the cap as in the sketch).
  * The anchors of each protein are then sorted (cub::DeviceSegmentedSort, ascending 64-bit
  * keys: equal keys are equal values, so any sort leaves the reference's array).
  */
@@ -21,6 +26,7 @@
 #include <stdint.h>
 #include <cub/cub.cuh>
 #include "plk.h"
+#include "seed_hmm.cuh"
 
 extern "C" void plk_add_launches(uint64_t n);
 
@@ -238,7 +244,104 @@ __global__ void __launch_bounds__(32 * SD_EMIT_WARPS) k_seed_emit(plk_seed_args_
 	}
 }
 
+/* HMM-profile queries: one thread per match state, its offered groups (seed_hmm.cuh) */
+__global__ void __launch_bounds__(256) k_seed_hmm_alts(plk_seed_args_t A)
+{
+	const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= A.n_state) return;
+	((sh_alts_t*)A.alts)[s] = sh_state_alts(A.emit + s * 20, A.pos_loss);
+}
+
+/* one warp per protein, 32 windows of its profile at a time: each lane counts its window's
+ * seeds, a warp scan places them after the protein's own seeds (the sketch's), and the lane
+ * walks its window again to write them.  The protein's slots hold its own seeds (at most
+ * len) and at most min(seed_max, 4^kmer) per window */
+__global__ void __launch_bounds__(256) k_seed_hmm_enum(plk_seed_args_t A)
+{
+	const int lane = threadIdx.x & 31;
+	const int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	if (q >= A.n) return;  /* whole warps */
+	const int32_t kmer = A.kmer, el = A.e_len[q], mx = A.seed_max;
+	const int32_t n_win = mx > 0 && el >= kmer ? el - kmer + 1 : 0;
+	const sh_alts_t *al = (const sh_alts_t*)A.alts + A.e_off[q];
+	const int32_t n0 = A.n_seed[q];
+	uint64_t *out = A.seeds + A.soff[q] + n0;
+	int64_t k = 0;
+	for (int32_t w0 = 0; w0 < n_win; w0 += 32) {
+		const int32_t w = w0 + lane;
+		int64_t c = 0;
+		if (w < n_win) c = sh_window_seeds(al + w, kmer, A.mod_bit, A.win_loss, mx, w + kmer - 1, 0);
+		int64_t inc = c;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const int64_t t = __shfl_up_sync(0xffffffffu, inc, o);
+			if (lane >= o) inc += t;
+		}
+		if (c > 0) sh_window_seeds(al + w, kmer, A.mod_bit, A.win_loss, mx, w + kmer - 1, out + k + inc - c);
+		k += __shfl_sync(0xffffffffu, inc, 31);
+	}
+	__syncwarp();
+	if (lane == 0) A.n_seed[q] = n0 + (int32_t)k, A.seed_end[q] = A.soff[q] + n0 + k;
+}
+
+/* one warp per protein: its seeds, sorted (sorted + soff, n_seed of them), without
+ * duplicates into its slots (mp_sketch_query with a profile, map.c:338-342), their bucket
+ * sizes, and the cap over them (sd_finish) */
+__global__ void __launch_bounds__(256) k_seed_unique(plk_seed_args_t A, const uint64_t *sorted)
+{
+	const int lane = threadIdx.x & 31;
+	const int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	if (q >= A.n) return;  /* whole warps */
+	const int64_t base = A.soff[q];
+	const int32_t n_in = A.n_seed[q];
+	const uint64_t *in = sorted + base;
+	uint64_t *sd = A.seeds + base;
+	uint32_t *cnt = A.cnt + base;
+	int32_t n = 0;
+	uint64_t last = 0;
+	for (int32_t j0 = 0; j0 < n_in; j0 += 32) {
+		const int32_t j = j0 + lane;
+		const uint64_t v = j < n_in ? in[j] : 0;
+		uint64_t prev = __shfl_up_sync(0xffffffffu, v, 1);
+		if (lane == 0) prev = last;
+		const bool keep = j < n_in && (j == 0 || v != prev);
+		const unsigned bal = __ballot_sync(0xffffffffu, keep);
+		if (keep) {
+			const int32_t t = n + __popc(bal & ((1u << lane) - 1));
+			sd[t] = v;
+			cnt[t] = (uint32_t)sd_bucket_size(A.ki, A.n_bucket, A.n_kb, (int64_t)(v >> 32));
+		}
+		n += __popc(bal);
+		last = __shfl_sync(0xffffffffu, v, 31);
+	}
+	sd_finish(A, q, cnt, n, lane);
+}
+
 }  // namespace
+
+extern "C" int plk_seed_hmm_alts(const plk_seed_args_t *a, void *stream)
+{
+	if (a->n_state <= 0) return 0;
+	k_seed_hmm_alts<<<(unsigned)((a->n_state + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*a);
+	plk_add_launches(1);
+	return (int)cudaGetLastError();
+}
+
+extern "C" int plk_seed_hmm_enum(const plk_seed_args_t *a, void *stream)
+{
+	if (a->n <= 0) return 0;
+	k_seed_hmm_enum<<<(unsigned)((a->n * 32 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*a);
+	plk_add_launches(1);
+	return (int)cudaGetLastError();
+}
+
+extern "C" int plk_seed_unique(const plk_seed_args_t *a, const uint64_t *sorted, void *stream)
+{
+	if (a->n <= 0) return 0;
+	k_seed_unique<<<(unsigned)((a->n * 32 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*a, sorted);
+	plk_add_launches(1);
+	return (int)cudaGetLastError();
+}
 
 extern "C" int plk_seed_sketch(const plk_seed_args_t *a, void *stream)
 {

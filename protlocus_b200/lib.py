@@ -149,6 +149,14 @@ def load() -> C.CDLL:
     lib.pl_seed_anchors_opt_device.restype = C.c_int64
     lib.pl_seed_qname_hash.argtypes = [C.c_char_p]
     lib.pl_seed_qname_hash.restype = C.c_uint32
+    lib.pl_seed_anchors_hmm_host.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
+                                             C.c_void_p, C.POINTER(SeedOpt), C.POINTER(SeedHmm), C.c_void_p,
+                                             C.c_void_p, C.c_int64]
+    lib.pl_seed_anchors_hmm_host.restype = C.c_int64
+    lib.pl_seed_anchors_hmm_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
+                                               C.c_void_p, C.POINTER(SeedOpt), C.POINTER(SeedHmm), C.c_void_p,
+                                               C.POINTER(C.c_void_p)]
+    lib.pl_seed_anchors_hmm_device.restype = C.c_int64
     lib.pl_pf_decide.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_double, C.c_int32,
                                  C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.pl_pf_decide.restype = C.c_int
@@ -631,6 +639,12 @@ class SeedOpt(C.Structure):
                 ("qname_hash", C.c_void_p)]
 
 
+class SeedHmm(C.Structure):
+    """pl_seed_hmm_t"""
+    _fields_ = [("emit", C.c_void_p), ("n_state", C.c_int64), ("e_off", C.c_void_p), ("e_len", C.c_void_p),
+                ("pos_loss", C.c_int32), ("win_loss", C.c_int32), ("seed_max", C.c_int32), ("pad", C.c_int32)]
+
+
 class SeedIndex:
     """A pl_seed_index_t: the mapper's k-mer index (ki int64 bucket starts, kb uint32 block ids) on a device."""
 
@@ -648,10 +662,26 @@ class SeedIndex:
             self.h = None
 
 
-def seed_anchors(eng, index: SeedIndex, proteins, max_occ: int, repeat_cap: int = 0, budget: int = 0, names=None):
+def seed_anchors(eng, index: SeedIndex, proteins, max_occ: int, repeat_cap: int = 0, budget: int = 0, names=None,
+                 profiles=None, pos_loss: int = 6, win_loss: int = 8, seed_max: int = 16):
     """Anchors of a list of proteins (bytes) through pl_seed_anchors_opt_host: a list of sorted uint64 arrays.
-    repeat_cap > 0: the accuracy mode's repeat rescue, with the proteins' names (bytes)."""
+    repeat_cap > 0: the accuracy mode's repeat rescue, with the proteins' names (bytes).
+    profiles: per protein its profile's match emissions (m x 20 int16, HMMER column order), the
+    proteins their consensus: HMM-profile queries through pl_seed_anchors_hmm_host, with the
+    profile-derived seeds' options (hmm_seed_pos_loss, hmm_seed_win_loss, hmm_seed_max)."""
     n = len(proteins)
+    hmm = None
+    if profiles is not None:
+        if len(profiles) != n:
+            raise ValueError("one profile per protein")
+        tabs = [np.ascontiguousarray(e, dtype=np.int16).reshape(-1, 20) for e in profiles]
+        e_len = np.array([t.shape[0] for t in tabs], dtype=np.int32)
+        e_off = np.zeros(n, dtype=np.int64)
+        if n > 1:
+            e_off[1:] = np.cumsum(e_len[:-1])
+        emit = np.ascontiguousarray(np.concatenate(tabs) if n and e_len.sum() else np.zeros((1, 20), np.int16))
+        hmm = SeedHmm(emit.ctypes.data, int(e_len.sum()), e_off.ctypes.data, e_len.ctypes.data, pos_loss, win_loss,
+                      seed_max, 0)
     qh = np.array([eng.lib.pl_seed_qname_hash(nm) for nm in (names or [b""] * n)], dtype=np.uint32)
     opt = SeedOpt(max_occ, repeat_cap, budget, qh.ctypes.data if n else None)
     lens = np.array([len(p) for p in proteins], dtype=np.int32)
@@ -664,8 +694,14 @@ def seed_anchors(eng, index: SeedIndex, proteins, max_occ: int, repeat_cap: int 
     cap = 1 << 20
     for _ in range(2):
         a = np.zeros(max(cap, 1), dtype=np.uint64)
-        tot = eng.lib.pl_seed_anchors_opt_host(eng.h, index.h, n, seq.ctypes.data, int(lens.sum()), offs.ctypes.data,
-                                               lens.ctypes.data, C.byref(opt), a_off.ctypes.data, a.ctypes.data, cap)
+        if hmm is None:
+            tot = eng.lib.pl_seed_anchors_opt_host(eng.h, index.h, n, seq.ctypes.data, int(lens.sum()),
+                                                   offs.ctypes.data, lens.ctypes.data, C.byref(opt),
+                                                   a_off.ctypes.data, a.ctypes.data, cap)
+        else:
+            tot = eng.lib.pl_seed_anchors_hmm_host(eng.h, index.h, n, seq.ctypes.data, int(lens.sum()),
+                                                   offs.ctypes.data, lens.ctypes.data, C.byref(opt), C.byref(hmm),
+                                                   a_off.ctypes.data, a.ctypes.data, cap)
         if tot < 0:
             raise RuntimeError("pl_seed_anchors_host: " + error())
         if tot <= cap:

@@ -543,34 +543,35 @@ def seeds_hmm_query(seq: bytes, emit, kmer: int, mod_bit: int, pos_loss: int, wi
 
 
 def anchors_hmm(ki, kb, kmer: int, mod_bit: int, max_occ: int, seq: bytes, emit, pos_loss: int, win_loss: int,
-                seed_max: int):
-    """The anchors of an HMM-profile query (seeds_hmm_query, then the default cap and
-    collection), from the restatement."""
+                seed_max: int, repeat_cap: int = 0, budget: int = 0, qname: bytes = b""):
+    """The anchors of an HMM-profile query (seeds_hmm_query, then the cap and the collection,
+    with the repeat rescue for a query named qname when repeat_cap > 0), from the restatement."""
     e = _i16p(emit).reshape(-1, 20)
     p = _seed_port()
     p.sp_anchors_hmm.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
-                                 C.c_char_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
-                                 C.POINTER(C.POINTER(C.c_uint64))]
+                                 C.c_int32, C.c_int64, C.c_uint32, C.c_char_p, C.c_int32, C.c_void_p, C.c_int32,
+                                 C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.POINTER(C.c_uint64))]
     p.sp_anchors_hmm.restype = C.c_int64
     return _seed_take(p.sp_anchors_hmm, p.sp_free, ki.ctypes.data, ki.size, kb.ctypes.data, kb.size, kmer, mod_bit,
-                      max_occ, seq, len(seq), e.ctypes.data, e.shape[0], pos_loss, win_loss, seed_max)
+                      max_occ, repeat_cap, budget, seed_qname_hash(qname), seq, len(seq), e.ctypes.data, e.shape[0],
+                      pos_loss, win_loss, seed_max)
 
 
 def ref_hmm_query(path: str, kmer: int, mod_bit: int, pos_loss: int, win_loss: int, seed_max: int,
-                  ki=None, kb=None, max_occ: int = 20000):
-    """The reference on an HMMER3 file: its parser, the consensus as the query, and
-    mp_sketch_query's seeds (ki None) or mp_map_coarse's anchors; None when
-    oracle/_ref/libseed_ref.so is not built."""
+                  ki=None, kb=None, max_occ: int = 20000, repeat_cap: int = 0, budget: int = 0):
+    """The reference on an HMMER3 file: its parser, the consensus as the query (the profile's
+    name its name), and mp_sketch_query's seeds (ki None) or mp_map_coarse's anchors (with the
+    repeat rescue when repeat_cap > 0); None when oracle/_ref/libseed_ref.so is not built."""
     lib = seed_ref_lib()
     if lib is None:
         return None
     f = lib.ref_seed_hmm_query
     f.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
-                  C.c_int32, C.c_int32, C.POINTER(C.POINTER(C.c_uint64))]
+                  C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.POINTER(C.c_uint64))]
     f.restype = C.c_int64
     return _seed_take(f, lib.ref_seed_free, path.encode(), None if ki is None else ki.ctypes.data,
                       None if kb is None else kb.ctypes.data, 0 if kb is None else kb.size, kmer, mod_bit, max_occ,
-                      pos_loss, win_loss, seed_max)
+                      repeat_cap, budget, pos_loss, win_loss, seed_max)
 
 
 def ref_hmm_tables(path: str):

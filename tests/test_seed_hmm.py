@@ -244,3 +244,23 @@ def test_sketch_hmm_losses_past_16_bits(kind):
                 assert np.array_equal(ref, port), (kind, kmer, mod_bit, pos_loss, win_loss, mx, n, ref.size, port.size)
             total += port.size
     assert total > 0
+
+
+@need_ref
+@pytest.mark.parametrize("cap,budget", [(5, 7), (64, 300), (20, 0)])
+def test_hmm_query_rescue_equals_reference(tmp_path, cap, budget):
+    """An HMM-profile query with the accuracy mode's repeat rescue (map.c:360-384): the budget
+    handed out over the merged seeds in their sorted order, from the hash of the query's name
+    (the profile's name, as mp_map_hmm_file names the query); an index with 5 % repeat buckets."""
+    from protlocus_b200.hmm import parse_hmmer3
+    rng = np.random.default_rng(501 + cap)
+    ki, kb = O.seed_index(rng, kmer=6, mod_bit=1, mean_occ=2.0, n_block=50_000, hot=1 << 15, hot_occ=300)
+    for path in _profiles(tmp_path, 5, 503 + cap):
+        cons, emit = O.ref_hmm_tables(path)
+        name = parse_hmmer3(open(path).read())[0]["name"].encode()
+        for pos_loss, win_loss, mx in [(6, 8, 16), (12, 20, 64)]:
+            ref = O.ref_hmm_query(path, 6, 1, pos_loss, win_loss, mx, ki=ki, kb=kb, max_occ=20, repeat_cap=cap,
+                                  budget=budget)
+            port = O.anchors_hmm(ki, kb, 6, 1, 20, cons, emit, pos_loss, win_loss, mx, repeat_cap=cap, budget=budget,
+                                 qname=name)
+            assert np.array_equal(ref, port), (path, cap, budget, mx, ref.size, port.size)
