@@ -34,7 +34,7 @@ def _device_u64(ptr: int, n: int) -> np.ndarray:
     import torch
 
     class _View:
-        __cuda_array_interface__ = {"shape": (n,), "typestr": "<i8", "data": (ptr, True), "version": 2}
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "<i8", "data": (ptr, False), "version": 2}
     return torch.as_tensor(_View(), device="cuda").cpu().numpy().view(np.uint64)
 
 
