@@ -83,13 +83,14 @@ def parse():
                     help="keep the engine's default tuning instead of autotuning it on the workload (global DP)")
     ap.add_argument("--workload", default="global",
                     choices=["global", "ext", "hmm", "gapless", "forward", "prefilter", "extra", "prescreen", "chain",
-                             "seed", "refgpu"],
+                             "seed", "seed_hmm", "refgpu"],
                     help="global: the batched global spliced DP (headline); ext: the batched extension DP; "
                          "hmm: the integer profile-HMM DP; gapless: the gapless X-drop prefilter; "
                          "forward: the recheck Forward score; prefilter: learned candidate prefilter vs the plain "
                          "batched DP over the held-out seed's candidates; extra: alignment statistics and exon "
                          "features from the CIGAR; prescreen: banded gapped profile-ORF alignment; chain: anchor "
-                         "chaining (mp_chain) of the coarse mapping")
+                         "chaining (mp_chain) of the coarse mapping; seed: the coarse mapping's seeding of protein "
+                         "queries; seed_hmm: the same for HMM-profile queries (profile-derived seeds)")
     ap.add_argument("--peptides", type=int, default=20000, help="peptides per step (--workload forward)")
     ap.add_argument("--candidates", type=int, default=131072, help="candidates of 8 anchors (--workload gapless)")
     ap.add_argument("--profiles", type=int, default=16, help="profiles per step (--workload hmm)")
@@ -139,6 +140,16 @@ def pack(jobs):
     for q in range(n):
         tab[q].nt_off, tab[q].aa_off, tab[q].ss_off, tab[q].nl, tab[q].al = nt_off[q], aa_off[q], -1, nl[q], al[q]
     return nt, aa, nt_off, aa_off, nl, al, tab
+
+
+def hbm_peak():
+    """The HBM copy bandwidth (GB/s) a memory-bound line is measured against, and its source: the
+    pool's measured figure in MEASURED_PEAKS.json when that file is present, else the fallback."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback HBM copy bandwidth of this pool (6.65 TB/s)"
 
 
 class Clocks:
@@ -365,6 +376,8 @@ def main():
         return main_chain(args)
     if args.workload == "seed":
         return main_seed(args)
+    if args.workload == "seed_hmm":
+        return main_seed_hmm(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -1544,8 +1557,7 @@ def main_extra(args):
     nfeat = sum(r.n_feat for r, _ in res)
     # algorithmic bytes: the aligned codons' bases and residues, the CIGAR, the records in and out
     alg = int(sum(3 * a["qe"] + a["qe"] for a in alns) + 4 * ncig + 80 * n + 56 * nfeat)
-    peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]) \
-        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    peak, _ = hbm_peak()
     cpu = None
     if R.is_root:
         k = min(n, 2000)
@@ -1695,13 +1707,30 @@ def seed_workload(seed: int):
     for L_ in lens:
         prots.append(seq[o:o + L_].tobytes())
         o += int(L_)
+    ki, kb = seed_index_100mb(rng)
+    return prots, ki, kb
+
+
+def seed_index_100mb(rng):
+    """The synthetic 100 Mb genome index of seed_workload (ki bucket starts, kb block ids)."""
     n_bucket = 1 << 23
     cnt = rng.poisson(12.0, size=n_bucket).astype(np.int64)
     cnt[rng.choice(n_bucket, size=256, replace=False)] = rng.integers(10000, 30000, size=256)
     ki = np.zeros(n_bucket, dtype=np.int64)
     ki[1:] = np.cumsum(cnt[:-1])
     kb = rng.integers(0, (100_000_000 >> 8) * 2, size=int(cnt.sum()), dtype=np.uint32)
-    return prots, ki, kb
+    return ki, kb
+
+
+def seed_hmm_workload(seed: int):
+    """1000 synthetic Plan7 profiles (50-800 match states, protlocus_b200.hmm.synthetic_profiles) as
+    HMM-profile queries (each the consensus of its profile with its match emissions) against the index of
+    seed_workload; the HMMER3 texts for the reference arm."""
+    from protlocus_b200.hmm import consensus, parse_hmmer3, synthetic_profiles
+    texts, _ = synthetic_profiles(1000, seed=seed, m_min=50, m_max=800)
+    emits = [parse_hmmer3(t)[0]["emit"] for t in texts]
+    ki, kb = seed_index_100mb(np.random.default_rng(seed + 1))
+    return texts, [consensus(e) for e in emits], emits, ki, kb
 
 
 def main_seed(args):
@@ -1800,6 +1829,7 @@ def main_seed(args):
     k_s = R.max(tm["dp_ms"] / 1e3 / args.steps)
     value = R.sum(int(tot)) / k_s
     r = cpu_sample(args.cpu_seconds / 2) if R.is_root else None
+    hbm = hbm_peak()
     if R.is_root:
         line = {"metric": metric, "value": round(value, 1), "unit": "anchors/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": round(k_s * 1e3, 3),
@@ -1813,8 +1843,8 @@ def main_seed(args):
                 "gpu_launches": int(launches),
                 "roofline": {"bound": "hbm", "kernel": "k_seed_emit + segmented sort",
                              "achieved": round(int(tot) * SEED_BYTES_PER_ANCHOR / k_s / 1e9, 2), "unit": "GB/s",
-                             "peak": 6650.0, "frac": round(int(tot) * SEED_BYTES_PER_ANCHOR / k_s / 1e9 / 6650.0, 4),
-                             "peak_source": "fallback HBM copy bandwidth of this pool (6.65 TB/s)", "traffic": None,
+                             "peak": hbm[0], "frac": round(int(tot) * SEED_BYTES_PER_ANCHOR / k_s / 1e9 / hbm[0], 4),
+                             "peak_source": hbm[1], "traffic": None,
                              "note": "algorithmic bytes: the anchor written and its block id read; the sort's passes "
                                      "and the per-protein sketch are on top"},
                 "clocks": clk}
@@ -1822,6 +1852,160 @@ def main_seed(args):
             line["cpu_baseline"] = {"value": round(r[0], 1), "unit": "anchors/s", "cores": threads, "kind": "reference",
                                     "sample": f"{r[1]} of {n} proteins, map.c's seeding steps per protein over a "
                                               "thread pool"}
+        print(json.dumps(line), flush=True)
+    idx.close()
+    eng.close()
+    R.close()
+    return 0
+
+
+def main_seed_hmm(args):
+    """One step = the seeding of 1000 HMM-profile queries (mp_map_hmm_file's query, the consensus, with
+    mp_sketch_query's profile-derived seeds at the defaults hmm_seed_pos_loss 6, hmm_seed_win_loss 8,
+    hmm_seed_max 16; then mp_cal_max_occ with max_occ 20000, mp_collect_anchors, the anchor sort) against a
+    100 Mb genome's index.  value: anchors/s of the device kernels (engine CUDA events); e2e:
+    pl_seed_anchors_hmm_host from host buffers (the consensus sequences and emission tables up, the
+    anchors back), wall clock."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    R = Ranks("nccl")
+    if args.impl == "reference" and not R.is_root:
+        R.close()
+        return 0
+    texts, prots, emits, ki, kb = seed_hmm_workload(R.seed(41))
+    max_occ, pos_loss, win_loss, seed_max = 20000, 6, 8, 16
+    desc = ("mp_map_coarse seeding of 1000 HMM-profile queries (synthetic Plan7 profiles of 50-800 match states; "
+            "the consensus's seeds and the profile-derived ones, pos_loss 6, win_loss 8, 16 per window; kmer 6 "
+            "mod_bit 1, occurrence cap, anchors, sort) against a synthetic 100 Mb genome index (2^23 buckets, "
+            "Poisson(12) blocks each, 256 repeat buckets)")
+    metric = "HMM-profile query seeding anchors/s (mp_sketch_query with a profile + anchors, bit-exact) at 1 B200"
+    threads = os.cpu_count() or 1
+
+    def cpu_sample(seconds):
+        from concurrent.futures import ThreadPoolExecutor
+        lib = O.seed_ref_lib()
+        if lib is None:
+            return None
+        lib.ref_hmm_load.argtypes, lib.ref_hmm_load.restype = [C.c_char_p], C.c_void_p
+        lib.ref_hmm_free.argtypes = [C.c_void_p]
+        f = lib.ref_seed_hmm_run
+        f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                      C.c_int32, C.c_int32, C.POINTER(C.POINTER(C.c_uint64))]
+        f.restype = C.c_int64
+        with tempfile.TemporaryDirectory() as tmp:  # the reference's parser reads files
+            hs = []
+            for q, t in enumerate(texts):
+                path = os.path.join(tmp, f"p{q}.hmm")
+                with open(path, "w") as fh:
+                    fh.write(t)
+                hs.append(lib.ref_hmm_load(path.encode()))
+
+        def one(h):
+            out = C.POINTER(C.c_uint64)()
+            m = f(h, ki.ctypes.data, kb.ctypes.data, kb.size, 6, 1, max_occ, pos_loss, win_loss, seed_max,
+                  C.byref(out))
+            lib.ref_seed_free(out)
+            return m
+        k, n_anc = 0, 0
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as ex:
+            while time.perf_counter() - t0 < seconds and k < len(hs):
+                chunk = hs[k:k + 4 * threads]
+                n_anc += sum(ex.map(one, chunk))
+                k += len(chunk)
+        secs = time.perf_counter() - t0
+        for h in hs:
+            lib.ref_hmm_free(h)
+        return n_anc / secs, k, secs
+
+    if args.impl == "reference":
+        r = cpu_sample(max(2.0, args.cpu_seconds))
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libseed_ref.so not built"}), flush=True)
+        else:
+            v, k, secs = r
+            print(json.dumps({"metric": metric, "value": round(v, 1), "unit": "anchors/s", "n_gpus": args.gpus,
+                              "steps": 1, "warmup": 0, "ms_per_step": round(secs * 1e3, 2), "higher_is_better": True,
+                              "scaling": "weak", "vs_baseline": None, "dtype": "uint64", "data": "synthetic",
+                              "impl": "reference", "config": {"workload": desc},
+                              "cpu_baseline": {"value": round(v, 1), "unit": "anchors/s", "cores": threads,
+                                               "kind": "reference", "sample": f"{k} of 1000 profiles, the reference's "
+                                               "seeding steps per parsed profile over a thread pool"},
+                              "e2e": {"value": round(v, 1), "unit": "anchors/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+        R.close()
+        return 0
+    eng = L.Engine(R.local)
+    idx = L.SeedIndex(ki, kb, 6, 1, R.local)
+    n = len(prots)
+    lens = np.array([len(p) for p in prots], dtype=np.int32)
+    offs = np.zeros(n, dtype=np.int64)
+    offs[1:] = np.cumsum(lens[:-1])
+    seq = np.frombuffer(b"".join(prots), dtype=np.uint8).copy()
+    e_len = np.array([e.shape[0] for e in emits], dtype=np.int32)
+    e_off = np.zeros(n, dtype=np.int64)
+    e_off[1:] = np.cumsum(e_len[:-1])
+    emit = np.ascontiguousarray(np.concatenate(emits).astype(np.int16))
+    hmm = L.SeedHmm(emit.ctypes.data, int(e_len.sum()), e_off.ctypes.data, e_len.ctypes.data, pos_loss, win_loss,
+                    seed_max, 0)
+    opt = L.SeedOpt(max_occ, 0, 0, None)
+    a_off = np.zeros(n + 1, dtype=np.int64)
+    tot = eng.lib.pl_seed_anchors_hmm_host(eng.h, idx.h, n, seq.ctypes.data, seq.size, offs.ctypes.data,
+                                           lens.ctypes.data, C.byref(opt), C.byref(hmm), a_off.ctypes.data, None, 0)
+    if tot < 0:
+        raise RuntimeError("pl_seed_anchors_hmm_host: " + L.error())
+    a = np.zeros(max(int(tot), 1), dtype=np.uint64)
+
+    def step():
+        r = eng.lib.pl_seed_anchors_hmm_host(eng.h, idx.h, n, seq.ctypes.data, seq.size, offs.ctypes.data,
+                                             lens.ctypes.data, C.byref(opt), C.byref(hmm), a_off.ctypes.data,
+                                             a.ctypes.data, a.size)
+        if r != tot:
+            raise RuntimeError("pl_seed_anchors_hmm_host: " + L.error())
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    for q in range(0, n, 97):  # parity on a sample: the restatement, pinned to the reference
+        want = O.anchors_hmm(ki, kb, 6, 1, max_occ, prots[q], emits[q], pos_loss, win_loss, seed_max)
+        if not np.array_equal(a[a_off[q]:a_off[q + 1]], want):
+            raise RuntimeError(f"HMM seeding parity: profile {q}")
+    clocks = Clocks(R.local)
+    eng.set_timing(True)
+    launches0 = L.load().pl_kernel_launch_count()
+    R.barrier()
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    te = R.max((time.perf_counter() - t0) / args.steps)
+    clk = clocks.stop()
+    launches = L.load().pl_kernel_launch_count() - launches0
+    k_s = R.max(eng.times()["dp_ms"] / 1e3 / args.steps)
+    r = cpu_sample(args.cpu_seconds / 2) if R.is_root else None
+    hbm = hbm_peak()
+    if R.is_root:
+        line = {"metric": metric, "value": round(R.sum(int(tot)) / k_s, 1), "unit": "anchors/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": round(k_s * 1e3, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "uint64", "data": "synthetic",
+                "config": {"workload": desc, "anchors_per_step": int(tot), "profiles": n,
+                           "l2": "the index (464 MB) exceeds L2"},
+                "e2e": {"value": round(R.sum(int(tot)) / te, 1), "unit": "anchors/s", "ms_per_step": round(te * 1e3, 3),
+                        "h2d_bytes_per_step": int(seq.nbytes + offs.nbytes + lens.nbytes + emit.nbytes + e_off.nbytes
+                                                  + e_len.nbytes + (n + 1) * 8 + a_off.nbytes),
+                        "d2h_bytes_per_step": int(tot) * 8 + n * 8,
+                        "api": "pl_seed_anchors_hmm_host (C ABI, host buffers), wall clock"},
+                "gpu_launches": int(launches),
+                "roofline": {"bound": "hbm", "kernel": "k_seed_emit + segmented sorts",
+                             "achieved": round(int(tot) * SEED_BYTES_PER_ANCHOR / k_s / 1e9, 2), "unit": "GB/s",
+                             "peak": hbm[0], "frac": round(int(tot) * SEED_BYTES_PER_ANCHOR / k_s / 1e9 / hbm[0], 4),
+                             "peak_source": hbm[1], "traffic": None,
+                             "note": "algorithmic bytes: the anchor written and its block id read; the profile "
+                                     "windows' walk, the seeds' sort and deduplication are on top"},
+                "clocks": clk}
+        if r is not None:
+            line["cpu_baseline"] = {"value": round(r[0], 1), "unit": "anchors/s", "cores": threads, "kind": "reference",
+                                    "sample": f"{r[1]} of {n} profiles, the reference's seeding steps per parsed "
+                                              "profile over a thread pool"}
         print(json.dumps(line), flush=True)
     idx.close()
     eng.close()

@@ -84,27 +84,21 @@ int64_t ref_sketch_hmm(const int16_t *emit, int32_t len, int32_t kmer, int32_t m
 	return sd.n;
 }
 
-/* a profile read from an HMMER3 text file by the reference's parser (hmm.c:112-195), its
- * consensus the query and its name the query name, as mp_map_hmm_file runs it
- * (map.c:1184-1196): the seeds of mp_sketch_query (consensus and profile-derived, sorted
- * and deduplicated, map.c:332-343) when ki is NULL, else the anchors of mp_map_coarse's
- * seeding steps (map.c:565-572), with the accuracy mode's repeat rescue when
- * repeat_cap > 0 */
-__attribute__((visibility("default")))
-int64_t ref_seed_hmm_query(const char *hmm_path, const int64_t *ki, const uint32_t *kb, int64_t n_kb, int32_t kmer,
+/* a profile read by the reference's parser (hmm.c:112-195), its consensus the query and
+ * its name the query name, as mp_map_hmm_file runs it (map.c:1184-1196): the seeds of
+ * mp_sketch_query (consensus and profile-derived, sorted and deduplicated, map.c:332-343)
+ * when ki is NULL, else the anchors of mp_map_coarse's seeding steps (map.c:565-572), with
+ * the accuracy mode's repeat rescue when repeat_cap > 0 */
+static int64_t ref_hmm_seed_steps(mp_hmm_t *h, const int64_t *ki, const uint32_t *kb, int64_t n_kb, int32_t kmer,
 		int32_t mod_bit, int32_t max_occ_opt, int32_t repeat_cap, int64_t anchor_budget, int32_t pos_loss,
 		int32_t win_loss, int32_t seed_max, uint64_t **out)
 {
 	mp_idx_t mi;
 	mp_mapopt_t opt;
 	mp64_v sd = {0, 0, 0};
-	mp_hmm_t *h = mp_hmm_read(hmm_path);
-	const char *cons;
-	int32_t max_occ, qlen;
+	const char *cons = mp_hmm_consensus(h);
+	int32_t max_occ, qlen = mp_hmm_length(h);
 	int64_t n_a = 0, n_rescued = 0;
-	*out = 0;
-	if (!h) return -1;
-	cons = mp_hmm_consensus(h), qlen = mp_hmm_length(h);
 	mp_mapopt_init(&opt);
 	opt.hmm = h, opt.max_occ = max_occ_opt;
 	opt.hmm_seed_pos_loss = pos_loss, opt.hmm_seed_win_loss = win_loss;
@@ -114,7 +108,6 @@ int64_t ref_seed_hmm_query(const char *hmm_path, const int64_t *ki, const uint32
 	}
 	mp_sketch_query(0, &opt, cons, qlen, kmer, mod_bit, seed_max, &sd);
 	if (!ki) {
-		mp_hmm_destroy(h);
 		*out = sd.a;
 		return sd.n;
 	}
@@ -129,8 +122,37 @@ int64_t ref_seed_hmm_query(const char *hmm_path, const int64_t *ki, const uint32
 	*out = mp_collect_anchors(0, &mi, &opt, &sd, max_occ, mp_hmm_name(h), &n_a, &n_rescued);
 	kfree(0, sd.a);
 	radix_sort_mp64(*out, *out + n_a);
-	mp_hmm_destroy(h);
 	return n_a;
+}
+
+/* the same on an HMMER3 file, read for this call */
+__attribute__((visibility("default")))
+int64_t ref_seed_hmm_query(const char *hmm_path, const int64_t *ki, const uint32_t *kb, int64_t n_kb, int32_t kmer,
+		int32_t mod_bit, int32_t max_occ_opt, int32_t repeat_cap, int64_t anchor_budget, int32_t pos_loss,
+		int32_t win_loss, int32_t seed_max, uint64_t **out)
+{
+	mp_hmm_t *h = mp_hmm_read(hmm_path);
+	int64_t n;
+	*out = 0;
+	if (!h) return -1;
+	n = ref_hmm_seed_steps(h, ki, kb, n_kb, kmer, mod_bit, max_occ_opt, repeat_cap, anchor_budget, pos_loss, win_loss,
+			seed_max, out);
+	mp_hmm_destroy(h);
+	return n;
+}
+
+/* a profile read once (ref_hmm_load) and seeded many times (ref_seed_hmm_run), for timing
+ * the reference's seeding without its parser */
+__attribute__((visibility("default"))) void *ref_hmm_load(const char *hmm_path) { return mp_hmm_read(hmm_path); }
+__attribute__((visibility("default"))) void ref_hmm_free(void *h) { mp_hmm_destroy((mp_hmm_t*)h); }
+__attribute__((visibility("default")))
+int64_t ref_seed_hmm_run(void *h, const int64_t *ki, const uint32_t *kb, int64_t n_kb, int32_t kmer, int32_t mod_bit,
+		int32_t max_occ_opt, int32_t pos_loss, int32_t win_loss, int32_t seed_max, uint64_t **out)
+{
+	*out = 0;
+	if (!h) return -1;
+	return ref_hmm_seed_steps((mp_hmm_t*)h, ki, kb, n_kb, kmer, mod_bit, max_occ_opt, 0, 0, pos_loss, win_loss,
+			seed_max, out);
 }
 
 /* the consensus the reference's parser derives (hmm.c:181-189), len + 1 bytes with the 0 */

@@ -101,6 +101,14 @@ def parse_hmmer3(text: str):
     return out
 
 
+def consensus(emit) -> bytes:
+    """A profile's consensus as the parser derives it (hmm.c:181-189): per match state the
+    HMMER letter of its largest emission, the first column among equal ones.  An HMM-profile
+    query is mapped as this sequence (map.c:1184-1196)."""
+    e = np.asarray(emit, dtype=np.int16).reshape(-1, 20)
+    return bytes(ord(ALPHABET[int(j)]) for j in np.argmax(e, axis=1))
+
+
 def _fmt(p: float) -> str:
     return "*" if p <= 0 else f"{-math.log(p):.5f}"
 

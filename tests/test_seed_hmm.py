@@ -264,3 +264,13 @@ def test_hmm_query_rescue_equals_reference(tmp_path, cap, budget):
             port = O.anchors_hmm(ki, kb, 6, 1, 20, cons, emit, pos_loss, win_loss, mx, repeat_cap=cap, budget=budget,
                                  qname=name)
             assert np.array_equal(ref, port), (path, cap, budget, mx, ref.size, port.size)
+
+
+@need_ref
+def test_package_consensus_equals_reference_parser(tmp_path):
+    """protlocus_b200.hmm.consensus, the query an HMM-profile mapping seeds from, equals the
+    consensus the reference's parser stores (hmm.c:181-189), '*' emissions included."""
+    from protlocus_b200.hmm import consensus
+    for path in _profiles(tmp_path, 6, 71):
+        cons, emit = O.ref_hmm_tables(path)
+        assert consensus(emit) == cons == O.hmm_consensus(emit)
