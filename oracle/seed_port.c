@@ -1,7 +1,7 @@
 /*
  * seed_port.c -- test infrastructure: a plain C restatement of the coarse mapper's
- * seeding (the checker of protlocus_b200/csrc/seed.cu), in the default mode (no
- * profile-derived seeds, no repeat rescue):
+ * seeding (the checker of protlocus_b200/csrc/seed.cu), for protein queries and for
+ * HMM-profile queries (sp_sketch_hmm, sp_seeds_hmm_query, sp_anchors_hmm below):
  *
  *   sketch    mp_sketch_prot (sketch.c:18-37): residues in the 13-letter alphabet of
  *             nasw-tab.c:12 (codes 14 and 15, '*', 'X' and other bytes, restart the
