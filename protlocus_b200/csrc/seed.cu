@@ -330,7 +330,7 @@ extern "C" int plk_seed_hmm_alts(const plk_seed_args_t *a, void *stream)
 extern "C" int plk_seed_hmm_enum(const plk_seed_args_t *a, void *stream)
 {
 	if (a->n <= 0) return 0;
-	k_seed_hmm_enum<<<(unsigned)((a->n * 32 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*a);
+	k_seed_hmm_enum<<<(unsigned)(((int64_t)a->n * 32 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*a);
 	plk_add_launches(1);
 	return (int)cudaGetLastError();
 }
@@ -338,7 +338,7 @@ extern "C" int plk_seed_hmm_enum(const plk_seed_args_t *a, void *stream)
 extern "C" int plk_seed_unique(const plk_seed_args_t *a, const uint64_t *sorted, void *stream)
 {
 	if (a->n <= 0) return 0;
-	k_seed_unique<<<(unsigned)((a->n * 32 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*a, sorted);
+	k_seed_unique<<<(unsigned)(((int64_t)a->n * 32 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*a, sorted);
 	plk_add_launches(1);
 	return (int)cudaGetLastError();
 }
@@ -346,7 +346,7 @@ extern "C" int plk_seed_unique(const plk_seed_args_t *a, const uint64_t *sorted,
 extern "C" int plk_seed_sketch(const plk_seed_args_t *a, void *stream)
 {
 	if (a->n <= 0) return 0;
-	k_seed_sketch<<<(unsigned)((a->n * 32 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*a);
+	k_seed_sketch<<<(unsigned)(((int64_t)a->n * 32 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*a);
 	plk_add_launches(1);
 	return (int)cudaGetLastError();
 }
@@ -354,7 +354,7 @@ extern "C" int plk_seed_sketch(const plk_seed_args_t *a, void *stream)
 extern "C" int plk_seed_take(const plk_seed_args_t *a, void *stream)
 {
 	if (a->n <= 0) return 0;
-	k_seed_take<<<(unsigned)((a->n * 32 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*a);
+	k_seed_take<<<(unsigned)(((int64_t)a->n * 32 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*a);
 	plk_add_launches(1);
 	return (int)cudaGetLastError();
 }
@@ -362,7 +362,7 @@ extern "C" int plk_seed_take(const plk_seed_args_t *a, void *stream)
 extern "C" int plk_seed_emit(const plk_seed_args_t *a, void *stream)
 {
 	if (a->n <= 0) return 0;
-	k_seed_emit<<<(unsigned)((a->n * 32 + 32 * SD_EMIT_WARPS - 1) / (32 * SD_EMIT_WARPS)), 32 * SD_EMIT_WARPS, 0,
+	k_seed_emit<<<(unsigned)(((int64_t)a->n * 32 + 32 * SD_EMIT_WARPS - 1) / (32 * SD_EMIT_WARPS)), 32 * SD_EMIT_WARPS, 0,
 			(cudaStream_t)stream>>>(*a);
 	plk_add_launches(1);
 	return (int)cudaGetLastError();
